@@ -1,0 +1,157 @@
+/*
+ * shmap-b200: C ABI of the B200 long-read mapping path (libshmapgpu.so).
+ *
+ * The reference (shmap-rs v1.4.3, crate `shmap`) exposes this path through its
+ * Rust API and the `shmap -s -p -k -r -t -m` command line; it has no FFI of its
+ * own. These entry points are what a Rust (or any C-ABI) host binds to replace
+ * that API one call for one call. Each declaration names the reference
+ * function it stands in for.
+ *
+ * Conventions: every call returns an int status (SHM_OK = 0, negative on
+ * error). Host buffers are caller-owned; device buffers are owned by the
+ * context or the index. A context serves one host thread at a time.
+ * Sequences are raw ASCII bytes exactly as the reference's FASTA reader hands
+ * them to FracMinHash::sketch (any case; bytes other than ACGTacgt hash as 0).
+ */
+#ifndef SHMAP_GPU_H
+#define SHMAP_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    SHM_OK = 0,
+    SHM_ERR_INVALID = -1,   /* bad argument (message via shm_last_error) */
+    SHM_ERR_CUDA = -2,      /* CUDA runtime error */
+    SHM_ERR_NOMEM = -3,     /* device allocation failed / over the HBM budget */
+    SHM_ERR_CAPACITY = -4,  /* an output buffer is too small */
+    SHM_ERR_TIMEOUT = -5    /* a bounded device wait ran out */
+};
+
+/* Metric (src/types.rs:299-322). bucket_LCS is not on the device path. */
+enum { SHM_CONTAINMENT = 0, SHM_JACCARD = 1, SHM_BUCKET_SH = 2 };
+
+/* Mapping parameters: the fields of Params (src/params.rs:20-186) that the
+ * mapping path reads. Defaults are the CLI defaults (shm_params_default). */
+typedef struct shm_params {
+    int32_t k;              /* -k */
+    double h_frac;          /* -r */
+    int32_t max_matches;    /* -M, -1 = none */
+    double theta;           /* -t */
+    double min_diff;        /* -d */
+    double max_overlap;     /* -o */
+    int32_t metric;         /* -m */
+    int32_t no_bucket_pruning; /* -P (NBP) */
+    int32_t one_sweep;      /* -B (OS) */
+    int32_t abs_pos;        /* -F (AP) */
+} shm_params;
+
+/* One read's outcome: everything the reference's PAF line is made of
+ * (src/mapping.rs:87-107, 161-182, 228-247; src/shmap/mod.rs:871-943).
+ * status: 0 mapped, 1 nothing cleared -t, 2 sketch below MIN_HALFLEN
+ * (src/shmap/mod.rs:750-783), 3 internal capacity exceeded (retried). */
+typedef struct shm_map_record {
+    double score, sh, score2;
+    int32_t status;
+    int32_t read_len, sketch_size, seeds;
+    int32_t p_start, p_end, segm_id, t_l, t_r;
+    int32_t same_strand, intersection, s_sz;
+    int32_t bucket_seg, bucket_b;
+    int32_t has_second, intersection2, bucket2_seg, bucket2_b;
+    int32_t total_matches, max_seed_matches, seed_matches, seeded_buckets, final_buckets;
+    int32_t reserved;
+} shm_map_record;
+#ifdef __cplusplus
+static_assert(sizeof(shm_map_record) == 120, "shm_map_record layout is part of the ABI");
+#endif
+
+/* SketchIndex statistics (src/index.rs:343-376, printed by index.rs:665-700). */
+typedef struct shm_index_stats {
+    int64_t segments, total_nucls, indexed_hits, indexed_kmers, highest_freq_kmer;
+    int64_t blacklisted_kmers, blacklisted_hits, sketched_kmers;
+} shm_index_stats;
+
+typedef struct shm_ctx shm_ctx;
+typedef struct shm_index shm_index;
+
+/* Last error message of this thread (static storage). */
+const char* shm_last_error(void);
+
+/* Fills the CLI defaults of src/params.rs:29-116. */
+void shm_params_default(shm_params* p);
+
+/* Params::validate (src/params.rs:191-263): SHM_OK or SHM_ERR_INVALID with the
+ * reference's message in shm_last_error(). */
+int shm_params_validate(const shm_params* p);
+
+/* A device context: one CUDA device, one stream, grow-only scratch.
+ * hbm_budget bytes (0 = no limit) bounds the scratch the context keeps. */
+int shm_ctx_create(int device, size_t hbm_budget, shm_ctx** out);
+int shm_ctx_destroy(shm_ctx* ctx);
+
+/* FracMinHash::sketch_slice_into (src/sketch.rs:167-209) for one host
+ * sequence: writes up to cap k-mers (r, h, strand) in sequence order and the
+ * total count to *n_out (SHM_ERR_CAPACITY if it exceeds cap). */
+int shm_sketch(shm_ctx* ctx, const uint8_t* seq, int64_t len, int32_t k, double h_frac, int32_t offset,
+               int32_t* r, uint64_t* h, uint8_t* strand, int64_t cap, int64_t* n_out);
+
+/* FracMinHash::h_thres (src/sketch.rs:126-132). */
+uint64_t shm_h_thres(double h_frac);
+
+/* SketchIndex::build_index (src/index.rs:384-663) from segments already read:
+ * `seq` holds every segment's bases back to back, seg_off[n_seg+1] are byte
+ * offsets, names are '\n'-joined (file order = segm_id order). */
+int shm_index_build(shm_ctx* ctx, const uint8_t* seq, const int64_t* seg_off, int32_t n_seg, const char* names,
+                    int32_t k, double h_frac, int32_t max_matches, shm_index** out);
+int shm_index_destroy(shm_index* idx);
+int shm_index_stats_get(const shm_index* idx, shm_index_stats* out);
+
+/* SketchIndex::count (src/index.rs:204-213) for n hashes. */
+int shm_index_count(shm_ctx* ctx, const shm_index* idx, const uint64_t* h, int64_t n, int32_t* out);
+
+/* SketchIndex::single_hit / multi_hits (src/index.rs:192-201): the hit list of
+ * one hash in (segm_id, r) order; *n_out = its length. */
+int shm_index_hits(shm_ctx* ctx, const shm_index* idx, uint64_t h, int32_t* segm_id, int32_t* tpos, int32_t* r,
+                   uint8_t* strand, int64_t cap, int64_t* n_out);
+
+/* RefSegment::kmers of one segment (src/sketch.rs:16-27). */
+int shm_index_segment(shm_ctx* ctx, const shm_index* idx, int32_t seg, int32_t* r, uint64_t* h, uint8_t* strand,
+                      int64_t cap, int64_t* n_out, char* name, int32_t name_cap, int32_t* seg_len);
+
+/* Mapper::map_reads / SHMapper::map_read (src/mapper.rs:15-17,
+ * src/shmap/mod.rs:374-971) for n host reads: seqs holds the reads back to
+ * back with offs[n+1] byte offsets. One record per read, in input order.
+ * Reads are cut into device batches; host<->device copies are inside. */
+int shm_map_batch(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
+                  int32_t n, shm_map_record* out);
+
+/* The same for reads already in device memory (d_seqs 16-byte aligned with 16
+ * readable bytes past the end; d_offs device, h_offs the same offsets on the
+ * host); d_out is device memory. Used to time the device path alone. */
+int shm_map_batch_device(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* d_seqs,
+                         const int64_t* d_offs, const int64_t* h_offs, int32_t n, shm_map_record* d_out);
+
+/* One read per call, every stage launched for that read alone: the plain
+ * one-read-per-launch GPU form the batched path is compared against. */
+int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
+                  int32_t n, shm_map_record* out);
+
+/* PAF text of the mapped reads (src/mapping.rs:87-107, 161-182, 228-247;
+ * src/shmap/mod.rs:871-943): one line per record with status 0, t:f: from
+ * map_time[i] (NULL = 0). names are '\n'-joined. Returns the bytes needed in
+ * *n_out; writes at most cap bytes. */
+int shm_format_paf(const shm_index* idx, const shm_params* p, const shm_map_record* rec, int32_t n, const char* names,
+                   const double* map_time, char* buf, int64_t cap, int64_t* n_out);
+
+/* Kernel launches this context issued so far (the bench reports the count
+ * inside its timed region). */
+int64_t shm_ctx_launches(const shm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SHMAP_GPU_H */

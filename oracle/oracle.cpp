@@ -8,8 +8,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <fstream>
-#include <sstream>
 #include <thread>
 
 namespace oracle {
@@ -517,11 +515,36 @@ static std::string ff(double x, int prec) {
     return buf;
 }
 
+// String building without iostreams (this library is loaded next to other
+// copies of the C++ runtime, and their stream locales must not meet).
+struct Out {
+    std::string s;
+    Out& operator<<(const std::string& v) {
+        s += v;
+        return *this;
+    }
+    Out& operator<<(const char* v) {
+        s += v;
+        return *this;
+    }
+    Out& operator<<(char v) {
+        s += v;
+        return *this;
+    }
+    Out& operator<<(long long v) {
+        char b[32];
+        std::snprintf(b, sizeof b, "%lld", v);
+        s += b;
+        return *this;
+    }
+    Out& operator<<(int32_t v) { return *this << (long long)v; }
+};
+
 std::string Mapping::paf(const std::string& query_id) const {
-    std::ostringstream o;
+    Out o;
     o << query_id << '\t' << read_len << '\t' << p_start << '\t' << p_end << '\t' << strand << '\t'
       << (segm ? segm->name : std::string()) << '\t' << (segm ? segm->sz : -1) << '\t' << t_l << '\t' << t_r << '\t'
-      << read_len << '\t' << read_len << '\t' << (int)mapq;
+      << read_len << '\t' << read_len << '\t' << (int32_t)mapq;
     o << "\tp:i:" << p_sz << "\ts:i:" << s_sz << "\tI:i:" << intersection << "\tI2:i:" << intersection2
       << "\tIdiff:i:" << (int32_t)(intersection - intersection2) << "\tIsdiff:f:" << ff(sigmas_diff, 5)
       << "\tJ:f:" << ff(j, 5) << "\tJ2:f:" << ff(j2, 5) << "\tJdiff:f:" << ff(j - j2, 5) << "\tsh:f:" << ff(sh, 5)
@@ -533,13 +556,13 @@ std::string Mapping::paf(const std::string& query_id) const {
           << "\tseed_matches:i:" << seed_matches << "\ttotal_matches:i:" << total_matches
           << "\tmatch_inefficiency:f:" << ff(match_inefficiency, 3) << "\tseeded_buckets:i:" << seeded_buckets
           << "\tfinal_buckets:i:" << final_buckets << "\tFPTP:f:" << ff(fptp, 3);
-    return o.str();
+    return o.s;
 }
 
 std::string unmapped_line(const std::string& query_id, QPos read_len) {
-    std::ostringstream o;
+    Out o;
     o << query_id << '\t' << read_len << "\t0\t0\t*\t*\t0\t0\t0\t0\t0\t0";
-    return o.str();
+    return o.s;
 }
 
 // ---------------------------------------------------------------- shmap/*.rs
@@ -991,12 +1014,15 @@ std::string render_paf(ReadResult& rr, const std::string& query_id, const Params
 
 // ---------------------------------------------------------------- io
 bool read_fasta(const std::string& path, std::vector<FastaRecord>& out, std::string* err) {
-    std::ifstream f(path, std::ios::binary);
+    FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) {
         if (err) *err = "failed to open " + path;
         return false;
     }
-    std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    std::string data;
+    char chunk[1 << 16];
+    for (size_t got; (got = std::fread(chunk, 1, sizeof chunk, f)) > 0;) data.append(chunk, got);
+    std::fclose(f);
     size_t pos = 0, n = data.size();
     FastaRecord* cur = nullptr;
     while (pos < n) {

@@ -1,0 +1,176 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes wrapper of the CPU oracle (liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use this, as
+the checker. It restates shmap-rs's mapping path sequentially in C++ (see
+oracle.hpp); the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+CLI = os.path.join(HERE, "shmap_oracle")
+
+METRICS = {"Containment": 0, "Jaccard": 1, "bucket_SH": 2, "bucket_LCS": 3}
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+class OParams(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_int32), ("h_frac", ctypes.c_double), ("max_matches", ctypes.c_int32),
+                ("theta", ctypes.c_double), ("min_diff", ctypes.c_double), ("max_overlap", ctypes.c_double),
+                ("metric", ctypes.c_int32), ("no_bucket_pruning", ctypes.c_int32), ("one_sweep", ctypes.c_int32),
+                ("abs_pos", ctypes.c_int32)]
+
+
+RECORD_DTYPE = np.dtype(
+    [("score", "<f8"), ("sh", "<f8"), ("score2", "<f8")]
+    + [(n, "<i4") for n in (
+        "status", "read_len", "sketch_size", "seeds", "p_start", "p_end", "segm_id", "t_l", "t_r",
+        "same_strand", "intersection", "s_sz", "bucket_seg", "bucket_b", "has_second", "intersection2",
+        "bucket2_seg", "bucket2_b", "total_matches", "max_seed_matches", "seed_matches",
+        "seeded_buckets", "final_buckets", "reserved")],
+    align=True,
+)
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        P, i32, i64, u64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+        for name, res, args in [
+            ("orc_sketch", i64, [P, i64, i32, dbl, i32, P, P, P, i64]),
+            ("orc_h_thres", u64, [i32, dbl]),
+            ("orc_index_build", P, [P, P, i32, ctypes.c_char_p, i32, dbl, i32, i32]),
+            ("orc_index_free", None, [P]),
+            ("orc_index_stats", None, [P, P]),
+            ("orc_index_count", None, [P, P, i64, P]),
+            ("orc_index_hits", i64, [P, u64, P, P, P, P, i64]),
+            ("orc_segment_sketch", i64, [P, i32, P, P, P, i64]),
+            ("orc_map", i32, [P, P, P, P, i32, i32, P]),
+            ("orc_paf", i64, [P, P, P, P, ctypes.c_char_p, i32, i32, P, i64]),
+            ("orc_time_map", dbl, [P, P, P, P, i32, i32]),
+        ]:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data if a.size else 0
+
+
+def params(k=15, h_frac=0.05, max_matches=None, theta=0.9, min_diff=0.02, max_overlap=0.5, metric="Containment",
+           no_bucket_pruning=False, one_sweep=False, abs_pos=False) -> OParams:
+    return OParams(k, h_frac, -1 if max_matches is None else max_matches, theta, min_diff, max_overlap,
+                   METRICS[metric], int(no_bucket_pruning), int(one_sweep), int(abs_pos))
+
+
+def sketch(seq: bytes, k: int, h_frac: float, offset: int = 0):
+    buf = np.frombuffer(seq, np.uint8)
+    cap = max(0, len(seq) - k + 1)
+    r = np.zeros(cap, np.int32)
+    h = np.zeros(cap, np.uint64)
+    st = np.zeros(cap, np.uint8)
+    n = lib().orc_sketch(_p(buf), len(seq), k, h_frac, offset, _p(r), _p(h), _p(st), cap)
+    return r[:n], h[:n], st[:n]
+
+
+def h_thres(h_frac: float, k: int = 15) -> int:
+    return int(lib().orc_h_thres(k, h_frac))
+
+
+class Index:
+    STATS = ("segments", "total_nucls", "indexed_hits", "indexed_kmers", "highest_freq_kmer",
+             "blacklisted_kmers", "blacklisted_hits", "sketched_kmers")
+
+    def __init__(self, names: Sequence[str], seq: np.ndarray, seg_off: np.ndarray, k: int, h_frac: float,
+                 max_matches: Optional[int] = None, threads: int = 1):
+        self.seq = np.ascontiguousarray(seq, np.uint8)
+        self.seg_off = np.ascontiguousarray(seg_off, np.int64)
+        self.names = list(names)
+        self.h = lib().orc_index_build(_p(self.seq), _p(self.seg_off), len(self.names),
+                                       "\n".join(self.names).encode(), k, h_frac,
+                                       -1 if max_matches is None else max_matches, threads)
+
+    @classmethod
+    def from_records(cls, records, k, h_frac, max_matches=None, threads=1):
+        seqs = [s for _, s in records]
+        off = np.zeros(len(seqs) + 1, np.int64)
+        off[1:] = np.cumsum([len(s) for s in seqs])
+        buf = np.frombuffer(b"".join(seqs), np.uint8) if seqs else np.zeros(0, np.uint8)
+        return cls([n for n, _ in records], buf, off, k, h_frac, max_matches, threads)
+
+    def __del__(self):
+        try:
+            lib().orc_index_free(self.h)
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        out = np.zeros(8, np.int64)
+        lib().orc_index_stats(self.h, _p(out))
+        return dict(zip(self.STATS, (int(x) for x in out)))
+
+    def count(self, hashes) -> np.ndarray:
+        hashes = np.ascontiguousarray(hashes, np.uint64)
+        out = np.zeros(len(hashes), np.int32)
+        lib().orc_index_count(self.h, _p(hashes), len(hashes), _p(out))
+        return out
+
+    def hits(self, h: int):
+        n = lib().orc_index_hits(self.h, h, 0, 0, 0, 0, 0)
+        seg, tpos, r = (np.zeros(n, np.int32) for _ in range(3))
+        st = np.zeros(n, np.uint8)
+        lib().orc_index_hits(self.h, h, _p(seg), _p(tpos), _p(r), _p(st), n)
+        return seg, tpos, r, st
+
+    def segment(self, i: int):
+        n = lib().orc_segment_sketch(self.h, i, 0, 0, 0, 0)
+        r = np.zeros(n, np.int32)
+        h = np.zeros(n, np.uint64)
+        st = np.zeros(n, np.uint8)
+        lib().orc_segment_sketch(self.h, i, _p(r), _p(h), _p(st), n)
+        return r, h, st
+
+    def map_reads(self, p: OParams, seq: np.ndarray, offs: np.ndarray, threads: int = 1) -> np.ndarray:
+        seq = np.ascontiguousarray(seq, np.uint8)
+        offs = np.ascontiguousarray(offs, np.int64)
+        out = np.zeros(len(offs) - 1, RECORD_DTYPE)
+        lib().orc_map(self.h, ctypes.byref(p), _p(seq), _p(offs), len(offs) - 1, threads, _p(out))
+        return out
+
+    def paf(self, p: OParams, seq: np.ndarray, offs: np.ndarray, names: Sequence[str], threads: int = 1) -> str:
+        seq = np.ascontiguousarray(seq, np.uint8)
+        offs = np.ascontiguousarray(offs, np.int64)
+        joined = "\n".join(names).encode()
+        n = lib().orc_paf(self.h, ctypes.byref(p), _p(seq), _p(offs), joined, len(offs) - 1, threads, 0, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        lib().orc_paf(self.h, ctypes.byref(p), _p(seq), _p(offs), joined, len(offs) - 1, threads, buf, n)
+        return buf.raw[:n].decode()
+
+    def time_map(self, p: OParams, seq: np.ndarray, offs: np.ndarray, threads: int) -> float:
+        seq = np.ascontiguousarray(seq, np.uint8)
+        offs = np.ascontiguousarray(offs, np.int64)
+        return float(lib().orc_time_map(self.h, ctypes.byref(p), _p(seq), _p(offs), len(offs) - 1, threads))
+
+
+def run_cli(args: Sequence[str]) -> subprocess.CompletedProcess:
+    if not os.path.exists(CLI):
+        build()
+    return subprocess.run([CLI, *args], capture_output=True, text=True)

@@ -1,0 +1,379 @@
+// The C ABI of include/shmap_gpu.h. Every entry point catches CUDA and host
+// errors and turns them into status codes; nothing here falls back to the CPU.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/shmap_gpu.h"
+#include "shm_common.cuh"
+#include "shm_internal.hpp"
+#include "shm_map.cuh"
+#include "shm_prims.cuh"
+#include "shm_sketch.cuh"
+
+struct shm_ctx {
+    shm::MapCtx* m = nullptr;
+};
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define SHM_GUARD_BEGIN try {
+#define SHM_GUARD_END                                                                                   \
+    }                                                                                                   \
+    catch (const shm_cuda_error& e) {                                                                   \
+        if (e.err == cudaErrorMemoryAllocation) return fail(SHM_ERR_NOMEM, cudaGetErrorString(e.err)); \
+        return fail(SHM_ERR_CUDA, cudaGetErrorString(e.err));                                         \
+    }                                                                                                   \
+    catch (const std::bad_alloc&) {                                                                     \
+        return fail(SHM_ERR_NOMEM, "host allocation failed");                                           \
+    }
+
+static std::vector<std::string> split_names(const char* joined, int32_t n) {
+    std::vector<std::string> v;
+    const char* s = joined ? joined : "";
+    for (int32_t i = 0; i < n; i++) {
+        const char* e = std::strchr(s, '\n');
+        if (!e) e = s + std::strlen(s);
+        v.emplace_back(s, (size_t)(e - s));
+        s = *e ? e + 1 : e;
+    }
+    return v;
+}
+
+extern "C" {
+
+const char* shm_last_error(void) { return g_err.c_str(); }
+
+void shm_params_default(shm_params* p) {
+    p->k = 15;
+    p->h_frac = 0.05;
+    p->max_matches = -1;
+    p->theta = 0.9;
+    p->min_diff = 0.02;
+    p->max_overlap = 0.5;
+    p->metric = SHM_CONTAINMENT;
+    p->no_bucket_pruning = 0;
+    p->one_sweep = 0;
+    p->abs_pos = 0;
+}
+
+static std::string fmt_g(double x) {  // Rust `{}` for an f64 that needs no exponent
+    char b[64];
+    std::snprintf(b, sizeof b, "%.17g", x);
+    // shortest representation that round-trips
+    for (int prec = 1; prec <= 17; prec++) {
+        std::snprintf(b, sizeof b, "%.*g", prec, x);
+        if (std::strtod(b, nullptr) == x) break;
+    }
+    return b;
+}
+
+int shm_params_validate(const shm_params* p) {
+    if (!p) return fail(SHM_ERR_INVALID, "null params");
+    if (p->k <= 0) return fail(SHM_ERR_INVALID, "K-mer length (-k) should be positive. You provided " + std::to_string(p->k) + ".");
+    if (!(p->h_frac > 0.0) || p->h_frac > 1.0)
+        return fail(SHM_ERR_INVALID, "Given hash ratio (-r) should be between 0 and 1. You provided " + fmt_g(p->h_frac) + ".");
+    if (p->max_matches != -1 && p->max_matches <= 0)
+        return fail(SHM_ERR_INVALID, "The number of seed matches (-M) should be positive. You provided " + std::to_string(p->max_matches) + ".");
+    if (p->theta < 0.0 || p->theta > 1.0)
+        return fail(SHM_ERR_INVALID, "The threshold (-t) should be between 0 and 1. You provided " + fmt_g(p->theta) + ".");
+    if (p->min_diff < 0.0)
+        return fail(SHM_ERR_INVALID, "The minimum difference (-d) should be >= 0. You provided " + fmt_g(p->min_diff) + ".");
+    if (p->max_overlap < 0.0 || p->max_overlap > 1.0)
+        return fail(SHM_ERR_INVALID, "The maximum overlap (-o) should be between 0 and 1. You provided " + fmt_g(p->max_overlap) + ".");
+    if (p->metric < SHM_CONTAINMENT || p->metric > SHM_BUCKET_SH)
+        return fail(SHM_ERR_INVALID, "unsupported metric on the device path (bucket_LCS is not implemented)");
+    return SHM_OK;
+}
+
+uint64_t shm_h_thres(double h_frac) { return shm::h_thres(h_frac); }
+
+int shm_ctx_create(int device, size_t hbm_budget, shm_ctx** out) {
+    if (!out) return fail(SHM_ERR_INVALID, "null out");
+    SHM_GUARD_BEGIN
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(SHM_ERR_CUDA, "no CUDA device available");
+    if (device < 0 || device >= n) return fail(SHM_ERR_INVALID, "device index out of range");
+    auto* c = new shm_ctx();
+    c->m = shm::mapctx_create(device, hbm_budget);
+    *out = c;
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_ctx_destroy(shm_ctx* ctx) {
+    if (!ctx) return SHM_OK;
+    shm::mapctx_destroy(ctx->m);
+    delete ctx;
+    return SHM_OK;
+}
+
+int64_t shm_ctx_launches(const shm_ctx* ctx) { return ctx && ctx->m ? ctx->m->launches : 0; }
+
+int shm_sketch(shm_ctx* ctx, const uint8_t* seq, int64_t len, int32_t k, double h_frac, int32_t offset, int32_t* r,
+               uint64_t* h, uint8_t* strand, int64_t cap, int64_t* n_out) {
+    if (!ctx || !n_out || (len > 0 && !seq)) return fail(SHM_ERR_INVALID, "null argument");
+    if (k <= 0) return fail(SHM_ERR_INVALID, "K-mer length (-k) should be positive.");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(ctx->m->device));
+    cudaStream_t s = ctx->m->stream;
+    *n_out = 0;
+    if (len < k) return SHM_OK;
+    const int64_t nw = len - k + 1;
+    const uint64_t n_chunks = (uint64_t)((nw + shm::SKETCH_WIN - 1) / shm::SKETCH_WIN);
+    shm::DevBuf<uint8_t> d_seq;
+    shm::DevBuf<int64_t> d_off;
+    shm::DevBuf<uint64_t> d_coff, d_h;
+    shm::DevBuf<uint32_t> d_cnt, d_out, d_rs;
+    d_seq.reserve((size_t)len + 32);
+    SHM_CUDA(cudaMemsetAsync(d_seq.p + len, 0, 32, s));
+    SHM_CUDA(cudaMemcpyAsync(d_seq.p, seq, (size_t)len, cudaMemcpyHostToDevice, s));
+    int64_t off[2] = {0, len};
+    uint64_t coff[2] = {0, n_chunks};
+    d_off.reserve(2);
+    d_coff.reserve(2);
+    SHM_CUDA(cudaMemcpyAsync(d_off.p, off, sizeof off, cudaMemcpyHostToDevice, s));
+    SHM_CUDA(cudaMemcpyAsync(d_coff.p, coff, sizeof coff, cudaMemcpyHostToDevice, s));
+    d_cnt.reserve(n_chunks + 1);
+    d_out.reserve(n_chunks + 1);
+    shm::SketchLuts* L = shm::create_device_luts(k, s);
+    shm::SketchArgs a{};
+    a.seq = d_seq.p;
+    a.seq_off = d_off.p;
+    a.chunk_off = d_coff.p;
+    a.n_seq = 1;
+    a.n_chunks = n_chunks;
+    a.k = k;
+    a.thr = shm::h_thres(h_frac);
+    a.r_offset = offset;
+    a.chunk_cnt = d_cnt.p;
+    shm::launch_sketch(shm::SK_COUNT, a, L, s);
+    shm::exclusive_scan_u32(d_cnt.p, d_out.p, n_chunks, s);
+    uint32_t total = 0;
+    SHM_CUDA(cudaMemcpyAsync(&total, d_out.p + n_chunks, sizeof total, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaStreamSynchronize(s));
+    d_h.reserve((size_t)total + 1);
+    d_rs.reserve((size_t)total + 1);
+    a.chunk_out = d_out.p;
+    a.out_h = d_h.p;
+    a.out_rs = d_rs.p;
+    shm::launch_sketch(shm::SK_WRITE, a, L, s);
+    ctx->m->launches += 3;
+    std::vector<uint64_t> hh(total);
+    std::vector<uint32_t> rs(total);
+    SHM_CUDA(cudaMemcpyAsync(hh.data(), d_h.p, sizeof(uint64_t) * total, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(rs.data(), d_rs.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaStreamSynchronize(s));
+    SHM_CUDA(cudaFree(L));
+    *n_out = total;
+    if ((int64_t)total > cap) return fail(SHM_ERR_CAPACITY, "output capacity too small");
+    for (uint32_t i = 0; i < total; i++) {
+        if (r) r[i] = (int32_t)(rs[i] >> 1);
+        if (h) h[i] = hh[i];
+        if (strand) strand[i] = (uint8_t)(rs[i] & 1u);
+    }
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_index_build(shm_ctx* ctx, const uint8_t* seq, const int64_t* seg_off, int32_t n_seg, const char* names,
+                    int32_t k, double h_frac, int32_t max_matches, shm_index** out) {
+    if (!ctx || !out || !seg_off || n_seg < 0) return fail(SHM_ERR_INVALID, "null argument");
+    if (k <= 0) return fail(SHM_ERR_INVALID, "K-mer length (-k) should be positive.");
+    if (!(h_frac > 0.0) || h_frac > 1.0) return fail(SHM_ERR_INVALID, "Given hash ratio (-r) should be between 0 and 1.");
+    if (max_matches != -1 && max_matches <= 0) return fail(SHM_ERR_INVALID, "The number of seed matches (-M) should be positive.");
+    uint64_t windows = 0;
+    for (int32_t i = 0; i < n_seg; i++) {
+        int64_t L = seg_off[i + 1] - seg_off[i];
+        if (L < 0 || L > INT32_MAX) return fail(SHM_ERR_INVALID, "segment length out of range (0 .. 2^31-1)");
+        if (L >= k) windows += (uint64_t)(L - k + 1);
+    }
+    if (windows >= 0xfffffff0ULL) return fail(SHM_ERR_INVALID, "more than 2^32 reference windows");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(ctx->m->device));
+    auto* ix = new shm_index();
+    ix->s = shm::build_index(seq, seg_off, n_seg, split_names(names, n_seg), k, h_frac, max_matches, ctx->m->stream);
+    ctx->m->launches += 40;
+    *out = ix;
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_index_destroy(shm_index* idx) {
+    if (!idx) return SHM_OK;
+    if (idx->s) {
+        cudaSetDevice(idx->s->device);
+        delete idx->s;
+    }
+    delete idx;
+    return SHM_OK;
+}
+
+int shm_index_stats_get(const shm_index* idx, shm_index_stats* out) {
+    if (!idx || !out) return fail(SHM_ERR_INVALID, "null argument");
+    *out = idx->s->stats;
+    return SHM_OK;
+}
+
+__global__ void k_count(shm::DevIndex I, const uint64_t* h, int64_t n, int32_t* out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t a, c;
+        shm::idx_lookup(I, h[i], a, c);
+        out[i] = (int32_t)c;
+    }
+}
+
+__global__ void k_one_list(shm::DevIndex I, uint64_t h, uint32_t* ac) {
+    uint32_t a, c;
+    shm::idx_lookup(I, h, a, c);
+    ac[0] = a;
+    ac[1] = c;
+}
+
+int shm_index_count(shm_ctx* ctx, const shm_index* idx, const uint64_t* h, int64_t n, int32_t* out) {
+    if (!ctx || !idx || (n > 0 && (!h || !out))) return fail(SHM_ERR_INVALID, "null argument");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(ctx->m->device));
+    if (n == 0) return SHM_OK;
+    cudaStream_t s = ctx->m->stream;
+    shm::DevBuf<uint64_t> dh;
+    shm::DevBuf<int32_t> dout;
+    dh.reserve((size_t)n);
+    dout.reserve((size_t)n);
+    SHM_CUDA(cudaMemcpyAsync(dh.p, h, sizeof(uint64_t) * (size_t)n, cudaMemcpyHostToDevice, s));
+    k_count<<<shm::grid_for((size_t)n, 256), 256, 0, s>>>(idx->s->dev, dh.p, n, dout.p);
+    SHM_CUDA(cudaGetLastError());
+    ctx->m->launches++;
+    SHM_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaStreamSynchronize(s));
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_index_hits(shm_ctx* ctx, const shm_index* idx, uint64_t h, int32_t* segm_id, int32_t* tpos, int32_t* r,
+                   uint8_t* strand, int64_t cap, int64_t* n_out) {
+    if (!ctx || !idx || !n_out) return fail(SHM_ERR_INVALID, "null argument");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(ctx->m->device));
+    cudaStream_t s = ctx->m->stream;
+    const shm::IndexStorage* ix = idx->s;
+    shm::DevBuf<uint32_t> ac;
+    ac.reserve(2);
+    k_one_list<<<1, 1, 0, s>>>(ix->dev, h, ac.p);
+    SHM_CUDA(cudaGetLastError());
+    ctx->m->launches++;
+    uint32_t hac[2];
+    SHM_CUDA(cudaMemcpyAsync(hac, ac.p, sizeof hac, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaStreamSynchronize(s));
+    *n_out = hac[1];
+    if ((int64_t)hac[1] > cap) return fail(SHM_ERR_CAPACITY, "output capacity too small");
+    std::vector<uint32_t> g(hac[1]), rs(hac[1]);
+    if (hac[1]) {
+        SHM_CUDA(cudaMemcpy(g.data(), ix->hits.p + hac[0], sizeof(uint32_t) * hac[1], cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < hac[1]; i++)
+            SHM_CUDA(cudaMemcpy(&rs[i], ix->ref_rs.p + g[i], sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
+    for (uint32_t i = 0; i < hac[1]; i++) {
+        int32_t sg = (int32_t)(std::upper_bound(ix->h_seg_off.begin(), ix->h_seg_off.end(), g[i]) - ix->h_seg_off.begin()) - 1;
+        // a segment with no k-mers shares its offset with the next one: take the last segment starting at or before g
+        if (segm_id) segm_id[i] = sg;
+        if (tpos) tpos[i] = (int32_t)(g[i] - ix->h_seg_off[(size_t)sg]);
+        if (r) r[i] = (int32_t)(rs[i] >> 1);
+        if (strand) strand[i] = (uint8_t)(rs[i] & 1u);
+    }
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_index_segment(shm_ctx* ctx, const shm_index* idx, int32_t seg, int32_t* r, uint64_t* h, uint8_t* strand,
+                      int64_t cap, int64_t* n_out, char* name, int32_t name_cap, int32_t* seg_len) {
+    if (!ctx || !idx || !n_out) return fail(SHM_ERR_INVALID, "null argument");
+    const shm::IndexStorage* ix = idx->s;
+    if (seg < 0 || seg >= (int32_t)ix->names.size()) return fail(SHM_ERR_INVALID, "segment out of range");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(ctx->m->device));
+    const uint32_t a = ix->h_seg_off[(size_t)seg], b = ix->h_seg_off[(size_t)seg + 1];
+    *n_out = b - a;
+    if (seg_len) *seg_len = ix->seg_len[(size_t)seg];
+    if (name && name_cap > 0) {
+        std::snprintf(name, (size_t)name_cap, "%s", ix->names[(size_t)seg].c_str());
+    }
+    if ((int64_t)(b - a) > cap) return fail(SHM_ERR_CAPACITY, "output capacity too small");
+    std::vector<uint64_t> hh(b - a);
+    std::vector<uint32_t> rs(b - a);
+    if (b > a) {
+        SHM_CUDA(cudaMemcpy(hh.data(), ix->ref_h.p + a, sizeof(uint64_t) * (b - a), cudaMemcpyDeviceToHost));
+        SHM_CUDA(cudaMemcpy(rs.data(), ix->ref_rs.p + a, sizeof(uint32_t) * (b - a), cudaMemcpyDeviceToHost));
+    }
+    for (uint32_t i = 0; i < b - a; i++) {
+        if (r) r[i] = (int32_t)(rs[i] >> 1);
+        if (h) h[i] = hh[i];
+        if (strand) strand[i] = (uint8_t)(rs[i] & 1u);
+    }
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+static int check_map_args(shm_ctx* ctx, const shm_index* idx, const shm_params* p, int32_t n) {
+    if (!ctx || !idx || !p || n < 0) return fail(SHM_ERR_INVALID, "null argument");
+    int v = shm_params_validate(p);
+    if (v != SHM_OK) return v;
+    if (p->k != idx->s->k) return fail(SHM_ERR_INVALID, "params.k differs from the index's k");
+    if (p->h_frac != idx->s->h_frac) return fail(SHM_ERR_INVALID, "params.h_frac differs from the index's h_frac");
+    return SHM_OK;
+}
+
+static int check_reads(const int64_t* offs, int32_t n) {
+    for (int32_t i = 0; i < n; i++) {
+        int64_t L = offs[i + 1] - offs[i];
+        if (L < 0 || L >= ((int64_t)1 << 30)) return fail(SHM_ERR_INVALID, "read length out of range (0 .. 2^30-1)");
+    }
+    return SHM_OK;
+}
+
+int shm_map_batch(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
+                  int32_t n, shm_map_record* out) {
+    int v = check_map_args(ctx, idx, p, n);
+    if (v != SHM_OK) return v;
+    if (n > 0 && (!seqs || !offs || !out)) return fail(SHM_ERR_INVALID, "null argument");
+    if ((v = check_reads(offs, n)) != SHM_OK) return v;
+    SHM_GUARD_BEGIN
+    shm::map_host(ctx->m, idx->s, *p, seqs, offs, n, out, false);
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
+                  int32_t n, shm_map_record* out) {
+    int v = check_map_args(ctx, idx, p, n);
+    if (v != SHM_OK) return v;
+    if (n > 0 && (!seqs || !offs || !out)) return fail(SHM_ERR_INVALID, "null argument");
+    if ((v = check_reads(offs, n)) != SHM_OK) return v;
+    SHM_GUARD_BEGIN
+    shm::map_host(ctx->m, idx->s, *p, seqs, offs, n, out, true);
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_map_batch_device(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* d_seqs,
+                         const int64_t* d_offs, const int64_t* h_offs, int32_t n, shm_map_record* d_out) {
+    (void)d_offs;
+    int v = check_map_args(ctx, idx, p, n);
+    if (v != SHM_OK) return v;
+    if (n > 0 && (!d_seqs || !h_offs || !d_out)) return fail(SHM_ERR_INVALID, "null argument");
+    if ((v = check_reads(h_offs, n)) != SHM_OK) return v;
+    SHM_GUARD_BEGIN
+    shm::map_device(ctx->m, idx->s, *p, d_seqs, h_offs, n, d_out, false);
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+}  // extern "C"

@@ -1,0 +1,340 @@
+// The reference index built on the device (SketchIndex::build_index,
+// src/index.rs:384-663).
+//
+// 1. Every segment is sketched in order (count, scan, write) so reference
+//    k-mer ids (gidx) run in (segment file order, tpos) order.
+// 2. (hash, gidx) pairs are radix-sorted stably by hash: each hash's hits come
+//    out in gidx order = (segm_id, r) order, the order finalize_shard gives its
+//    multi-hit lists (src/index.rs:295-315).
+// 3. Runs of equal hashes become a CSR (keys, key_off, hits). With -M, the
+//    reference keeps the first min(n, M+2) hits of a hash (insert_hit's cap,
+//    src/index.rs:286-288, plus the migrated single hit) and then erases every
+//    list longer than M (src/index.rs:360-376): a hash survives iff n <= M.
+// 4. hit_fw is the prefix count of forward-strand hits (codirection sums of a
+//    hit range in O(1)); dir maps the top bits of a hash to its first key.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "shm_common.cuh"
+#include "shm_internal.hpp"
+#include "shm_prims.cuh"
+#include "shm_sketch.cuh"
+
+namespace shm {
+
+uint64_t h_thres(double h_frac) {
+    if (h_frac < 1.0) {
+        double x = h_frac * (double)UINT64_MAX;
+        if (std::isnan(x) || x <= 0.0) return 0;
+        if (x >= 18446744073709551616.0) return UINT64_MAX;
+        return (uint64_t)x;
+    }
+    return UINT64_MAX;
+}
+
+__global__ void k_iota(uint32_t* v, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        v[i] = (uint32_t)i;
+}
+
+__global__ void k_seg_offsets(const uint64_t* __restrict__ chunk_off, const uint32_t* __restrict__ chunk_out,
+                              int32_t n_seg, uint32_t* __restrict__ seg_off) {
+    for (int32_t s = blockIdx.x * blockDim.x + threadIdx.x; s <= n_seg; s += gridDim.x * blockDim.x)
+        seg_off[s] = chunk_out[chunk_off[s]];
+}
+
+__global__ void k_key_flags(const uint64_t* __restrict__ ks, size_t n, uint32_t* __restrict__ flag) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        flag[i] = (i == 0 || ks[i] != ks[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_key_emit(const uint64_t* __restrict__ ks, size_t n, const uint32_t* __restrict__ fscan,
+                           uint64_t* __restrict__ keys, uint32_t* __restrict__ key_off) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (i == 0 || ks[i] != ks[i - 1]) {
+            uint32_t j = fscan[i];
+            keys[j] = ks[i];
+            key_off[j] = (uint32_t)i;
+        }
+    }
+}
+
+struct IdxStatsDev {
+    unsigned long long indexed_hits, blacklisted_kmers, blacklisted_hits, kept_keys, kept_hits;
+    unsigned int highest;
+};
+
+// Per-key cap/erase decision and statistics (src/index.rs:264-291, 343-376).
+__global__ void k_key_keep(const uint32_t* __restrict__ key_off, uint32_t n_keys, int32_t max_matches,
+                           uint32_t* __restrict__ keep, uint32_t* __restrict__ keep_hits, IdxStatsDev* st) {
+    unsigned long long ih = 0, bk = 0, bh = 0;
+    unsigned int hi = 0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_keys; j += gridDim.x * blockDim.x) {
+        uint32_t len = key_off[j + 1] - key_off[j];
+        uint32_t capped = len;
+        bool kept = true;
+        if (max_matches >= 0) {
+            uint32_t cap = (uint32_t)max_matches + 2u;
+            capped = len < cap ? len : cap;
+            kept = len <= (uint32_t)max_matches;
+        }
+        ih += capped;
+        hi = capped > hi ? capped : hi;
+        if (!kept) {
+            bk += 1;
+            bh += capped;
+        }
+        keep[j] = kept ? 1u : 0u;
+        keep_hits[j] = kept ? len : 0u;
+    }
+    atomicAdd(&st->indexed_hits, ih);
+    atomicAdd(&st->blacklisted_kmers, bk);
+    atomicAdd(&st->blacklisted_hits, bh);
+    atomicMax(&st->highest, hi);
+}
+
+// Moves the kept keys and their hit lists to their compacted places.
+__global__ void k_compact_keys(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ key_off,
+                               uint32_t n_keys, const uint32_t* __restrict__ keep_scan,
+                               const uint32_t* __restrict__ hits_scan, uint64_t* __restrict__ nkeys,
+                               uint32_t* __restrict__ nkey_off) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n_keys; j += gridDim.x * blockDim.x) {
+        if (keep_scan[j + 1] != keep_scan[j]) {
+            nkeys[keep_scan[j]] = keys[j];
+            nkey_off[keep_scan[j]] = hits_scan[j];
+        }
+    }
+}
+
+// Per hit: its key id (from the inclusive flag scan) and its compacted place.
+__global__ void k_compact_hits(const uint32_t* __restrict__ vals, size_t n, const uint32_t* __restrict__ fscan,
+                               const uint32_t* __restrict__ flag, const uint32_t* __restrict__ key_off,
+                               const uint32_t* __restrict__ keep_scan, const uint32_t* __restrict__ hits_scan,
+                               uint32_t* __restrict__ nhits) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint32_t kid = fscan[i] + flag[i] - 1u;
+        if (keep_scan[kid + 1] != keep_scan[kid]) nhits[hits_scan[kid] + ((uint32_t)i - key_off[kid])] = vals[i];
+    }
+}
+
+__global__ void k_fw_flags(const uint32_t* __restrict__ hits, size_t n, const uint32_t* __restrict__ ref_rs,
+                           uint32_t* __restrict__ f) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        f[i] = (ref_rs[hits[i]] & 1u) ? 0u : 1u;
+}
+
+__device__ __forceinline__ int64_t dir_bucket(uint64_t h, int lz, int bits) {
+    return (int64_t)((h << lz) >> (64 - bits));
+}
+
+__global__ void k_dir_fill(const uint64_t* __restrict__ keys, uint32_t n_keys, uint32_t* __restrict__ dir,
+                           int64_t nb, int lz, int bits) {
+    if (n_keys == 0) {
+        for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += (int64_t)gridDim.x * blockDim.x)
+            dir[b] = 0;
+        return;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_keys; i += gridDim.x * blockDim.x) {
+        int64_t bi = dir_bucket(keys[i], lz, bits);
+        int64_t bp = i > 0 ? dir_bucket(keys[i - 1], lz, bits) : -1;
+        for (int64_t b = bp + 1; b <= bi; b++) dir[b] = i;
+        if (i == n_keys - 1)
+            for (int64_t b = bi + 1; b <= nb; b++) dir[b] = n_keys;
+    }
+}
+
+IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_t n_seg,
+                          const std::vector<std::string>& names, int32_t k, double h_frac, int32_t max_matches,
+                          cudaStream_t s) {
+    auto* ix = new IndexStorage();
+    try {
+        SHM_CUDA(cudaGetDevice(&ix->device));
+        ix->k = k;
+        ix->h_frac = h_frac;
+        ix->max_matches = max_matches;
+        ix->names = names;
+        const uint64_t thr = h_thres(h_frac);
+        const int64_t total_bases = seg_off_b[n_seg] - seg_off_b[0];
+
+        // chunk layout per segment (host)
+        std::vector<uint64_t> chunk_off((size_t)n_seg + 1, 0);
+        std::vector<int64_t> soff((size_t)n_seg + 1, 0);
+        for (int32_t i = 0; i < n_seg; i++) {
+            int64_t L = seg_off_b[i + 1] - seg_off_b[i];
+            soff[(size_t)i + 1] = soff[(size_t)i] + L;
+            ix->seg_len.push_back((int32_t)L);
+            int64_t nw = L - k + 1;
+            uint64_t ch = nw > 0 ? (uint64_t)((nw + SKETCH_WIN - 1) / SKETCH_WIN) : 0;
+            chunk_off[(size_t)i + 1] = chunk_off[(size_t)i] + ch;
+        }
+        const uint64_t n_chunks = chunk_off[(size_t)n_seg];
+
+        DevBuf<uint8_t> d_seq;
+        DevBuf<int64_t> d_soff;
+        DevBuf<uint64_t> d_chunk_off;
+        DevBuf<uint32_t> d_ccnt, d_cout;
+        d_seq.reserve((size_t)total_bases + 32);
+        SHM_CUDA(cudaMemsetAsync(d_seq.p + total_bases, 0, 32, s));
+        SHM_CUDA(cudaMemcpyAsync(d_seq.p, h_seq + seg_off_b[0], (size_t)total_bases, cudaMemcpyHostToDevice, s));
+        d_soff.reserve((size_t)n_seg + 1);
+        SHM_CUDA(cudaMemcpyAsync(d_soff.p, soff.data(), sizeof(int64_t) * ((size_t)n_seg + 1), cudaMemcpyHostToDevice, s));
+        d_chunk_off.reserve((size_t)n_seg + 1);
+        SHM_CUDA(cudaMemcpyAsync(d_chunk_off.p, chunk_off.data(), sizeof(uint64_t) * ((size_t)n_seg + 1),
+                                 cudaMemcpyHostToDevice, s));
+        d_ccnt.reserve(n_chunks + 1);
+        d_cout.reserve(n_chunks + 1);
+
+        SketchLuts* luts = create_device_luts(k, s);
+        SketchArgs a{};
+        a.seq = d_seq.p;
+        a.seq_off = d_soff.p;
+        a.chunk_off = d_chunk_off.p;
+        a.n_seq = n_seg;
+        a.n_chunks = n_chunks;
+        a.k = k;
+        a.thr = thr;
+        a.r_offset = 0;
+        a.chunk_cnt = d_ccnt.p;
+        launch_sketch(SK_COUNT, a, luts, s);
+        exclusive_scan_u32(d_ccnt.p, d_cout.p, n_chunks, s);
+        uint32_t n_kmers = 0;
+        SHM_CUDA(cudaMemcpyAsync(&n_kmers, d_cout.p + n_chunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaStreamSynchronize(s));
+        ix->ref_h.reserve((size_t)n_kmers + 1);
+        ix->ref_rs.reserve((size_t)n_kmers + 1);
+        a.chunk_out = d_cout.p;
+        a.out_h = ix->ref_h.p;
+        a.out_rs = ix->ref_rs.p;
+        launch_sketch(SK_WRITE, a, luts, s);
+        ix->seg_off.reserve((size_t)n_seg + 1);
+        k_seg_offsets<<<grid_for((size_t)n_seg + 1, 128), 128, 0, s>>>(d_chunk_off.p, d_cout.p, n_seg, ix->seg_off.p);
+        SHM_CUDA(cudaGetLastError());
+        SHM_CUDA(cudaFree(luts));
+        d_seq.release();
+        d_ccnt.release();
+        d_cout.release();
+        ix->h_seg_off.resize((size_t)n_seg + 1);
+        SHM_CUDA(cudaMemcpyAsync(ix->h_seg_off.data(), ix->seg_off.p, sizeof(uint32_t) * ((size_t)n_seg + 1),
+                                 cudaMemcpyDeviceToHost, s));
+        ix->seg_sz.reserve((size_t)n_seg + 1);
+        SHM_CUDA(cudaMemcpyAsync(ix->seg_sz.p, ix->seg_len.data(), sizeof(int32_t) * (size_t)n_seg,
+                                 cudaMemcpyHostToDevice, s));
+
+        // 2. stable sort of (hash, gidx) by hash
+        const size_t n = n_kmers;
+        DevBuf<uint64_t> k0, k1;
+        DevBuf<uint32_t> v0, v1;
+        k0.reserve(n + 1);
+        k1.reserve(n + 1);
+        v0.reserve(n + 1);
+        v1.reserve(n + 1);
+        SHM_CUDA(cudaMemcpyAsync(k0.p, ix->ref_h.p, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+        k_iota<<<grid_for(n, 256), 256, 0, s>>>(v0.p, n);
+        SHM_CUDA(cudaGetLastError());
+        int key_bits = thr == 0 ? 0 : 64 - __builtin_clzll(thr);
+        bool flipped = radix_sort_pairs(k0.p, v0.p, k1.p, v1.p, n, key_bits, s);
+        uint64_t* ks = flipped ? k1.p : k0.p;
+        uint32_t* vals = flipped ? v1.p : v0.p;
+
+        // 3. CSR over runs of equal hashes
+        DevBuf<uint32_t> flag, fscan;
+        flag.reserve(n + 1);
+        fscan.reserve(n + 1);
+        k_key_flags<<<grid_for(n, 256), 256, 0, s>>>(ks, n, flag.p);
+        SHM_CUDA(cudaGetLastError());
+        exclusive_scan_u32(flag.p, fscan.p, n, s);
+        uint32_t n_keys = 0;
+        SHM_CUDA(cudaMemcpyAsync(&n_keys, fscan.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaStreamSynchronize(s));
+        DevBuf<uint64_t> keys_all;
+        DevBuf<uint32_t> key_off_all;
+        keys_all.reserve((size_t)n_keys + 1);
+        key_off_all.reserve((size_t)n_keys + 1);
+        k_key_emit<<<grid_for(n, 256), 256, 0, s>>>(ks, n, fscan.p, keys_all.p, key_off_all.p);
+        SHM_CUDA(cudaGetLastError());
+        uint32_t nn = (uint32_t)n;
+        SHM_CUDA(cudaMemcpyAsync(key_off_all.p + n_keys, &nn, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+
+        IdxStatsDev* dst = nullptr;
+        SHM_CUDA(cudaMallocAsync(&dst, sizeof(IdxStatsDev), s));
+        SHM_CUDA(cudaMemsetAsync(dst, 0, sizeof(IdxStatsDev), s));
+        DevBuf<uint32_t> keep, keep_hits, keep_scan, hits_scan;
+        keep.reserve((size_t)n_keys + 1);
+        keep_hits.reserve((size_t)n_keys + 1);
+        keep_scan.reserve((size_t)n_keys + 1);
+        hits_scan.reserve((size_t)n_keys + 1);
+        k_key_keep<<<grid_for(n_keys, 256), 256, 0, s>>>(key_off_all.p, n_keys, max_matches, keep.p, keep_hits.p, dst);
+        SHM_CUDA(cudaGetLastError());
+        IdxStatsDev hst{};
+        SHM_CUDA(cudaMemcpyAsync(&hst, dst, sizeof hst, cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaFreeAsync(dst, s));
+        exclusive_scan_u32(keep.p, keep_scan.p, n_keys, s);
+        exclusive_scan_u32(keep_hits.p, hits_scan.p, n_keys, s);
+        uint32_t n_kept = 0, n_hits = 0;
+        SHM_CUDA(cudaMemcpyAsync(&n_kept, keep_scan.p + n_keys, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaMemcpyAsync(&n_hits, hits_scan.p + n_keys, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaStreamSynchronize(s));
+
+        ix->keys.reserve((size_t)n_kept + 1);
+        ix->key_off.reserve((size_t)n_kept + 1);
+        ix->hits.reserve((size_t)n_hits + 1);
+        k_compact_keys<<<grid_for(n_keys, 256), 256, 0, s>>>(keys_all.p, key_off_all.p, n_keys, keep_scan.p,
+                                                             hits_scan.p, ix->keys.p, ix->key_off.p);
+        SHM_CUDA(cudaGetLastError());
+        SHM_CUDA(cudaMemcpyAsync(ix->key_off.p + n_kept, &n_hits, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        k_compact_hits<<<grid_for(n, 256), 256, 0, s>>>(vals, n, fscan.p, flag.p, key_off_all.p, keep_scan.p,
+                                                        hits_scan.p, ix->hits.p);
+        SHM_CUDA(cudaGetLastError());
+
+        // 4. forward-strand prefix and the hash directory
+        ix->hit_fw.reserve((size_t)n_hits + 1);
+        k_fw_flags<<<grid_for(n_hits, 256), 256, 0, s>>>(ix->hits.p, n_hits, ix->ref_rs.p, flag.p);
+        SHM_CUDA(cudaGetLastError());
+        exclusive_scan_u32(flag.p, ix->hit_fw.p, n_hits, s);
+        int bits = 1;
+        while (bits < 30 && (1u << bits) < n_kept) bits++;
+        int lz = thr == 0 ? 63 : __builtin_clzll(thr);
+        const int64_t nb = (int64_t)1 << bits;
+        ix->dir.reserve((size_t)nb + 1);
+        k_dir_fill<<<grid_for(std::max<size_t>(n_kept, 1), 256), 256, 0, s>>>(ix->keys.p, n_kept, ix->dir.p, nb, lz,
+                                                                             bits);
+        SHM_CUDA(cudaGetLastError());
+        SHM_CUDA(cudaStreamSynchronize(s));
+
+        DevIndex& d = ix->dev;
+        d.k = k;
+        d.n_seg = n_seg;
+        d.thr = thr;
+        d.seg_off = ix->seg_off.p;
+        d.seg_sz = ix->seg_sz.p;
+        d.ref_h = ix->ref_h.p;
+        d.ref_rs = ix->ref_rs.p;
+        d.keys = ix->keys.p;
+        d.key_off = ix->key_off.p;
+        d.hits = ix->hits.p;
+        d.hit_fw = ix->hit_fw.p;
+        d.dir = ix->dir.p;
+        d.dir_bits = bits;
+        d.dir_lz = lz;
+        d.n_keys = n_kept;
+        d.n_kmers = n_kmers;
+        d.n_hits = n_hits;
+
+        shm_index_stats& st = ix->stats;
+        st.segments = n_seg;
+        st.total_nucls = total_bases;
+        st.indexed_hits = (int64_t)hst.indexed_hits;
+        st.indexed_kmers = n_keys;
+        st.highest_freq_kmer = hst.highest;
+        st.blacklisted_kmers = (int64_t)hst.blacklisted_kmers;
+        st.blacklisted_hits = (int64_t)hst.blacklisted_hits;
+        st.sketched_kmers = n_kmers;
+        return ix;
+    } catch (...) {
+        delete ix;
+        throw;
+    }
+}
+
+}  // namespace shm

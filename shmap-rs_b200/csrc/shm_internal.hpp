@@ -1,0 +1,65 @@
+// Host-side objects behind the C ABI (context, index, batch scratch).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/shmap_gpu.h"
+#include "shm_common.cuh"
+#include "shm_sketch.cuh"
+
+namespace shm {
+
+uint64_t h_thres(double h_frac);  // src/sketch.rs:126-132
+
+// A device buffer that only grows; released by the destructor.
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;  // elements
+    void reserve(size_t n) {
+        if (n <= cap && p) return;
+        if (p) SHM_CUDA(cudaFree(p));
+        p = nullptr;
+        size_t want = n < 16 ? 16 : n;
+        SHM_CUDA(cudaMalloc(&p, want * sizeof(T)));
+        cap = want;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    ~DevBuf() { release(); }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+struct IndexStorage {
+    DevIndex dev{};
+    DevBuf<uint32_t> seg_off, key_off, hits, hit_fw, dir, ref_rs;
+    DevBuf<int32_t> seg_sz;
+    DevBuf<uint64_t> ref_h, keys;
+    std::vector<std::string> names;
+    std::vector<int32_t> seg_len;        // bases
+    std::vector<uint32_t> h_seg_off;     // k-mer offsets (n_seg+1)
+    shm_index_stats stats{};
+    int32_t k = 0;
+    double h_frac = 0;
+    int32_t max_matches = -1;
+    int device = 0;
+};
+
+IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off, int32_t n_seg,
+                          const std::vector<std::string>& names, int32_t k, double h_frac, int32_t max_matches,
+                          cudaStream_t s);
+
+}  // namespace shm
+
+// The opaque handles of the C ABI.
+struct shm_index {
+    shm::IndexStorage* s;
+};

@@ -1,0 +1,1376 @@
+// The per-read mapping path (SHMapper::map_read, src/shmap/mod.rs:653-971)
+// as a sequence of batch-wide kernels over thousands of reads:
+//
+//  K1 sketch        reads -> k-mers                       (src/sketch.rs:167-209)
+//  K2 seedprep      group by hash, count() probes, rarest-first order, S and
+//                   the seeding prefix; p_ht               (seeding.rs:26-77, mod.rs:682-748)
+//  K3 contrib       every hit of every processed seed -> bucket contributions
+//                   into a per-read hash table             (seeding.rs:98-212, buckets.rs:642-674)
+//  K4 bscan         distinct buckets; which ones can still clear a threshold
+//  K5 extend        seed-heuristic extension, one warp per bucket (pruning.rs:10-119)
+//  K6 cidx          candidates grouped per read
+//  K7 refine        sliding-window Containment/Jaccard, one warp per candidate
+//                   (scoring.rs:189-291)
+//  K8 sweep         the two ordered sweeps of match_rest and the record
+//                   (scoring.rs:367-489, mod.rs:816-943)
+//
+// Exactness of the reformulation (why the parallel stages reproduce the
+// sequential sweep bit for bit):
+//  * sh = 1 - (seeds - matches)/m never increases as seeds are added (each
+//    seed adds occs to seeds and at most occs to matches), so
+//    seed_heuristic_pass(thr) keeps a bucket iff its sh after ALL seeds
+//    (sh_final) is >= thr, and then reports sh_final. The in-place pruning
+//    state only changes how far the CPU had to look, not the outcome.
+//  * pass 1 admits only scores > thr >= theta, so pass 2's threshold
+//    best*(1-d) is >= fl(theta*fl(1-d)) = theta_low. Extending every bucket
+//    until sh < theta_low therefore decides every survival test of both
+//    passes, and refining the buckets with sh_final >= theta_low covers every
+//    bucket either pass scores. The sweeps then run on those results in the
+//    reference's order (matches desc, (segm_id, b) asc).
+//  * a seed's contribution to bucket (g, b) is the aggregate over its hits
+//    with pos in [b*h, (b+2)*h) of segment g: exactly what match_seeds'
+//    two-slot stream flushes (matches clamped to occs). Hit lists are sorted,
+//    so that aggregate is a range found by binary search, and every touched
+//    bucket is emitted once, by the first hit of its first run.
+//  * best_fixed_length's multiset intersection over window [l, r(l)) is
+//    sum_s min(c_s, occs_s): position j counts for window l iff l <= j < r(l)
+//    and the occs-th previous occurrence of its seed lies before l. Each j
+//    therefore adds 1 on an interval of l, and the per-l intersection is a
+//    prefix sum; the first l with the maximal score wins, as the strict `>`
+//    of the sequential loop does.
+// All scores use explicit round-to-nearest f64 intrinsics.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "shm_common.cuh"
+#include "shm_map.cuh"
+#include "shm_prims.cuh"
+#include "shm_sketch.cuh"
+
+namespace shm {
+
+struct BatchMax {
+    unsigned int m_max, nu_max, half_max, n_overflow;
+};
+
+struct BatchView {
+    int32_t n;
+    DevParams P;
+    DevIndex I;
+    double theta2;
+    const uint8_t* seq;
+    const int64_t* roff;
+    const uint64_t* kcap_off;
+    uint32_t* kcnt;
+    uint64_t* km_h;
+    uint32_t* km_rs;
+    uint64_t* sd_h;
+    uint32_t *sd_a, *sd_cnt, *sd_os, *sd_hpre, *sd_ooff;
+    const uint64_t* pht_off;
+    uint64_t* pht_key;
+    uint32_t* pht_val;
+    int32_t *r_status, *r_m, *r_nu, *r_nproc, *r_S, *r_S0, *r_half, *r_maxseed;
+    int64_t* r_smatch;
+    uint32_t* r_seeded;
+    uint64_t *hw, *hw_off, *bt_size, *bt_off;
+    BSlot* bt;
+    BucketJob* jobs;
+    uint32_t* n_jobs;
+    uint32_t job_cap;
+    uint32_t *ccnt, *coff, *ccur, *cidx;
+    uint32_t* ovf_list;
+    BatchMax* mx;
+    shm_map_record* out;
+};
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ uint64_t pow2_ceil(uint64_t x) {
+    if (x <= 1) return 1;
+    return 1ULL << (64 - __clzll((long long)(x - 1)));
+}
+
+template <class T>
+__device__ T block_scan_excl(T v, T* sh_warp, T* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    T inc = warp_inclusive_scan(v);
+    if (lane == 31) sh_warp[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        T w = lane < nw ? sh_warp[lane] : T(0);
+        T wi = warp_inclusive_scan(w);
+        if (lane < nw) sh_warp[lane] = wi - w;
+        if (lane == nw - 1) *total = wi;
+    }
+    __syncthreads();
+    T r = sh_warp[wid] + inc - v;
+    __syncthreads();
+    return r;
+}
+
+template <class T>
+__device__ T block_reduce_sum(T v, T* sh_warp) {
+    T tot;
+    block_scan_excl<T>(v, sh_warp, &tot);
+    __syncthreads();
+    return tot;
+}
+
+__device__ uint32_t block_reduce_max(uint32_t v, uint32_t* sh_warp) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) sh_warp[wid] = v;
+    __syncthreads();
+    uint32_t r = 0;
+    for (int i = 0; i < nw; i++) r = max(r, sh_warp[i]);
+    __syncthreads();
+    return r;
+}
+
+// Bitonic sort of (A,B) pairs ascending by (A, B), P a power of two.
+__device__ void bitonic_ab(uint64_t* A, uint32_t* B, uint32_t P) {
+    for (uint32_t k = 2; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                bool asc = (i & k) == 0;
+                uint64_t ai = A[i], al = A[l];
+                uint32_t bi = B[i], bl = B[l];
+                bool gt = ai > al || (ai == al && bi > bl);
+                if (gt == asc) {
+                    A[i] = al;
+                    A[l] = ai;
+                    B[i] = bl;
+                    B[l] = bi;
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__device__ void bitonic_u64(uint64_t* A, uint32_t P) {
+    for (uint32_t k = 2; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                bool asc = (i & k) == 0;
+                uint64_t ai = A[i], al = A[l];
+                if ((ai > al) == asc) {
+                    A[i] = al;
+                    A[l] = ai;
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__device__ __forceinline__ bool pht_lookup(const BatchView& v, int32_t q, uint64_t h, uint32_t& idx) {
+    const uint64_t base = v.pht_off[q];
+    const uint64_t mask = v.pht_off[q + 1] - base - 1;
+    uint64_t i = mix64(h) & mask;
+    for (;;) {
+        uint32_t val = v.pht_val[base + i];
+        if (val == 0xffffffffu) return false;
+        if (v.pht_key[base + i] == h) {
+            idx = val;
+            return true;
+        }
+        i = (i + 1) & mask;
+    }
+}
+
+__device__ __forceinline__ void pht_insert(const BatchView& v, int32_t q, uint64_t h, uint32_t idx) {
+    const uint64_t base = v.pht_off[q];
+    const uint64_t mask = v.pht_off[q + 1] - base - 1;
+    uint64_t i = mix64(h) & mask;
+    for (;;) {
+        if (atomicCAS(v.pht_val + base + i, 0xffffffffu, idx) == 0xffffffffu) {
+            v.pht_key[base + i] = h;
+            return;
+        }
+        i = (i + 1) & mask;
+    }
+}
+
+// ------------------------------------------------------------------ K2 seedprep
+// One CTA per read. Arrays (P = power of two >= the read's k-mer capacity):
+// A/B element keys, GA/GB group hash and occs<<1|strand, GF first index then
+// count(), GD hit-list start, E rarest-first sort keys.
+struct SeedArrays {
+    uint64_t *A, *GA, *E;
+    uint32_t *B, *GB, *GF, *GD;
+};
+
+__device__ SeedArrays carve(uint8_t* base, uint32_t P) {
+    SeedArrays s;
+    s.A = (uint64_t*)base;
+    s.GA = s.A + P;
+    s.E = s.GA + P;
+    s.B = (uint32_t*)(s.E + P);
+    s.GB = s.B + P;
+    s.GF = s.GB + P;
+    s.GD = s.GF + P;
+    return s;
+}
+constexpr size_t SEED_BYTES_PER_ELEM = 3 * 8 + 4 * 4;
+
+__device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const SeedArrays& S_) {
+    __shared__ uint64_t sw64[32];
+    __shared__ uint32_t sw32[32];
+    __shared__ uint64_t t64;
+    __shared__ uint32_t t32;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int64_t read_len = v.roff[q + 1] - v.roff[q];
+    const uint64_t kb = v.kcap_off[q];
+    const uint32_t cap = (uint32_t)(v.kcap_off[q + 1] - kb);
+    const uint32_t m = v.kcnt[q];
+    if (tid == 0) {
+        v.hw[q] = 0;
+        v.bt_size[q] = 0;
+        v.r_nproc[q] = 0;
+        v.r_nu[q] = 0;
+        v.r_S0[q] = 0;
+        v.r_smatch[q] = 0;
+        v.r_maxseed[q] = 0;
+        v.r_m[q] = (int32_t)m;
+        v.r_half[q] = 0;
+    }
+    if (m > cap || cap > P) {
+        if (tid == 0) v.r_status[q] = ST_OVERFLOW;
+        return;
+    }
+    int32_t S = __double2int_rz(__dmul_rn(__dsub_rn(1.0, v.theta2), (double)m)) + 1;
+    const int32_t halflen = v.P.ap ? (int32_t)read_len : (int32_t)m;
+    if (halflen < MIN_HALFLEN) {
+        if (tid == 0) {
+            v.r_status[q] = ST_SHORT_SKETCH;
+            v.r_S[q] = S;
+        }
+        return;
+    }
+    const uint32_t Pm = (uint32_t)pow2_ceil(m);
+    for (uint32_t i = tid; i < Pm; i += nt) {
+        if (i < m) {
+            S_.A[i] = v.km_h[kb + i];
+            uint32_t rs = v.km_rs[kb + i];
+            S_.B[i] = ((0x3fffffffu - (rs >> 1)) << 1) | (rs & 1u);
+        } else {
+            S_.A[i] = ~0ULL;
+            S_.B[i] = 0xffffffffu;
+        }
+    }
+    __syncthreads();
+    bitonic_ab(S_.A, S_.B, Pm);  // (h asc, r desc): src/shmap/seeding.rs:28-34
+
+    // groups of equal hashes (src/shmap/seeding.rs:45-67)
+    const uint32_t per = (m + nt - 1) / nt;
+    const uint32_t i0 = min(m, (uint32_t)tid * per), i1 = min(m, i0 + per);
+    uint32_t nf = 0;
+    for (uint32_t i = i0; i < i1; i++) nf += (i == 0 || S_.A[i] != S_.A[i - 1]) ? 1u : 0u;
+    uint32_t gbase = block_scan_excl<uint32_t>(nf, sw32, &t32);
+    const uint32_t n_u = t32;
+    {
+        uint32_t c = gbase;
+        for (uint32_t i = i0; i < i1; i++)
+            if (i == 0 || S_.A[i] != S_.A[i - 1]) {
+                S_.GF[c] = i;
+                S_.GA[c] = S_.A[i];
+                c++;
+            }
+    }
+    __syncthreads();
+    {
+        uint32_t c = gbase;
+        for (uint32_t i = i0; i < i1; i++) {
+            if (i == 0 || S_.A[i] != S_.A[i - 1]) c++;
+            if (i + 1 == m || S_.A[i + 1] != S_.A[i]) {
+                uint32_t g = c - 1;
+                uint32_t occs = i - S_.GF[g] + 1;
+                S_.GB[g] = (occs << 1) | (S_.B[i] & 1u);  // representative: smallest r (seeding.rs:56)
+            }
+        }
+    }
+    __syncthreads();
+    if (v.P.os) S = (int32_t)n_u;  // mod.rs:732-736
+    // count() probes (index.rs:204-213) and the hit-list start of each group
+    for (uint32_t g = tid; g < n_u; g += nt) {
+        uint32_t a, cnt;
+        idx_lookup(v.I, S_.GA[g], a, cnt);
+        S_.GD[g] = a;
+        S_.GF[g] = cnt;
+    }
+    __syncthreads();
+    // rarest first, stable over hash order (seeding.rs:71): key (hits_in_t, group)
+    const uint32_t Pu = (uint32_t)pow2_ceil(n_u);
+    for (uint32_t g = tid; g < Pu; g += nt) S_.E[g] = g < n_u ? (((uint64_t)S_.GF[g] << 32) | g) : ~0ULL;
+    __syncthreads();
+    bitonic_u64(S_.E, Pu);
+
+    // seeding prefix: seed i is processed iff sum(occs before i) < S (seeding.rs:101)
+    const uint32_t per2 = (n_u + nt - 1) / nt;
+    const uint32_t j0 = min(n_u, (uint32_t)tid * per2), j1 = min(n_u, j0 + per2);
+    uint32_t so = 0;
+    uint64_t sc = 0;
+    for (uint32_t i = j0; i < j1; i++) {
+        uint32_t g = (uint32_t)(S_.E[i] & 0xffffffffu);
+        so += S_.GB[g] >> 1;
+        sc += S_.E[i] >> 32;
+    }
+    uint32_t po = block_scan_excl<uint32_t>(so, sw32, &t32);
+    uint64_t pc = block_scan_excl<uint64_t>(sc, sw64, &t64);
+    uint32_t l_np = 0, l_s0 = 0, l_max = 0;
+    uint64_t l_sm = 0;
+    for (uint32_t i = j0; i < j1; i++) {
+        const uint64_t e = S_.E[i];
+        const uint32_t g = (uint32_t)(e & 0xffffffffu), cnt = (uint32_t)(e >> 32);
+        const uint32_t os = S_.GB[g], occs = os >> 1;
+        v.sd_h[kb + i] = S_.GA[g];
+        v.sd_os[kb + i] = os;
+        v.sd_cnt[kb + i] = cnt;
+        v.sd_a[kb + i] = S_.GD[g];
+        v.sd_ooff[kb + i] = po;
+        if ((int64_t)po < (int64_t)S) {
+            v.sd_hpre[kb + i] = (uint32_t)pc;
+            l_np++;
+            l_s0 += occs;
+            l_sm += cnt;
+            l_max = max(l_max, cnt);
+        }
+        pht_insert(v, q, S_.GA[g], i);
+        po += occs;
+        pc += cnt;
+    }
+    const uint32_t n_proc = block_reduce_sum<uint32_t>(l_np, sw32);
+    const uint32_t S0 = block_reduce_sum<uint32_t>(l_s0, sw32);
+    const uint64_t smatch = block_reduce_sum<uint64_t>(l_sm, sw64);
+    const uint32_t mxs = block_reduce_max(l_max, sw32);
+    if (tid == 0) {
+        v.r_status[q] = ST_UNMAPPED;
+        v.r_nu[q] = (int32_t)n_u;
+        v.r_nproc[q] = (int32_t)n_proc;
+        v.r_S[q] = S;
+        v.r_S0[q] = (int32_t)S0;
+        v.r_smatch[q] = (int64_t)smatch;
+        v.r_maxseed[q] = (int32_t)mxs;
+        v.r_half[q] = halflen;
+        if (smatch >= 0xffffffffULL) {
+            v.r_status[q] = ST_OVERFLOW;
+        } else {
+            v.hw[q] = smatch;
+            v.bt_size[q] = smatch ? max((uint64_t)16, pow2_ceil(4 * smatch)) : 0;
+        }
+        atomicMax(&v.mx->m_max, m);
+        atomicMax(&v.mx->nu_max, n_u);
+        atomicMax(&v.mx->half_max, (uint32_t)halflen);
+    }
+}
+
+template <bool GLOBAL>
+__global__ void __launch_bounds__(256) k_seedprep(BatchView v, const int32_t* __restrict__ list, int32_t n_list,
+                                                  uint32_t P, uint8_t* gscr, size_t gscr_per_cta) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint8_t* base = GLOBAL ? gscr + (size_t)blockIdx.x * gscr_per_cta : smem;
+    SeedArrays S_ = carve(base, P);
+    for (int32_t li = blockIdx.x; li < n_list; li += gridDim.x) {
+        seedprep_one(v, list[li], P, S_);
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ K3 contributions
+__device__ __forceinline__ int64_t hit_pos(const DevIndex& I, uint32_t g, int32_t seg, bool ap) {
+    return ap ? (int64_t)(__ldg(I.ref_rs + g) >> 1) : (int64_t)(g - __ldg(I.seg_off + seg));
+}
+
+// Hits of one seed's list [a, a+cnt) in segment g with pos in [lo, hi): returns [A, B).
+__device__ __forceinline__ void seed_range(const DevIndex& I, uint32_t a, uint32_t cnt, int32_t g, int64_t lo,
+                                           int64_t hi, bool ap, uint32_t& A, uint32_t& B) {
+    const uint32_t s_lo = __ldg(I.seg_off + g), s_hi = __ldg(I.seg_off + g + 1);
+    if (!ap) {
+        uint64_t glo = (uint64_t)s_lo + (uint64_t)max(lo, (int64_t)0);
+        uint64_t ghi = min((uint64_t)s_lo + (uint64_t)max(hi, (int64_t)0), (uint64_t)s_hi);
+        glo = min(glo, (uint64_t)s_hi);
+        A = hits_lower_bound(I.hits, a, cnt, (uint32_t)glo);
+        B = hits_lower_bound(I.hits, a, cnt, (uint32_t)ghi);
+        if (B < A) B = A;
+        return;
+    }
+    uint32_t sA = hits_lower_bound(I.hits, a, cnt, s_lo), sB = hits_lower_bound(I.hits, a, cnt, s_hi);
+    auto lb_r = [&](int64_t rv) {
+        uint32_t l = sA, len = sB - sA;
+        while (len > 0) {
+            uint32_t half = len >> 1;
+            if ((int64_t)(__ldg(I.ref_rs + __ldg(I.hits + l + half)) >> 1) < rv) {
+                l += half + 1;
+                len -= half + 1;
+            } else {
+                len = half;
+            }
+        }
+        return l;
+    };
+    A = lb_r(lo);
+    B = lb_r(hi);
+    if (B < A) B = A;
+}
+
+struct Agg {
+    int32_t count, codir, rmin, rmax;
+};
+
+__device__ __forceinline__ Agg range_agg(const DevIndex& I, uint32_t A, uint32_t B, uint32_t seed_strand) {
+    Agg r;
+    r.count = (int32_t)(B - A);
+    if (r.count <= 0) {
+        r.count = 0;
+        r.codir = 0;
+        r.rmin = INT32_MAX;
+        r.rmax = -1;
+        return r;
+    }
+    int32_t fw = (int32_t)(__ldg(I.hit_fw + B) - __ldg(I.hit_fw + A));
+    int32_t same = seed_strand ? r.count - fw : fw;
+    r.codir = 2 * same - r.count;
+    r.rmin = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + A)) >> 1);
+    r.rmax = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B - 1)) >> 1);
+    return r;
+}
+
+__device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t seg, int64_t bb, int32_t matches,
+                                       int32_t codir, int32_t rmin, int32_t rmax) {
+    const uint64_t base = v.bt_off[q];
+    const uint64_t mask = v.bt_off[q + 1] - base - 1;
+    const unsigned long long key = ((unsigned long long)(uint32_t)seg << 32) | (uint32_t)bb;
+    uint64_t i = mix64(key) & mask;
+    BSlot* s;
+    for (;;) {
+        s = v.bt + base + i;
+        unsigned long long prev = atomicCAS(&s->key, EMPTY_KEY, key);
+        if (prev == EMPTY_KEY || prev == key) break;
+        i = (i + 1) & mask;
+    }
+    atomicAdd(&s->matches, matches);
+    atomicAdd(&s->codir, codir);
+    atomicMin(&s->rmin, rmin);
+    atomicMax(&s->rmax, rmax);
+}
+
+__device__ __forceinline__ uint32_t ub_u64(const uint64_t* a, uint32_t n, uint64_t x) {  // first index with a[i] > x
+    uint32_t lo = 0, len = n;
+    while (len > 0) {
+        uint32_t half = len >> 1;
+        if (a[lo + half] <= x) {
+            lo += half + 1;
+            len -= half + 1;
+        } else {
+            len = half;
+        }
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t ub_u32(const uint32_t* a, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, len = n;
+    while (len > 0) {
+        uint32_t half = len >> 1;
+        if (a[lo + half] <= x) {
+            lo += half + 1;
+            len -= half + 1;
+        } else {
+            len = half;
+        }
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_contrib(BatchView v) {
+    const uint64_t total = v.hw_off[v.n];
+    const bool ap = v.P.ap != 0;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const int32_t q = (int32_t)ub_u64(v.hw_off, (uint32_t)v.n + 1, w) - 1;
+        const uint32_t u = (uint32_t)(w - v.hw_off[q]);
+        const uint64_t kb = v.kcap_off[q];
+        const uint32_t np = (uint32_t)v.r_nproc[q];
+        const uint32_t j = ub_u32(v.sd_hpre + kb, np, u) - 1;
+        const uint32_t t = u - v.sd_hpre[kb + j];
+        const uint32_t a = v.sd_a[kb + j], cnt = v.sd_cnt[kb + j], os = v.sd_os[kb + j];
+        const uint32_t occs = os >> 1, sstr = os & 1u;
+        const int64_t h = v.r_half[q];
+        const DevIndex& I = v.I;
+        const uint32_t g_t = __ldg(I.hits + a + t);
+        const int32_t seg_t = seg_of(I, g_t);
+        const int64_t b_t = hit_pos(I, g_t, seg_t, ap) / h;
+        bool first = true, prev_is_bm1 = false;
+        if (t > 0) {
+            const uint32_t g_p = __ldg(I.hits + a + t - 1);
+            const int32_t seg_p = seg_of(I, g_p);
+            const int64_t b_p = hit_pos(I, g_p, seg_p, ap) / h;
+            first = !(seg_p == seg_t && b_p == b_t);
+            prev_is_bm1 = seg_p == seg_t && b_p == b_t - 1;
+        }
+        if (!first) continue;
+        if (cnt == 1) {
+            const uint32_t rs = __ldg(I.ref_rs + g_t);
+            const int32_t cd = ((rs & 1u) == sstr) ? 1 : -1, r = (int32_t)(rs >> 1);
+            bt_add(v, q, seg_t, b_t, 1, cd, r, r);  // add_to_pos (buckets.rs:642-662)
+            if (b_t > 0) bt_add(v, q, seg_t, b_t - 1, 1, cd, r, r);
+            continue;
+        }
+        // streamed multi-hit seed: one clamped contribution per bucket (seeding.rs:113-205)
+        for (int e = 0; e < 2; e++) {
+            const int64_t bb = b_t - e;
+            if (bb < 0) break;
+            if (e == 1 && prev_is_bm1) break;
+            uint32_t A, B;
+            seed_range(I, a, cnt, seg_t, bb * h, (bb + 2) * h, ap, A, B);
+            Agg g = range_agg(I, A, B, sstr);
+            bt_add(v, q, seg_t, bb, min(g.count, (int32_t)occs), g.codir, g.rmin, g.rmax);
+        }
+    }
+}
+
+__global__ void k_bt_init(BSlot* bt, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        BSlot s;
+        s.key = EMPTY_KEY;
+        s.matches = 0;
+        s.codir = 0;
+        s.rmin = INT32_MAX;
+        s.rmax = -1;
+        bt[i] = s;
+    }
+}
+
+// ------------------------------------------------------------------ K4 distinct buckets
+__global__ void __launch_bounds__(256) k_bscan(BatchView v) {
+    const uint64_t total = v.bt_off[v.n];
+    for (uint64_t si = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; si < total;
+         si += (uint64_t)gridDim.x * blockDim.x) {
+        const BSlot s = v.bt[si];
+        if (s.key == EMPTY_KEY) continue;
+        const int32_t q = (int32_t)ub_u64(v.bt_off, (uint32_t)v.n + 1, si) - 1;
+        atomicAdd(v.r_seeded + q, 1u);  // seeded_buckets (mod.rs:794)
+        BucketJob j;
+        j.read = q;
+        j.seg = (int32_t)(s.key >> 32);
+        j.bb = (int32_t)(s.key & 0xffffffffu);
+        j.m0 = s.matches;
+        j.matches = s.matches;
+        j.codir = s.codir;
+        j.rmin = s.rmin;
+        j.rmax = s.rmax;
+        j.pad0 = j.pad1 = 0;
+        j.score = -1.0;
+        j.t_l = j.t_r = j.inter = j.same = j.s_sz = -1;
+        if (v.P.nbp) {
+            j.sh = 1.0;  // seed_heuristic_pass does nothing under NBP (pruning.rs:351)
+            j.is_cand = 1;
+        } else {
+            const double sh0 = hseed(v.r_m[q], v.r_S0[q], s.matches);
+            if (sh0 < v.P.theta_low) continue;
+            j.sh = sh0;
+            j.is_cand = 0;
+        }
+        uint32_t ji = atomicAdd(v.n_jobs, 1u);
+        if (ji < v.job_cap) {
+            v.jobs[ji] = j;
+            if (j.is_cand) atomicAdd(v.ccnt + q, 1u);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ K5 extension
+// One warp per bucket; 32 remaining seeds per step, matches_in_bucket for each
+// (pruning.rs:18-80), then an inclusive scan of (seeds, matches) finds the
+// first prefix whose sh drops below theta_low.
+__global__ void __launch_bounds__(256) k_extend(BatchView v) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t njobs = min(*v.n_jobs, v.job_cap);
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const bool ap = v.P.ap != 0;
+    for (uint32_t ji = wid; ji < njobs; ji += nwarps) {
+        BucketJob* J = v.jobs + ji;
+        const int32_t q = J->read, seg = J->seg, bb = J->bb;
+        const int32_t m = v.r_m[q], n_u = v.r_nu[q], np = v.r_nproc[q];
+        const int64_t h = v.r_half[q];
+        const uint64_t kb = v.kcap_off[q];
+        int32_t seeds = v.r_S0[q], matches = J->matches, codir = J->codir, rmin = J->rmin, rmax = J->rmax;
+        bool stopped = false;
+        for (int32_t i0 = np; i0 < n_u; i0 += 32) {
+            const int32_t i = i0 + lane;
+            const bool valid = i < n_u;
+            int32_t ds = 0, dm = 0, dc = 0, rmn = INT32_MAX, rmx = -1;
+            if (valid) {
+                const uint32_t os = v.sd_os[kb + i], cnt = v.sd_cnt[kb + i];
+                ds = (int32_t)(os >> 1);
+                if (cnt > 0) {
+                    uint32_t A, B;
+                    seed_range(v.I, v.sd_a[kb + i], cnt, seg, (int64_t)bb * h, ((int64_t)bb + 2) * h, ap, A, B);
+                    Agg g = range_agg(v.I, A, B, os & 1u);
+                    dm = min(g.count, ds);
+                    dc = g.codir;
+                    rmn = g.rmin;
+                    rmx = g.rmax;
+                }
+            }
+            const int32_t ps = warp_inclusive_scan(ds), pm = warp_inclusive_scan(dm);
+            const bool low = valid && hseed(m, seeds + ps, matches + pm) < v.P.theta_low;
+            if (__any_sync(0xffffffffu, low)) {
+                stopped = true;
+                break;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                dc += __shfl_xor_sync(0xffffffffu, dc, o);
+                rmn = min(rmn, __shfl_xor_sync(0xffffffffu, rmn, o));
+                rmx = max(rmx, __shfl_xor_sync(0xffffffffu, rmx, o));
+            }
+            seeds += __shfl_sync(0xffffffffu, ps, 31);
+            matches += __shfl_sync(0xffffffffu, pm, 31);
+            codir += dc;
+            rmin = min(rmin, rmn);
+            rmax = max(rmax, rmx);
+        }
+        if (lane == 0 && !stopped) {
+            J->sh = hseed(m, seeds, matches);
+            J->matches = matches;
+            J->codir = codir;
+            J->rmin = rmin;
+            J->rmax = rmax;
+            J->is_cand = 1;
+            atomicAdd(v.ccnt + q, 1u);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ K6 candidates per read
+__global__ void k_cidx(BatchView v) {
+    const uint32_t njobs = min(*v.n_jobs, v.job_cap);
+    for (uint32_t ji = blockIdx.x * blockDim.x + threadIdx.x; ji < njobs; ji += gridDim.x * blockDim.x) {
+        if (!v.jobs[ji].is_cand) continue;
+        const int32_t q = v.jobs[ji].read;
+        v.cidx[v.coff[q] + atomicAdd(v.ccur + q, 1u)] = ji;
+    }
+}
+
+// ------------------------------------------------------------------ K7 refinement
+struct RefScratch {
+    int32_t* base;
+    size_t per_warp;  // ints
+    uint32_t nu_max, wmax;
+};
+
+__global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t ncand = v.coff[v.n];
+    int32_t* cntA = rsc.base + (size_t)wid * rsc.per_warp;
+    int32_t* D = cntA + rsc.nu_max;
+    int32_t* C = D + rsc.wmax + 1;
+    int32_t* PC = C + rsc.wmax + 1;
+    int32_t* ring = PC + rsc.wmax + 1;
+    const bool ap = v.P.ap != 0;
+    const DevIndex& I = v.I;
+    for (uint32_t ci = wid; ci < ncand; ci += nwarps) {
+        BucketJob* J = v.jobs + v.cidx[ci];
+        const int32_t q = J->read;
+        if (v.P.metric == 2) {  // bucket_SH (scoring.rs:311-325)
+            if (lane == 0) {
+                J->score = J->sh;
+                J->t_l = J->rmin;
+                J->t_r = J->rmax;
+                J->inter = J->matches;
+                J->same = J->codir;
+                J->s_sz = J->rmax - J->rmin;
+            }
+            continue;
+        }
+        const int32_t m = v.r_m[q], n_u = v.r_nu[q];
+        const int64_t h = v.r_half[q];
+        const uint64_t kb = v.kcap_off[q];
+        const int32_t seg = J->seg;
+        const uint32_t G0 = __ldg(I.seg_off + seg), Gend = __ldg(I.seg_off + seg + 1);
+        const int64_t seglen = (int64_t)(Gend - G0);
+        const int64_t from = (int64_t)J->bb * h;
+        const int64_t end = min(((int64_t)J->bb + 2) * h, seglen);
+        const int32_t W = (int32_t)(end - from);
+        for (int32_t i = lane; i < n_u; i += 32) cntA[i] = 0;
+        for (int32_t i = lane; i <= W; i += 32) D[i] = 0;
+        __syncwarp();
+        // phase 1: seed of every position, its occurrence interval of windows
+        for (int32_t c0 = 0; c0 < W; c0 += 32) {
+            const int32_t x = c0 + lane;  // position from + x
+            const bool valid = x < W;
+            int32_t s = -1;
+            uint32_t os = 0, rs = 0;
+            if (valid) {
+                const uint32_t gid = G0 + (uint32_t)(from + x);
+                rs = __ldg(I.ref_rs + gid);
+                uint32_t si;
+                if (pht_lookup(v, q, __ldg(I.ref_h + gid), si)) {
+                    s = (int32_t)si;
+                    os = v.sd_os[kb + si];
+                }
+            }
+            if (valid) C[x] = s >= 0 ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
+            const unsigned peers = __match_any_sync(0xffffffffu, s);
+            int32_t t = 0, occ = 1, rho = 0, gsz = 0;
+            uint32_t ooff = 0;
+            if (s >= 0) {
+                occ = (int32_t)(os >> 1);
+                rho = __popc(peers & lt);
+                gsz = __popc(peers);
+                t = cntA[s] + rho;
+                ooff = v.sd_ooff[kb + s];
+                int64_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
+                if (t >= occ) {
+                    if (rho >= occ) p = c0 + (int32_t)(__fns(peers, 0, rho - occ + 1));
+                    else p = ring[ooff + (uint32_t)(t % occ)];
+                }
+                int64_t Lj;
+                if (!ap) {
+                    Lj = (int64_t)x - m + 1;
+                } else {  // first l with R[l] > R[x] - m
+                    const int64_t rv = (int64_t)(rs >> 1) - m;
+                    int32_t lo = 0, len = x;
+                    while (len > 0) {
+                        int32_t half = len >> 1;
+                        if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
+                            lo += half + 1;
+                            len -= half + 1;
+                        } else {
+                            len = half;
+                        }
+                    }
+                    Lj = lo;
+                }
+                int64_t st = max(max(p + 1, Lj), (int64_t)0);
+                if (st <= x) {
+                    atomicAdd(D + st, 1);
+                    atomicAdd(D + x + 1, -1);
+                }
+            }
+            __syncwarp();
+            if (s >= 0) {
+                if (rho >= gsz - occ) ring[ooff + (uint32_t)(t % occ)] = x;
+                if (rho == gsz - 1) cntA[s] = t + 1;
+            }
+            __syncwarp();
+        }
+        // phase 2a: prefix of strand agreement
+        int32_t carry = 0;
+        for (int32_t c0 = 0; c0 < W; c0 += 32) {
+            const int32_t x = c0 + lane;
+            int32_t cv = x < W ? C[x] : 0;
+            int32_t inc = warp_inclusive_scan(cv);
+            if (x < W) PC[x + 1] = carry + inc;
+            carry += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        if (lane == 0) PC[0] = 0;
+        __syncwarp();
+        // phase 2b: intersection per window start, score, first maximum
+        double best = -1.0;
+        int32_t bl = -1, bI = 0, bS = 0, br = 0;
+        int32_t icarry = 0;
+        for (int32_t c0 = 0; c0 < W; c0 += 32) {
+            const int32_t x = c0 + lane;
+            int32_t dv = x < W ? D[x] : 0;
+            int32_t inc = warp_inclusive_scan(dv) + icarry;
+            icarry = __shfl_sync(0xffffffffu, inc, 31);
+            if (x < W) {
+                int32_t r;
+                if (!ap) {
+                    r = (int32_t)min((int64_t)x + m, (int64_t)W);
+                } else {
+                    const int64_t lim = (int64_t)(__ldg(I.ref_rs + G0 + from + x) >> 1) + m;
+                    int32_t lo = x, len = W - x;
+                    while (len > 0) {
+                        int32_t half = len >> 1;
+                        if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) < lim) {
+                            lo += half + 1;
+                            len -= half + 1;
+                        } else {
+                            len = half;
+                        }
+                    }
+                    r = lo;
+                }
+                const int32_t I_ = inc, sk = r - x;
+                const double score = v.P.metric == 1 ? __ddiv_rn((double)I_, (double)(m + sk - I_))
+                                                     : __ddiv_rn((double)I_, (double)m);
+                if (score > best) {
+                    best = score;
+                    bl = x;
+                    bI = I_;
+                    bS = PC[r] - PC[x];
+                    br = r;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            int32_t obl = __shfl_xor_sync(0xffffffffu, bl, o);
+            int32_t obI = __shfl_xor_sync(0xffffffffu, bI, o);
+            int32_t obS = __shfl_xor_sync(0xffffffffu, bS, o);
+            int32_t obr = __shfl_xor_sync(0xffffffffu, br, o);
+            bool take = ob > best || (ob == best && obl >= 0 && (bl < 0 || obl < bl));
+            if (take) {
+                best = ob;
+                bl = obl;
+                bI = obI;
+                bS = obS;
+                br = obr;
+            }
+        }
+        if (lane == 0) {
+            J->score = best;
+            if (bl >= 0) {
+                const int32_t tl = (int32_t)(__ldg(I.ref_rs + G0 + from + bl) >> 1);
+                const int32_t tr = (int32_t)(__ldg(I.ref_rs + G0 + from + br - 1) >> 1);
+                J->t_l = tl;
+                J->t_r = tr;
+                J->inter = bI;
+                J->same = bS;
+                J->s_sz = tr - tl + 1;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ K8 sweeps and record
+__device__ __forceinline__ bool cand_less(const BucketJob& a, const BucketJob& b) {
+    if (a.m0 != b.m0) return a.m0 > b.m0;  // get_sorted_buckets: matches desc (buckets.rs:697-704)
+    if (a.seg != b.seg) return a.seg < b.seg;
+    return a.bb < b.bb;
+}
+
+__device__ double overlap_of(const BucketJob& a, const BucketJob& b) {  // mapping.rs:412-420
+    if (a.seg != b.seg) return -0.0;
+    int32_t cap = max(0, min(a.t_r, b.t_r) - max(a.t_l, b.t_l));
+    int32_t cup = max(a.t_r, b.t_r) - min(a.t_l, b.t_l);
+    return __ddiv_rn((double)cap, (double)cup);
+}
+
+__global__ void __launch_bounds__(128) k_sweep(BatchView v, uint32_t* __restrict__ sort_scr) {
+    __shared__ uint32_t sidx[1024];
+    for (int32_t q = blockIdx.x; q < v.n; q += gridDim.x) {
+        const uint32_t c0 = v.coff[q], nc = v.coff[q + 1] - c0;
+        uint32_t* ix = nc <= 1024 ? sidx : sort_scr + c0;
+        for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) ix[i] = v.cidx[c0 + i];
+        __syncthreads();
+        // odd-even transposition sort (few candidates per read)
+        for (uint32_t phase = 0; phase < nc; phase++) {
+            for (uint32_t i = 2 * threadIdx.x + (phase & 1); i + 1 < nc; i += 2 * blockDim.x) {
+                if (cand_less(v.jobs[ix[i + 1]], v.jobs[ix[i]])) {
+                    uint32_t t = ix[i];
+                    ix[i] = ix[i + 1];
+                    ix[i + 1] = t;
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const int32_t st = v.r_status[q];
+            shm_map_record rec;
+            memset(&rec, 0, sizeof rec);
+            rec.read_len = (int32_t)(v.roff[q + 1] - v.roff[q]);
+            rec.sketch_size = v.r_m[q];
+            rec.seeds = v.r_S[q];
+            rec.total_matches = (int32_t)v.r_smatch[q];
+            rec.seed_matches = (int32_t)v.r_smatch[q];
+            rec.max_seed_matches = v.r_maxseed[q];
+            rec.seeded_buckets = (int32_t)v.r_seeded[q];
+            rec.bucket_seg = rec.bucket_b = rec.bucket2_seg = rec.bucket2_b = -1;
+            rec.intersection2 = -1;
+            rec.score2 = -1.0;
+            rec.status = st;
+            if (st == ST_UNMAPPED) {
+                const bool nbp = v.P.nbp != 0;
+                int32_t fb = 0;
+                // pass 1 (mod.rs:816-832): thr = theta, no forbidden region
+                double thr = v.P.theta;
+                int32_t b1 = -1;
+                for (uint32_t i = 0; i < nc; i++) {
+                    const BucketJob& c = v.jobs[ix[i]];
+                    if (!nbp && !(c.sh >= thr)) continue;
+                    if (c.score > thr) {
+                        fb++;
+                        if (b1 < 0 || c.score > v.jobs[b1].score) {
+                            thr = fmax(thr, c.score);
+                            b1 = (int32_t)ix[i];
+                        }
+                    }
+                }
+                int32_t b2 = -1;
+                if (b1 >= 0) {
+                    // pass 2 (mod.rs:835-859): thr = best * (1 - d), best forbidden
+                    const BucketJob& B1 = v.jobs[b1];
+                    thr = __dmul_rn(B1.score, __dsub_rn(1.0, v.P.min_diff));
+                    for (uint32_t i = 0; i < nc; i++) {
+                        const BucketJob& c = v.jobs[ix[i]];
+                        if (!nbp && !(c.sh >= thr)) continue;
+                        if (c.score > thr) {
+                            fb++;
+                            if (overlap_of(c, B1) < v.P.max_overlap) {
+                                if (b2 < 0 || c.score > v.jobs[b2].score) {
+                                    thr = fmax(thr, c.score);
+                                    b2 = (int32_t)ix[i];
+                                }
+                            }
+                        }
+                    }
+                }
+                rec.final_buckets = fb;
+                if (b1 >= 0) {
+                    const BucketJob& B = v.jobs[b1];
+                    rec.status = ST_MAPPED;
+                    rec.score = B.score;
+                    rec.sh = B.sh;
+                    rec.p_start = 0;
+                    rec.p_end = v.P.metric == 2 ? rec.read_len - 1 : rec.read_len - v.P.k - 1;
+                    rec.segm_id = B.seg;
+                    rec.t_l = B.t_l;
+                    rec.t_r = B.t_r;
+                    rec.same_strand = B.same;
+                    rec.intersection = B.inter;
+                    rec.s_sz = B.s_sz;
+                    rec.bucket_seg = B.seg;
+                    rec.bucket_b = B.bb;
+                    if (b2 >= 0) {
+                        const BucketJob& C2 = v.jobs[b2];
+                        rec.has_second = 1;
+                        rec.intersection2 = C2.inter;
+                        rec.score2 = C2.score;
+                        rec.bucket2_seg = C2.seg;
+                        rec.bucket2_b = C2.bb;
+                    }
+                }
+            } else if (st == ST_OVERFLOW) {
+                uint32_t k = atomicAdd(&v.mx->n_overflow, 1u);
+                v.ovf_list[k] = (uint32_t)q;
+            }
+            v.out[q] = rec;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ host side
+struct MapScratch {
+    DevBuf<uint8_t> seq;
+    DevBuf<int64_t> roff;
+    DevBuf<uint64_t> chunk_off, kcap_off, pht_off, km_h, sd_h, pht_key, hw, hw_off, bt_size, bt_off;
+    DevBuf<uint32_t> kcnt, km_rs, sd_a, sd_cnt, sd_os, sd_hpre, sd_ooff, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
+        cidx, sort_scr, ovf_list;
+    DevBuf<int32_t> r_i32, lists, ref_scr;
+    DevBuf<int64_t> r_smatch;
+    DevBuf<BSlot> bt;
+    DevBuf<BucketJob> jobs;
+    DevBuf<BatchMax> mx;
+    DevBuf<uint8_t> seed_gscr;
+    DevBuf<shm_map_record> out;
+    SketchLuts* luts = nullptr;
+    int32_t luts_k = -1;
+};
+
+MapCtx* mapctx_create(int device, size_t hbm_budget) {
+    SHM_CUDA(cudaSetDevice(device));
+    auto* c = new MapCtx();
+    c->device = device;
+    c->hbm_budget = hbm_budget;
+    SHM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->scr = new MapScratch();
+    return c;
+}
+
+void mapctx_destroy(MapCtx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->scr) {
+        if (c->scr->luts) cudaFree(c->scr->luts);
+        delete c->scr;
+    }
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+static uint64_t pow2_host(uint64_t x) {
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// k-mer capacity of a read of nw windows: the reference's own estimate
+// mean + 6 sigma + 16 (src/sketch.rs:143-146); reads that beat it are retried
+// with the exact bound.
+static uint64_t kmer_cap(int64_t nw, double h_frac, bool exact) {
+    if (nw <= 0) return 0;
+    if (exact || h_frac >= 1.0) return (uint64_t)nw;
+    double mean = std::max(0.0, (double)nw * h_frac);
+    uint64_t c = (uint64_t)(mean + 6.0 * std::sqrt(mean)) + 16;
+    return std::min<uint64_t>(c, (uint64_t)nw);
+}
+
+struct BatchPlan {
+    std::vector<int64_t> roff;
+    std::vector<uint64_t> chunk_off, kcap_off, pht_off;
+    std::vector<int32_t> list_s, list_m, list_g;
+    uint32_t P_s = 512, P_m = 2048, P_g = 0;
+};
+
+static const uint32_t P_SMALL = 512, P_MED = 2048;
+
+static void plan_batch(const int64_t* h_offs, int32_t n, int32_t k, double h_frac, bool exact, BatchPlan& bp) {
+    bp.roff.assign((size_t)n + 1, 0);
+    bp.chunk_off.assign((size_t)n + 1, 0);
+    bp.kcap_off.assign((size_t)n + 1, 0);
+    bp.pht_off.assign((size_t)n + 1, 0);
+    bp.list_s.clear();
+    bp.list_m.clear();
+    bp.list_g.clear();
+    bp.P_g = 0;
+    for (int32_t i = 0; i < n; i++) {
+        int64_t L = h_offs[i + 1] - h_offs[i];
+        bp.roff[(size_t)i + 1] = bp.roff[(size_t)i] + L;
+        int64_t nw = L - k + 1;
+        bp.chunk_off[(size_t)i + 1] = bp.chunk_off[(size_t)i] + (nw > 0 ? (uint64_t)((nw + SKETCH_WIN - 1) / SKETCH_WIN) : 0);
+        uint64_t cap = kmer_cap(nw, h_frac, exact);
+        bp.kcap_off[(size_t)i + 1] = bp.kcap_off[(size_t)i] + cap;
+        bp.pht_off[(size_t)i + 1] = bp.pht_off[(size_t)i] + std::max<uint64_t>(16, pow2_host(2 * cap));
+        uint64_t P = pow2_host(std::max<uint64_t>(cap, 1));
+        if (P <= P_SMALL) bp.list_s.push_back(i);
+        else if (P <= P_MED) bp.list_m.push_back(i);
+        else {
+            bp.list_g.push_back(i);
+            bp.P_g = std::max<uint32_t>(bp.P_g, (uint32_t)P);
+        }
+    }
+}
+
+template <class T>
+static void upload(DevBuf<T>& b, const std::vector<T>& h, cudaStream_t s) {
+    b.reserve(h.size() + 1);
+    if (!h.empty()) SHM_CUDA(cudaMemcpyAsync(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+}
+
+#define LAUNCHED(c) ((c)->launches++)
+
+// Maps one batch whose bytes are already on the device at d_seq (relative
+// offsets h_offs[i] - h_offs[0]). Returns the reads that overflowed a
+// capacity (retried by the caller with exact bounds).
+static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
+                                      const int64_t* h_offs, int32_t n, shm_map_record* d_out, bool exact) {
+    cudaStream_t s = c->stream;
+    MapScratch& S = *c->scr;
+    BatchPlan bp;
+    plan_batch(h_offs, n, p.k, p.h_frac, exact, bp);
+    if (!S.luts || S.luts_k != p.k) {
+        if (S.luts) SHM_CUDA(cudaFree(S.luts));
+        S.luts = create_device_luts(p.k, s);
+        S.luts_k = p.k;
+    }
+    const uint64_t kcap = bp.kcap_off[(size_t)n], phtn = bp.pht_off[(size_t)n];
+    upload(S.roff, bp.roff, s);
+    upload(S.chunk_off, bp.chunk_off, s);
+    upload(S.kcap_off, bp.kcap_off, s);
+    upload(S.pht_off, bp.pht_off, s);
+    S.kcnt.reserve((size_t)n);
+    S.km_h.reserve(kcap + 1);
+    S.km_rs.reserve(kcap + 1);
+    S.sd_h.reserve(kcap + 1);
+    S.sd_a.reserve(kcap + 1);
+    S.sd_cnt.reserve(kcap + 1);
+    S.sd_os.reserve(kcap + 1);
+    S.sd_hpre.reserve(kcap + 1);
+    S.sd_ooff.reserve(kcap + 1);
+    S.pht_key.reserve(phtn);
+    S.pht_val.reserve(phtn);
+    S.r_i32.reserve((size_t)n * 8);
+    S.r_smatch.reserve((size_t)n);
+    S.r_seeded.reserve((size_t)n);
+    S.hw.reserve((size_t)n);
+    S.hw_off.reserve((size_t)n + 1);
+    S.bt_size.reserve((size_t)n);
+    S.bt_off.reserve((size_t)n + 1);
+    S.ccnt.reserve((size_t)n);
+    S.coff.reserve((size_t)n + 1);
+    S.ccur.reserve((size_t)n);
+    S.ovf_list.reserve((size_t)n);
+    S.n_jobs.reserve(1);
+    S.mx.reserve(1);
+    SHM_CUDA(cudaMemsetAsync(S.kcnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    SHM_CUDA(cudaMemsetAsync(S.pht_val.p, 0xff, sizeof(uint32_t) * phtn, s));
+    SHM_CUDA(cudaMemsetAsync(S.r_seeded.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    SHM_CUDA(cudaMemsetAsync(S.ccnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    SHM_CUDA(cudaMemsetAsync(S.ccur.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    SHM_CUDA(cudaMemsetAsync(S.n_jobs.p, 0, sizeof(uint32_t), s));
+    SHM_CUDA(cudaMemsetAsync(S.mx.p, 0, sizeof(BatchMax), s));
+    SHM_CUDA(cudaMemsetAsync(S.r_i32.p, 0, sizeof(int32_t) * (size_t)n * 8, s));
+    SHM_CUDA(cudaMemsetAsync(S.hw.p, 0, sizeof(uint64_t) * (size_t)n, s));
+    SHM_CUDA(cudaMemsetAsync(S.bt_size.p, 0, sizeof(uint64_t) * (size_t)n, s));
+
+    BatchView v{};
+    v.n = n;
+    v.I = ix->dev;
+    v.P.k = p.k;
+    v.P.thr = ix->dev.thr;
+    v.P.theta = p.theta;
+    v.P.min_diff = p.min_diff;
+    v.P.max_overlap = p.max_overlap;
+    v.P.theta_low = p.theta * (1.0 - p.min_diff);
+    v.P.metric = p.metric;
+    v.P.nbp = p.no_bucket_pruning;
+    v.P.os = p.one_sweep;
+    v.P.ap = p.abs_pos;
+    v.theta2 = p.theta - p.min_diff;
+    v.seq = d_seq;
+    v.roff = S.roff.p;
+    v.kcap_off = S.kcap_off.p;
+    v.kcnt = S.kcnt.p;
+    v.km_h = S.km_h.p;
+    v.km_rs = S.km_rs.p;
+    v.sd_h = S.sd_h.p;
+    v.sd_a = S.sd_a.p;
+    v.sd_cnt = S.sd_cnt.p;
+    v.sd_os = S.sd_os.p;
+    v.sd_hpre = S.sd_hpre.p;
+    v.sd_ooff = S.sd_ooff.p;
+    v.pht_off = S.pht_off.p;
+    v.pht_key = S.pht_key.p;
+    v.pht_val = S.pht_val.p;
+    int32_t* ri = S.r_i32.p;
+    v.r_status = ri;
+    v.r_m = ri + n;
+    v.r_nu = ri + 2 * (size_t)n;
+    v.r_nproc = ri + 3 * (size_t)n;
+    v.r_S = ri + 4 * (size_t)n;
+    v.r_S0 = ri + 5 * (size_t)n;
+    v.r_half = ri + 6 * (size_t)n;
+    v.r_maxseed = ri + 7 * (size_t)n;
+    v.r_smatch = S.r_smatch.p;
+    v.r_seeded = S.r_seeded.p;
+    v.hw = S.hw.p;
+    v.hw_off = S.hw_off.p;
+    v.bt_size = S.bt_size.p;
+    v.bt_off = S.bt_off.p;
+    v.n_jobs = S.n_jobs.p;
+    v.ccnt = S.ccnt.p;
+    v.coff = S.coff.p;
+    v.ccur = S.ccur.p;
+    v.ovf_list = S.ovf_list.p;
+    v.mx = S.mx.p;
+    v.out = d_out;
+
+    // K1
+    SketchArgs a{};
+    a.seq = d_seq;
+    a.seq_off = S.roff.p;
+    a.chunk_off = S.chunk_off.p;
+    a.n_seq = n;
+    a.n_chunks = bp.chunk_off[(size_t)n];
+    a.k = p.k;
+    a.thr = ix->dev.thr;
+    a.r_offset = 0;
+    a.kmer_off = S.kcap_off.p;
+    a.kmer_cnt = S.kcnt.p;
+    a.out_h = S.km_h.p;
+    a.out_rs = S.km_rs.p;
+    launch_sketch(SK_APPEND, a, S.luts, s);
+    LAUNCHED(c);
+
+    // K2 per size bin
+    auto seed_bin = [&](const std::vector<int32_t>& L, uint32_t P, bool global) {
+        if (L.empty()) return;
+        S.lists.reserve(L.size());
+        SHM_CUDA(cudaMemcpyAsync(S.lists.p, L.data(), sizeof(int32_t) * L.size(), cudaMemcpyHostToDevice, s));
+        const size_t bytes = SEED_BYTES_PER_ELEM * P;
+        if (!global) {
+            int grid = grid_for(L.size() * 256, 256, 8);
+            SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            k_seedprep<false><<<grid, 256, bytes, s>>>(v, S.lists.p, (int32_t)L.size(), P, nullptr, 0);
+        } else {
+            int grid = (int)std::min<size_t>(L.size(), 296);
+            S.seed_gscr.reserve(bytes * (size_t)grid);
+            k_seedprep<true><<<grid, 256, 0, s>>>(v, S.lists.p, (int32_t)L.size(), P, S.seed_gscr.p, bytes);
+        }
+        SHM_CUDA(cudaGetLastError());
+        LAUNCHED(c);
+        SHM_CUDA(cudaStreamSynchronize(s));  // the list buffer is reused by the next bin
+    };
+    seed_bin(bp.list_s, P_SMALL, false);
+    seed_bin(bp.list_m, P_MED, false);
+    seed_bin(bp.list_g, bp.P_g, true);
+
+    exclusive_scan_u64(S.hw.p, S.hw_off.p, (size_t)n, s);
+    exclusive_scan_u64(S.bt_size.p, S.bt_off.p, (size_t)n, s);
+    uint64_t totals[2];
+    BatchMax hm{};
+    SHM_CUDA(cudaMemcpyAsync(&totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(&totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(&hm, S.mx.p, sizeof hm, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaStreamSynchronize(s));
+    const uint64_t hw_total = totals[0], bt_total = totals[1];
+
+    S.bt.reserve(bt_total + 1);
+    v.bt = S.bt.p;
+    if (bt_total) {
+        k_bt_init<<<grid_for(bt_total, 256), 256, 0, s>>>(S.bt.p, bt_total);
+        SHM_CUDA(cudaGetLastError());
+        LAUNCHED(c);
+    }
+    if (hw_total) {
+        k_contrib<<<grid_for(hw_total, 256, 8), 256, 0, s>>>(v);
+        SHM_CUDA(cudaGetLastError());
+        LAUNCHED(c);
+    }
+    uint32_t job_cap = (uint32_t)std::min<uint64_t>(bt_total + 1, (uint64_t)n * 64 + (1u << 20));
+    for (int attempt = 0;; attempt++) {
+        S.jobs.reserve(job_cap);
+        v.jobs = S.jobs.p;
+        v.job_cap = job_cap;
+        if (bt_total) {
+            k_bscan<<<grid_for(bt_total, 256, 8), 256, 0, s>>>(v);
+            SHM_CUDA(cudaGetLastError());
+            LAUNCHED(c);
+        }
+        uint32_t nj = 0;
+        SHM_CUDA(cudaMemcpyAsync(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaStreamSynchronize(s));
+        if (nj <= job_cap) break;
+        job_cap = nj;  // retry with room for every job
+        SHM_CUDA(cudaMemsetAsync(S.n_jobs.p, 0, sizeof(uint32_t), s));
+        SHM_CUDA(cudaMemsetAsync(S.ccnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
+        SHM_CUDA(cudaMemsetAsync(S.r_seeded.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    }
+    if (!p.no_bucket_pruning) {
+        k_extend<<<grid_for((size_t)job_cap * 32, 256, 8), 256, 0, s>>>(v);
+        SHM_CUDA(cudaGetLastError());
+        LAUNCHED(c);
+    }
+    exclusive_scan_u32(S.ccnt.p, S.coff.p, (size_t)n, s);
+    S.cidx.reserve(job_cap + 1);
+    S.sort_scr.reserve(job_cap + 1);
+    v.cidx = S.cidx.p;
+    k_cidx<<<grid_for(job_cap, 256, 8), 256, 0, s>>>(v);
+    SHM_CUDA(cudaGetLastError());
+    LAUNCHED(c);
+
+    RefScratch rsc{};
+    rsc.nu_max = hm.nu_max + 1;
+    rsc.wmax = 2 * hm.half_max + 2;
+    rsc.per_warp = (size_t)rsc.nu_max + 3 * ((size_t)rsc.wmax + 1) + (size_t)hm.m_max + 1;
+    size_t warps = (size_t)grid_for((size_t)job_cap * 32, 256, 8) * 8;
+    const size_t budget_ints = (size_t)1 << 28;  // 1 GiB of refinement scratch at most
+    while (warps > 8 && warps * rsc.per_warp > budget_ints) warps /= 2;
+    S.ref_scr.reserve(warps * rsc.per_warp);
+    rsc.base = S.ref_scr.p;
+    k_refine<<<(unsigned)std::max<size_t>(1, warps / 8), 256, 0, s>>>(v, rsc);
+    SHM_CUDA(cudaGetLastError());
+    LAUNCHED(c);
+    k_sweep<<<grid_for((size_t)n * 128, 128, 16), 128, 0, s>>>(v, S.sort_scr.p);
+    SHM_CUDA(cudaGetLastError());
+    LAUNCHED(c);
+
+    BatchMax fin{};
+    SHM_CUDA(cudaMemcpyAsync(&fin, S.mx.p, sizeof fin, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaStreamSynchronize(s));
+    std::vector<int32_t> ovf;
+    if (fin.n_overflow) {
+        std::vector<uint32_t> l(fin.n_overflow);
+        SHM_CUDA(cudaMemcpy(l.data(), S.ovf_list.p, sizeof(uint32_t) * l.size(), cudaMemcpyDeviceToHost));
+        for (uint32_t x : l) ovf.push_back((int32_t)x);
+        std::sort(ovf.begin(), ovf.end());
+    }
+    return ovf;
+}
+
+static const int64_t BATCH_BASES = (int64_t)256 << 20;
+static const int32_t BATCH_READS = 32768;
+
+void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
+                int32_t n, shm_map_record* d_out, bool plain) {
+    SHM_CUDA(cudaSetDevice(c->device));
+    int32_t i = 0;
+    while (i < n) {
+        int32_t j = i + 1;
+        if (!plain)
+            while (j < n && j - i < BATCH_READS && h_offs[j + 1] - h_offs[i] <= BATCH_BASES) j++;
+        const uint8_t* dseq = d_seq + (h_offs[i] - h_offs[0]);
+        // the batch's first read must start on a 16-byte boundary for the vector loads
+        std::vector<int32_t> ovf;
+        if (((uintptr_t)dseq & 15) == 0) {
+            ovf = run_batch(c, ix, p, dseq, h_offs + i, j - i, d_out + i, false);
+        } else {
+            MapScratch& S = *c->scr;
+            const int64_t nb = h_offs[j] - h_offs[i];
+            S.seq.reserve((size_t)nb + 32);
+            SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
+            SHM_CUDA(cudaMemcpyAsync(S.seq.p, dseq, (size_t)nb, cudaMemcpyDeviceToDevice, c->stream));
+            ovf = run_batch(c, ix, p, S.seq.p, h_offs + i, j - i, d_out + i, false);
+        }
+        // reads that beat a capacity estimate: once more, with exact bounds, one at a time
+        for (int32_t r : ovf) {
+            const int32_t g = i + r;
+            MapScratch& S = *c->scr;
+            const int64_t nb = h_offs[g + 1] - h_offs[g];
+            S.seq.reserve((size_t)nb + 32);
+            SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
+            SHM_CUDA(cudaMemcpyAsync(S.seq.p, d_seq + (h_offs[g] - h_offs[0]), (size_t)nb, cudaMemcpyDeviceToDevice,
+                                     c->stream));
+            std::vector<int32_t> again = run_batch(c, ix, p, S.seq.p, h_offs + g, 1, d_out + g, true);
+            if (!again.empty()) {
+                std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n", g);
+                throw shm_cuda_error(cudaErrorMemoryAllocation);
+            }
+        }
+        i = j;
+    }
+    SHM_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
+              int32_t n, shm_map_record* out, bool plain) {
+    SHM_CUDA(cudaSetDevice(c->device));
+    MapScratch& S = *c->scr;
+    int32_t i = 0;
+    while (i < n) {
+        int32_t j = i + 1;
+        if (!plain)
+            while (j < n && j - i < BATCH_READS && offs[j + 1] - offs[i] <= BATCH_BASES) j++;
+        const int64_t nb = offs[j] - offs[i];
+        S.seq.reserve((size_t)nb + 32);
+        S.out.reserve((size_t)(j - i));
+        SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
+        SHM_CUDA(cudaMemcpyAsync(S.seq.p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, c->stream));
+        std::vector<int64_t> ho(offs + i, offs + j + 1);
+        std::vector<int32_t> ovf = run_batch(c, ix, p, S.seq.p, ho.data(), j - i, S.out.p, false);
+        SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
+                                 c->stream));
+        SHM_CUDA(cudaStreamSynchronize(c->stream));
+        for (int32_t r : ovf) {
+            const int32_t g = i + r;
+            const int64_t lb = offs[g + 1] - offs[g];
+            DevBuf<uint8_t> one;
+            one.reserve((size_t)lb + 32);
+            SHM_CUDA(cudaMemsetAsync(one.p + lb, 0, 32, c->stream));
+            SHM_CUDA(cudaMemcpyAsync(one.p, seqs + offs[g], (size_t)lb, cudaMemcpyHostToDevice, c->stream));
+            int64_t o2[2] = {offs[g], offs[g + 1]};
+            std::vector<int32_t> again = run_batch(c, ix, p, one.p, o2, 1, S.out.p, true);
+            if (!again.empty()) {
+                std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n", g);
+                throw shm_cuda_error(cudaErrorMemoryAllocation);
+            }
+            SHM_CUDA(cudaMemcpyAsync(out + g, S.out.p, sizeof(shm_map_record), cudaMemcpyDeviceToHost, c->stream));
+            SHM_CUDA(cudaStreamSynchronize(c->stream));
+        }
+        i = j;
+    }
+}
+
+}  // namespace shm

@@ -1,0 +1,57 @@
+// Batched mapping on the device (see shm_map.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/shmap_gpu.h"
+#include "shm_internal.hpp"
+
+namespace shm {
+
+// One slot of a read's bucket hash table: a bucket (segm_id, b) and its
+// content after seeding (src/buckets.rs:64-73).
+struct BSlot {
+    unsigned long long key;  // (u64)segm_id << 32 | b, EMPTY_KEY when free
+    int32_t matches, codir, rmin, rmax;
+};
+
+// A bucket taken past seeding: extended by the seed heuristic, then (if it
+// can still clear a threshold) refined.
+struct BucketJob {
+    int32_t read, seg, bb, m0;            // location, matches after seeding (the sort key)
+    int32_t matches, codir, rmin, rmax;   // content after extension
+    double sh;                            // final seed-heuristic score (1.0 when pruning is off)
+    int32_t is_cand, pad0;
+    double score;                         // refinement result
+    int32_t t_l, t_r, inter, same, s_sz, pad1;
+};
+
+struct MapScratch;  // grow-only device buffers owned by a context
+
+struct MapCtx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    MapScratch* scr = nullptr;
+    size_t hbm_budget = 0;
+    int64_t launches = 0;
+    // host staging
+    uint8_t* h_pinned = nullptr;
+    size_t h_pinned_cap = 0;
+};
+
+MapCtx* mapctx_create(int device, size_t hbm_budget);
+void mapctx_destroy(MapCtx* c);
+
+// Maps reads [0, n) whose bytes are at d_seq (device) with host offsets
+// h_offs[0..n] (h_offs[0] may be nonzero: bytes are relative to d_seq - h_offs[0]).
+// Writes n records to d_out (device). plain = one read per launch sequence.
+void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
+                int32_t n, shm_map_record* d_out, bool plain);
+
+// Host-buffer form: copies each batch in, maps it, copies records out.
+void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
+              int32_t n, shm_map_record* out, bool plain);
+
+}  // namespace shm

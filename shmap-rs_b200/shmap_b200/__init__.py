@@ -1,0 +1,302 @@
+"""Python binding of the B200 mapping path (ctypes over lib/libshmapgpu.so).
+
+The library is the product: CUDA kernels for sm_100a behind the C ABI of
+include/shmap_gpu.h. This module only marshals arguments; it never computes a
+mapping itself, and it raises if the library is missing instead of falling
+back to anything.
+
+The API mirrors the reference crate's entry points for this path:
+``FracMinHash.sketch`` (src/sketch.rs), ``SketchIndex.build_index`` /
+``count`` (src/index.rs), ``Mapper.map_reads`` (src/mapper.rs,
+src/shmap/mod.rs) and the PAF writer (src/mapping.rs).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_DIR = os.path.join(PKG_ROOT, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libshmapgpu.so")
+SYNTH_PATH = os.path.join(LIB_DIR, "libshmapsynth.so")
+CLI_PATH = os.path.join(PKG_ROOT, "bin", "shmap")
+
+SHM_OK = 0
+CONTAINMENT, JACCARD, BUCKET_SH = 0, 1, 2
+METRICS = {"Containment": CONTAINMENT, "Jaccard": JACCARD, "bucket_SH": BUCKET_SH}
+
+# shm_map_record (include/shmap_gpu.h)
+RECORD_DTYPE = np.dtype(
+    [("score", "<f8"), ("sh", "<f8"), ("score2", "<f8")]
+    + [(n, "<i4") for n in (
+        "status", "read_len", "sketch_size", "seeds", "p_start", "p_end", "segm_id", "t_l", "t_r",
+        "same_strand", "intersection", "s_sz", "bucket_seg", "bucket_b", "has_second", "intersection2",
+        "bucket2_seg", "bucket2_b", "total_matches", "max_seed_matches", "seed_matches",
+        "seeded_buckets", "final_buckets", "reserved")],
+    align=True,
+)
+assert RECORD_DTYPE.itemsize == 120  # sizeof(shm_map_record)
+
+
+class ShmError(RuntimeError):
+    """A non-zero status from the C ABI, with the library's message."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"shmap-b200 error {code}: {msg}")
+        self.code = code
+
+
+class CParams(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_int32), ("h_frac", ctypes.c_double), ("max_matches", ctypes.c_int32),
+                ("theta", ctypes.c_double), ("min_diff", ctypes.c_double), ("max_overlap", ctypes.c_double),
+                ("metric", ctypes.c_int32), ("no_bucket_pruning", ctypes.c_int32), ("one_sweep", ctypes.c_int32),
+                ("abs_pos", ctypes.c_int32)]
+
+
+class CIndexStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "segments", "total_nucls", "indexed_hits", "indexed_kmers", "highest_freq_kmer",
+        "blacklisted_kmers", "blacklisted_hits", "sketched_kmers")]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libshmapgpu.so (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `make -C {PKG_ROOT}`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, i32, i64, u64, dbl, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double, ctypes.c_size_t
+    sig = {
+        "shm_last_error": (ctypes.c_char_p, []),
+        "shm_params_default": (None, [P]),
+        "shm_params_validate": (ctypes.c_int, [P]),
+        "shm_h_thres": (u64, [dbl]),
+        "shm_ctx_create": (ctypes.c_int, [ctypes.c_int, sz, P]),
+        "shm_ctx_destroy": (ctypes.c_int, [P]),
+        "shm_ctx_launches": (i64, [P]),
+        "shm_sketch": (ctypes.c_int, [P, P, i64, i32, dbl, i32, P, P, P, i64, P]),
+        "shm_index_build": (ctypes.c_int, [P, P, P, i32, ctypes.c_char_p, i32, dbl, i32, P]),
+        "shm_index_destroy": (ctypes.c_int, [P]),
+        "shm_index_stats_get": (ctypes.c_int, [P, P]),
+        "shm_index_count": (ctypes.c_int, [P, P, P, i64, P]),
+        "shm_index_hits": (ctypes.c_int, [P, P, u64, P, P, P, P, i64, P]),
+        "shm_index_segment": (ctypes.c_int, [P, P, i32, P, P, P, i64, P, ctypes.c_char_p, i32, P]),
+        "shm_map_batch": (ctypes.c_int, [P, P, P, P, P, i32, P]),
+        "shm_map_plain": (ctypes.c_int, [P, P, P, P, P, i32, P]),
+        "shm_map_batch_device": (ctypes.c_int, [P, P, P, P, P, P, i32, P]),
+        "shm_format_paf": (ctypes.c_int, [P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != SHM_OK:
+        raise ShmError(rc, lib().shm_last_error().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data if a.size else 0
+
+
+@dataclass
+class Params:
+    """The CLI parameters the mapping path reads (src/params.rs:20-186)."""
+    k: int = 15
+    h_frac: float = 0.05
+    max_matches: Optional[int] = None
+    theta: float = 0.9
+    min_diff: float = 0.02
+    max_overlap: float = 0.5
+    metric: str = "Containment"
+    no_bucket_pruning: bool = False
+    one_sweep: bool = False
+    abs_pos: bool = False
+
+    def c(self) -> CParams:
+        if self.metric not in METRICS:
+            raise ValueError(f"metric {self.metric!r} is not on the device path")
+        return CParams(self.k, self.h_frac, -1 if self.max_matches is None else self.max_matches, self.theta,
+                       self.min_diff, self.max_overlap, METRICS[self.metric], int(self.no_bucket_pruning),
+                       int(self.one_sweep), int(self.abs_pos))
+
+    def validate(self) -> None:
+        """Params::validate (src/params.rs:191-263); raises ShmError with the reference's message."""
+        cp = self.c()
+        _check(lib().shm_params_validate(ctypes.byref(cp)))
+
+
+def h_thres(h_frac: float) -> int:
+    return int(lib().shm_h_thres(h_frac))
+
+
+def pack(seqs: Sequence[bytes]) -> tuple[np.ndarray, np.ndarray]:
+    """Concatenates sequences into (bytes, offsets[n+1])."""
+    offs = np.zeros(len(seqs) + 1, dtype=np.int64)
+    if seqs:
+        offs[1:] = np.cumsum([len(s) for s in seqs])
+    buf = np.frombuffer(b"".join(seqs), dtype=np.uint8) if seqs else np.zeros(0, np.uint8)
+    return np.ascontiguousarray(buf), offs
+
+
+class Context:
+    """A device context (one GPU, one stream, grow-only scratch)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().shm_ctx_create(device, hbm_budget, ctypes.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib().shm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self) -> int:
+        return int(lib().shm_ctx_launches(self.h))
+
+    def sketch(self, seq: bytes, k: int, h_frac: float, offset: int = 0):
+        """FracMinHash::sketch_slice_into: arrays (r, h, strand) in sequence order."""
+        buf = np.frombuffer(seq, dtype=np.uint8)
+        cap = max(0, len(seq) - k + 1)
+        r = np.zeros(cap, np.int32)
+        h = np.zeros(cap, np.uint64)
+        st = np.zeros(cap, np.uint8)
+        n = ctypes.c_int64()
+        _check(lib().shm_sketch(self.h, _ptr(buf), len(seq), k, h_frac, offset, _ptr(r), _ptr(h), _ptr(st), cap,
+                                ctypes.byref(n)))
+        return r[:n.value], h[:n.value], st[:n.value]
+
+
+class SketchIndex:
+    """The reference index on the device (SketchIndex, src/index.rs)."""
+
+    def __init__(self, ctx: Context, names: Sequence[str], seq: np.ndarray, seg_off: np.ndarray, k: int,
+                 h_frac: float, max_matches: Optional[int] = None):
+        self.ctx = ctx
+        self.names = list(names)
+        self.k, self.h_frac = k, h_frac
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        seg_off = np.ascontiguousarray(seg_off, dtype=np.int64)
+        h = ctypes.c_void_p()
+        joined = "\n".join(self.names).encode()
+        _check(lib().shm_index_build(ctx.h, _ptr(seq), _ptr(seg_off), len(self.names), joined, k, h_frac,
+                                     -1 if max_matches is None else max_matches, ctypes.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_records(cls, ctx: Context, records: Sequence[tuple[str, bytes]], k: int, h_frac: float,
+                     max_matches: Optional[int] = None) -> "SketchIndex":
+        seq, off = pack([s for _, s in records])
+        return cls(ctx, [n for n, _ in records], seq, off, k, h_frac, max_matches)
+
+    def close(self) -> None:
+        if self.h:
+            lib().shm_index_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        st = CIndexStats()
+        _check(lib().shm_index_stats_get(self.h, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in CIndexStats._fields_}
+
+    def count(self, hashes: np.ndarray) -> np.ndarray:
+        """SketchIndex::count for every hash."""
+        hashes = np.ascontiguousarray(hashes, dtype=np.uint64)
+        out = np.zeros(len(hashes), np.int32)
+        _check(lib().shm_index_count(self.ctx.h, self.h, _ptr(hashes), len(hashes), _ptr(out)))
+        return out
+
+    def hits(self, h: int):
+        """The hit list of a hash in (segm_id, r) order: arrays (segm_id, tpos, r, strand)."""
+        n = ctypes.c_int64()
+        lib().shm_index_hits(self.ctx.h, self.h, h, 0, 0, 0, 0, 0, ctypes.byref(n))
+        cap = n.value
+        seg, tpos, r = (np.zeros(cap, np.int32) for _ in range(3))
+        st = np.zeros(cap, np.uint8)
+        _check(lib().shm_index_hits(self.ctx.h, self.h, h, _ptr(seg), _ptr(tpos), _ptr(r), _ptr(st), cap,
+                                    ctypes.byref(n)))
+        return seg, tpos, r, st
+
+    def segment(self, i: int):
+        """A segment's sketch (r, h, strand), its name and length."""
+        n = ctypes.c_int64()
+        nm = ctypes.create_string_buffer(4096)
+        ln = ctypes.c_int32()
+        lib().shm_index_segment(self.ctx.h, self.h, i, 0, 0, 0, 0, ctypes.byref(n), nm, 4096, ctypes.byref(ln))
+        cap = n.value
+        r = np.zeros(cap, np.int32)
+        h = np.zeros(cap, np.uint64)
+        st = np.zeros(cap, np.uint8)
+        _check(lib().shm_index_segment(self.ctx.h, self.h, i, _ptr(r), _ptr(h), _ptr(st), cap, ctypes.byref(n), nm,
+                                       4096, ctypes.byref(ln)))
+        return r, h, st, nm.value.decode(), ln.value
+
+    def map_reads(self, params: Params, seq: np.ndarray, offs: np.ndarray, plain: bool = False) -> np.ndarray:
+        """Mapper::map_reads for reads packed as (bytes, offsets): one record per read, in input order."""
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        n = len(offs) - 1
+        out = np.zeros(n, RECORD_DTYPE)
+        cp = params.c()
+        f = lib().shm_map_plain if plain else lib().shm_map_batch
+        _check(f(self.ctx.h, self.h, ctypes.byref(cp), _ptr(seq), _ptr(offs), n, _ptr(out)))
+        return out
+
+    def map_reads_device(self, params: Params, d_seq_ptr: int, h_offs: np.ndarray, d_out_ptr: int) -> None:
+        """The device-resident form: reads and records already in device memory."""
+        h_offs = np.ascontiguousarray(h_offs, dtype=np.int64)
+        cp = params.c()
+        _check(lib().shm_map_batch_device(self.ctx.h, self.h, ctypes.byref(cp), d_seq_ptr, 0, _ptr(h_offs),
+                                          len(h_offs) - 1, d_out_ptr))
+
+    def format_paf(self, params: Params, records: np.ndarray, names: Sequence[str],
+                   map_time: Optional[np.ndarray] = None) -> str:
+        """PAF lines of the mapped reads (src/mapping.rs Display impls)."""
+        records = np.ascontiguousarray(records, dtype=RECORD_DTYPE)
+        joined = "\n".join(names).encode()
+        cp = params.c()
+        mt = None if map_time is None else np.ascontiguousarray(map_time, dtype=np.float64)
+        need = ctypes.c_int64()
+        _check(lib().shm_format_paf(self.h, ctypes.byref(cp), _ptr(records), len(records), joined,
+                                    0 if mt is None else _ptr(mt), 0, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(need.value + 1)
+        _check(lib().shm_format_paf(self.h, ctypes.byref(cp), _ptr(records), len(records), joined,
+                                    0 if mt is None else _ptr(mt), buf, need.value, ctypes.byref(need)))
+        return buf.raw[:need.value].decode()
+
+
+def strip_timing(paf: str) -> str:
+    """Drops the wall-clock t:f: tag, as the reference's own golden test does (tests/golden_paf.rs:13-23)."""
+    return "\n".join("\t".join(f for f in line.split("\t") if not f.startswith("t:f:"))
+                     for line in paf.splitlines())
+
+
+from . import synth  # noqa: E402  (seeded workloads)
+from . import fasta  # noqa: E402

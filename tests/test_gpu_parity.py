@@ -1,0 +1,248 @@
+"""Parity of the device path with the CPU oracle (bit-exact: integers, hashes,
+indices and the f64 scores alike), through the C ABI. Run on a B200 with
+`pytest -m gpu`."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import shmap_b200 as sb
+from helpers import (floor_reads, floor_reference, lcg_dna, pack, record_mismatches, strip_t, thread_parity_workload,
+                     xorshift_dna)
+from shmap_b200 import fasta, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _both_indexes(ctx, records, k, r, max_matches=None):
+    g = sb.SketchIndex.from_records(ctx, records, k, r, max_matches)
+    o = O.Index.from_records(records, k, r, max_matches, threads=4)
+    return g, o
+
+
+def _compare_mapping(g, o, reads, **pkw):
+    names = [n for n, _ in reads]
+    seq, offs = pack([s for _, s in reads])
+    gp = sb.Params(**pkw)
+    op = O.params(**pkw)
+    grec = g.map_reads(gp, seq, offs)
+    orec = o.map_reads(op, seq, offs, threads=8)
+    mm = record_mismatches(grec, orec)
+    assert not mm, f"record mismatches (read, field, gpu, oracle): {mm}"
+    gpaf = strip_t(g.format_paf(gp, grec, names))
+    opaf = strip_t(o.paf(op, seq, offs, names, threads=8))
+    assert gpaf == opaf
+    return grec, gpaf
+
+
+# ---------------------------------------------------------------- sketch
+@pytest.mark.parametrize("k", [1, 5, 8, 15, 25, 31, 32, 33, 64, 65, 100])
+@pytest.mark.parametrize("r", [1.0, 0.5, 0.01])
+def test_sketch_parity(gpu_ctx, k, r):
+    seq = bytearray(lcg_dna(1000 + k, 5000))
+    for i in range(0, len(seq), 331):
+        seq[i] = ord("n")
+    for i in range(100, 160):
+        seq[i] = ord("N")
+    for i in range(2000, 2400):
+        seq[i] = seq[i] | 0x20  # lower case
+    seq[3000:3004] = b"RYK-"
+    seq = bytes(seq)
+    for off in (0, 7, 123456):
+        a = gpu_ctx.sketch(seq, k, r, off)
+        b = O.sketch(seq, k, r, off)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), (k, r, off)
+
+
+def test_sketch_edge_lengths(gpu_ctx):
+    for n in (0, 1, 7, 8, 9, 63, 64, 65, 127, 128, 129, 1000):
+        s = xorshift_dna(n + 3, n)
+        a = gpu_ctx.sketch(s, 8, 1.0)
+        b = O.sketch(s, 8, 1.0)
+        assert all(np.array_equal(x, y) for x, y in zip(a, b)), n
+
+
+# ---------------------------------------------------------------- index
+def test_index_known_answers(gpu_ctx):
+    """src/index.rs:715-769."""
+    for fa, counts, hits, kmers in ((">ref\nACCAGTACCA\n", [2, 1, 1, 1, 1, 1, 2], 7, 6),
+                                    (">segm1\nACCAGTACCA\n>segm2\nGGACCA\n", [3, 1, 1, 1, 1, 1, 3], 10, 8)):
+        recs = [(b.split("\n", 1)[0], b.split("\n", 1)[1].replace("\n", "").encode()) for b in fa.strip().split(">")[1:]]
+        g = sb.SketchIndex.from_records(gpu_ctx, recs, 4, 1.0)
+        _, h, _ = gpu_ctx.sketch(b"ACCAGTACCA", 4, 1.0)
+        assert list(g.count(h)) == counts
+        st = g.stats()
+        assert st["indexed_hits"] == hits and st["indexed_kmers"] == kmers
+
+
+@pytest.mark.parametrize("mm", [None, 1, 3])
+def test_index_parity_with_max_matches(gpu_ctx, mm):
+    """src/index.rs:264-376 incl. the -M cap, the erase and the statistics."""
+    rep = b"ACGTACGTACGTACGTACGT"
+    recs = [(f"segm{i}", rep + b"TTTTGGGGCCCCAAAA" + str(i).encode()) for i in range(10)]
+    recs += [("rand", xorshift_dna(5, 3000)), ("empty", b""), ("short", b"ACG"), ("rand2", xorshift_dna(6, 2000))]
+    for k, r in ((6, 1.0), (4, 1.0), (11, 0.5)):
+        g, o = _both_indexes(gpu_ctx, recs, k, r, mm)
+        assert g.stats() == o.stats()
+        for i in range(len(recs)):
+            gr, gh, gs, nm, ln = g.segment(i)
+            orr, oh, os_ = o.segment(i)
+            assert np.array_equal(gr, orr) and np.array_equal(gh, oh) and np.array_equal(gs, os_)
+            assert nm == recs[i][0] and ln == len(recs[i][1])
+        hs = np.unique(np.concatenate([o.segment(i)[1] for i in range(len(recs))] + [np.arange(50, dtype=np.uint64)]))
+        assert np.array_equal(g.count(hs), o.count(hs))
+        for h in hs[:: max(1, len(hs) // 200)]:
+            for x, y in zip(g.hits(int(h)), o.hits(int(h))):
+                assert np.array_equal(x, y)
+
+
+def test_index_parity_synthetic_genome(gpu_ctx):
+    gen = synth.Genome(synth.scaled(synth.REFS["human31"], 0.004))
+    recs = gen.records()
+    g, o = _both_indexes(gpu_ctx, recs, 25, 0.01)
+    assert g.stats() == o.stats()
+    allh = np.concatenate([o.segment(i)[1] for i in range(len(recs))])
+    assert np.array_equal(g.count(allh), o.count(allh))
+    rng = np.random.default_rng(0)
+    for h in rng.choice(allh, 300, replace=False):
+        for x, y in zip(g.hits(int(h)), o.hits(int(h))):
+            assert np.array_equal(x, y)
+
+
+# ---------------------------------------------------------------- mapping
+def test_golden_paf(gpu_ctx, golden_dir):
+    """tests/golden_paf.rs:25-53 on the device path."""
+    refs = fasta.read_fastx(os.path.join(golden_dir, "tiny_ref.fa"))
+    reads = fasta.read_fastx(os.path.join(golden_dir, "tiny_reads.fa"))
+    g = sb.SketchIndex.from_records(gpu_ctx, refs, 8, 1.0)
+    p = sb.Params(k=8, h_frac=1.0, theta=0.1)
+    seq, offs = pack([s for _, s in reads])
+    rec = g.map_reads(p, seq, offs)
+    paf = g.format_paf(p, rec, [n for n, _ in reads])
+    want = open(os.path.join(golden_dir, "tiny.golden.paf")).read().rstrip("\n")
+    assert strip_t(paf) == strip_t(want)
+
+
+def test_thread_parity_workload(gpu_ctx):
+    refs, reads = thread_parity_workload()
+    g, o = _both_indexes(gpu_ctx, refs, 12, 0.5)
+    rec, paf = _compare_mapping(g, o, reads, k=12, h_frac=0.5, theta=0.2)
+    assert len(paf.splitlines()) >= 50
+
+
+def test_sketch_floor(gpu_ctx):
+    """tests/short_read_sketch_floor.rs: K..K+3 unmapped, K+4.. mapped."""
+    ref = floor_reference()
+    g, o = _both_indexes(gpu_ctx, [("ref", ref)], 8, 1.0)
+    rec, _ = _compare_mapping(g, o, floor_reads(ref, [8, 9, 10, 11]), k=8, h_frac=1.0, theta=0.4)
+    assert (rec["status"] == 2).all()
+    rec, paf = _compare_mapping(g, o, floor_reads(ref, [12, 20, 48]), k=8, h_frac=1.0, theta=0.4)
+    assert (rec["status"] == 0).all() and len(paf.splitlines()) == 3
+    rec, paf = _compare_mapping(g, o, floor_reads(ref, [28, 8, 28, 9, 28]), k=8, h_frac=1.0, theta=0.4)
+    assert len(paf.splitlines()) == 3
+
+
+@pytest.fixture(scope="module")
+def uniform(gpu_ctx):
+    gen = synth.Genome(synth.REFS["uniform5m"])
+    reads = gen.reads(synth.READS["fixed10k"])
+    g, o = _both_indexes(gpu_ctx, gen.records(), 25, 0.01)
+    return gen, reads, g, o
+
+
+@pytest.mark.parametrize("pkw", [
+    dict(theta=0.4),
+    dict(theta=0.4, min_diff=0.075, max_overlap=0.3),
+    dict(theta=0.4, metric="Jaccard"),
+    dict(theta=0.4, metric="bucket_SH"),
+    dict(theta=0.9),
+    dict(theta=0.0),
+    dict(theta=0.4, min_diff=1.5),
+])
+def test_uniform_workload(uniform, pkw):
+    """The 5 Mbp / 2,000 x 10 kb workload at k=25, r=0.01."""
+    gen, (names, seq, offs), g, o = uniform
+    reads = [(names[i], seq[offs[i]:offs[i + 1]].tobytes()) for i in range(len(names))]
+    rec, paf = _compare_mapping(g, o, reads, k=25, h_frac=0.01, **pkw)
+    if pkw.get("theta") == 0.4 and "metric" not in pkw:
+        assert (rec["status"] == 0).mean() > 0.95
+
+
+@pytest.mark.parametrize("flags", [dict(no_bucket_pruning=True), dict(one_sweep=True), dict(abs_pos=True),
+                                   dict(no_bucket_pruning=True, one_sweep=True, abs_pos=True)])
+def test_const_generic_variants(gpu_ctx, uniform, flags):
+    """The (NBP, OS, AP) variants of src/mapper.rs:25-40."""
+    gen, (names, seq, offs), g, o = uniform
+    reads = [(names[i], seq[offs[i]:offs[i + 1]].tobytes()) for i in range(0, 300)]
+    _compare_mapping(g, o, reads, k=25, h_frac=0.01, theta=0.4, **flags)
+    refs, tr = thread_parity_workload()
+    g2, o2 = _both_indexes(gpu_ctx, refs, 12, 0.5)
+    _compare_mapping(g2, o2, tr, k=12, h_frac=0.5, theta=0.2, **flags)
+    _compare_mapping(g2, o2, tr, k=12, h_frac=0.5, theta=0.2, metric="bucket_SH", **flags)
+
+
+@pytest.fixture(scope="module")
+def human_small(gpu_ctx):
+    gen = synth.Genome(synth.scaled(synth.REFS["human31"], 0.01))
+    return gen
+
+
+@pytest.mark.parametrize("preset,r,metric", [("hifi", 0.01, "Containment"), ("ont", 0.01, "Containment"),
+                                             ("ont", 0.01, "Jaccard"), ("dense", 0.10, "bucket_SH"),
+                                             ("dense", 0.10, "Containment")])
+def test_human_like_workloads(gpu_ctx, human_small, preset, r, metric):
+    """Satellite arrays, interspersed repeats, HiFi/ONT/dense read shapes at 1% scale."""
+    gen = human_small
+    names, seq, offs = gen.reads(synth.scaled(synth.READS[preset], 300 / synth.READS[preset].n_reads))
+    reads = [(names[i], seq[offs[i]:offs[i + 1]].tobytes()) for i in range(len(names))]
+    g, o = _both_indexes(gpu_ctx, gen.records(), 25, r)
+    rec, paf = _compare_mapping(g, o, reads, k=25, h_frac=r, theta=0.4, metric=metric)
+    assert (rec["status"] == 0).mean() > 0.5
+
+
+def test_max_matches_mapping(gpu_ctx, human_small):
+    gen = human_small
+    names, seq, offs = gen.reads(synth.scaled(synth.READS["dense"], 0.001))
+    reads = [(names[i], seq[offs[i]:offs[i + 1]].tobytes()) for i in range(len(names))]
+    g, o = _both_indexes(gpu_ctx, gen.records(), 25, 0.01, max_matches=5)
+    _compare_mapping(g, o, reads, k=25, h_frac=0.01, theta=0.4, max_matches=5)
+
+
+def test_edge_reads(gpu_ctx, uniform):
+    """Empty, shorter than k, all-N (every window hashes to 0 and is kept: the
+    capacity-overflow retry), lower case, IUPAC bytes."""
+    gen, (names, seq, offs), g, o = uniform
+    r0 = seq[offs[0]:offs[1]].tobytes()
+    r1 = seq[offs[1]:offs[2]].tobytes()
+    reads = [("empty", b""), ("short", b"ACGTACGT"), ("allN", b"N" * 5000), ("lower", r0.lower()),
+             ("withN", r1[:3000] + b"N" * 500 + r1[3500:]), ("iupac", r0.replace(b"A", b"R", 50)),
+             ("ok", r1), ("mixedN", (b"N" * 30 + r0[:200]) * 20)]
+    _compare_mapping(g, o, reads, k=25, h_frac=0.01, theta=0.4)
+
+
+def test_plain_equals_batched(gpu_ctx, uniform):
+    """One-read-per-launch and batched forms give identical records (the
+    device analogue of the reference's thread-count invariance)."""
+    gen, (names, seq, offs), g, o = uniform
+    p = sb.Params(k=25, h_frac=0.01, theta=0.4)
+    sub = offs[:101]
+    a = g.map_reads(p, seq[: sub[-1]], sub)
+    b = g.map_reads(p, seq[: sub[-1]], sub, plain=True)
+    assert not record_mismatches(a, b)
+
+
+def test_device_resident_entry(gpu_ctx, uniform):
+    import torch
+
+    gen, (names, seq, offs), g, o = uniform
+    p = sb.Params(k=25, h_frac=0.01, theta=0.4)
+    d_seq = torch.empty(len(seq) + 32, dtype=torch.uint8, device="cuda")
+    d_seq[: len(seq)].copy_(torch.from_numpy(np.ascontiguousarray(seq)))
+    d_out = torch.empty(len(names) * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    g.map_reads_device(p, d_seq.data_ptr(), offs, d_out.data_ptr())
+    torch.cuda.synchronize()
+    rec = d_out.cpu().numpy().view(sb.RECORD_DTYPE)
+    want = o.map_reads(O.params(k=25, h_frac=0.01, theta=0.4), seq, offs, threads=8)
+    assert not record_mismatches(rec, want)
