@@ -41,6 +41,8 @@
 // All scores use explicit round-to-nearest f64 intrinsics.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -109,10 +111,11 @@ __device__ T block_scan_excl(T v, T* sh_warp, T* total) {
     return r;
 }
 
+// Block-wide sum; sh_tot must be shared memory (every thread reads it back).
 template <class T>
-__device__ T block_reduce_sum(T v, T* sh_warp) {
-    T tot;
-    block_scan_excl<T>(v, sh_warp, &tot);
+__device__ T block_reduce_sum(T v, T* sh_warp, T* sh_tot) {
+    block_scan_excl<T>(v, sh_warp, sh_tot);
+    T tot = *sh_tot;
     __syncthreads();
     return tot;
 }
@@ -342,9 +345,9 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
         po += occs;
         pc += cnt;
     }
-    const uint32_t n_proc = block_reduce_sum<uint32_t>(l_np, sw32);
-    const uint32_t S0 = block_reduce_sum<uint32_t>(l_s0, sw32);
-    const uint64_t smatch = block_reduce_sum<uint64_t>(l_sm, sw64);
+    const uint32_t n_proc = block_reduce_sum<uint32_t>(l_np, sw32, &t32);
+    const uint32_t S0 = block_reduce_sum<uint32_t>(l_s0, sw32, &t32);
+    const uint64_t smatch = block_reduce_sum<uint64_t>(l_sm, sw64, &t64);
     const uint32_t mxs = block_reduce_max(l_max, sw32);
     if (tid == 0) {
         v.r_status[q] = ST_UNMAPPED;
@@ -1216,6 +1219,27 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     SHM_CUDA(cudaMemcpyAsync(&hm, S.mx.p, sizeof hm, cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaStreamSynchronize(s));
     const uint64_t hw_total = totals[0], bt_total = totals[1];
+    const bool debug = std::getenv("SHMAP_DEBUG") != nullptr;
+    if (debug) {
+        std::fprintf(stderr, "[shmap] batch n=%d kcap=%llu hw_total=%llu bt_total=%llu m_max=%u nu_max=%u half_max=%u\n",
+                     n, (unsigned long long)kcap, (unsigned long long)hw_total, (unsigned long long)bt_total, hm.m_max,
+                     hm.nu_max, hm.half_max);
+        if (n <= 8) {
+            std::vector<int32_t> ri((size_t)n * 8);
+            std::vector<uint32_t> kc((size_t)n);
+            std::vector<uint64_t> hw((size_t)n), bs((size_t)n);
+            SHM_CUDA(cudaMemcpy(ri.data(), S.r_i32.p, sizeof(int32_t) * ri.size(), cudaMemcpyDeviceToHost));
+            SHM_CUDA(cudaMemcpy(kc.data(), S.kcnt.p, sizeof(uint32_t) * kc.size(), cudaMemcpyDeviceToHost));
+            SHM_CUDA(cudaMemcpy(hw.data(), S.hw.p, sizeof(uint64_t) * hw.size(), cudaMemcpyDeviceToHost));
+            SHM_CUDA(cudaMemcpy(bs.data(), S.bt_size.p, sizeof(uint64_t) * bs.size(), cudaMemcpyDeviceToHost));
+            for (int32_t q = 0; q < n; q++)
+                std::fprintf(stderr,
+                             "[shmap]  read %d kcnt=%u status=%d m=%d nu=%d nproc=%d S=%d S0=%d half=%d maxseed=%d "
+                             "hw=%llu bt=%llu\n",
+                             q, kc[q], ri[q], ri[n + q], ri[2 * n + q], ri[3 * n + q], ri[4 * n + q], ri[5 * n + q],
+                             ri[6 * n + q], ri[7 * n + q], (unsigned long long)hw[q], (unsigned long long)bs[q]);
+        }
+    }
 
     S.bt.reserve(bt_total + 1);
     v.bt = S.bt.p;
@@ -1280,6 +1304,22 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     BatchMax fin{};
     SHM_CUDA(cudaMemcpyAsync(&fin, S.mx.p, sizeof fin, cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaStreamSynchronize(s));
+    if (debug) {
+        uint32_t nj = 0, nc = 0;
+        SHM_CUDA(cudaMemcpy(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost));
+        SHM_CUDA(cudaMemcpy(&nc, S.coff.p + n, sizeof nc, cudaMemcpyDeviceToHost));
+        std::fprintf(stderr, "[shmap] jobs=%u (cap %u) candidates=%u overflow=%u\n", nj, job_cap, nc, fin.n_overflow);
+        if (nj && nj <= 16) {
+            std::vector<BucketJob> jb(nj);
+            SHM_CUDA(cudaMemcpy(jb.data(), S.jobs.p, sizeof(BucketJob) * nj, cudaMemcpyDeviceToHost));
+            for (auto& j : jb)
+                std::fprintf(stderr,
+                             "[shmap]  job read=%d seg=%d bb=%d m0=%d matches=%d codir=%d r=[%d,%d] sh=%.6f cand=%d "
+                             "score=%.6f t=[%d,%d] I=%d same=%d\n",
+                             j.read, j.seg, j.bb, j.m0, j.matches, j.codir, j.rmin, j.rmax, j.sh, j.is_cand, j.score,
+                             j.t_l, j.t_r, j.inter, j.same);
+        }
+    }
     std::vector<int32_t> ovf;
     if (fin.n_overflow) {
         std::vector<uint32_t> l(fin.n_overflow);

@@ -189,17 +189,23 @@ def human_small(gpu_ctx):
     return gen
 
 
-@pytest.mark.parametrize("preset,r,metric", [("hifi", 0.01, "Containment"), ("ont", 0.01, "Containment"),
-                                             ("ont", 0.01, "Jaccard"), ("dense", 0.10, "bucket_SH"),
-                                             ("dense", 0.10, "Containment")])
-def test_human_like_workloads(gpu_ctx, human_small, preset, r, metric):
-    """Satellite arrays, interspersed repeats, HiFi/ONT/dense read shapes at 1% scale."""
+@pytest.mark.parametrize("preset,r,metric,theta", [("hifi", 0.01, "Containment", 0.4),
+                                                   ("ont", 0.01, "Containment", 0.4),
+                                                   ("ont", 0.01, "Containment", 0.05),
+                                                   ("ont", 0.01, "Jaccard", 0.05),
+                                                   ("dense", 0.10, "bucket_SH", 0.4),
+                                                   ("dense", 0.10, "Containment", 0.4)])
+def test_human_like_workloads(gpu_ctx, human_small, preset, r, metric, theta):
+    """Satellite arrays, interspersed repeats, HiFi/ONT/dense read shapes at 1% scale.
+    (At 7% errors only ~0.93^25 = 16% of 25-mers survive, so ONT reads clear
+    -t 0.4 nowhere, in the oracle as on the device; a low -t maps them.)"""
     gen = human_small
     names, seq, offs = gen.reads(synth.scaled(synth.READS[preset], 300 / synth.READS[preset].n_reads))
     reads = [(names[i], seq[offs[i]:offs[i + 1]].tobytes()) for i in range(len(names))]
     g, o = _both_indexes(gpu_ctx, gen.records(), 25, r)
-    rec, paf = _compare_mapping(g, o, reads, k=25, h_frac=r, theta=0.4, metric=metric)
-    assert (rec["status"] == 0).mean() > 0.5
+    rec, paf = _compare_mapping(g, o, reads, k=25, h_frac=r, theta=theta, metric=metric)
+    if preset != "ont" or theta < 0.1:
+        assert (rec["status"] == 0).mean() > 0.5
 
 
 def test_max_matches_mapping(gpu_ctx, human_small):
