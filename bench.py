@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Throughput of the B200 long-read mapping path (reads/s), one JSON line.
+
+Workload (default): the human-scale HiFi-like configuration - a seeded 3.1 Gbp
+synthetic reference in 24 contigs of 50-250 Mbp with 3% tandem satellite
+arrays and 5% interspersed 6 kb repeats, and 150,000 lognormal(23 kb, 6 kb)
+reads clipped to 1-60 kb with 0.5% errors; k=25, r=0.01, t=0.4, Containment.
+A step maps every read of the workload once. The index is built on the device
+before timing. Inputs (3.4 GB of reads, a 1 GB index) are larger than L2.
+
+  value     reads/s with the reads already resident in HBM (device events,
+            max over ranks)
+  e2e       the same through shm_map_batch from pinned host buffers: the
+            host->device copy of the reads and the device->host copy of the
+            records are inside the timed region
+  roofline  the stage that takes the most device time, its algorithmic
+            bytes per launch over its average launch time (CUDA events on the
+            library's stream during the timed steps), against the measured
+            HBM copy bandwidth
+  cpu_baseline  the CPU oracle (the C++ restatement of the reference path;
+            the reference's Rust binary cannot be built here) on a bounded
+            sample of the same reads with every host core
+
+--impl reference times that CPU implementation alone (rank 0) on the same
+workload, each step a bounded sample.
+Multi-GPU: one process per GPU, each builds its own replica of the index and
+maps its own read set (weak scaling); no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "shmap-rs_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (reference preset, read preset, k, r, theta, metric, description)
+    "hifi": ("human31", "hifi", 25, 0.01, 0.4, "Containment",
+             "3.1 Gbp human-scale reference (24 contigs, 3% satellites, 5% repeats), 150,000 HiFi-like reads "
+             "(lognormal 23+-6 kb, 0.5% errors), k=25 r=0.01 t=0.4 Containment"),
+    "uniform": ("uniform5m", "fixed10k", 25, 0.01, 0.4, "Containment",
+                "5 Mbp uniform reference in 4 contigs, 2,000 x 10 kb reads with 1% errors, k=25 r=0.01 t=0.4"),
+    "ont": ("human31", "ont", 25, 0.01, 0.4, "Containment",
+            "3.1 Gbp human-scale reference, 92,000 ONT-like reads (lognormal 24+-15 kb, 7% errors)"),
+    "dense": ("human31", "dense", 25, 0.10, 0.4, "Containment",
+              "3.1 Gbp human-scale reference at r=0.10, 125,000 reads of 15 kb (1% errors, 20% satellite)"),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) > 8:
+                for i, n in enumerate(names):
+                    if r[5 + i].strip().lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def make_workload(name: str, rank: int, scale: float):
+    from shmap_b200 import synth
+
+    rp, qp, k, r, theta, metric, desc = WORKLOADS[name]
+    rspec = synth.REFS[rp]
+    qspec = synth.READS[qp]
+    if scale != 1.0:
+        rspec = synth.scaled(rspec, scale)
+        qspec = synth.scaled(qspec, scale)
+    qspec = synth.replace(qspec, seed=qspec.seed + 1000 * rank) if rank else qspec
+    t0 = time.time()
+    gen = synth.Genome(rspec)
+    t1 = time.time()
+    names, seq, offs = gen.reads(qspec)
+    t2 = time.time()
+    log(f"[bench] rank {rank}: reference {len(gen.seq) / 1e9:.3f} Gbp in {t1 - t0:.1f}s, "
+        f"{len(names)} reads / {len(seq) / 1e9:.3f} Gbp in {t2 - t1:.1f}s")
+    return gen, names, seq, offs, dict(k=k, r=r, theta=theta, metric=metric, desc=desc)
+
+
+def algorithmic_bytes(stage: str, w: dict) -> tuple[float, str]:
+    """Algorithmic bytes of one stage over the counted work (the per-unit figures
+    of the measurement plan): see DESIGN.md."""
+    if stage == "sketch":
+        return (w["bases"] * (1.0 / 4 + 1.0 / 8) + 16.0 * w["kmers"],
+                "ceil(L/4)+ceil(L/8) input bytes per base (2-bit + N-mask) + 16 B per selected k-mer")
+    if stage in ("seedprep",):
+        return 32.0 * w["distinct_seeds"] + 12.0 * w["kmers"], "32 B per count() probe + 12 B per read k-mer"
+    if stage in ("contrib", "extend", "bscan"):
+        return (32.0 * w["distinct_seeds"] + 12.0 * (w["seed_hits"] + w["extension_seeds"]),
+                "32 B per count() probe + 12 B per hit touched")
+    if stage == "refine":
+        return 12.0 * w["refine_kmers"], "12 B per reference k-mer of every refined window"
+    return 0.0, "n/a"
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import shmap_b200 as sb
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    gen, names, seq, offs, wk = make_workload(args.workload, rank, args.scale)
+    ctx = sb.Context(local)
+    t0 = time.time()
+    idx = sb.SketchIndex(ctx, gen.names, gen.seq, gen.seg_off, wk["k"], wk["r"])
+    torch.cuda.synchronize()
+    index_s = time.time() - t0
+    st = idx.stats()
+    log(f"[bench] rank {rank}: index on device in {index_s:.2f}s: {st}")
+    p = sb.Params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=wk["metric"])
+    n = len(names)
+    nbytes = int(offs[-1])
+
+    # device-resident inputs
+    d_seq = torch.empty(nbytes + 32, dtype=torch.uint8, device=f"cuda:{local}")
+    d_seq[:nbytes].copy_(torch.from_numpy(np.ascontiguousarray(seq)))
+    d_seq[nbytes:].zero_()
+    d_out = torch.empty(n * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+
+    def device_step():
+        idx.map_reads_device(p, d_seq.data_ptr(), offs, d_out.data_ptr())
+
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+    ctx.set_timing(False)
+    ctx.set_timing(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        device_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launches - launches0
+    clk = clocks.stop()
+    stages = ctx.stage_times()
+    work = ctx.work_stats()
+    ctx.set_timing(False)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    rec = d_out.cpu().numpy().view(sb.RECORD_DTYPE)
+    mapped = float((rec["status"] == 0).mean())
+
+    # end to end through the public C ABI, from pinned host memory
+    h_seq = torch.empty(nbytes + 32, dtype=torch.uint8).pin_memory()
+    h_seq[:nbytes].copy_(torch.from_numpy(np.ascontiguousarray(seq)))
+    h_out_t = torch.empty(n * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    h_seq_np = h_seq.numpy()
+    h_out = h_out_t.numpy().view(sb.RECORD_DTYPE)
+
+    def e2e_step():
+        cp = p.c()
+        sb._check(sb.lib().shm_map_batch(ctx.h, idx.h, ctypes.byref(cp), h_seq_np.ctypes.data,
+                                         offs.ctypes.data, n, h_out.ctypes.data))
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - w0) * 1e3)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    if not np.array_equal(h_out.view(np.uint8), rec.view(np.uint8)):
+        raise RuntimeError("e2e records differ from the device-resident records")
+
+    # plain one-read-per-launch form on a sample
+    plain = None
+    if rank == 0 and args.plain_sample > 0:
+        m = min(n, args.plain_sample)
+        sub_offs = offs[: m + 1].copy()
+        sub_seq = np.ascontiguousarray(seq[: sub_offs[-1]])
+        t0 = time.perf_counter()
+        prec = idx.map_reads(p, sub_seq, sub_offs, plain=True)
+        pt = time.perf_counter() - t0
+        if not np.array_equal(prec.view(np.uint8), rec[:m].view(np.uint8)):
+            raise RuntimeError("plain records differ from the batched records")
+        plain = {"reads_per_s": m / pt, "sample_reads": m}
+
+    result = None
+    if rank == 0:
+        reads_total = n * world
+        value = reads_total * args.steps / (ms / 1e3)
+        mbp = float(nbytes) * world * args.steps / (ms / 1e3) / 1e6
+        peak, peak_kind = load_peaks()
+        traffic = load_traffic()
+        top = max((s for s in stages if s != "aux"), key=lambda s: stages[s][0])
+        top_ms, top_calls = stages[top]
+        per_launch_s = top_ms / 1e3 / max(1, top_calls)
+        alg, alg_desc = algorithmic_bytes(top, work)
+        alg_per_launch = alg / max(1, top_calls)
+        achieved = alg_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+        tr = traffic.get(args.workload, {}).get(top)
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": tr, "kernel": top,
+                "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
+                "avg_launch_ms": round(per_launch_s * 1e3, 4), "launches": top_calls,
+                "algorithmic_bytes_per_launch": round(alg_per_launch), "algorithmic_bytes": alg_desc}
+        e2e_value = reads_total * args.steps / (e2e_ms / 1e3)
+        result = {
+            "metric": "reads/s (mapping, byte-identical PAF records)", "value": round(value, 1), "unit": "reads/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded generator, shapes of the benchmark configuration)",
+            "config": {"workload": args.workload, "description": wk["desc"], "reads_per_gpu": n,
+                       "bases_per_gpu": nbytes, "k": wk["k"], "r": wk["r"], "theta": wk["theta"],
+                       "metric": wk["metric"], "l2": "inputs larger than L2 (reads and index are GB-sized)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "scale": args.scale},
+            "mbp_per_s": round(mbp, 1),
+            "mapped_fraction": round(mapped, 4),
+            "index_build_s": round(index_s, 3),
+            "index": st,
+            "stages_ms": {k: round(v[0] / args.steps, 3) for k, v in stages.items()},
+            "work_per_step": {k: v // max(1, args.steps) for k, v in work.items()},
+            "roofline": roof,
+            "e2e": {"value": round(e2e_value, 1), "unit": "reads/s", "h2d_bytes_per_step": int(nbytes + 8 * (n + 1)),
+                    "d2h_bytes_per_step": int(n * sb.RECORD_DTYPE.itemsize), "ms_per_step": round(e2e_ms / args.steps, 3)},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        if plain:
+            result["plain_form"] = {"reads_per_s": round(plain["reads_per_s"], 1), "sample_reads": plain["sample_reads"],
+                                    "batched_e2e_over_plain": round(e2e_value / plain["reads_per_s"], 1)}
+    if world > 1:
+        torch.distributed.barrier()
+    idx.close()
+    ctx.close()
+    return result, (gen, names, seq, offs, wk)
+
+
+def cpu_reference(gen, names, seq, offs, wk, target_s: float, threads: int, steps: int = 1):
+    """The CPU oracle on a bounded sample: returns (reads/s, sample description, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # the checker / CPU baseline, never the measured product
+
+    t0 = time.time()
+    oi = O.Index(gen.names, gen.seq, gen.seg_off, wk["k"], wk["r"], threads=threads)
+    log(f"[bench] CPU oracle index in {time.time() - t0:.1f}s with {threads} threads")
+    p = O.params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=wk["metric"])
+    m = min(len(names), max(threads * 8, 256))
+    t = oi.time_map(p, seq, offs[: m + 1], threads)
+    rate = m / max(t, 1e-6)
+    m = int(min(len(names), max(m, rate * target_s)))
+    rates = []
+    for s in range(steps):
+        a = (s * m) % max(1, len(names) - m + 1)
+        sub = offs[a: a + m + 1] - offs[a]
+        t = oi.time_map(p, seq[offs[a]:], sub, threads)
+        rates.append(m / t)
+    return rates, f"{m} of the workload's {len(names)} reads per step, mapped by the C++ oracle with {threads} threads"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="hifi")
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests and profiling)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size, in seconds of work")
+    ap.add_argument("--plain-sample", type=int, default=400)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        gen, names, seq, offs, wk = make_workload(args.workload, 0, args.scale)
+        per_step = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+        rates, sample = cpu_reference(gen, names, seq, offs, wk, per_step, threads, steps=args.warmup + args.steps)
+        timed = rates[args.warmup:] or rates
+        v = statistics.mean(timed)
+        line = {"metric": "reads/s (mapping, byte-identical PAF records)", "value": round(v, 1), "unit": "reads/s",
+                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": args.workload, "description": wk["desc"]},
+                "cpu_baseline": {"value": round(v, 1), "unit": "reads/s", "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": round(v, 1), "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "the reference is Rust and no Rust toolchain exists on this image; this arm times the C++ "
+                        "restatement of its mapping path (oracle/) with every host core"}
+        print(json.dumps(line), flush=True)
+        return
+
+    result, data = run_ours(args, rank, world, local)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            gen, names, seq, offs, wk = data
+            rates, sample = cpu_reference(gen, names, seq, offs, wk, args.cpu_seconds, threads)
+            result["cpu_baseline"] = {"value": round(rates[0], 1), "unit": "reads/s", "cores": threads, "kind": "port",
+                                      "sample": sample}
+            result["cpu_baseline"]["e2e_speedup"] = round(result["e2e"]["value"] / rates[0], 2)
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

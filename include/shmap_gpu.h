@@ -147,9 +147,28 @@ int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const
 int shm_format_paf(const shm_index* idx, const shm_params* p, const shm_map_record* rec, int32_t n, const char* names,
                    const double* map_time, char* buf, int64_t cap, int64_t* n_out);
 
-/* Kernel launches this context issued so far (the bench reports the count
- * inside its timed region). */
+/* Kernel launches this library issued so far in this process (the bench
+ * reports the count inside its timed region). */
 int64_t shm_ctx_launches(const shm_ctx* ctx);
+
+/* The CUDA stream (cudaStream_t) every call of this context runs on, so a
+ * caller can bracket calls with its own events on the same stream. */
+void* shm_ctx_stream(const shm_ctx* ctx);
+
+/* Per-stage device timing with CUDA events on the context's stream (off by
+ * default). shm_ctx_stage_times fills up to n stages: accumulated
+ * milliseconds and number of timed launches; returns the number of stages.
+ * shm_stage_name(i) names stage i. on = 0 also clears the totals. */
+int shm_ctx_set_timing(shm_ctx* ctx, int on);
+int shm_ctx_stage_times(const shm_ctx* ctx, double* ms, int64_t* launches, int n);
+const char* shm_stage_name(int i);
+
+/* Work counters of every mapping call of this context (reads, bases,
+ * sketched k-mers, distinct seeds, processed seeds, seed hits gathered,
+ * buckets, bucket jobs, extension seeds, candidates, refined reference
+ * k-mers); cleared with shm_ctx_set_timing(ctx, 0). Returns the count. */
+int shm_ctx_work_stats(const shm_ctx* ctx, int64_t* out, int n);
+const char* shm_work_stat_name(int i);
 
 #ifdef __cplusplus
 }

@@ -116,7 +116,44 @@ int shm_ctx_destroy(shm_ctx* ctx) {
     return SHM_OK;
 }
 
-int64_t shm_ctx_launches(const shm_ctx* ctx) { return ctx && ctx->m ? ctx->m->launches : 0; }
+int64_t shm_ctx_launches(const shm_ctx* ctx) {
+    (void)ctx;
+    return shm::kernel_launches();
+}
+
+void* shm_ctx_stream(const shm_ctx* ctx) { return ctx && ctx->m ? (void*)ctx->m->stream : nullptr; }
+
+int shm_ctx_set_timing(shm_ctx* ctx, int on) {
+    if (!ctx) return fail(SHM_ERR_INVALID, "null ctx");
+    ctx->m->timing = on != 0;
+    if (!on) {
+        for (int i = 0; i < shm::N_STAGES; i++) {
+            ctx->m->stage_ms[i] = 0;
+            ctx->m->stage_calls[i] = 0;
+        }
+        for (int i = 0; i < shm::N_WORK; i++) ctx->m->work[i] = 0;
+    }
+    return SHM_OK;
+}
+
+int shm_ctx_stage_times(const shm_ctx* ctx, double* ms, int64_t* launches, int n) {
+    if (!ctx) return fail(SHM_ERR_INVALID, "null ctx");
+    for (int i = 0; i < shm::N_STAGES && i < n; i++) {
+        if (ms) ms[i] = ctx->m->stage_ms[i];
+        if (launches) launches[i] = ctx->m->stage_calls[i];
+    }
+    return shm::N_STAGES;
+}
+
+const char* shm_stage_name(int i) { return i >= 0 && i < shm::N_STAGES ? shm::STAGE_NAMES[i] : ""; }
+
+int shm_ctx_work_stats(const shm_ctx* ctx, int64_t* out, int n) {
+    if (!ctx) return fail(SHM_ERR_INVALID, "null ctx");
+    for (int i = 0; i < shm::N_WORK && i < n; i++) out[i] = ctx->m->work[i];
+    return shm::N_WORK;
+}
+
+const char* shm_work_stat_name(int i) { return i >= 0 && i < shm::N_WORK ? shm::WORK_NAMES[i] : ""; }
 
 int shm_sketch(shm_ctx* ctx, const uint8_t* seq, int64_t len, int32_t k, double h_frac, int32_t offset, int32_t* r,
                uint64_t* h, uint8_t* strand, int64_t cap, int64_t* n_out) {

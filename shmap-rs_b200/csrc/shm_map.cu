@@ -44,6 +44,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <tuple>
 #include <vector>
 
 #include "shm_common.cuh"
@@ -55,6 +56,7 @@ namespace shm {
 
 struct BatchMax {
     unsigned int m_max, nu_max, half_max, n_overflow;
+    unsigned long long kmers, distinct, proc_seeds, hits, buckets, ext_seeds, refine_kmers;
 };
 
 struct BatchView {
@@ -367,6 +369,10 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
         atomicMax(&v.mx->m_max, m);
         atomicMax(&v.mx->nu_max, n_u);
         atomicMax(&v.mx->half_max, (uint32_t)halflen);
+        atomicAdd(&v.mx->kmers, (unsigned long long)m);
+        atomicAdd(&v.mx->distinct, (unsigned long long)n_u);
+        atomicAdd(&v.mx->proc_seeds, (unsigned long long)n_proc);
+        atomicAdd(&v.mx->hits, (unsigned long long)smatch);
     }
 }
 
@@ -554,6 +560,7 @@ __global__ void __launch_bounds__(256) k_bscan(BatchView v) {
         if (s.key == EMPTY_KEY) continue;
         const int32_t q = (int32_t)ub_u64(v.bt_off, (uint32_t)v.n + 1, si) - 1;
         atomicAdd(v.r_seeded + q, 1u);  // seeded_buckets (mod.rs:794)
+        atomicAdd(&v.mx->buckets, 1ULL);
         BucketJob j;
         j.read = q;
         j.seg = (int32_t)(s.key >> 32);
@@ -600,7 +607,9 @@ __global__ void __launch_bounds__(256) k_extend(BatchView v) {
         const uint64_t kb = v.kcap_off[q];
         int32_t seeds = v.r_S0[q], matches = J->matches, codir = J->codir, rmin = J->rmin, rmax = J->rmax;
         bool stopped = false;
+        int32_t examined = 0;
         for (int32_t i0 = np; i0 < n_u; i0 += 32) {
+            examined += min(32, n_u - i0);
             const int32_t i = i0 + lane;
             const bool valid = i < n_u;
             int32_t ds = 0, dm = 0, dc = 0, rmn = INT32_MAX, rmx = -1;
@@ -635,6 +644,7 @@ __global__ void __launch_bounds__(256) k_extend(BatchView v) {
             rmin = min(rmin, rmn);
             rmax = max(rmax, rmx);
         }
+        if (lane == 0) atomicAdd(&v.mx->ext_seeds, (unsigned long long)examined);
         if (lane == 0 && !stopped) {
             J->sh = hseed(m, seeds, matches);
             J->matches = matches;
@@ -699,6 +709,7 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
         const int64_t from = (int64_t)J->bb * h;
         const int64_t end = min(((int64_t)J->bb + 2) * h, seglen);
         const int32_t W = (int32_t)(end - from);
+        if (lane == 0 && W > 0) atomicAdd(&v.mx->refine_kmers, (unsigned long long)W);
         for (int32_t i = lane; i < n_u; i += 32) cntA[i] = 0;
         for (int32_t i = lane; i <= W; i += 32) D[i] = 0;
         __syncwarp();
@@ -963,6 +974,52 @@ __global__ void __launch_bounds__(128) k_sweep(BatchView v, uint32_t* __restrict
 }
 
 // ------------------------------------------------------------------ host side
+const char* const STAGE_NAMES[N_STAGES] = {"sketch", "seedprep", "contrib", "bscan", "extend", "refine", "sweep", "aux"};
+const char* const WORK_NAMES[N_WORK] = {"reads", "bases", "kmers", "distinct_seeds", "processed_seeds",
+                                        "seed_hits", "buckets", "bucket_jobs", "extension_seeds", "candidates",
+                                        "refine_kmers"};
+
+// Event pairs around each stage of a batch, read back once the batch is done.
+struct StageTimer {
+    MapCtx* c;
+    size_t used = 0;
+    int cur = 0;
+    cudaEvent_t a = nullptr;
+    std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> rec;
+    explicit StageTimer(MapCtx* cc) : c(cc) {}
+    cudaEvent_t get() {
+        if (used < c->ev_pool.size()) return c->ev_pool[used++];
+        cudaEvent_t e;
+        SHM_CUDA(cudaEventCreate(&e));
+        c->ev_pool.push_back(e);
+        used++;
+        return e;
+    }
+    void begin(int st) {
+        count_launch();
+        if (!c->timing) return;
+        cur = st;
+        a = get();
+        SHM_CUDA(cudaEventRecord(a, c->stream));
+    }
+    void end() {
+        if (!c->timing) return;
+        cudaEvent_t b = get();
+        SHM_CUDA(cudaEventRecord(b, c->stream));
+        rec.emplace_back(cur, a, b);
+    }
+    void collect() {  // after the stream is synchronized
+        for (auto& r : rec) {
+            float ms = 0;
+            SHM_CUDA(cudaEventElapsedTime(&ms, std::get<1>(r), std::get<2>(r)));
+            c->stage_ms[std::get<0>(r)] += ms;
+            c->stage_calls[std::get<0>(r)] += 1;
+        }
+        rec.clear();
+        used = 0;
+    }
+};
+
 struct MapScratch {
     DevBuf<uint8_t> seq;
     DevBuf<int64_t> roff;
@@ -1062,7 +1119,6 @@ static void upload(DevBuf<T>& b, const std::vector<T>& h, cudaStream_t s) {
     if (!h.empty()) SHM_CUDA(cudaMemcpyAsync(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
 }
 
-#define LAUNCHED(c) ((c)->launches++)
 
 // Maps one batch whose bytes are already on the device at d_seq (relative
 // offsets h_offs[i] - h_offs[0]). Returns the reads that overflowed a
@@ -1071,6 +1127,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
                                       const int64_t* h_offs, int32_t n, shm_map_record* d_out, bool exact) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
+    StageTimer T(c);
     BatchPlan bp;
     plan_batch(h_offs, n, p.k, p.h_frac, exact, bp);
     if (!S.luts || S.luts_k != p.k) {
@@ -1184,8 +1241,9 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     a.kmer_cnt = S.kcnt.p;
     a.out_h = S.km_h.p;
     a.out_rs = S.km_rs.p;
+    T.begin(STG_SKETCH);
     launch_sketch(SK_APPEND, a, S.luts, s);
-    LAUNCHED(c);
+    T.end();
 
     // K2 per size bin
     auto seed_bin = [&](const std::vector<int32_t>& L, uint32_t P, bool global) {
@@ -1193,6 +1251,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
         S.lists.reserve(L.size());
         SHM_CUDA(cudaMemcpyAsync(S.lists.p, L.data(), sizeof(int32_t) * L.size(), cudaMemcpyHostToDevice, s));
         const size_t bytes = SEED_BYTES_PER_ELEM * P;
+        T.begin(STG_SEEDPREP);
         if (!global) {
             int grid = grid_for(L.size() * 256, 256, 8);
             SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -1203,7 +1262,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
             k_seedprep<true><<<grid, 256, 0, s>>>(v, S.lists.p, (int32_t)L.size(), P, S.seed_gscr.p, bytes);
         }
         SHM_CUDA(cudaGetLastError());
-        LAUNCHED(c);
+        T.end();
         SHM_CUDA(cudaStreamSynchronize(s));  // the list buffer is reused by the next bin
     };
     seed_bin(bp.list_s, P_SMALL, false);
@@ -1244,14 +1303,16 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     S.bt.reserve(bt_total + 1);
     v.bt = S.bt.p;
     if (bt_total) {
+        T.begin(STG_AUX);
         k_bt_init<<<grid_for(bt_total, 256), 256, 0, s>>>(S.bt.p, bt_total);
         SHM_CUDA(cudaGetLastError());
-        LAUNCHED(c);
+        T.end();
     }
     if (hw_total) {
+        T.begin(STG_CONTRIB);
         k_contrib<<<grid_for(hw_total, 256, 8), 256, 0, s>>>(v);
         SHM_CUDA(cudaGetLastError());
-        LAUNCHED(c);
+        T.end();
     }
     uint32_t job_cap = (uint32_t)std::min<uint64_t>(bt_total + 1, (uint64_t)n * 64 + (1u << 20));
     for (int attempt = 0;; attempt++) {
@@ -1259,9 +1320,10 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
         v.jobs = S.jobs.p;
         v.job_cap = job_cap;
         if (bt_total) {
+            T.begin(STG_BSCAN);
             k_bscan<<<grid_for(bt_total, 256, 8), 256, 0, s>>>(v);
             SHM_CUDA(cudaGetLastError());
-            LAUNCHED(c);
+            T.end();
         }
         uint32_t nj = 0;
         SHM_CUDA(cudaMemcpyAsync(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost, s));
@@ -1273,17 +1335,19 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
         SHM_CUDA(cudaMemsetAsync(S.r_seeded.p, 0, sizeof(uint32_t) * (size_t)n, s));
     }
     if (!p.no_bucket_pruning) {
+        T.begin(STG_EXTEND);
         k_extend<<<grid_for((size_t)job_cap * 32, 256, 8), 256, 0, s>>>(v);
         SHM_CUDA(cudaGetLastError());
-        LAUNCHED(c);
+        T.end();
     }
     exclusive_scan_u32(S.ccnt.p, S.coff.p, (size_t)n, s);
     S.cidx.reserve(job_cap + 1);
     S.sort_scr.reserve(job_cap + 1);
     v.cidx = S.cidx.p;
+    T.begin(STG_AUX);
     k_cidx<<<grid_for(job_cap, 256, 8), 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
-    LAUNCHED(c);
+    T.end();
 
     RefScratch rsc{};
     rsc.nu_max = hm.nu_max + 1;
@@ -1294,16 +1358,35 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     while (warps > 8 && warps * rsc.per_warp > budget_ints) warps /= 2;
     S.ref_scr.reserve(warps * rsc.per_warp);
     rsc.base = S.ref_scr.p;
+    T.begin(STG_REFINE);
     k_refine<<<(unsigned)std::max<size_t>(1, warps / 8), 256, 0, s>>>(v, rsc);
     SHM_CUDA(cudaGetLastError());
-    LAUNCHED(c);
+    T.end();
+    T.begin(STG_SWEEP);
     k_sweep<<<grid_for((size_t)n * 128, 128, 16), 128, 0, s>>>(v, S.sort_scr.p);
     SHM_CUDA(cudaGetLastError());
-    LAUNCHED(c);
+    T.end();
 
     BatchMax fin{};
     SHM_CUDA(cudaMemcpyAsync(&fin, S.mx.p, sizeof fin, cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaStreamSynchronize(s));
+    T.collect();
+    {
+        uint32_t nj = 0, nc = 0;
+        SHM_CUDA(cudaMemcpy(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost));
+        SHM_CUDA(cudaMemcpy(&nc, S.coff.p + n, sizeof nc, cudaMemcpyDeviceToHost));
+        c->work[W_READS] += n;
+        c->work[W_BASES] += h_offs[n] - h_offs[0];
+        c->work[W_KMERS] += (int64_t)fin.kmers;
+        c->work[W_DISTINCT] += (int64_t)fin.distinct;
+        c->work[W_PROC_SEEDS] += (int64_t)fin.proc_seeds;
+        c->work[W_HITS] += (int64_t)fin.hits;
+        c->work[W_BUCKETS] += (int64_t)fin.buckets;
+        c->work[W_JOBS] += nj;
+        c->work[W_EXT_SEEDS] += (int64_t)fin.ext_seeds;
+        c->work[W_CANDS] += nc;
+        c->work[W_REFINE_KMERS] += (int64_t)fin.refine_kmers;
+    }
     if (debug) {
         uint32_t nj = 0, nc = 0;
         SHM_CUDA(cudaMemcpy(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost));

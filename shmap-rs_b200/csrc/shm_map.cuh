@@ -30,6 +30,16 @@ struct BucketJob {
 
 struct MapScratch;  // grow-only device buffers owned by a context
 
+// Stages timed with CUDA events on the context's stream when timing is on.
+enum Stage { STG_SKETCH, STG_SEEDPREP, STG_CONTRIB, STG_BSCAN, STG_EXTEND, STG_REFINE, STG_SWEEP, STG_AUX, N_STAGES };
+extern const char* const STAGE_NAMES[N_STAGES];
+
+// Work done, accumulated over every batch of a context: the units the
+// roofline's algorithmic bytes are counted in.
+enum Work { W_READS, W_BASES, W_KMERS, W_DISTINCT, W_PROC_SEEDS, W_HITS, W_BUCKETS, W_JOBS, W_EXT_SEEDS, W_CANDS,
+            W_REFINE_KMERS, N_WORK };
+extern const char* const WORK_NAMES[N_WORK];
+
 struct MapCtx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -39,6 +49,13 @@ struct MapCtx {
     // host staging
     uint8_t* h_pinned = nullptr;
     size_t h_pinned_cap = 0;
+    // work counters (always on): see WORK_NAMES
+    int64_t work[16] = {};
+    // stage timing
+    bool timing = false;
+    double stage_ms[N_STAGES] = {};
+    int64_t stage_calls[N_STAGES] = {};
+    std::vector<cudaEvent_t> ev_pool;
 };
 
 MapCtx* mapctx_create(int device, size_t hbm_budget);

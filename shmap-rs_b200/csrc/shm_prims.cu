@@ -1,6 +1,7 @@
 // Exclusive scan (reduce / scan-of-sums / apply, recursive) and the stable LSD
 // radix sort used to build the reference index on the device.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "shm_common.cuh"
@@ -9,6 +10,10 @@
 namespace shm {
 
 static int g_num_sms = 0;
+static std::atomic<int64_t> g_launches{0};
+
+int64_t kernel_launches() { return g_launches.load(); }
+void count_launch(int64_t n) { g_launches.fetch_add(n); }
 
 int grid_for(size_t work, int block, int max_blocks_per_sm) {
     if (g_num_sms == 0) {
@@ -95,6 +100,7 @@ static void exclusive_scan_impl(const T* in, T* out, size_t n, cudaStream_t s) {
     if (nb == 1) {
         k_scan_apply<T><<<1, SCAN_THREADS, 0, s>>>(in, n, nullptr, out, true);
         SHM_CUDA(cudaGetLastError());
+        count_launch();
         return;
     }
     T* sums = nullptr;
@@ -104,6 +110,7 @@ static void exclusive_scan_impl(const T* in, T* out, size_t n, cudaStream_t s) {
     exclusive_scan_impl<T>(sums, sums, nb, s);  // in-place is safe: each level reads before it writes per tile
     k_scan_apply<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums, out, true);
     SHM_CUDA(cudaGetLastError());
+    count_launch(2);
     SHM_CUDA(cudaFreeAsync(sums, s));
 }
 
@@ -212,6 +219,7 @@ bool radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, si
         exclusive_scan_u32(hist, off, (size_t)RS_BINS * nb, s);
         k_rs_scatter<<<nb, RS_THREADS, 0, s>>>(ki, vi, n, shift, off, nb, ko, vo);
         SHM_CUDA(cudaGetLastError());
+        count_launch(2);
         flipped = !flipped;
     }
     SHM_CUDA(cudaFreeAsync(hist, s));

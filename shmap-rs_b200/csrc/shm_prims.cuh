@@ -16,6 +16,10 @@ void exclusive_scan_u64(const uint64_t* in, uint64_t* out, size_t n, cudaStream_
 bool radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, size_t n, int key_bits,
                       cudaStream_t s);
 
+// Kernels this process launched (every launch site of the library bumps it).
+int64_t kernel_launches();
+void count_launch(int64_t n = 1);
+
 // Grid size for grid-stride kernels: a multiple of the SM count.
 int grid_for(size_t work, int block, int max_blocks_per_sm = 8);
 

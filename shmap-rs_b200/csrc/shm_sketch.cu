@@ -154,6 +154,7 @@ void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStrea
     else if (mode == SK_WRITE) k_sketch<SK_WRITE><<<grid, 256, 0, s>>>(a, L);
     else k_sketch<SK_APPEND><<<grid, 256, 0, s>>>(a, L);
     SHM_CUDA(cudaGetLastError());
+    count_launch();
 }
 
 }  // namespace shm

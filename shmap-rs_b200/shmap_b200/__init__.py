@@ -94,6 +94,12 @@ def lib() -> ctypes.CDLL:
         "shm_map_plain": (ctypes.c_int, [P, P, P, P, P, i32, P]),
         "shm_map_batch_device": (ctypes.c_int, [P, P, P, P, P, P, i32, P]),
         "shm_format_paf": (ctypes.c_int, [P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
+        "shm_ctx_stream": (P, [P]),
+        "shm_ctx_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
+        "shm_ctx_stage_times": (ctypes.c_int, [P, P, P, ctypes.c_int]),
+        "shm_stage_name": (ctypes.c_char_p, [ctypes.c_int]),
+        "shm_ctx_work_stats": (ctypes.c_int, [P, P, ctypes.c_int]),
+        "shm_work_stat_name": (ctypes.c_char_p, [ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -174,6 +180,27 @@ class Context:
     @property
     def launches(self) -> int:
         return int(lib().shm_ctx_launches(self.h))
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t (as an int) every call of this context runs on."""
+        return int(lib().shm_ctx_stream(self.h) or 0)
+
+    def set_timing(self, on: bool) -> None:
+        _check(lib().shm_ctx_set_timing(self.h, int(on)))
+
+    def stage_times(self) -> dict:
+        """{stage: (milliseconds, timed launches)} accumulated since timing was switched on."""
+        ms = np.zeros(16, np.float64)
+        cnt = np.zeros(16, np.int64)
+        n = lib().shm_ctx_stage_times(self.h, _ptr(ms), _ptr(cnt), 16)
+        return {lib().shm_stage_name(i).decode(): (float(ms[i]), int(cnt[i])) for i in range(n)}
+
+    def work_stats(self) -> dict:
+        """Work counters of every mapping call since the last reset (set_timing(False))."""
+        out = np.zeros(32, np.int64)
+        n = lib().shm_ctx_work_stats(self.h, _ptr(out), 32)
+        return {lib().shm_work_stat_name(i).decode(): int(out[i]) for i in range(n)}
 
     def sketch(self, seq: bytes, k: int, h_frac: float, offset: int = 0):
         """FracMinHash::sketch_slice_into: arrays (r, h, strand) in sequence order."""
