@@ -856,38 +856,99 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
 }
 
 // ------------------------------------------------------------------ K8 sweeps and record
-__device__ __forceinline__ bool cand_less(const BucketJob& a, const BucketJob& b) {
+// Per read (one warp): the candidates in the reference's bucket order, then
+// the two sweeps on their precomputed results. Small candidate sets are
+// staged in shared memory and rank-sorted; large ones are bitonic-sorted in a
+// global scratch region by the same warp.
+constexpr int SWEEP_WARPS = 4;
+constexpr int SWEEP_CAP = 64;
+
+struct SweepCand {
+    double sh, score;
+    int32_t seg, bb, m0, t_l, t_r, job;
+};
+
+__device__ __forceinline__ bool sc_less(const SweepCand& a, const SweepCand& b) {
     if (a.m0 != b.m0) return a.m0 > b.m0;  // get_sorted_buckets: matches desc (buckets.rs:697-704)
     if (a.seg != b.seg) return a.seg < b.seg;
     return a.bb < b.bb;
 }
 
-__device__ double overlap_of(const BucketJob& a, const BucketJob& b) {  // mapping.rs:412-420
+__device__ __forceinline__ SweepCand load_cand(const BucketJob& j, uint32_t ji) {
+    SweepCand c;
+    c.sh = j.sh;
+    c.score = j.score;
+    c.seg = j.seg;
+    c.bb = j.bb;
+    c.m0 = j.m0;
+    c.t_l = j.t_l;
+    c.t_r = j.t_r;
+    c.job = (int32_t)ji;
+    return c;
+}
+
+__device__ double overlap_of(const SweepCand& a, const SweepCand& b) {  // mapping.rs:412-420
     if (a.seg != b.seg) return -0.0;
     int32_t cap = max(0, min(a.t_r, b.t_r) - max(a.t_l, b.t_l));
     int32_t cup = max(a.t_r, b.t_r) - min(a.t_l, b.t_l);
     return __ddiv_rn((double)cap, (double)cup);
 }
 
-__global__ void __launch_bounds__(128) k_sweep(BatchView v, uint32_t* __restrict__ sort_scr) {
-    __shared__ uint32_t sidx[1024];
-    for (int32_t q = blockIdx.x; q < v.n; q += gridDim.x) {
+__global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCand* __restrict__ big_scr) {
+    __shared__ SweepCand sm[SWEEP_WARPS][SWEEP_CAP];
+    __shared__ SweepCand srt[SWEEP_WARPS][SWEEP_CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int32_t gw = blockIdx.x * SWEEP_WARPS + w, nwarps = gridDim.x * SWEEP_WARPS;
+    for (int32_t q = gw; q < v.n; q += nwarps) {
         const uint32_t c0 = v.coff[q], nc = v.coff[q + 1] - c0;
-        uint32_t* ix = nc <= 1024 ? sidx : sort_scr + c0;
-        for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) ix[i] = v.cidx[c0 + i];
-        __syncthreads();
-        // odd-even transposition sort (few candidates per read)
-        for (uint32_t phase = 0; phase < nc; phase++) {
-            for (uint32_t i = 2 * threadIdx.x + (phase & 1); i + 1 < nc; i += 2 * blockDim.x) {
-                if (cand_less(v.jobs[ix[i + 1]], v.jobs[ix[i]])) {
-                    uint32_t t = ix[i];
-                    ix[i] = ix[i + 1];
-                    ix[i + 1] = t;
+        const SweepCand* L;
+        if (nc <= SWEEP_CAP) {
+            for (uint32_t i = lane; i < nc; i += 32) {
+                uint32_t ji = v.cidx[c0 + i];
+                sm[w][i] = load_cand(v.jobs[ji], ji);
+            }
+            __syncwarp();
+            for (uint32_t i = lane; i < nc; i += 32) {
+                const SweepCand me = sm[w][i];
+                uint32_t rank = 0;
+                for (uint32_t k = 0; k < nc; k++) rank += sc_less(sm[w][k], me) ? 1u : 0u;
+                srt[w][rank] = me;
+            }
+            __syncwarp();
+            L = srt[w];
+        } else {
+            // regions of 2*nc slots at 2*c0 hold a power of two >= nc
+            SweepCand* G = big_scr + 2 * (size_t)c0;
+            uint32_t P = 1;
+            while (P < nc) P <<= 1;
+            for (uint32_t i = lane; i < P; i += 32) {
+                if (i < nc) {
+                    uint32_t ji = v.cidx[c0 + i];
+                    G[i] = load_cand(v.jobs[ji], ji);
+                } else {
+                    G[i].m0 = INT32_MIN;  // sorts after every real candidate
+                    G[i].seg = INT32_MAX;
+                    G[i].bb = INT32_MAX;
+                    G[i].job = -1;
                 }
             }
-            __syncthreads();
+            __syncwarp();
+            for (uint32_t k = 2; k <= P; k <<= 1)
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t t = lane; t < P / 2; t += 32) {
+                        uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                        bool asc = (i & k) == 0;
+                        SweepCand a = G[i], b = G[l];
+                        if (sc_less(b, a) == asc) {
+                            G[i] = b;
+                            G[l] = a;
+                        }
+                    }
+                    __syncwarp();
+                }
+            L = G;
         }
-        if (threadIdx.x == 0) {
+        if (lane == 0) {
             const int32_t st = v.r_status[q];
             shm_map_record rec;
             memset(&rec, 0, sizeof rec);
@@ -909,30 +970,30 @@ __global__ void __launch_bounds__(128) k_sweep(BatchView v, uint32_t* __restrict
                 double thr = v.P.theta;
                 int32_t b1 = -1;
                 for (uint32_t i = 0; i < nc; i++) {
-                    const BucketJob& c = v.jobs[ix[i]];
+                    const SweepCand& c = L[i];
                     if (!nbp && !(c.sh >= thr)) continue;
                     if (c.score > thr) {
                         fb++;
-                        if (b1 < 0 || c.score > v.jobs[b1].score) {
+                        if (b1 < 0 || c.score > L[b1].score) {
                             thr = fmax(thr, c.score);
-                            b1 = (int32_t)ix[i];
+                            b1 = (int32_t)i;
                         }
                     }
                 }
                 int32_t b2 = -1;
                 if (b1 >= 0) {
                     // pass 2 (mod.rs:835-859): thr = best * (1 - d), best forbidden
-                    const BucketJob& B1 = v.jobs[b1];
+                    const SweepCand B1 = L[b1];
                     thr = __dmul_rn(B1.score, __dsub_rn(1.0, v.P.min_diff));
                     for (uint32_t i = 0; i < nc; i++) {
-                        const BucketJob& c = v.jobs[ix[i]];
+                        const SweepCand& c = L[i];
                         if (!nbp && !(c.sh >= thr)) continue;
                         if (c.score > thr) {
                             fb++;
                             if (overlap_of(c, B1) < v.P.max_overlap) {
-                                if (b2 < 0 || c.score > v.jobs[b2].score) {
+                                if (b2 < 0 || c.score > L[b2].score) {
                                     thr = fmax(thr, c.score);
-                                    b2 = (int32_t)ix[i];
+                                    b2 = (int32_t)i;
                                 }
                             }
                         }
@@ -940,7 +1001,7 @@ __global__ void __launch_bounds__(128) k_sweep(BatchView v, uint32_t* __restrict
                 }
                 rec.final_buckets = fb;
                 if (b1 >= 0) {
-                    const BucketJob& B = v.jobs[b1];
+                    const BucketJob& B = v.jobs[L[b1].job];
                     rec.status = ST_MAPPED;
                     rec.score = B.score;
                     rec.sh = B.sh;
@@ -955,7 +1016,7 @@ __global__ void __launch_bounds__(128) k_sweep(BatchView v, uint32_t* __restrict
                     rec.bucket_seg = B.seg;
                     rec.bucket_b = B.bb;
                     if (b2 >= 0) {
-                        const BucketJob& C2 = v.jobs[b2];
+                        const BucketJob& C2 = v.jobs[L[b2].job];
                         rec.has_second = 1;
                         rec.intersection2 = C2.inter;
                         rec.score2 = C2.score;
@@ -969,7 +1030,7 @@ __global__ void __launch_bounds__(128) k_sweep(BatchView v, uint32_t* __restrict
             }
             v.out[q] = rec;
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -1031,6 +1092,7 @@ struct MapScratch {
     DevBuf<BSlot> bt;
     DevBuf<BucketJob> jobs;
     DevBuf<BatchMax> mx;
+    DevBuf<SweepCand> sweep_scr;
     DevBuf<uint8_t> seed_gscr;
     DevBuf<shm_map_record> out;
     SketchLuts* luts = nullptr;
@@ -1245,29 +1307,36 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     launch_sketch(SK_APPEND, a, S.luts, s);
     T.end();
 
-    // K2 per size bin
-    auto seed_bin = [&](const std::vector<int32_t>& L, uint32_t P, bool global) {
-        if (L.empty()) return;
-        S.lists.reserve(L.size());
-        SHM_CUDA(cudaMemcpyAsync(S.lists.p, L.data(), sizeof(int32_t) * L.size(), cudaMemcpyHostToDevice, s));
+    // K2 per size bin: the three read lists go up in one copy
+    std::vector<int32_t> lists;
+    lists.reserve((size_t)n);
+    lists.insert(lists.end(), bp.list_s.begin(), bp.list_s.end());
+    lists.insert(lists.end(), bp.list_m.begin(), bp.list_m.end());
+    lists.insert(lists.end(), bp.list_g.begin(), bp.list_g.end());
+    S.lists.reserve(lists.size() + 1);
+    SHM_CUDA(cudaMemcpyAsync(S.lists.p, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice, s));
+    auto seed_bin = [&](size_t at, size_t len, uint32_t P, bool global) {
+        if (len == 0) return;
         const size_t bytes = SEED_BYTES_PER_ELEM * P;
         T.begin(STG_SEEDPREP);
         if (!global) {
-            int grid = grid_for(L.size() * 256, 256, 8);
-            SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-            k_seedprep<false><<<grid, 256, bytes, s>>>(v, S.lists.p, (int32_t)L.size(), P, nullptr, 0);
+            int grid = grid_for(len * 256, 256, 8);
+            if ((int)bytes > c->seed_smem_set) {
+                SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+                c->seed_smem_set = (int)bytes;
+            }
+            k_seedprep<false><<<grid, 256, bytes, s>>>(v, S.lists.p + at, (int32_t)len, P, nullptr, 0);
         } else {
-            int grid = (int)std::min<size_t>(L.size(), 296);
+            int grid = (int)std::min<size_t>(len, 296);
             S.seed_gscr.reserve(bytes * (size_t)grid);
-            k_seedprep<true><<<grid, 256, 0, s>>>(v, S.lists.p, (int32_t)L.size(), P, S.seed_gscr.p, bytes);
+            k_seedprep<true><<<grid, 256, 0, s>>>(v, S.lists.p + at, (int32_t)len, P, S.seed_gscr.p, bytes);
         }
         SHM_CUDA(cudaGetLastError());
         T.end();
-        SHM_CUDA(cudaStreamSynchronize(s));  // the list buffer is reused by the next bin
     };
-    seed_bin(bp.list_s, P_SMALL, false);
-    seed_bin(bp.list_m, P_MED, false);
-    seed_bin(bp.list_g, bp.P_g, true);
+    seed_bin(0, bp.list_s.size(), P_SMALL, false);
+    seed_bin(bp.list_s.size(), bp.list_m.size(), P_MED, false);
+    seed_bin(bp.list_s.size() + bp.list_m.size(), bp.list_g.size(), bp.P_g, true);
 
     exclusive_scan_u64(S.hw.p, S.hw_off.p, (size_t)n, s);
     exclusive_scan_u64(S.bt_size.p, S.bt_off.p, (size_t)n, s);
@@ -1342,7 +1411,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     }
     exclusive_scan_u32(S.ccnt.p, S.coff.p, (size_t)n, s);
     S.cidx.reserve(job_cap + 1);
-    S.sort_scr.reserve(job_cap + 1);
+    S.sweep_scr.reserve(2 * (size_t)job_cap + 2);
     v.cidx = S.cidx.p;
     T.begin(STG_AUX);
     k_cidx<<<grid_for(job_cap, 256, 8), 256, 0, s>>>(v);
@@ -1363,7 +1432,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     SHM_CUDA(cudaGetLastError());
     T.end();
     T.begin(STG_SWEEP);
-    k_sweep<<<grid_for((size_t)n * 128, 128, 16), 128, 0, s>>>(v, S.sort_scr.p);
+    k_sweep<<<grid_for((size_t)n * 32, SWEEP_WARPS * 32, 16), SWEEP_WARPS * 32, 0, s>>>(v, S.sweep_scr.p);
     SHM_CUDA(cudaGetLastError());
     T.end();
 
@@ -1413,47 +1482,73 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     return ovf;
 }
 
-static const int64_t BATCH_BASES = (int64_t)256 << 20;
-static const int32_t BATCH_READS = 32768;
+static const int64_t BATCH_BASES = (int64_t)1 << 30;
+static const int32_t BATCH_READS = 65536;
+
+__global__ void k_scatter_records(const shm_map_record* __restrict__ src, const int32_t* __restrict__ idx, int32_t n,
+                                  shm_map_record* __restrict__ dst) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[idx[i]] = src[i];
+}
+
+// Reads that beat a capacity estimate are mapped again, together, with exact
+// bounds. `bytes_of(i)` returns the host or device address of read i; the
+// reads are gathered into one staging buffer first.
+template <class CopyFn>
+static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params& p, const std::vector<int32_t>& ovf,
+                            const int64_t* offs, CopyFn copy_read, shm_map_record* d_out) {
+    if (ovf.empty()) return;
+    cudaStream_t s = c->stream;
+    MapScratch& S = *c->scr;
+    std::vector<int64_t> o(ovf.size() + 1, 0);
+    for (size_t i = 0; i < ovf.size(); i++) o[i + 1] = o[i] + (offs[ovf[i] + 1] - offs[ovf[i]]);
+    DevBuf<uint8_t> stage;
+    stage.reserve((size_t)o.back() + 32);
+    SHM_CUDA(cudaMemsetAsync(stage.p + o.back(), 0, 32, s));
+    for (size_t i = 0; i < ovf.size(); i++) copy_read(stage.p + o[i], ovf[i]);
+    DevBuf<shm_map_record> tmp;
+    tmp.reserve(ovf.size());
+    std::vector<int32_t> again = run_batch(c, ix, p, stage.p, o.data(), (int32_t)ovf.size(), tmp.p, true);
+    if (!again.empty()) {
+        std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n", ovf[again[0]]);
+        throw shm_cuda_error(cudaErrorMemoryAllocation);
+    }
+    DevBuf<int32_t> di;
+    di.reserve(ovf.size());
+    SHM_CUDA(cudaMemcpyAsync(di.p, ovf.data(), sizeof(int32_t) * ovf.size(), cudaMemcpyHostToDevice, s));
+    k_scatter_records<<<grid_for(ovf.size(), 256), 256, 0, s>>>(tmp.p, di.p, (int32_t)ovf.size(), d_out);
+    SHM_CUDA(cudaGetLastError());
+    count_launch();
+    SHM_CUDA(cudaStreamSynchronize(s));
+}
 
 void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
                 int32_t n, shm_map_record* d_out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
+    MapScratch& S = *c->scr;
+    std::vector<int32_t> ovf_all;
     int32_t i = 0;
     while (i < n) {
         int32_t j = i + 1;
         if (!plain)
             while (j < n && j - i < BATCH_READS && h_offs[j + 1] - h_offs[i] <= BATCH_BASES) j++;
         const uint8_t* dseq = d_seq + (h_offs[i] - h_offs[0]);
-        // the batch's first read must start on a 16-byte boundary for the vector loads
         std::vector<int32_t> ovf;
         if (((uintptr_t)dseq & 15) == 0) {
             ovf = run_batch(c, ix, p, dseq, h_offs + i, j - i, d_out + i, false);
-        } else {
-            MapScratch& S = *c->scr;
+        } else {  // the batch's first read must start on a 16-byte boundary for the vector loads
             const int64_t nb = h_offs[j] - h_offs[i];
             S.seq.reserve((size_t)nb + 32);
             SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
             SHM_CUDA(cudaMemcpyAsync(S.seq.p, dseq, (size_t)nb, cudaMemcpyDeviceToDevice, c->stream));
             ovf = run_batch(c, ix, p, S.seq.p, h_offs + i, j - i, d_out + i, false);
         }
-        // reads that beat a capacity estimate: once more, with exact bounds, one at a time
-        for (int32_t r : ovf) {
-            const int32_t g = i + r;
-            MapScratch& S = *c->scr;
-            const int64_t nb = h_offs[g + 1] - h_offs[g];
-            S.seq.reserve((size_t)nb + 32);
-            SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
-            SHM_CUDA(cudaMemcpyAsync(S.seq.p, d_seq + (h_offs[g] - h_offs[0]), (size_t)nb, cudaMemcpyDeviceToDevice,
-                                     c->stream));
-            std::vector<int32_t> again = run_batch(c, ix, p, S.seq.p, h_offs + g, 1, d_out + g, true);
-            if (!again.empty()) {
-                std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n", g);
-                throw shm_cuda_error(cudaErrorMemoryAllocation);
-            }
-        }
+        for (int32_t r : ovf) ovf_all.push_back(i + r);
         i = j;
     }
+    retry_overflows(c, ix, p, ovf_all, h_offs, [&](uint8_t* dst, int32_t g) {
+        SHM_CUDA(cudaMemcpyAsync(dst, d_seq + (h_offs[g] - h_offs[0]), (size_t)(h_offs[g + 1] - h_offs[g]),
+                                 cudaMemcpyDeviceToDevice, c->stream));
+    }, d_out);
     SHM_CUDA(cudaStreamSynchronize(c->stream));
 }
 
@@ -1461,6 +1556,7 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
               int32_t n, shm_map_record* out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
     MapScratch& S = *c->scr;
+    std::vector<int32_t> ovf_all;
     int32_t i = 0;
     while (i < n) {
         int32_t j = i + 1;
@@ -1471,28 +1567,24 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         S.out.reserve((size_t)(j - i));
         SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
         SHM_CUDA(cudaMemcpyAsync(S.seq.p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, c->stream));
-        std::vector<int64_t> ho(offs + i, offs + j + 1);
-        std::vector<int32_t> ovf = run_batch(c, ix, p, S.seq.p, ho.data(), j - i, S.out.p, false);
+        std::vector<int32_t> ovf = run_batch(c, ix, p, S.seq.p, offs + i, j - i, S.out.p, false);
         SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  c->stream));
         SHM_CUDA(cudaStreamSynchronize(c->stream));
-        for (int32_t r : ovf) {
-            const int32_t g = i + r;
-            const int64_t lb = offs[g + 1] - offs[g];
-            DevBuf<uint8_t> one;
-            one.reserve((size_t)lb + 32);
-            SHM_CUDA(cudaMemsetAsync(one.p + lb, 0, 32, c->stream));
-            SHM_CUDA(cudaMemcpyAsync(one.p, seqs + offs[g], (size_t)lb, cudaMemcpyHostToDevice, c->stream));
-            int64_t o2[2] = {offs[g], offs[g + 1]};
-            std::vector<int32_t> again = run_batch(c, ix, p, one.p, o2, 1, S.out.p, true);
-            if (!again.empty()) {
-                std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n", g);
-                throw shm_cuda_error(cudaErrorMemoryAllocation);
-            }
-            SHM_CUDA(cudaMemcpyAsync(out + g, S.out.p, sizeof(shm_map_record), cudaMemcpyDeviceToHost, c->stream));
-            SHM_CUDA(cudaStreamSynchronize(c->stream));
-        }
+        for (int32_t r : ovf) ovf_all.push_back(i + r);
         i = j;
+    }
+    if (!ovf_all.empty()) {
+        DevBuf<shm_map_record> all;
+        all.reserve((size_t)n);
+        // only the retried slots are read back: write them through a device copy of their records
+        retry_overflows(c, ix, p, ovf_all, offs, [&](uint8_t* dst, int32_t g) {
+            SHM_CUDA(cudaMemcpyAsync(dst, seqs + offs[g], (size_t)(offs[g + 1] - offs[g]), cudaMemcpyHostToDevice,
+                                     c->stream));
+        }, all.p);
+        for (int32_t g : ovf_all)
+            SHM_CUDA(cudaMemcpyAsync(out + g, all.p + g, sizeof(shm_map_record), cudaMemcpyDeviceToHost, c->stream));
+        SHM_CUDA(cudaStreamSynchronize(c->stream));
     }
 }
 
