@@ -287,7 +287,10 @@ def run_ours(args, rank, world, local):
         alg, alg_desc = algorithmic_bytes(top, work)
         alg_per_launch = alg / max(1, top_calls)
         achieved = alg_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
-        tr = traffic.get(args.workload, {}).get(top)
+        tr = None
+        tinfo = traffic.get(args.workload, {}).get(top)
+        if tinfo and tinfo.get("unit") in work:
+            tr = round(tinfo["bytes_per_unit"] * work[tinfo["unit"]] / max(1, top_calls))
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": tr, "kernel": top,
                 "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
