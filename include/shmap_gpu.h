@@ -170,6 +170,24 @@ const char* shm_stage_name(int i);
 int shm_ctx_work_stats(const shm_ctx* ctx, int64_t* out, int n);
 const char* shm_work_stat_name(int i);
 
+/* No counterpart in the reference. The sketch of shm_sketch, for one sequence
+ * already in device memory, for callers that must not allocate device memory
+ * here: a host whose device memory is fully reserved by its own pool
+ * allocator, or a latency-critical loop that cannot pay for cudaMalloc /
+ * cudaFree (which may synchronize the device). It allocates nothing: the
+ * caller passes d_seq (16-byte aligned, 16 readable bytes past the end) and
+ * the outputs d_h[cap] (hashes) and d_rs[cap] (r << 1 | strand), in sequence
+ * order; *n_out gets the count (SHM_ERR_CAPACITY if it exceeds cap). Its
+ * temporaries live in a static device array of about 0.5 MiB that every GPU
+ * loading the library holds until exit, shared by all calls: calls that
+ * overlap on the GPU race and must be serialized by the caller. Inputs longer
+ * than 4,194,304 windows (4,194,304 + k - 1 bases) are rejected with
+ * SHM_ERR_INVALID. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture. stream = NULL runs on the default stream. */
+int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, double h_frac, int32_t offset,
+                              uint64_t* d_h, uint32_t* d_rs, int64_t cap, int64_t* n_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,6 +25,10 @@ static int fail(int code, const std::string& msg) {
     return code;
 }
 
+namespace shm {
+void set_last_error(const std::string& m) { g_err = m; }
+}  // namespace shm
+
 #define SHM_GUARD_BEGIN try {
 #define SHM_GUARD_END                                                                                   \
     }                                                                                                   \

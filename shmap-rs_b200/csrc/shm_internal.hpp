@@ -14,6 +14,9 @@ namespace shm {
 
 uint64_t h_thres(double h_frac);  // src/sketch.rs:126-132
 
+// Sets the message shm_last_error() returns on this thread.
+void set_last_error(const std::string& m);
+
 // A device buffer that only grows; released by the destructor.
 template <class T>
 struct DevBuf {

@@ -158,3 +158,37 @@ void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStrea
 }
 
 }  // namespace shm
+
+namespace shm {
+
+// The same five tables as build_luts, computed on the device (for callers
+// that may not copy from the host or allocate).
+__global__ void k_fill_luts(SketchLuts* L, int32_t k) {
+    const uint64_t v[4] = {0x3c8bfbb395c60474ULL, 0x3193c18562a02b4cULL, 0x20323ed082572324ULL,
+                           0x295549f54be24456ULL};
+    for (int c = threadIdx.x; c < 256; c += blockDim.x) {
+        int fi = -1;
+        switch (c) {
+            case 'A': case 'a': fi = 0; break;
+            case 'C': case 'c': fi = 1; break;
+            case 'G': case 'g': fi = 2; break;
+            case 'T': case 't': fi = 3; break;
+        }
+        uint64_t fw = fi >= 0 ? v[fi] : 0, rc = fi >= 0 ? v[3 - fi] : 0;
+        L->fw[c] = fw;
+        L->rc[c] = rc;
+        L->fw_k[c] = rotl64(fw, (uint32_t)k);
+        L->rc_r1[c] = rotr64(rc, 1);
+        L->rc_k1[c] = rotl64(rc, (uint32_t)(k - 1));
+    }
+}
+
+size_t sketch_luts_bytes() { return sizeof(SketchLuts); }
+
+void launch_fill_luts(SketchLuts* d, int32_t k, cudaStream_t s) {
+    k_fill_luts<<<1, 256, 0, s>>>(d, k);
+    SHM_CUDA(cudaGetLastError());
+    count_launch();
+}
+
+}  // namespace shm

@@ -40,4 +40,9 @@ struct SketchLuts;
 SketchLuts* create_device_luts(int32_t k, cudaStream_t s);
 void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* luts, cudaStream_t s);
 
+// Builds the tables on the device into caller-provided device memory of
+// sketch_luts_bytes() bytes (8-byte aligned); no host copy, no allocation.
+size_t sketch_luts_bytes();
+void launch_fill_luts(SketchLuts* d, int32_t k, cudaStream_t s);
+
 }  // namespace shm

@@ -100,6 +100,7 @@ def lib() -> ctypes.CDLL:
         "shm_stage_name": (ctypes.c_char_p, [ctypes.c_int]),
         "shm_ctx_work_stats": (ctypes.c_int, [P, P, ctypes.c_int]),
         "shm_work_stat_name": (ctypes.c_char_p, [ctypes.c_int]),
+        "shm_sketch_device_noalloc": (ctypes.c_int, [P, i64, i32, dbl, i32, P, P, i64, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
