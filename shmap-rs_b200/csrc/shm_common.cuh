@@ -26,7 +26,7 @@ struct shm_cuda_error {
 
 namespace shm {
 
-constexpr int SKETCH_WIN = 64;           // windows rolled by one thread
+constexpr int SKETCH_WIN = 128;          // windows rolled by one thread
 constexpr int MIN_HALFLEN = 5;           // src/buckets.rs:15
 constexpr uint64_t EMPTY_KEY = ~0ULL;    // empty slot of the per-read hash tables
 constexpr int SEED_SMEM_MAX = 4096;      // largest sketch sorted in shared memory
@@ -57,7 +57,7 @@ struct DevIndex {
     const uint32_t* hit_fw;   // n_hits+1: prefix count of forward-strand hits
     const uint32_t* dir;      // (1 << dir_bits) + 1: first key of each hash range
     int32_t dir_bits;
-    int32_t dir_lz;           // leading zero bits of thr (hashes never use them)
+    uint64_t dir_mul;         // range of h: __umul64hi(h, dir_mul), monotone, < 2^dir_bits for h <= thr
     uint32_t n_keys, n_kmers, n_hits;
 };
 
@@ -103,7 +103,7 @@ __device__ __forceinline__ bool idx_lookup(const DevIndex& I, uint64_t h, uint32
     cnt = 0;
     a = 0;
     if (h > I.thr || I.n_keys == 0) return false;
-    uint32_t b = (uint32_t)((h << I.dir_lz) >> (64 - I.dir_bits));
+    uint32_t b = (uint32_t)__umul64hi(h, I.dir_mul);
     uint32_t lo = __ldg(I.dir + b), hi = __ldg(I.dir + b + 1);
     while (hi - lo > 8) {
         uint32_t mid = (lo + hi) >> 1;

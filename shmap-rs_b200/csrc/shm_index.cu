@@ -124,23 +124,18 @@ __global__ void k_fw_flags(const uint32_t* __restrict__ hits, size_t n, const ui
         f[i] = (ref_rs[hits[i]] & 1u) ? 0u : 1u;
 }
 
-__device__ __forceinline__ int64_t dir_bucket(uint64_t h, int lz, int bits) {
-    return (int64_t)((h << lz) >> (64 - bits));
-}
+__device__ __forceinline__ int64_t dir_bucket(uint64_t h, uint64_t mul) { return (int64_t)__umul64hi(h, mul); }
 
+// dir[b] = first key whose range is >= b; the ranges past the last key point at n_keys.
 __global__ void k_dir_fill(const uint64_t* __restrict__ keys, uint32_t n_keys, uint32_t* __restrict__ dir,
-                           int64_t nb, int lz, int bits) {
-    if (n_keys == 0) {
-        for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b <= nb; b += (int64_t)gridDim.x * blockDim.x)
-            dir[b] = 0;
-        return;
-    }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_keys; i += gridDim.x * blockDim.x) {
-        int64_t bi = dir_bucket(keys[i], lz, bits);
-        int64_t bp = i > 0 ? dir_bucket(keys[i - 1], lz, bits) : -1;
-        for (int64_t b = bp + 1; b <= bi; b++) dir[b] = i;
-        if (i == n_keys - 1)
-            for (int64_t b = bi + 1; b <= nb; b++) dir[b] = n_keys;
+                           int64_t nb, uint64_t mul) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nthreads = (int64_t)gridDim.x * blockDim.x;
+    const int64_t blast = n_keys ? dir_bucket(keys[n_keys - 1], mul) : -1;
+    for (int64_t b = blast + 1 + tid; b <= nb; b += nthreads) dir[b] = n_keys;
+    for (int64_t i = tid; i < (int64_t)n_keys; i += nthreads) {
+        int64_t bi = dir_bucket(keys[i], mul);
+        int64_t bp = i > 0 ? dir_bucket(keys[i - 1], mul) : -1;
+        for (int64_t b = bp + 1; b <= bi; b++) dir[b] = (uint32_t)i;
     }
 }
 
@@ -294,11 +289,13 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
         exclusive_scan_u32(flag.p, ix->hit_fw.p, n_hits, s);
         int bits = 1;
         while (bits < 30 && (1u << bits) < n_kept) bits++;
-        int lz = thr == 0 ? 63 : __builtin_clzll(thr);
         const int64_t nb = (int64_t)1 << bits;
+        // mul = floor(2^64 * nb / (thr + 1)): h <= thr maps monotonically onto [0, nb)
+        unsigned __int128 m128 = ((unsigned __int128)nb << 64) / ((unsigned __int128)thr + 1);
+        const uint64_t mul = m128 > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)m128;
         ix->dir.reserve((size_t)nb + 1);
-        k_dir_fill<<<grid_for(std::max<size_t>(n_kept, 1), 256), 256, 0, s>>>(ix->keys.p, n_kept, ix->dir.p, nb, lz,
-                                                                             bits);
+        k_dir_fill<<<grid_for((size_t)std::max<int64_t>(nb, (int64_t)n_kept), 256), 256, 0, s>>>(ix->keys.p, n_kept,
+                                                                                               ix->dir.p, nb, mul);
         SHM_CUDA(cudaGetLastError());
         SHM_CUDA(cudaStreamSynchronize(s));
 
@@ -316,7 +313,7 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
         d.hit_fw = ix->hit_fw.p;
         d.dir = ix->dir.p;
         d.dir_bits = bits;
-        d.dir_lz = lz;
+        d.dir_mul = mul;
         d.n_keys = n_kept;
         d.n_kmers = n_kmers;
         d.n_hits = n_hits;

@@ -80,6 +80,7 @@ struct BatchView {
     uint32_t* r_seeded;
     uint64_t *hw, *hw_off, *bt_size, *bt_off;
     BSlot* bt;
+    uint32_t* bt_list;  // per read, the slots of its distinct buckets (r_seeded[q] of them)
     BucketJob* jobs;
     uint32_t* n_jobs;
     uint32_t job_cap;
@@ -197,6 +198,19 @@ __device__ __forceinline__ void pht_insert(const BatchView& v, int32_t q, uint64
         }
         i = (i + 1) & mask;
     }
+}
+
+// Upper bound on the buckets one processed seed contributes to (and so on its
+// emissions in k_contrib): a single hit touches 2; a list spanning gidx range
+// [first, last] over n segments touches at most (last-first)/h + 3 per
+// segment spanned, and never more than 2 per hit. Sizes the bucket tables.
+__device__ __forceinline__ uint64_t seed_bucket_bound(const BatchView& v, uint32_t a, uint32_t cnt, int64_t h) {
+    if (cnt == 0) return 0;
+    if (cnt == 1 || v.P.ap) return 2ULL * cnt;
+    const uint32_t g0 = __ldg(v.I.hits + a), g1 = __ldg(v.I.hits + a + cnt - 1);
+    const int32_t s0 = seg_of(v.I, g0), s1 = seg_of(v.I, g1);
+    const uint64_t span = (uint64_t)(g1 - g0) / (uint64_t)h + 1 + 3ULL * (uint64_t)(s1 - s0 + 1);
+    return min((uint64_t)(2ULL * cnt), span);
 }
 
 // ------------------------------------------------------------------ K2 seedprep
@@ -326,7 +340,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
     uint32_t po = block_scan_excl<uint32_t>(so, sw32, &t32);
     uint64_t pc = block_scan_excl<uint64_t>(sc, sw64, &t64);
     uint32_t l_np = 0, l_s0 = 0, l_max = 0;
-    uint64_t l_sm = 0;
+    uint64_t l_sm = 0, l_eb = 0;
     for (uint32_t i = j0; i < j1; i++) {
         const uint64_t e = S_.E[i];
         const uint32_t g = (uint32_t)(e & 0xffffffffu), cnt = (uint32_t)(e >> 32);
@@ -342,6 +356,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
             l_s0 += occs;
             l_sm += cnt;
             l_max = max(l_max, cnt);
+            l_eb += seed_bucket_bound(v, S_.GD[g], cnt, halflen);
         }
         pht_insert(v, q, S_.GA[g], i);
         po += occs;
@@ -350,6 +365,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
     const uint32_t n_proc = block_reduce_sum<uint32_t>(l_np, sw32, &t32);
     const uint32_t S0 = block_reduce_sum<uint32_t>(l_s0, sw32, &t32);
     const uint64_t smatch = block_reduce_sum<uint64_t>(l_sm, sw64, &t64);
+    const uint64_t ebound = block_reduce_sum<uint64_t>(l_eb, sw64, &t64);
     const uint32_t mxs = block_reduce_max(l_max, sw32);
     if (tid == 0) {
         v.r_status[q] = ST_UNMAPPED;
@@ -364,7 +380,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
             v.r_status[q] = ST_OVERFLOW;
         } else {
             v.hw[q] = smatch;
-            v.bt_size[q] = smatch ? max((uint64_t)16, pow2_ceil(4 * smatch)) : 0;
+            v.bt_size[q] = smatch ? max((uint64_t)16, pow2_ceil(2 * ebound)) : 0;
         }
         atomicMax(&v.mx->m_max, m);
         atomicMax(&v.mx->nu_max, n_u);
@@ -385,6 +401,217 @@ __global__ void __launch_bounds__(256) k_seedprep(BatchView v, const int32_t* __
     for (int32_t li = blockIdx.x; li < n_list; li += gridDim.x) {
         seedprep_one(v, list[li], P, S_);
         __syncthreads();
+    }
+}
+
+// The same stage with one warp per read (reads whose k-mer capacity fits a
+// per-warp slice of P <= 1024 elements): no block barriers. Per warp:
+// A (u64) hashes, compacted in place into group hashes; E (u64) rarest-first
+// keys; B (u32) element keys, compacted into occs << 1 | strand; D (u32)
+// hit-list starts.
+constexpr size_t SEEDW_BYTES_PER_ELEM = 8 + 8 + 4 + 4;
+
+__device__ void warp_bitonic_ab(uint64_t* A, uint32_t* B, uint32_t P, int lane) {
+    for (uint32_t k = 2; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = lane; t < P / 2; t += 32) {
+                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                bool asc = (i & k) == 0;
+                uint64_t ai = A[i], al = A[l];
+                uint32_t bi = B[i], bl = B[l];
+                bool gt = ai > al || (ai == al && bi > bl);
+                if (gt == asc) {
+                    A[i] = al;
+                    A[l] = ai;
+                    B[i] = bl;
+                    B[l] = bi;
+                }
+            }
+            __syncwarp();
+        }
+}
+
+__device__ void warp_bitonic_u64(uint64_t* A, uint32_t P, int lane) {
+    for (uint32_t k = 2; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = lane; t < P / 2; t += 32) {
+                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                bool asc = (i & k) == 0;
+                uint64_t ai = A[i], al = A[l];
+                if ((ai > al) == asc) {
+                    A[i] = al;
+                    A[l] = ai;
+                }
+            }
+            __syncwarp();
+        }
+}
+
+__device__ void seedprep_warp(const BatchView& v, int32_t q, uint32_t P, uint64_t* A, uint64_t* E, uint32_t* B,
+                              uint32_t* D) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u, le = lt | (1u << lane);
+    const int64_t read_len = v.roff[q + 1] - v.roff[q];
+    const uint64_t kb = v.kcap_off[q];
+    const uint32_t cap = (uint32_t)(v.kcap_off[q + 1] - kb);
+    const uint32_t m = v.kcnt[q];
+    if (lane == 0) {
+        v.hw[q] = 0;
+        v.bt_size[q] = 0;
+        v.r_nproc[q] = 0;
+        v.r_nu[q] = 0;
+        v.r_S0[q] = 0;
+        v.r_smatch[q] = 0;
+        v.r_maxseed[q] = 0;
+        v.r_m[q] = (int32_t)m;
+        v.r_half[q] = 0;
+    }
+    if (m > cap || cap > P) {
+        if (lane == 0) v.r_status[q] = ST_OVERFLOW;
+        return;
+    }
+    int32_t S = __double2int_rz(__dmul_rn(__dsub_rn(1.0, v.theta2), (double)m)) + 1;
+    const int32_t halflen = v.P.ap ? (int32_t)read_len : (int32_t)m;
+    if (halflen < MIN_HALFLEN) {
+        if (lane == 0) {
+            v.r_status[q] = ST_SHORT_SKETCH;
+            v.r_S[q] = S;
+        }
+        return;
+    }
+    const uint32_t Pm = max((uint32_t)2, (uint32_t)pow2_ceil(m));
+    for (uint32_t i = lane; i < Pm; i += 32) {
+        if (i < m) {
+            A[i] = v.km_h[kb + i];
+            uint32_t rs = v.km_rs[kb + i];
+            B[i] = ((0x3fffffffu - (rs >> 1)) << 1) | (rs & 1u);
+        } else {
+            A[i] = ~0ULL;
+            B[i] = 0xffffffffu;
+        }
+    }
+    __syncwarp();
+    warp_bitonic_ab(A, B, Pm, lane);  // (h asc, r desc): src/shmap/seeding.rs:28-34
+
+    // groups of equal hashes, compacted in place (group g lands at index g <= its elements)
+    uint32_t n_u = 0, open_start = 0;
+    uint64_t carry_h = 0;
+    for (uint32_t c0 = 0; c0 < m; c0 += 32) {
+        const uint32_t i = c0 + lane;
+        const bool valid = i < m;
+        const uint64_t h = valid ? A[i] : 0;
+        const uint32_t b = valid ? B[i] : 0;
+        const uint64_t hn = (i + 1 < m) ? A[i + 1] : 0;
+        const uint64_t hp_lane = __shfl_up_sync(0xffffffffu, h, 1);
+        const uint64_t hp = lane == 0 ? carry_h : hp_lane;
+        const bool first = valid && (i == 0 || h != hp);
+        const bool last = valid && (i + 1 == m || hn != h);
+        const unsigned fmask = __ballot_sync(0xffffffffu, first);
+        const uint32_t gid = n_u + __popc(fmask & le) - 1;
+        const unsigned fle = fmask & le;
+        const uint32_t start = fle ? c0 + (31 - __clz(fle)) : open_start;
+        __syncwarp();
+        if (first) A[gid] = h;
+        if (last) B[gid] = ((i - start + 1) << 1) | (b & 1u);  // representative: smallest r (seeding.rs:56)
+        n_u += __popc(fmask);
+        open_start = __shfl_sync(0xffffffffu, start, 31);
+        carry_h = __shfl_sync(0xffffffffu, h, 31);
+        __syncwarp();
+    }
+    if (v.P.os) S = (int32_t)n_u;  // mod.rs:732-736
+    // count() probes (index.rs:204-213); rarest first, stable over hash order (seeding.rs:71)
+    const uint32_t Pu = max((uint32_t)2, (uint32_t)pow2_ceil(n_u));
+    for (uint32_t g = lane; g < Pu; g += 32) {
+        if (g < n_u) {
+            uint32_t a, cnt;
+            idx_lookup(v.I, A[g], a, cnt);
+            D[g] = a;
+            E[g] = ((uint64_t)cnt << 32) | g;
+        } else {
+            E[g] = ~0ULL;
+        }
+    }
+    __syncwarp();
+    warp_bitonic_u64(E, Pu, lane);
+
+    // seeding prefix: seed i is processed iff sum(occs before i) < S (seeding.rs:101)
+    uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
+    uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
+    for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
+        const uint32_t i = c0 + lane;
+        const bool valid = i < n_u;
+        const uint64_t e = valid ? E[i] : 0;
+        const uint32_t g = (uint32_t)(e & 0xffffffffu), cnt = (uint32_t)(e >> 32);
+        const uint32_t os = valid ? B[g] : 0, occs = os >> 1;
+        const uint32_t oi = warp_inclusive_scan(occs);
+        const uint64_t ci = warp_inclusive_scan((uint64_t)(valid ? cnt : 0));
+        const uint32_t po = po_carry + oi - occs;
+        const uint64_t pc = pc_carry + ci - (valid ? cnt : 0);
+        if (valid) {
+            const uint64_t hg = A[g];
+            v.sd_h[kb + i] = hg;
+            v.sd_os[kb + i] = os;
+            v.sd_cnt[kb + i] = cnt;
+            v.sd_a[kb + i] = D[g];
+            v.sd_ooff[kb + i] = po;
+            if ((int64_t)po < (int64_t)S) {
+                v.sd_hpre[kb + i] = (uint32_t)pc;
+                l_np++;
+                l_s0 += occs;
+                l_sm += cnt;
+                l_max = max(l_max, cnt);
+                l_eb += seed_bucket_bound(v, D[g], cnt, halflen);
+            }
+            pht_insert(v, q, hg, i);
+        }
+        po_carry += __shfl_sync(0xffffffffu, oi, 31);
+        pc_carry += __shfl_sync(0xffffffffu, ci, 31);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l_np += __shfl_xor_sync(0xffffffffu, l_np, o);
+        l_s0 += __shfl_xor_sync(0xffffffffu, l_s0, o);
+        l_sm += __shfl_xor_sync(0xffffffffu, l_sm, o);
+        l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
+        l_max = max(l_max, __shfl_xor_sync(0xffffffffu, l_max, o));
+    }
+    if (lane == 0) {
+        v.r_status[q] = ST_UNMAPPED;
+        v.r_nu[q] = (int32_t)n_u;
+        v.r_nproc[q] = (int32_t)l_np;
+        v.r_S[q] = S;
+        v.r_S0[q] = (int32_t)l_s0;
+        v.r_smatch[q] = (int64_t)l_sm;
+        v.r_maxseed[q] = (int32_t)l_max;
+        v.r_half[q] = halflen;
+        if (l_sm >= 0xffffffffULL) {
+            v.r_status[q] = ST_OVERFLOW;
+        } else {
+            v.hw[q] = l_sm;
+            v.bt_size[q] = l_sm ? max((uint64_t)16, pow2_ceil(2 * l_eb)) : 0;
+        }
+        atomicMax(&v.mx->m_max, m);
+        atomicMax(&v.mx->nu_max, n_u);
+        atomicMax(&v.mx->half_max, (uint32_t)halflen);
+        atomicAdd(&v.mx->kmers, (unsigned long long)m);
+        atomicAdd(&v.mx->distinct, (unsigned long long)n_u);
+        atomicAdd(&v.mx->proc_seeds, (unsigned long long)l_np);
+        atomicAdd(&v.mx->hits, (unsigned long long)l_sm);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_seedprep_w(BatchView v, const int32_t* __restrict__ list, int32_t n_list,
+                                                    uint32_t P) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    uint8_t* base = smem + (size_t)wib * SEEDW_BYTES_PER_ELEM * P;
+    uint64_t* A = (uint64_t*)base;
+    uint64_t* E = A + P;
+    uint32_t* B = (uint32_t*)(E + P);
+    uint32_t* D = B + P;
+    for (int32_t li = blockIdx.x * wpb + wib; li < n_list; li += gridDim.x * wpb) {
+        seedprep_warp(v, list[li], P, A, E, B, D);
+        __syncwarp();
     }
 }
 
@@ -457,7 +684,11 @@ __device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t se
     for (;;) {
         s = v.bt + base + i;
         unsigned long long prev = atomicCAS(&s->key, EMPTY_KEY, key);
-        if (prev == EMPTY_KEY || prev == key) break;
+        if (prev == EMPTY_KEY) {  // a new bucket: list it for k_bscan (seeded_buckets, mod.rs:794)
+            v.bt_list[base + atomicAdd(v.r_seeded + q, 1u)] = (uint32_t)i;
+            break;
+        }
+        if (prev == key) break;
         i = (i + 1) & mask;
     }
     atomicAdd(&s->matches, matches);
@@ -553,39 +784,41 @@ __global__ void k_bt_init(BSlot* bt, uint64_t n) {
 
 // ------------------------------------------------------------------ K4 distinct buckets
 __global__ void __launch_bounds__(256) k_bscan(BatchView v) {
-    const uint64_t total = v.bt_off[v.n];
-    for (uint64_t si = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; si < total;
-         si += (uint64_t)gridDim.x * blockDim.x) {
-        const BSlot s = v.bt[si];
-        if (s.key == EMPTY_KEY) continue;
-        const int32_t q = (int32_t)ub_u64(v.bt_off, (uint32_t)v.n + 1, si) - 1;
-        atomicAdd(v.r_seeded + q, 1u);  // seeded_buckets (mod.rs:794)
-        atomicAdd(&v.mx->buckets, 1ULL);
-        BucketJob j;
-        j.read = q;
-        j.seg = (int32_t)(s.key >> 32);
-        j.bb = (int32_t)(s.key & 0xffffffffu);
-        j.m0 = s.matches;
-        j.matches = s.matches;
-        j.codir = s.codir;
-        j.rmin = s.rmin;
-        j.rmax = s.rmax;
-        j.pad0 = j.pad1 = 0;
-        j.score = -1.0;
-        j.t_l = j.t_r = j.inter = j.same = j.s_sz = -1;
-        if (v.P.nbp) {
-            j.sh = 1.0;  // seed_heuristic_pass does nothing under NBP (pruning.rs:351)
-            j.is_cand = 1;
-        } else {
-            const double sh0 = hseed(v.r_m[q], v.r_S0[q], s.matches);
-            if (sh0 < v.P.theta_low) continue;
-            j.sh = sh0;
-            j.is_cand = 0;
-        }
-        uint32_t ji = atomicAdd(v.n_jobs, 1u);
-        if (ji < v.job_cap) {
-            v.jobs[ji] = j;
-            if (j.is_cand) atomicAdd(v.ccnt + q, 1u);
+    const int lane = threadIdx.x & 31;
+    const int32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int32_t q = wid; q < v.n; q += nwarps) {
+        const uint32_t nb = v.r_seeded[q];
+        if (nb == 0) continue;
+        const uint64_t base = v.bt_off[q];
+        if (lane == 0) atomicAdd(&v.mx->buckets, (unsigned long long)nb);
+        for (uint32_t j = lane; j < nb; j += 32) {
+            const BSlot s = v.bt[base + v.bt_list[base + j]];
+            BucketJob jb;
+            jb.read = q;
+            jb.seg = (int32_t)(s.key >> 32);
+            jb.bb = (int32_t)(s.key & 0xffffffffu);
+            jb.m0 = s.matches;
+            jb.matches = s.matches;
+            jb.codir = s.codir;
+            jb.rmin = s.rmin;
+            jb.rmax = s.rmax;
+            jb.pad0 = jb.pad1 = 0;
+            jb.score = -1.0;
+            jb.t_l = jb.t_r = jb.inter = jb.same = jb.s_sz = -1;
+            if (v.P.nbp) {
+                jb.sh = 1.0;  // seed_heuristic_pass does nothing under NBP (pruning.rs:351)
+                jb.is_cand = 1;
+            } else {
+                const double sh0 = hseed(v.r_m[q], v.r_S0[q], s.matches);
+                if (sh0 < v.P.theta_low) continue;
+                jb.sh = sh0;
+                jb.is_cand = 0;
+            }
+            uint32_t ji = atomicAdd(v.n_jobs, 1u);
+            if (ji < v.job_cap) {
+                v.jobs[ji] = jb;
+                if (jb.is_cand) atomicAdd(v.ccnt + q, 1u);
+            }
         }
     }
 }
@@ -1090,6 +1323,7 @@ struct MapScratch {
     DevBuf<int32_t> r_i32, lists, ref_scr;
     DevBuf<int64_t> r_smatch;
     DevBuf<BSlot> bt;
+    DevBuf<uint32_t> bt_list;
     DevBuf<BucketJob> jobs;
     DevBuf<BatchMax> mx;
     DevBuf<SweepCand> sweep_scr;
@@ -1139,23 +1373,25 @@ static uint64_t kmer_cap(int64_t nw, double h_frac, bool exact) {
     return std::min<uint64_t>(c, (uint64_t)nw);
 }
 
+// Seed-preparation bins by the power of two P >= a read's k-mer capacity:
+// warp-per-read slices for P <= 1024, a CTA per read for P <= 4096, a CTA with
+// global scratch beyond.
+constexpr int N_SEED_BINS = 5;
+static const uint32_t SEED_BIN_P[N_SEED_BINS - 1] = {256, 512, 1024, 4096};
+
 struct BatchPlan {
     std::vector<int64_t> roff;
     std::vector<uint64_t> chunk_off, kcap_off, pht_off;
-    std::vector<int32_t> list_s, list_m, list_g;
-    uint32_t P_s = 512, P_m = 2048, P_g = 0;
+    std::vector<int32_t> bins[N_SEED_BINS];
+    uint32_t P_g = 0;
 };
-
-static const uint32_t P_SMALL = 512, P_MED = 2048;
 
 static void plan_batch(const int64_t* h_offs, int32_t n, int32_t k, double h_frac, bool exact, BatchPlan& bp) {
     bp.roff.assign((size_t)n + 1, 0);
     bp.chunk_off.assign((size_t)n + 1, 0);
     bp.kcap_off.assign((size_t)n + 1, 0);
     bp.pht_off.assign((size_t)n + 1, 0);
-    bp.list_s.clear();
-    bp.list_m.clear();
-    bp.list_g.clear();
+    for (auto& b : bp.bins) b.clear();
     bp.P_g = 0;
     for (int32_t i = 0; i < n; i++) {
         int64_t L = h_offs[i + 1] - h_offs[i];
@@ -1166,12 +1402,10 @@ static void plan_batch(const int64_t* h_offs, int32_t n, int32_t k, double h_fra
         bp.kcap_off[(size_t)i + 1] = bp.kcap_off[(size_t)i] + cap;
         bp.pht_off[(size_t)i + 1] = bp.pht_off[(size_t)i] + std::max<uint64_t>(16, pow2_host(2 * cap));
         uint64_t P = pow2_host(std::max<uint64_t>(cap, 1));
-        if (P <= P_SMALL) bp.list_s.push_back(i);
-        else if (P <= P_MED) bp.list_m.push_back(i);
-        else {
-            bp.list_g.push_back(i);
-            bp.P_g = std::max<uint32_t>(bp.P_g, (uint32_t)P);
-        }
+        int b = 0;
+        while (b < N_SEED_BINS - 1 && P > SEED_BIN_P[b]) b++;
+        bp.bins[b].push_back(i);
+        if (b == N_SEED_BINS - 1) bp.P_g = std::max<uint32_t>(bp.P_g, (uint32_t)P);
     }
 }
 
@@ -1307,36 +1541,48 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     launch_sketch(SK_APPEND, a, S.luts, s);
     T.end();
 
-    // K2 per size bin: the three read lists go up in one copy
+    // K2 per size bin: the bin lists go up in one copy
     std::vector<int32_t> lists;
     lists.reserve((size_t)n);
-    lists.insert(lists.end(), bp.list_s.begin(), bp.list_s.end());
-    lists.insert(lists.end(), bp.list_m.begin(), bp.list_m.end());
-    lists.insert(lists.end(), bp.list_g.begin(), bp.list_g.end());
+    size_t bin_at[N_SEED_BINS];
+    for (int bi = 0; bi < N_SEED_BINS; bi++) {
+        bin_at[bi] = lists.size();
+        lists.insert(lists.end(), bp.bins[bi].begin(), bp.bins[bi].end());
+    }
     S.lists.reserve(lists.size() + 1);
     SHM_CUDA(cudaMemcpyAsync(S.lists.p, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice, s));
-    auto seed_bin = [&](size_t at, size_t len, uint32_t P, bool global) {
-        if (len == 0) return;
-        const size_t bytes = SEED_BYTES_PER_ELEM * P;
+    for (int bi = 0; bi < N_SEED_BINS; bi++) {
+        const size_t len = bp.bins[bi].size();
+        if (len == 0) continue;
+        const int32_t* L = S.lists.p + bin_at[bi];
         T.begin(STG_SEEDPREP);
-        if (!global) {
-            int grid = grid_for(len * 256, 256, 8);
+        if (bi < 3) {  // warp per read
+            const uint32_t P = SEED_BIN_P[bi];
+            const int wpb = P <= 512 ? 8 : 4;
+            const size_t bytes = SEEDW_BYTES_PER_ELEM * P * (size_t)wpb;
+            if ((int)bytes > c->seedw_smem_set) {
+                SHM_CUDA(cudaFuncSetAttribute(k_seedprep_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+                c->seedw_smem_set = (int)bytes;
+            }
+            int grid = grid_for(len * 32, wpb * 32, 2048 / (wpb * 32));
+            k_seedprep_w<<<grid, wpb * 32, bytes, s>>>(v, L, (int32_t)len, P);
+        } else if (bi == 3) {  // CTA per read
+            const uint32_t P = SEED_BIN_P[bi];
+            const size_t bytes = SEED_BYTES_PER_ELEM * P;
             if ((int)bytes > c->seed_smem_set) {
                 SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
                 c->seed_smem_set = (int)bytes;
             }
-            k_seedprep<false><<<grid, 256, bytes, s>>>(v, S.lists.p + at, (int32_t)len, P, nullptr, 0);
-        } else {
+            k_seedprep<false><<<grid_for(len * 256, 256, 8), 256, bytes, s>>>(v, L, (int32_t)len, P, nullptr, 0);
+        } else {  // CTA per read, global scratch
+            const size_t bytes = SEED_BYTES_PER_ELEM * bp.P_g;
             int grid = (int)std::min<size_t>(len, 296);
             S.seed_gscr.reserve(bytes * (size_t)grid);
-            k_seedprep<true><<<grid, 256, 0, s>>>(v, S.lists.p + at, (int32_t)len, P, S.seed_gscr.p, bytes);
+            k_seedprep<true><<<grid, 256, 0, s>>>(v, L, (int32_t)len, bp.P_g, S.seed_gscr.p, bytes);
         }
         SHM_CUDA(cudaGetLastError());
         T.end();
-    };
-    seed_bin(0, bp.list_s.size(), P_SMALL, false);
-    seed_bin(bp.list_s.size(), bp.list_m.size(), P_MED, false);
-    seed_bin(bp.list_s.size() + bp.list_m.size(), bp.list_g.size(), bp.P_g, true);
+    }
 
     exclusive_scan_u64(S.hw.p, S.hw_off.p, (size_t)n, s);
     exclusive_scan_u64(S.bt_size.p, S.bt_off.p, (size_t)n, s);
@@ -1370,7 +1616,9 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     }
 
     S.bt.reserve(bt_total + 1);
+    S.bt_list.reserve(bt_total + 1);
     v.bt = S.bt.p;
+    v.bt_list = S.bt_list.p;
     if (bt_total) {
         T.begin(STG_AUX);
         k_bt_init<<<grid_for(bt_total, 256), 256, 0, s>>>(S.bt.p, bt_total);
@@ -1390,7 +1638,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
         v.job_cap = job_cap;
         if (bt_total) {
             T.begin(STG_BSCAN);
-            k_bscan<<<grid_for(bt_total, 256, 8), 256, 0, s>>>(v);
+            k_bscan<<<grid_for((size_t)n * 32, 256, 8), 256, 0, s>>>(v);
             SHM_CUDA(cudaGetLastError());
             T.end();
         }
@@ -1401,7 +1649,6 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
         job_cap = nj;  // retry with room for every job
         SHM_CUDA(cudaMemsetAsync(S.n_jobs.p, 0, sizeof(uint32_t), s));
         SHM_CUDA(cudaMemsetAsync(S.ccnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
-        SHM_CUDA(cudaMemsetAsync(S.r_seeded.p, 0, sizeof(uint32_t) * (size_t)n, s));
     }
     if (!p.no_bucket_pruning) {
         T.begin(STG_EXTEND);
@@ -1498,7 +1745,6 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
                             const int64_t* offs, CopyFn copy_read, shm_map_record* d_out) {
     if (ovf.empty()) return;
     cudaStream_t s = c->stream;
-    MapScratch& S = *c->scr;
     std::vector<int64_t> o(ovf.size() + 1, 0);
     for (size_t i = 0; i < ovf.size(); i++) o[i + 1] = o[i] + (offs[ovf[i] + 1] - offs[ovf[i]]);
     DevBuf<uint8_t> stage;

@@ -51,7 +51,8 @@ struct MapCtx {
     size_t h_pinned_cap = 0;
     // work counters (always on): see WORK_NAMES
     int64_t work[16] = {};
-    int seed_smem_set = 0;  // dynamic shared memory the seed kernel has been allowed so far
+    int seed_smem_set = 0;   // dynamic shared memory the seed kernels have been allowed so far
+    int seedw_smem_set = 0;
     // stage timing
     bool timing = false;
     double stage_ms[N_STAGES] = {};

@@ -28,7 +28,8 @@ namespace {
 
 // Largest input: NOALLOC_MAX_CHUNKS runs of SKETCH_WIN windows.
 constexpr int64_t NOALLOC_MAX_CHUNKS = 1 << 16;
-constexpr int64_t NOALLOC_MAX_WINDOWS = NOALLOC_MAX_CHUNKS * shm::SKETCH_WIN;  // 4,194,304
+constexpr int64_t NOALLOC_MAX_WINDOWS = 4194304;
+static_assert(NOALLOC_MAX_WINDOWS <= NOALLOC_MAX_CHUNKS * shm::SKETCH_WIN, "scratch holds every run of the limit");
 constexpr size_t NOALLOC_LUT_BYTES = 5 * 256 * 8;                              // the five lookup tables
 constexpr size_t NOALLOC_OFF_BYTES = 64;                                       // seq_off[2], chunk_off[2]
 constexpr size_t NOALLOC_SCRATCH_BYTES =

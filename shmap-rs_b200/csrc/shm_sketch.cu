@@ -37,29 +37,34 @@ void build_luts(int32_t k, SketchLuts* L) {
     }
 }
 
-// Sequential byte reader over global memory with 16-byte aligned loads.
-struct ByteStream {
-    const uint8_t* base;
-    uint64_t next;  // absolute byte index of the next byte to return
-    uint4 buf;
-    uint64_t buf_at;  // absolute index of buf's first byte
-    __device__ __forceinline__ void init(const uint8_t* b, uint64_t at) {
-        base = b;
-        next = at;
-        buf_at = ~0ULL;
-    }
-    __device__ __forceinline__ uint32_t get() {
-        uint64_t blk = next & ~15ULL;
-        if (blk != buf_at) {
-            buf = __ldg(reinterpret_cast<const uint4*>(base + blk));
-            buf_at = blk;
+// Fixed 64-bit rotates by one (two funnel shifts each).
+__device__ __forceinline__ uint64_t rotl1(uint64_t x) {
+    uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+    return ((uint64_t)__funnelshift_l(lo, hi, 1) << 32) | __funnelshift_l(hi, lo, 1);
+}
+__device__ __forceinline__ uint64_t rotr1(uint64_t x) {
+    uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+    return ((uint64_t)__funnelshift_r(hi, lo, 1) << 32) | __funnelshift_r(lo, hi, 1);
+}
+
+// One selected window: record it by the kernel's mode.
+template <int MODE>
+__device__ __forceinline__ void emit_kmer(const SketchArgs& a, int32_t q, uint64_t h, uint32_t rs, uint64_t out_base,
+                                          uint32_t out_cap, uint32_t& n_sel) {
+    if (MODE == SK_COUNT) {
+        n_sel++;
+    } else if (MODE == SK_WRITE) {
+        a.out_h[out_base + n_sel] = h;
+        a.out_rs[out_base + n_sel] = rs;
+        n_sel++;
+    } else {
+        uint32_t slot = atomicAdd(a.kmer_cnt + q, 1u);
+        if (slot < out_cap) {
+            a.out_h[out_base + slot] = h;
+            a.out_rs[out_base + slot] = rs;
         }
-        uint32_t o = (uint32_t)(next & 15);
-        uint32_t w = o < 8 ? (o < 4 ? buf.x : buf.y) : (o < 12 ? buf.z : buf.w);
-        next++;
-        return (w >> ((o & 3) * 8)) & 0xff;
     }
-};
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_sketch(SketchArgs a, const SketchLuts* __restrict__ luts) {
@@ -88,8 +93,8 @@ __global__ void __launch_bounds__(256) k_sketch(SketchArgs a, const SketchLuts* 
         const int64_t s0 = __ldg(a.seq_off + q), L_ = __ldg(a.seq_off + q + 1) - s0;
         const int64_t nw = L_ - k + 1;
         const int64_t w0 = (int64_t)(c - __ldg(a.chunk_off + q)) * SKETCH_WIN;
-        const int64_t w1 = min(w0 + (int64_t)SKETCH_WIN, nw);
-        if (w0 >= w1) continue;
+        const int32_t cnt = (int32_t)(min(w0 + (int64_t)SKETCH_WIN, nw) - w0);  // windows of this run
+        if (cnt <= 0) continue;
         uint64_t out_base = 0;
         uint32_t out_cap = 0;
         uint32_t n_sel = 0;
@@ -98,40 +103,43 @@ __global__ void __launch_bounds__(256) k_sketch(SketchArgs a, const SketchLuts* 
             out_base = a.kmer_off[q];
             out_cap = (uint32_t)(a.kmer_off[q + 1] - out_base);
         }
-        // first window, by definition
-        ByteStream in;
-        in.init(a.seq, (uint64_t)(s0 + w0));
+        const uint8_t* p = a.seq + (s0 + w0);
+        const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;  // r of the run's first window
+        // first window, by definition (tests/nthash_equivalence.rs:31-61)
         uint64_t fw = 0, rc = 0;
         for (int i = 0; i < k; i++) {
-            uint32_t b = in.get();
+            uint32_t b = __ldg(p + i);
             fw ^= rotl64(L.fw[b], (uint32_t)(k - 1 - i));
             rc ^= rotl64(L.rc[b], (uint32_t)i);
         }
-        ByteStream out;
-        out.init(a.seq, (uint64_t)(s0 + w0));
-        for (int64_t w = w0;;) {
+        {
             const uint64_t h = fw ^ rc;
-            if (h <= thr) {
-                const int32_t r = (int32_t)(w + k - 1) + a.r_offset;
-                const uint32_t rs = ((uint32_t)r << 1) | (fw > rc ? 1u : 0u);
-                if (MODE == SK_COUNT) {
-                    n_sel++;
-                } else if (MODE == SK_WRITE) {
-                    a.out_h[out_base + n_sel] = h;
-                    a.out_rs[out_base + n_sel] = rs;
-                    n_sel++;
-                } else {
-                    uint32_t slot = atomicAdd(a.kmer_cnt + q, 1u);
-                    if (slot < out_cap) {
-                        a.out_h[out_base + slot] = h;
-                        a.out_rs[out_base + slot] = rs;
-                    }
+            if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)r0 << 1) | (fw > rc ? 1u : 0u), out_base, out_cap, n_sel);
+        }
+        // rolling: window t takes base p[t + k - 1] in and drops p[t - 1]; both byte
+        // streams are read as aligned 32-bit words realigned by one funnel shift
+        const uintptr_t ai = (uintptr_t)(p + k), ao = (uintptr_t)p;
+        const uint32_t shi = (uint32_t)(ai & 3) * 8, sho = (uint32_t)(ao & 3) * 8;
+        const uint32_t* wi = (const uint32_t*)(ai & ~(uintptr_t)3);
+        const uint32_t* wo = (const uint32_t*)(ao & ~(uintptr_t)3);
+        uint32_t li = __ldg(wi), lo_ = __ldg(wo);
+        for (int32_t t = 1; t < cnt; t += 4) {
+            const uint32_t hi_i = __ldg(++wi), hi_o = __ldg(++wo);
+            const uint32_t ib4 = __funnelshift_r(li, hi_i, shi), ob4 = __funnelshift_r(lo_, hi_o, sho);
+            li = hi_i;
+            lo_ = hi_o;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (t + j < cnt) {
+                    const uint32_t ib = (ib4 >> (8 * j)) & 0xffu, ob = (ob4 >> (8 * j)) & 0xffu;
+                    fw = rotl1(fw) ^ L.fw_k[ob] ^ L.fw[ib];
+                    rc = rotr1(rc) ^ L.rc_r1[ob] ^ L.rc_k1[ib];
+                    const uint64_t h = fw ^ rc;
+                    if (h <= thr)
+                        emit_kmer<MODE>(a, q, h, ((uint32_t)(r0 + t + j) << 1) | (fw > rc ? 1u : 0u), out_base,
+                                        out_cap, n_sel);
                 }
             }
-            if (++w >= w1) break;
-            const uint32_t ib = in.get(), ob = out.get();
-            fw = rotl64(fw, 1) ^ L.fw_k[ob] ^ L.fw[ib];
-            rc = rotr64(rc, 1) ^ L.rc_r1[ob] ^ L.rc_k1[ib];
         }
         if (MODE == SK_COUNT) a.chunk_cnt[c] = n_sel;
     }
