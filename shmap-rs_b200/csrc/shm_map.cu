@@ -40,6 +40,8 @@
 //    of the sequential loop does.
 // All scores use explicit round-to-nearest f64 intrinsics.
 #include <algorithm>
+#include <chrono>
+#include <string>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -57,6 +59,14 @@ namespace shm {
 struct BatchMax {
     unsigned int m_max, nu_max, half_max, n_overflow;
     unsigned long long kmers, distinct, proc_seeds, hits, buckets, ext_seeds, refine_kmers;
+};
+
+// Small device-to-host reads of a batch, landing in pinned memory.
+struct HostReads {
+    uint64_t totals[2];  // hit words, bucket-table slots
+    BatchMax hm;         // after seed preparation
+    uint32_t nj, nc;     // bucket jobs, candidates
+    BatchMax fin;        // after the sweep
 };
 
 struct BatchView {
@@ -140,7 +150,7 @@ __device__ void bitonic_ab(uint64_t* A, uint32_t* B, uint32_t P) {
     for (uint32_t k = 2; k <= P; k <<= 1)
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
-                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;  // j is a power of two
                 bool asc = (i & k) == 0;
                 uint64_t ai = A[i], al = A[l];
                 uint32_t bi = B[i], bl = B[l];
@@ -160,7 +170,7 @@ __device__ void bitonic_u64(uint64_t* A, uint32_t P) {
     for (uint32_t k = 2; k <= P; k <<= 1)
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
-                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;  // j is a power of two
                 bool asc = (i & k) == 0;
                 uint64_t ai = A[i], al = A[l];
                 if ((ai > al) == asc) {
@@ -214,6 +224,41 @@ __device__ __forceinline__ uint64_t seed_bucket_bound(const BatchView& v, uint32
 }
 
 // ------------------------------------------------------------------ K2 seedprep
+// The per-read fields every seed-preparation form starts from; false when
+// the read stops here (overflow or a sketch below MIN_HALFLEN).
+__device__ __forceinline__ bool seed_prologue(const BatchView& v, int32_t q, uint32_t P, bool leader, uint32_t& m,
+                                              uint64_t& kb, int32_t& S, int32_t& halflen) {
+    const int64_t read_len = v.roff[q + 1] - v.roff[q];
+    kb = v.kcap_off[q];
+    const uint32_t cap = (uint32_t)(v.kcap_off[q + 1] - kb);
+    m = v.kcnt[q];
+    if (leader) {
+        v.hw[q] = 0;
+        v.bt_size[q] = 0;
+        v.r_nproc[q] = 0;
+        v.r_nu[q] = 0;
+        v.r_S0[q] = 0;
+        v.r_smatch[q] = 0;
+        v.r_maxseed[q] = 0;
+        v.r_m[q] = (int32_t)m;
+        v.r_half[q] = 0;
+    }
+    if (m > cap || m > P) {
+        if (leader) v.r_status[q] = ST_OVERFLOW;
+        return false;
+    }
+    S = __double2int_rz(__dmul_rn(__dsub_rn(1.0, v.theta2), (double)m)) + 1;
+    halflen = v.P.ap ? (int32_t)read_len : (int32_t)m;
+    if (halflen < MIN_HALFLEN) {
+        if (leader) {
+            v.r_status[q] = ST_SHORT_SKETCH;
+            v.r_S[q] = S;
+        }
+        return false;
+    }
+    return true;
+}
+
 // One CTA per read. Arrays (P = power of two >= the read's k-mer capacity):
 // A/B element keys, GA/GB group hash and occs<<1|strand, GF first index then
 // count(), GD hit-list start, E rarest-first sort keys.
@@ -241,34 +286,10 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
     __shared__ uint64_t t64;
     __shared__ uint32_t t32;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int64_t read_len = v.roff[q + 1] - v.roff[q];
-    const uint64_t kb = v.kcap_off[q];
-    const uint32_t cap = (uint32_t)(v.kcap_off[q + 1] - kb);
-    const uint32_t m = v.kcnt[q];
-    if (tid == 0) {
-        v.hw[q] = 0;
-        v.bt_size[q] = 0;
-        v.r_nproc[q] = 0;
-        v.r_nu[q] = 0;
-        v.r_S0[q] = 0;
-        v.r_smatch[q] = 0;
-        v.r_maxseed[q] = 0;
-        v.r_m[q] = (int32_t)m;
-        v.r_half[q] = 0;
-    }
-    if (m > cap || cap > P) {
-        if (tid == 0) v.r_status[q] = ST_OVERFLOW;
-        return;
-    }
-    int32_t S = __double2int_rz(__dmul_rn(__dsub_rn(1.0, v.theta2), (double)m)) + 1;
-    const int32_t halflen = v.P.ap ? (int32_t)read_len : (int32_t)m;
-    if (halflen < MIN_HALFLEN) {
-        if (tid == 0) {
-            v.r_status[q] = ST_SHORT_SKETCH;
-            v.r_S[q] = S;
-        }
-        return;
-    }
+    uint32_t m;
+    uint64_t kb;
+    int32_t S, halflen;
+    if (!seed_prologue(v, q, P, tid == 0, m, kb, S, halflen)) return;
     const uint32_t Pm = (uint32_t)pow2_ceil(m);
     for (uint32_t i = tid; i < Pm; i += nt) {
         if (i < m) {
@@ -393,11 +414,13 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
 }
 
 template <bool GLOBAL>
-__global__ void __launch_bounds__(256) k_seedprep(BatchView v, const int32_t* __restrict__ list, int32_t n_list,
-                                                  uint32_t P, uint8_t* gscr, size_t gscr_per_cta) {
+__global__ void __launch_bounds__(256) k_seedprep(BatchView v, const int32_t* __restrict__ list,
+                                                  const uint32_t* __restrict__ n_list_d, uint32_t P, uint8_t* gscr,
+                                                  size_t gscr_per_cta) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint8_t* base = GLOBAL ? gscr + (size_t)blockIdx.x * gscr_per_cta : smem;
     SeedArrays S_ = carve(base, P);
+    const int32_t n_list = (int32_t)*n_list_d;
     for (int32_t li = blockIdx.x; li < n_list; li += gridDim.x) {
         seedprep_one(v, list[li], P, S_);
         __syncthreads();
@@ -415,7 +438,7 @@ __device__ void warp_bitonic_ab(uint64_t* A, uint32_t* B, uint32_t P, int lane) 
     for (uint32_t k = 2; k <= P; k <<= 1)
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             for (uint32_t t = lane; t < P / 2; t += 32) {
-                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;  // j is a power of two
                 bool asc = (i & k) == 0;
                 uint64_t ai = A[i], al = A[l];
                 uint32_t bi = B[i], bl = B[l];
@@ -435,7 +458,7 @@ __device__ void warp_bitonic_u64(uint64_t* A, uint32_t P, int lane) {
     for (uint32_t k = 2; k <= P; k <<= 1)
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             for (uint32_t t = lane; t < P / 2; t += 32) {
-                uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;  // j is a power of two
                 bool asc = (i & k) == 0;
                 uint64_t ai = A[i], al = A[l];
                 if ((ai > al) == asc) {
@@ -451,34 +474,10 @@ __device__ void seedprep_warp(const BatchView& v, int32_t q, uint32_t P, uint64_
                               uint32_t* D) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u, le = lt | (1u << lane);
-    const int64_t read_len = v.roff[q + 1] - v.roff[q];
-    const uint64_t kb = v.kcap_off[q];
-    const uint32_t cap = (uint32_t)(v.kcap_off[q + 1] - kb);
-    const uint32_t m = v.kcnt[q];
-    if (lane == 0) {
-        v.hw[q] = 0;
-        v.bt_size[q] = 0;
-        v.r_nproc[q] = 0;
-        v.r_nu[q] = 0;
-        v.r_S0[q] = 0;
-        v.r_smatch[q] = 0;
-        v.r_maxseed[q] = 0;
-        v.r_m[q] = (int32_t)m;
-        v.r_half[q] = 0;
-    }
-    if (m > cap || cap > P) {
-        if (lane == 0) v.r_status[q] = ST_OVERFLOW;
-        return;
-    }
-    int32_t S = __double2int_rz(__dmul_rn(__dsub_rn(1.0, v.theta2), (double)m)) + 1;
-    const int32_t halflen = v.P.ap ? (int32_t)read_len : (int32_t)m;
-    if (halflen < MIN_HALFLEN) {
-        if (lane == 0) {
-            v.r_status[q] = ST_SHORT_SKETCH;
-            v.r_S[q] = S;
-        }
-        return;
-    }
+    uint32_t m;
+    uint64_t kb;
+    int32_t S, halflen;
+    if (!seed_prologue(v, q, P, lane == 0, m, kb, S, halflen)) return;
     const uint32_t Pm = max((uint32_t)2, (uint32_t)pow2_ceil(m));
     for (uint32_t i = lane; i < Pm; i += 32) {
         if (i < m) {
@@ -600,9 +599,10 @@ __device__ void seedprep_warp(const BatchView& v, int32_t q, uint32_t P, uint64_
     }
 }
 
-__global__ void __launch_bounds__(256) k_seedprep_w(BatchView v, const int32_t* __restrict__ list, int32_t n_list,
-                                                    uint32_t P) {
+__global__ void __launch_bounds__(256) k_seedprep_w(BatchView v, const int32_t* __restrict__ list,
+                                                    const uint32_t* __restrict__ n_list_d, uint32_t P) {
     extern __shared__ __align__(16) uint8_t smem[];
+    const int32_t n_list = (int32_t)*n_list_d;
     const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     uint8_t* base = smem + (size_t)wib * SEEDW_BYTES_PER_ELEM * P;
     uint64_t* A = (uint64_t*)base;
@@ -612,6 +612,261 @@ __global__ void __launch_bounds__(256) k_seedprep_w(BatchView v, const int32_t* 
     for (int32_t li = blockIdx.x * wpb + wib; li < n_list; li += gridDim.x * wpb) {
         seedprep_warp(v, list[li], P, A, E, B, D);
         __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ K2 register form
+// Reads whose sketch has m <= 32 * EPL k-mers: one warp per read with the
+// k-mers in registers, EPL per lane (element e = r * 32 + lane). The bitonic
+// network's stages with partners in another lane are shuffles, the others
+// register compare-exchanges; every lane works on EPL independent elements,
+// so the sorts are not latency-bound. Shared memory holds only the groups:
+// hash GA[g] and occs << 1 | strand GB[g], 12 bytes per element.
+constexpr int SEEDR_WARPS = 8;
+
+template <int EPL>
+__device__ __forceinline__ void wreg_stage_lane(uint64_t (&A)[EPL], uint32_t (&B)[EPL], int R, uint32_t k, uint32_t j,
+                                                int lane) {
+    const bool lower = (lane & j) == 0;
+#pragma unroll
+    for (int r = 0; r < EPL; r++) {
+        if (r < R) {
+            const uint64_t pa = __shfl_xor_sync(0xffffffffu, A[r], j);
+            const uint32_t pb = __shfl_xor_sync(0xffffffffu, B[r], j);
+            const bool asc = ((((uint32_t)r << 5) | (uint32_t)lane) & k) == 0;
+            const bool pless = pa < A[r] || (pa == A[r] && pb < B[r]);
+            // the lower element of an ascending pair keeps the minimum, and so on
+            if (pless == (lower == asc)) {
+                A[r] = pa;
+                B[r] = pb;
+            }
+        }
+    }
+}
+
+template <int EPL, int JR>
+__device__ __forceinline__ void wreg_stage_reg(uint64_t (&A)[EPL], uint32_t (&B)[EPL], int R, uint32_t k) {
+    if constexpr (JR < EPL) {
+#pragma unroll
+        for (int r = 0; r < EPL; r++) {
+            if ((r & JR) == 0 && r < R) {  // R is a power of two above JR, so r | JR < R too
+                const int s2 = r | JR;
+                const bool asc = (((uint32_t)r << 5) & k) == 0;  // k >= 64: a bit of r
+                const bool gt = A[r] > A[s2] || (A[r] == A[s2] && B[r] > B[s2]);
+                if (gt == asc) {
+                    const uint64_t ta = A[r];
+                    A[r] = A[s2];
+                    A[s2] = ta;
+                    const uint32_t tb = B[r];
+                    B[r] = B[s2];
+                    B[s2] = tb;
+                }
+            }
+        }
+    }
+}
+
+// Ascending sort of the R * 32 elements (A, B) of a warp (R a power of two).
+template <int EPL>
+__device__ void wreg_sort(uint64_t (&A)[EPL], uint32_t (&B)[EPL], int R, int lane) {
+    const uint32_t n = (uint32_t)R << 5;
+    for (uint32_t k = 2; k <= n; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j < 32) {
+                wreg_stage_lane<EPL>(A, B, R, k, j, lane);
+            } else {
+                switch (j >> 5) {
+                    case 1: wreg_stage_reg<EPL, 1>(A, B, R, k); break;
+                    case 2: wreg_stage_reg<EPL, 2>(A, B, R, k); break;
+                    case 4: wreg_stage_reg<EPL, 4>(A, B, R, k); break;
+                    case 8: wreg_stage_reg<EPL, 8>(A, B, R, k); break;
+                    case 16: wreg_stage_reg<EPL, 16>(A, B, R, k); break;
+                    default: break;
+                }
+            }
+        }
+    }
+}
+
+template <int EPL>
+__device__ void seedprep_reg(const BatchView& v, int32_t q, uint64_t* GA, uint32_t* GB) {
+    const int lane = threadIdx.x & 31;
+    const unsigned le = (2u << lane) - 1u;  // lanes <= this one
+    uint32_t m;
+    uint64_t kb;
+    int32_t S, halflen;
+    if (!seed_prologue(v, q, 32u * EPL, lane == 0, m, kb, S, halflen)) return;
+    const int R = (int)(max((uint32_t)32, (uint32_t)pow2_ceil(m)) >> 5);
+    uint64_t A[EPL];
+    uint32_t B[EPL];
+#pragma unroll
+    for (int r = 0; r < EPL; r++) {
+        const uint32_t e = ((uint32_t)r << 5) | (uint32_t)lane;
+        if (r < R && e < m) {
+            A[r] = v.km_h[kb + e];
+            const uint32_t rs = v.km_rs[kb + e];
+            B[r] = ((0x3fffffffu - (rs >> 1)) << 1) | (rs & 1u);
+        } else {
+            A[r] = ~0ULL;
+            B[r] = 0xffffffffu;
+        }
+    }
+    wreg_sort<EPL>(A, B, R, lane);  // (h asc, r desc): src/shmap/seeding.rs:28-34
+
+    // groups of equal hashes (src/shmap/seeding.rs:45-67)
+    uint32_t n_u = 0, open_start = 0;
+    uint64_t carry_h = 0;
+#pragma unroll
+    for (int r = 0; r < EPL; r++) {
+        if (r < R) {
+            const uint32_t e = ((uint32_t)r << 5) | (uint32_t)lane;
+            const bool valid = e < m;
+            const uint64_t h = A[r];
+            uint64_t hp = __shfl_up_sync(0xffffffffu, h, 1);
+            if (lane == 0) hp = carry_h;
+            uint64_t hn = __shfl_down_sync(0xffffffffu, h, 1);
+            const uint64_t nx = __shfl_sync(0xffffffffu, A[r + 1 < EPL ? r + 1 : r], 0);
+            if (lane == 31) hn = nx;  // element e + 1 sits in the next register (irrelevant past m - 1)
+            const bool first = valid && (e == 0 || h != hp);
+            const bool last = valid && (e + 1 == m || hn != h);
+            const unsigned fmask = __ballot_sync(0xffffffffu, first);
+            const unsigned fle = fmask & le;
+            const uint32_t gid = n_u + __popc(fle) - 1;
+            const uint32_t start = fle ? (((uint32_t)r << 5) + 31 - __clz(fle)) : open_start;
+            if (first) GA[gid] = h;
+            if (last) GB[gid] = ((e - start + 1) << 1) | (B[r] & 1u);  // representative: smallest r (seeding.rs:56)
+            n_u += __popc(fmask);
+            open_start = __shfl_sync(0xffffffffu, start, 31);
+            carry_h = __shfl_sync(0xffffffffu, h, 31);
+        }
+    }
+    __syncwarp();
+    if (v.P.os) S = (int32_t)n_u;  // mod.rs:732-736
+
+    // count() probes (index.rs:204-213); rarest first, stable over hash order
+    // (seeding.rs:71): keys cnt << 32 | g with the hit-list start alongside
+    const int Ru = (int)(max((uint32_t)32, (uint32_t)pow2_ceil(n_u)) >> 5);
+#pragma unroll
+    for (int r = 0; r < EPL; r++) {
+        if (r < Ru) {
+            const uint32_t g = ((uint32_t)r << 5) | (uint32_t)lane;
+            if (g < n_u) {
+                uint32_t a, cnt;
+                idx_lookup(v.I, GA[g], a, cnt);
+                A[r] = ((uint64_t)cnt << 32) | g;
+                B[r] = a;
+            } else {
+                A[r] = ~0ULL;
+                B[r] = 0xffffffffu;
+            }
+        }
+    }
+    wreg_sort<EPL>(A, B, Ru, lane);
+
+    // seeding prefix: seed i is processed iff sum(occs before i) < S (seeding.rs:101)
+    uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
+    uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
+#pragma unroll
+    for (int r = 0; r < EPL; r++) {
+        if (r < Ru) {
+            const uint32_t i = ((uint32_t)r << 5) | (uint32_t)lane;
+            const bool valid = i < n_u;
+            const uint32_t g = (uint32_t)(A[r] & 0xffffffffu), cnt = valid ? (uint32_t)(A[r] >> 32) : 0u;
+            const uint32_t os = valid ? GB[g] : 0u, occs = os >> 1;
+            const uint32_t oi = warp_inclusive_scan(occs);
+            const uint64_t ci = warp_inclusive_scan((uint64_t)cnt);
+            const uint32_t po = po_carry + oi - occs;
+            const uint64_t pc = pc_carry + ci - cnt;
+            if (valid) {
+                const uint64_t hg = GA[g];
+                const uint32_t a = B[r];
+                v.sd_h[kb + i] = hg;
+                v.sd_os[kb + i] = os;
+                v.sd_cnt[kb + i] = cnt;
+                v.sd_a[kb + i] = a;
+                v.sd_ooff[kb + i] = po;
+                if ((int64_t)po < (int64_t)S) {
+                    v.sd_hpre[kb + i] = (uint32_t)pc;
+                    l_np++;
+                    l_s0 += occs;
+                    l_sm += cnt;
+                    l_max = max(l_max, cnt);
+                    l_eb += seed_bucket_bound(v, a, cnt, halflen);
+                }
+                pht_insert(v, q, hg, i);
+            }
+            po_carry += __shfl_sync(0xffffffffu, oi, 31);
+            pc_carry += __shfl_sync(0xffffffffu, ci, 31);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l_np += __shfl_xor_sync(0xffffffffu, l_np, o);
+        l_s0 += __shfl_xor_sync(0xffffffffu, l_s0, o);
+        l_sm += __shfl_xor_sync(0xffffffffu, l_sm, o);
+        l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
+        l_max = max(l_max, __shfl_xor_sync(0xffffffffu, l_max, o));
+    }
+    if (lane == 0) {
+        v.r_status[q] = ST_UNMAPPED;
+        v.r_nu[q] = (int32_t)n_u;
+        v.r_nproc[q] = (int32_t)l_np;
+        v.r_S[q] = S;
+        v.r_S0[q] = (int32_t)l_s0;
+        v.r_smatch[q] = (int64_t)l_sm;
+        v.r_maxseed[q] = (int32_t)l_max;
+        v.r_half[q] = halflen;
+        if (l_sm >= 0xffffffffULL) {
+            v.r_status[q] = ST_OVERFLOW;
+        } else {
+            v.hw[q] = l_sm;
+            v.bt_size[q] = l_sm ? max((uint64_t)16, pow2_ceil(2 * l_eb)) : 0;
+        }
+        atomicMax(&v.mx->m_max, m);
+        atomicMax(&v.mx->nu_max, n_u);
+        atomicMax(&v.mx->half_max, (uint32_t)halflen);
+        atomicAdd(&v.mx->kmers, (unsigned long long)m);
+        atomicAdd(&v.mx->distinct, (unsigned long long)n_u);
+        atomicAdd(&v.mx->proc_seeds, (unsigned long long)l_np);
+        atomicAdd(&v.mx->hits, (unsigned long long)l_sm);
+    }
+}
+
+template <int EPL>
+__global__ void __launch_bounds__(SEEDR_WARPS * 32) k_seedprep_r(BatchView v, const int32_t* __restrict__ list,
+                                                                 const uint32_t* __restrict__ n_list) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int wib = threadIdx.x >> 5;
+    uint64_t* GA = (uint64_t*)smem + (size_t)wib * 32 * EPL;
+    uint32_t* GB = (uint32_t*)((uint64_t*)smem + (size_t)SEEDR_WARPS * 32 * EPL) + (size_t)wib * 32 * EPL;
+    const int32_t n = (int32_t)*n_list;
+    for (int32_t li = blockIdx.x * SEEDR_WARPS + wib; li < n; li += gridDim.x * SEEDR_WARPS) {
+        seedprep_reg<EPL>(v, list[li], GA, GB);
+        __syncwarp();
+    }
+}
+
+// Seed-preparation bins by the actual sketch size m of each read (reads past
+// their k-mer capacity go to bin 0, whose prologue marks them overflowed):
+// m <= 256 and m <= 512 register forms, m <= 1024 warp with shared arrays,
+// m <= 4096 CTA in shared memory, larger CTA with global scratch.
+constexpr int N_SEED_BINS = 5;
+__global__ void k_seed_bins(BatchView v, int32_t* __restrict__ lists, uint32_t* __restrict__ bin_cnt) {
+    const int lane = threadIdx.x & 31;
+    for (int32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < v.n; base += gridDim.x * blockDim.x) {
+        const int32_t q = base + lane;
+        int b = -1;
+        if (q < v.n) {
+            const uint32_t m = v.kcnt[q];
+            const uint32_t cap = (uint32_t)(v.kcap_off[q + 1] - v.kcap_off[q]);
+            b = m > cap ? 0 : m <= 256 ? 0 : m <= 512 ? 1 : m <= 1024 ? 2 : m <= 4096 ? 3 : 4;
+        }
+        const unsigned same = __match_any_sync(0xffffffffu, b);
+        const int leader = __ffs(same) - 1;
+        uint32_t at = 0;
+        if (lane == leader && b >= 0) at = atomicAdd(bin_cnt + b, (uint32_t)__popc(same));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (b >= 0) lists[(size_t)b * v.n + at + __popc(same & ((1u << lane) - 1u))] = q;
     }
 }
 
@@ -1169,7 +1424,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
             for (uint32_t k = 2; k <= P; k <<= 1)
                 for (uint32_t j = k >> 1; j > 0; j >>= 1) {
                     for (uint32_t t = lane; t < P / 2; t += 32) {
-                        uint32_t i = 2 * j * (t / j) + (t % j), l = i + j;
+                        uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;  // j is a power of two
                         bool asc = (i & k) == 0;
                         SweepCand a = G[i], b = G[l];
                         if (sc_less(b, a) == asc) {
@@ -1259,7 +1514,8 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
                 }
             } else if (st == ST_OVERFLOW) {
                 uint32_t k = atomicAdd(&v.mx->n_overflow, 1u);
-                v.ovf_list[k] = (uint32_t)q;
+                v.ovf_list[2 * (size_t)k] = (uint32_t)q;
+                v.ovf_list[2 * (size_t)k + 1] = v.kcnt[q];
             }
             v.out[q] = rec;
         }
@@ -1274,6 +1530,30 @@ const char* const WORK_NAMES[N_WORK] = {"reads", "bases", "kmers", "distinct_see
                                         "refine_kmers"};
 
 // Event pairs around each stage of a batch, read back once the batch is done.
+// Host-side phase clock, printed per batch when SHMAP_HOSTPROF is set.
+struct HostClock {
+    bool on;
+    std::chrono::steady_clock::time_point t0, last;
+    std::string line;
+    HostClock() : on(std::getenv("SHMAP_HOSTPROF") != nullptr) {
+        if (on) t0 = last = std::chrono::steady_clock::now();
+    }
+    void mark(const char* what) {
+        if (!on) return;
+        auto now = std::chrono::steady_clock::now();
+        char b[64];
+        std::snprintf(b, sizeof b, " %s=%.3f", what, std::chrono::duration<double, std::milli>(now - last).count());
+        line += b;
+        last = now;
+    }
+    void print(const char* tag, int32_t n) {
+        if (!on) return;
+        std::fprintf(stderr, "[shmap-host] %s n=%d total=%.3f%s\n", tag, n,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(),
+                     line.c_str());
+    }
+};
+
 struct StageTimer {
     MapCtx* c;
     size_t used = 0;
@@ -1315,12 +1595,17 @@ struct StageTimer {
 };
 
 struct MapScratch {
-    DevBuf<uint8_t> seq;
-    DevBuf<int64_t> roff;
-    DevBuf<uint64_t> chunk_off, kcap_off, pht_off, km_h, sd_h, pht_key, hw, hw_off, bt_size, bt_off;
+    DevBuf<uint8_t> seqb[2];  // host-form batches: one mapped, the next arriving
+    DevBuf<uint8_t> plan;  // BatchPlan's arrays on the device
+    DevBuf<int32_t> seed_lists;  // N_SEED_BINS lists of n reads
+    DevBuf<uint32_t> bin_cnt;
+    DevBuf<uint8_t> retry_seq;  // reads mapped again with exact bounds
+    DevBuf<shm_map_record> retry_out, retry_all;
+    DevBuf<int32_t> retry_idx;
+    DevBuf<uint64_t> km_h, sd_h, pht_key, hw, hw_off, bt_size, bt_off;
     DevBuf<uint32_t> kcnt, km_rs, sd_a, sd_cnt, sd_os, sd_hpre, sd_ooff, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
         cidx, sort_scr, ovf_list;
-    DevBuf<int32_t> r_i32, lists, ref_scr;
+    DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
     DevBuf<BSlot> bt;
     DevBuf<uint32_t> bt_list;
@@ -1339,7 +1624,13 @@ MapCtx* mapctx_create(int device, size_t hbm_budget) {
     c->device = device;
     c->hbm_budget = hbm_budget;
     SHM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    SHM_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    SHM_CUDA(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+    SHM_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    SHM_CUDA(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
+    for (auto& e : c->copied) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     c->scr = new MapScratch();
+    SHM_CUDA(cudaHostAlloc(&c->h_reads, sizeof(HostReads), cudaHostAllocDefault));
     return c;
 }
 
@@ -1352,6 +1643,17 @@ void mapctx_destroy(MapCtx* c) {
         delete c->scr;
     }
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->h_reads) cudaFreeHost(c->h_reads);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    for (auto& e : c->copied)
+        if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->side_stream) {
+        cudaStreamSynchronize(c->side_stream);
+        cudaStreamDestroy(c->side_stream);
+    }
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1364,78 +1666,108 @@ static uint64_t pow2_host(uint64_t x) {
 
 // k-mer capacity of a read of nw windows: the reference's own estimate
 // mean + 6 sigma + 16 (src/sketch.rs:143-146); reads that beat it are retried
-// with the exact bound.
-static uint64_t kmer_cap(int64_t nw, double h_frac, bool exact) {
+// with the count the first pass found.
+static uint64_t kmer_cap(int64_t nw, double h_frac) {
     if (nw <= 0) return 0;
-    if (exact || h_frac >= 1.0) return (uint64_t)nw;
+    if (h_frac >= 1.0) return (uint64_t)nw;
     double mean = std::max(0.0, (double)nw * h_frac);
     uint64_t c = (uint64_t)(mean + 6.0 * std::sqrt(mean)) + 16;
     return std::min<uint64_t>(c, (uint64_t)nw);
 }
 
-// Seed-preparation bins by the power of two P >= a read's k-mer capacity:
-// warp-per-read slices for P <= 1024, a CTA per read for P <= 4096, a CTA with
-// global scratch beyond.
-constexpr int N_SEED_BINS = 5;
-static const uint32_t SEED_BIN_P[N_SEED_BINS - 1] = {256, 512, 1024, 4096};
-
+// A batch's per-read plan, written by the host straight into pinned memory
+// and sent up in one copy: offsets of the reads, of their sketch runs, of
+// their k-mer capacities and of their probe tables.
 struct BatchPlan {
-    std::vector<int64_t> roff;
-    std::vector<uint64_t> chunk_off, kcap_off, pht_off;
-    std::vector<int32_t> bins[N_SEED_BINS];
-    uint32_t P_g = 0;
+    int64_t* roff;         // n+1
+    uint64_t* chunk_off;   // n+1
+    uint64_t* kcap_off;    // n+1
+    uint64_t* pht_off;     // n+1
+    uint32_t n_cap_512 = 0, n_cap_1024 = 0, n_cap_4096 = 0;  // reads whose capacity exceeds 512 / 1024 / 4096
+    uint32_t P_g = 0;                          // power of two >= every capacity above 4096
+    size_t bytes = 0;
+    static size_t layout(int32_t n) { return 4 * ((size_t)n + 1) * 8; }
+    void carve(uint8_t* base, int32_t n) {
+        const size_t a = ((size_t)n + 1) * 8;
+        bytes = layout(n);
+        roff = (int64_t*)base;
+        chunk_off = (uint64_t*)(base + a);
+        kcap_off = (uint64_t*)(base + 2 * a);
+        pht_off = (uint64_t*)(base + 3 * a);
+    }
 };
 
-static void plan_batch(const int64_t* h_offs, int32_t n, int32_t k, double h_frac, bool exact, BatchPlan& bp) {
-    bp.roff.assign((size_t)n + 1, 0);
-    bp.chunk_off.assign((size_t)n + 1, 0);
-    bp.kcap_off.assign((size_t)n + 1, 0);
-    bp.pht_off.assign((size_t)n + 1, 0);
-    for (auto& b : bp.bins) b.clear();
+// Grow-only pinned host staging of a context (the plan of the batch in flight).
+static uint8_t* pinned_stage(MapCtx* c, size_t bytes) {
+    if (bytes > c->h_pinned_cap) {
+        if (c->h_pinned) SHM_CUDA(cudaFreeHost(c->h_pinned));
+        c->h_pinned = nullptr;
+        c->h_pinned_cap = 0;
+        const size_t want = std::max<size_t>(bytes + bytes / 4, (size_t)1 << 20);
+        SHM_CUDA(cudaHostAlloc((void**)&c->h_pinned, want, cudaHostAllocDefault));
+        c->h_pinned_cap = want;
+    }
+    return c->h_pinned;
+}
+
+// caps = null: capacities from the estimate; else caps[i] k-mers for read i
+// (the counts a previous pass found).
+static void plan_batch(MapCtx* c, const int64_t* h_offs, int32_t n, int32_t k, double h_frac, const uint32_t* caps,
+                       BatchPlan& bp) {
+    bp.carve(pinned_stage(c, BatchPlan::layout(n)), n);
     bp.P_g = 0;
+    bp.n_cap_512 = bp.n_cap_1024 = bp.n_cap_4096 = 0;
+    bp.roff[0] = 0;
+    bp.chunk_off[0] = 0;
+    bp.kcap_off[0] = 0;
+    bp.pht_off[0] = 0;
     for (int32_t i = 0; i < n; i++) {
-        int64_t L = h_offs[i + 1] - h_offs[i];
-        bp.roff[(size_t)i + 1] = bp.roff[(size_t)i] + L;
-        int64_t nw = L - k + 1;
-        bp.chunk_off[(size_t)i + 1] = bp.chunk_off[(size_t)i] + (nw > 0 ? (uint64_t)((nw + SKETCH_WIN - 1) / SKETCH_WIN) : 0);
-        uint64_t cap = kmer_cap(nw, h_frac, exact);
-        bp.kcap_off[(size_t)i + 1] = bp.kcap_off[(size_t)i] + cap;
-        bp.pht_off[(size_t)i + 1] = bp.pht_off[(size_t)i] + std::max<uint64_t>(16, pow2_host(2 * cap));
-        uint64_t P = pow2_host(std::max<uint64_t>(cap, 1));
-        int b = 0;
-        while (b < N_SEED_BINS - 1 && P > SEED_BIN_P[b]) b++;
-        bp.bins[b].push_back(i);
-        if (b == N_SEED_BINS - 1) bp.P_g = std::max<uint32_t>(bp.P_g, (uint32_t)P);
+        const int64_t L = h_offs[i + 1] - h_offs[i];
+        bp.roff[i + 1] = bp.roff[i] + L;
+        const int64_t nw = L - k + 1;
+        bp.chunk_off[i + 1] = bp.chunk_off[i] + (nw > 0 ? (uint64_t)((nw + SKETCH_WIN - 1) / SKETCH_WIN) : 0);
+        const uint64_t cap = caps ? (uint64_t)caps[i] : kmer_cap(nw, h_frac);
+        bp.kcap_off[i + 1] = bp.kcap_off[i] + cap;
+        bp.pht_off[i + 1] = bp.pht_off[i] + std::max<uint64_t>(16, pow2_host(2 * cap));
+        if (cap > 512) bp.n_cap_512++;
+        if (cap > 1024) bp.n_cap_1024++;
+        if (cap > 4096) {
+            bp.n_cap_4096++;
+            bp.P_g = std::max<uint32_t>(bp.P_g, (uint32_t)pow2_host(cap));
+        }
     }
 }
 
-template <class T>
-static void upload(DevBuf<T>& b, const std::vector<T>& h, cudaStream_t s) {
-    b.reserve(h.size() + 1);
-    if (!h.empty()) SHM_CUDA(cudaMemcpyAsync(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
-}
-
+// A read that overflowed a capacity, with its sketch size.
+struct Overflow {
+    int32_t read;
+    uint32_t m;
+};
 
 // Maps one batch whose bytes are already on the device at d_seq (relative
-// offsets h_offs[i] - h_offs[0]). Returns the reads that overflowed a
-// capacity (retried by the caller with exact bounds).
-static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
-                                      const int64_t* h_offs, int32_t n, shm_map_record* d_out, bool exact) {
+// offsets h_offs[i] - h_offs[0]); caps as for plan_batch. Returns the reads
+// that overflowed a capacity (retried by the caller with their counts).
+static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
+                                       const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
     StageTimer T(c);
+    HostClock H;
     BatchPlan bp;
-    plan_batch(h_offs, n, p.k, p.h_frac, exact, bp);
+    plan_batch(c, h_offs, n, p.k, p.h_frac, caps, bp);
+    H.mark("plan");
     if (!S.luts || S.luts_k != p.k) {
         if (S.luts) SHM_CUDA(cudaFree(S.luts));
         S.luts = create_device_luts(p.k, s);
         S.luts_k = p.k;
     }
     const uint64_t kcap = bp.kcap_off[(size_t)n], phtn = bp.pht_off[(size_t)n];
-    upload(S.roff, bp.roff, s);
-    upload(S.chunk_off, bp.chunk_off, s);
-    upload(S.kcap_off, bp.kcap_off, s);
-    upload(S.pht_off, bp.pht_off, s);
+    // the plan goes up in one copy from pinned memory; the pinned block is
+    // rewritten only by the next batch, after this one's first synchronize
+    S.plan.reserve(bp.bytes);
+    SHM_CUDA(cudaMemcpyAsync(S.plan.p, c->h_pinned, bp.bytes, cudaMemcpyHostToDevice, s));
+    BatchPlan dp;
+    dp.carve(S.plan.p, n);
     S.kcnt.reserve((size_t)n);
     S.km_h.reserve(kcap + 1);
     S.km_rs.reserve(kcap + 1);
@@ -1457,7 +1789,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     S.ccnt.reserve((size_t)n);
     S.coff.reserve((size_t)n + 1);
     S.ccur.reserve((size_t)n);
-    S.ovf_list.reserve((size_t)n);
+    S.ovf_list.reserve(2 * (size_t)n);
     S.n_jobs.reserve(1);
     S.mx.reserve(1);
     SHM_CUDA(cudaMemsetAsync(S.kcnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
@@ -1470,6 +1802,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     SHM_CUDA(cudaMemsetAsync(S.r_i32.p, 0, sizeof(int32_t) * (size_t)n * 8, s));
     SHM_CUDA(cudaMemsetAsync(S.hw.p, 0, sizeof(uint64_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.bt_size.p, 0, sizeof(uint64_t) * (size_t)n, s));
+    H.mark("upload");
 
     BatchView v{};
     v.n = n;
@@ -1486,8 +1819,8 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     v.P.ap = p.abs_pos;
     v.theta2 = p.theta - p.min_diff;
     v.seq = d_seq;
-    v.roff = S.roff.p;
-    v.kcap_off = S.kcap_off.p;
+    v.roff = dp.roff;
+    v.kcap_off = dp.kcap_off;
     v.kcnt = S.kcnt.p;
     v.km_h = S.km_h.p;
     v.km_rs = S.km_rs.p;
@@ -1497,7 +1830,7 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     v.sd_os = S.sd_os.p;
     v.sd_hpre = S.sd_hpre.p;
     v.sd_ooff = S.sd_ooff.p;
-    v.pht_off = S.pht_off.p;
+    v.pht_off = dp.pht_off;
     v.pht_key = S.pht_key.p;
     v.pht_val = S.pht_val.p;
     int32_t* ri = S.r_i32.p;
@@ -1526,14 +1859,14 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     // K1
     SketchArgs a{};
     a.seq = d_seq;
-    a.seq_off = S.roff.p;
-    a.chunk_off = S.chunk_off.p;
+    a.seq_off = dp.roff;
+    a.chunk_off = dp.chunk_off;
     a.n_seq = n;
     a.n_chunks = bp.chunk_off[(size_t)n];
     a.k = p.k;
     a.thr = ix->dev.thr;
     a.r_offset = 0;
-    a.kmer_off = S.kcap_off.p;
+    a.kmer_off = dp.kcap_off;
     a.kmer_cnt = S.kcnt.p;
     a.out_h = S.km_h.p;
     a.out_rs = S.km_rs.p;
@@ -1541,58 +1874,82 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     launch_sketch(SK_APPEND, a, S.luts, s);
     T.end();
 
-    // K2 per size bin: the bin lists go up in one copy
-    std::vector<int32_t> lists;
-    lists.reserve((size_t)n);
-    size_t bin_at[N_SEED_BINS];
-    for (int bi = 0; bi < N_SEED_BINS; bi++) {
-        bin_at[bi] = lists.size();
-        lists.insert(lists.end(), bp.bins[bi].begin(), bp.bins[bi].end());
+    // K2: bins by the actual sketch sizes, then one launch per bin (each
+    // reads its own count on the device; empty bins return at once)
+    S.bin_cnt.reserve(N_SEED_BINS);
+    S.seed_lists.reserve((size_t)N_SEED_BINS * (size_t)n);
+    SHM_CUDA(cudaMemsetAsync(S.bin_cnt.p, 0, sizeof(uint32_t) * N_SEED_BINS, s));
+    const int32_t* LB = S.seed_lists.p;
+    const uint32_t* NB = S.bin_cnt.p;
+    T.begin(STG_SEEDPREP);  // one span: bins, the side stream's large bins, the join
+    k_seed_bins<<<grid_for((size_t)n, 256, 8), 256, 0, s>>>(v, S.seed_lists.p, S.bin_cnt.p);
+    SHM_CUDA(cudaGetLastError());
+    // the few reads with large sketches go on the side stream, so that their
+    // long per-read latency overlaps the bulk of the reads on the main stream
+    // (a read of bin b has capacity >= m, which bounds each bin's size on the host)
+    const bool side = bp.n_cap_512 > 0;
+    if (side) {
+        SHM_CUDA(cudaEventRecord(c->fork, s));
+        SHM_CUDA(cudaStreamWaitEvent(c->side_stream, c->fork, 0));
     }
-    S.lists.reserve(lists.size() + 1);
-    SHM_CUDA(cudaMemcpyAsync(S.lists.p, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice, s));
-    for (int bi = 0; bi < N_SEED_BINS; bi++) {
-        const size_t len = bp.bins[bi].size();
-        if (len == 0) continue;
-        const int32_t* L = S.lists.p + bin_at[bi];
-        T.begin(STG_SEEDPREP);
-        if (bi < 3) {  // warp per read
-            const uint32_t P = SEED_BIN_P[bi];
-            const int wpb = P <= 512 ? 8 : 4;
-            const size_t bytes = SEEDW_BYTES_PER_ELEM * P * (size_t)wpb;
-            if ((int)bytes > c->seedw_smem_set) {
-                SHM_CUDA(cudaFuncSetAttribute(k_seedprep_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-                c->seedw_smem_set = (int)bytes;
-            }
-            int grid = grid_for(len * 32, wpb * 32, 2048 / (wpb * 32));
-            k_seedprep_w<<<grid, wpb * 32, bytes, s>>>(v, L, (int32_t)len, P);
-        } else if (bi == 3) {  // CTA per read
-            const uint32_t P = SEED_BIN_P[bi];
-            const size_t bytes = SEED_BYTES_PER_ELEM * P;
-            if ((int)bytes > c->seed_smem_set) {
-                SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-                c->seed_smem_set = (int)bytes;
-            }
-            k_seedprep<false><<<grid_for(len * 256, 256, 8), 256, bytes, s>>>(v, L, (int32_t)len, P, nullptr, 0);
-        } else {  // CTA per read, global scratch
-            const size_t bytes = SEED_BYTES_PER_ELEM * bp.P_g;
-            int grid = (int)std::min<size_t>(len, 296);
-            S.seed_gscr.reserve(bytes * (size_t)grid);
-            k_seedprep<true><<<grid, 256, 0, s>>>(v, L, (int32_t)len, bp.P_g, S.seed_gscr.p, bytes);
-        }
+    cudaStream_t s2 = c->side_stream;
+    if (bp.P_g) {  // m > 4096: CTA per read, global scratch
+        const size_t bytes = SEED_BYTES_PER_ELEM * bp.P_g;
+        const int grid = (int)std::min<size_t>(bp.n_cap_4096, 296);
+        S.seed_gscr.reserve(bytes * (size_t)grid);
+        k_seedprep<true><<<grid, 256, 0, s2>>>(v, LB + 4 * (size_t)n, NB + 4, bp.P_g, S.seed_gscr.p, bytes);
         SHM_CUDA(cudaGetLastError());
-        T.end();
+        count_launch();
     }
+    if (bp.n_cap_1024) {  // 1024 < m <= 4096: CTA per read
+        const uint32_t P = 4096;
+        const size_t bytes = SEED_BYTES_PER_ELEM * P;
+        if ((int)bytes > c->seed_smem_set) {
+            SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            c->seed_smem_set = (int)bytes;
+        }
+        k_seedprep<false><<<grid_for((size_t)bp.n_cap_1024 * 256, 256, 1), 256, bytes, s2>>>(v, LB + 3 * (size_t)n,
+                                                                                               NB + 3, P, nullptr, 0);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+    }
+    if (bp.n_cap_512) {  // 512 < m <= 1024: warp per read, shared arrays
+        const uint32_t P = 1024;
+        const int wpb = 4;
+        const size_t bytes = SEEDW_BYTES_PER_ELEM * P * (size_t)wpb;
+        if ((int)bytes > c->seedw_smem_set) {
+            SHM_CUDA(cudaFuncSetAttribute(k_seedprep_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            c->seedw_smem_set = (int)bytes;
+        }
+        k_seedprep_w<<<grid_for((size_t)bp.n_cap_512 * 32, wpb * 32, 2048 / (wpb * 32)), wpb * 32, bytes, s2>>>(
+            v, LB + 2 * (size_t)n, NB + 2, P);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+    }
+    if (side) SHM_CUDA(cudaEventRecord(c->join, s2));
+    {
+        const int wgrid = grid_for((size_t)n * 32, SEEDR_WARPS * 32, 4);
+        k_seedprep_r<8><<<wgrid, SEEDR_WARPS * 32, SEEDR_WARPS * 32 * 8 * 12, s>>>(v, LB, NB);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+        k_seedprep_r<16><<<wgrid, SEEDR_WARPS * 32, SEEDR_WARPS * 32 * 16 * 12, s>>>(v, LB + n, NB + 1);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+    }
+    if (side) SHM_CUDA(cudaStreamWaitEvent(s, c->join, 0));
+    T.end();
 
     exclusive_scan_u64(S.hw.p, S.hw_off.p, (size_t)n, s);
     exclusive_scan_u64(S.bt_size.p, S.bt_off.p, (size_t)n, s);
-    uint64_t totals[2];
-    BatchMax hm{};
-    SHM_CUDA(cudaMemcpyAsync(&totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    SHM_CUDA(cudaMemcpyAsync(&totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    SHM_CUDA(cudaMemcpyAsync(&hm, S.mx.p, sizeof hm, cudaMemcpyDeviceToHost, s));
+    HostReads& R = *(HostReads*)c->h_reads;
+    SHM_CUDA(cudaMemcpyAsync(&R.totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(&R.totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(&R.hm, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
+    H.mark("enq1");
     SHM_CUDA(cudaStreamSynchronize(s));
-    const uint64_t hw_total = totals[0], bt_total = totals[1];
+    H.mark("sync1");
+    const uint64_t hw_total = R.totals[0], bt_total = R.totals[1];
+    const BatchMax hm = R.hm;
     const bool debug = std::getenv("SHMAP_DEBUG") != nullptr;
     if (debug) {
         std::fprintf(stderr, "[shmap] batch n=%d kcap=%llu hw_total=%llu bt_total=%llu m_max=%u nu_max=%u half_max=%u\n",
@@ -1642,9 +1999,11 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
             SHM_CUDA(cudaGetLastError());
             T.end();
         }
-        uint32_t nj = 0;
-        SHM_CUDA(cudaMemcpyAsync(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaMemcpyAsync(&R.nj, S.n_jobs.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        H.mark("enq2");
         SHM_CUDA(cudaStreamSynchronize(s));
+        H.mark("sync2");
+        const uint32_t nj = R.nj;
         if (nj <= job_cap) break;
         job_cap = nj;  // retry with room for every job
         SHM_CUDA(cudaMemsetAsync(S.n_jobs.p, 0, sizeof(uint32_t), s));
@@ -1683,14 +2042,16 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
     SHM_CUDA(cudaGetLastError());
     T.end();
 
-    BatchMax fin{};
-    SHM_CUDA(cudaMemcpyAsync(&fin, S.mx.p, sizeof fin, cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(&R.fin, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(&R.nj, S.n_jobs.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(&R.nc, S.coff.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    H.mark("enq3");
     SHM_CUDA(cudaStreamSynchronize(s));
+    H.mark("sync3");
     T.collect();
+    const BatchMax fin = R.fin;
     {
-        uint32_t nj = 0, nc = 0;
-        SHM_CUDA(cudaMemcpy(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost));
-        SHM_CUDA(cudaMemcpy(&nc, S.coff.p + n, sizeof nc, cudaMemcpyDeviceToHost));
+        const uint32_t nj = R.nj, nc = R.nc;
         c->work[W_READS] += n;
         c->work[W_BASES] += h_offs[n] - h_offs[0];
         c->work[W_KMERS] += (int64_t)fin.kmers;
@@ -1719,119 +2080,161 @@ static std::vector<int32_t> run_batch(MapCtx* c, const IndexStorage* ix, const s
                              j.t_l, j.t_r, j.inter, j.same);
         }
     }
-    std::vector<int32_t> ovf;
-    if (fin.n_overflow) {
-        std::vector<uint32_t> l(fin.n_overflow);
+    std::vector<Overflow> ovf;
+    if (fin.n_overflow) {  // pairs (read, m) in ovf_list
+        std::vector<uint32_t> l(2 * (size_t)fin.n_overflow);
         SHM_CUDA(cudaMemcpy(l.data(), S.ovf_list.p, sizeof(uint32_t) * l.size(), cudaMemcpyDeviceToHost));
-        for (uint32_t x : l) ovf.push_back((int32_t)x);
-        std::sort(ovf.begin(), ovf.end());
+        for (size_t i = 0; i < fin.n_overflow; i++) ovf.push_back(Overflow{(int32_t)l[2 * i], l[2 * i + 1]});
+        std::sort(ovf.begin(), ovf.end(), [](const Overflow& x, const Overflow& y) { return x.read < y.read; });
     }
+    H.mark("tail");
+    H.print(caps ? "retry-batch" : "batch", n);
     return ovf;
 }
 
-static const int64_t BATCH_BASES = (int64_t)1 << 30;
-static const int32_t BATCH_READS = 65536;
+// Batch limits: device-resident reads in few large batches; host reads in
+// smaller ones so that copying batch b+1 overlaps mapping batch b.
+static const int64_t DEV_BATCH_BASES = (int64_t)1 << 31;
+static const int32_t DEV_BATCH_READS = 1 << 17;
+static const int64_t HOST_BATCH_BASES = (int64_t)1 << 29;
+static const int32_t HOST_BATCH_READS = 1 << 15;
 
 __global__ void k_scatter_records(const shm_map_record* __restrict__ src, const int32_t* __restrict__ idx, int32_t n,
                                   shm_map_record* __restrict__ dst) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[idx[i]] = src[i];
 }
 
-// Reads that beat a capacity estimate are mapped again, together, with exact
-// bounds. `bytes_of(i)` returns the host or device address of read i; the
-// reads are gathered into one staging buffer first.
+// Reads that beat their k-mer capacity estimate are mapped again, together,
+// with their counts as capacities. `copy_read(dst, g)` copies read g's bytes
+// (host or device) into the staging buffer.
 template <class CopyFn>
-static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params& p, const std::vector<int32_t>& ovf,
+static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params& p, const std::vector<Overflow>& ovf,
                             const int64_t* offs, CopyFn copy_read, shm_map_record* d_out) {
     if (ovf.empty()) return;
     cudaStream_t s = c->stream;
+    MapScratch& S = *c->scr;
     std::vector<int64_t> o(ovf.size() + 1, 0);
-    for (size_t i = 0; i < ovf.size(); i++) o[i + 1] = o[i] + (offs[ovf[i] + 1] - offs[ovf[i]]);
-    DevBuf<uint8_t> stage;
-    stage.reserve((size_t)o.back() + 32);
-    SHM_CUDA(cudaMemsetAsync(stage.p + o.back(), 0, 32, s));
-    for (size_t i = 0; i < ovf.size(); i++) copy_read(stage.p + o[i], ovf[i]);
-    DevBuf<shm_map_record> tmp;
-    tmp.reserve(ovf.size());
-    std::vector<int32_t> again = run_batch(c, ix, p, stage.p, o.data(), (int32_t)ovf.size(), tmp.p, true);
+    std::vector<uint32_t> caps(ovf.size());
+    for (size_t i = 0; i < ovf.size(); i++) {
+        o[i + 1] = o[i] + (offs[ovf[i].read + 1] - offs[ovf[i].read]);
+        caps[i] = ovf[i].m;
+    }
+    S.retry_seq.reserve((size_t)o.back() + 32);
+    SHM_CUDA(cudaMemsetAsync(S.retry_seq.p + o.back(), 0, 32, s));
+    for (size_t i = 0; i < ovf.size(); i++) copy_read(S.retry_seq.p + o[i], ovf[i].read);
+    S.retry_out.reserve(ovf.size());
+    std::vector<Overflow> again =
+        run_batch(c, ix, p, S.retry_seq.p, o.data(), (int32_t)ovf.size(), S.retry_out.p, caps.data());
     if (!again.empty()) {
-        std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n", ovf[again[0]]);
+        std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n",
+                     ovf[again[0].read].read);
         throw shm_cuda_error(cudaErrorMemoryAllocation);
     }
-    DevBuf<int32_t> di;
-    di.reserve(ovf.size());
-    SHM_CUDA(cudaMemcpyAsync(di.p, ovf.data(), sizeof(int32_t) * ovf.size(), cudaMemcpyHostToDevice, s));
-    k_scatter_records<<<grid_for(ovf.size(), 256), 256, 0, s>>>(tmp.p, di.p, (int32_t)ovf.size(), d_out);
+    // the slot list goes up through the pinned staging (free again: run_batch has synchronized)
+    int32_t* h_idx = (int32_t*)pinned_stage(c, sizeof(int32_t) * ovf.size());
+    for (size_t i = 0; i < ovf.size(); i++) h_idx[i] = ovf[i].read;
+    S.retry_idx.reserve(ovf.size());
+    SHM_CUDA(cudaMemcpyAsync(S.retry_idx.p, h_idx, sizeof(int32_t) * ovf.size(), cudaMemcpyHostToDevice, s));
+    k_scatter_records<<<grid_for(ovf.size(), 256), 256, 0, s>>>(S.retry_out.p, S.retry_idx.p, (int32_t)ovf.size(),
+                                                                d_out);
     SHM_CUDA(cudaGetLastError());
     count_launch();
     SHM_CUDA(cudaStreamSynchronize(s));
 }
 
-void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
-                int32_t n, shm_map_record* d_out, bool plain) {
-    SHM_CUDA(cudaSetDevice(c->device));
-    MapScratch& S = *c->scr;
-    std::vector<int32_t> ovf_all;
+// Batches of at most max_reads reads and max_bases bases (one read at a time
+// in the plain form).
+static std::vector<std::pair<int32_t, int32_t>> cut_batches(const int64_t* offs, int32_t n, bool plain,
+                                                            int32_t max_reads, int64_t max_bases) {
+    std::vector<std::pair<int32_t, int32_t>> b;
     int32_t i = 0;
     while (i < n) {
         int32_t j = i + 1;
         if (!plain)
-            while (j < n && j - i < BATCH_READS && h_offs[j + 1] - h_offs[i] <= BATCH_BASES) j++;
-        const uint8_t* dseq = d_seq + (h_offs[i] - h_offs[0]);
-        std::vector<int32_t> ovf;
-        if (((uintptr_t)dseq & 15) == 0) {
-            ovf = run_batch(c, ix, p, dseq, h_offs + i, j - i, d_out + i, false);
-        } else {  // the batch's first read must start on a 16-byte boundary for the vector loads
-            const int64_t nb = h_offs[j] - h_offs[i];
-            S.seq.reserve((size_t)nb + 32);
-            SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
-            SHM_CUDA(cudaMemcpyAsync(S.seq.p, dseq, (size_t)nb, cudaMemcpyDeviceToDevice, c->stream));
-            ovf = run_batch(c, ix, p, S.seq.p, h_offs + i, j - i, d_out + i, false);
-        }
-        for (int32_t r : ovf) ovf_all.push_back(i + r);
+            while (j < n && j - i < max_reads && offs[j + 1] - offs[i] <= max_bases) j++;
+        b.emplace_back(i, j);
         i = j;
     }
+    return b;
+}
+
+void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
+                int32_t n, shm_map_record* d_out, bool plain) {
+    SHM_CUDA(cudaSetDevice(c->device));
+    std::vector<Overflow> ovf_all;
+    for (auto [i, j] : cut_batches(h_offs, n, plain, DEV_BATCH_READS, DEV_BATCH_BASES)) {
+        // the sketch reads exactly the batch's bytes, at any alignment
+        const uint8_t* dseq = d_seq + (h_offs[i] - h_offs[0]);
+        for (const Overflow& o : run_batch(c, ix, p, dseq, h_offs + i, j - i, d_out + i, nullptr))
+            ovf_all.push_back(Overflow{i + o.read, o.m});
+    }
+    HostClock H;
     retry_overflows(c, ix, p, ovf_all, h_offs, [&](uint8_t* dst, int32_t g) {
         SHM_CUDA(cudaMemcpyAsync(dst, d_seq + (h_offs[g] - h_offs[0]), (size_t)(h_offs[g + 1] - h_offs[g]),
                                  cudaMemcpyDeviceToDevice, c->stream));
     }, d_out);
     SHM_CUDA(cudaStreamSynchronize(c->stream));
+    H.mark("retry");
+    H.print("retries", (int32_t)ovf_all.size());
 }
 
+// Host-buffer form. Batch b+1's bytes go up on the copy stream while batch b
+// is mapped (two device buffers), so the transfer of the reads overlaps the
+// mapping when `seqs` is pinned; records come back batch by batch.
 void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
               int32_t n, shm_map_record* out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
     MapScratch& S = *c->scr;
-    std::vector<int32_t> ovf_all;
-    int32_t i = 0;
-    while (i < n) {
-        int32_t j = i + 1;
-        if (!plain)
-            while (j < n && j - i < BATCH_READS && offs[j + 1] - offs[i] <= BATCH_BASES) j++;
-        const int64_t nb = offs[j] - offs[i];
-        S.seq.reserve((size_t)nb + 32);
-        S.out.reserve((size_t)(j - i));
-        SHM_CUDA(cudaMemsetAsync(S.seq.p + nb, 0, 32, c->stream));
-        SHM_CUDA(cudaMemcpyAsync(S.seq.p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, c->stream));
-        std::vector<int32_t> ovf = run_batch(c, ix, p, S.seq.p, offs + i, j - i, S.out.p, false);
-        SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
-                                 c->stream));
-        SHM_CUDA(cudaStreamSynchronize(c->stream));
-        for (int32_t r : ovf) ovf_all.push_back(i + r);
-        i = j;
+    cudaStream_t s = c->stream;
+    const auto batches = cut_batches(offs, n, plain, HOST_BATCH_READS, HOST_BATCH_BASES);
+    int64_t max_nb = 0;
+    int32_t max_n = 0;
+    for (auto [i, j] : batches) {
+        max_nb = std::max<int64_t>(max_nb, offs[j] - offs[i]);
+        max_n = std::max(max_n, j - i);
     }
+    S.seqb[0].reserve((size_t)max_nb + 32);
+    S.seqb[1].reserve((size_t)max_nb + 32);
+    S.out.reserve((size_t)std::max(max_n, 1));
+    auto send = [&](size_t b) {  // on the copy stream
+        const auto [i, j] = batches[b];
+        const int64_t nb = offs[j] - offs[i];
+        DevBuf<uint8_t>& buf = S.seqb[b & 1];
+        SHM_CUDA(cudaMemsetAsync(buf.p + nb, 0, 32, c->copy_stream));
+        SHM_CUDA(cudaMemcpyAsync(buf.p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, c->copy_stream));
+        SHM_CUDA(cudaEventRecord(c->copied[b & 1], c->copy_stream));
+    };
+    std::vector<Overflow> ovf_all;
+    HostClock H;
+    if (!batches.empty()) send(0);
+    H.mark("send0");
+    for (size_t b = 0; b < batches.size(); b++) {
+        const auto [i, j] = batches[b];
+        SHM_CUDA(cudaStreamWaitEvent(s, c->copied[b & 1], 0));
+        // the other buffer's last reader (batch b-1) has finished: run_batch synchronizes
+        if (b + 1 < batches.size()) send(b + 1);
+        H.mark("send");
+        for (const Overflow& o : run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr))
+            ovf_all.push_back(Overflow{i + o.read, o.m});
+        H.mark("run");
+        SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
+                                 s));
+    }
+    SHM_CUDA(cudaStreamSynchronize(s));
+    H.mark("sync");
     if (!ovf_all.empty()) {
-        DevBuf<shm_map_record> all;
+        DevBuf<shm_map_record>& all = S.retry_all;
         all.reserve((size_t)n);
         // only the retried slots are read back: write them through a device copy of their records
         retry_overflows(c, ix, p, ovf_all, offs, [&](uint8_t* dst, int32_t g) {
-            SHM_CUDA(cudaMemcpyAsync(dst, seqs + offs[g], (size_t)(offs[g + 1] - offs[g]), cudaMemcpyHostToDevice,
-                                     c->stream));
+            SHM_CUDA(cudaMemcpyAsync(dst, seqs + offs[g], (size_t)(offs[g + 1] - offs[g]), cudaMemcpyHostToDevice, s));
         }, all.p);
-        for (int32_t g : ovf_all)
-            SHM_CUDA(cudaMemcpyAsync(out + g, all.p + g, sizeof(shm_map_record), cudaMemcpyDeviceToHost, c->stream));
-        SHM_CUDA(cudaStreamSynchronize(c->stream));
+        for (const Overflow& o : ovf_all)
+            SHM_CUDA(cudaMemcpyAsync(out + o.read, all.p + o.read, sizeof(shm_map_record), cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaStreamSynchronize(s));
     }
+    H.mark("retry");
+    H.print("host-form", n);
 }
 
 }  // namespace shm

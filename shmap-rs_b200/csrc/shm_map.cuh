@@ -43,12 +43,17 @@ extern const char* const WORK_NAMES[N_WORK];
 struct MapCtx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // host-to-device copies of the next batch
+    cudaEvent_t copied[2] = {nullptr, nullptr};
+    cudaStream_t side_stream = nullptr;  // seed preparation of the few reads with large sketches
+    cudaEvent_t fork = nullptr, join = nullptr;
     MapScratch* scr = nullptr;
     size_t hbm_budget = 0;
     int64_t launches = 0;
-    // host staging
+    // host staging (pinned): the plan of the batch in flight, small readbacks
     uint8_t* h_pinned = nullptr;
     size_t h_pinned_cap = 0;
+    void* h_reads = nullptr;
     // work counters (always on): see WORK_NAMES
     int64_t work[16] = {};
     int seed_smem_set = 0;   // dynamic shared memory the seed kernels have been allowed so far

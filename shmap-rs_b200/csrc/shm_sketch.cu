@@ -66,82 +66,176 @@ __device__ __forceinline__ void emit_kmer(const SketchArgs& a, int32_t q, uint64
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(256) k_sketch(SketchArgs a, const SketchLuts* __restrict__ luts) {
-    __shared__ SketchLuts L;
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        L.fw[i] = luts->fw[i];
-        L.rc[i] = luts->rc[i];
-        L.fw_k[i] = luts->fw_k[i];
-        L.rc_r1[i] = luts->rc_r1[i];
-        L.rc_k1[i] = luts->rc_k1[i];
+// Lookup tables as the rolling step reads them: the entering base's pair
+// {fw, rc rotated left by k-1} and the leaving base's pair {fw rotated left
+// by k, rc rotated right by 1}, one 16-byte shared load each.
+struct LutPair {
+    uint64_t a, b;
+};
+
+constexpr int SK_THREADS = 256;                                  // one run of SKETCH_WIN windows per thread
+constexpr int SK_TILE_CAP = SK_THREADS * SKETCH_WIN + 1024;       // bytes a CTA stages per tile
+constexpr int SK_TILE_WORDS = SK_TILE_CAP / 4 + 8;                // + slack for the word past the last byte
+constexpr int SK_TILE_PWORDS = SK_TILE_WORDS + SK_TILE_WORDS / 32 + 1;
+
+// Staged bytes carry one pad word after every 32 words: the runs of
+// neighbouring threads start SKETCH_WIN bytes apart, so without the pad every
+// lane of a warp would read the same bank.
+__device__ __forceinline__ int pword(int w) { return w + (w >> 5); }
+
+template <bool STAGED>
+__device__ __forceinline__ uint32_t fetch_word(const uint32_t* tile, const uint8_t* base, int64_t w, int64_t first,
+                                               int64_t lim) {
+    if (STAGED) return tile[pword((int)w)];
+    // unstaged: bytes of `base` outside [first, lim) read as 0
+    uint32_t v = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int64_t x = 4 * w + j;
+        if (x >= first && x < lim) v |= (uint32_t)__ldg(base + x) << (8 * j);
     }
-    __syncthreads();
+    return v;
+}
+
+// Rolls the windows [1, cnt) of one run whose bytes start at word-aligned
+// offset `x` (in bytes) from `base`; window 0 has already been emitted.
+template <int MODE, bool STAGED>
+__device__ __forceinline__ void roll_run(const SketchArgs& a, const LutPair* __restrict__ Lin,
+                                         const LutPair* __restrict__ Lout, const uint32_t* tile, const uint8_t* base,
+                                         int64_t x, int64_t first, int64_t lim, int32_t cnt, int k, uint64_t thr, int32_t q,
+                                         int32_t r0, uint64_t out_base, uint32_t out_cap, uint32_t& n_sel,
+                                         uint64_t fw, uint64_t rc) {
+    // window t takes base x+t+k-1 in and drops base x+t-1
+    const int64_t xi = x + k, xo = x;
+    const uint32_t shi = (uint32_t)(xi & 3) * 8, sho = (uint32_t)(xo & 3) * 8;
+    int64_t wi = xi >> 2, wo = xo >> 2;
+    uint32_t li = fetch_word<STAGED>(tile, base, wi, first, lim),
+             lo_ = fetch_word<STAGED>(tile, base, wo, first, lim);
+    int32_t t = 1;
+    auto step = [&](uint32_t ib, uint32_t ob, int32_t tt) {
+        const LutPair pi = Lin[ib], po = Lout[ob];
+        fw = rotl1(fw) ^ po.a ^ pi.a;
+        rc = rotr1(rc) ^ po.b ^ pi.b;
+        const uint64_t h = fw ^ rc;
+        if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)(r0 + tt) << 1) | (fw > rc ? 1u : 0u), out_base, out_cap, n_sel);
+    };
+    for (; t + 4 <= cnt; t += 4) {
+        const uint32_t hi_i = fetch_word<STAGED>(tile, base, ++wi, first, lim);
+        const uint32_t hi_o = fetch_word<STAGED>(tile, base, ++wo, first, lim);
+        const uint32_t ib4 = __funnelshift_r(li, hi_i, shi), ob4 = __funnelshift_r(lo_, hi_o, sho);
+        li = hi_i;
+        lo_ = hi_o;
+#pragma unroll
+        for (int j = 0; j < 4; j++) step((ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu, t + j);
+    }
+    if (t < cnt) {
+        const uint32_t hi_i = fetch_word<STAGED>(tile, base, ++wi, first, lim);
+        const uint32_t hi_o = fetch_word<STAGED>(tile, base, ++wo, first, lim);
+        const uint32_t ib4 = __funnelshift_r(li, hi_i, shi), ob4 = __funnelshift_r(lo_, hi_o, sho);
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            if (t + j < cnt) step((ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu, t + j);
+    }
+}
+
+// Each CTA takes tiles of SK_THREADS consecutive runs. Runs are laid out in
+// sequence order, so a tile's bytes are one contiguous range of `seq`: it is
+// staged in shared memory with coalesced 16-byte loads and the runs roll out
+// of shared memory. A tile whose range does not fit (many sequences shorter
+// than k between its runs) rolls from global memory instead.
+template <int MODE>
+__global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const SketchLuts* __restrict__ luts) {
+    __shared__ LutPair Lin[256], Lout[256];
+    __shared__ uint32_t tile[SK_TILE_PWORDS];
+    __shared__ int64_t s_lo, s_hi;
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        Lin[i] = LutPair{luts->fw[i], luts->rc_k1[i]};
+        Lout[i] = LutPair{luts->fw_k[i], luts->rc_r1[i]};
+    }
     const int k = a.k;
     const uint64_t thr = a.thr;
     const uint64_t n_chunks = a.n_chunks;
-    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n_chunks;
-         c += (uint64_t)gridDim.x * blockDim.x) {
-        // sequence of this chunk: upper_bound over chunk_off
-        int32_t lo = 0, hi = a.n_seq;
-        while (hi - lo > 1) {
-            int32_t mid = (lo + hi) >> 1;
-            if (__ldg(a.chunk_off + mid) <= c) lo = mid;
-            else hi = mid;
+    const uint64_t n_tiles = (n_chunks + SK_THREADS - 1) / SK_THREADS;
+    for (uint64_t tl = blockIdx.x; tl < n_tiles; tl += gridDim.x) {
+        const uint64_t c = tl * SK_THREADS + threadIdx.x;
+        const uint64_t c_last = min(tl * SK_THREADS + SK_THREADS, n_chunks) - 1;
+        int32_t q = 0, cnt = 0;
+        int64_t start = 0, w0 = 0;  // byte offset of the run in `seq`, its first window in the sequence
+        if (c < n_chunks) {
+            int32_t lo = 0, hi = a.n_seq;  // upper_bound over chunk_off
+            while (hi - lo > 1) {
+                int32_t mid = (lo + hi) >> 1;
+                if (__ldg(a.chunk_off + mid) <= c) lo = mid;
+                else hi = mid;
+            }
+            q = lo;
+            const int64_t s0 = __ldg(a.seq_off + q), nw = __ldg(a.seq_off + q + 1) - s0 - k + 1;
+            w0 = (int64_t)(c - __ldg(a.chunk_off + q)) * SKETCH_WIN;
+            cnt = (int32_t)(min(w0 + (int64_t)SKETCH_WIN, nw) - w0);
+            start = s0 + w0;
+            if (c == tl * SK_THREADS) s_lo = start;
+            if (c == c_last) s_hi = start + cnt + k - 1;
         }
-        const int32_t q = lo;
-        const int64_t s0 = __ldg(a.seq_off + q), L_ = __ldg(a.seq_off + q + 1) - s0;
-        const int64_t nw = L_ - k + 1;
-        const int64_t w0 = (int64_t)(c - __ldg(a.chunk_off + q)) * SKETCH_WIN;
-        const int32_t cnt = (int32_t)(min(w0 + (int64_t)SKETCH_WIN, nw) - w0);  // windows of this run
-        if (cnt <= 0) continue;
-        uint64_t out_base = 0;
-        uint32_t out_cap = 0;
-        uint32_t n_sel = 0;
-        if (MODE == SK_WRITE) out_base = a.chunk_out[c];
-        if (MODE == SK_APPEND) {
-            out_base = a.kmer_off[q];
-            out_cap = (uint32_t)(a.kmer_off[q + 1] - out_base);
-        }
-        const uint8_t* p = a.seq + (s0 + w0);
-        const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;  // r of the run's first window
-        // first window, by definition (tests/nthash_equivalence.rs:31-61)
-        uint64_t fw = 0, rc = 0;
-        for (int i = 0; i < k; i++) {
-            uint32_t b = __ldg(p + i);
-            fw ^= rotl64(L.fw[b], (uint32_t)(k - 1 - i));
-            rc ^= rotl64(L.rc[b], (uint32_t)i);
-        }
-        {
-            const uint64_t h = fw ^ rc;
-            if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)r0 << 1) | (fw > rc ? 1u : 0u), out_base, out_cap, n_sel);
-        }
-        // rolling: window t takes base p[t + k - 1] in and drops p[t - 1]; both byte
-        // streams are read as aligned 32-bit words realigned by one funnel shift
-        const uintptr_t ai = (uintptr_t)(p + k), ao = (uintptr_t)p;
-        const uint32_t shi = (uint32_t)(ai & 3) * 8, sho = (uint32_t)(ao & 3) * 8;
-        const uint32_t* wi = (const uint32_t*)(ai & ~(uintptr_t)3);
-        const uint32_t* wo = (const uint32_t*)(ao & ~(uintptr_t)3);
-        uint32_t li = __ldg(wi), lo_ = __ldg(wo);
-        for (int32_t t = 1; t < cnt; t += 4) {
-            const uint32_t hi_i = __ldg(++wi), hi_o = __ldg(++wo);
-            const uint32_t ib4 = __funnelshift_r(li, hi_i, shi), ob4 = __funnelshift_r(lo_, hi_o, sho);
-            li = hi_i;
-            lo_ = hi_o;
+        __syncthreads();  // s_lo/s_hi written; the previous tile's readers are done
+        const int64_t lo_b = s_lo, hi_b = s_hi;
+        const uint8_t* A0 = (const uint8_t*)((uintptr_t)(a.seq + lo_b) & ~(uintptr_t)15);
+        const int64_t lim = (int64_t)((a.seq + hi_b) - A0);  // staged bytes are [A0 + (lo - A0), A0 + lim)
+        const int64_t first = (int64_t)((a.seq + lo_b) - A0);
+        const bool staged = lim <= (int64_t)SK_TILE_CAP;
+        if (staged) {
+            const int nv = (int)((lim + 15) >> 4);
+            for (int v = threadIdx.x; v < nv; v += SK_THREADS) {
+                uint32_t wv[4];
+                if (16 * v >= first && 16 * v + 16 <= lim) {
+                    const uint4 u = __ldg((const uint4*)(A0 + 16 * v));
+                    wv[0] = u.x; wv[1] = u.y; wv[2] = u.z; wv[3] = u.w;
+                } else {
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (t + j < cnt) {
-                    const uint32_t ib = (ib4 >> (8 * j)) & 0xffu, ob = (ob4 >> (8 * j)) & 0xffu;
-                    fw = rotl1(fw) ^ L.fw_k[ob] ^ L.fw[ib];
-                    rc = rotr1(rc) ^ L.rc_r1[ob] ^ L.rc_k1[ib];
-                    const uint64_t h = fw ^ rc;
-                    if (h <= thr)
-                        emit_kmer<MODE>(a, q, h, ((uint32_t)(r0 + t + j) << 1) | (fw > rc ? 1u : 0u), out_base,
-                                        out_cap, n_sel);
+                    for (int m = 0; m < 4; m++) {
+                        uint32_t w = 0;
+                        for (int j = 0; j < 4; j++) {
+                            const int64_t xx = 16 * v + 4 * m + j;
+                            if (xx >= first && xx < lim) w |= (uint32_t)__ldg(A0 + xx) << (8 * j);
+                        }
+                        wv[m] = w;
+                    }
                 }
+#pragma unroll
+                for (int m = 0; m < 4; m++) tile[pword(4 * v + m)] = wv[m];
             }
         }
-        if (MODE == SK_COUNT) a.chunk_cnt[c] = n_sel;
+        __syncthreads();
+        if (cnt > 0) {
+            uint64_t out_base = 0;
+            uint32_t out_cap = 0, n_sel = 0;
+            if (MODE == SK_WRITE) out_base = a.chunk_out[c];
+            if (MODE == SK_APPEND) {
+                out_base = a.kmer_off[q];
+                out_cap = (uint32_t)(a.kmer_off[q + 1] - out_base);
+            }
+            const int64_t x = (int64_t)((a.seq + start) - A0);  // run's first byte relative to A0
+            const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;  // r of the run's first window
+            // first window, by definition (tests/nthash_equivalence.rs:31-61);
+            // rc(b) rotated left by i is rc_r1(b) rotated left by i + 1
+            uint64_t fw = 0, rc = 0;
+            for (int i = 0; i < k; i++) {
+                const int64_t xx = x + i;
+                const uint32_t b = staged ? (tile[pword((int)(xx >> 2))] >> (8 * (xx & 3))) & 0xffu : __ldg(A0 + xx);
+                fw ^= rotl64(Lin[b].a, (uint32_t)(k - 1 - i));
+                rc ^= rotl64(Lout[b].b, (uint32_t)(i + 1));
+            }
+            const uint64_t h = fw ^ rc;
+            if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)r0 << 1) | (fw > rc ? 1u : 0u), out_base, out_cap, n_sel);
+            if (staged)
+                roll_run<MODE, true>(a, Lin, Lout, tile, A0, x, first, lim, cnt, k, thr, q, r0, out_base, out_cap, n_sel, fw, rc);
+            else
+                roll_run<MODE, false>(a, Lin, Lout, tile, A0, x, first, lim, cnt, k, thr, q, r0, out_base, out_cap, n_sel, fw,
+                                      rc);
+            if (MODE == SK_COUNT) a.chunk_cnt[c] = n_sel;
+        } else if (MODE == SK_COUNT && c < n_chunks) {
+            a.chunk_cnt[c] = 0;
+        }
+        __syncthreads();  // the tile is free for the next one
     }
 }
 
@@ -157,10 +251,11 @@ SketchLuts* create_device_luts(int32_t k, cudaStream_t s) {
 
 void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStream_t s) {
     if (a.n_chunks == 0) return;
-    int grid = grid_for(a.n_chunks, 256, 8);
-    if (mode == SK_COUNT) k_sketch<SK_COUNT><<<grid, 256, 0, s>>>(a, L);
-    else if (mode == SK_WRITE) k_sketch<SK_WRITE><<<grid, 256, 0, s>>>(a, L);
-    else k_sketch<SK_APPEND><<<grid, 256, 0, s>>>(a, L);
+    const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
+    const int grid = grid_for(n_tiles, 1, 5);  // tiles, at most 5 resident CTAs per SM
+    if (mode == SK_COUNT) k_sketch<SK_COUNT><<<grid, SK_THREADS, 0, s>>>(a, L);
+    else if (mode == SK_WRITE) k_sketch<SK_WRITE><<<grid, SK_THREADS, 0, s>>>(a, L);
+    else k_sketch<SK_APPEND><<<grid, SK_THREADS, 0, s>>>(a, L);
     SHM_CUDA(cudaGetLastError());
     count_launch();
 }
