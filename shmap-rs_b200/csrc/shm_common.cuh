@@ -69,6 +69,9 @@ struct DevParams {
     double theta_low;  // fl(theta * fl(1 - min_diff)): lowest threshold either sweep can use
     int32_t metric;    // 0 Containment, 1 Jaccard, 2 bucket_SH
     int32_t nbp, os, ap;
+    // slot_mul[b] = min(2^64 - 1, floor(2^(64+b) / (thr + 1))): __umul64hi(h, slot_mul[b])
+    // maps h <= thr monotonically onto [0, 2^b)
+    uint64_t slot_mul[16];
 };
 
 __device__ __forceinline__ uint64_t rotl64(uint64_t x, uint32_t n) {

@@ -870,6 +870,249 @@ __global__ void k_seed_bins(BatchView v, int32_t* __restrict__ lists, uint32_t* 
     }
 }
 
+// ------------------------------------------------------------------ K2 counting form
+// Seed preparation with one warp per read and work linear in m: the k-mers
+// are bucketed by a counting sort on h -> h * Ht / (thr + 1) (order
+// preserving, about one k-mer per bucket for Ht >= m), each bucket is put in
+// hash order by insertion, equal hashes are grouped in place, and the groups
+// are put rarest first by a stable least-significant-digit radix sort on
+// their hit counts, which keeps hash order among equal counts: the order of
+// src/shmap/seeding.rs:28-71. Shared memory per warp, for capacity C:
+//   Sh (8C), Srs (4C): the bucketed k-mers, then the groups in place (hash,
+//                      then occs << 1 | strand of the smallest r)
+//   Rc (4C): bucket offsets, then each group's count() hit count
+//   Ra (4C): each group's hit-list start
+//   P0, P1 (4C each): radix permutations; RH (256 words): digit offsets
+__host__ __device__ constexpr size_t seedc_bytes(uint32_t C) { return 28 * (size_t)C + 1024; }
+
+// Exclusive scan, in place, of the n (a multiple of 32) words X[0..n): lane l
+// owns n/32 consecutive words.
+__device__ __forceinline__ void warp_scan_words(uint32_t* X, uint32_t n, int lane) {
+    const uint32_t per = n >> 5, b0 = (uint32_t)lane * per;
+    uint32_t sum = 0;
+    for (uint32_t j = 0; j < per; j++) sum += X[b0 + j];
+    uint32_t run = warp_inclusive_scan(sum) - sum;
+    for (uint32_t j = 0; j < per; j++) {
+        const uint32_t c = X[b0 + j];
+        X[b0 + j] = run;
+        run += c;
+    }
+}
+
+__device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_t* base) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u, le = lt | (1u << lane);
+    uint32_t m;
+    uint64_t kb;
+    int32_t S, halflen;
+    if (!seed_prologue(v, q, C, lane == 0, m, kb, S, halflen)) return;
+    uint64_t* Sh = (uint64_t*)base;
+    uint32_t* Srs = (uint32_t*)(Sh + C);
+    uint32_t* Rc = Srs + C;
+    uint32_t* Ra = Rc + C;
+    uint32_t* P0 = Ra + C;
+    uint32_t* P1 = P0 + C;
+    uint32_t* RH = P1 + C;
+
+    // counting sort by bucket: Ht = power of two in [32, C], >= m
+    const uint32_t Ht = max((uint32_t)32, (uint32_t)pow2_ceil(m));
+    const uint64_t mul = v.P.slot_mul[31 - __clz(Ht)];
+    for (uint32_t i = lane; i < Ht; i += 32) Rc[i] = 0;
+    __syncwarp();
+    for (uint32_t i = lane; i < m; i += 32) atomicAdd(&Rc[(uint32_t)__umul64hi(v.km_h[kb + i], mul)], 1u);
+    __syncwarp();
+    warp_scan_words(Rc, Ht, lane);
+    __syncwarp();
+    for (uint32_t i = lane; i < m; i += 32) {
+        const uint64_t h = v.km_h[kb + i];
+        const uint32_t pos = atomicAdd(&Rc[(uint32_t)__umul64hi(h, mul)], 1u);
+        Sh[pos] = h;
+        Srs[pos] = v.km_rs[kb + i];
+    }
+    __syncwarp();
+    // bucket b now spans [Rc[b-1], Rc[b]); insertion by hash (equal hashes stay put)
+    {
+        const uint32_t per = Ht >> 5, b0 = (uint32_t)lane * per;
+        uint32_t s0 = b0 ? Rc[b0 - 1] : 0u;
+        for (uint32_t j = 0; j < per; j++) {
+            const uint32_t e1 = Rc[b0 + j];
+            for (uint32_t x = s0 + 1; x < e1; x++) {
+                const uint64_t hx = Sh[x];
+                const uint32_t rx = Srs[x];
+                uint32_t y = x;
+                while (y > s0 && Sh[y - 1] > hx) {
+                    Sh[y] = Sh[y - 1];
+                    Srs[y] = Srs[y - 1];
+                    y--;
+                }
+                Sh[y] = hx;
+                Srs[y] = rx;
+            }
+            s0 = e1;
+        }
+    }
+    __syncwarp();
+
+    // groups of equal hashes, compacted in place (src/shmap/seeding.rs:45-67);
+    // Srs[g] keeps the group's smallest r << 1 | strand until its last element
+    // writes occs << 1 | that strand (the representative: seeding.rs:56)
+    uint32_t n_u = 0, open_start = 0;
+    uint64_t carry_h = 0;
+    for (uint32_t c0 = 0; c0 < m; c0 += 32) {
+        const uint32_t e = c0 + lane;
+        const bool valid = e < m;
+        const uint64_t h = valid ? Sh[e] : 0;
+        const uint32_t rs = valid ? Srs[e] : 0;
+        const uint64_t hn = (e + 1 < m) ? Sh[e + 1] : 0;
+        uint64_t hp = __shfl_up_sync(0xffffffffu, h, 1);
+        if (lane == 0) hp = carry_h;
+        const bool first = valid && (e == 0 || h != hp);
+        const bool last = valid && (e + 1 == m || hn != h);
+        const unsigned fmask = __ballot_sync(0xffffffffu, first);
+        const unsigned fle = fmask & le;
+        const uint32_t gid = n_u + __popc(fle) - 1;
+        const uint32_t start = fle ? (c0 + 31 - __clz(fle)) : open_start;
+        __syncwarp();  // this chunk is read before anything is written at gid <= e
+        if (first) {
+            Sh[gid] = h;
+            Srs[gid] = rs;
+        }
+        __syncwarp();
+        if (valid && !first) atomicMin(&Srs[gid], rs);
+        __syncwarp();
+        if (last) Srs[gid] = ((e - start + 1) << 1) | (Srs[gid] & 1u);
+        n_u += __popc(fmask);
+        open_start = __shfl_sync(0xffffffffu, start, 31);
+        carry_h = __shfl_sync(0xffffffffu, h, 31);
+        __syncwarp();
+    }
+    if (v.P.os) S = (int32_t)n_u;  // mod.rs:732-736
+
+    // count() probes (index.rs:204-213)
+    uint32_t maxc = 0;
+    for (uint32_t g = lane; g < n_u; g += 32) {
+        uint32_t a, cnt;
+        idx_lookup(v.I, Sh[g], a, cnt);
+        Rc[g] = cnt;
+        Ra[g] = a;
+        maxc = max(maxc, cnt);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
+    __syncwarp();
+
+    // rarest first, stable over hash order (seeding.rs:71): LSD radix on the
+    // count, 8 bits a pass, as many passes as the largest count needs
+    const uint32_t* ord = nullptr;  // null: identity
+    uint32_t* pout = P0;
+    for (int sh = 0; sh < 32 && (maxc >> sh) != 0; sh += 8) {
+        for (uint32_t i = lane; i < 256; i += 32) RH[i] = 0;
+        __syncwarp();
+        for (uint32_t i = lane; i < n_u; i += 32) {
+            const uint32_t g = ord ? ord[i] : i;
+            atomicAdd(&RH[(Rc[g] >> sh) & 255u], 1u);
+        }
+        __syncwarp();
+        warp_scan_words(RH, 256, lane);
+        __syncwarp();
+        for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
+            const uint32_t i = c0 + lane;
+            const bool valid = i < n_u;
+            const uint32_t g = valid ? (ord ? ord[i] : i) : 0u;
+            const uint32_t d = valid ? (Rc[g] >> sh) & 255u : 256u + (uint32_t)lane;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const int leader = __ffs(peers) - 1;
+            uint32_t at = (valid && lane == leader) ? RH[d] : 0u;
+            at = __shfl_sync(0xffffffffu, at, leader);
+            if (valid) pout[at + __popc(peers & lt)] = g;
+            __syncwarp();
+            if (valid && lane == leader) RH[d] = at + __popc(peers);
+            __syncwarp();
+        }
+        ord = pout;
+        pout = pout == P0 ? P1 : P0;
+    }
+
+    // seeding prefix: seed i is processed iff sum(occs before i) < S (seeding.rs:101)
+    uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
+    uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
+    for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
+        const uint32_t i = c0 + lane;
+        const bool valid = i < n_u;
+        const uint32_t g = valid ? (ord ? ord[i] : i) : 0u;
+        const uint32_t cnt = valid ? Rc[g] : 0u;
+        const uint32_t os = valid ? Srs[g] : 0u, occs = os >> 1;
+        const uint32_t oi = warp_inclusive_scan(occs);
+        const uint64_t ci = warp_inclusive_scan((uint64_t)cnt);
+        const uint32_t po = po_carry + oi - occs;
+        const uint64_t pc = pc_carry + ci - cnt;
+        if (valid) {
+            const uint64_t hg = Sh[g];
+            const uint32_t a = Ra[g];
+            v.sd_h[kb + i] = hg;
+            v.sd_os[kb + i] = os;
+            v.sd_cnt[kb + i] = cnt;
+            v.sd_a[kb + i] = a;
+            v.sd_ooff[kb + i] = po;
+            if ((int64_t)po < (int64_t)S) {
+                v.sd_hpre[kb + i] = (uint32_t)pc;
+                l_np++;
+                l_s0 += occs;
+                l_sm += cnt;
+                l_max = max(l_max, cnt);
+                l_eb += seed_bucket_bound(v, a, cnt, halflen);
+            }
+            pht_insert(v, q, hg, i);
+        }
+        po_carry += __shfl_sync(0xffffffffu, oi, 31);
+        pc_carry += __shfl_sync(0xffffffffu, ci, 31);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l_np += __shfl_xor_sync(0xffffffffu, l_np, o);
+        l_s0 += __shfl_xor_sync(0xffffffffu, l_s0, o);
+        l_sm += __shfl_xor_sync(0xffffffffu, l_sm, o);
+        l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
+        l_max = max(l_max, __shfl_xor_sync(0xffffffffu, l_max, o));
+    }
+    if (lane == 0) {
+        v.r_status[q] = ST_UNMAPPED;
+        v.r_nu[q] = (int32_t)n_u;
+        v.r_nproc[q] = (int32_t)l_np;
+        v.r_S[q] = S;
+        v.r_S0[q] = (int32_t)l_s0;
+        v.r_smatch[q] = (int64_t)l_sm;
+        v.r_maxseed[q] = (int32_t)l_max;
+        v.r_half[q] = halflen;
+        if (l_sm >= 0xffffffffULL) {
+            v.r_status[q] = ST_OVERFLOW;
+        } else {
+            v.hw[q] = l_sm;
+            v.bt_size[q] = l_sm ? max((uint64_t)16, pow2_ceil(2 * l_eb)) : 0;
+        }
+        atomicMax(&v.mx->m_max, m);
+        atomicMax(&v.mx->nu_max, n_u);
+        atomicMax(&v.mx->half_max, (uint32_t)halflen);
+        atomicAdd(&v.mx->kmers, (unsigned long long)m);
+        atomicAdd(&v.mx->distinct, (unsigned long long)n_u);
+        atomicAdd(&v.mx->proc_seeds, (unsigned long long)l_np);
+        atomicAdd(&v.mx->hits, (unsigned long long)l_sm);
+    }
+}
+
+template <uint32_t C, int W>
+__global__ void __launch_bounds__(W * 32) k_seedprep_c(BatchView v, const int32_t* __restrict__ list,
+                                                       const uint32_t* __restrict__ n_list) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int wib = threadIdx.x >> 5;
+    uint8_t* base = smem + (size_t)wib * seedc_bytes(C);
+    const int32_t n = (int32_t)*n_list;
+    for (int32_t li = blockIdx.x * W + wib; li < n; li += gridDim.x * W) {
+        seedprep_count(v, list[li], C, base);
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------------ K3 contributions
 __device__ __forceinline__ int64_t hit_pos(const DevIndex& I, uint32_t g, int32_t seg, bool ap) {
     return ap ? (int64_t)(__ldg(I.ref_rs + g) >> 1) : (int64_t)(g - __ldg(I.seg_off + seg));
@@ -1630,7 +1873,6 @@ MapCtx* mapctx_create(int device, size_t hbm_budget) {
     SHM_CUDA(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
     for (auto& e : c->copied) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     c->scr = new MapScratch();
-    SHM_CUDA(cudaHostAlloc(&c->h_reads, sizeof(HostReads), cudaHostAllocDefault));
     return c;
 }
 
@@ -1643,7 +1885,7 @@ void mapctx_destroy(MapCtx* c) {
         delete c->scr;
     }
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
-    if (c->h_reads) cudaFreeHost(c->h_reads);
+    if (c->h_slots) cudaFreeHost(c->h_slots);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (auto& e : c->copied)
         if (e) cudaEventDestroy(e);
@@ -1744,14 +1986,76 @@ struct Overflow {
     uint32_t m;
 };
 
-// Maps one batch whose bytes are already on the device at d_seq (relative
-// offsets h_offs[i] - h_offs[0]); caps as for plan_batch. Returns the reads
-// that overflowed a capacity (retried by the caller with their counts).
-static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
-                                       const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps) {
+// Where a batch's results land on the host (pinned): the small reads, then
+// its overflow list (up to n pairs read, m).
+struct BatchSlot {
+    HostReads* R;
+    uint32_t* ovf;
+    int32_t i0, n;
+    int64_t bases;
+};
+
+// Pinned per-call result slots for batches of the given sizes.
+static std::vector<BatchSlot> batch_slots(MapCtx* c, const std::vector<std::pair<int32_t, int32_t>>& b,
+                                          const int64_t* offs) {
+    size_t bytes = 0;
+    for (auto [i, j] : b) bytes += (sizeof(HostReads) + 63) / 64 * 64 + (8 * (size_t)(j - i) + 63) / 64 * 64;
+    if (bytes > c->h_slots_cap) {
+        if (c->h_slots) SHM_CUDA(cudaFreeHost(c->h_slots));
+        c->h_slots = nullptr;
+        c->h_slots_cap = 0;
+        const size_t want = std::max<size_t>(bytes + bytes / 4, (size_t)1 << 16);
+        SHM_CUDA(cudaHostAlloc(&c->h_slots, want, cudaHostAllocDefault));
+        c->h_slots_cap = want;
+    }
+    std::vector<BatchSlot> out;
+    uint8_t* at = (uint8_t*)c->h_slots;
+    for (auto [i, j] : b) {
+        BatchSlot sl;
+        sl.R = (HostReads*)at;
+        at += (sizeof(HostReads) + 63) / 64 * 64;
+        sl.ovf = (uint32_t*)at;
+        at += (8 * (size_t)(j - i) + 63) / 64 * 64;
+        sl.i0 = i;
+        sl.n = j - i;
+        sl.bases = offs[j] - offs[i];
+        out.push_back(sl);
+    }
+    return out;
+}
+
+// After the stream has drained: a batch's work counters and its overflowed
+// reads (indices offset by the batch's first read), appended to `ovf`.
+static void collect_batch(MapCtx* c, const BatchSlot& sl, std::vector<Overflow>& ovf) {
+    const HostReads& R = *sl.R;
+    const BatchMax& fin = R.fin;
+    c->work[W_READS] += sl.n;
+    c->work[W_BASES] += sl.bases;
+    c->work[W_KMERS] += (int64_t)fin.kmers;
+    c->work[W_DISTINCT] += (int64_t)fin.distinct;
+    c->work[W_PROC_SEEDS] += (int64_t)fin.proc_seeds;
+    c->work[W_HITS] += (int64_t)fin.hits;
+    c->work[W_BUCKETS] += (int64_t)fin.buckets;
+    c->work[W_JOBS] += R.nj;
+    c->work[W_EXT_SEEDS] += (int64_t)fin.ext_seeds;
+    c->work[W_CANDS] += R.nc;
+    c->work[W_REFINE_KMERS] += (int64_t)fin.refine_kmers;
+    const size_t at = ovf.size();
+    for (uint32_t i = 0; i < fin.n_overflow && i < (uint32_t)sl.n; i++)
+        ovf.push_back(Overflow{sl.i0 + (int32_t)sl.ovf[2 * i], sl.ovf[2 * i + 1]});
+    std::sort(ovf.begin() + at, ovf.end(), [](const Overflow& x, const Overflow& y) { return x.read < y.read; });
+}
+
+// Enqueues the mapping of one batch whose bytes are already on the device at
+// d_seq (relative offsets h_offs[i] - h_offs[0]); caps as for plan_batch.
+// The host waits once, for the sizes of the bucket tables; everything after
+// is queued, and the batch's results reach `sl` when the stream drains
+// (collect_batch then lists the reads that overflowed a capacity).
+static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
+                      const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps, StageTimer& T,
+                      const BatchSlot& sl) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
-    StageTimer T(c);
     HostClock H;
     BatchPlan bp;
     plan_batch(c, h_offs, n, p.k, p.h_frac, caps, bp);
@@ -1817,6 +2121,12 @@ static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const 
     v.P.nbp = p.no_bucket_pruning;
     v.P.os = p.one_sweep;
     v.P.ap = p.abs_pos;
+    for (int b = 0; b < 16; b++) {
+        const unsigned __int128 num = (unsigned __int128)1 << (64 + b);
+        const unsigned __int128 den = (unsigned __int128)ix->dev.thr + 1;
+        const unsigned __int128 q128 = num / den;
+        v.P.slot_mul[b] = q128 > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)q128;
+    }
     v.theta2 = p.theta - p.min_diff;
     v.seq = d_seq;
     v.roff = dp.roff;
@@ -1913,26 +2223,27 @@ static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const 
         SHM_CUDA(cudaGetLastError());
         count_launch();
     }
-    if (bp.n_cap_512) {  // 512 < m <= 1024: warp per read, shared arrays
-        const uint32_t P = 1024;
-        const int wpb = 4;
-        const size_t bytes = SEEDW_BYTES_PER_ELEM * P * (size_t)wpb;
-        if ((int)bytes > c->seedw_smem_set) {
-            SHM_CUDA(cudaFuncSetAttribute(k_seedprep_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-            c->seedw_smem_set = (int)bytes;
-        }
-        k_seedprep_w<<<grid_for((size_t)bp.n_cap_512 * 32, wpb * 32, 2048 / (wpb * 32)), wpb * 32, bytes, s2>>>(
-            v, LB + 2 * (size_t)n, NB + 2, P);
+    if (!c->seedc_smem_set) {
+        SHM_CUDA(cudaFuncSetAttribute(k_seedprep_c<256, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(8 * seedc_bytes(256))));
+        SHM_CUDA(cudaFuncSetAttribute(k_seedprep_c<512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(4 * seedc_bytes(512))));
+        SHM_CUDA(cudaFuncSetAttribute(k_seedprep_c<1024, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(4 * seedc_bytes(1024))));
+        c->seedc_smem_set = 1;
+    }
+    if (bp.n_cap_512) {  // 512 < m <= 1024
+        k_seedprep_c<1024, 4><<<grid_for((size_t)bp.n_cap_512 * 32, 128, 1), 128, 4 * seedc_bytes(1024), s2>>>(
+            v, LB + 2 * (size_t)n, NB + 2);
         SHM_CUDA(cudaGetLastError());
         count_launch();
     }
     if (side) SHM_CUDA(cudaEventRecord(c->join, s2));
     {
-        const int wgrid = grid_for((size_t)n * 32, SEEDR_WARPS * 32, 4);
-        k_seedprep_r<8><<<wgrid, SEEDR_WARPS * 32, SEEDR_WARPS * 32 * 8 * 12, s>>>(v, LB, NB);
+        k_seedprep_c<256, 8><<<grid_for((size_t)n * 32, 256, 3), 256, 8 * seedc_bytes(256), s>>>(v, LB, NB);
         SHM_CUDA(cudaGetLastError());
         count_launch();
-        k_seedprep_r<16><<<wgrid, SEEDR_WARPS * 32, SEEDR_WARPS * 32 * 16 * 12, s>>>(v, LB + n, NB + 1);
+        k_seedprep_c<512, 4><<<grid_for((size_t)n * 32, 128, 3), 128, 4 * seedc_bytes(512), s>>>(v, LB + n, NB + 1);
         SHM_CUDA(cudaGetLastError());
         count_launch();
     }
@@ -1941,7 +2252,7 @@ static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const 
 
     exclusive_scan_u64(S.hw.p, S.hw_off.p, (size_t)n, s);
     exclusive_scan_u64(S.bt_size.p, S.bt_off.p, (size_t)n, s);
-    HostReads& R = *(HostReads*)c->h_reads;
+    HostReads& R = *sl.R;
     SHM_CUDA(cudaMemcpyAsync(&R.totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaMemcpyAsync(&R.totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaMemcpyAsync(&R.hm, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
@@ -1988,26 +2299,17 @@ static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const 
         SHM_CUDA(cudaGetLastError());
         T.end();
     }
-    uint32_t job_cap = (uint32_t)std::min<uint64_t>(bt_total + 1, (uint64_t)n * 64 + (1u << 20));
-    for (int attempt = 0;; attempt++) {
-        S.jobs.reserve(job_cap);
-        v.jobs = S.jobs.p;
-        v.job_cap = job_cap;
-        if (bt_total) {
-            T.begin(STG_BSCAN);
-            k_bscan<<<grid_for((size_t)n * 32, 256, 8), 256, 0, s>>>(v);
-            SHM_CUDA(cudaGetLastError());
-            T.end();
-        }
-        SHM_CUDA(cudaMemcpyAsync(&R.nj, S.n_jobs.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        H.mark("enq2");
-        SHM_CUDA(cudaStreamSynchronize(s));
-        H.mark("sync2");
-        const uint32_t nj = R.nj;
-        if (nj <= job_cap) break;
-        job_cap = nj;  // retry with room for every job
-        SHM_CUDA(cudaMemsetAsync(S.n_jobs.p, 0, sizeof(uint32_t), s));
-        SHM_CUDA(cudaMemsetAsync(S.ccnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    // a job per touched bucket-table slot at most: bt_total bounds the jobs
+    if (bt_total + 1 > (uint64_t)UINT32_MAX) throw shm_cuda_error(cudaErrorMemoryAllocation);
+    const uint32_t job_cap = (uint32_t)(bt_total + 1);
+    S.jobs.reserve(job_cap);
+    v.jobs = S.jobs.p;
+    v.job_cap = job_cap;
+    if (bt_total) {
+        T.begin(STG_BSCAN);
+        k_bscan<<<grid_for((size_t)n * 32, 256, 8), 256, 0, s>>>(v);
+        SHM_CUDA(cudaGetLastError());
+        T.end();
     }
     if (!p.no_bucket_pruning) {
         T.begin(STG_EXTEND);
@@ -2045,33 +2347,15 @@ static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const 
     SHM_CUDA(cudaMemcpyAsync(&R.fin, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaMemcpyAsync(&R.nj, S.n_jobs.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaMemcpyAsync(&R.nc, S.coff.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    H.mark("enq3");
-    SHM_CUDA(cudaStreamSynchronize(s));
-    H.mark("sync3");
-    T.collect();
-    const BatchMax fin = R.fin;
-    {
-        const uint32_t nj = R.nj, nc = R.nc;
-        c->work[W_READS] += n;
-        c->work[W_BASES] += h_offs[n] - h_offs[0];
-        c->work[W_KMERS] += (int64_t)fin.kmers;
-        c->work[W_DISTINCT] += (int64_t)fin.distinct;
-        c->work[W_PROC_SEEDS] += (int64_t)fin.proc_seeds;
-        c->work[W_HITS] += (int64_t)fin.hits;
-        c->work[W_BUCKETS] += (int64_t)fin.buckets;
-        c->work[W_JOBS] += nj;
-        c->work[W_EXT_SEEDS] += (int64_t)fin.ext_seeds;
-        c->work[W_CANDS] += nc;
-        c->work[W_REFINE_KMERS] += (int64_t)fin.refine_kmers;
-    }
+    SHM_CUDA(cudaMemcpyAsync(sl.ovf, S.ovf_list.p, 2 * sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    H.mark("enq_rest");
     if (debug) {
-        uint32_t nj = 0, nc = 0;
-        SHM_CUDA(cudaMemcpy(&nj, S.n_jobs.p, sizeof nj, cudaMemcpyDeviceToHost));
-        SHM_CUDA(cudaMemcpy(&nc, S.coff.p + n, sizeof nc, cudaMemcpyDeviceToHost));
-        std::fprintf(stderr, "[shmap] jobs=%u (cap %u) candidates=%u overflow=%u\n", nj, job_cap, nc, fin.n_overflow);
-        if (nj && nj <= 16) {
-            std::vector<BucketJob> jb(nj);
-            SHM_CUDA(cudaMemcpy(jb.data(), S.jobs.p, sizeof(BucketJob) * nj, cudaMemcpyDeviceToHost));
+        SHM_CUDA(cudaStreamSynchronize(s));
+        std::fprintf(stderr, "[shmap] jobs=%u (cap %u) candidates=%u overflow=%u\n", R.nj, job_cap, R.nc,
+                     R.fin.n_overflow);
+        if (R.nj && R.nj <= 16) {
+            std::vector<BucketJob> jb(R.nj);
+            SHM_CUDA(cudaMemcpy(jb.data(), S.jobs.p, sizeof(BucketJob) * R.nj, cudaMemcpyDeviceToHost));
             for (auto& j : jb)
                 std::fprintf(stderr,
                              "[shmap]  job read=%d seg=%d bb=%d m0=%d matches=%d codir=%d r=[%d,%d] sh=%.6f cand=%d "
@@ -2080,16 +2364,7 @@ static std::vector<Overflow> run_batch(MapCtx* c, const IndexStorage* ix, const 
                              j.t_l, j.t_r, j.inter, j.same);
         }
     }
-    std::vector<Overflow> ovf;
-    if (fin.n_overflow) {  // pairs (read, m) in ovf_list
-        std::vector<uint32_t> l(2 * (size_t)fin.n_overflow);
-        SHM_CUDA(cudaMemcpy(l.data(), S.ovf_list.p, sizeof(uint32_t) * l.size(), cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < fin.n_overflow; i++) ovf.push_back(Overflow{(int32_t)l[2 * i], l[2 * i + 1]});
-        std::sort(ovf.begin(), ovf.end(), [](const Overflow& x, const Overflow& y) { return x.read < y.read; });
-    }
-    H.mark("tail");
     H.print(caps ? "retry-batch" : "batch", n);
-    return ovf;
 }
 
 // Batch limits: device-resident reads in few large batches; host reads in
@@ -2123,14 +2398,20 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
     SHM_CUDA(cudaMemsetAsync(S.retry_seq.p + o.back(), 0, 32, s));
     for (size_t i = 0; i < ovf.size(); i++) copy_read(S.retry_seq.p + o[i], ovf[i].read);
     S.retry_out.reserve(ovf.size());
-    std::vector<Overflow> again =
-        run_batch(c, ix, p, S.retry_seq.p, o.data(), (int32_t)ovf.size(), S.retry_out.p, caps.data());
+    StageTimer T(c);
+    const std::vector<std::pair<int32_t, int32_t>> one{{0, (int32_t)ovf.size()}};
+    const std::vector<BatchSlot> sl = batch_slots(c, one, o.data());
+    run_batch(c, ix, p, S.retry_seq.p, o.data(), (int32_t)ovf.size(), S.retry_out.p, caps.data(), T, sl[0]);
+    SHM_CUDA(cudaStreamSynchronize(s));
+    T.collect();
+    std::vector<Overflow> again;
+    collect_batch(c, sl[0], again);
     if (!again.empty()) {
         std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n",
                      ovf[again[0].read].read);
         throw shm_cuda_error(cudaErrorMemoryAllocation);
     }
-    // the slot list goes up through the pinned staging (free again: run_batch has synchronized)
+    // the slot list goes up through the pinned staging (free: the stream has drained)
     int32_t* h_idx = (int32_t*)pinned_stage(c, sizeof(int32_t) * ovf.size());
     for (size_t i = 0; i < ovf.size(); i++) h_idx[i] = ovf[i].read;
     S.retry_idx.reserve(ovf.size());
@@ -2161,13 +2442,18 @@ static std::vector<std::pair<int32_t, int32_t>> cut_batches(const int64_t* offs,
 void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
                 int32_t n, shm_map_record* d_out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
-    std::vector<Overflow> ovf_all;
-    for (auto [i, j] : cut_batches(h_offs, n, plain, DEV_BATCH_READS, DEV_BATCH_BASES)) {
+    const auto batches = cut_batches(h_offs, n, plain, DEV_BATCH_READS, DEV_BATCH_BASES);
+    const std::vector<BatchSlot> slots = batch_slots(c, batches, h_offs);
+    StageTimer T(c);
+    for (size_t b = 0; b < batches.size(); b++) {
+        const auto [i, j] = batches[b];
         // the sketch reads exactly the batch's bytes, at any alignment
-        const uint8_t* dseq = d_seq + (h_offs[i] - h_offs[0]);
-        for (const Overflow& o : run_batch(c, ix, p, dseq, h_offs + i, j - i, d_out + i, nullptr))
-            ovf_all.push_back(Overflow{i + o.read, o.m});
+        run_batch(c, ix, p, d_seq + (h_offs[i] - h_offs[0]), h_offs + i, j - i, d_out + i, nullptr, T, slots[b]);
     }
+    SHM_CUDA(cudaStreamSynchronize(c->stream));
+    T.collect();
+    std::vector<Overflow> ovf_all;
+    for (const BatchSlot& sl : slots) collect_batch(c, sl, ovf_all);
     HostClock H;
     retry_overflows(c, ix, p, ovf_all, h_offs, [&](uint8_t* dst, int32_t g) {
         SHM_CUDA(cudaMemcpyAsync(dst, d_seq + (h_offs[g] - h_offs[0]), (size_t)(h_offs[g + 1] - h_offs[g]),
@@ -2204,23 +2490,27 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         SHM_CUDA(cudaMemcpyAsync(buf.p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, c->copy_stream));
         SHM_CUDA(cudaEventRecord(c->copied[b & 1], c->copy_stream));
     };
-    std::vector<Overflow> ovf_all;
+    const std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
+    StageTimer T(c);
     HostClock H;
     if (!batches.empty()) send(0);
     H.mark("send0");
     for (size_t b = 0; b < batches.size(); b++) {
         const auto [i, j] = batches[b];
         SHM_CUDA(cudaStreamWaitEvent(s, c->copied[b & 1], 0));
-        // the other buffer's last reader (batch b-1) has finished: run_batch synchronizes
+        // the other buffer's last reader (batch b-1) has finished: run_batch waited for
+        // this batch's bucket-table sizes, which come after all of batch b-1's work
         if (b + 1 < batches.size()) send(b + 1);
         H.mark("send");
-        for (const Overflow& o : run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr))
-            ovf_all.push_back(Overflow{i + o.read, o.m});
+        run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr, T, slots[b]);
         H.mark("run");
         SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s));
     }
     SHM_CUDA(cudaStreamSynchronize(s));
+    T.collect();
+    std::vector<Overflow> ovf_all;
+    for (const BatchSlot& sl : slots) collect_batch(c, sl, ovf_all);
     H.mark("sync");
     if (!ovf_all.empty()) {
         DevBuf<shm_map_record>& all = S.retry_all;

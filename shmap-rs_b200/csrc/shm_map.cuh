@@ -53,11 +53,13 @@ struct MapCtx {
     // host staging (pinned): the plan of the batch in flight, small readbacks
     uint8_t* h_pinned = nullptr;
     size_t h_pinned_cap = 0;
-    void* h_reads = nullptr;
+    void* h_slots = nullptr;  // per-call batch results
+    size_t h_slots_cap = 0;
     // work counters (always on): see WORK_NAMES
     int64_t work[16] = {};
     int seed_smem_set = 0;   // dynamic shared memory the seed kernels have been allowed so far
     int seedw_smem_set = 0;
+    int seedc_smem_set = 0;
     // stage timing
     bool timing = false;
     double stage_ms[N_STAGES] = {};
