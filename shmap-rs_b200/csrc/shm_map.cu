@@ -182,14 +182,16 @@ __device__ void bitonic_u64(uint64_t* A, uint32_t P) {
         }
 }
 
+// The sketch hashes are uniform in [0, thr], so their low bits pick the slot.
 __device__ __forceinline__ bool pht_lookup(const BatchView& v, int32_t q, uint64_t h, uint32_t& idx) {
     const uint64_t base = v.pht_off[q];
     const uint64_t mask = v.pht_off[q + 1] - base - 1;
-    uint64_t i = mix64(h) & mask;
+    uint64_t i = h & mask;
     for (;;) {
-        uint32_t val = v.pht_val[base + i];
+        const uint32_t val = v.pht_val[base + i];
+        const uint64_t key = v.pht_key[base + i];
         if (val == 0xffffffffu) return false;
-        if (v.pht_key[base + i] == h) {
+        if (key == h) {
             idx = val;
             return true;
         }
@@ -200,7 +202,7 @@ __device__ __forceinline__ bool pht_lookup(const BatchView& v, int32_t q, uint64
 __device__ __forceinline__ void pht_insert(const BatchView& v, int32_t q, uint64_t h, uint32_t idx) {
     const uint64_t base = v.pht_off[q];
     const uint64_t mask = v.pht_off[q + 1] - base - 1;
-    uint64_t i = mix64(h) & mask;
+    uint64_t i = h & mask;
     for (;;) {
         if (atomicCAS(v.pht_val + base + i, 0xffffffffu, idx) == 0xffffffffu) {
             v.pht_key[base + i] = h;
@@ -1412,8 +1414,7 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
     const uint32_t ncand = v.coff[v.n];
     int32_t* cntA = rsc.base + (size_t)wid * rsc.per_warp;
     int32_t* D = cntA + rsc.nu_max;
-    int32_t* C = D + rsc.wmax + 1;
-    int32_t* PC = C + rsc.wmax + 1;
+    int32_t* PC = D + rsc.wmax + 1;
     int32_t* ring = PC + rsc.wmax + 1;
     const bool ap = v.P.ap != 0;
     const DevIndex& I = v.I;
@@ -1444,7 +1445,10 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
         for (int32_t i = lane; i < n_u; i += 32) cntA[i] = 0;
         for (int32_t i = lane; i <= W; i += 32) D[i] = 0;
         __syncwarp();
-        // phase 1: seed of every position, its occurrence interval of windows
+        // phase 1: seed of every position, its occurrence interval of windows,
+        // and the prefix PC of strand agreement (+1 same strand, -1 opposite)
+        int32_t pc_carry = 0;
+        if (lane == 0) PC[0] = 0;
         for (int32_t c0 = 0; c0 < W; c0 += 32) {
             const int32_t x = c0 + lane;  // position from + x
             const bool valid = x < W;
@@ -1459,7 +1463,12 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
                     os = v.sd_os[kb + si];
                 }
             }
-            if (valid) C[x] = s >= 0 ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
+            {
+                const int32_t cv = (valid && s >= 0) ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
+                const int32_t inc = warp_inclusive_scan(cv);
+                if (valid) PC[x + 1] = pc_carry + inc;
+                pc_carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
             const unsigned peers = __match_any_sync(0xffffffffu, s);
             int32_t t = 0, occ = 1, rho = 0, gsz = 0;
             uint32_t ooff = 0;
@@ -1504,20 +1513,14 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
             }
             __syncwarp();
         }
-        // phase 2a: prefix of strand agreement
-        int32_t carry = 0;
-        for (int32_t c0 = 0; c0 < W; c0 += 32) {
-            const int32_t x = c0 + lane;
-            int32_t cv = x < W ? C[x] : 0;
-            int32_t inc = warp_inclusive_scan(cv);
-            if (x < W) PC[x + 1] = carry + inc;
-            carry += __shfl_sync(0xffffffffu, inc, 31);
-        }
-        if (lane == 0) PC[0] = 0;
         __syncwarp();
-        // phase 2b: intersection per window start, score, first maximum
+        // phase 2: intersection per window start, score, first maximum. Under
+        // Containment every score is I / m for the same m, and distinct I < 2^31
+        // give distinct quotients, so the first maximum of I is the first
+        // maximum of the score: the division is done once, for the winner.
+        const bool jac = v.P.metric == 1;
         double best = -1.0;
-        int32_t bl = -1, bI = 0, bS = 0, br = 0;
+        int32_t bl = -1, bI = -1, bS = 0, br = 0;
         int32_t icarry = 0;
         for (int32_t c0 = 0; c0 < W; c0 += 32) {
             const int32_t x = c0 + lane;
@@ -1543,10 +1546,15 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
                     r = lo;
                 }
                 const int32_t I_ = inc, sk = r - x;
-                const double score = v.P.metric == 1 ? __ddiv_rn((double)I_, (double)(m + sk - I_))
-                                                     : __ddiv_rn((double)I_, (double)m);
-                if (score > best) {
-                    best = score;
+                bool better;
+                if (jac) {
+                    const double score = __ddiv_rn((double)I_, (double)(m + sk - I_));
+                    better = score > best;
+                    if (better) best = score;
+                } else {
+                    better = I_ > bI;
+                }
+                if (better) {
                     bl = x;
                     bI = I_;
                     bS = PC[r] - PC[x];
@@ -1561,7 +1569,8 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
             int32_t obI = __shfl_xor_sync(0xffffffffu, bI, o);
             int32_t obS = __shfl_xor_sync(0xffffffffu, bS, o);
             int32_t obr = __shfl_xor_sync(0xffffffffu, br, o);
-            bool take = ob > best || (ob == best && obl >= 0 && (bl < 0 || obl < bl));
+            const bool take = jac ? (ob > best || (ob == best && obl >= 0 && (bl < 0 || obl < bl)))
+                                  : (obI > bI || (obI == bI && obl >= 0 && (bl < 0 || obl < bl)));
             if (take) {
                 best = ob;
                 bl = obl;
@@ -1570,6 +1579,7 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
                 br = obr;
             }
         }
+        if (!jac && bl >= 0) best = __ddiv_rn((double)bI, (double)m);
         if (lane == 0) {
             J->score = best;
             if (bl >= 0) {
@@ -2329,7 +2339,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     RefScratch rsc{};
     rsc.nu_max = hm.nu_max + 1;
     rsc.wmax = 2 * hm.half_max + 2;
-    rsc.per_warp = (size_t)rsc.nu_max + 3 * ((size_t)rsc.wmax + 1) + (size_t)hm.m_max + 1;
+    rsc.per_warp = (size_t)rsc.nu_max + 2 * ((size_t)rsc.wmax + 1) + (size_t)hm.m_max + 1;
     size_t warps = (size_t)grid_for((size_t)job_cap * 32, 256, 8) * 8;
     const size_t budget_ints = (size_t)1 << 28;  // 1 GiB of refinement scratch at most
     while (warps > 8 && warps * rsc.per_warp > budget_ints) warps /= 2;

@@ -47,29 +47,10 @@ __device__ __forceinline__ uint64_t rotr1(uint64_t x) {
     return ((uint64_t)__funnelshift_r(hi, lo, 1) << 32) | __funnelshift_r(lo, hi, 1);
 }
 
-// One selected window: record it by the kernel's mode.
-template <int MODE>
-__device__ __forceinline__ void emit_kmer(const SketchArgs& a, int32_t q, uint64_t h, uint32_t rs, uint64_t out_base,
-                                          uint32_t out_cap, uint32_t& n_sel) {
-    if (MODE == SK_COUNT) {
-        n_sel++;
-    } else if (MODE == SK_WRITE) {
-        a.out_h[out_base + n_sel] = h;
-        a.out_rs[out_base + n_sel] = rs;
-        n_sel++;
-    } else {
-        uint32_t slot = atomicAdd(a.kmer_cnt + q, 1u);
-        if (slot < out_cap) {
-            a.out_h[out_base + slot] = h;
-            a.out_rs[out_base + slot] = rs;
-        }
-    }
-}
-
 // Lookup tables as the rolling step reads them: the entering base's pair
 // {fw, rc rotated left by k-1} and the leaving base's pair {fw rotated left
 // by k, rc rotated right by 1}, one 16-byte shared load each.
-struct LutPair {
+struct __align__(16) LutPair {
     uint64_t a, b;
 };
 
@@ -77,65 +58,150 @@ constexpr int SK_THREADS = 256;                                  // one run of S
 constexpr int SK_TILE_CAP = SK_THREADS * SKETCH_WIN + 1024;       // bytes a CTA stages per tile
 constexpr int SK_TILE_WORDS = SK_TILE_CAP / 4 + 8;                // + slack for the word past the last byte
 constexpr int SK_TILE_PWORDS = SK_TILE_WORDS + SK_TILE_WORDS / 32 + 1;
+constexpr int SK_TILE_BYTES = (SK_TILE_PWORDS * 4 + 15) / 16 * 16; // the tile, rounded to 16 bytes
+constexpr int SK_TB = 4;                                          // selections a thread buffers (append mode)
 
 // Staged bytes carry one pad word after every 32 words: the runs of
 // neighbouring threads start SKETCH_WIN bytes apart, so without the pad every
 // lane of a warp would read the same bank.
 __device__ __forceinline__ int pword(int w) { return w + (w >> 5); }
 
-template <bool STAGED>
-__device__ __forceinline__ uint32_t fetch_word(const uint32_t* tile, const uint8_t* base, int64_t w, int64_t first,
-                                               int64_t lim) {
-    if (STAGED) return tile[pword((int)w)];
-    // unstaged: bytes of `base` outside [first, lim) read as 0
-    uint32_t v = 0;
+// The bytes of a tile, staged in shared memory (offsets relative to the tile).
+struct StagedBytes {
+    const uint32_t* tile;
+    __device__ __forceinline__ uint32_t word(int w) const { return tile[pword(w)]; }
+    __device__ __forceinline__ uint32_t byte(int x) const { return (tile[pword(x >> 2)] >> (8 * (x & 3))) & 0xffu; }
+};
+
+// The same bytes read from global memory (a tile too large to stage): bytes
+// of `base` outside [first, lim) read as 0.
+struct GlobalBytes {
+    const uint8_t* base;
+    int64_t first, lim;
+    __device__ __forceinline__ uint32_t word(int64_t w) const {
+        uint32_t v = 0;
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const int64_t x = 4 * w + j;
-        if (x >= first && x < lim) v |= (uint32_t)__ldg(base + x) << (8 * j);
+        for (int j = 0; j < 4; j++) {
+            const int64_t x = 4 * w + j;
+            if (x >= first && x < lim) v |= (uint32_t)__ldg(base + x) << (8 * j);
+        }
+        return v;
     }
-    return v;
+    __device__ __forceinline__ uint32_t byte(int64_t x) const { return __ldg(base + x); }
+};
+
+// Where a thread's selections go. Count and write modes: a counter and the
+// run's own output range. Append mode: SK_TB slots of shared memory
+// (thread-interleaved), emptied into the read's list when full and at the end
+// of the run.
+struct Emit {
+    uint64_t out_base;
+    uint32_t out_cap, n_sel;
+    uint64_t* bh;  // bh[j * SK_THREADS], br[j * SK_THREADS]: this thread's slots
+    uint32_t* br;
+};
+
+// Reserves n slots of read q's list and writes this thread's buffered selections there.
+__device__ __forceinline__ void drain(const SketchArgs& a, int32_t q, Emit& e, uint32_t base) {
+    for (uint32_t j = 0; j < e.n_sel; j++) {
+        const uint32_t slot = base + j;
+        if (slot < e.out_cap) {
+            a.out_h[e.out_base + slot] = e.bh[j * SK_THREADS];
+            a.out_rs[e.out_base + slot] = e.br[j * SK_THREADS];
+        }
+    }
+    e.n_sel = 0;
 }
 
-// Rolls the windows [1, cnt) of one run whose bytes start at word-aligned
-// offset `x` (in bytes) from `base`; window 0 has already been emitted.
-template <int MODE, bool STAGED>
-__device__ __forceinline__ void roll_run(const SketchArgs& a, const LutPair* __restrict__ Lin,
-                                         const LutPair* __restrict__ Lout, const uint32_t* tile, const uint8_t* base,
-                                         int64_t x, int64_t first, int64_t lim, int32_t cnt, int k, uint64_t thr, int32_t q,
-                                         int32_t r0, uint64_t out_base, uint32_t out_cap, uint32_t& n_sel,
-                                         uint64_t fw, uint64_t rc) {
-    // window t takes base x+t+k-1 in and drops base x+t-1
-    const int64_t xi = x + k, xo = x;
-    const uint32_t shi = (uint32_t)(xi & 3) * 8, sho = (uint32_t)(xo & 3) * 8;
-    int64_t wi = xi >> 2, wo = xo >> 2;
-    uint32_t li = fetch_word<STAGED>(tile, base, wi, first, lim),
-             lo_ = fetch_word<STAGED>(tile, base, wo, first, lim);
-    int32_t t = 1;
-    auto step = [&](uint32_t ib, uint32_t ob, int32_t tt) {
-        const LutPair pi = Lin[ib], po = Lout[ob];
-        fw = rotl1(fw) ^ po.a ^ pi.a;
-        rc = rotr1(rc) ^ po.b ^ pi.b;
+template <int MODE>
+__device__ __forceinline__ void emit_kmer(const SketchArgs& a, int32_t q, uint64_t h, uint32_t rs, Emit& e) {
+    if (MODE == SK_COUNT) {
+        e.n_sel++;
+    } else if (MODE == SK_WRITE) {
+        a.out_h[e.out_base + e.n_sel] = h;
+        a.out_rs[e.out_base + e.n_sel] = rs;
+        e.n_sel++;
+    } else {
+        if (e.n_sel == SK_TB) drain(a, q, e, atomicAdd(a.kmer_cnt + q, (uint32_t)SK_TB));
+        e.bh[e.n_sel * SK_THREADS] = h;
+        e.br[e.n_sel * SK_THREADS] = rs;
+        e.n_sel++;
+    }
+}
+
+// One rolling step: byte ib enters, byte ob leaves.
+__device__ __forceinline__ void roll(uint64_t& fw, uint64_t& rc, const LutPair* __restrict__ Lin,
+                                     const LutPair* __restrict__ Lout, uint32_t ib, uint32_t ob) {
+    const LutPair pi = Lin[ib], po = Lout[ob];
+    fw = rotl1(fw) ^ po.a ^ pi.a;
+    rc = rotr1(rc) ^ po.b ^ pi.b;
+}
+
+// Window selection: h = fw ^ rc <= thr. The high words decide all but about
+// one window in a hundred (for thr near 1% of the range); the full compare
+// runs only for those.
+template <int MODE>
+__device__ __forceinline__ void check(const SketchArgs& a, uint64_t fw, uint64_t rc, uint32_t thr_hi, uint64_t thr,
+                                      int32_t q, int32_t r, Emit& e) {
+    const uint32_t hh = (uint32_t)(fw >> 32) ^ (uint32_t)(rc >> 32);
+    if (hh <= thr_hi) {
         const uint64_t h = fw ^ rc;
-        if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)(r0 + tt) << 1) | (fw > rc ? 1u : 0u), out_base, out_cap, n_sel);
-    };
-    for (; t + 4 <= cnt; t += 4) {
-        const uint32_t hi_i = fetch_word<STAGED>(tile, base, ++wi, first, lim);
-        const uint32_t hi_o = fetch_word<STAGED>(tile, base, ++wo, first, lim);
+        if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)r << 1) | (fw > rc ? 1u : 0u), e);
+    }
+}
+
+// The windows [0, cnt) of one run whose first byte is at offset x of `src`.
+// Window 0 is reached by rolling its k bytes in from the all-zero state: a
+// window of k non-ACGT bytes hashes to 0 on both strands, and the leaving
+// bytes of those steps are such bytes. Window t > 0 takes byte x+t+k-1 in and
+// drops byte x+t-1.
+template <int MODE, class Src, class Idx>
+__device__ __forceinline__ void sketch_run(const SketchArgs& a, const LutPair* __restrict__ Lin,
+                                           const LutPair* __restrict__ Lout, const Src& src, Idx x, int32_t cnt,
+                                           int k, uint64_t thr, int32_t q, int32_t r0, Emit& e) {
+    if (cnt <= 0) return;
+    const uint32_t thr_hi = (uint32_t)(thr >> 32);
+    uint64_t fw = 0, rc = 0;
+    for (int i = 0; i < k; i++) {
+        const LutPair pi = Lin[src.byte(x + i)];
+        fw = rotl1(fw) ^ pi.a;
+        rc = rotr1(rc) ^ pi.b;
+    }
+    check<MODE>(a, fw, rc, thr_hi, thr, q, r0, e);
+    const Idx xi = x + k, xo = x;
+    const uint32_t shi = (uint32_t)(xi & 3) * 8, sho = (uint32_t)(xo & 3) * 8;
+    Idx wi = xi >> 2, wo = xo >> 2;
+    uint32_t li = src.word(wi), lo_ = src.word(wo);
+    int32_t t = 1;
+    for (; t + 3 < cnt; t += 4) {
+        const uint32_t hi_i = src.word(++wi), hi_o = src.word(++wo);
         const uint32_t ib4 = __funnelshift_r(li, hi_i, shi), ob4 = __funnelshift_r(lo_, hi_o, sho);
         li = hi_i;
         lo_ = hi_o;
 #pragma unroll
-        for (int j = 0; j < 4; j++) step((ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu, t + j);
+        for (int j = 0; j < 4; j++) {
+            roll(fw, rc, Lin, Lout, (ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu);
+            check<MODE>(a, fw, rc, thr_hi, thr, q, r0 + t + j, e);
+        }
     }
     if (t < cnt) {
-        const uint32_t hi_i = fetch_word<STAGED>(tile, base, ++wi, first, lim);
-        const uint32_t hi_o = fetch_word<STAGED>(tile, base, ++wo, first, lim);
+        const uint32_t hi_i = src.word(++wi), hi_o = src.word(++wo);
         const uint32_t ib4 = __funnelshift_r(li, hi_i, shi), ob4 = __funnelshift_r(lo_, hi_o, sho);
 #pragma unroll
-        for (int j = 0; j < 3; j++)
-            if (t + j < cnt) step((ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu, t + j);
+        for (int j = 0; j < 3; j++) {
+            if (t + j < cnt) {
+                roll(fw, rc, Lin, Lout, (ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu);
+                check<MODE>(a, fw, rc, thr_hi, thr, q, r0 + t + j, e);
+            }
+        }
     }
+}
+
+// Dynamic shared memory of a k_sketch CTA: the staged tile, then (append
+// mode) the threads' selection slots: hashes, then r << 1 | strand.
+static_assert(SK_TILE_BYTES % 16 == 0, "the selection slots stay 8-byte aligned");
+constexpr size_t sk_dyn_bytes(int mode) {
+    return (size_t)SK_TILE_BYTES + (mode == SK_APPEND ? (size_t)SK_TB * SK_THREADS * 12 : 0);
 }
 
 // Each CTA takes tiles of SK_THREADS consecutive runs. Runs are laid out in
@@ -146,25 +212,45 @@ __device__ __forceinline__ void roll_run(const SketchArgs& a, const LutPair* __r
 template <int MODE>
 __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const SketchLuts* __restrict__ luts) {
     __shared__ LutPair Lin[256], Lout[256];
-    __shared__ uint32_t tile[SK_TILE_PWORDS];
     __shared__ int64_t s_lo, s_hi;
+    __shared__ int32_t s_q[2];
+    extern __shared__ __align__(16) uint8_t sk_dyn[];
+    uint32_t* tile = (uint32_t*)sk_dyn;
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         Lin[i] = LutPair{luts->fw[i], luts->rc_k1[i]};
         Lout[i] = LutPair{luts->fw_k[i], luts->rc_r1[i]};
     }
+    Emit e{0, 0, 0, nullptr, nullptr};
+    if (MODE == SK_APPEND) {
+        e.bh = (uint64_t*)(sk_dyn + SK_TILE_BYTES) + threadIdx.x;
+        e.br = (uint32_t*)(sk_dyn + SK_TILE_BYTES + (size_t)SK_TB * SK_THREADS * 8) + threadIdx.x;
+    }
+    const int lane = threadIdx.x & 31;
     const int k = a.k;
     const uint64_t thr = a.thr;
     const uint64_t n_chunks = a.n_chunks;
     const uint64_t n_tiles = (n_chunks + SK_THREADS - 1) / SK_THREADS;
     for (uint64_t tl = blockIdx.x; tl < n_tiles; tl += gridDim.x) {
-        const uint64_t c = tl * SK_THREADS + threadIdx.x;
-        const uint64_t c_last = min(tl * SK_THREADS + SK_THREADS, n_chunks) - 1;
+        const uint64_t c0 = tl * SK_THREADS, c = c0 + threadIdx.x;
+        const uint64_t c_last = min(c0 + SK_THREADS, n_chunks) - 1;
+        if (threadIdx.x == 0 || threadIdx.x == 32) {  // sequences of the tile's first and last runs
+            const uint64_t cc = threadIdx.x == 0 ? c0 : c_last;
+            int32_t lo = 0, hi = a.n_seq;  // upper_bound over chunk_off
+            while (hi - lo > 1) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (__ldg(a.chunk_off + mid) <= cc) lo = mid;
+                else hi = mid;
+            }
+            s_q[threadIdx.x == 0 ? 0 : 1] = lo;
+        }
+        __syncthreads();
         int32_t q = 0, cnt = 0;
         int64_t start = 0, w0 = 0;  // byte offset of the run in `seq`, its first window in the sequence
         if (c < n_chunks) {
-            int32_t lo = 0, hi = a.n_seq;  // upper_bound over chunk_off
+            // the run's sequence lies between those of the tile's first and last runs
+            int32_t lo = s_q[0], hi = s_q[1] + 1;
             while (hi - lo > 1) {
-                int32_t mid = (lo + hi) >> 1;
+                const int32_t mid = (lo + hi) >> 1;
                 if (__ldg(a.chunk_off + mid) <= c) lo = mid;
                 else hi = mid;
             }
@@ -173,13 +259,13 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
             w0 = (int64_t)(c - __ldg(a.chunk_off + q)) * SKETCH_WIN;
             cnt = (int32_t)(min(w0 + (int64_t)SKETCH_WIN, nw) - w0);
             start = s0 + w0;
-            if (c == tl * SK_THREADS) s_lo = start;
+            if (c == c0) s_lo = start;
             if (c == c_last) s_hi = start + cnt + k - 1;
         }
         __syncthreads();  // s_lo/s_hi written; the previous tile's readers are done
         const int64_t lo_b = s_lo, hi_b = s_hi;
         const uint8_t* A0 = (const uint8_t*)((uintptr_t)(a.seq + lo_b) & ~(uintptr_t)15);
-        const int64_t lim = (int64_t)((a.seq + hi_b) - A0);  // staged bytes are [A0 + (lo - A0), A0 + lim)
+        const int64_t lim = (int64_t)((a.seq + hi_b) - A0);  // the tile's bytes are [first, lim) from A0
         const int64_t first = (int64_t)((a.seq + lo_b) - A0);
         const bool staged = lim <= (int64_t)SK_TILE_CAP;
         if (staged) {
@@ -188,7 +274,10 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
                 uint32_t wv[4];
                 if (16 * v >= first && 16 * v + 16 <= lim) {
                     const uint4 u = __ldg((const uint4*)(A0 + 16 * v));
-                    wv[0] = u.x; wv[1] = u.y; wv[2] = u.z; wv[3] = u.w;
+                    wv[0] = u.x;
+                    wv[1] = u.y;
+                    wv[2] = u.z;
+                    wv[3] = u.w;
                 } else {
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
@@ -205,35 +294,43 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
             }
         }
         __syncthreads();
+        e.n_sel = 0;
+        e.out_base = 0;
+        e.out_cap = 0;
         if (cnt > 0) {
-            uint64_t out_base = 0;
-            uint32_t out_cap = 0, n_sel = 0;
-            if (MODE == SK_WRITE) out_base = a.chunk_out[c];
+            if (MODE == SK_WRITE) e.out_base = a.chunk_out[c];
             if (MODE == SK_APPEND) {
-                out_base = a.kmer_off[q];
-                out_cap = (uint32_t)(a.kmer_off[q + 1] - out_base);
+                e.out_base = a.kmer_off[q];
+                e.out_cap = (uint32_t)(a.kmer_off[q + 1] - e.out_base);
             }
-            const int64_t x = (int64_t)((a.seq + start) - A0);  // run's first byte relative to A0
-            const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;  // r of the run's first window
-            // first window, by definition (tests/nthash_equivalence.rs:31-61);
-            // rc(b) rotated left by i is rc_r1(b) rotated left by i + 1
-            uint64_t fw = 0, rc = 0;
-            for (int i = 0; i < k; i++) {
-                const int64_t xx = x + i;
-                const uint32_t b = staged ? (tile[pword((int)(xx >> 2))] >> (8 * (xx & 3))) & 0xffu : __ldg(A0 + xx);
-                fw ^= rotl64(Lin[b].a, (uint32_t)(k - 1 - i));
-                rc ^= rotl64(Lout[b].b, (uint32_t)(i + 1));
+        }
+        const int64_t x = (int64_t)((a.seq + start) - A0);      // the run's first byte from A0
+        const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;  // r of the run's first window
+        if (staged)
+            sketch_run<MODE>(a, Lin, Lout, StagedBytes{tile}, (int)x, cnt, k, thr, q, r0, e);
+        else
+            sketch_run<MODE>(a, Lin, Lout, GlobalBytes{A0, first, lim}, x, cnt, k, thr, q, r0, e);
+        if (MODE == SK_COUNT && c < n_chunks) a.chunk_cnt[c] = e.n_sel;
+        if (MODE == SK_APPEND) {
+            // every lane: the run's buffered selections go to the read's list, one
+            // counter update per read and warp (a warp's runs are consecutive, so
+            // the lanes of one read are contiguous)
+            const uint32_t nb = e.n_sel;
+            uint32_t incl = nb;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
             }
-            const uint64_t h = fw ^ rc;
-            if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)r0 << 1) | (fw > rc ? 1u : 0u), out_base, out_cap, n_sel);
-            if (staged)
-                roll_run<MODE, true>(a, Lin, Lout, tile, A0, x, first, lim, cnt, k, thr, q, r0, out_base, out_cap, n_sel, fw, rc);
-            else
-                roll_run<MODE, false>(a, Lin, Lout, tile, A0, x, first, lim, cnt, k, thr, q, r0, out_base, out_cap, n_sel, fw,
-                                      rc);
-            if (MODE == SK_COUNT) a.chunk_cnt[c] = n_sel;
-        } else if (MODE == SK_COUNT && c < n_chunks) {
-            a.chunk_cnt[c] = 0;
+            const uint32_t excl = incl - nb;
+            const unsigned peers = __match_any_sync(0xffffffffu, cnt > 0 ? q : -1);
+            const int leader = __ffs(peers) - 1, last = 31 - __clz(peers);
+            const uint32_t g0 = __shfl_sync(0xffffffffu, excl, leader);
+            const uint32_t gtot = __shfl_sync(0xffffffffu, incl, last) - g0;
+            uint32_t base = 0;
+            if (lane == leader && cnt > 0 && gtot) base = atomicAdd(a.kmer_cnt + q, gtot);
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (nb) drain(a, q, e, base + excl - g0);
         }
         __syncthreads();  // the tile is free for the next one
     }
@@ -253,9 +350,17 @@ void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStrea
     if (a.n_chunks == 0) return;
     const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
     const int grid = grid_for(n_tiles, 1, 5);  // tiles, at most 5 resident CTAs per SM
-    if (mode == SK_COUNT) k_sketch<SK_COUNT><<<grid, SK_THREADS, 0, s>>>(a, L);
-    else if (mode == SK_WRITE) k_sketch<SK_WRITE><<<grid, SK_THREADS, 0, s>>>(a, L);
-    else k_sketch<SK_APPEND><<<grid, SK_THREADS, 0, s>>>(a, L);
+    const size_t dyn = sk_dyn_bytes(mode);
+    if (mode == SK_COUNT) {
+        SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        k_sketch<SK_COUNT><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    } else if (mode == SK_WRITE) {
+        SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_WRITE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        k_sketch<SK_WRITE><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    } else {
+        SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_APPEND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        k_sketch<SK_APPEND><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    }
     SHM_CUDA(cudaGetLastError());
     count_launch();
 }
