@@ -1224,48 +1224,91 @@ __device__ __forceinline__ uint32_t ub_u32(const uint32_t* a, uint32_t n, uint32
     return lo;
 }
 
+// Each thread takes CONTRIB_RUN consecutive hit words: the first word's read
+// and seed come from two binary searches, the rest by stepping through the
+// seed's hit list (sorted by gidx) and on to the next seed or read. The
+// previous hit's bucket and the current segment's bounds are carried along.
+constexpr int CONTRIB_RUN = 8;
+
+__device__ __forceinline__ int32_t seg_step(const DevIndex& I, uint32_t g, int32_t seg, uint32_t& s_lo,
+                                            uint32_t& s_hi) {
+    if (seg >= 0 && g >= s_lo && g < s_hi) return seg;
+    seg = seg_of(I, g);
+    s_lo = __ldg(I.seg_off + seg);
+    s_hi = __ldg(I.seg_off + seg + 1);
+    return seg;
+}
+
 __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
     const uint64_t total = v.hw_off[v.n];
     const bool ap = v.P.ap != 0;
-    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
-        const int32_t q = (int32_t)ub_u64(v.hw_off, (uint32_t)v.n + 1, w) - 1;
-        const uint32_t u = (uint32_t)(w - v.hw_off[q]);
-        const uint64_t kb = v.kcap_off[q];
-        const uint32_t np = (uint32_t)v.r_nproc[q];
-        const uint32_t j = ub_u32(v.sd_hpre + kb, np, u) - 1;
-        const uint32_t t = u - v.sd_hpre[kb + j];
-        const uint32_t a = v.sd_a[kb + j], cnt = v.sd_cnt[kb + j], os = v.sd_os[kb + j];
-        const uint32_t occs = os >> 1, sstr = os & 1u;
-        const int64_t h = v.r_half[q];
-        const DevIndex& I = v.I;
-        const uint32_t g_t = __ldg(I.hits + a + t);
-        const int32_t seg_t = seg_of(I, g_t);
-        const int64_t b_t = hit_pos(I, g_t, seg_t, ap) / h;
-        bool first = true, prev_is_bm1 = false;
+    const DevIndex& I = v.I;
+    const uint64_t nrun = (total + CONTRIB_RUN - 1) / CONTRIB_RUN;
+    for (uint64_t rn = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; rn < nrun;
+         rn += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t w = rn * CONTRIB_RUN;
+        const uint64_t wend = min(w + CONTRIB_RUN, total);
+        int32_t q = (int32_t)ub_u64(v.hw_off, (uint32_t)v.n + 1, w) - 1;
+        uint64_t kb = v.kcap_off[q];
+        uint32_t np = (uint32_t)v.r_nproc[q];
+        uint32_t h = (uint32_t)v.r_half[q];
+        uint32_t j = ub_u32(v.sd_hpre + kb, np, (uint32_t)(w - v.hw_off[q])) - 1;
+        uint32_t t = (uint32_t)(w - v.hw_off[q]) - v.sd_hpre[kb + j];
+        uint32_t a = v.sd_a[kb + j], cnt = v.sd_cnt[kb + j], os = v.sd_os[kb + j];
+        int32_t seg = -1;
+        uint32_t s_lo = 0, s_hi = 0;
+        int32_t seg_p = -1;  // bucket of the seed's previous hit (seg_p < 0: none)
+        uint32_t b_p = 0;
         if (t > 0) {
             const uint32_t g_p = __ldg(I.hits + a + t - 1);
-            const int32_t seg_p = seg_of(I, g_p);
-            const int64_t b_p = hit_pos(I, g_p, seg_p, ap) / h;
-            first = !(seg_p == seg_t && b_p == b_t);
-            prev_is_bm1 = seg_p == seg_t && b_p == b_t - 1;
+            seg_p = seg = seg_step(I, g_p, seg, s_lo, s_hi);
+            b_p = (ap ? (__ldg(I.ref_rs + g_p) >> 1) : g_p - s_lo) / h;
         }
-        if (!first) continue;
-        if (cnt == 1) {
-            const uint32_t rs = __ldg(I.ref_rs + g_t);
-            const int32_t cd = ((rs & 1u) == sstr) ? 1 : -1, r = (int32_t)(rs >> 1);
-            bt_add(v, q, seg_t, b_t, 1, cd, r, r);  // add_to_pos (buckets.rs:642-662)
-            if (b_t > 0) bt_add(v, q, seg_t, b_t - 1, 1, cd, r, r);
-            continue;
-        }
-        // streamed multi-hit seed: one clamped contribution per bucket (seeding.rs:113-205)
-        for (int e = 0; e < 2; e++) {
-            const int64_t bb = b_t - e;
-            if (bb < 0) break;
-            if (e == 1 && prev_is_bm1) break;
-            uint32_t A, B;
-            seed_range(I, a, cnt, seg_t, bb * h, (bb + 2) * h, ap, A, B);
-            Agg g = range_agg(I, A, B, sstr);
-            bt_add(v, q, seg_t, bb, min(g.count, (int32_t)occs), g.codir, g.rmin, g.rmax);
+        for (;;) {
+            const uint32_t occs = os >> 1, sstr = os & 1u;
+            const uint32_t g_t = __ldg(I.hits + a + t);
+            seg = seg_step(I, g_t, seg, s_lo, s_hi);
+            const uint32_t b_t = (ap ? (__ldg(I.ref_rs + g_t) >> 1) : g_t - s_lo) / h;
+            const bool first = !(seg_p == seg && b_p == b_t);
+            const bool prev_is_bm1 = seg_p == seg && b_p + 1 == b_t;
+            if (first) {
+                if (cnt == 1) {
+                    const uint32_t rs = __ldg(I.ref_rs + g_t);
+                    const int32_t cd = ((rs & 1u) == sstr) ? 1 : -1, r = (int32_t)(rs >> 1);
+                    bt_add(v, q, seg, b_t, 1, cd, r, r);  // add_to_pos (buckets.rs:642-662)
+                    if (b_t > 0) bt_add(v, q, seg, (int64_t)b_t - 1, 1, cd, r, r);
+                } else {
+                    // streamed multi-hit seed: one clamped contribution per bucket (seeding.rs:113-205)
+                    for (int e = 0; e < 2; e++) {
+                        const int64_t bb = (int64_t)b_t - e;
+                        if (bb < 0) break;
+                        if (e == 1 && prev_is_bm1) break;
+                        uint32_t A, B;
+                        seed_range(I, a, cnt, seg, bb * (int64_t)h, (bb + 2) * (int64_t)h, ap, A, B);
+                        Agg g = range_agg(I, A, B, sstr);
+                        bt_add(v, q, seg, bb, min(g.count, (int32_t)occs), g.codir, g.rmin, g.rmax);
+                    }
+                }
+            }
+            if (++w >= wend) break;
+            seg_p = seg;
+            b_p = b_t;
+            if (++t == cnt) {  // next seed of the read, or the next read with hits
+                t = 0;
+                seg_p = -1;
+                if (++j == np) {
+                    do {
+                        q++;
+                    } while (v.hw_off[q + 1] <= w);
+                    kb = v.kcap_off[q];
+                    np = (uint32_t)v.r_nproc[q];
+                    h = (uint32_t)v.r_half[q];
+                    j = ub_u32(v.sd_hpre + kb, np, 0u) - 1;  // past the seeds without hits
+                }
+                a = v.sd_a[kb + j];
+                cnt = v.sd_cnt[kb + j];
+                os = v.sd_os[kb + j];
+            }
         }
     }
 }
