@@ -22,9 +22,14 @@ template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t cap = 0;  // elements
+    // Grows (never shrinks). Queued work may still use the old buffer, so a
+    // growth waits for the device first.
     void reserve(size_t n) {
         if (n <= cap && p) return;
-        if (p) SHM_CUDA(cudaFree(p));
+        if (p) {
+            SHM_CUDA(cudaDeviceSynchronize());
+            SHM_CUDA(cudaFree(p));
+        }
         p = nullptr;
         size_t want = n < 16 ? 16 : n;
         SHM_CUDA(cudaMalloc(&p, want * sizeof(T)));

@@ -91,6 +91,8 @@ struct BatchView {
     uint64_t *hw, *hw_off, *bt_size, *bt_off;
     BSlot* bt;
     uint32_t* bt_list;  // per read, the slots of its distinct buckets (r_seeded[q] of them)
+    uint64_t bt_cap;    // most slots a read's bucket table gets (a power of two >= 16)
+    uint32_t* r_flags;  // per read: nonzero when its bucket table passed its load limit
     BucketJob* jobs;
     uint32_t* n_jobs;
     uint32_t job_cap;
@@ -223,6 +225,14 @@ __device__ __forceinline__ uint64_t seed_bucket_bound(const BatchView& v, uint32
     const int32_t s0 = seg_of(v.I, g0), s1 = seg_of(v.I, g1);
     const uint64_t span = (uint64_t)(g1 - g0) / (uint64_t)h + 1 + 3ULL * (uint64_t)(s1 - s0 + 1);
     return min((uint64_t)(2ULL * cnt), span);
+}
+
+// Slots of a read's bucket table: twice the bound on its distinct buckets
+// (a power of two, at least 16), capped at v.bt_cap. A capped table that
+// fills past its load limit marks the read, which is then mapped again with
+// the full bound.
+__device__ __forceinline__ uint64_t bt_slots(const BatchView& v, uint64_t ebound) {
+    return min(max((uint64_t)16, pow2_ceil(2 * ebound)), v.bt_cap);
 }
 
 // ------------------------------------------------------------------ K2 seedprep
@@ -403,7 +413,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
             v.r_status[q] = ST_OVERFLOW;
         } else {
             v.hw[q] = smatch;
-            v.bt_size[q] = smatch ? max((uint64_t)16, pow2_ceil(2 * ebound)) : 0;
+            v.bt_size[q] = smatch ? bt_slots(v, ebound) : 0;
         }
         atomicMax(&v.mx->m_max, m);
         atomicMax(&v.mx->nu_max, n_u);
@@ -429,429 +439,10 @@ __global__ void __launch_bounds__(256) k_seedprep(BatchView v, const int32_t* __
     }
 }
 
-// The same stage with one warp per read (reads whose k-mer capacity fits a
-// per-warp slice of P <= 1024 elements): no block barriers. Per warp:
-// A (u64) hashes, compacted in place into group hashes; E (u64) rarest-first
-// keys; B (u32) element keys, compacted into occs << 1 | strand; D (u32)
-// hit-list starts.
-constexpr size_t SEEDW_BYTES_PER_ELEM = 8 + 8 + 4 + 4;
-
-__device__ void warp_bitonic_ab(uint64_t* A, uint32_t* B, uint32_t P, int lane) {
-    for (uint32_t k = 2; k <= P; k <<= 1)
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t t = lane; t < P / 2; t += 32) {
-                uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;  // j is a power of two
-                bool asc = (i & k) == 0;
-                uint64_t ai = A[i], al = A[l];
-                uint32_t bi = B[i], bl = B[l];
-                bool gt = ai > al || (ai == al && bi > bl);
-                if (gt == asc) {
-                    A[i] = al;
-                    A[l] = ai;
-                    B[i] = bl;
-                    B[l] = bi;
-                }
-            }
-            __syncwarp();
-        }
-}
-
-__device__ void warp_bitonic_u64(uint64_t* A, uint32_t P, int lane) {
-    for (uint32_t k = 2; k <= P; k <<= 1)
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t t = lane; t < P / 2; t += 32) {
-                uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;  // j is a power of two
-                bool asc = (i & k) == 0;
-                uint64_t ai = A[i], al = A[l];
-                if ((ai > al) == asc) {
-                    A[i] = al;
-                    A[l] = ai;
-                }
-            }
-            __syncwarp();
-        }
-}
-
-__device__ void seedprep_warp(const BatchView& v, int32_t q, uint32_t P, uint64_t* A, uint64_t* E, uint32_t* B,
-                              uint32_t* D) {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u, le = lt | (1u << lane);
-    uint32_t m;
-    uint64_t kb;
-    int32_t S, halflen;
-    if (!seed_prologue(v, q, P, lane == 0, m, kb, S, halflen)) return;
-    const uint32_t Pm = max((uint32_t)2, (uint32_t)pow2_ceil(m));
-    for (uint32_t i = lane; i < Pm; i += 32) {
-        if (i < m) {
-            A[i] = v.km_h[kb + i];
-            uint32_t rs = v.km_rs[kb + i];
-            B[i] = ((0x3fffffffu - (rs >> 1)) << 1) | (rs & 1u);
-        } else {
-            A[i] = ~0ULL;
-            B[i] = 0xffffffffu;
-        }
-    }
-    __syncwarp();
-    warp_bitonic_ab(A, B, Pm, lane);  // (h asc, r desc): src/shmap/seeding.rs:28-34
-
-    // groups of equal hashes, compacted in place (group g lands at index g <= its elements)
-    uint32_t n_u = 0, open_start = 0;
-    uint64_t carry_h = 0;
-    for (uint32_t c0 = 0; c0 < m; c0 += 32) {
-        const uint32_t i = c0 + lane;
-        const bool valid = i < m;
-        const uint64_t h = valid ? A[i] : 0;
-        const uint32_t b = valid ? B[i] : 0;
-        const uint64_t hn = (i + 1 < m) ? A[i + 1] : 0;
-        const uint64_t hp_lane = __shfl_up_sync(0xffffffffu, h, 1);
-        const uint64_t hp = lane == 0 ? carry_h : hp_lane;
-        const bool first = valid && (i == 0 || h != hp);
-        const bool last = valid && (i + 1 == m || hn != h);
-        const unsigned fmask = __ballot_sync(0xffffffffu, first);
-        const uint32_t gid = n_u + __popc(fmask & le) - 1;
-        const unsigned fle = fmask & le;
-        const uint32_t start = fle ? c0 + (31 - __clz(fle)) : open_start;
-        __syncwarp();
-        if (first) A[gid] = h;
-        if (last) B[gid] = ((i - start + 1) << 1) | (b & 1u);  // representative: smallest r (seeding.rs:56)
-        n_u += __popc(fmask);
-        open_start = __shfl_sync(0xffffffffu, start, 31);
-        carry_h = __shfl_sync(0xffffffffu, h, 31);
-        __syncwarp();
-    }
-    if (v.P.os) S = (int32_t)n_u;  // mod.rs:732-736
-    // count() probes (index.rs:204-213); rarest first, stable over hash order (seeding.rs:71)
-    const uint32_t Pu = max((uint32_t)2, (uint32_t)pow2_ceil(n_u));
-    for (uint32_t g = lane; g < Pu; g += 32) {
-        if (g < n_u) {
-            uint32_t a, cnt;
-            idx_lookup(v.I, A[g], a, cnt);
-            D[g] = a;
-            E[g] = ((uint64_t)cnt << 32) | g;
-        } else {
-            E[g] = ~0ULL;
-        }
-    }
-    __syncwarp();
-    warp_bitonic_u64(E, Pu, lane);
-
-    // seeding prefix: seed i is processed iff sum(occs before i) < S (seeding.rs:101)
-    uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
-    uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
-    for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
-        const uint32_t i = c0 + lane;
-        const bool valid = i < n_u;
-        const uint64_t e = valid ? E[i] : 0;
-        const uint32_t g = (uint32_t)(e & 0xffffffffu), cnt = (uint32_t)(e >> 32);
-        const uint32_t os = valid ? B[g] : 0, occs = os >> 1;
-        const uint32_t oi = warp_inclusive_scan(occs);
-        const uint64_t ci = warp_inclusive_scan((uint64_t)(valid ? cnt : 0));
-        const uint32_t po = po_carry + oi - occs;
-        const uint64_t pc = pc_carry + ci - (valid ? cnt : 0);
-        if (valid) {
-            const uint64_t hg = A[g];
-            v.sd_h[kb + i] = hg;
-            v.sd_os[kb + i] = os;
-            v.sd_cnt[kb + i] = cnt;
-            v.sd_a[kb + i] = D[g];
-            v.sd_ooff[kb + i] = po;
-            if ((int64_t)po < (int64_t)S) {
-                v.sd_hpre[kb + i] = (uint32_t)pc;
-                l_np++;
-                l_s0 += occs;
-                l_sm += cnt;
-                l_max = max(l_max, cnt);
-                l_eb += seed_bucket_bound(v, D[g], cnt, halflen);
-            }
-            pht_insert(v, q, hg, i);
-        }
-        po_carry += __shfl_sync(0xffffffffu, oi, 31);
-        pc_carry += __shfl_sync(0xffffffffu, ci, 31);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        l_np += __shfl_xor_sync(0xffffffffu, l_np, o);
-        l_s0 += __shfl_xor_sync(0xffffffffu, l_s0, o);
-        l_sm += __shfl_xor_sync(0xffffffffu, l_sm, o);
-        l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
-        l_max = max(l_max, __shfl_xor_sync(0xffffffffu, l_max, o));
-    }
-    if (lane == 0) {
-        v.r_status[q] = ST_UNMAPPED;
-        v.r_nu[q] = (int32_t)n_u;
-        v.r_nproc[q] = (int32_t)l_np;
-        v.r_S[q] = S;
-        v.r_S0[q] = (int32_t)l_s0;
-        v.r_smatch[q] = (int64_t)l_sm;
-        v.r_maxseed[q] = (int32_t)l_max;
-        v.r_half[q] = halflen;
-        if (l_sm >= 0xffffffffULL) {
-            v.r_status[q] = ST_OVERFLOW;
-        } else {
-            v.hw[q] = l_sm;
-            v.bt_size[q] = l_sm ? max((uint64_t)16, pow2_ceil(2 * l_eb)) : 0;
-        }
-        atomicMax(&v.mx->m_max, m);
-        atomicMax(&v.mx->nu_max, n_u);
-        atomicMax(&v.mx->half_max, (uint32_t)halflen);
-        atomicAdd(&v.mx->kmers, (unsigned long long)m);
-        atomicAdd(&v.mx->distinct, (unsigned long long)n_u);
-        atomicAdd(&v.mx->proc_seeds, (unsigned long long)l_np);
-        atomicAdd(&v.mx->hits, (unsigned long long)l_sm);
-    }
-}
-
-__global__ void __launch_bounds__(256) k_seedprep_w(BatchView v, const int32_t* __restrict__ list,
-                                                    const uint32_t* __restrict__ n_list_d, uint32_t P) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    const int32_t n_list = (int32_t)*n_list_d;
-    const int wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    uint8_t* base = smem + (size_t)wib * SEEDW_BYTES_PER_ELEM * P;
-    uint64_t* A = (uint64_t*)base;
-    uint64_t* E = A + P;
-    uint32_t* B = (uint32_t*)(E + P);
-    uint32_t* D = B + P;
-    for (int32_t li = blockIdx.x * wpb + wib; li < n_list; li += gridDim.x * wpb) {
-        seedprep_warp(v, list[li], P, A, E, B, D);
-        __syncwarp();
-    }
-}
-
-// ------------------------------------------------------------------ K2 register form
-// Reads whose sketch has m <= 32 * EPL k-mers: one warp per read with the
-// k-mers in registers, EPL per lane (element e = r * 32 + lane). The bitonic
-// network's stages with partners in another lane are shuffles, the others
-// register compare-exchanges; every lane works on EPL independent elements,
-// so the sorts are not latency-bound. Shared memory holds only the groups:
-// hash GA[g] and occs << 1 | strand GB[g], 12 bytes per element.
-constexpr int SEEDR_WARPS = 8;
-
-template <int EPL>
-__device__ __forceinline__ void wreg_stage_lane(uint64_t (&A)[EPL], uint32_t (&B)[EPL], int R, uint32_t k, uint32_t j,
-                                                int lane) {
-    const bool lower = (lane & j) == 0;
-#pragma unroll
-    for (int r = 0; r < EPL; r++) {
-        if (r < R) {
-            const uint64_t pa = __shfl_xor_sync(0xffffffffu, A[r], j);
-            const uint32_t pb = __shfl_xor_sync(0xffffffffu, B[r], j);
-            const bool asc = ((((uint32_t)r << 5) | (uint32_t)lane) & k) == 0;
-            const bool pless = pa < A[r] || (pa == A[r] && pb < B[r]);
-            // the lower element of an ascending pair keeps the minimum, and so on
-            if (pless == (lower == asc)) {
-                A[r] = pa;
-                B[r] = pb;
-            }
-        }
-    }
-}
-
-template <int EPL, int JR>
-__device__ __forceinline__ void wreg_stage_reg(uint64_t (&A)[EPL], uint32_t (&B)[EPL], int R, uint32_t k) {
-    if constexpr (JR < EPL) {
-#pragma unroll
-        for (int r = 0; r < EPL; r++) {
-            if ((r & JR) == 0 && r < R) {  // R is a power of two above JR, so r | JR < R too
-                const int s2 = r | JR;
-                const bool asc = (((uint32_t)r << 5) & k) == 0;  // k >= 64: a bit of r
-                const bool gt = A[r] > A[s2] || (A[r] == A[s2] && B[r] > B[s2]);
-                if (gt == asc) {
-                    const uint64_t ta = A[r];
-                    A[r] = A[s2];
-                    A[s2] = ta;
-                    const uint32_t tb = B[r];
-                    B[r] = B[s2];
-                    B[s2] = tb;
-                }
-            }
-        }
-    }
-}
-
-// Ascending sort of the R * 32 elements (A, B) of a warp (R a power of two).
-template <int EPL>
-__device__ void wreg_sort(uint64_t (&A)[EPL], uint32_t (&B)[EPL], int R, int lane) {
-    const uint32_t n = (uint32_t)R << 5;
-    for (uint32_t k = 2; k <= n; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            if (j < 32) {
-                wreg_stage_lane<EPL>(A, B, R, k, j, lane);
-            } else {
-                switch (j >> 5) {
-                    case 1: wreg_stage_reg<EPL, 1>(A, B, R, k); break;
-                    case 2: wreg_stage_reg<EPL, 2>(A, B, R, k); break;
-                    case 4: wreg_stage_reg<EPL, 4>(A, B, R, k); break;
-                    case 8: wreg_stage_reg<EPL, 8>(A, B, R, k); break;
-                    case 16: wreg_stage_reg<EPL, 16>(A, B, R, k); break;
-                    default: break;
-                }
-            }
-        }
-    }
-}
-
-template <int EPL>
-__device__ void seedprep_reg(const BatchView& v, int32_t q, uint64_t* GA, uint32_t* GB) {
-    const int lane = threadIdx.x & 31;
-    const unsigned le = (2u << lane) - 1u;  // lanes <= this one
-    uint32_t m;
-    uint64_t kb;
-    int32_t S, halflen;
-    if (!seed_prologue(v, q, 32u * EPL, lane == 0, m, kb, S, halflen)) return;
-    const int R = (int)(max((uint32_t)32, (uint32_t)pow2_ceil(m)) >> 5);
-    uint64_t A[EPL];
-    uint32_t B[EPL];
-#pragma unroll
-    for (int r = 0; r < EPL; r++) {
-        const uint32_t e = ((uint32_t)r << 5) | (uint32_t)lane;
-        if (r < R && e < m) {
-            A[r] = v.km_h[kb + e];
-            const uint32_t rs = v.km_rs[kb + e];
-            B[r] = ((0x3fffffffu - (rs >> 1)) << 1) | (rs & 1u);
-        } else {
-            A[r] = ~0ULL;
-            B[r] = 0xffffffffu;
-        }
-    }
-    wreg_sort<EPL>(A, B, R, lane);  // (h asc, r desc): src/shmap/seeding.rs:28-34
-
-    // groups of equal hashes (src/shmap/seeding.rs:45-67)
-    uint32_t n_u = 0, open_start = 0;
-    uint64_t carry_h = 0;
-#pragma unroll
-    for (int r = 0; r < EPL; r++) {
-        if (r < R) {
-            const uint32_t e = ((uint32_t)r << 5) | (uint32_t)lane;
-            const bool valid = e < m;
-            const uint64_t h = A[r];
-            uint64_t hp = __shfl_up_sync(0xffffffffu, h, 1);
-            if (lane == 0) hp = carry_h;
-            uint64_t hn = __shfl_down_sync(0xffffffffu, h, 1);
-            const uint64_t nx = __shfl_sync(0xffffffffu, A[r + 1 < EPL ? r + 1 : r], 0);
-            if (lane == 31) hn = nx;  // element e + 1 sits in the next register (irrelevant past m - 1)
-            const bool first = valid && (e == 0 || h != hp);
-            const bool last = valid && (e + 1 == m || hn != h);
-            const unsigned fmask = __ballot_sync(0xffffffffu, first);
-            const unsigned fle = fmask & le;
-            const uint32_t gid = n_u + __popc(fle) - 1;
-            const uint32_t start = fle ? (((uint32_t)r << 5) + 31 - __clz(fle)) : open_start;
-            if (first) GA[gid] = h;
-            if (last) GB[gid] = ((e - start + 1) << 1) | (B[r] & 1u);  // representative: smallest r (seeding.rs:56)
-            n_u += __popc(fmask);
-            open_start = __shfl_sync(0xffffffffu, start, 31);
-            carry_h = __shfl_sync(0xffffffffu, h, 31);
-        }
-    }
-    __syncwarp();
-    if (v.P.os) S = (int32_t)n_u;  // mod.rs:732-736
-
-    // count() probes (index.rs:204-213); rarest first, stable over hash order
-    // (seeding.rs:71): keys cnt << 32 | g with the hit-list start alongside
-    const int Ru = (int)(max((uint32_t)32, (uint32_t)pow2_ceil(n_u)) >> 5);
-#pragma unroll
-    for (int r = 0; r < EPL; r++) {
-        if (r < Ru) {
-            const uint32_t g = ((uint32_t)r << 5) | (uint32_t)lane;
-            if (g < n_u) {
-                uint32_t a, cnt;
-                idx_lookup(v.I, GA[g], a, cnt);
-                A[r] = ((uint64_t)cnt << 32) | g;
-                B[r] = a;
-            } else {
-                A[r] = ~0ULL;
-                B[r] = 0xffffffffu;
-            }
-        }
-    }
-    wreg_sort<EPL>(A, B, Ru, lane);
-
-    // seeding prefix: seed i is processed iff sum(occs before i) < S (seeding.rs:101)
-    uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
-    uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
-#pragma unroll
-    for (int r = 0; r < EPL; r++) {
-        if (r < Ru) {
-            const uint32_t i = ((uint32_t)r << 5) | (uint32_t)lane;
-            const bool valid = i < n_u;
-            const uint32_t g = (uint32_t)(A[r] & 0xffffffffu), cnt = valid ? (uint32_t)(A[r] >> 32) : 0u;
-            const uint32_t os = valid ? GB[g] : 0u, occs = os >> 1;
-            const uint32_t oi = warp_inclusive_scan(occs);
-            const uint64_t ci = warp_inclusive_scan((uint64_t)cnt);
-            const uint32_t po = po_carry + oi - occs;
-            const uint64_t pc = pc_carry + ci - cnt;
-            if (valid) {
-                const uint64_t hg = GA[g];
-                const uint32_t a = B[r];
-                v.sd_h[kb + i] = hg;
-                v.sd_os[kb + i] = os;
-                v.sd_cnt[kb + i] = cnt;
-                v.sd_a[kb + i] = a;
-                v.sd_ooff[kb + i] = po;
-                if ((int64_t)po < (int64_t)S) {
-                    v.sd_hpre[kb + i] = (uint32_t)pc;
-                    l_np++;
-                    l_s0 += occs;
-                    l_sm += cnt;
-                    l_max = max(l_max, cnt);
-                    l_eb += seed_bucket_bound(v, a, cnt, halflen);
-                }
-                pht_insert(v, q, hg, i);
-            }
-            po_carry += __shfl_sync(0xffffffffu, oi, 31);
-            pc_carry += __shfl_sync(0xffffffffu, ci, 31);
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        l_np += __shfl_xor_sync(0xffffffffu, l_np, o);
-        l_s0 += __shfl_xor_sync(0xffffffffu, l_s0, o);
-        l_sm += __shfl_xor_sync(0xffffffffu, l_sm, o);
-        l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
-        l_max = max(l_max, __shfl_xor_sync(0xffffffffu, l_max, o));
-    }
-    if (lane == 0) {
-        v.r_status[q] = ST_UNMAPPED;
-        v.r_nu[q] = (int32_t)n_u;
-        v.r_nproc[q] = (int32_t)l_np;
-        v.r_S[q] = S;
-        v.r_S0[q] = (int32_t)l_s0;
-        v.r_smatch[q] = (int64_t)l_sm;
-        v.r_maxseed[q] = (int32_t)l_max;
-        v.r_half[q] = halflen;
-        if (l_sm >= 0xffffffffULL) {
-            v.r_status[q] = ST_OVERFLOW;
-        } else {
-            v.hw[q] = l_sm;
-            v.bt_size[q] = l_sm ? max((uint64_t)16, pow2_ceil(2 * l_eb)) : 0;
-        }
-        atomicMax(&v.mx->m_max, m);
-        atomicMax(&v.mx->nu_max, n_u);
-        atomicMax(&v.mx->half_max, (uint32_t)halflen);
-        atomicAdd(&v.mx->kmers, (unsigned long long)m);
-        atomicAdd(&v.mx->distinct, (unsigned long long)n_u);
-        atomicAdd(&v.mx->proc_seeds, (unsigned long long)l_np);
-        atomicAdd(&v.mx->hits, (unsigned long long)l_sm);
-    }
-}
-
-template <int EPL>
-__global__ void __launch_bounds__(SEEDR_WARPS * 32) k_seedprep_r(BatchView v, const int32_t* __restrict__ list,
-                                                                 const uint32_t* __restrict__ n_list) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    const int wib = threadIdx.x >> 5;
-    uint64_t* GA = (uint64_t*)smem + (size_t)wib * 32 * EPL;
-    uint32_t* GB = (uint32_t*)((uint64_t*)smem + (size_t)SEEDR_WARPS * 32 * EPL) + (size_t)wib * 32 * EPL;
-    const int32_t n = (int32_t)*n_list;
-    for (int32_t li = blockIdx.x * SEEDR_WARPS + wib; li < n; li += gridDim.x * SEEDR_WARPS) {
-        seedprep_reg<EPL>(v, list[li], GA, GB);
-        __syncwarp();
-    }
-}
-
 // Seed-preparation bins by the actual sketch size m of each read (reads past
 // their k-mer capacity go to bin 0, whose prologue marks them overflowed):
-// m <= 256 and m <= 512 register forms, m <= 1024 warp with shared arrays,
-// m <= 4096 CTA in shared memory, larger CTA with global scratch.
+// m <= 256, 512 and 1024 the counting form (a warp per read), m <= 4096 a
+// CTA per read in shared memory, larger a CTA with global scratch.
 constexpr int N_SEED_BINS = 5;
 __global__ void k_seed_bins(BatchView v, int32_t* __restrict__ lists, uint32_t* __restrict__ bin_cnt) {
     const int lane = threadIdx.x & 31;
@@ -1090,7 +681,7 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
             v.r_status[q] = ST_OVERFLOW;
         } else {
             v.hw[q] = l_sm;
-            v.bt_size[q] = l_sm ? max((uint64_t)16, pow2_ceil(2 * l_eb)) : 0;
+            v.bt_size[q] = l_sm ? bt_slots(v, l_eb) : 0;
         }
         atomicMax(&v.mx->m_max, m);
         atomicMax(&v.mx->nu_max, n_u);
@@ -1179,13 +770,20 @@ __device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t se
     const uint64_t base = v.bt_off[q];
     const uint64_t mask = v.bt_off[q + 1] - base - 1;
     const unsigned long long key = ((unsigned long long)(uint32_t)seg << 32) | (uint32_t)bb;
+    if (v.r_flags[q]) return;  // the read is mapped again
     uint64_t i = mix64(key) & mask;
     BSlot* s;
-    for (;;) {
+    for (uint64_t probe = 0;; probe++) {
+        if (probe > mask) {  // every slot taken by other buckets
+            atomicOr(v.r_flags + q, 1u);
+            return;
+        }
         s = v.bt + base + i;
         unsigned long long prev = atomicCAS(&s->key, EMPTY_KEY, key);
         if (prev == EMPTY_KEY) {  // a new bucket: list it for k_bscan (seeded_buckets, mod.rs:794)
-            v.bt_list[base + atomicAdd(v.r_seeded + q, 1u)] = (uint32_t)i;
+            const uint32_t at = atomicAdd(v.r_seeded + q, 1u);  // < slots: every listed bucket holds a slot
+            v.bt_list[base + at] = (uint32_t)i;
+            if ((uint64_t)at + 1 > ((mask + 1) >> 1) + ((mask + 1) >> 2)) atomicOr(v.r_flags + q, 1u);  // load > 3/4
             break;
         }
         if (prev == key) break;
@@ -1313,7 +911,9 @@ __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
     }
 }
 
-__global__ void k_bt_init(BSlot* bt, uint64_t n) {
+// Empties the first *total slots (the total is read on the device).
+__global__ void k_bt_init(BSlot* bt, const uint64_t* __restrict__ total) {
+    const uint64_t n = *total;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         BSlot s;
         s.key = EMPTY_KEY;
@@ -1332,6 +932,10 @@ __global__ void __launch_bounds__(256) k_bscan(BatchView v) {
     for (int32_t q = wid; q < v.n; q += nwarps) {
         const uint32_t nb = v.r_seeded[q];
         if (nb == 0) continue;
+        if (v.r_flags[q]) {  // its capped bucket table filled up: mapped again with the full bound
+            if (lane == 0) v.r_status[q] = ST_OVERFLOW;
+            continue;
+        }
         const uint64_t base = v.bt_off[q];
         if (lane == 0) atomicAdd(&v.mx->buckets, (unsigned long long)nb);
         for (uint32_t j = lane; j < nb; j += 32) {
@@ -1900,7 +1504,7 @@ struct MapScratch {
     DevBuf<int32_t> retry_idx;
     DevBuf<uint64_t> km_h, sd_h, pht_key, hw, hw_off, bt_size, bt_off;
     DevBuf<uint32_t> kcnt, km_rs, sd_a, sd_cnt, sd_os, sd_hpre, sd_ooff, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
-        cidx, sort_scr, ovf_list;
+        cidx, sort_scr, ovf_list, r_flags;
     DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
     DevBuf<BSlot> bt;
@@ -1925,6 +1529,7 @@ MapCtx* mapctx_create(int device, size_t hbm_budget) {
     SHM_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
     SHM_CUDA(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
     for (auto& e : c->copied) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : c->sketched) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     c->scr = new MapScratch();
     return c;
 }
@@ -1941,6 +1546,8 @@ void mapctx_destroy(MapCtx* c) {
     if (c->h_slots) cudaFreeHost(c->h_slots);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (auto& e : c->copied)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->sketched)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->side_stream) {
@@ -1980,6 +1587,8 @@ struct BatchPlan {
     uint64_t* pht_off;     // n+1
     uint32_t n_cap_512 = 0, n_cap_1024 = 0, n_cap_4096 = 0;  // reads whose capacity exceeds 512 / 1024 / 4096
     uint32_t P_g = 0;                          // power of two >= every capacity above 4096
+    uint64_t max_cap = 0;                      // largest k-mer capacity of a read
+    int64_t max_len = 0;                       // longest read
     size_t bytes = 0;
     static size_t layout(int32_t n) { return 4 * ((size_t)n + 1) * 8; }
     void carve(uint8_t* base, int32_t n) {
@@ -2005,12 +1614,15 @@ static uint8_t* pinned_stage(MapCtx* c, size_t bytes) {
     return c->h_pinned;
 }
 
-// caps = null: capacities from the estimate; else caps[i] k-mers for read i
-// (the counts a previous pass found).
-static void plan_batch(MapCtx* c, const int64_t* h_offs, int32_t n, int32_t k, double h_frac, const uint32_t* caps,
-                       BatchPlan& bp) {
-    bp.carve(pinned_stage(c, BatchPlan::layout(n)), n);
+// Written into pinned memory at h_plan (BatchPlan::layout(n) bytes). caps =
+// null: capacities from the estimate; else caps[i] k-mers for read i (the
+// counts a previous pass found).
+static void plan_batch(uint8_t* h_plan, const int64_t* h_offs, int32_t n, int32_t k, double h_frac,
+                       const uint32_t* caps, BatchPlan& bp) {
+    bp.carve(h_plan, n);
     bp.P_g = 0;
+    bp.max_cap = 0;
+    bp.max_len = 0;
     bp.n_cap_512 = bp.n_cap_1024 = bp.n_cap_4096 = 0;
     bp.roff[0] = 0;
     bp.chunk_off[0] = 0;
@@ -2023,6 +1635,8 @@ static void plan_batch(MapCtx* c, const int64_t* h_offs, int32_t n, int32_t k, d
         bp.chunk_off[i + 1] = bp.chunk_off[i] + (nw > 0 ? (uint64_t)((nw + SKETCH_WIN - 1) / SKETCH_WIN) : 0);
         const uint64_t cap = caps ? (uint64_t)caps[i] : kmer_cap(nw, h_frac);
         bp.kcap_off[i + 1] = bp.kcap_off[i] + cap;
+        bp.max_cap = std::max(bp.max_cap, cap);
+        bp.max_len = std::max(bp.max_len, L);
         bp.pht_off[i + 1] = bp.pht_off[i] + std::max<uint64_t>(16, pow2_host(2 * cap));
         if (cap > 512) bp.n_cap_512++;
         if (cap > 1024) bp.n_cap_1024++;
@@ -2046,7 +1660,25 @@ struct BatchSlot {
     uint32_t* ovf;
     int32_t i0, n;
     int64_t bases;
+    uint32_t job_cap;  // set by run_batch: more jobs than this and the batch is mapped again
 };
+
+// The bucket tables of a batch mapped without waiting for its sizes get at
+// most 512 slots a read (reads needing more are mapped again), and at most 64
+// bucket jobs a read on average (a batch with more is mapped again). The
+// environment variables SHMAP_BT_FAST_SLOTS (a power of two >= 16) and
+// SHMAP_FAST_JOB_CAP lower them, so that tests reach both fallbacks.
+static uint64_t fast_bt_slots() {
+    const char* e = std::getenv("SHMAP_BT_FAST_SLOTS");
+    const uint64_t v = e ? std::strtoull(e, nullptr, 10) : 0;
+    return (v >= 16 && (v & (v - 1)) == 0 && v <= 512) ? v : 512;
+}
+static uint32_t fast_job_cap(int32_t n) {
+    const char* e = std::getenv("SHMAP_FAST_JOB_CAP");
+    const uint64_t v = e ? std::strtoull(e, nullptr, 10) : 0;
+    const uint64_t cap = std::min<uint64_t>(fast_bt_slots() * (uint64_t)n + 1, 64 * (uint64_t)n + (1u << 20));
+    return (uint32_t)(v >= 1 ? std::min(v, cap) : cap);
+}
 
 // Pinned per-call result slots for batches of the given sizes.
 static std::vector<BatchSlot> batch_slots(MapCtx* c, const std::vector<std::pair<int32_t, int32_t>>& b,
@@ -2105,13 +1737,13 @@ static void collect_batch(MapCtx* c, const BatchSlot& sl, std::vector<Overflow>&
 // is queued, and the batch's results reach `sl` when the stream drains
 // (collect_batch then lists the reads that overflowed a capacity).
 static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
-                      const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps, StageTimer& T,
-                      const BatchSlot& sl) {
+                      const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps, bool exact,
+                      uint8_t* h_plan, StageTimer& T, BatchSlot& sl) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
     HostClock H;
     BatchPlan bp;
-    plan_batch(c, h_offs, n, p.k, p.h_frac, caps, bp);
+    plan_batch(h_plan, h_offs, n, p.k, p.h_frac, caps, bp);
     H.mark("plan");
     if (!S.luts || S.luts_k != p.k) {
         if (S.luts) SHM_CUDA(cudaFree(S.luts));
@@ -2119,10 +1751,9 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         S.luts_k = p.k;
     }
     const uint64_t kcap = bp.kcap_off[(size_t)n], phtn = bp.pht_off[(size_t)n];
-    // the plan goes up in one copy from pinned memory; the pinned block is
-    // rewritten only by the next batch, after this one's first synchronize
+    // the plan goes up in one copy from its own pinned block
     S.plan.reserve(bp.bytes);
-    SHM_CUDA(cudaMemcpyAsync(S.plan.p, c->h_pinned, bp.bytes, cudaMemcpyHostToDevice, s));
+    SHM_CUDA(cudaMemcpyAsync(S.plan.p, h_plan, bp.bytes, cudaMemcpyHostToDevice, s));
     BatchPlan dp;
     dp.carve(S.plan.p, n);
     S.kcnt.reserve((size_t)n);
@@ -2139,6 +1770,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     S.r_i32.reserve((size_t)n * 8);
     S.r_smatch.reserve((size_t)n);
     S.r_seeded.reserve((size_t)n);
+    S.r_flags.reserve((size_t)n);
     S.hw.reserve((size_t)n);
     S.hw_off.reserve((size_t)n + 1);
     S.bt_size.reserve((size_t)n);
@@ -2152,6 +1784,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     SHM_CUDA(cudaMemsetAsync(S.kcnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.pht_val.p, 0xff, sizeof(uint32_t) * phtn, s));
     SHM_CUDA(cudaMemsetAsync(S.r_seeded.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    SHM_CUDA(cudaMemsetAsync(S.r_flags.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.ccnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.ccur.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.n_jobs.p, 0, sizeof(uint32_t), s));
@@ -2207,6 +1840,8 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     v.r_maxseed = ri + 7 * (size_t)n;
     v.r_smatch = S.r_smatch.p;
     v.r_seeded = S.r_seeded.p;
+    v.r_flags = S.r_flags.p;
+    v.bt_cap = exact ? ((uint64_t)1 << 62) : fast_bt_slots();
     v.hw = S.hw.p;
     v.hw_off = S.hw_off.p;
     v.bt_size = S.bt_size.p;
@@ -2236,6 +1871,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     T.begin(STG_SKETCH);
     launch_sketch(SK_APPEND, a, S.luts, s);
     T.end();
+    if (c->sketch_done) SHM_CUDA(cudaEventRecord(c->sketch_done, s));  // the batch's bytes are free again
 
     // K2: bins by the actual sketch sizes, then one launch per bin (each
     // reads its own count on the device; empty bins return at once)
@@ -2306,84 +1942,97 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     exclusive_scan_u64(S.hw.p, S.hw_off.p, (size_t)n, s);
     exclusive_scan_u64(S.bt_size.p, S.bt_off.p, (size_t)n, s);
     HostReads& R = *sl.R;
-    SHM_CUDA(cudaMemcpyAsync(&R.totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    SHM_CUDA(cudaMemcpyAsync(&R.totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    SHM_CUDA(cudaMemcpyAsync(&R.hm, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
-    H.mark("enq1");
-    SHM_CUDA(cudaStreamSynchronize(s));
-    H.mark("sync1");
-    const uint64_t hw_total = R.totals[0], bt_total = R.totals[1];
-    const BatchMax hm = R.hm;
     const bool debug = std::getenv("SHMAP_DEBUG") != nullptr;
-    if (debug) {
-        std::fprintf(stderr, "[shmap] batch n=%d kcap=%llu hw_total=%llu bt_total=%llu m_max=%u nu_max=%u half_max=%u\n",
-                     n, (unsigned long long)kcap, (unsigned long long)hw_total, (unsigned long long)bt_total, hm.m_max,
-                     hm.nu_max, hm.half_max);
-        if (n <= 8) {
-            std::vector<int32_t> ri((size_t)n * 8);
-            std::vector<uint32_t> kc((size_t)n);
-            std::vector<uint64_t> hw((size_t)n), bs((size_t)n);
-            SHM_CUDA(cudaMemcpy(ri.data(), S.r_i32.p, sizeof(int32_t) * ri.size(), cudaMemcpyDeviceToHost));
-            SHM_CUDA(cudaMemcpy(kc.data(), S.kcnt.p, sizeof(uint32_t) * kc.size(), cudaMemcpyDeviceToHost));
-            SHM_CUDA(cudaMemcpy(hw.data(), S.hw.p, sizeof(uint64_t) * hw.size(), cudaMemcpyDeviceToHost));
-            SHM_CUDA(cudaMemcpy(bs.data(), S.bt_size.p, sizeof(uint64_t) * bs.size(), cudaMemcpyDeviceToHost));
-            for (int32_t q = 0; q < n; q++)
-                std::fprintf(stderr,
-                             "[shmap]  read %d kcnt=%u status=%d m=%d nu=%d nproc=%d S=%d S0=%d half=%d maxseed=%d "
-                             "hw=%llu bt=%llu\n",
-                             q, kc[q], ri[q], ri[n + q], ri[2 * n + q], ri[3 * n + q], ri[4 * n + q], ri[5 * n + q],
-                             ri[6 * n + q], ri[7 * n + q], (unsigned long long)hw[q], (unsigned long long)bs[q]);
+    // Sizes after seeding. Exact mode: wait for the bucket tables' total and
+    // the batch maxima. Otherwise bounds the host knows: capped tables, the
+    // largest capacity and read.
+    uint64_t bt_slots_alloc;
+    uint32_t job_cap, m_max, nu_max, half_max;
+    if (exact || debug) {
+        SHM_CUDA(cudaMemcpyAsync(&R.totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaMemcpyAsync(&R.totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaMemcpyAsync(&R.hm, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
+        H.mark("enq1");
+        SHM_CUDA(cudaStreamSynchronize(s));
+        H.mark("sync1");
+        if (debug) {
+            std::fprintf(stderr,
+                         "[shmap] batch n=%d kcap=%llu hw_total=%llu bt_total=%llu m_max=%u nu_max=%u half_max=%u\n", n,
+                         (unsigned long long)kcap, (unsigned long long)R.totals[0], (unsigned long long)R.totals[1],
+                         R.hm.m_max, R.hm.nu_max, R.hm.half_max);
+            if (n <= 8) {
+                std::vector<int32_t> ri((size_t)n * 8);
+                std::vector<uint32_t> kc((size_t)n);
+                std::vector<uint64_t> hw((size_t)n), bs((size_t)n);
+                SHM_CUDA(cudaMemcpy(ri.data(), S.r_i32.p, sizeof(int32_t) * ri.size(), cudaMemcpyDeviceToHost));
+                SHM_CUDA(cudaMemcpy(kc.data(), S.kcnt.p, sizeof(uint32_t) * kc.size(), cudaMemcpyDeviceToHost));
+                SHM_CUDA(cudaMemcpy(hw.data(), S.hw.p, sizeof(uint64_t) * hw.size(), cudaMemcpyDeviceToHost));
+                SHM_CUDA(cudaMemcpy(bs.data(), S.bt_size.p, sizeof(uint64_t) * bs.size(), cudaMemcpyDeviceToHost));
+                for (int32_t q = 0; q < n; q++)
+                    std::fprintf(stderr,
+                                 "[shmap]  read %d kcnt=%u status=%d m=%d nu=%d nproc=%d S=%d S0=%d half=%d maxseed=%d "
+                                 "hw=%llu bt=%llu\n",
+                                 q, kc[q], ri[q], ri[n + q], ri[2 * n + q], ri[3 * n + q], ri[4 * n + q], ri[5 * n + q],
+                                 ri[6 * n + q], ri[7 * n + q], (unsigned long long)hw[q], (unsigned long long)bs[q]);
+            }
         }
     }
+    if (exact) {
+        bt_slots_alloc = R.totals[1];
+        // a job per touched bucket-table slot at most: the total bounds the jobs
+        if (bt_slots_alloc + 1 > (uint64_t)UINT32_MAX) throw shm_cuda_error(cudaErrorMemoryAllocation);
+        job_cap = (uint32_t)(bt_slots_alloc + 1);
+        m_max = R.hm.m_max;
+        nu_max = R.hm.nu_max;
+        half_max = R.hm.half_max;
+    } else {
+        bt_slots_alloc = v.bt_cap * (uint64_t)n;
+        job_cap = fast_job_cap(n);
+        m_max = nu_max = (uint32_t)bp.max_cap;  // m <= capacity, distinct seeds <= m
+        half_max = p.abs_pos ? (uint32_t)bp.max_len : (uint32_t)bp.max_cap;
+    }
+    sl.job_cap = job_cap;
+    const int wide = grid_for((size_t)1 << 40, 256, 8);  // a full grid for kernels that read their counts on the device
 
-    S.bt.reserve(bt_total + 1);
-    S.bt_list.reserve(bt_total + 1);
+    S.bt.reserve(bt_slots_alloc + 1);
+    S.bt_list.reserve(bt_slots_alloc + 1);
     v.bt = S.bt.p;
     v.bt_list = S.bt_list.p;
-    if (bt_total) {
-        T.begin(STG_AUX);
-        k_bt_init<<<grid_for(bt_total, 256), 256, 0, s>>>(S.bt.p, bt_total);
-        SHM_CUDA(cudaGetLastError());
-        T.end();
-    }
-    if (hw_total) {
-        T.begin(STG_CONTRIB);
-        k_contrib<<<grid_for(hw_total, 256, 8), 256, 0, s>>>(v);
-        SHM_CUDA(cudaGetLastError());
-        T.end();
-    }
-    // a job per touched bucket-table slot at most: bt_total bounds the jobs
-    if (bt_total + 1 > (uint64_t)UINT32_MAX) throw shm_cuda_error(cudaErrorMemoryAllocation);
-    const uint32_t job_cap = (uint32_t)(bt_total + 1);
+    T.begin(STG_AUX);
+    k_bt_init<<<wide, 256, 0, s>>>(S.bt.p, S.bt_off.p + n);
+    SHM_CUDA(cudaGetLastError());
+    T.end();
+    T.begin(STG_CONTRIB);
+    k_contrib<<<wide, 256, 0, s>>>(v);
+    SHM_CUDA(cudaGetLastError());
+    T.end();
     S.jobs.reserve(job_cap);
     v.jobs = S.jobs.p;
     v.job_cap = job_cap;
-    if (bt_total) {
-        T.begin(STG_BSCAN);
-        k_bscan<<<grid_for((size_t)n * 32, 256, 8), 256, 0, s>>>(v);
-        SHM_CUDA(cudaGetLastError());
-        T.end();
-    }
+    T.begin(STG_BSCAN);
+    k_bscan<<<grid_for((size_t)n * 32, 256, 8), 256, 0, s>>>(v);
+    SHM_CUDA(cudaGetLastError());
+    T.end();
     if (!p.no_bucket_pruning) {
         T.begin(STG_EXTEND);
-        k_extend<<<grid_for((size_t)job_cap * 32, 256, 8), 256, 0, s>>>(v);
+        k_extend<<<wide, 256, 0, s>>>(v);
         SHM_CUDA(cudaGetLastError());
         T.end();
     }
     exclusive_scan_u32(S.ccnt.p, S.coff.p, (size_t)n, s);
-    S.cidx.reserve(job_cap + 1);
+    S.cidx.reserve((size_t)job_cap + 1);
     S.sweep_scr.reserve(2 * (size_t)job_cap + 2);
     v.cidx = S.cidx.p;
     T.begin(STG_AUX);
-    k_cidx<<<grid_for(job_cap, 256, 8), 256, 0, s>>>(v);
+    k_cidx<<<wide, 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
     T.end();
 
     RefScratch rsc{};
-    rsc.nu_max = hm.nu_max + 1;
-    rsc.wmax = 2 * hm.half_max + 2;
-    rsc.per_warp = (size_t)rsc.nu_max + 2 * ((size_t)rsc.wmax + 1) + (size_t)hm.m_max + 1;
-    size_t warps = (size_t)grid_for((size_t)job_cap * 32, 256, 8) * 8;
+    rsc.nu_max = nu_max + 1;
+    rsc.wmax = 2 * half_max + 2;
+    rsc.per_warp = (size_t)rsc.nu_max + 2 * ((size_t)rsc.wmax + 1) + (size_t)m_max + 1;
+    size_t warps = (size_t)wide * 8;
     const size_t budget_ints = (size_t)1 << 28;  // 1 GiB of refinement scratch at most
     while (warps > 8 && warps * rsc.per_warp > budget_ints) warps /= 2;
     S.ref_scr.reserve(warps * rsc.per_warp);
@@ -2417,7 +2066,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
                              j.t_l, j.t_r, j.inter, j.same);
         }
     }
-    H.print(caps ? "retry-batch" : "batch", n);
+    H.print(exact ? "exact-batch" : "batch", n);
 }
 
 // Batch limits: device-resident reads in few large batches; host reads in
@@ -2453,8 +2102,10 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
     S.retry_out.reserve(ovf.size());
     StageTimer T(c);
     const std::vector<std::pair<int32_t, int32_t>> one{{0, (int32_t)ovf.size()}};
-    const std::vector<BatchSlot> sl = batch_slots(c, one, o.data());
-    run_batch(c, ix, p, S.retry_seq.p, o.data(), (int32_t)ovf.size(), S.retry_out.p, caps.data(), T, sl[0]);
+    std::vector<BatchSlot> sl = batch_slots(c, one, o.data());
+    uint8_t* h_plan = pinned_stage(c, BatchPlan::layout((int32_t)ovf.size()));
+    run_batch(c, ix, p, S.retry_seq.p, o.data(), (int32_t)ovf.size(), S.retry_out.p, caps.data(), true, h_plan, T,
+              sl[0]);
     SHM_CUDA(cudaStreamSynchronize(s));
     T.collect();
     std::vector<Overflow> again;
@@ -2492,18 +2143,43 @@ static std::vector<std::pair<int32_t, int32_t>> cut_batches(const int64_t* offs,
     return b;
 }
 
+// Pinned plan blocks for every batch of a call (batches are queued without
+// waiting, so each keeps its own until the stream drains).
+static std::vector<uint8_t*> plan_blocks(MapCtx* c, const std::vector<std::pair<int32_t, int32_t>>& b) {
+    size_t total = 0;
+    for (auto [i, j] : b) total += (BatchPlan::layout(j - i) + 63) / 64 * 64;
+    uint8_t* base = pinned_stage(c, total);
+    std::vector<uint8_t*> out;
+    for (auto [i, j] : b) {
+        out.push_back(base);
+        base += (BatchPlan::layout(j - i) + 63) / 64 * 64;
+    }
+    return out;
+}
+
 void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
                 int32_t n, shm_map_record* d_out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
     const auto batches = cut_batches(h_offs, n, plain, DEV_BATCH_READS, DEV_BATCH_BASES);
-    const std::vector<BatchSlot> slots = batch_slots(c, batches, h_offs);
+    std::vector<BatchSlot> slots = batch_slots(c, batches, h_offs);
+    const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
+    // every batch is queued without a wait; the sketch reads exactly the
+    // batch's bytes, at any alignment
     for (size_t b = 0; b < batches.size(); b++) {
         const auto [i, j] = batches[b];
-        // the sketch reads exactly the batch's bytes, at any alignment
-        run_batch(c, ix, p, d_seq + (h_offs[i] - h_offs[0]), h_offs + i, j - i, d_out + i, nullptr, T, slots[b]);
+        run_batch(c, ix, p, d_seq + (h_offs[i] - h_offs[0]), h_offs + i, j - i, d_out + i, nullptr, false, plans[b], T,
+                  slots[b]);
     }
     SHM_CUDA(cudaStreamSynchronize(c->stream));
+    // a batch with more bucket jobs than its capacity is mapped again with exact sizes
+    for (size_t b = 0; b < batches.size(); b++) {
+        if (slots[b].R->nj <= slots[b].job_cap) continue;
+        const auto [i, j] = batches[b];
+        run_batch(c, ix, p, d_seq + (h_offs[i] - h_offs[0]), h_offs + i, j - i, d_out + i, nullptr, true, plans[b], T,
+                  slots[b]);
+        SHM_CUDA(cudaStreamSynchronize(c->stream));
+    }
     T.collect();
     std::vector<Overflow> ovf_all;
     for (const BatchSlot& sl : slots) collect_batch(c, sl, ovf_all);
@@ -2518,8 +2194,9 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
 }
 
 // Host-buffer form. Batch b+1's bytes go up on the copy stream while batch b
-// is mapped (two device buffers), so the transfer of the reads overlaps the
-// mapping when `seqs` is pinned; records come back batch by batch.
+// is mapped (two device buffers, each reused once the sketch of the batch
+// before has read it), so the transfer of the reads overlaps the mapping when
+// `seqs` is pinned; records come back batch by batch.
 void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
               int32_t n, shm_map_record* out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
@@ -2535,36 +2212,48 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     S.seqb[0].reserve((size_t)max_nb + 32);
     S.seqb[1].reserve((size_t)max_nb + 32);
     S.out.reserve((size_t)std::max(max_n, 1));
-    auto send = [&](size_t b) {  // on the copy stream
+    auto send = [&](size_t b) {  // on the copy stream, after the sketch that last read the buffer
         const auto [i, j] = batches[b];
         const int64_t nb = offs[j] - offs[i];
         DevBuf<uint8_t>& buf = S.seqb[b & 1];
+        SHM_CUDA(cudaStreamWaitEvent(c->copy_stream, c->sketched[b & 1], 0));
         SHM_CUDA(cudaMemsetAsync(buf.p + nb, 0, 32, c->copy_stream));
         SHM_CUDA(cudaMemcpyAsync(buf.p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, c->copy_stream));
         SHM_CUDA(cudaEventRecord(c->copied[b & 1], c->copy_stream));
     };
-    const std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
+    std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
+    const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
     HostClock H;
     if (!batches.empty()) send(0);
-    H.mark("send0");
     for (size_t b = 0; b < batches.size(); b++) {
         const auto [i, j] = batches[b];
         SHM_CUDA(cudaStreamWaitEvent(s, c->copied[b & 1], 0));
-        // the other buffer's last reader (batch b-1) has finished: run_batch waited for
-        // this batch's bucket-table sizes, which come after all of batch b-1's work
         if (b + 1 < batches.size()) send(b + 1);
-        H.mark("send");
-        run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr, T, slots[b]);
-        H.mark("run");
+        c->sketch_done = c->sketched[b & 1];
+        run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b]);
+        c->sketch_done = nullptr;
         SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s));
     }
+    H.mark("enqueue");
     SHM_CUDA(cudaStreamSynchronize(s));
+    H.mark("drain");
+    // a batch with more bucket jobs than its capacity is mapped again with exact sizes
+    for (size_t b = 0; b < batches.size(); b++) {
+        if (slots[b].R->nj <= slots[b].job_cap) continue;
+        const auto [i, j] = batches[b];
+        const int64_t nb = offs[j] - offs[i];
+        SHM_CUDA(cudaMemsetAsync(S.seqb[0].p + nb, 0, 32, s));
+        SHM_CUDA(cudaMemcpyAsync(S.seqb[0].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, s));
+        run_batch(c, ix, p, S.seqb[0].p, offs + i, j - i, S.out.p, nullptr, true, plans[b], T, slots[b]);
+        SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
+                                 s));
+        SHM_CUDA(cudaStreamSynchronize(s));
+    }
     T.collect();
     std::vector<Overflow> ovf_all;
     for (const BatchSlot& sl : slots) collect_batch(c, sl, ovf_all);
-    H.mark("sync");
     if (!ovf_all.empty()) {
         DevBuf<shm_map_record>& all = S.retry_all;
         all.reserve((size_t)n);

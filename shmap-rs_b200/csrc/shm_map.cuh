@@ -45,6 +45,8 @@ struct MapCtx {
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;  // host-to-device copies of the next batch
     cudaEvent_t copied[2] = {nullptr, nullptr};
+    cudaEvent_t sketched[2] = {nullptr, nullptr};  // the sketch of the batch in each buffer has read it
+    cudaEvent_t sketch_done = nullptr;             // recorded by run_batch after its sketch when set
     cudaStream_t side_stream = nullptr;  // seed preparation of the few reads with large sketches
     cudaEvent_t fork = nullptr, join = nullptr;
     MapScratch* scr = nullptr;
@@ -58,7 +60,6 @@ struct MapCtx {
     // work counters (always on): see WORK_NAMES
     int64_t work[16] = {};
     int seed_smem_set = 0;   // dynamic shared memory the seed kernels have been allowed so far
-    int seedw_smem_set = 0;
     int seedc_smem_set = 0;
     // stage timing
     bool timing = false;

@@ -252,3 +252,30 @@ def test_device_resident_entry(gpu_ctx, uniform):
     rec = d_out.cpu().numpy().view(sb.RECORD_DTYPE)
     want = o.map_reads(O.params(k=25, h_frac=0.01, theta=0.4), seq, offs, threads=8)
     assert not record_mismatches(rec, want)
+
+
+@pytest.mark.parametrize("env", [{"SHMAP_BT_FAST_SLOTS": "16"}, {"SHMAP_FAST_JOB_CAP": "7"},
+                                 {"SHMAP_BT_FAST_SLOTS": "32", "SHMAP_FAST_JOB_CAP": "40"}])
+def test_capacity_fallbacks(gpu_ctx, human_small, env, monkeypatch):
+    """Batches are queued without waiting for their sizes: bucket tables are
+    capped per read (a read whose table fills is mapped again with the full
+    bound) and bucket jobs per batch (a batch with more is mapped again with
+    exact sizes). Tiny caps force both paths; the records must not change."""
+    for key, val in env.items():
+        monkeypatch.setenv(key, val)
+    gen = human_small
+    names, seq, offs = gen.reads(synth.scaled(synth.READS["hifi"], 200 / synth.READS["hifi"].n_reads))
+    reads = [(names[i], seq[offs[i]:offs[i + 1]].tobytes()) for i in range(len(names))]
+    g, o = _both_indexes(gpu_ctx, gen.records(), 25, 0.01)
+    rec, paf = _compare_mapping(g, o, reads, k=25, h_frac=0.01, theta=0.4)
+    assert (rec["status"] == 0).mean() > 0.5
+    import torch
+
+    p = sb.Params(k=25, h_frac=0.01, theta=0.4)
+    pseq, poffs = pack([s for _, s in reads])
+    d_seq = torch.empty(len(pseq) + 32, dtype=torch.uint8, device="cuda")
+    d_seq[: len(pseq)].copy_(torch.from_numpy(np.ascontiguousarray(pseq)))
+    d_out = torch.empty(len(reads) * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    g.map_reads_device(p, d_seq.data_ptr(), poffs, d_out.data_ptr())
+    torch.cuda.synchronize()
+    assert not record_mismatches(d_out.cpu().numpy().view(sb.RECORD_DTYPE), rec)
