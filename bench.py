@@ -98,12 +98,18 @@ class ClockSampler:
         self.p = None
 
     def start(self):
+        """Starts sampling and returns once the first sample is written: nvidia-smi's
+        own start-up stays out of the timed region."""
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
                                        "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 10 and self.p.poll() is None and os.path.getsize(self.f.name) == 0:
+            time.sleep(0.02)
 
     def stop(self):
         if self.p is None:
@@ -151,13 +157,14 @@ def make_workload(name: str, rank: int, scale: float):
 
 
 def algorithmic_bytes(stage: str, w: dict) -> tuple[float, str]:
-    """Algorithmic bytes of one stage over the counted work (the per-unit figures
-    of the measurement plan): see DESIGN.md."""
+    """Bytes a stage must move at the least, over the counted work: its inputs
+    read once and its outputs written once."""
     if stage == "sketch":
-        return (w["bases"] * (1.0 / 4 + 1.0 / 8) + 16.0 * w["kmers"],
-                "ceil(L/4)+ceil(L/8) input bytes per base (2-bit + N-mask) + 16 B per selected k-mer")
-    if stage in ("seedprep",):
-        return 32.0 * w["distinct_seeds"] + 12.0 * w["kmers"], "32 B per count() probe + 12 B per read k-mer"
+        return (1.0 * w["bases"] + 12.0 * w["kmers"],
+                "1 B per read base + 12 B per selected k-mer (hash, r << 1 | strand)")
+    if stage == "seedprep":
+        return (12.0 * w["kmers"] + 68.0 * w["distinct_seeds"],
+                "12 B per read k-mer + 32 B per count() probe + 36 B of seed record and probe-table entry per seed")
     if stage in ("contrib", "extend", "bscan"):
         return (32.0 * w["distinct_seeds"] + 12.0 * (w["seed_hits"] + w["extension_seeds"]),
                 "32 B per count() probe + 12 B per hit touched")

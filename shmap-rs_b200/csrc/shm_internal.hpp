@@ -1,6 +1,8 @@
 // Host-side objects behind the C ABI (context, index, batch scratch).
 #pragma once
 #include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
 #include <stdint.h>
 
 #include <string>
@@ -30,6 +32,8 @@ struct DevBuf {
             SHM_CUDA(cudaDeviceSynchronize());
             SHM_CUDA(cudaFree(p));
         }
+        if (std::getenv("SHMAP_HOSTPROF"))
+            std::fprintf(stderr, "[shmap-host] grow %zu -> %zu bytes\n", cap * sizeof(T), n * sizeof(T));
         p = nullptr;
         size_t want = n < 16 ? 16 : n;
         SHM_CUDA(cudaMalloc(&p, want * sizeof(T)));

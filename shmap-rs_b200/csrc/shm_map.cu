@@ -1054,15 +1054,17 @@ struct RefScratch {
     uint32_t nu_max, wmax;
 };
 
-__global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
+constexpr int REFINE_WARPS = 8;
+
+__global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefScratch rsc) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t ncand = v.coff[v.n];
-    int32_t* cntA = rsc.base + (size_t)wid * rsc.per_warp;
-    int32_t* D = cntA + rsc.nu_max;
-    int32_t* PC = D + rsc.wmax + 1;
-    int32_t* ring = PC + rsc.wmax + 1;
+    int32_t* const cntA = rsc.base + (size_t)wid * rsc.per_warp;
+    int32_t* const D = cntA + rsc.nu_max;
+    int32_t* const PC = D + rsc.wmax + 1;
+    int32_t* const ring = PC + rsc.wmax + 1;
     const bool ap = v.P.ap != 0;
     const DevIndex& I = v.I;
     for (uint32_t ci = wid; ci < ncand; ci += nwarps) {
@@ -1127,8 +1129,10 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
                 ooff = v.sd_ooff[kb + s];
                 int64_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
                 if (t >= occ) {
-                    if (rho >= occ) p = c0 + (int32_t)(__fns(peers, 0, rho - occ + 1));
-                    else p = ring[ooff + (uint32_t)(t % occ)];
+                    if (rho >= occ)  // in this chunk: the peer occ places before this lane
+                        p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
+                    else
+                        p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
                 }
                 int64_t Lj;
                 if (!ap) {
@@ -1155,7 +1159,7 @@ __global__ void __launch_bounds__(256) k_refine(BatchView v, RefScratch rsc) {
             }
             __syncwarp();
             if (s >= 0) {
-                if (rho >= gsz - occ) ring[ooff + (uint32_t)(t % occ)] = x;
+                if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = x;
                 if (rho == gsz - 1) cntA[s] = t + 1;
             }
             __syncwarp();
@@ -1994,8 +1998,10 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     sl.job_cap = job_cap;
     const int wide = grid_for((size_t)1 << 40, 256, 8);  // a full grid for kernels that read their counts on the device
 
+    H.mark("sizes");
     S.bt.reserve(bt_slots_alloc + 1);
     S.bt_list.reserve(bt_slots_alloc + 1);
+    H.mark("bt_res");
     v.bt = S.bt.p;
     v.bt_list = S.bt_list.p;
     T.begin(STG_AUX);
@@ -2006,7 +2012,9 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     k_contrib<<<wide, 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
     T.end();
+    H.mark("contrib");
     S.jobs.reserve(job_cap);
+    H.mark("jobs_res");
     v.jobs = S.jobs.p;
     v.job_cap = job_cap;
     T.begin(STG_BSCAN);
@@ -2019,9 +2027,12 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         SHM_CUDA(cudaGetLastError());
         T.end();
     }
+    H.mark("extend");
     exclusive_scan_u32(S.ccnt.p, S.coff.p, (size_t)n, s);
+    H.mark("scan");
     S.cidx.reserve((size_t)job_cap + 1);
     S.sweep_scr.reserve(2 * (size_t)job_cap + 2);
+    H.mark("cidx_res");
     v.cidx = S.cidx.p;
     T.begin(STG_AUX);
     k_cidx<<<wide, 256, 0, s>>>(v);
@@ -2036,9 +2047,10 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     const size_t budget_ints = (size_t)1 << 28;  // 1 GiB of refinement scratch at most
     while (warps > 8 && warps * rsc.per_warp > budget_ints) warps /= 2;
     S.ref_scr.reserve(warps * rsc.per_warp);
+    H.mark("ref_res");
     rsc.base = S.ref_scr.p;
     T.begin(STG_REFINE);
-    k_refine<<<(unsigned)std::max<size_t>(1, warps / 8), 256, 0, s>>>(v, rsc);
+    k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, 0, s>>>(v, rsc);
     SHM_CUDA(cudaGetLastError());
     T.end();
     T.begin(STG_SWEEP);

@@ -7,7 +7,37 @@
 #include "shm_common.cuh"
 #include "shm_prims.cuh"
 
+#include <mutex>
+
 namespace shm {
+
+// Temporaries of the primitives come from one stream-ordered pool per device
+// that keeps its memory (release threshold: never), so that a call after a
+// synchronize does not map the pool's memory again.
+static cudaMemPool_t prim_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    SHM_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    if (dev < 0 || dev >= 64) throw shm_cuda_error(cudaErrorInvalidDevice);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        SHM_CUDA(cudaMemPoolCreate(&pools[dev], &props));
+        uint64_t keep = UINT64_MAX;
+        SHM_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return pools[dev];
+}
+
+template <class T>
+static void pool_alloc(T** p, size_t bytes, cudaStream_t s) {
+    SHM_CUDA(cudaMallocFromPoolAsync((void**)p, bytes, prim_pool(), s));
+}
+
 
 static int g_num_sms = 0;
 static std::atomic<int64_t> g_launches{0};
@@ -104,7 +134,7 @@ static void exclusive_scan_impl(const T* in, T* out, size_t n, cudaStream_t s) {
         return;
     }
     T* sums = nullptr;
-    SHM_CUDA(cudaMallocAsync(&sums, sizeof(T) * (nb + 1), s));
+    pool_alloc(&sums, sizeof(T) * (nb + 1), s);
     k_scan_reduce<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums);
     SHM_CUDA(cudaGetLastError());
     exclusive_scan_impl<T>(sums, sums, nb, s);  // in-place is safe: each level reads before it writes per tile
@@ -206,8 +236,8 @@ bool radix_sort_pairs(uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, si
     }
     const uint32_t nb = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
     uint32_t *hist = nullptr, *off = nullptr;
-    SHM_CUDA(cudaMallocAsync(&hist, sizeof(uint32_t) * (size_t)RS_BINS * nb, s));
-    SHM_CUDA(cudaMallocAsync(&off, sizeof(uint32_t) * ((size_t)RS_BINS * nb + 1), s));
+    pool_alloc(&hist, sizeof(uint32_t) * (size_t)RS_BINS * nb, s);
+    pool_alloc(&off, sizeof(uint32_t) * ((size_t)RS_BINS * nb + 1), s);
     bool flipped = false;
     for (int shift = 0; shift < key_bits; shift += 8) {
         uint64_t* ki = flipped ? k1 : k0;

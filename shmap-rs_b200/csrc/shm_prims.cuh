@@ -1,6 +1,6 @@
 // Device-wide primitives written for this path: an exclusive scan and a
 // stable LSD radix sort of (u64 key, u32 value) pairs. Temporaries come from
-// the stream-ordered allocator of the calling stream.
+// a stream-ordered pool per device that keeps its memory.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>

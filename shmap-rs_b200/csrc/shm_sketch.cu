@@ -13,6 +13,8 @@
 #include "shm_prims.cuh"
 #include "shm_sketch.cuh"
 
+#include <mutex>
+
 namespace shm {
 
 struct SketchLuts {
@@ -351,16 +353,25 @@ void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStrea
     const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
     const int grid = grid_for(n_tiles, 1, 5);  // tiles, at most 5 resident CTAs per SM
     const size_t dyn = sk_dyn_bytes(mode);
-    if (mode == SK_COUNT) {
-        SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        k_sketch<SK_COUNT><<<grid, SK_THREADS, dyn, s>>>(a, L);
-    } else if (mode == SK_WRITE) {
-        SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_WRITE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        k_sketch<SK_WRITE><<<grid, SK_THREADS, dyn, s>>>(a, L);
-    } else {
-        SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_APPEND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        k_sketch<SK_APPEND><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    {  // the dynamic shared memory limit, once per device and mode
+        static std::mutex mu;
+        static bool done[3][64] = {};
+        int dev = 0;
+        SHM_CUDA(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> g(mu);
+        if (dev >= 0 && dev < 64 && !done[mode][dev]) {
+            if (mode == SK_COUNT)
+                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            else if (mode == SK_WRITE)
+                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_WRITE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            else
+                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_APPEND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            done[mode][dev] = true;
+        }
     }
+    if (mode == SK_COUNT) k_sketch<SK_COUNT><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    else if (mode == SK_WRITE) k_sketch<SK_WRITE><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    else k_sketch<SK_APPEND><<<grid, SK_THREADS, dyn, s>>>(a, L);
     SHM_CUDA(cudaGetLastError());
     count_launch();
 }
