@@ -321,7 +321,9 @@ def run_ours(args, rank, world, local):
             "work_per_step": {k: v // max(1, args.steps) for k, v in work.items()},
             "roofline": roof,
             "e2e": {"value": round(e2e_value, 1), "unit": "reads/s", "h2d_bytes_per_step": int(nbytes + 8 * (n + 1)),
-                    "d2h_bytes_per_step": int(n * sb.RECORD_DTYPE.itemsize), "ms_per_step": round(e2e_ms / args.steps, 3)},
+                    "d2h_bytes_per_step": int(n * sb.RECORD_DTYPE.itemsize), "ms_per_step": round(e2e_ms / args.steps, 3),
+                    # the reads cross PCIe once: this rate against the link's ~55 GB/s is what bounds e2e
+                    "h2d_gb_per_s": round(nbytes * args.steps / (e2e_ms / 1e3) / 1e9, 1)},
             "gpu_launches": int(launches),
             "clocks": clk,
         }

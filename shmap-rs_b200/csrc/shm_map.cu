@@ -1504,7 +1504,8 @@ struct MapScratch {
     DevBuf<int32_t> seed_lists;  // N_SEED_BINS lists of n reads
     DevBuf<uint32_t> bin_cnt;
     DevBuf<uint8_t> retry_seq;  // reads mapped again with exact bounds
-    DevBuf<shm_map_record> retry_out, retry_all;
+    DevBuf<shm_map_record> retry_out;
+    DevBuf<int64_t> retry_list;
     DevBuf<int32_t> retry_idx;
     DevBuf<uint64_t> km_h, sd_h, pht_key, hw, hw_off, bt_size, bt_off;
     DevBuf<uint32_t> kcnt, km_rs, sd_a, sd_cnt, sd_os, sd_hpre, sd_ooff, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
@@ -2093,50 +2094,105 @@ __global__ void k_scatter_records(const shm_map_record* __restrict__ src, const 
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[idx[i]] = src[i];
 }
 
+// Copies read i of a list (bytes [src[3i], src[3i] + src[3i+2]) of `base`) to
+// staged + src[3i+1]; one block per read.
+__global__ void k_gather_reads(const uint8_t* __restrict__ base, const int64_t* __restrict__ list, int32_t n,
+                               uint8_t* __restrict__ staged) {
+    for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int64_t from = list[3 * (size_t)i], to = list[3 * (size_t)i + 1], len = list[3 * (size_t)i + 2];
+        for (int64_t j = threadIdx.x; j < len; j += blockDim.x) staged[to + j] = base[from + j];
+    }
+}
+
+// Where retried reads come from and where their records go: device memory
+// (read g at d_seq + offs[g] - offs[0], record g at d_out[g]) or host memory
+// (read g at h_seq + offs[g], record g at h_out[g]).
+struct RetryIO {
+    const uint8_t* d_seq;
+    shm_map_record* d_out;
+    const uint8_t* h_seq;
+    shm_map_record* h_out;
+};
+
 // Reads that beat their k-mer capacity estimate are mapped again, together,
-// with their counts as capacities. `copy_read(dst, g)` copies read g's bytes
-// (host or device) into the staging buffer.
-template <class CopyFn>
+// with their counts as capacities: first as a queued batch (capped bucket
+// tables), then, for any read that overflows again, with exact sizes.
 static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params& p, const std::vector<Overflow>& ovf,
-                            const int64_t* offs, CopyFn copy_read, shm_map_record* d_out) {
+                            const int64_t* offs, const RetryIO& io, bool exact = false) {
     if (ovf.empty()) return;
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
-    std::vector<int64_t> o(ovf.size() + 1, 0);
-    std::vector<uint32_t> caps(ovf.size());
-    for (size_t i = 0; i < ovf.size(); i++) {
-        o[i + 1] = o[i] + (offs[ovf[i].read + 1] - offs[ovf[i].read]);
-        caps[i] = ovf[i].m;
+    const int32_t n = (int32_t)ovf.size();
+    std::vector<int64_t> o((size_t)n + 1, 0);
+    std::vector<uint32_t> caps((size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+        o[(size_t)i + 1] = o[(size_t)i] + (offs[ovf[i].read + 1] - offs[ovf[i].read]);
+        caps[(size_t)i] = ovf[i].m;
     }
-    S.retry_seq.reserve((size_t)o.back() + 32);
-    SHM_CUDA(cudaMemsetAsync(S.retry_seq.p + o.back(), 0, 32, s));
-    for (size_t i = 0; i < ovf.size(); i++) copy_read(S.retry_seq.p + o[i], ovf[i].read);
-    S.retry_out.reserve(ovf.size());
+    const int64_t nb = o.back();
+    // one pinned block: the gather list or the reads' bytes, the plan, the record slots
+    const size_t list_bytes = io.d_seq ? 24 * (size_t)n : (size_t)nb;
+    const size_t plan_at = (list_bytes + 63) / 64 * 64;
+    const size_t idx_at = plan_at + (BatchPlan::layout(n) + 63) / 64 * 64;
+    uint8_t* pin = pinned_stage(c, idx_at + sizeof(int32_t) * (size_t)n);
+    S.retry_seq.reserve((size_t)nb + 32);
+    SHM_CUDA(cudaMemsetAsync(S.retry_seq.p + nb, 0, 32, s));
+    if (io.d_seq) {  // device reads: one gather kernel
+        int64_t* lst = (int64_t*)pin;
+        for (int32_t i = 0; i < n; i++) {
+            lst[3 * (size_t)i] = offs[ovf[i].read] - offs[0];
+            lst[3 * (size_t)i + 1] = o[(size_t)i];
+            lst[3 * (size_t)i + 2] = o[(size_t)i + 1] - o[(size_t)i];
+        }
+        S.retry_list.reserve(3 * (size_t)n);
+        SHM_CUDA(cudaMemcpyAsync(S.retry_list.p, lst, 24 * (size_t)n, cudaMemcpyHostToDevice, s));
+        k_gather_reads<<<(unsigned)std::min<int32_t>(n, 1184), 256, 0, s>>>(io.d_seq, S.retry_list.p, n,
+                                                                           S.retry_seq.p);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+    } else {  // host reads: gathered into pinned memory, one copy
+        for (int32_t i = 0; i < n; i++)
+            std::memcpy(pin + o[(size_t)i], io.h_seq + offs[ovf[i].read], (size_t)(o[(size_t)i + 1] - o[(size_t)i]));
+        SHM_CUDA(cudaMemcpyAsync(S.retry_seq.p, pin, (size_t)nb, cudaMemcpyHostToDevice, s));
+    }
+    S.retry_out.reserve((size_t)n);
     StageTimer T(c);
-    const std::vector<std::pair<int32_t, int32_t>> one{{0, (int32_t)ovf.size()}};
+    const std::vector<std::pair<int32_t, int32_t>> one{{0, n}};
     std::vector<BatchSlot> sl = batch_slots(c, one, o.data());
-    uint8_t* h_plan = pinned_stage(c, BatchPlan::layout((int32_t)ovf.size()));
-    run_batch(c, ix, p, S.retry_seq.p, o.data(), (int32_t)ovf.size(), S.retry_out.p, caps.data(), true, h_plan, T,
-              sl[0]);
+    run_batch(c, ix, p, S.retry_seq.p, o.data(), n, S.retry_out.p, caps.data(), exact, pin + plan_at, T, sl[0]);
     SHM_CUDA(cudaStreamSynchronize(s));
+    if (sl[0].R->nj > sl[0].job_cap) {  // too many bucket jobs for the queued sizes
+        run_batch(c, ix, p, S.retry_seq.p, o.data(), n, S.retry_out.p, caps.data(), true, pin + plan_at, T, sl[0]);
+        SHM_CUDA(cudaStreamSynchronize(s));
+    }
     T.collect();
     std::vector<Overflow> again;
     collect_batch(c, sl[0], again);
-    if (!again.empty()) {
+    if (exact && !again.empty()) {
         std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n",
                      ovf[again[0].read].read);
         throw shm_cuda_error(cudaErrorMemoryAllocation);
     }
-    // the slot list goes up through the pinned staging (free: the stream has drained)
-    int32_t* h_idx = (int32_t*)pinned_stage(c, sizeof(int32_t) * ovf.size());
-    for (size_t i = 0; i < ovf.size(); i++) h_idx[i] = ovf[i].read;
-    S.retry_idx.reserve(ovf.size());
-    SHM_CUDA(cudaMemcpyAsync(S.retry_idx.p, h_idx, sizeof(int32_t) * ovf.size(), cudaMemcpyHostToDevice, s));
-    k_scatter_records<<<grid_for(ovf.size(), 256), 256, 0, s>>>(S.retry_out.p, S.retry_idx.p, (int32_t)ovf.size(),
-                                                                d_out);
-    SHM_CUDA(cudaGetLastError());
-    count_launch();
-    SHM_CUDA(cudaStreamSynchronize(s));
+    if (io.d_out) {  // records to their slots on the device
+        int32_t* h_idx = (int32_t*)(pin + idx_at);
+        for (int32_t i = 0; i < n; i++) h_idx[i] = ovf[i].read;
+        S.retry_idx.reserve((size_t)n);
+        SHM_CUDA(cudaMemcpyAsync(S.retry_idx.p, h_idx, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, s));
+        k_scatter_records<<<grid_for((size_t)n, 256), 256, 0, s>>>(S.retry_out.p, S.retry_idx.p, n, io.d_out);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+        SHM_CUDA(cudaStreamSynchronize(s));
+    } else {  // records to their slots on the host, through pinned memory
+        shm_map_record* h_rec = (shm_map_record*)pinned_stage(c, sizeof(shm_map_record) * (size_t)n);
+        SHM_CUDA(cudaMemcpyAsync(h_rec, S.retry_out.p, sizeof(shm_map_record) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        SHM_CUDA(cudaStreamSynchronize(s));
+        for (int32_t i = 0; i < n; i++) io.h_out[ovf[i].read] = h_rec[i];
+    }
+    if (!again.empty()) {  // a capped bucket table filled up: those reads once more, with exact sizes
+        std::vector<Overflow> sub;
+        for (const Overflow& a : again) sub.push_back(Overflow{ovf[a.read].read, a.m});
+        retry_overflows(c, ix, p, sub, offs, io, true);
+    }
 }
 
 // Batches of at most max_reads reads and max_bases bases (one read at a time
@@ -2196,11 +2252,7 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
     std::vector<Overflow> ovf_all;
     for (const BatchSlot& sl : slots) collect_batch(c, sl, ovf_all);
     HostClock H;
-    retry_overflows(c, ix, p, ovf_all, h_offs, [&](uint8_t* dst, int32_t g) {
-        SHM_CUDA(cudaMemcpyAsync(dst, d_seq + (h_offs[g] - h_offs[0]), (size_t)(h_offs[g + 1] - h_offs[g]),
-                                 cudaMemcpyDeviceToDevice, c->stream));
-    }, d_out);
-    SHM_CUDA(cudaStreamSynchronize(c->stream));
+    retry_overflows(c, ix, p, ovf_all, h_offs, RetryIO{d_seq, d_out, nullptr, nullptr});
     H.mark("retry");
     H.print("retries", (int32_t)ovf_all.size());
 }
@@ -2266,17 +2318,7 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     T.collect();
     std::vector<Overflow> ovf_all;
     for (const BatchSlot& sl : slots) collect_batch(c, sl, ovf_all);
-    if (!ovf_all.empty()) {
-        DevBuf<shm_map_record>& all = S.retry_all;
-        all.reserve((size_t)n);
-        // only the retried slots are read back: write them through a device copy of their records
-        retry_overflows(c, ix, p, ovf_all, offs, [&](uint8_t* dst, int32_t g) {
-            SHM_CUDA(cudaMemcpyAsync(dst, seqs + offs[g], (size_t)(offs[g + 1] - offs[g]), cudaMemcpyHostToDevice, s));
-        }, all.p);
-        for (const Overflow& o : ovf_all)
-            SHM_CUDA(cudaMemcpyAsync(out + o.read, all.p + o.read, sizeof(shm_map_record), cudaMemcpyDeviceToHost, s));
-        SHM_CUDA(cudaStreamSynchronize(s));
-    }
+    retry_overflows(c, ix, p, ovf_all, offs, RetryIO{nullptr, nullptr, seqs, out});
     H.mark("retry");
     H.print("host-form", n);
 }
