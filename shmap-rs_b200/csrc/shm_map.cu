@@ -463,6 +463,127 @@ __global__ void k_seed_bins(BatchView v, int32_t* __restrict__ lists, uint32_t* 
     }
 }
 
+// count() probes for U hashes of one lane at once (index.rs:204-213): the
+// directory, key and hit-list loads of the U probes are issued together, so
+// a lane waits for three rounds of loads instead of 3U.
+template <int U>
+__device__ __forceinline__ void idx_lookup_u(const DevIndex& I, const uint64_t (&h)[U], const bool (&on)[U],
+                                             uint32_t (&a)[U], uint32_t (&cnt)[U]) {
+    uint32_t lo[U], hi[U], at[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        a[u] = 0;
+        cnt[u] = 0;
+        lo[u] = hi[u] = 0;
+        at[u] = 0xffffffffu;
+        if (on[u] && h[u] <= I.thr && I.n_keys != 0) {
+            const uint32_t b = (uint32_t)__umul64hi(h[u], I.dir_mul);
+            lo[u] = __ldg(I.dir + b);
+            hi[u] = __ldg(I.dir + b + 1);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        while (hi[u] - lo[u] > 8) {  // a crowded directory range (rare)
+            const uint32_t mid = (lo[u] + hi[u]) >> 1;
+            if (__ldg(I.keys + mid) <= h[u]) lo[u] = mid;
+            else hi[u] = mid;
+        }
+    }
+    uint64_t k0[U], k1[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {  // the first two keys of every range at once
+        k0[u] = lo[u] < hi[u] ? __ldg(I.keys + lo[u]) : 0;
+        k1[u] = lo[u] + 1 < hi[u] ? __ldg(I.keys + lo[u] + 1) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        if (lo[u] < hi[u] && k0[u] == h[u]) {
+            at[u] = lo[u];
+        } else if (lo[u] + 1 < hi[u] && k0[u] < h[u]) {
+            if (k1[u] == h[u]) {
+                at[u] = lo[u] + 1;
+            } else if (k1[u] < h[u]) {
+                for (uint32_t i = lo[u] + 2; i < hi[u]; i++) {
+                    const uint64_t kk = __ldg(I.keys + i);
+                    if (kk == h[u]) {
+                        at[u] = i;
+                        break;
+                    }
+                    if (kk > h[u]) break;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        if (at[u] != 0xffffffffu) {
+            a[u] = __ldg(I.key_off + at[u]);
+            cnt[u] = __ldg(I.key_off + at[u] + 1) - a[u];
+        }
+    }
+}
+
+// pht_insert for U seeds of one lane; the compare-and-swaps of the U probes
+// are issued together.
+template <int U>
+__device__ __forceinline__ void pht_insert_u(const BatchView& v, int32_t q, const uint64_t (&h)[U],
+                                             const uint32_t (&idx)[U], const bool (&on)[U]) {
+    const uint64_t base = v.pht_off[q];
+    const uint64_t mask = v.pht_off[q + 1] - base - 1;
+    uint64_t i[U];
+    bool pend[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        i[u] = h[u] & mask;
+        pend[u] = on[u];
+    }
+    for (;;) {  // the table has at least twice as many slots as seeds: every insert ends
+        bool more = false;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (!pend[u]) continue;
+            if (atomicCAS(v.pht_val + base + i[u], 0xffffffffu, idx[u]) == 0xffffffffu) {
+                v.pht_key[base + i[u]] = h[u];
+                pend[u] = false;
+            } else {
+                i[u] = (i[u] + 1) & mask;
+                more = true;
+            }
+        }
+        if (!more) break;
+    }
+}
+
+// seed_bucket_bound summed over U seeds of one lane (those with on[u]); the
+// hit-list ends of the U seeds are loaded together.
+template <int U>
+__device__ __forceinline__ uint64_t seed_bucket_bound_u(const BatchView& v, const uint32_t (&a)[U],
+                                                        const uint32_t (&cnt)[U], const bool (&on)[U], int64_t h) {
+    uint32_t g0[U], g1[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        g0[u] = g1[u] = 0;
+        if (on[u] && cnt[u] > 1 && !v.P.ap) {
+            g0[u] = __ldg(v.I.hits + a[u]);
+            g1[u] = __ldg(v.I.hits + a[u] + cnt[u] - 1);
+        }
+    }
+    uint64_t sum = 0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        if (!on[u] || cnt[u] == 0) continue;
+        if (cnt[u] == 1 || v.P.ap) {
+            sum += 2ULL * cnt[u];
+            continue;
+        }
+        const int32_t s0 = seg_of(v.I, g0[u]), s1 = seg_of(v.I, g1[u]);
+        const uint64_t span = (uint64_t)(g1[u] - g0[u]) / (uint64_t)h + 1 + 3ULL * (uint64_t)(s1 - s0 + 1);
+        sum += min((uint64_t)(2ULL * cnt[u]), span);
+    }
+    return sum;
+}
+
 // ------------------------------------------------------------------ K2 counting form
 // Seed preparation with one warp per read and work linear in m: the k-mers
 // are bucketed by a counting sort on h -> h * Ht / (thr + 1) (order
@@ -477,6 +598,7 @@ __global__ void k_seed_bins(BatchView v, int32_t* __restrict__ lists, uint32_t* 
 //   Ra (4C): each group's hit-list start
 //   P0, P1 (4C each): radix permutations; RH (256 words): digit offsets
 __host__ __device__ constexpr size_t seedc_bytes(uint32_t C) { return 28 * (size_t)C + 1024; }
+constexpr int SEEDC_U = 4;  // groups a lane probes at once
 
 // Exclusive scan, in place, of the n (a multiple of 32) words X[0..n): lane l
 // owns n/32 consecutive words.
@@ -581,14 +703,28 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
     }
     if (v.P.os) S = (int32_t)n_u;  // mod.rs:732-736
 
-    // count() probes (index.rs:204-213)
+    // count() probes (index.rs:204-213), SEEDC_U groups a lane at once
     uint32_t maxc = 0;
-    for (uint32_t g = lane; g < n_u; g += 32) {
-        uint32_t a, cnt;
-        idx_lookup(v.I, Sh[g], a, cnt);
-        Rc[g] = cnt;
-        Ra[g] = a;
-        maxc = max(maxc, cnt);
+    for (uint32_t g0 = 0; g0 < n_u; g0 += 32 * SEEDC_U) {
+        uint64_t hh[SEEDC_U];
+        bool on[SEEDC_U];
+        uint32_t a[SEEDC_U], cnt[SEEDC_U];
+#pragma unroll
+        for (int u = 0; u < SEEDC_U; u++) {
+            const uint32_t g = g0 + 32 * u + lane;
+            on[u] = g < n_u;
+            hh[u] = on[u] ? Sh[g] : 0;
+        }
+        idx_lookup_u<SEEDC_U>(v.I, hh, on, a, cnt);
+#pragma unroll
+        for (int u = 0; u < SEEDC_U; u++) {
+            const uint32_t g = g0 + 32 * u + lane;
+            if (on[u]) {
+                Rc[g] = cnt[u];
+                Ra[g] = a[u];
+                maxc = max(maxc, cnt[u]);
+            }
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
@@ -626,7 +762,8 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
         pout = pout == P0 ? P1 : P0;
     }
 
-    // seeding prefix: seed i is processed iff sum(occs before i) < S (seeding.rs:101)
+    // seeding prefix: seed i is processed iff sum(occs before i) < S
+    // (seeding.rs:101); the processed seeds are a prefix of the order
     uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
     uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
     for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
@@ -640,12 +777,10 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
         const uint32_t po = po_carry + oi - occs;
         const uint64_t pc = pc_carry + ci - cnt;
         if (valid) {
-            const uint64_t hg = Sh[g];
-            const uint32_t a = Ra[g];
-            v.sd_h[kb + i] = hg;
+            v.sd_h[kb + i] = Sh[g];
             v.sd_os[kb + i] = os;
             v.sd_cnt[kb + i] = cnt;
-            v.sd_a[kb + i] = a;
+            v.sd_a[kb + i] = Ra[g];
             v.sd_ooff[kb + i] = po;
             if ((int64_t)po < (int64_t)S) {
                 v.sd_hpre[kb + i] = (uint32_t)pc;
@@ -653,9 +788,7 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
                 l_s0 += occs;
                 l_sm += cnt;
                 l_max = max(l_max, cnt);
-                l_eb += seed_bucket_bound(v, a, cnt, halflen);
             }
-            pht_insert(v, q, hg, i);
         }
         po_carry += __shfl_sync(0xffffffffu, oi, 31);
         pc_carry += __shfl_sync(0xffffffffu, ci, 31);
@@ -665,9 +798,29 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
         l_np += __shfl_xor_sync(0xffffffffu, l_np, o);
         l_s0 += __shfl_xor_sync(0xffffffffu, l_s0, o);
         l_sm += __shfl_xor_sync(0xffffffffu, l_sm, o);
-        l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
         l_max = max(l_max, __shfl_xor_sync(0xffffffffu, l_max, o));
     }
+    // bucket bounds of the processed seeds and the probe table, SEEDC_U seeds a
+    // lane at once (both are independent of the order they are done in)
+    for (uint32_t c0 = 0; c0 < n_u; c0 += 32 * SEEDC_U) {
+        uint64_t hh[SEEDC_U];
+        uint32_t a[SEEDC_U], cnt[SEEDC_U], ii[SEEDC_U];
+        bool on[SEEDC_U], proc[SEEDC_U];
+#pragma unroll
+        for (int u = 0; u < SEEDC_U; u++) {
+            ii[u] = c0 + 32 * u + lane;
+            on[u] = ii[u] < n_u;
+            proc[u] = ii[u] < l_np;
+            const uint32_t g = on[u] ? (ord ? ord[ii[u]] : ii[u]) : 0u;
+            hh[u] = on[u] ? Sh[g] : 0;
+            a[u] = on[u] ? Ra[g] : 0u;
+            cnt[u] = on[u] ? Rc[g] : 0u;
+        }
+        l_eb += seed_bucket_bound_u<SEEDC_U>(v, a, cnt, proc, halflen);
+        pht_insert_u<SEEDC_U>(v, q, hh, ii, on);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
     if (lane == 0) {
         v.r_status[q] = ST_UNMAPPED;
         v.r_nu[q] = (int32_t)n_u;
