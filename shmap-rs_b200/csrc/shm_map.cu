@@ -634,10 +634,12 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
     const uint64_t mul = v.P.slot_mul[31 - __clz(Ht)];
     for (uint32_t i = lane; i < Ht; i += 32) Rc[i] = 0;
     __syncwarp();
+#pragma unroll 4
     for (uint32_t i = lane; i < m; i += 32) atomicAdd(&Rc[(uint32_t)__umul64hi(v.km_h[kb + i], mul)], 1u);
     __syncwarp();
     warp_scan_words(Rc, Ht, lane);
     __syncwarp();
+#pragma unroll 4
     for (uint32_t i = lane; i < m; i += 32) {
         const uint64_t h = v.km_h[kb + i];
         const uint32_t pos = atomicAdd(&Rc[(uint32_t)__umul64hi(h, mul)], 1u);
@@ -1207,6 +1209,47 @@ struct RefScratch {
     uint32_t nu_max, wmax;
 };
 
+// pht_lookup for U hashes of one lane, the probes issued together; s[u] =
+// the seed index, or -1 when absent (or !on[u]).
+template <int U>
+__device__ __forceinline__ void pht_lookup_u(const BatchView& v, int32_t q, const uint64_t (&h)[U], const bool (&on)[U],
+                                             int32_t (&s)[U]) {
+    const uint64_t base = v.pht_off[q];
+    const uint64_t mask = v.pht_off[q + 1] - base - 1;
+    uint64_t i[U];
+    bool pend[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        i[u] = h[u] & mask;
+        pend[u] = on[u];
+        s[u] = -1;
+    }
+    for (;;) {  // the table keeps empty slots (at least twice as many slots as seeds): every probe ends
+        uint32_t val[U];
+        uint64_t key[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            val[u] = pend[u] ? v.pht_val[base + i[u]] : 0xffffffffu;
+            key[u] = pend[u] ? v.pht_key[base + i[u]] : 0;
+        }
+        bool more = false;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (!pend[u]) continue;
+            if (val[u] == 0xffffffffu) {
+                pend[u] = false;
+            } else if (key[u] == h[u]) {
+                s[u] = (int32_t)val[u];
+                pend[u] = false;
+            } else {
+                i[u] = (i[u] + 1) & mask;
+                more = true;
+            }
+        }
+        if (!more) break;
+    }
+}
+
 constexpr int REFINE_WARPS = 8;
 
 __global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefScratch rsc) {
@@ -1248,74 +1291,90 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefSc
         for (int32_t i = lane; i <= W; i += 32) D[i] = 0;
         __syncwarp();
         // phase 1: seed of every position, its occurrence interval of windows,
-        // and the prefix PC of strand agreement (+1 same strand, -1 opposite)
+        // and the prefix PC of strand agreement (+1 same strand, -1 opposite).
+        // Two chunks of 32 positions at a time: their reference k-mers, probe
+        // lookups and seed records are fetched together, then the chunks are
+        // folded in order.
         int32_t pc_carry = 0;
         if (lane == 0) PC[0] = 0;
-        for (int32_t c0 = 0; c0 < W; c0 += 32) {
-            const int32_t x = c0 + lane;  // position from + x
-            const bool valid = x < W;
-            int32_t s = -1;
-            uint32_t os = 0, rs = 0;
-            if (valid) {
-                const uint32_t gid = G0 + (uint32_t)(from + x);
-                rs = __ldg(I.ref_rs + gid);
-                uint32_t si;
-                if (pht_lookup(v, q, __ldg(I.ref_h + gid), si)) {
-                    s = (int32_t)si;
-                    os = v.sd_os[kb + si];
-                }
+        for (int32_t c00 = 0; c00 < W; c00 += 64) {
+            uint64_t hx[2];
+            uint32_t rsx[2], osx[2], ooffx[2];
+            bool on[2];
+            int32_t sx[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int32_t x = c00 + 32 * u + lane;
+                on[u] = x < W;
+                const uint32_t gid = G0 + (uint32_t)(from + (on[u] ? x : 0));
+                hx[u] = on[u] ? __ldg(I.ref_h + gid) : 0;
+                rsx[u] = on[u] ? __ldg(I.ref_rs + gid) : 0;
             }
-            {
-                const int32_t cv = (valid && s >= 0) ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
-                const int32_t inc = warp_inclusive_scan(cv);
-                if (valid) PC[x + 1] = pc_carry + inc;
-                pc_carry += __shfl_sync(0xffffffffu, inc, 31);
+            pht_lookup_u<2>(v, q, hx, on, sx);
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                osx[u] = sx[u] >= 0 ? v.sd_os[kb + sx[u]] : 0u;
+                ooffx[u] = sx[u] >= 0 ? v.sd_ooff[kb + sx[u]] : 0u;
             }
-            const unsigned peers = __match_any_sync(0xffffffffu, s);
-            int32_t t = 0, occ = 1, rho = 0, gsz = 0;
-            uint32_t ooff = 0;
-            if (s >= 0) {
-                occ = (int32_t)(os >> 1);
-                rho = __popc(peers & lt);
-                gsz = __popc(peers);
-                t = cntA[s] + rho;
-                ooff = v.sd_ooff[kb + s];
-                int64_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
-                if (t >= occ) {
-                    if (rho >= occ)  // in this chunk: the peer occ places before this lane
-                        p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
-                    else
-                        p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int32_t c0 = c00 + 32 * u;
+                if (c0 >= W) break;  // warp-uniform
+                const int32_t x = c0 + lane;
+                const bool valid = on[u];
+                const int32_t s = sx[u];
+                const uint32_t os = osx[u], rs = rsx[u];
+                {
+                    const int32_t cv = (valid && s >= 0) ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
+                    const int32_t inc = warp_inclusive_scan(cv);
+                    if (valid) PC[x + 1] = pc_carry + inc;
+                    pc_carry += __shfl_sync(0xffffffffu, inc, 31);
                 }
-                int64_t Lj;
-                if (!ap) {
-                    Lj = (int64_t)x - m + 1;
-                } else {  // first l with R[l] > R[x] - m
-                    const int64_t rv = (int64_t)(rs >> 1) - m;
-                    int32_t lo = 0, len = x;
-                    while (len > 0) {
-                        int32_t half = len >> 1;
-                        if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
-                            lo += half + 1;
-                            len -= half + 1;
-                        } else {
-                            len = half;
-                        }
+                const unsigned peers = __match_any_sync(0xffffffffu, s);
+                int32_t t = 0, occ = 1, rho = 0, gsz = 0;
+                const uint32_t ooff = ooffx[u];
+                if (s >= 0) {
+                    occ = (int32_t)(os >> 1);
+                    rho = __popc(peers & lt);
+                    gsz = __popc(peers);
+                    t = cntA[s] + rho;
+                    int64_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
+                    if (t >= occ) {
+                        if (rho >= occ)  // in this chunk: the peer occ places before this lane
+                            p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
+                        else
+                            p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
                     }
-                    Lj = lo;
+                    int64_t Lj;
+                    if (!ap) {
+                        Lj = (int64_t)x - m + 1;
+                    } else {  // first l with R[l] > R[x] - m
+                        const int64_t rv = (int64_t)(rs >> 1) - m;
+                        int32_t lo = 0, len = x;
+                        while (len > 0) {
+                            int32_t half = len >> 1;
+                            if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
+                                lo += half + 1;
+                                len -= half + 1;
+                            } else {
+                                len = half;
+                            }
+                        }
+                        Lj = lo;
+                    }
+                    int64_t st = max(max(p + 1, Lj), (int64_t)0);
+                    if (st <= x) {
+                        atomicAdd(D + st, 1);
+                        atomicAdd(D + x + 1, -1);
+                    }
                 }
-                int64_t st = max(max(p + 1, Lj), (int64_t)0);
-                if (st <= x) {
-                    atomicAdd(D + st, 1);
-                    atomicAdd(D + x + 1, -1);
+                __syncwarp();
+                if (s >= 0) {
+                    if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = x;
+                    if (rho == gsz - 1) cntA[s] = t + 1;
                 }
+                __syncwarp();
             }
-            __syncwarp();
-            if (s >= 0) {
-                if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = x;
-                if (rho == gsz - 1) cntA[s] = t + 1;
-            }
-            __syncwarp();
         }
         __syncwarp();
         // phase 2: intersection per window start, score, first maximum. Under
