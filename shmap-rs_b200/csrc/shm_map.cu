@@ -1251,6 +1251,7 @@ __device__ __forceinline__ void pht_lookup_u(const BatchView& v, int32_t q, cons
 }
 
 constexpr int REFINE_WARPS = 8;
+constexpr int REFINE_U = 2;  // position chunks whose seeds are fetched together
 
 __global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefScratch rsc) {
     const int lane = threadIdx.x & 31;
@@ -1292,32 +1293,32 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefSc
         __syncwarp();
         // phase 1: seed of every position, its occurrence interval of windows,
         // and the prefix PC of strand agreement (+1 same strand, -1 opposite).
-        // Two chunks of 32 positions at a time: their reference k-mers, probe
-        // lookups and seed records are fetched together, then the chunks are
-        // folded in order.
+        // REFINE_U chunks of 32 positions at a time: their reference k-mers,
+        // probe lookups and seed records are fetched together, then the chunks
+        // are folded in order.
         int32_t pc_carry = 0;
         if (lane == 0) PC[0] = 0;
-        for (int32_t c00 = 0; c00 < W; c00 += 64) {
-            uint64_t hx[2];
-            uint32_t rsx[2], osx[2], ooffx[2];
-            bool on[2];
-            int32_t sx[2];
+        for (int32_t c00 = 0; c00 < W; c00 += 32 * REFINE_U) {
+            uint64_t hx[REFINE_U];
+            uint32_t rsx[REFINE_U], osx[REFINE_U], ooffx[REFINE_U];
+            bool on[REFINE_U];
+            int32_t sx[REFINE_U];
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < REFINE_U; u++) {
                 const int32_t x = c00 + 32 * u + lane;
                 on[u] = x < W;
                 const uint32_t gid = G0 + (uint32_t)(from + (on[u] ? x : 0));
                 hx[u] = on[u] ? __ldg(I.ref_h + gid) : 0;
                 rsx[u] = on[u] ? __ldg(I.ref_rs + gid) : 0;
             }
-            pht_lookup_u<2>(v, q, hx, on, sx);
+            pht_lookup_u<REFINE_U>(v, q, hx, on, sx);
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < REFINE_U; u++) {
                 osx[u] = sx[u] >= 0 ? v.sd_os[kb + sx[u]] : 0u;
                 ooffx[u] = sx[u] >= 0 ? v.sd_ooff[kb + sx[u]] : 0u;
             }
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < REFINE_U; u++) {
                 const int32_t c0 = c00 + 32 * u;
                 if (c0 >= W) break;  // warp-uniform
                 const int32_t x = c0 + lane;
