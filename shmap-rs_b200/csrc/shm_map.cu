@@ -1253,8 +1253,202 @@ __device__ __forceinline__ void pht_lookup_u(const BatchView& v, int32_t q, cons
 constexpr int REFINE_WARPS = 8;
 constexpr int REFINE_U = 2;  // position chunks whose seeds are fetched together
 
-__global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefScratch rsc) {
-    const int lane = threadIdx.x & 31;
+// One candidate window (best_fixed_length, src/shmap/scoring.rs:189-291).
+// cntA (per seed: occurrences seen) and ring (per seed: positions of its last
+// occs occurrences) come from the warp's shared slice when the read is small
+// enough, else from its global scratch; D and PC always from global scratch.
+__device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int32_t q, int32_t* cntA, int32_t* D,
+                                           int32_t* PC, int32_t* ring, int lane, unsigned lt) {
+    const bool ap = v.P.ap != 0;
+    const DevIndex& I = v.I;
+    const int32_t m = v.r_m[q], n_u = v.r_nu[q];
+    const int64_t h = v.r_half[q];
+    const uint64_t kb = v.kcap_off[q];
+    const int32_t seg = J->seg;
+    const uint32_t G0 = __ldg(I.seg_off + seg), Gend = __ldg(I.seg_off + seg + 1);
+    const int64_t seglen = (int64_t)(Gend - G0);
+    const int64_t from = (int64_t)J->bb * h;
+    const int64_t end = min(((int64_t)J->bb + 2) * h, seglen);
+    const int32_t W = (int32_t)(end - from);
+    if (lane == 0 && W > 0) atomicAdd(&v.mx->refine_kmers, (unsigned long long)W);
+    for (int32_t i = lane; i < n_u; i += 32) cntA[i] = 0;
+    for (int32_t i = lane; i <= W; i += 32) D[i] = 0;
+    __syncwarp();
+    // phase 1: seed of every position, its occurrence interval of windows,
+    // and the prefix PC of strand agreement (+1 same strand, -1 opposite).
+    // REFINE_U chunks of 32 positions at a time: their reference k-mers,
+    // probe lookups and seed records are fetched together, then the chunks
+    // are folded in order.
+    int32_t pc_carry = 0;
+    if (lane == 0) PC[0] = 0;
+    for (int32_t c00 = 0; c00 < W; c00 += 32 * REFINE_U) {
+        uint64_t hx[REFINE_U];
+        uint32_t rsx[REFINE_U], osx[REFINE_U], ooffx[REFINE_U];
+        bool on[REFINE_U];
+        int32_t sx[REFINE_U];
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++) {
+            const int32_t x = c00 + 32 * u + lane;
+            on[u] = x < W;
+            const uint32_t gid = G0 + (uint32_t)(from + (on[u] ? x : 0));
+            hx[u] = on[u] ? __ldg(I.ref_h + gid) : 0;
+            rsx[u] = on[u] ? __ldg(I.ref_rs + gid) : 0;
+        }
+        pht_lookup_u<REFINE_U>(v, q, hx, on, sx);
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++) {
+            osx[u] = sx[u] >= 0 ? v.sd_os[kb + sx[u]] : 0u;
+            ooffx[u] = sx[u] >= 0 ? v.sd_ooff[kb + sx[u]] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++) {
+            const int32_t c0 = c00 + 32 * u;
+            if (c0 >= W) break;  // warp-uniform
+            const int32_t x = c0 + lane;
+            const bool valid = on[u];
+            const int32_t s = sx[u];
+            const uint32_t os = osx[u], rs = rsx[u];
+            {
+                const int32_t cv = (valid && s >= 0) ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
+                const int32_t inc = warp_inclusive_scan(cv);
+                if (valid) PC[x + 1] = pc_carry + inc;
+                pc_carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, s);
+            int32_t t = 0, occ = 1, rho = 0, gsz = 0;
+            const uint32_t ooff = ooffx[u];
+            if (s >= 0) {
+                occ = (int32_t)(os >> 1);
+                rho = __popc(peers & lt);
+                gsz = __popc(peers);
+                t = cntA[s] + rho;
+                int64_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
+                if (t >= occ) {
+                    if (rho >= occ)  // in this chunk: the peer occ places before this lane
+                        p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
+                    else
+                        p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
+                }
+                int64_t Lj;
+                if (!ap) {
+                    Lj = (int64_t)x - m + 1;
+                } else {  // first l with R[l] > R[x] - m
+                    const int64_t rv = (int64_t)(rs >> 1) - m;
+                    int32_t lo = 0, len = x;
+                    while (len > 0) {
+                        int32_t half = len >> 1;
+                        if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
+                            lo += half + 1;
+                            len -= half + 1;
+                        } else {
+                            len = half;
+                        }
+                    }
+                    Lj = lo;
+                }
+                int64_t st = max(max(p + 1, Lj), (int64_t)0);
+                if (st <= x) {
+                    atomicAdd(D + st, 1);
+                    atomicAdd(D + x + 1, -1);
+                }
+            }
+            __syncwarp();
+            if (s >= 0) {
+                if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = x;
+                if (rho == gsz - 1) cntA[s] = t + 1;
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    // phase 2: intersection per window start, score, first maximum. Under
+    // Containment every score is I / m for the same m, and distinct I < 2^31
+    // give distinct quotients, so the first maximum of I is the first
+    // maximum of the score: the division is done once, for the winner.
+    const bool jac = v.P.metric == 1;
+    double best = -1.0;
+    int32_t bl = -1, bI = -1, bS = 0, br = 0;
+    int32_t icarry = 0;
+    for (int32_t c0 = 0; c0 < W; c0 += 32) {
+        const int32_t x = c0 + lane;
+        int32_t dv = x < W ? D[x] : 0;
+        int32_t inc = warp_inclusive_scan(dv) + icarry;
+        icarry = __shfl_sync(0xffffffffu, inc, 31);
+        if (x < W) {
+            int32_t r;
+            if (!ap) {
+                r = (int32_t)min((int64_t)x + m, (int64_t)W);
+            } else {
+                const int64_t lim = (int64_t)(__ldg(I.ref_rs + G0 + from + x) >> 1) + m;
+                int32_t lo = x, len = W - x;
+                while (len > 0) {
+                    int32_t half = len >> 1;
+                    if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) < lim) {
+                        lo += half + 1;
+                        len -= half + 1;
+                    } else {
+                        len = half;
+                    }
+                }
+                r = lo;
+            }
+            const int32_t I_ = inc, sk = r - x;
+            bool better;
+            if (jac) {
+                const double score = __ddiv_rn((double)I_, (double)(m + sk - I_));
+                better = score > best;
+                if (better) best = score;
+            } else {
+                better = I_ > bI;
+            }
+            if (better) {
+                bl = x;
+                bI = I_;
+                bS = PC[r] - PC[x];
+                br = r;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int32_t obl = __shfl_xor_sync(0xffffffffu, bl, o);
+        int32_t obI = __shfl_xor_sync(0xffffffffu, bI, o);
+        int32_t obS = __shfl_xor_sync(0xffffffffu, bS, o);
+        int32_t obr = __shfl_xor_sync(0xffffffffu, br, o);
+        const bool take = jac ? (ob > best || (ob == best && obl >= 0 && (bl < 0 || obl < bl)))
+                              : (obI > bI || (obI == bI && obl >= 0 && (bl < 0 || obl < bl)));
+        if (take) {
+            best = ob;
+            bl = obl;
+            bI = obI;
+            bS = obS;
+            br = obr;
+        }
+    }
+    if (!jac && bl >= 0) best = __ddiv_rn((double)bI, (double)m);
+    if (lane == 0) {
+        J->score = best;
+        if (bl >= 0) {
+            const int32_t tl = (int32_t)(__ldg(I.ref_rs + G0 + from + bl) >> 1);
+            const int32_t tr = (int32_t)(__ldg(I.ref_rs + G0 + from + br - 1) >> 1);
+            J->t_l = tl;
+            J->t_r = tr;
+            J->inter = bI;
+            J->same = bS;
+            J->s_sz = tr - tl + 1;
+        }
+    }
+}
+
+// Shared slices for the per-seed state of reads with m <= REFINE_SM: the
+// counts and rings are read back within a chunk's dependent chain, so they
+// are kept on chip; the difference array and the strand prefix stay global.
+constexpr int REFINE_SM = 512;
+
+__global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, RefScratch rsc) {
+    __shared__ int32_t s_cnt[REFINE_WARPS][REFINE_SM], s_ring[REFINE_WARPS][REFINE_SM];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t ncand = v.coff[v.n];
@@ -1262,8 +1456,6 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefSc
     int32_t* const D = cntA + rsc.nu_max;
     int32_t* const PC = D + rsc.wmax + 1;
     int32_t* const ring = PC + rsc.wmax + 1;
-    const bool ap = v.P.ap != 0;
-    const DevIndex& I = v.I;
     for (uint32_t ci = wid; ci < ncand; ci += nwarps) {
         BucketJob* J = v.jobs + v.cidx[ci];
         const int32_t q = J->read;
@@ -1278,184 +1470,10 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32) k_refine(BatchView v, RefSc
             }
             continue;
         }
-        const int32_t m = v.r_m[q], n_u = v.r_nu[q];
-        const int64_t h = v.r_half[q];
-        const uint64_t kb = v.kcap_off[q];
-        const int32_t seg = J->seg;
-        const uint32_t G0 = __ldg(I.seg_off + seg), Gend = __ldg(I.seg_off + seg + 1);
-        const int64_t seglen = (int64_t)(Gend - G0);
-        const int64_t from = (int64_t)J->bb * h;
-        const int64_t end = min(((int64_t)J->bb + 2) * h, seglen);
-        const int32_t W = (int32_t)(end - from);
-        if (lane == 0 && W > 0) atomicAdd(&v.mx->refine_kmers, (unsigned long long)W);
-        for (int32_t i = lane; i < n_u; i += 32) cntA[i] = 0;
-        for (int32_t i = lane; i <= W; i += 32) D[i] = 0;
-        __syncwarp();
-        // phase 1: seed of every position, its occurrence interval of windows,
-        // and the prefix PC of strand agreement (+1 same strand, -1 opposite).
-        // REFINE_U chunks of 32 positions at a time: their reference k-mers,
-        // probe lookups and seed records are fetched together, then the chunks
-        // are folded in order.
-        int32_t pc_carry = 0;
-        if (lane == 0) PC[0] = 0;
-        for (int32_t c00 = 0; c00 < W; c00 += 32 * REFINE_U) {
-            uint64_t hx[REFINE_U];
-            uint32_t rsx[REFINE_U], osx[REFINE_U], ooffx[REFINE_U];
-            bool on[REFINE_U];
-            int32_t sx[REFINE_U];
-#pragma unroll
-            for (int u = 0; u < REFINE_U; u++) {
-                const int32_t x = c00 + 32 * u + lane;
-                on[u] = x < W;
-                const uint32_t gid = G0 + (uint32_t)(from + (on[u] ? x : 0));
-                hx[u] = on[u] ? __ldg(I.ref_h + gid) : 0;
-                rsx[u] = on[u] ? __ldg(I.ref_rs + gid) : 0;
-            }
-            pht_lookup_u<REFINE_U>(v, q, hx, on, sx);
-#pragma unroll
-            for (int u = 0; u < REFINE_U; u++) {
-                osx[u] = sx[u] >= 0 ? v.sd_os[kb + sx[u]] : 0u;
-                ooffx[u] = sx[u] >= 0 ? v.sd_ooff[kb + sx[u]] : 0u;
-            }
-#pragma unroll
-            for (int u = 0; u < REFINE_U; u++) {
-                const int32_t c0 = c00 + 32 * u;
-                if (c0 >= W) break;  // warp-uniform
-                const int32_t x = c0 + lane;
-                const bool valid = on[u];
-                const int32_t s = sx[u];
-                const uint32_t os = osx[u], rs = rsx[u];
-                {
-                    const int32_t cv = (valid && s >= 0) ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
-                    const int32_t inc = warp_inclusive_scan(cv);
-                    if (valid) PC[x + 1] = pc_carry + inc;
-                    pc_carry += __shfl_sync(0xffffffffu, inc, 31);
-                }
-                const unsigned peers = __match_any_sync(0xffffffffu, s);
-                int32_t t = 0, occ = 1, rho = 0, gsz = 0;
-                const uint32_t ooff = ooffx[u];
-                if (s >= 0) {
-                    occ = (int32_t)(os >> 1);
-                    rho = __popc(peers & lt);
-                    gsz = __popc(peers);
-                    t = cntA[s] + rho;
-                    int64_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
-                    if (t >= occ) {
-                        if (rho >= occ)  // in this chunk: the peer occ places before this lane
-                            p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
-                        else
-                            p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
-                    }
-                    int64_t Lj;
-                    if (!ap) {
-                        Lj = (int64_t)x - m + 1;
-                    } else {  // first l with R[l] > R[x] - m
-                        const int64_t rv = (int64_t)(rs >> 1) - m;
-                        int32_t lo = 0, len = x;
-                        while (len > 0) {
-                            int32_t half = len >> 1;
-                            if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
-                                lo += half + 1;
-                                len -= half + 1;
-                            } else {
-                                len = half;
-                            }
-                        }
-                        Lj = lo;
-                    }
-                    int64_t st = max(max(p + 1, Lj), (int64_t)0);
-                    if (st <= x) {
-                        atomicAdd(D + st, 1);
-                        atomicAdd(D + x + 1, -1);
-                    }
-                }
-                __syncwarp();
-                if (s >= 0) {
-                    if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = x;
-                    if (rho == gsz - 1) cntA[s] = t + 1;
-                }
-                __syncwarp();
-            }
-        }
-        __syncwarp();
-        // phase 2: intersection per window start, score, first maximum. Under
-        // Containment every score is I / m for the same m, and distinct I < 2^31
-        // give distinct quotients, so the first maximum of I is the first
-        // maximum of the score: the division is done once, for the winner.
-        const bool jac = v.P.metric == 1;
-        double best = -1.0;
-        int32_t bl = -1, bI = -1, bS = 0, br = 0;
-        int32_t icarry = 0;
-        for (int32_t c0 = 0; c0 < W; c0 += 32) {
-            const int32_t x = c0 + lane;
-            int32_t dv = x < W ? D[x] : 0;
-            int32_t inc = warp_inclusive_scan(dv) + icarry;
-            icarry = __shfl_sync(0xffffffffu, inc, 31);
-            if (x < W) {
-                int32_t r;
-                if (!ap) {
-                    r = (int32_t)min((int64_t)x + m, (int64_t)W);
-                } else {
-                    const int64_t lim = (int64_t)(__ldg(I.ref_rs + G0 + from + x) >> 1) + m;
-                    int32_t lo = x, len = W - x;
-                    while (len > 0) {
-                        int32_t half = len >> 1;
-                        if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) < lim) {
-                            lo += half + 1;
-                            len -= half + 1;
-                        } else {
-                            len = half;
-                        }
-                    }
-                    r = lo;
-                }
-                const int32_t I_ = inc, sk = r - x;
-                bool better;
-                if (jac) {
-                    const double score = __ddiv_rn((double)I_, (double)(m + sk - I_));
-                    better = score > best;
-                    if (better) best = score;
-                } else {
-                    better = I_ > bI;
-                }
-                if (better) {
-                    bl = x;
-                    bI = I_;
-                    bS = PC[r] - PC[x];
-                    br = r;
-                }
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            int32_t obl = __shfl_xor_sync(0xffffffffu, bl, o);
-            int32_t obI = __shfl_xor_sync(0xffffffffu, bI, o);
-            int32_t obS = __shfl_xor_sync(0xffffffffu, bS, o);
-            int32_t obr = __shfl_xor_sync(0xffffffffu, br, o);
-            const bool take = jac ? (ob > best || (ob == best && obl >= 0 && (bl < 0 || obl < bl)))
-                                  : (obI > bI || (obI == bI && obl >= 0 && (bl < 0 || obl < bl)));
-            if (take) {
-                best = ob;
-                bl = obl;
-                bI = obI;
-                bS = obS;
-                br = obr;
-            }
-        }
-        if (!jac && bl >= 0) best = __ddiv_rn((double)bI, (double)m);
-        if (lane == 0) {
-            J->score = best;
-            if (bl >= 0) {
-                const int32_t tl = (int32_t)(__ldg(I.ref_rs + G0 + from + bl) >> 1);
-                const int32_t tr = (int32_t)(__ldg(I.ref_rs + G0 + from + br - 1) >> 1);
-                J->t_l = tl;
-                J->t_r = tr;
-                J->inter = bI;
-                J->same = bS;
-                J->s_sz = tr - tl + 1;
-            }
-        }
+        if (v.r_m[q] <= REFINE_SM)  // then n_u <= m and the rings hold m positions
+            refine_one(v, J, q, s_cnt[wib], D, PC, s_ring[wib], lane, lt);
+        else
+            refine_one(v, J, q, cntA, D, PC, ring, lane, lt);
         __syncwarp();
     }
 }
