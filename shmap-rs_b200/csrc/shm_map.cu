@@ -69,6 +69,13 @@ struct HostReads {
     BatchMax fin;        // after the sweep
 };
 
+// A seed of a read, in rarest-first order: its hit-list start and length in
+// the index, occurrences << 1 | strand of its smallest r, and the offset of
+// its occurrences among all of the read's (one 16-byte load for every reader).
+struct __align__(16) SeedRec {
+    uint32_t a, cnt, os, ooff;
+};
+
 struct BatchView {
     int32_t n;
     DevParams P;
@@ -80,8 +87,8 @@ struct BatchView {
     uint32_t* kcnt;
     uint64_t* km_h;
     uint32_t* km_rs;
-    uint64_t* sd_h;
-    uint32_t *sd_a, *sd_cnt, *sd_os, *sd_hpre, *sd_ooff;
+    SeedRec* sd;        // per read, its seeds in rarest-first order
+    uint32_t* sd_hpre;  // hit words before each processed seed
     const uint64_t* pht_off;
     uint64_t* pht_key;
     uint32_t* pht_val;
@@ -185,22 +192,6 @@ __device__ void bitonic_u64(uint64_t* A, uint32_t P) {
 }
 
 // The sketch hashes are uniform in [0, thr], so their low bits pick the slot.
-__device__ __forceinline__ bool pht_lookup(const BatchView& v, int32_t q, uint64_t h, uint32_t& idx) {
-    const uint64_t base = v.pht_off[q];
-    const uint64_t mask = v.pht_off[q + 1] - base - 1;
-    uint64_t i = h & mask;
-    for (;;) {
-        const uint32_t val = v.pht_val[base + i];
-        const uint64_t key = v.pht_key[base + i];
-        if (val == 0xffffffffu) return false;
-        if (key == h) {
-            idx = val;
-            return true;
-        }
-        i = (i + 1) & mask;
-    }
-}
-
 __device__ __forceinline__ void pht_insert(const BatchView& v, int32_t q, uint64_t h, uint32_t idx) {
     const uint64_t base = v.pht_off[q];
     const uint64_t mask = v.pht_off[q + 1] - base - 1;
@@ -378,11 +369,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
         const uint64_t e = S_.E[i];
         const uint32_t g = (uint32_t)(e & 0xffffffffu), cnt = (uint32_t)(e >> 32);
         const uint32_t os = S_.GB[g], occs = os >> 1;
-        v.sd_h[kb + i] = S_.GA[g];
-        v.sd_os[kb + i] = os;
-        v.sd_cnt[kb + i] = cnt;
-        v.sd_a[kb + i] = S_.GD[g];
-        v.sd_ooff[kb + i] = po;
+        v.sd[kb + i] = SeedRec{S_.GD[g], cnt, os, po};
         if ((int64_t)po < (int64_t)S) {
             v.sd_hpre[kb + i] = (uint32_t)pc;
             l_np++;
@@ -779,11 +766,7 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
         const uint32_t po = po_carry + oi - occs;
         const uint64_t pc = pc_carry + ci - cnt;
         if (valid) {
-            v.sd_h[kb + i] = Sh[g];
-            v.sd_os[kb + i] = os;
-            v.sd_cnt[kb + i] = cnt;
-            v.sd_a[kb + i] = Ra[g];
-            v.sd_ooff[kb + i] = po;
+            v.sd[kb + i] = SeedRec{Ra[g], cnt, os, po};
             if ((int64_t)po < (int64_t)S) {
                 v.sd_hpre[kb + i] = (uint32_t)pc;
                 l_np++;
@@ -1007,7 +990,8 @@ __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
         uint32_t h = (uint32_t)v.r_half[q];
         uint32_t j = ub_u32(v.sd_hpre + kb, np, (uint32_t)(w - v.hw_off[q])) - 1;
         uint32_t t = (uint32_t)(w - v.hw_off[q]) - v.sd_hpre[kb + j];
-        uint32_t a = v.sd_a[kb + j], cnt = v.sd_cnt[kb + j], os = v.sd_os[kb + j];
+        SeedRec sr = v.sd[kb + j];
+        uint32_t a = sr.a, cnt = sr.cnt, os = sr.os;
         int32_t seg = -1;
         uint32_t s_lo = 0, s_hi = 0;
         int32_t seg_p = -1;  // bucket of the seed's previous hit (seg_p < 0: none)
@@ -1058,9 +1042,10 @@ __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
                     h = (uint32_t)v.r_half[q];
                     j = ub_u32(v.sd_hpre + kb, np, 0u) - 1;  // past the seeds without hits
                 }
-                a = v.sd_a[kb + j];
-                cnt = v.sd_cnt[kb + j];
-                os = v.sd_os[kb + j];
+                sr = v.sd[kb + j];
+                a = sr.a;
+                cnt = sr.cnt;
+                os = sr.os;
             }
         }
     }
@@ -1149,11 +1134,12 @@ __global__ void __launch_bounds__(256) k_extend(BatchView v) {
             const bool valid = i < n_u;
             int32_t ds = 0, dm = 0, dc = 0, rmn = INT32_MAX, rmx = -1;
             if (valid) {
-                const uint32_t os = v.sd_os[kb + i], cnt = v.sd_cnt[kb + i];
+                const SeedRec sr = v.sd[kb + i];
+                const uint32_t os = sr.os, cnt = sr.cnt;
                 ds = (int32_t)(os >> 1);
                 if (cnt > 0) {
                     uint32_t A, B;
-                    seed_range(v.I, v.sd_a[kb + i], cnt, seg, (int64_t)bb * h, ((int64_t)bb + 2) * h, ap, A, B);
+                    seed_range(v.I, sr.a, cnt, seg, (int64_t)bb * h, ((int64_t)bb + 2) * h, ap, A, B);
                     Agg g = range_agg(v.I, A, B, os & 1u);
                     dm = min(g.count, ds);
                     dc = g.codir;
@@ -1297,8 +1283,9 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
         pht_lookup_u<REFINE_U>(v, q, hx, on, sx);
 #pragma unroll
         for (int u = 0; u < REFINE_U; u++) {
-            osx[u] = sx[u] >= 0 ? v.sd_os[kb + sx[u]] : 0u;
-            ooffx[u] = sx[u] >= 0 ? v.sd_ooff[kb + sx[u]] : 0u;
+            const SeedRec sr = sx[u] >= 0 ? v.sd[kb + sx[u]] : SeedRec{0u, 0u, 0u, 0u};
+            osx[u] = sr.os;
+            ooffx[u] = sr.ooff;
         }
 #pragma unroll
         for (int u = 0; u < REFINE_U; u++) {
@@ -1738,8 +1725,9 @@ struct MapScratch {
     DevBuf<shm_map_record> retry_out;
     DevBuf<int64_t> retry_list;
     DevBuf<int32_t> retry_idx;
-    DevBuf<uint64_t> km_h, sd_h, pht_key, hw, hw_off, bt_size, bt_off;
-    DevBuf<uint32_t> kcnt, km_rs, sd_a, sd_cnt, sd_os, sd_hpre, sd_ooff, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
+    DevBuf<uint64_t> km_h, pht_key, hw, hw_off, bt_size, bt_off;
+    DevBuf<SeedRec> sd;
+    DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
         cidx, sort_scr, ovf_list, r_flags;
     DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
@@ -1995,12 +1983,8 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     S.kcnt.reserve((size_t)n);
     S.km_h.reserve(kcap + 1);
     S.km_rs.reserve(kcap + 1);
-    S.sd_h.reserve(kcap + 1);
-    S.sd_a.reserve(kcap + 1);
-    S.sd_cnt.reserve(kcap + 1);
-    S.sd_os.reserve(kcap + 1);
+    S.sd.reserve(kcap + 1);
     S.sd_hpre.reserve(kcap + 1);
-    S.sd_ooff.reserve(kcap + 1);
     S.pht_key.reserve(phtn);
     S.pht_val.reserve(phtn);
     S.r_i32.reserve((size_t)n * 8);
@@ -2056,12 +2040,8 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     v.kcnt = S.kcnt.p;
     v.km_h = S.km_h.p;
     v.km_rs = S.km_rs.p;
-    v.sd_h = S.sd_h.p;
-    v.sd_a = S.sd_a.p;
-    v.sd_cnt = S.sd_cnt.p;
-    v.sd_os = S.sd_os.p;
+    v.sd = S.sd.p;
     v.sd_hpre = S.sd_hpre.p;
-    v.sd_ooff = S.sd_ooff.p;
     v.pht_off = dp.pht_off;
     v.pht_key = S.pht_key.p;
     v.pht_val = S.pht_val.p;
