@@ -1309,22 +1309,23 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
                 rho = __popc(peers & lt);
                 gsz = __popc(peers);
                 t = cntA[s] + rho;
-                int64_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
+                int32_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
+                // (positions, r and m are below 2^31: 32-bit arithmetic throughout)
                 if (t >= occ) {
                     if (rho >= occ)  // in this chunk: the peer occ places before this lane
                         p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
                     else
                         p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
                 }
-                int64_t Lj;
+                int32_t Lj;
                 if (!ap) {
-                    Lj = (int64_t)x - m + 1;
+                    Lj = x - m + 1;
                 } else {  // first l with R[l] > R[x] - m
-                    const int64_t rv = (int64_t)(rs >> 1) - m;
+                    const int32_t rv = (int32_t)(rs >> 1) - m;
                     int32_t lo = 0, len = x;
                     while (len > 0) {
                         int32_t half = len >> 1;
-                        if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
+                        if ((int32_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
                             lo += half + 1;
                             len -= half + 1;
                         } else {
@@ -1333,7 +1334,7 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
                     }
                     Lj = lo;
                 }
-                int64_t st = max(max(p + 1, Lj), (int64_t)0);
+                const int32_t st = max(max(p + 1, Lj), 0);
                 if (st <= x) {
                     atomicAdd(D + st, 1);
                     atomicAdd(D + x + 1, -1);
@@ -1364,13 +1365,13 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
         if (x < W) {
             int32_t r;
             if (!ap) {
-                r = (int32_t)min((int64_t)x + m, (int64_t)W);
+                r = min(x + m, W);
             } else {
-                const int64_t lim = (int64_t)(__ldg(I.ref_rs + G0 + from + x) >> 1) + m;
+                const int32_t lim = (int32_t)(__ldg(I.ref_rs + G0 + from + x) >> 1) + m;
                 int32_t lo = x, len = W - x;
                 while (len > 0) {
                     int32_t half = len >> 1;
-                    if ((int64_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) < lim) {
+                    if ((int32_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) < lim) {
                         lo += half + 1;
                         len -= half + 1;
                     } else {
