@@ -903,6 +903,18 @@ __device__ __forceinline__ Agg range_agg(const DevIndex& I, uint32_t A, uint32_t
     return r;
 }
 
+// A bucket's matches and codirection sum in one 64-bit word: the sum of
+// packed values is matches_sum << 32 plus codir_sum (two's complement), and
+// both sums stay below 2^31 in magnitude, so the low half is codir_sum and
+// the rest is matches_sum.
+__device__ __forceinline__ unsigned long long bt_pack(int32_t matches, int32_t codir) {
+    return ((unsigned long long)(uint32_t)matches << 32) + (unsigned long long)(long long)codir;
+}
+__device__ __forceinline__ void bt_unpack(unsigned long long mc, int32_t& matches, int32_t& codir) {
+    codir = (int32_t)(uint32_t)mc;
+    matches = (int32_t)((mc - (unsigned long long)(long long)codir) >> 32);
+}
+
 __device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t seg, int64_t bb, int32_t matches,
                                        int32_t codir, int32_t rmin, int32_t rmax) {
     const uint64_t base = v.bt_off[q];
@@ -927,8 +939,7 @@ __device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t se
         if (prev == key) break;
         i = (i + 1) & mask;
     }
-    atomicAdd(&s->matches, matches);
-    atomicAdd(&s->codir, codir);
+    atomicAdd(&s->mc, bt_pack(matches, codir));
     atomicMin(&s->rmin, rmin);
     atomicMax(&s->rmax, rmax);
 }
@@ -1057,8 +1068,7 @@ __global__ void k_bt_init(BSlot* bt, const uint64_t* __restrict__ total) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         BSlot s;
         s.key = EMPTY_KEY;
-        s.matches = 0;
-        s.codir = 0;
+        s.mc = 0;
         s.rmin = INT32_MAX;
         s.rmax = -1;
         bt[i] = s;
@@ -1084,9 +1094,11 @@ __global__ void __launch_bounds__(256) k_bscan(BatchView v) {
             jb.read = q;
             jb.seg = (int32_t)(s.key >> 32);
             jb.bb = (int32_t)(s.key & 0xffffffffu);
-            jb.m0 = s.matches;
-            jb.matches = s.matches;
-            jb.codir = s.codir;
+            int32_t s_matches, s_codir;
+            bt_unpack(s.mc, s_matches, s_codir);
+            jb.m0 = s_matches;
+            jb.matches = s_matches;
+            jb.codir = s_codir;
             jb.rmin = s.rmin;
             jb.rmax = s.rmax;
             jb.pad0 = jb.pad1 = 0;
@@ -1096,7 +1108,7 @@ __global__ void __launch_bounds__(256) k_bscan(BatchView v) {
                 jb.sh = 1.0;  // seed_heuristic_pass does nothing under NBP (pruning.rs:351)
                 jb.is_cand = 1;
             } else {
-                const double sh0 = hseed(v.r_m[q], v.r_S0[q], s.matches);
+                const double sh0 = hseed(v.r_m[q], v.r_S0[q], s_matches);
                 if (sh0 < v.P.theta_low) continue;
                 jb.sh = sh0;
                 jb.is_cand = 0;
@@ -1785,10 +1797,8 @@ void mapctx_destroy(MapCtx* c) {
     delete c;
 }
 
-static uint64_t pow2_host(uint64_t x) {
-    uint64_t p = 1;
-    while (p < x) p <<= 1;
-    return p;
+static uint64_t pow2_host(uint64_t x) {  // smallest power of two >= x (1 for x <= 1)
+    return x <= 1 ? 1 : (uint64_t)1 << (64 - __builtin_clzll(x - 1));
 }
 
 // k-mer capacity of a read of nw windows: the reference's own estimate

@@ -14,7 +14,8 @@ namespace shm {
 // content after seeding (src/buckets.rs:64-73).
 struct BSlot {
     unsigned long long key;  // (u64)segm_id << 32 | b, EMPTY_KEY when free
-    int32_t matches, codir, rmin, rmax;
+    unsigned long long mc;   // matches << 32 plus codir (signed), summed by one 64-bit atomic add
+    int32_t rmin, rmax;
 };
 
 // A bucket taken past seeding: extended by the seed heuristic, then (if it
