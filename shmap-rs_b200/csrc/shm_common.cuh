@@ -101,6 +101,17 @@ __device__ __forceinline__ int32_t seg_of(const DevIndex& I, uint32_t g) {
     return lo;
 }
 
+// The same over a copy of seg_off (for instance in shared memory).
+__device__ __forceinline__ int32_t seg_of_in(const uint32_t* seg_off, int32_t n_seg, uint32_t g) {
+    int32_t lo = 0, hi = n_seg;
+    while (hi - lo > 1) {
+        int32_t mid = (lo + hi) >> 1;
+        if (seg_off[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // SketchIndex::count + hit-list lookup (src/index.rs:192-213).
 __device__ __forceinline__ bool idx_lookup(const DevIndex& I, uint64_t h, uint32_t& a, uint32_t& cnt) {
     cnt = 0;

@@ -543,10 +543,12 @@ __device__ __forceinline__ void pht_insert_u(const BatchView& v, int32_t q, cons
 }
 
 // seed_bucket_bound summed over U seeds of one lane (those with on[u]); the
-// hit-list ends of the U seeds are loaded together.
+// hit-list ends of the U seeds are loaded together, and their segments found
+// in `segs`, a copy of seg_off.
 template <int U>
 __device__ __forceinline__ uint64_t seed_bucket_bound_u(const BatchView& v, const uint32_t (&a)[U],
-                                                        const uint32_t (&cnt)[U], const bool (&on)[U], int64_t h) {
+                                                        const uint32_t (&cnt)[U], const bool (&on)[U], int64_t h,
+                                                        const uint32_t* segs) {
     uint32_t g0[U], g1[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -564,7 +566,7 @@ __device__ __forceinline__ uint64_t seed_bucket_bound_u(const BatchView& v, cons
             sum += 2ULL * cnt[u];
             continue;
         }
-        const int32_t s0 = seg_of(v.I, g0[u]), s1 = seg_of(v.I, g1[u]);
+        const int32_t s0 = seg_of_in(segs, v.I.n_seg, g0[u]), s1 = seg_of_in(segs, v.I.n_seg, g1[u]);
         const uint64_t span = (uint64_t)(g1[u] - g0[u]) / (uint64_t)h + 1 + 3ULL * (uint64_t)(s1 - s0 + 1);
         sum += min((uint64_t)(2ULL * cnt[u]), span);
     }
@@ -585,7 +587,8 @@ __device__ __forceinline__ uint64_t seed_bucket_bound_u(const BatchView& v, cons
 //   Ra (4C): each group's hit-list start
 //   P0, P1 (4C each): radix permutations; RH (256 words): digit offsets
 __host__ __device__ constexpr size_t seedc_bytes(uint32_t C) { return 28 * (size_t)C + 1024; }
-constexpr int SEEDC_U = 4;  // groups a lane probes at once
+constexpr int SEEDC_U = 4;       // groups a lane probes at once
+constexpr int SEEDC_SEGS = 1024;  // references with at most this many segments keep seg_off in shared memory
 
 // Exclusive scan, in place, of the n (a multiple of 32) words X[0..n): lane l
 // owns n/32 consecutive words.
@@ -601,7 +604,7 @@ __device__ __forceinline__ void warp_scan_words(uint32_t* X, uint32_t n, int lan
     }
 }
 
-__device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_t* base) {
+__device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_t* base, const uint32_t* segs) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u, le = lt | (1u << lane);
     uint32_t m;
@@ -801,7 +804,7 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
             a[u] = on[u] ? Ra[g] : 0u;
             cnt[u] = on[u] ? Rc[g] : 0u;
         }
-        l_eb += seed_bucket_bound_u<SEEDC_U>(v, a, cnt, proc, halflen);
+        l_eb += seed_bucket_bound_u<SEEDC_U>(v, a, cnt, proc, halflen, segs);
         pht_insert_u<SEEDC_U>(v, q, hh, ii, on);
     }
 #pragma unroll
@@ -835,11 +838,17 @@ template <uint32_t C, int W>
 __global__ void __launch_bounds__(W * 32) k_seedprep_c(BatchView v, const int32_t* __restrict__ list,
                                                        const uint32_t* __restrict__ n_list) {
     extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint32_t s_seg[SEEDC_SEGS + 1];  // seg_off, for references of at most SEEDC_SEGS segments
     const int wib = threadIdx.x >> 5;
     uint8_t* base = smem + (size_t)wib * seedc_bytes(C);
     const int32_t n = (int32_t)*n_list;
+    const bool staged = v.I.n_seg <= SEEDC_SEGS;
+    if (staged)
+        for (int i = threadIdx.x; i <= v.I.n_seg; i += blockDim.x) s_seg[i] = __ldg(v.I.seg_off + i);
+    __syncthreads();
+    const uint32_t* segs = staged ? s_seg : v.I.seg_off;
     for (int32_t li = blockIdx.x * W + wib; li < n; li += gridDim.x * W) {
-        seedprep_count(v, list[li], C, base);
+        seedprep_count(v, list[li], C, base, segs);
         __syncwarp();
     }
 }
