@@ -61,7 +61,6 @@ constexpr int SK_TILE_CAP = SK_THREADS * SKETCH_WIN + 1024;       // bytes a CTA
 constexpr int SK_TILE_WORDS = SK_TILE_CAP / 4 + 8;                // + slack for the word past the last byte
 constexpr int SK_TILE_PWORDS = SK_TILE_WORDS + SK_TILE_WORDS / 32 + 1;
 constexpr int SK_TILE_BYTES = (SK_TILE_PWORDS * 4 + 15) / 16 * 16; // the tile, rounded to 16 bytes
-constexpr int SK_TB = 4;                                          // selections a thread buffers (append mode)
 
 // Staged bytes carry one pad word after every 32 words: the runs of
 // neighbouring threads start SKETCH_WIN bytes apart, so without the pad every
@@ -92,29 +91,24 @@ struct GlobalBytes {
     __device__ __forceinline__ uint32_t byte(int64_t x) const { return __ldg(base + x); }
 };
 
-// Where a thread's selections go. Count and write modes: a counter and the
-// run's own output range. Append mode: SK_TB slots of shared memory
-// (thread-interleaved), emptied into the read's list when full and at the end
-// of the run.
+constexpr int SK_LB = 16;  // selections a thread holds per run (append mode)
+
+// Where a thread's selections go: its count, and (write mode) the run's
+// output range from chunk_out[c]. Append
+// mode holds the run's first SK_LB selections in thread-local slots (cached
+// local memory), moved to the read's list after the run with one counter
+// update per read and warp; selections past SK_LB take a slot of the list
+// one at a time.
 struct Emit {
     uint64_t out_base;
     uint32_t out_cap, n_sel;
-    uint64_t* bh;  // bh[j * SK_THREADS], br[j * SK_THREADS]: this thread's slots
-    uint32_t* br;
+    uint64_t bh[SK_LB];
+    uint32_t br[SK_LB];
 };
 
-// Reserves n slots of read q's list and writes this thread's buffered selections there.
-__device__ __forceinline__ void drain(const SketchArgs& a, int32_t q, Emit& e, uint32_t base) {
-    for (uint32_t j = 0; j < e.n_sel; j++) {
-        const uint32_t slot = base + j;
-        if (slot < e.out_cap) {
-            a.out_h[e.out_base + slot] = e.bh[j * SK_THREADS];
-            a.out_rs[e.out_base + slot] = e.br[j * SK_THREADS];
-        }
-    }
-    e.n_sel = 0;
-}
-
+// One selection, recorded by the kernel's mode. The bodies stay short (no
+// loops, no waits on results): they sit in the rolling loop's rarely taken
+// branch, and anything larger there slows every window.
 template <int MODE>
 __device__ __forceinline__ void emit_kmer(const SketchArgs& a, int32_t q, uint64_t h, uint32_t rs, Emit& e) {
     if (MODE == SK_COUNT) {
@@ -123,11 +117,16 @@ __device__ __forceinline__ void emit_kmer(const SketchArgs& a, int32_t q, uint64
         a.out_h[e.out_base + e.n_sel] = h;
         a.out_rs[e.out_base + e.n_sel] = rs;
         e.n_sel++;
-    } else {
-        if (e.n_sel == SK_TB) drain(a, q, e, atomicAdd(a.kmer_cnt + q, (uint32_t)SK_TB));
-        e.bh[e.n_sel * SK_THREADS] = h;
-        e.br[e.n_sel * SK_THREADS] = rs;
+    } else if (e.n_sel < (uint32_t)SK_LB) {
+        e.bh[e.n_sel] = h;
+        e.br[e.n_sel] = rs;
         e.n_sel++;
+    } else {
+        const uint32_t slot = atomicAdd(a.kmer_cnt + q, 1u);
+        if (slot < e.out_cap) {
+            a.out_h[e.out_base + slot] = h;
+            a.out_rs[e.out_base + slot] = rs;
+        }
     }
 }
 
@@ -199,12 +198,8 @@ __device__ __forceinline__ void sketch_run(const SketchArgs& a, const LutPair* _
     }
 }
 
-// Dynamic shared memory of a k_sketch CTA: the staged tile, then (append
-// mode) the threads' selection slots: hashes, then r << 1 | strand.
-static_assert(SK_TILE_BYTES % 16 == 0, "the selection slots stay 8-byte aligned");
-constexpr size_t sk_dyn_bytes(int mode) {
-    return (size_t)SK_TILE_BYTES + (mode == SK_APPEND ? (size_t)SK_TB * SK_THREADS * 12 : 0);
-}
+// Dynamic shared memory of a k_sketch CTA: the staged tile.
+constexpr size_t sk_dyn_bytes(int) { return (size_t)SK_TILE_BYTES; }
 
 // Each CTA takes tiles of SK_THREADS consecutive runs. Runs are laid out in
 // sequence order, so a tile's bytes are one contiguous range of `seq`: it is
@@ -222,11 +217,7 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
         Lin[i] = LutPair{luts->fw[i], luts->rc_k1[i]};
         Lout[i] = LutPair{luts->fw_k[i], luts->rc_r1[i]};
     }
-    Emit e{0, 0, 0, nullptr, nullptr};
-    if (MODE == SK_APPEND) {
-        e.bh = (uint64_t*)(sk_dyn + SK_TILE_BYTES) + threadIdx.x;
-        e.br = (uint32_t*)(sk_dyn + SK_TILE_BYTES + (size_t)SK_TB * SK_THREADS * 8) + threadIdx.x;
-    }
+    Emit e;
     const int lane = threadIdx.x & 31;
     const int k = a.k;
     const uint64_t thr = a.thr;
@@ -314,9 +305,9 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
             sketch_run<MODE>(a, Lin, Lout, GlobalBytes{A0, first, lim}, x, cnt, k, thr, q, r0, e);
         if (MODE == SK_COUNT && c < n_chunks) a.chunk_cnt[c] = e.n_sel;
         if (MODE == SK_APPEND) {
-            // every lane: the run's buffered selections go to the read's list, one
-            // counter update per read and warp (a warp's runs are consecutive, so
-            // the lanes of one read are contiguous)
+            // the held selections go to the read's list: a warp's runs are
+            // consecutive, so the lanes of one read are contiguous and take one
+            // range of the list between them
             const uint32_t nb = e.n_sel;
             uint32_t incl = nb;
 #pragma unroll
@@ -324,15 +315,19 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
                 const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
-            const uint32_t excl = incl - nb;
             const unsigned peers = __match_any_sync(0xffffffffu, cnt > 0 ? q : -1);
             const int leader = __ffs(peers) - 1, last = 31 - __clz(peers);
-            const uint32_t g0 = __shfl_sync(0xffffffffu, excl, leader);
+            const uint32_t g0 = __shfl_sync(0xffffffffu, incl - nb, leader);
             const uint32_t gtot = __shfl_sync(0xffffffffu, incl, last) - g0;
             uint32_t base = 0;
             if (lane == leader && cnt > 0 && gtot) base = atomicAdd(a.kmer_cnt + q, gtot);
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (nb) drain(a, q, e, base + excl - g0);
+            base = __shfl_sync(0xffffffffu, base, leader) + (incl - nb) - g0;
+            for (uint32_t j = 0; j < nb; j++) {
+                if (base + j < e.out_cap) {
+                    a.out_h[e.out_base + base + j] = e.bh[j];
+                    a.out_rs[e.out_base + base + j] = e.br[j];
+                }
+            }
         }
         __syncthreads();  // the tile is free for the next one
     }
