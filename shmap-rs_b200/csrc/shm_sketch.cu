@@ -71,7 +71,6 @@ __device__ __forceinline__ int pword(int w) { return w + (w >> 5); }
 struct StagedBytes {
     const uint32_t* tile;
     __device__ __forceinline__ uint32_t word(int w) const { return tile[pword(w)]; }
-    __device__ __forceinline__ uint32_t byte(int x) const { return (tile[pword(x >> 2)] >> (8 * (x & 3))) & 0xffu; }
 };
 
 // The same bytes read from global memory (a tile too large to stage): bytes
@@ -88,7 +87,6 @@ struct GlobalBytes {
         }
         return v;
     }
-    __device__ __forceinline__ uint32_t byte(int64_t x) const { return __ldg(base + x); }
 };
 
 constexpr int SK_LB = 16;  // selections a thread holds per run (append mode)
@@ -130,6 +128,9 @@ __device__ __forceinline__ void emit_kmer(const SketchArgs& a, int32_t q, uint64
     }
 }
 
+// Byte j of a word, as a table index (one byte permute).
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, int j) { return __byte_perm(w, 0u, 0x4440u + (uint32_t)j); }
+
 // One rolling step: byte ib enters, byte ob leaves.
 __device__ __forceinline__ void roll(uint64_t& fw, uint64_t& rc, const LutPair* __restrict__ Lin,
                                      const LutPair* __restrict__ Lout, uint32_t ib, uint32_t ob) {
@@ -163,10 +164,23 @@ __device__ __forceinline__ void sketch_run(const SketchArgs& a, const LutPair* _
     if (cnt <= 0) return;
     const uint32_t thr_hi = (uint32_t)(thr >> 32);
     uint64_t fw = 0, rc = 0;
-    for (int i = 0; i < k; i++) {
-        const LutPair pi = Lin[src.byte(x + i)];
-        fw = rotl1(fw) ^ pi.a;
-        rc = rotr1(rc) ^ pi.b;
+    {  // bytes x .. x+k-1, four per word read (bytes past x+k-1 are read, not used)
+        const uint32_t sh = (uint32_t)(x & 3) * 8;
+        Idx w = x >> 2;
+        uint32_t lw = src.word(w);
+        for (int i = 0; i < k; i += 4) {
+            const uint32_t hw = src.word(++w);
+            const uint32_t b4 = __funnelshift_r(lw, hw, sh);
+            lw = hw;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (i + j < k) {
+                    const LutPair pi = Lin[byte_of(b4, j)];
+                    fw = rotl1(fw) ^ pi.a;
+                    rc = rotr1(rc) ^ pi.b;
+                }
+            }
+        }
     }
     check<MODE>(a, fw, rc, thr_hi, thr, q, r0, e);
     const Idx xi = x + k, xo = x;
@@ -181,7 +195,7 @@ __device__ __forceinline__ void sketch_run(const SketchArgs& a, const LutPair* _
         lo_ = hi_o;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            roll(fw, rc, Lin, Lout, (ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu);
+            roll(fw, rc, Lin, Lout, byte_of(ib4, j), byte_of(ob4, j));
             check<MODE>(a, fw, rc, thr_hi, thr, q, r0 + t + j, e);
         }
     }
@@ -191,7 +205,7 @@ __device__ __forceinline__ void sketch_run(const SketchArgs& a, const LutPair* _
 #pragma unroll
         for (int j = 0; j < 3; j++) {
             if (t + j < cnt) {
-                roll(fw, rc, Lin, Lout, (ib4 >> (8 * j)) & 0xffu, (ob4 >> (8 * j)) & 0xffu);
+                roll(fw, rc, Lin, Lout, byte_of(ib4, j), byte_of(ob4, j));
                 check<MODE>(a, fw, rc, thr_hi, thr, q, r0 + t + j, e);
             }
         }
