@@ -59,6 +59,8 @@ namespace shm {
 struct BatchMax {
     unsigned int m_max, nu_max, half_max, n_overflow;
     unsigned long long kmers, distinct, proc_seeds, hits, buckets, ext_seeds, refine_kmers;
+    unsigned int refine_next;  // next candidate chunk k_refine_chip takes
+    unsigned int n_far;        // candidates refined by k_refine (listed in cfar)
 };
 
 // Small device-to-host reads of a batch, landing in pinned memory.
@@ -88,6 +90,7 @@ struct BatchView {
     uint64_t* km_h;
     uint32_t* km_rs;
     SeedRec* sd;        // per read, its seeds in rarest-first order
+    uint64_t* sd_h;     // per read, the hash of each seed (reads refined on chip only)
     uint32_t* sd_hpre;  // hit words before each processed seed
     const uint64_t* pht_off;
     uint64_t* pht_key;
@@ -104,6 +107,7 @@ struct BatchView {
     uint32_t* n_jobs;
     uint32_t job_cap;
     uint32_t *ccnt, *coff, *ccur, *cidx;
+    uint32_t* cfar;  // the jobs of the candidates not refined on chip (mx->n_far of them)
     uint32_t* ovf_list;
     BatchMax* mx;
     shm_map_record* out;
@@ -189,6 +193,17 @@ __device__ void bitonic_u64(uint64_t* A, uint32_t P) {
             }
             __syncthreads();
         }
+}
+
+// Reads refined on chip (k_refine_chip): Containment or Jaccard without
+// absolute positions, m and the bucket half-length at most RCHIP_M, so that
+// the read's seed table, per-seed state and a window's difference array fit
+// a warp's shared slice. Their seed preparation writes the seed hashes
+// (sd_h) instead of the global probe table; every other read keeps the
+// global table and k_refine.
+constexpr int RCHIP_M = 248;
+__device__ __forceinline__ bool refine_on_chip(const DevParams& P, uint32_t m, int32_t halflen) {
+    return !P.ap && P.metric != 2 && m <= (uint32_t)RCHIP_M && halflen <= RCHIP_M;
 }
 
 // The sketch hashes are uniform in [0, thr], so their low bits pick the slot.
@@ -756,6 +771,8 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
 
     // seeding prefix: seed i is processed iff sum(occs before i) < S
     // (seeding.rs:101); the processed seeds are a prefix of the order
+    const bool chip = refine_on_chip(v.P, m, halflen);
+    const bool pht = !chip && v.P.metric != 2;  // bucket_SH refines nothing
     uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
     uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
     for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
@@ -770,6 +787,7 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
         const uint64_t pc = pc_carry + ci - cnt;
         if (valid) {
             v.sd[kb + i] = SeedRec{Ra[g], cnt, os, po};
+            if (chip) v.sd_h[kb + i] = Sh[g];
             if ((int64_t)po < (int64_t)S) {
                 v.sd_hpre[kb + i] = (uint32_t)pc;
                 l_np++;
@@ -805,7 +823,7 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
             cnt[u] = on[u] ? Rc[g] : 0u;
         }
         l_eb += seed_bucket_bound_u<SEEDC_U>(v, a, cnt, proc, halflen, segs);
-        pht_insert_u<SEEDC_U>(v, q, hh, ii, on);
+        if (pht) pht_insert_u<SEEDC_U>(v, q, hh, ii, on);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) l_eb += __shfl_xor_sync(0xffffffffu, l_eb, o);
@@ -1200,12 +1218,27 @@ __global__ void __launch_bounds__(256) k_extend(BatchView v) {
 }
 
 // ------------------------------------------------------------------ K6 candidates per read
+// Also lists the candidates k_refine takes (those not refined on chip), one
+// counter update per warp.
 __global__ void k_cidx(BatchView v) {
     const uint32_t njobs = min(*v.n_jobs, v.job_cap);
-    for (uint32_t ji = blockIdx.x * blockDim.x + threadIdx.x; ji < njobs; ji += gridDim.x * blockDim.x) {
-        if (!v.jobs[ji].is_cand) continue;
-        const int32_t q = v.jobs[ji].read;
-        v.cidx[v.coff[q] + atomicAdd(v.ccur + q, 1u)] = ji;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < njobs; b += gridDim.x * blockDim.x) {
+        const uint32_t ji = b + (uint32_t)lane;
+        bool far = false;
+        if (ji < njobs && v.jobs[ji].is_cand) {
+            const int32_t q = v.jobs[ji].read;
+            v.cidx[v.coff[q] + atomicAdd(v.ccur + q, 1u)] = ji;
+            far = !refine_on_chip(v.P, (uint32_t)v.r_m[q], v.r_half[q]);
+        }
+        const unsigned fm = __ballot_sync(0xffffffffu, far);
+        if (fm) {
+            const int leader = __ffs(fm) - 1;
+            uint32_t at = 0;
+            if (lane == leader) at = atomicAdd(&v.mx->n_far, (uint32_t)__popc(fm));
+            at = __shfl_sync(0xffffffffu, at, leader);
+            if (far) v.cfar[at + __popc(fm & ((1u << lane) - 1u))] = ji;
+        }
     }
 }
 
@@ -1460,13 +1493,13 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t ncand = v.coff[v.n];
+    const uint32_t nfar = v.mx->n_far;
     int32_t* const cntA = rsc.base + (size_t)wid * rsc.per_warp;
     int32_t* const D = cntA + rsc.nu_max;
     int32_t* const PC = D + rsc.wmax + 1;
     int32_t* const ring = PC + rsc.wmax + 1;
-    for (uint32_t ci = wid; ci < ncand; ci += nwarps) {
-        BucketJob* J = v.jobs + v.cidx[ci];
+    for (uint32_t ci = wid; ci < nfar; ci += nwarps) {
+        BucketJob* J = v.jobs + v.cfar[ci];
         const int32_t q = J->read;
         if (v.P.metric == 2) {  // bucket_SH (scoring.rs:311-325)
             if (lane == 0) {
@@ -1484,6 +1517,288 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
         else
             refine_one(v, J, q, cntA, D, PC, ring, lane, lt);
         __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ K7 refinement on chip
+// Candidates of the reads refine_on_chip selects, a warp at a time: the
+// read's seed table is built in the warp's shared slice from its seed hashes
+// and records, then its candidate windows are refined against it, with the
+// per-seed counts and rings and the window's difference array on chip too.
+// Only the reference k-mers of the windows are read from global memory.
+// Per-warp slice (7 KB, so that four 8-warp CTAs fit an SM):
+//   tslot  u16[RCHIP_T]      probe table: seed index + 1, or 0 (empty)
+//   shash  u64[RCHIP_M]      each seed's hash
+//   sinfo  u32[RCHIP_M]      occs << 1 | strand, ring offset << 16
+//   D      i32[2 RCHIP_M]    difference array over window starts
+//   cntA   u16[RCHIP_M]      occurrences seen per seed
+//   ring   u16[RCHIP_M]      positions of each seed's last occs occurrences
+//   smask  u32[2 RCHIP_M/16] per 32 positions: ballots of same / opposite strand
+constexpr int RCHIP_WARPS = 8;
+constexpr int RCHIP_CHUNK = 8;  // candidates a warp takes at once (<= 32)
+constexpr int RCHIP_T = 512;    // a power of two >= 2 RCHIP_M
+constexpr size_t RCHIP_OFF_HASH = 2 * (size_t)RCHIP_T;
+constexpr size_t RCHIP_OFF_INFO = RCHIP_OFF_HASH + 8 * (size_t)RCHIP_M;
+constexpr size_t RCHIP_OFF_D = RCHIP_OFF_INFO + 4 * (size_t)RCHIP_M;
+constexpr size_t RCHIP_OFF_CNT = RCHIP_OFF_D + 4 * 2 * (size_t)RCHIP_M;
+constexpr size_t RCHIP_OFF_RING = RCHIP_OFF_CNT + 2 * (size_t)RCHIP_M;
+constexpr size_t RCHIP_OFF_MASK = RCHIP_OFF_RING + 2 * (size_t)RCHIP_M;
+constexpr size_t RCHIP_SLICE = (RCHIP_OFF_MASK + 4 * 2 * ((2 * (size_t)RCHIP_M + 31) / 32) + 15) / 16 * 16;
+static_assert(RCHIP_T >= 2 * RCHIP_M && (RCHIP_T & (RCHIP_T - 1)) == 0, "probe table size");
+static_assert(RCHIP_OFF_HASH % 8 == 0 && RCHIP_OFF_D % 4 == 0 && RCHIP_OFF_MASK % 4 == 0, "slice alignment");
+static_assert(RCHIP_SLICE <= 7168, "four CTAs of RCHIP_WARPS warps per SM");
+
+// Seed of hash x in the on-chip table, or -1 (the table keeps empty slots).
+__device__ __forceinline__ int32_t chip_lookup(const uint16_t* tslot, const uint64_t* shash, uint32_t T, uint64_t x) {
+    uint32_t sl = (uint32_t)x & (T - 1);
+    for (;;) {
+        const uint32_t t = tslot[sl];
+        if (t == 0) return -1;
+        if (shash[t - 1] == x) return (int32_t)t - 1;
+        sl = (sl + 1) & (T - 1);
+    }
+}
+
+// Inserts seed i (hash hs) into the table: a compare-and-swap on the word
+// that holds the slot.
+__device__ __forceinline__ void chip_insert(uint16_t* tslot, uint32_t T, uint64_t hs, uint32_t i) {
+    uint32_t sl = (uint32_t)hs & (T - 1);
+    for (;;) {
+        uint32_t* w = (uint32_t*)tslot + (sl >> 1);
+        const uint32_t sh = (sl & 1u) * 16u;
+        uint32_t old = *(volatile uint32_t*)w;
+        while (((old >> sh) & 0xffffu) == 0) {
+            const uint32_t got = atomicCAS(w, old, old | ((i + 1u) << sh));
+            if (got == old) return;
+            old = got;  // the other slot of the word changed: look again
+        }
+        sl = (sl + 1) & (T - 1);
+    }
+}
+
+// best_fixed_length (src/shmap/scoring.rs:189-291) for one candidate window,
+// the arithmetic of refine_one with every per-read array on chip; the strand
+// agreement of the winning window is counted from the ballots.
+__device__ __forceinline__ void refine_chip_one(const BatchView& v, BucketJob* J, int32_t m, int32_t n_u, int64_t h,
+                                                uint32_t T, const uint16_t* tslot, const uint64_t* shash,
+                                                const uint32_t* sinfo, uint16_t* cntA, uint16_t* ring, int32_t* D,
+                                                uint32_t* smask, int lane, unsigned lt) {
+    const DevIndex& I = v.I;
+    const int32_t seg = J->seg;
+    const uint32_t G0 = __ldg(I.seg_off + seg), Gend = __ldg(I.seg_off + seg + 1);
+    const int64_t seglen = (int64_t)(Gend - G0);
+    const int64_t from = (int64_t)J->bb * h;
+    const int64_t end = min(((int64_t)J->bb + 2) * h, seglen);
+    const int32_t W = (int32_t)(end - from);  // <= 2 h <= 2 RCHIP_M
+    if (lane == 0 && W > 0) atomicAdd(&v.mx->refine_kmers, (unsigned long long)W);
+    for (int32_t i = lane; i < n_u; i += 32) cntA[i] = 0;
+    for (int32_t i = lane; i < W; i += 32) D[i] = 0;
+    __syncwarp();
+    // the reference k-mers of REFINE_U chunks of 32 positions; the next
+    // chunks' are loaded while these are folded
+    uint64_t hx[REFINE_U];
+    uint32_t rsx[REFINE_U];
+#pragma unroll
+    for (int u = 0; u < REFINE_U; u++) {
+        const int32_t x = 32 * u + lane;
+        const uint32_t gid = G0 + (uint32_t)(from + (x < W ? x : 0));
+        hx[u] = x < W ? __ldg(I.ref_h + gid) : 0;
+        rsx[u] = x < W ? __ldg(I.ref_rs + gid) : 0;
+    }
+    for (int32_t c00 = 0; c00 < W; c00 += 32 * REFINE_U) {
+        uint64_t hy[REFINE_U];
+        uint32_t ry[REFINE_U];
+        int32_t sx[REFINE_U];
+        uint32_t sxi[REFINE_U];
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++) {
+            const int32_t y = c00 + 32 * (REFINE_U + u) + lane;
+            const uint32_t gid = G0 + (uint32_t)(from + (y < W ? y : 0));
+            hy[u] = y < W ? __ldg(I.ref_h + gid) : 0;
+            ry[u] = y < W ? __ldg(I.ref_rs + gid) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++)  // the chunks' lookups together
+            sx[u] = c00 + 32 * u + lane < W ? chip_lookup(tslot, shash, T, hx[u]) : -1;
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++) sxi[u] = sx[u] >= 0 ? sinfo[sx[u]] : 0u;
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++) {
+            const int32_t c0 = c00 + 32 * u;
+            if (c0 >= W) break;  // warp-uniform
+            const int32_t x = c0 + lane;
+            const int32_t s = sx[u];
+            const uint32_t os = sxi[u] & 0xffffu, ooff = sxi[u] >> 16;
+            {
+                const bool same = s >= 0 && ((os ^ rsx[u]) & 1u) == 0;
+                const unsigned bs = __ballot_sync(0xffffffffu, same);
+                const unsigned bo = __ballot_sync(0xffffffffu, s >= 0 && !same);
+                if (lane == 0) {
+                    smask[2 * (c0 >> 5)] = bs;
+                    smask[2 * (c0 >> 5) + 1] = bo;
+                }
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, s);
+            int32_t t = 0, occ = 1, rho = 0, gsz = 0;
+            if (s >= 0) {
+                occ = (int32_t)(os >> 1);
+                rho = __popc(peers & lt);
+                gsz = __popc(peers);
+                t = (int32_t)cntA[s] + rho;
+                int32_t p = -1;  // position of the occ-th previous occurrence, -1 = none
+                if (t >= occ) {
+                    if (rho >= occ)  // in this chunk: the peer occ places before this lane
+                        p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
+                    else
+                        p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
+                }
+                const int32_t st = max(max(p + 1, x - m + 1), 0);
+                if (st <= x) {
+                    atomicAdd(D + st, 1);
+                    if (x + 1 < W) atomicAdd(D + x + 1, -1);  // D[W] is never read
+                }
+            }
+            __syncwarp();
+            if (s >= 0) {
+                if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = (uint16_t)x;
+                if (rho == gsz - 1) cntA[s] = (uint16_t)(t + 1);
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int u = 0; u < REFINE_U; u++) {
+            hx[u] = hy[u];
+            rsx[u] = ry[u];
+        }
+    }
+    __syncwarp();
+    // intersection per window start, score, first maximum (as refine_one)
+    const bool jac = v.P.metric == 1;
+    double best = -1.0;
+    int32_t bl = -1, bI = -1, br = 0;
+    int32_t icarry = 0;
+    for (int32_t c0 = 0; c0 < W; c0 += 32) {
+        const int32_t x = c0 + lane;
+        const int32_t dv = x < W ? D[x] : 0;
+        const int32_t inc = warp_inclusive_scan(dv) + icarry;
+        icarry = __shfl_sync(0xffffffffu, inc, 31);
+        if (x < W) {
+            const int32_t r = min(x + m, W);
+            const int32_t I_ = inc, sk = r - x;
+            bool better;
+            if (jac) {
+                const double score = __ddiv_rn((double)I_, (double)(m + sk - I_));
+                better = score > best;
+                if (better) best = score;
+            } else {
+                better = I_ > bI;
+            }
+            if (better) {
+                bl = x;
+                bI = I_;
+                br = r;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int32_t obl = __shfl_xor_sync(0xffffffffu, bl, o);
+        int32_t obI = __shfl_xor_sync(0xffffffffu, bI, o);
+        int32_t obr = __shfl_xor_sync(0xffffffffu, br, o);
+        const bool take = jac ? (ob > best || (ob == best && obl >= 0 && (bl < 0 || obl < bl)))
+                              : (obI > bI || (obI == bI && obl >= 0 && (bl < 0 || obl < bl)));
+        if (take) {
+            best = ob;
+            bl = obl;
+            bI = obI;
+            br = obr;
+        }
+    }
+    if (!jac && bl >= 0) best = __ddiv_rn((double)bI, (double)m);
+    // every lane holds the winner: the strand agreement over [bl, br) from
+    // the ballots, a lane per 32 positions
+    int32_t same = 0;
+    if (bl >= 0) {
+        const int32_t j = (bl >> 5) + lane, jl = (br - 1) >> 5;
+        if (j <= jl) {
+            uint32_t keep = 0xffffffffu;
+            if (j == (bl >> 5)) keep &= 0xffffffffu << (bl & 31);
+            if (j == jl) keep &= 0xffffffffu >> (31 - ((br - 1) & 31));
+            same = __popc(smask[2 * j] & keep) - __popc(smask[2 * j + 1] & keep);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) same += __shfl_xor_sync(0xffffffffu, same, o);
+    }
+    if (lane == 0) {
+        J->score = best;
+        if (bl >= 0) {
+            const int32_t tl = (int32_t)(__ldg(I.ref_rs + G0 + from + bl) >> 1);
+            const int32_t tr = (int32_t)(__ldg(I.ref_rs + G0 + from + br - 1) >> 1);
+            J->t_l = tl;
+            J->t_r = tr;
+            J->inter = bI;
+            J->same = same;
+            J->s_sz = tr - tl + 1;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(RCHIP_WARPS * 32, 4) k_refine_chip(BatchView v) {
+    extern __shared__ __align__(16) uint8_t rc_smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    uint8_t* base = rc_smem + (size_t)wib * RCHIP_SLICE;
+    uint16_t* tslot = (uint16_t*)base;
+    uint64_t* shash = (uint64_t*)(base + RCHIP_OFF_HASH);
+    uint32_t* sinfo = (uint32_t*)(base + RCHIP_OFF_INFO);
+    int32_t* D = (int32_t*)(base + RCHIP_OFF_D);
+    uint16_t* cntA = (uint16_t*)(base + RCHIP_OFF_CNT);
+    uint16_t* ring = (uint16_t*)(base + RCHIP_OFF_RING);
+    uint32_t* smask = (uint32_t*)(base + RCHIP_OFF_MASK);
+    // work comes in chunks of RCHIP_CHUNK consecutive candidates (a read's
+    // candidates are consecutive) from a batch counter, the next chunk's
+    // number fetched while this one is refined; the seed table is rebuilt
+    // only when the read changes
+    const uint32_t ncand = v.coff[v.n];
+    uint32_t nxt = 0;
+    if (lane == 0) nxt = atomicAdd(&v.mx->refine_next, 1u);
+    int32_t cur = -1;  // the read whose table is staged
+    uint32_t T = 32;
+    for (;;) {
+        const uint32_t ci0 = __shfl_sync(0xffffffffu, nxt, 0) * (uint32_t)RCHIP_CHUNK;
+        if (ci0 >= ncand) break;
+        if (lane == 0) nxt = atomicAdd(&v.mx->refine_next, 1u);
+        int32_t ql = -1;
+        bool onl = false;
+        if (lane < RCHIP_CHUNK && ci0 + lane < ncand) {
+            ql = v.jobs[v.cidx[ci0 + lane]].read;
+            onl = refine_on_chip(v.P, (uint32_t)v.r_m[ql], v.r_half[ql]);
+        }
+        const uint32_t nc = min((uint32_t)RCHIP_CHUNK, ncand - ci0);
+        for (uint32_t j = 0; j < nc; j++) {
+            const int32_t q = __shfl_sync(0xffffffffu, ql, (int)j);
+            if (!__shfl_sync(0xffffffffu, onl, (int)j)) continue;  // k_refine's
+            const int32_t m = v.r_m[q], n_u = v.r_nu[q];  // n_u <= m <= RCHIP_M
+            if (q != cur) {
+                const uint64_t kb = v.kcap_off[q];
+                T = max(32u, (uint32_t)pow2_ceil(2ULL * (uint64_t)n_u));  // <= RCHIP_T
+                for (uint32_t i = lane; i < T / 2; i += 32) ((uint32_t*)tslot)[i] = 0u;
+#pragma unroll 4
+                for (int32_t i = lane; i < n_u; i += 32) {
+                    const SeedRec sr = v.sd[kb + i];
+                    shash[i] = v.sd_h[kb + i];
+                    sinfo[i] = sr.os | (sr.ooff << 16);
+                }
+                __syncwarp();
+                for (int32_t i = lane; i < n_u; i += 32) chip_insert(tslot, T, shash[i], (uint32_t)i);
+                __syncwarp();
+                cur = q;
+            }
+            refine_chip_one(v, v.jobs + v.cidx[ci0 + j], m, n_u, (int64_t)v.r_half[q], T, tslot, shash, sinfo, cntA,
+                            ring, D, smask, lane, lt);
+            __syncwarp();
+        }
     }
 }
 
@@ -1749,8 +2064,9 @@ struct MapScratch {
     DevBuf<int32_t> retry_idx;
     DevBuf<uint64_t> km_h, pht_key, hw, hw_off, bt_size, bt_off;
     DevBuf<SeedRec> sd;
+    DevBuf<uint64_t> sd_h;
     DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
-        cidx, sort_scr, ovf_list, r_flags;
+        cidx, cfar, sort_scr, ovf_list, r_flags;
     DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
     DevBuf<BSlot> bt;
@@ -2004,6 +2320,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     S.km_h.reserve(kcap + 1);
     S.km_rs.reserve(kcap + 1);
     S.sd.reserve(kcap + 1);
+    S.sd_h.reserve(kcap + 1);
     S.sd_hpre.reserve(kcap + 1);
     S.pht_key.reserve(phtn);
     S.pht_val.reserve(phtn);
@@ -2061,6 +2378,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     v.km_h = S.km_h.p;
     v.km_rs = S.km_rs.p;
     v.sd = S.sd.p;
+    v.sd_h = S.sd_h.p;
     v.sd_hpre = S.sd_hpre.p;
     v.pht_off = dp.pht_off;
     v.pht_key = S.pht_key.p;
@@ -2263,9 +2581,11 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     exclusive_scan_u32(S.ccnt.p, S.coff.p, (size_t)n, s);
     H.mark("scan");
     S.cidx.reserve((size_t)job_cap + 1);
+    S.cfar.reserve((size_t)job_cap + 1);
     S.sweep_scr.reserve(2 * (size_t)job_cap + 2);
     H.mark("cidx_res");
     v.cidx = S.cidx.p;
+    v.cfar = S.cfar.p;
     T.begin(STG_AUX);
     k_cidx<<<wide, 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
@@ -2282,6 +2602,13 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     H.mark("ref_res");
     rsc.base = S.ref_scr.p;
     T.begin(STG_REFINE);
+    if (!c->rchip_smem_set) {
+        SHM_CUDA(cudaFuncSetAttribute(k_refine_chip, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(RCHIP_WARPS * RCHIP_SLICE)));
+        c->rchip_smem_set = 1;
+    }
+    k_refine_chip<<<grid_for((size_t)n * 32, RCHIP_WARPS * 32, 4), RCHIP_WARPS * 32, RCHIP_WARPS * RCHIP_SLICE, s>>>(v);
+    SHM_CUDA(cudaGetLastError());
     k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, 0, s>>>(v, rsc);
     SHM_CUDA(cudaGetLastError());
     T.end();

@@ -61,6 +61,7 @@ struct MapCtx {
     // work counters (always on): see WORK_NAMES
     int64_t work[16] = {};
     int seed_smem_set = 0;   // dynamic shared memory the seed kernels have been allowed so far
+    int rchip_smem_set = 0;  // k_refine_chip's dynamic shared memory allowed
     int seedc_smem_set = 0;
     // stage timing
     bool timing = false;
