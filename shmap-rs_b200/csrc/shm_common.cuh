@@ -58,6 +58,14 @@ struct DevIndex {
     const uint32_t* dir;      // (1 << dir_bits) + 1: first key of each hash range
     int32_t dir_bits;
     uint64_t dir_mul;         // range of h: __umul64hi(h, dir_mul), monotone, < 2^dir_bits for h <= thr
+    // Bucket table (null when thr is all ones): 1 << btab_bits buckets of two
+    // uint4, bucket __umul64hi(h, btab_mul) holding the first two keys of its
+    // hash range in key order, {key0, key1} then {a0, cnt0, a1, cnt1 | more << 31};
+    // an empty slot has key ~0 (no hash <= thr) and count 0, and `more` says
+    // the range has further keys (all above key1), found through dir.
+    const uint4* btab;
+    int32_t btab_bits;
+    uint64_t btab_mul;
     uint32_t n_keys, n_kmers, n_hits;
 };
 
@@ -112,11 +120,8 @@ __device__ __forceinline__ int32_t seg_of_in(const uint32_t* seg_off, int32_t n_
     return lo;
 }
 
-// SketchIndex::count + hit-list lookup (src/index.rs:192-213).
-__device__ __forceinline__ bool idx_lookup(const DevIndex& I, uint64_t h, uint32_t& a, uint32_t& cnt) {
-    cnt = 0;
-    a = 0;
-    if (h > I.thr || I.n_keys == 0) return false;
+// The hash-range search of idx_lookup, through the directory and the keys.
+__device__ __forceinline__ bool idx_lookup_dir(const DevIndex& I, uint64_t h, uint32_t& a, uint32_t& cnt) {
     uint32_t b = (uint32_t)__umul64hi(h, I.dir_mul);
     uint32_t lo = __ldg(I.dir + b), hi = __ldg(I.dir + b + 1);
     while (hi - lo > 8) {
@@ -134,6 +139,48 @@ __device__ __forceinline__ bool idx_lookup(const DevIndex& I, uint64_t h, uint32
         if (kk > h) break;
     }
     return false;
+}
+
+// The bucket of h in the bucket table (I.btab non-null, h <= thr).
+__device__ __forceinline__ const uint4* btab_bucket(const DevIndex& I, uint64_t h) {
+    return I.btab + 2 * (size_t)__umul64hi(h, I.btab_mul);
+}
+
+// Looks h up among a bucket's two keys k = {key0, key1}: returns the slot
+// (0 or 1) holding h, 2 when h may be among the range's further keys (key1
+// is present and below h: the slot's `more` flag decides), -1 when absent.
+__device__ __forceinline__ int btab_slot(uint4 k, uint64_t h) {
+    const uint64_t k0 = ((uint64_t)k.y << 32) | k.x, k1 = ((uint64_t)k.w << 32) | k.z;
+    if (k0 == h) return 0;
+    if (k1 == h) return 1;
+    return (k1 != ~0ULL && h > k1) ? 2 : -1;
+}
+
+// SketchIndex::count + hit-list lookup (src/index.rs:192-213): the bucket
+// table first (one 32-byte sector), the directory for the rest of a crowded
+// range.
+__device__ __forceinline__ bool idx_lookup(const DevIndex& I, uint64_t h, uint32_t& a, uint32_t& cnt) {
+    cnt = 0;
+    a = 0;
+    if (h > I.thr || I.n_keys == 0) return false;
+    if (I.btab) {
+        const uint4* p = btab_bucket(I, h);
+        const int sl = btab_slot(__ldg(p), h);
+        if (sl < 0) return false;
+        const uint4 ac = __ldg(p + 1);
+        if (sl == 0) {
+            a = ac.x;
+            cnt = ac.y;
+            return true;
+        }
+        if (sl == 1) {
+            a = ac.z;
+            cnt = ac.w & 0x7fffffffu;
+            return true;
+        }
+        if (!(ac.w >> 31)) return false;
+    }
+    return idx_lookup_dir(I, h, a, cnt);
 }
 
 // First index in hits[a, a+n) with hits[i] >= v.

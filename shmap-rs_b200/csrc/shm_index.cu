@@ -139,6 +139,41 @@ __global__ void k_dir_fill(const uint64_t* __restrict__ keys, uint32_t n_keys, u
     }
 }
 
+// The bucket table (DevIndex::btab) over the sorted keys: every key finds its
+// rank in its bucket from its two predecessors (the keys are sorted and the
+// bucket map is monotone), so each slot has one writer.
+__global__ void k_btab_clear(uint4* __restrict__ bt, int64_t nb) {
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (int64_t)gridDim.x * blockDim.x) {
+        bt[2 * b] = make_uint4(~0u, ~0u, ~0u, ~0u);
+        bt[2 * b + 1] = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+__global__ void k_btab_fill(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ key_off, uint32_t n_keys,
+                            uint4* __restrict__ bt, uint64_t mul) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)n_keys;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t h = keys[i];
+        const uint64_t b = __umul64hi(h, mul);
+        const bool p1 = i > 0 && __umul64hi(keys[i - 1], mul) == b;
+        if (p1 && i > 1 && __umul64hi(keys[i - 2], mul) == b) continue;  // third or later: through dir
+        const uint32_t a = key_off[i], c = key_off[i + 1] - a;
+        uint32_t* q0 = (uint32_t*)(bt + 2 * b);
+        uint32_t* q1 = (uint32_t*)(bt + 2 * b + 1);
+        if (!p1) {
+            q0[0] = (uint32_t)h;
+            q0[1] = (uint32_t)(h >> 32);
+            q1[0] = a;
+            q1[1] = c;
+        } else {
+            const bool more = i + 1 < (int64_t)n_keys && __umul64hi(keys[i + 1], mul) == b;
+            q0[2] = (uint32_t)h;
+            q0[3] = (uint32_t)(h >> 32);
+            q1[2] = a;
+            q1[3] = c | (more ? 0x80000000u : 0u);
+        }
+    }
+}
+
 IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_t n_seg,
                           const std::vector<std::string>& names, int32_t k, double h_frac, int32_t max_matches,
                           cudaStream_t s) {
@@ -297,6 +332,22 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
         k_dir_fill<<<grid_for((size_t)std::max<int64_t>(nb, (int64_t)n_kept), 256), 256, 0, s>>>(ix->keys.p, n_kept,
                                                                                                ix->dir.p, nb, mul);
         SHM_CUDA(cudaGetLastError());
+        // the bucket table: two buckets per key (at most 2^28), when no hash is
+        // all ones (thr below the maximum) and every count fits in 31 bits
+        int tbits = 0;
+        uint64_t tmul = 0;
+        if (thr != UINT64_MAX && n_kept > 0 && hst.highest < (1LL << 31)) {
+            tbits = std::min(bits + 1, 28);
+            const int64_t nt = (int64_t)1 << tbits;
+            unsigned __int128 t128 = ((unsigned __int128)nt << 64) / ((unsigned __int128)thr + 1);
+            tmul = t128 > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)t128;
+            ix->btab.reserve(2 * (size_t)nt);
+            k_btab_clear<<<grid_for((size_t)nt, 256), 256, 0, s>>>(ix->btab.p, nt);
+            SHM_CUDA(cudaGetLastError());
+            k_btab_fill<<<grid_for((size_t)n_kept, 256), 256, 0, s>>>(ix->keys.p, ix->key_off.p, n_kept, ix->btab.p,
+                                                                     tmul);
+            SHM_CUDA(cudaGetLastError());
+        }
         SHM_CUDA(cudaStreamSynchronize(s));
 
         DevIndex& d = ix->dev;
@@ -314,6 +365,9 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
         d.dir = ix->dir.p;
         d.dir_bits = bits;
         d.dir_mul = mul;
+        d.btab = tbits ? ix->btab.p : nullptr;
+        d.btab_bits = tbits;
+        d.btab_mul = tmul;
         d.n_keys = n_kept;
         d.n_kmers = n_kmers;
         d.n_hits = n_hits;

@@ -55,6 +55,7 @@ struct IndexStorage {
     DevBuf<uint32_t> seg_off, key_off, hits, hit_fw, dir, ref_rs;
     DevBuf<int32_t> seg_sz;
     DevBuf<uint64_t> ref_h, keys;
+    DevBuf<uint4> btab;
     std::vector<std::string> names;
     std::vector<int32_t> seg_len;        // bases
     std::vector<uint32_t> h_seg_off;     // k-mer offsets (n_seg+1)

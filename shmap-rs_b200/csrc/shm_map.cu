@@ -466,62 +466,42 @@ __global__ void k_seed_bins(BatchView v, int32_t* __restrict__ lists, uint32_t* 
 }
 
 // count() probes for U hashes of one lane at once (index.rs:204-213): the
-// directory, key and hit-list loads of the U probes are issued together, so
-// a lane waits for three rounds of loads instead of 3U.
+// bucket-table sectors of the U probes are loaded together (one round; the
+// hit-list start and count of a found key come from the same sector), and
+// the few probes that land in a crowded range finish through the directory.
 template <int U>
 __device__ __forceinline__ void idx_lookup_u(const DevIndex& I, const uint64_t (&h)[U], const bool (&on)[U],
                                              uint32_t (&a)[U], uint32_t (&cnt)[U]) {
-    uint32_t lo[U], hi[U], at[U];
+    if (!I.btab) {
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            a[u] = cnt[u] = 0;
+            if (on[u]) idx_lookup(I, h[u], a[u], cnt[u]);
+        }
+        return;
+    }
+    uint4 k[U];
+    bool live[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
         a[u] = 0;
         cnt[u] = 0;
-        lo[u] = hi[u] = 0;
-        at[u] = 0xffffffffu;
-        if (on[u] && h[u] <= I.thr && I.n_keys != 0) {
-            const uint32_t b = (uint32_t)__umul64hi(h[u], I.dir_mul);
-            lo[u] = __ldg(I.dir + b);
-            hi[u] = __ldg(I.dir + b + 1);
-        }
+        live[u] = on[u] && h[u] <= I.thr && I.n_keys != 0;
+        k[u] = live[u] ? __ldg(btab_bucket(I, h[u])) : make_uint4(~0u, ~0u, ~0u, ~0u);
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
-        while (hi[u] - lo[u] > 8) {  // a crowded directory range (rare)
-            const uint32_t mid = (lo[u] + hi[u]) >> 1;
-            if (__ldg(I.keys + mid) <= h[u]) lo[u] = mid;
-            else hi[u] = mid;
-        }
-    }
-    uint64_t k0[U], k1[U];
-#pragma unroll
-    for (int u = 0; u < U; u++) {  // the first two keys of every range at once
-        k0[u] = lo[u] < hi[u] ? __ldg(I.keys + lo[u]) : 0;
-        k1[u] = lo[u] + 1 < hi[u] ? __ldg(I.keys + lo[u] + 1) : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-        if (lo[u] < hi[u] && k0[u] == h[u]) {
-            at[u] = lo[u];
-        } else if (lo[u] + 1 < hi[u] && k0[u] < h[u]) {
-            if (k1[u] == h[u]) {
-                at[u] = lo[u] + 1;
-            } else if (k1[u] < h[u]) {
-                for (uint32_t i = lo[u] + 2; i < hi[u]; i++) {
-                    const uint64_t kk = __ldg(I.keys + i);
-                    if (kk == h[u]) {
-                        at[u] = i;
-                        break;
-                    }
-                    if (kk > h[u]) break;
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-        if (at[u] != 0xffffffffu) {
-            a[u] = __ldg(I.key_off + at[u]);
-            cnt[u] = __ldg(I.key_off + at[u] + 1) - a[u];
+        const int sl = live[u] ? btab_slot(k[u], h[u]) : -1;
+        if (sl < 0) continue;
+        const uint4 ac = __ldg(btab_bucket(I, h[u]) + 1);  // the same sector
+        if (sl == 0) {
+            a[u] = ac.x;
+            cnt[u] = ac.y;
+        } else if (sl == 1) {
+            a[u] = ac.z;
+            cnt[u] = ac.w & 0x7fffffffu;
+        } else if (ac.w >> 31) {
+            idx_lookup_dir(I, h[u], a[u], cnt[u]);
         }
     }
 }
