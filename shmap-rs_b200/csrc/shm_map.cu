@@ -888,6 +888,25 @@ __device__ __forceinline__ void seed_range(const DevIndex& I, uint32_t a, uint32
     if (B < A) B = A;
 }
 
+// First index in [lo, end) whose hit is >= v, or end, when every hit before lo
+// is below v: probes lo, lo+1, lo+3, lo+7, ... then a binary search in the
+// last gap, so a range of c hits costs about 2 log2(c) + 1 loads (one when
+// the next hit is already past v).
+__device__ __forceinline__ uint32_t hits_gallop(const uint32_t* __restrict__ hits, uint32_t lo, uint32_t end,
+                                                uint32_t v) {
+    uint32_t step = 1;
+    while (lo < end) {
+        const uint32_t pr = min(lo + step, end) - 1;
+        if (__ldg(hits + pr) >= v) {
+            end = pr;
+            break;
+        }
+        lo = pr + 1;
+        step <<= 1;
+    }
+    return hits_lower_bound(hits, lo, end - lo, v);
+}
+
 struct Agg {
     int32_t count, codir, rmin, rmax;
 };
@@ -1032,8 +1051,33 @@ __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
                     const int32_t cd = ((rs & 1u) == sstr) ? 1 : -1, r = (int32_t)(rs >> 1);
                     bt_add(v, q, seg, b_t, 1, cd, r, r);  // add_to_pos (buckets.rs:642-662)
                     if (b_t > 0) bt_add(v, q, seg, (int64_t)b_t - 1, 1, cd, r, r);
+                } else if (!ap) {
+                    // streamed multi-hit seed: one clamped contribution per bucket
+                    // (seeding.rs:113-205). Both of this hit's ranges, buckets b_t
+                    // and b_t - 1 (the latter unless the previous hit is in it),
+                    // start at this hit: the previous hit lies in a lower bucket
+                    // (below b_t - 1 when b_t - 1 is added) or an earlier segment.
+                    // Their ends are found by galloping forward.
+                    const uint32_t A = a + t, E = a + cnt;
+                    const uint64_t up1 = (uint64_t)s_lo + (uint64_t)(b_t + 1) * h, up0 = up1 + h;
+                    const uint32_t B1 = hits_gallop(I.hits, A + 1, E, (uint32_t)min(up1, (uint64_t)s_hi));
+                    const uint32_t B0 = hits_gallop(I.hits, B1, E, (uint32_t)min(up0, (uint64_t)s_hi));
+                    const int32_t r0 = (int32_t)(__ldg(I.ref_rs + g_t) >> 1);
+                    const uint32_t fwA = __ldg(I.hit_fw + A);
+                    {
+                        const int32_t c = (int32_t)(B0 - A), fw = (int32_t)(__ldg(I.hit_fw + B0) - fwA);
+                        const int32_t same = sstr ? c - fw : fw;
+                        const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B0 - 1)) >> 1);
+                        bt_add(v, q, seg, b_t, min(c, (int32_t)occs), 2 * same - c, r0, r1);
+                    }
+                    if (b_t > 0 && !prev_is_bm1) {
+                        const int32_t c = (int32_t)(B1 - A), fw = (int32_t)(__ldg(I.hit_fw + B1) - fwA);
+                        const int32_t same = sstr ? c - fw : fw;
+                        const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B1 - 1)) >> 1);
+                        bt_add(v, q, seg, (int64_t)b_t - 1, min(c, (int32_t)occs), 2 * same - c, r0, r1);
+                    }
                 } else {
-                    // streamed multi-hit seed: one clamped contribution per bucket (seeding.rs:113-205)
+                    // streamed multi-hit seed, absolute positions: the ranges by search
                     for (int e = 0; e < 2; e++) {
                         const int64_t bb = (int64_t)b_t - e;
                         if (bb < 0) break;
