@@ -911,11 +911,15 @@ struct Agg {
     int32_t count, codir, rmin, rmax;
 };
 
-__device__ __forceinline__ Agg range_agg(const DevIndex& I, uint32_t A, uint32_t B, uint32_t seed_strand) {
+// The hits [A, B) of a seed: their count and, when `full`, their
+// codirection and position range (only bucket_SH reports those: every other
+// metric leaves them unread).
+__device__ __forceinline__ Agg range_agg(const DevIndex& I, uint32_t A, uint32_t B, uint32_t seed_strand,
+                                         bool full = true) {
     Agg r;
     r.count = (int32_t)(B - A);
-    if (r.count <= 0) {
-        r.count = 0;
+    if (r.count <= 0 || !full) {
+        r.count = max(r.count, 0);
         r.codir = 0;
         r.rmin = INT32_MAX;
         r.rmax = -1;
@@ -966,8 +970,10 @@ __device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t se
         i = (i + 1) & mask;
     }
     atomicAdd(&s->mc, bt_pack(matches, codir));
-    atomicMin(&s->rmin, rmin);
-    atomicMax(&s->rmax, rmax);
+    if (v.P.metric == 2) {  // the position range is read by bucket_SH only
+        atomicMin(&s->rmin, rmin);
+        atomicMax(&s->rmax, rmax);
+    }
 }
 
 __device__ __forceinline__ uint32_t ub_u64(const uint64_t* a, uint32_t n, uint64_t x) {  // first index with a[i] > x
@@ -1015,6 +1021,7 @@ __device__ __forceinline__ int32_t seg_step(const DevIndex& I, uint32_t g, int32
 __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
     const uint64_t total = v.hw_off[v.n];
     const bool ap = v.P.ap != 0;
+    const bool sh_out = v.P.metric == 2;  // codirection and positions are reported (bucket_SH)
     const DevIndex& I = v.I;
     const uint64_t nrun = (total + CONTRIB_RUN - 1) / CONTRIB_RUN;
     for (uint64_t rn = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; rn < nrun;
@@ -1047,7 +1054,7 @@ __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
             const bool prev_is_bm1 = seg_p == seg && b_p + 1 == b_t;
             if (first) {
                 if (cnt == 1) {
-                    const uint32_t rs = __ldg(I.ref_rs + g_t);
+                    const uint32_t rs = sh_out ? __ldg(I.ref_rs + g_t) : 0u;
                     const int32_t cd = ((rs & 1u) == sstr) ? 1 : -1, r = (int32_t)(rs >> 1);
                     bt_add(v, q, seg, b_t, 1, cd, r, r);  // add_to_pos (buckets.rs:642-662)
                     if (b_t > 0) bt_add(v, q, seg, (int64_t)b_t - 1, 1, cd, r, r);
@@ -1062,19 +1069,25 @@ __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
                     const uint64_t up1 = (uint64_t)s_lo + (uint64_t)(b_t + 1) * h, up0 = up1 + h;
                     const uint32_t B1 = hits_gallop(I.hits, A + 1, E, (uint32_t)min(up1, (uint64_t)s_hi));
                     const uint32_t B0 = hits_gallop(I.hits, B1, E, (uint32_t)min(up0, (uint64_t)s_hi));
-                    const int32_t r0 = (int32_t)(__ldg(I.ref_rs + g_t) >> 1);
-                    const uint32_t fwA = __ldg(I.hit_fw + A);
-                    {
-                        const int32_t c = (int32_t)(B0 - A), fw = (int32_t)(__ldg(I.hit_fw + B0) - fwA);
-                        const int32_t same = sstr ? c - fw : fw;
-                        const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B0 - 1)) >> 1);
-                        bt_add(v, q, seg, b_t, min(c, (int32_t)occs), 2 * same - c, r0, r1);
-                    }
-                    if (b_t > 0 && !prev_is_bm1) {
-                        const int32_t c = (int32_t)(B1 - A), fw = (int32_t)(__ldg(I.hit_fw + B1) - fwA);
-                        const int32_t same = sstr ? c - fw : fw;
-                        const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B1 - 1)) >> 1);
-                        bt_add(v, q, seg, (int64_t)b_t - 1, min(c, (int32_t)occs), 2 * same - c, r0, r1);
+                    if (!sh_out) {  // matches only
+                        bt_add(v, q, seg, b_t, min((int32_t)(B0 - A), (int32_t)occs), 0, 0, 0);
+                        if (b_t > 0 && !prev_is_bm1)
+                            bt_add(v, q, seg, (int64_t)b_t - 1, min((int32_t)(B1 - A), (int32_t)occs), 0, 0, 0);
+                    } else {
+                        const int32_t r0 = (int32_t)(__ldg(I.ref_rs + g_t) >> 1);
+                        const uint32_t fwA = __ldg(I.hit_fw + A);
+                        {
+                            const int32_t c = (int32_t)(B0 - A), fw = (int32_t)(__ldg(I.hit_fw + B0) - fwA);
+                            const int32_t same = sstr ? c - fw : fw;
+                            const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B0 - 1)) >> 1);
+                            bt_add(v, q, seg, b_t, min(c, (int32_t)occs), 2 * same - c, r0, r1);
+                        }
+                        if (b_t > 0 && !prev_is_bm1) {
+                            const int32_t c = (int32_t)(B1 - A), fw = (int32_t)(__ldg(I.hit_fw + B1) - fwA);
+                            const int32_t same = sstr ? c - fw : fw;
+                            const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B1 - 1)) >> 1);
+                            bt_add(v, q, seg, (int64_t)b_t - 1, min(c, (int32_t)occs), 2 * same - c, r0, r1);
+                        }
                     }
                 } else {
                     // streamed multi-hit seed, absolute positions: the ranges by search
@@ -1084,7 +1097,7 @@ __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
                         if (e == 1 && prev_is_bm1) break;
                         uint32_t A, B;
                         seed_range(I, a, cnt, seg, bb * (int64_t)h, (bb + 2) * (int64_t)h, ap, A, B);
-                        Agg g = range_agg(I, A, B, sstr);
+                        Agg g = range_agg(I, A, B, sstr, sh_out);
                         bt_add(v, q, seg, bb, min(g.count, (int32_t)occs), g.codir, g.rmin, g.rmax);
                     }
                 }
@@ -1203,7 +1216,7 @@ __global__ void __launch_bounds__(256) k_extend(BatchView v) {
                 if (cnt > 0) {
                     uint32_t A, B;
                     seed_range(v.I, sr.a, cnt, seg, (int64_t)bb * h, ((int64_t)bb + 2) * h, ap, A, B);
-                    Agg g = range_agg(v.I, A, B, os & 1u);
+                    Agg g = range_agg(v.I, A, B, os & 1u, v.P.metric == 2);
                     dm = min(g.count, ds);
                     dc = g.codir;
                     rmn = g.rmin;
