@@ -378,6 +378,12 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
     }
     uint32_t po = block_scan_excl<uint32_t>(so, sw32, &t32);
     uint64_t pc = block_scan_excl<uint64_t>(sc, sw64, &t64);
+    const bool pht = v.P.metric != 2;  // bucket_SH refines nothing (these reads are never on chip)
+    if (pht) {  // the read's probe table starts empty
+        const uint64_t pb = v.pht_off[q], pe = v.pht_off[q + 1];
+        for (uint64_t i = pb + tid; i < pe; i += nt) v.pht_val[i] = 0xffffffffu;
+        __syncthreads();
+    }
     uint32_t l_np = 0, l_s0 = 0, l_max = 0;
     uint64_t l_sm = 0, l_eb = 0;
     for (uint32_t i = j0; i < j1; i++) {
@@ -393,7 +399,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
             l_max = max(l_max, cnt);
             l_eb += seed_bucket_bound(v, S_.GD[g], cnt, halflen);
         }
-        pht_insert(v, q, S_.GA[g], i);
+        if (pht) pht_insert(v, q, S_.GA[g], i);
         po += occs;
         pc += cnt;
     }
@@ -753,6 +759,11 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
     // (seeding.rs:101); the processed seeds are a prefix of the order
     const bool chip = refine_on_chip(v.P, m, halflen);
     const bool pht = !chip && v.P.metric != 2;  // bucket_SH refines nothing
+    if (pht) {  // the read's probe table starts empty (written before the inserts below)
+        const uint64_t pb = v.pht_off[q], pe = v.pht_off[q + 1];
+        for (uint64_t i = pb + lane; i < pe; i += 32) v.pht_val[i] = 0xffffffffu;
+        __syncwarp();
+    }
     uint32_t po_carry = 0, l_np = 0, l_s0 = 0, l_max = 0;
     uint64_t pc_carry = 0, l_sm = 0, l_eb = 0;
     for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
@@ -2164,13 +2175,16 @@ static uint64_t pow2_host(uint64_t x) {  // smallest power of two >= x (1 for x 
 }
 
 // k-mer capacity of a read of nw windows: the reference's own estimate
-// mean + 6 sigma + 16 (src/sketch.rs:143-146); reads that beat it are retried
-// with the count the first pass found.
+// mean + 6 sigma + 16 (src/sketch.rs:143-146), raised to twice the mean + 16.
+// The binomial estimate holds for unique sequence, but a read from a tandem
+// array selects each of its few k-mers once per copy: on human-like
+// references about 0.2% of long reads reach 1.5-2x the mean. Reads that beat
+// the capacity are retried with the count the first pass found.
 static uint64_t kmer_cap(int64_t nw, double h_frac) {
     if (nw <= 0) return 0;
     if (h_frac >= 1.0) return (uint64_t)nw;
     double mean = std::max(0.0, (double)nw * h_frac);
-    uint64_t c = (uint64_t)(mean + 6.0 * std::sqrt(mean)) + 16;
+    uint64_t c = std::max((uint64_t)(mean + 6.0 * std::sqrt(mean)), (uint64_t)(2.0 * mean)) + 16;
     return std::min<uint64_t>(c, (uint64_t)nw);
 }
 
@@ -2376,7 +2390,6 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     S.n_jobs.reserve(1);
     S.mx.reserve(1);
     SHM_CUDA(cudaMemsetAsync(S.kcnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
-    SHM_CUDA(cudaMemsetAsync(S.pht_val.p, 0xff, sizeof(uint32_t) * phtn, s));
     SHM_CUDA(cudaMemsetAsync(S.r_seeded.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.r_flags.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.ccnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
@@ -2681,6 +2694,9 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
 // smaller ones so that copying batch b+1 overlaps mapping batch b.
 static const int64_t DEV_BATCH_BASES = (int64_t)1 << 31;
 static const int32_t DEV_BATCH_READS = 1 << 17;
+// The first batch of a device-resident call is small, so the device starts
+// while the host plans the next batch (planning costs ~5 ns a read).
+static const int32_t DEV_FIRST_BATCH_READS = 1 << 14;
 static const int64_t HOST_BATCH_BASES = (int64_t)1 << 29;
 static const int32_t HOST_BATCH_READS = 1 << 15;
 
@@ -2793,13 +2809,15 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
 // Batches of at most max_reads reads and max_bases bases (one read at a time
 // in the plain form).
 static std::vector<std::pair<int32_t, int32_t>> cut_batches(const int64_t* offs, int32_t n, bool plain,
-                                                            int32_t max_reads, int64_t max_bases) {
+                                                            int32_t max_reads, int64_t max_bases,
+                                                            int32_t first_max_reads = 0) {
     std::vector<std::pair<int32_t, int32_t>> b;
     int32_t i = 0;
     while (i < n) {
         int32_t j = i + 1;
+        const int32_t lim = (i == 0 && first_max_reads > 0) ? first_max_reads : max_reads;
         if (!plain)
-            while (j < n && j - i < max_reads && offs[j + 1] - offs[i] <= max_bases) j++;
+            while (j < n && j - i < lim && offs[j + 1] - offs[i] <= max_bases) j++;
         b.emplace_back(i, j);
         i = j;
     }
@@ -2823,7 +2841,7 @@ static std::vector<uint8_t*> plan_blocks(MapCtx* c, const std::vector<std::pair<
 void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
                 int32_t n, shm_map_record* d_out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
-    const auto batches = cut_batches(h_offs, n, plain, DEV_BATCH_READS, DEV_BATCH_BASES);
+    const auto batches = cut_batches(h_offs, n, plain, DEV_BATCH_READS, DEV_BATCH_BASES, DEV_FIRST_BATCH_READS);
     std::vector<BatchSlot> slots = batch_slots(c, batches, h_offs);
     const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
