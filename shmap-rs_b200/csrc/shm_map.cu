@@ -586,10 +586,18 @@ __device__ __forceinline__ uint64_t seed_bucket_bound_u(const BatchView& v, cons
 //                      then occs << 1 | strand of the smallest r)
 //   Rc (4C): bucket offsets, then each group's count() hit count
 //   Ra (4C): each group's hit-list start
-//   P0, P1 (4C each): radix permutations; RH (256 words): digit offsets
-__host__ __device__ constexpr size_t seedc_bytes(uint32_t C) { return 28 * (size_t)C + 1024; }
+//   P0, P1 (2C each): radix permutations (16-bit group indices)
+//   RH (128 words): digit offsets of the 7-bit radix digits
+// followed, once per CTA, by seg_off when the reference has at most
+// SEEDC_SEGS segments (seedc_seg_bytes).
+constexpr int SEEDC_DIGIT = 7;
+__host__ __device__ constexpr size_t seedc_bytes(uint32_t C) { return 24 * (size_t)C + 4 * (1u << SEEDC_DIGIT); }
 constexpr int SEEDC_U = 4;       // groups a lane probes at once
 constexpr int SEEDC_SEGS = 1024;  // references with at most this many segments keep seg_off in shared memory
+static_assert(1024 <= 65536, "group indices of the largest bin fit 16 bits");
+inline size_t seedc_seg_bytes(int32_t n_seg) {
+    return n_seg <= SEEDC_SEGS ? (4 * (size_t)(n_seg + 1) + 15) / 16 * 16 : 0;
+}
 
 // Exclusive scan, in place, of the n (a multiple of 32) words X[0..n): lane l
 // owns n/32 consecutive words.
@@ -616,9 +624,9 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
     uint32_t* Srs = (uint32_t*)(Sh + C);
     uint32_t* Rc = Srs + C;
     uint32_t* Ra = Rc + C;
-    uint32_t* P0 = Ra + C;
-    uint32_t* P1 = P0 + C;
-    uint32_t* RH = P1 + C;
+    uint16_t* P0 = (uint16_t*)(Ra + C);
+    uint16_t* P1 = P0 + C;
+    uint32_t* RH = (uint32_t*)(P1 + C);
 
     // counting sort by bucket: Ht = power of two in [32, C], >= m
     const uint32_t Ht = max((uint32_t)32, (uint32_t)pow2_ceil(m));
@@ -724,29 +732,30 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
     __syncwarp();
 
     // rarest first, stable over hash order (seeding.rs:71): LSD radix on the
-    // count, 8 bits a pass, as many passes as the largest count needs
-    const uint32_t* ord = nullptr;  // null: identity
-    uint32_t* pout = P0;
-    for (int sh = 0; sh < 32 && (maxc >> sh) != 0; sh += 8) {
-        for (uint32_t i = lane; i < 256; i += 32) RH[i] = 0;
+    // count, SEEDC_DIGIT bits a pass, as many passes as the largest count needs
+    constexpr uint32_t ND = 1u << SEEDC_DIGIT;
+    const uint16_t* ord = nullptr;  // null: identity
+    uint16_t* pout = P0;
+    for (int sh = 0; sh < 32 && (maxc >> sh) != 0; sh += SEEDC_DIGIT) {
+        for (uint32_t i = lane; i < ND; i += 32) RH[i] = 0;
         __syncwarp();
         for (uint32_t i = lane; i < n_u; i += 32) {
             const uint32_t g = ord ? ord[i] : i;
-            atomicAdd(&RH[(Rc[g] >> sh) & 255u], 1u);
+            atomicAdd(&RH[(Rc[g] >> sh) & (ND - 1)], 1u);
         }
         __syncwarp();
-        warp_scan_words(RH, 256, lane);
+        warp_scan_words(RH, ND, lane);
         __syncwarp();
         for (uint32_t c0 = 0; c0 < n_u; c0 += 32) {
             const uint32_t i = c0 + lane;
             const bool valid = i < n_u;
             const uint32_t g = valid ? (ord ? ord[i] : i) : 0u;
-            const uint32_t d = valid ? (Rc[g] >> sh) & 255u : 256u + (uint32_t)lane;
+            const uint32_t d = valid ? (Rc[g] >> sh) & (ND - 1) : ND + (uint32_t)lane;
             const unsigned peers = __match_any_sync(0xffffffffu, d);
             const int leader = __ffs(peers) - 1;
             uint32_t at = (valid && lane == leader) ? RH[d] : 0u;
             at = __shfl_sync(0xffffffffu, at, leader);
-            if (valid) pout[at + __popc(peers & lt)] = g;
+            if (valid) pout[at + __popc(peers & lt)] = (uint16_t)g;
             __syncwarp();
             if (valid && lane == leader) RH[d] = at + __popc(peers);
             __syncwarp();
@@ -844,12 +853,12 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
 }
 
 template <uint32_t C, int W>
-__global__ void __launch_bounds__(W * 32) k_seedprep_c(BatchView v, const int32_t* __restrict__ list,
+__global__ void __launch_bounds__(W * 32, 4) k_seedprep_c(BatchView v, const int32_t* __restrict__ list,
                                                        const uint32_t* __restrict__ n_list) {
     extern __shared__ __align__(16) uint8_t smem[];
-    __shared__ uint32_t s_seg[SEEDC_SEGS + 1];  // seg_off, for references of at most SEEDC_SEGS segments
     const int wib = threadIdx.x >> 5;
     uint8_t* base = smem + (size_t)wib * seedc_bytes(C);
+    uint32_t* s_seg = (uint32_t*)(smem + (size_t)W * seedc_bytes(C));  // seg_off (seedc_seg_bytes)
     const int32_t n = (int32_t)*n_list;
     const bool staged = v.I.n_seg <= SEEDC_SEGS;
     if (staged)
@@ -2516,27 +2525,30 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         SHM_CUDA(cudaGetLastError());
         count_launch();
     }
+    const size_t sgb = seedc_seg_bytes(v.I.n_seg);
     if (!c->seedc_smem_set) {
+        const int sg = (int)seedc_seg_bytes(SEEDC_SEGS);
         SHM_CUDA(cudaFuncSetAttribute(k_seedprep_c<256, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(8 * seedc_bytes(256))));
+                                      (int)(8 * seedc_bytes(256)) + sg));
         SHM_CUDA(cudaFuncSetAttribute(k_seedprep_c<512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(4 * seedc_bytes(512))));
+                                      (int)(4 * seedc_bytes(512)) + sg));
         SHM_CUDA(cudaFuncSetAttribute(k_seedprep_c<1024, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(4 * seedc_bytes(1024))));
+                                      (int)(4 * seedc_bytes(1024)) + sg));
         c->seedc_smem_set = 1;
     }
     if (bp.n_cap_512) {  // 512 < m <= 1024
-        k_seedprep_c<1024, 4><<<grid_for((size_t)bp.n_cap_512 * 32, 128, 1), 128, 4 * seedc_bytes(1024), s2>>>(
+        k_seedprep_c<1024, 4><<<grid_for((size_t)bp.n_cap_512 * 32, 128, 1), 128, 4 * seedc_bytes(1024) + sgb, s2>>>(
             v, LB + 2 * (size_t)n, NB + 2);
         SHM_CUDA(cudaGetLastError());
         count_launch();
     }
     if (side) SHM_CUDA(cudaEventRecord(c->join, s2));
     {
-        k_seedprep_c<256, 8><<<grid_for((size_t)n * 32, 256, 3), 256, 8 * seedc_bytes(256), s>>>(v, LB, NB);
+        k_seedprep_c<256, 8><<<grid_for((size_t)n * 32, 256, 4), 256, 8 * seedc_bytes(256) + sgb, s>>>(v, LB, NB);
         SHM_CUDA(cudaGetLastError());
         count_launch();
-        k_seedprep_c<512, 4><<<grid_for((size_t)n * 32, 128, 3), 128, 4 * seedc_bytes(512), s>>>(v, LB + n, NB + 1);
+        k_seedprep_c<512, 4><<<grid_for((size_t)n * 32, 128, 4), 128, 4 * seedc_bytes(512) + sgb, s>>>(v, LB + n,
+                                                                                                      NB + 1);
         SHM_CUDA(cudaGetLastError());
         count_launch();
     }
