@@ -51,6 +51,7 @@
 
 #include "shm_common.cuh"
 #include "shm_map.cuh"
+#include "../host/pack.hpp"
 #include "shm_prims.cuh"
 #include "shm_sketch.cuh"
 
@@ -2121,6 +2122,7 @@ struct MapScratch {
     DevBuf<int32_t> retry_idx;
     DevBuf<uint64_t> km_h, pht_key, hw, hw_off, bt_size, bt_off;
     DevBuf<SeedRec> sd;
+    DevBuf<uint32_t> pk_codes[2], pk_mask[2];  // host-buffer batches, packed (host/pack.hpp)
     DevBuf<uint64_t> sd_h;
     DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
         cidx, cfar, sort_scr, ovf_list, r_flags;
@@ -2163,6 +2165,7 @@ void mapctx_destroy(MapCtx* c) {
     }
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->h_slots) cudaFreeHost(c->h_slots);
+    if (c->h_pack) cudaFreeHost(c->h_pack);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (auto& e : c->copied)
         if (e) cudaEventDestroy(e);
@@ -2352,13 +2355,15 @@ static void collect_batch(MapCtx* c, const BatchSlot& sl, std::vector<Overflow>&
 }
 
 // Enqueues the mapping of one batch whose bytes are already on the device at
-// d_seq (relative offsets h_offs[i] - h_offs[0]); caps as for plan_batch.
+// d_seq (relative offsets h_offs[i] - h_offs[0]), or packed (pk_codes,
+// pk_mask: host/pack.hpp) when those are set; caps as for plan_batch.
 // The host waits once, for the sizes of the bucket tables; everything after
 // is queued, and the batch's results reach `sl` when the stream drains
 // (collect_batch then lists the reads that overflowed a capacity).
 static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
                       const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps, bool exact,
-                      uint8_t* h_plan, StageTimer& T, BatchSlot& sl) {
+                      uint8_t* h_plan, StageTimer& T, BatchSlot& sl, const uint32_t* pk_codes = nullptr,
+                      const uint32_t* pk_mask = nullptr) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
     HostClock H;
@@ -2481,6 +2486,8 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     a.kmer_cnt = S.kcnt.p;
     a.out_h = S.km_h.p;
     a.out_rs = S.km_rs.p;
+    a.pk_codes = pk_codes;  // packed reads instead of d_seq when set
+    a.pk_mask = pk_mask;
     T.begin(STG_SKETCH);
     launch_sketch(SK_APPEND, a, S.luts, s);
     T.end();
@@ -2709,8 +2716,11 @@ static const int32_t DEV_BATCH_READS = 1 << 17;
 // The first batch of a device-resident call is small, so the device starts
 // while the host plans the next batch (planning costs ~5 ns a read).
 static const int32_t DEV_FIRST_BATCH_READS = 1 << 14;
-static const int64_t HOST_BATCH_BASES = (int64_t)1 << 29;
+static const int64_t HOST_BATCH_BASES = (int64_t)1 << 28;
 static const int32_t HOST_BATCH_READS = 1 << 15;
+// The first batch of a host-buffer call is small: its packing on the host is
+// the part of the call that nothing overlaps.
+static const int32_t HOST_FIRST_BATCH_READS = 1 << 12;
 
 __global__ void k_scatter_records(const shm_map_record* __restrict__ src, const int32_t* __restrict__ idx, int32_t n,
                                   shm_map_record* __restrict__ dst) {
@@ -2891,39 +2901,71 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     SHM_CUDA(cudaSetDevice(c->device));
     MapScratch& S = *c->scr;
     cudaStream_t s = c->stream;
-    const auto batches = cut_batches(offs, n, plain, HOST_BATCH_READS, HOST_BATCH_BASES);
+    const auto batches = cut_batches(offs, n, plain, HOST_BATCH_READS, HOST_BATCH_BASES, HOST_FIRST_BATCH_READS);
     int64_t max_nb = 0;
     int32_t max_n = 0;
     for (auto [i, j] : batches) {
         max_nb = std::max<int64_t>(max_nb, offs[j] - offs[i]);
         max_n = std::max(max_n, j - i);
     }
-    S.seqb[0].reserve((size_t)max_nb + 32);
-    S.seqb[1].reserve((size_t)max_nb + 32);
+    // reads go up packed: two pinned slots on the host, two device buffers
+    const size_t cwords = packed_code_words(max_nb), mwords = packed_mask_words(max_nb);
+    const size_t slot_bytes = (4 * (cwords + mwords) + 63) / 64 * 64;  // slots and their code words 64-byte aligned
+    if (2 * slot_bytes > c->h_pack_cap) {
+        if (c->h_pack) SHM_CUDA(cudaFreeHost(c->h_pack));
+        c->h_pack = nullptr;
+        c->h_pack_cap = 0;
+        SHM_CUDA(cudaHostAlloc(&c->h_pack, 2 * slot_bytes, cudaHostAllocDefault));
+        c->h_pack_cap = 2 * slot_bytes;
+    }
+    for (int k = 0; k < 2; k++) {
+        S.pk_codes[k].reserve(cwords);
+        S.pk_mask[k].reserve(mwords);
+    }
     S.out.reserve((size_t)std::max(max_n, 1));
-    auto send = [&](size_t b) {  // on the copy stream, after the sketch that last read the buffer
+    auto h_codes = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes); };
+    auto h_mask = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes + 4 * cwords); };
+    auto pack = [&](size_t b) {  // on the host threads in the background, once the slot's previous upload left
+        const auto [i, j] = batches[b];
+        SHM_CUDA(cudaEventSynchronize(c->copied[b & 1]));
+        pack_reads_host_start(seqs + offs[i], offs[j] - offs[i], h_codes(b), h_mask(b));
+    };
+    auto send = [&](size_t b) {  // on the copy stream, after the sketch that last read the buffers
         const auto [i, j] = batches[b];
         const int64_t nb = offs[j] - offs[i];
-        DevBuf<uint8_t>& buf = S.seqb[b & 1];
         SHM_CUDA(cudaStreamWaitEvent(c->copy_stream, c->sketched[b & 1], 0));
-        SHM_CUDA(cudaMemsetAsync(buf.p + nb, 0, 32, c->copy_stream));
-        SHM_CUDA(cudaMemcpyAsync(buf.p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, c->copy_stream));
+        SHM_CUDA(cudaMemcpyAsync(S.pk_codes[b & 1].p, h_codes(b), 4 * packed_code_words(nb), cudaMemcpyHostToDevice,
+                                 c->copy_stream));
+        SHM_CUDA(cudaMemcpyAsync(S.pk_mask[b & 1].p, h_mask(b), 4 * packed_mask_words(nb), cudaMemcpyHostToDevice,
+                                 c->copy_stream));
         SHM_CUDA(cudaEventRecord(c->copied[b & 1], c->copy_stream));
     };
     std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
     const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
     HostClock H;
-    if (!batches.empty()) send(0);
+    // batch b+1 is packed on the host threads while batch b is queued, b-1
+    // maps and b goes up
+    if (!batches.empty()) {
+        pack(0);
+        pack_reads_host_wait();
+        send(0);
+        if (batches.size() > 1) pack(1);
+    }
     for (size_t b = 0; b < batches.size(); b++) {
         const auto [i, j] = batches[b];
         SHM_CUDA(cudaStreamWaitEvent(s, c->copied[b & 1], 0));
-        if (b + 1 < batches.size()) send(b + 1);
         c->sketch_done = c->sketched[b & 1];
-        run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b]);
+        run_batch(c, ix, p, nullptr, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b],
+                  S.pk_codes[b & 1].p, S.pk_mask[b & 1].p);
         c->sketch_done = nullptr;
         SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s));
+        if (b + 1 < batches.size()) {
+            pack_reads_host_wait();
+            send(b + 1);
+            if (b + 2 < batches.size()) pack(b + 2);
+        }
     }
     H.mark("enqueue");
     SHM_CUDA(cudaStreamSynchronize(s));
@@ -2933,6 +2975,7 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         if (slots[b].R->nj <= slots[b].job_cap) continue;
         const auto [i, j] = batches[b];
         const int64_t nb = offs[j] - offs[i];
+        S.seqb[0].reserve((size_t)nb + 32);
         SHM_CUDA(cudaMemsetAsync(S.seqb[0].p + nb, 0, 32, s));
         SHM_CUDA(cudaMemcpyAsync(S.seqb[0].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, s));
         run_batch(c, ix, p, S.seqb[0].p, offs + i, j - i, S.out.p, nullptr, true, plans[b], T, slots[b]);

@@ -58,6 +58,8 @@ struct MapCtx {
     size_t h_pinned_cap = 0;
     void* h_slots = nullptr;  // per-call batch results
     size_t h_slots_cap = 0;
+    uint8_t* h_pack = nullptr;  // two slots of packed reads (codes, mask) on their way up
+    size_t h_pack_cap = 0;
     // work counters (always on): see WORK_NAMES
     int64_t work[16] = {};
     int seed_smem_set = 0;   // dynamic shared memory the seed kernels have been allowed so far

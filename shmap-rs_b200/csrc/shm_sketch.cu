@@ -91,6 +91,28 @@ struct GlobalBytes {
 
 constexpr int SK_LB = 16;  // selections a thread holds per run (append mode)
 
+// The same bytes from packed reads (codes and mask of base B0 + x): ACGT
+// letters (upper case) and 'N' for a masked base, 0 outside [first, lim).
+struct GlobalPacked {
+    const uint32_t* codes;
+    const uint32_t* mask;
+    int64_t B0, first, lim;
+    __device__ __forceinline__ uint32_t word(int64_t w) const {
+        uint32_t v = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t x = 4 * w + j;
+            if (x >= first && x < lim) {
+                const int64_t p = B0 + x;
+                const uint32_t c = (__ldg(codes + (p >> 4)) >> (2 * (p & 15))) & 3u;
+                const bool m = (__ldg(mask + (p >> 5)) >> (p & 31)) & 1u;
+                v |= (m ? 0x4eu : (uint32_t)"ACTG"[c]) << (8 * j);
+            }
+        }
+        return v;
+    }
+};
+
 // Where a thread's selections go: its count, and (write mode) the run's
 // output range from chunk_out[c]. Append
 // mode holds the run's first SK_LB selections in thread-local slots (cached
@@ -220,9 +242,15 @@ constexpr size_t sk_dyn_bytes(int) { return (size_t)SK_TILE_BYTES; }
 // staged in shared memory with coalesced 16-byte loads and the runs roll out
 // of shared memory. A tile whose range does not fit (many sequences shorter
 // than k between its runs) rolls from global memory instead.
-template <int MODE>
+//
+// PK: the tile is staged from packed reads instead, each code word unpacked
+// to four words of letters (a 256-entry table of four letters per code byte)
+// and masked bases set to 'N', so the rolling below sees the bytes that the
+// same read's upper-cased ASCII would give — the same hashes.
+template <int MODE, bool PK>
 __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const SketchLuts* __restrict__ luts) {
     __shared__ LutPair Lin[256], Lout[256];
+    __shared__ uint32_t s_unpack[PK ? 256 : 1];
     __shared__ int64_t s_lo, s_hi;
     __shared__ int32_t s_q[2];
     extern __shared__ __align__(16) uint8_t sk_dyn[];
@@ -230,6 +258,11 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         Lin[i] = LutPair{luts->fw[i], luts->rc_k1[i]};
         Lout[i] = LutPair{luts->fw_k[i], luts->rc_r1[i]};
+        if (PK) {
+            uint32_t w = 0;
+            for (int j = 0; j < 4; j++) w |= (uint32_t)"ACTG"[(i >> (2 * j)) & 3] << (8 * j);
+            s_unpack[i] = w;
+        }
     }
     Emit e;
     const int lane = threadIdx.x & 31;
@@ -271,11 +304,30 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
         }
         __syncthreads();  // s_lo/s_hi written; the previous tile's readers are done
         const int64_t lo_b = s_lo, hi_b = s_hi;
-        const uint8_t* A0 = (const uint8_t*)((uintptr_t)(a.seq + lo_b) & ~(uintptr_t)15);
-        const int64_t lim = (int64_t)((a.seq + hi_b) - A0);  // the tile's bytes are [first, lim) from A0
-        const int64_t first = (int64_t)((a.seq + lo_b) - A0);
+        // the tile's bytes are [first, lim) from A0 (ASCII) or from base B0 (packed), both 16-aligned
+        const uint8_t* A0 = PK ? nullptr : (const uint8_t*)((uintptr_t)(a.seq + lo_b) & ~(uintptr_t)15);
+        const int64_t B0 = lo_b & ~(int64_t)15;
+        const int64_t lim = PK ? hi_b - B0 : (int64_t)((a.seq + hi_b) - A0);
+        const int64_t first = PK ? lo_b - B0 : (int64_t)((a.seq + lo_b) - A0);
         const bool staged = lim <= (int64_t)SK_TILE_CAP;
-        if (staged) {
+        if (PK && staged) {
+            const int nv = (int)((lim + 15) >> 4);
+            for (int v = threadIdx.x; v < nv; v += SK_THREADS) {
+                const int64_t cwi = (B0 >> 4) + v;  // code word of bases B0 + 16v ..
+                const uint32_t cw = __ldg(a.pk_codes + cwi);
+                const uint32_t m16 = (__ldg(a.pk_mask + (cwi >> 1)) >> (16 * (cwi & 1))) & 0xffffu;
+#pragma unroll
+                for (int m = 0; m < 4; m++) {
+                    uint32_t w = s_unpack[(cw >> (8 * m)) & 0xffu];
+                    const uint32_t nib = (m16 >> (4 * m)) & 15u;
+                    if (nib) {  // masked bases: 'N' (byte j of M is 0xff for bit j of nib)
+                        const uint32_t M = ((nib * 0x00204081u) & 0x01010101u) * 0xffu;
+                        w = (w & ~M) | (0x4e4e4e4eu & M);
+                    }
+                    tile[pword(4 * v + m)] = w;
+                }
+            }
+        } else if (staged) {
             const int nv = (int)((lim + 15) >> 4);
             for (int v = threadIdx.x; v < nv; v += SK_THREADS) {
                 uint32_t wv[4];
@@ -311,10 +363,13 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
                 e.out_cap = (uint32_t)(a.kmer_off[q + 1] - e.out_base);
             }
         }
-        const int64_t x = (int64_t)((a.seq + start) - A0);      // the run's first byte from A0
-        const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;  // r of the run's first window
+        const int64_t x = PK ? start - B0 : (int64_t)((a.seq + start) - A0);  // the run's first byte in the tile
+        const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;              // r of the run's first window
         if (staged)
             sketch_run<MODE>(a, Lin, Lout, StagedBytes{tile}, (int)x, cnt, k, thr, q, r0, e);
+        else if (PK)
+            sketch_run<MODE>(a, Lin, Lout, GlobalPacked{a.pk_codes, a.pk_mask, B0, first, lim}, x, cnt, k, thr, q, r0,
+                             e);
         else
             sketch_run<MODE>(a, Lin, Lout, GlobalBytes{A0, first, lim}, x, cnt, k, thr, q, r0, e);
         if (MODE == SK_COUNT && c < n_chunks) a.chunk_cnt[c] = e.n_sel;
@@ -359,28 +414,38 @@ SketchLuts* create_device_luts(int32_t k, cudaStream_t s) {
 
 void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStream_t s) {
     if (a.n_chunks == 0) return;
+    const bool pk = a.pk_codes != nullptr;
+    if (pk && mode != SK_APPEND) throw shm_cuda_error(cudaErrorInvalidValue);
     const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
     const int grid = grid_for(n_tiles, 1, 5);  // tiles, at most 5 resident CTAs per SM
     const size_t dyn = sk_dyn_bytes(mode);
-    {  // the dynamic shared memory limit, once per device and mode
+    {  // the dynamic shared memory limit, once per device and kernel
         static std::mutex mu;
-        static bool done[3][64] = {};
+        static bool done[4][64] = {};
         int dev = 0;
         SHM_CUDA(cudaGetDevice(&dev));
+        const int kk = pk ? 3 : mode;
         std::lock_guard<std::mutex> g(mu);
-        if (dev >= 0 && dev < 64 && !done[mode][dev]) {
-            if (mode == SK_COUNT)
-                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        if (dev >= 0 && dev < 64 && !done[kk][dev]) {
+            if (pk)
+                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_APPEND, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)dyn));
+            else if (mode == SK_COUNT)
+                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_COUNT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)dyn));
             else if (mode == SK_WRITE)
-                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_WRITE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_WRITE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)dyn));
             else
-                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_APPEND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-            done[mode][dev] = true;
+                SHM_CUDA(cudaFuncSetAttribute(k_sketch<SK_APPEND, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)dyn));
+            done[kk][dev] = true;
         }
     }
-    if (mode == SK_COUNT) k_sketch<SK_COUNT><<<grid, SK_THREADS, dyn, s>>>(a, L);
-    else if (mode == SK_WRITE) k_sketch<SK_WRITE><<<grid, SK_THREADS, dyn, s>>>(a, L);
-    else k_sketch<SK_APPEND><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    if (pk) k_sketch<SK_APPEND, true><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    else if (mode == SK_COUNT) k_sketch<SK_COUNT, false><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    else if (mode == SK_WRITE) k_sketch<SK_WRITE, false><<<grid, SK_THREADS, dyn, s>>>(a, L);
+    else k_sketch<SK_APPEND, false><<<grid, SK_THREADS, dyn, s>>>(a, L);
     SHM_CUDA(cudaGetLastError());
     count_launch();
 }

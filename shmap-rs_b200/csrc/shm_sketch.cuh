@@ -32,6 +32,12 @@ struct SketchArgs {
     // outputs
     uint64_t* out_h;
     uint32_t* out_rs;  // r << 1 | strand
+    // SK_APPEND only: when set, the reads come as 2-bit codes and a non-ACGT
+    // mask instead of `seq` (the layout of host/pack.hpp: base p, relative to
+    // the batch, is bits 2(p & 15) of pk_codes[p >> 4], masked when bit p & 31
+    // of pk_mask[p >> 5] is set; two spare groups of 32 past the end)
+    const uint32_t* pk_codes;
+    const uint32_t* pk_mask;
 };
 
 // The five lookup tables of src/sketch.rs:50-97 for one k, in device memory

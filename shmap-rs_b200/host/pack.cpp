@@ -1,0 +1,240 @@
+// Host packing of reads into 2-bit codes and a non-ACGT mask, the form the
+// host-buffer path uploads (a quarter of the ASCII bytes, plus an eighth for
+// the mask). Codes: a byte b of ACGT in either case has code (b >> 1) & 3
+// (A 0, C 1, T 2, G 3); base p is bits 2(p & 15) of codes[p >> 4]. Mask: bit
+// p & 31 of mask[p >> 5] is set for every other byte (those hash to 0 on
+// both strands, src/sketch.rs:58-97) and for positions past the end.
+//
+// A byte is ACGT iff its upper-cased value equals the letter its code names:
+// 0x41 + 2c, plus 15 for c = 2 (T is 0x54); the AVX2 form tests 32 bytes at
+// once. The work is split over a persistent pool of host threads.
+#include "pack.hpp"
+
+#include <immintrin.h>
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace shm {
+namespace {
+
+// 32 bytes at s: codes of bases 0..31 (two words) and their mask word.
+inline void pack32_scalar(const uint8_t* s, uint32_t* codes, uint32_t* mask, int n) {
+    uint32_t c0 = 0, c1 = 0, m = 0;
+    for (int i = 0; i < 32; i++) {
+        uint32_t c = 0, bad = 1;
+        if (i < n) {
+            const uint32_t b = s[i];
+            c = (b >> 1) & 3u;
+            const uint32_t want = 0x41u + 2u * c + (c == 2 ? 15u : 0u);
+            bad = (b & 0xdfu) == want ? 0u : 1u;
+        }
+        if (i < 16) c0 |= c << (2 * i);
+        else c1 |= c << (2 * (i - 16));
+        m |= bad << i;
+    }
+    codes[0] = c0;
+    codes[1] = c1;
+    mask[0] = m;
+}
+
+__attribute__((target("avx2"))) void pack_range_avx2(const uint8_t* s, int64_t n32, uint32_t* codes, uint32_t* mask) {
+    const __m256i k3 = _mm256_set1_epi8(3), kdf = _mm256_set1_epi8((char)0xdf), k41 = _mm256_set1_epi8(0x41),
+                  k15 = _mm256_set1_epi8(15), k2 = _mm256_set1_epi8(2);
+    const __m256i m1 = _mm256_set1_epi16(0x0401), m2 = _mm256_set1_epi32(0x00100001);
+    // the low byte of every 32-bit lane (4 codes each) to the front of each 128-bit half
+    const __m256i gather = _mm256_setr_epi8(0, 4, 8, 12, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, 0, 4, 8,
+                                            12, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1);
+    for (int64_t g = 0; g < n32; g++) {
+        const __m256i v = _mm256_loadu_si256((const __m256i*)(s + 32 * g));
+        const __m256i c = _mm256_and_si256(_mm256_srli_epi16(v, 1), k3);
+        const __m256i u = _mm256_and_si256(v, kdf);
+        const __m256i is2 = _mm256_cmpeq_epi8(c, k2);
+        const __m256i want = _mm256_add_epi8(_mm256_add_epi8(k41, _mm256_add_epi8(c, c)), _mm256_and_si256(is2, k15));
+        const uint32_t good = (uint32_t)_mm256_movemask_epi8(_mm256_cmpeq_epi8(u, want));
+        // byte pairs c0 + 4 c1, then pairs of those + 16x: 8 code bits per 32-bit lane
+        const __m256i p = _mm256_madd_epi16(_mm256_maddubs_epi16(c, m1), m2);
+        const __m256i q = _mm256_shuffle_epi8(p, gather);
+        // streaming stores: the output is read next by the copy engine, and
+        // plain stores would first read every output line into the cache
+        const uint64_t cw = (uint64_t)(uint32_t)_mm256_extract_epi32(q, 0) |
+                            ((uint64_t)(uint32_t)_mm256_extract_epi32(q, 4) << 32);
+        _mm_stream_si64((long long*)(codes + 2 * g), (long long)cw);
+        _mm_stream_si32((int*)(mask + g), (int)~good);
+    }
+    _mm_sfence();
+}
+
+void pack_range_scalar(const uint8_t* s, int64_t n32, uint32_t* codes, uint32_t* mask) {
+    for (int64_t g = 0; g < n32; g++) pack32_scalar(s + 32 * g, codes + 2 * g, mask + g, 32);
+}
+
+bool have_avx2() {
+    static const bool v = __builtin_cpu_supports("avx2");
+    return v;
+}
+
+// Persistent workers. start(n, f) has them call f(0..n-1) and returns at
+// once; finish() waits until every call has returned and no worker holds
+// the job; run(n, f) does both, the caller working too. One job at a time.
+class Pool {
+  public:
+    Pool() {
+        const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+        for (unsigned i = 1; i < hc; i++) th_.emplace_back([this] { loop(); });
+    }
+    ~Pool() {
+        finish();
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    void start(int n, std::function<void(int)> f) {
+        finish();
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            job_.f = std::move(f);
+            job_.n = n;
+            job_.next.store(0);
+            job_.done = 0;
+            cur_ = &job_;
+            gen_++;
+        }
+        cv_.notify_all();
+    }
+    void finish() {
+        std::unique_lock<std::mutex> g(mu_);
+        if (!cur_) return;
+        done_cv_.wait(g, [&] { return job_.done == job_.n && active_ == 0; });
+        cur_ = nullptr;
+    }
+    void run(int n, std::function<void(int)> f) {
+        start(n, std::move(f));
+        work(job_);
+        finish();
+    }
+    int size() const { return (int)th_.size() + 1; }
+
+  private:
+    struct Job {
+        std::function<void(int)> f;
+        int n = 0;
+        std::atomic<int> next{0};
+        int done = 0;  // under mu_
+    };
+    void work(Job& j) {
+        for (;;) {
+            const int i = j.next.fetch_add(1);
+            if (i >= j.n) return;
+            j.f(i);
+            std::lock_guard<std::mutex> g(mu_);
+            if (++j.done == j.n) done_cv_.notify_all();
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            Job* j = nullptr;
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                j = cur_;
+                if (j) active_++;
+            }
+            if (!j) continue;
+            work(*j);
+            std::lock_guard<std::mutex> g(mu_);
+            if (--active_ == 0) done_cv_.notify_all();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    Job job_;
+    Job* cur_ = nullptr;
+    int active_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+Pool& pool() {
+    static Pool p;
+    return p;
+}
+
+// The whole 32-byte groups as pool tasks; the tail and two spare groups
+// (codes 0, every position masked) by the caller.
+static void pack_tail(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask) {
+    const int64_t n32 = nb / 32;
+    pack32_scalar(seq + 32 * n32, codes + 2 * n32, mask + n32, (int)(nb - 32 * n32));
+    for (int64_t g = n32 + 1; g < n32 + 3; g++) {
+        codes[2 * g] = codes[2 * g + 1] = 0;
+        mask[g] = ~0u;
+    }
+}
+
+static std::function<void(int)> pack_tasks(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask,
+                                           int& tasks) {
+    const int64_t n32 = nb / 32;
+    const int64_t per = std::max<int64_t>(1 << 15, (n32 + 4 * pool().size() - 1) / (4 * pool().size()));
+    tasks = (int)((n32 + per - 1) / per);
+    const bool avx2 = have_avx2();
+    return [=](int t) {
+        const int64_t g0 = per * t, g1 = std::min(n32, g0 + per);
+        if (avx2) pack_range_avx2(seq + 32 * g0, g1 - g0, codes + 2 * g0, mask + g0);
+        else pack_range_scalar(seq + 32 * g0, g1 - g0, codes + 2 * g0, mask + g0);
+    };
+}
+
+}  // namespace
+
+void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask) {
+    int tasks = 0;
+    auto f = pack_tasks(seq, nb, codes, mask, tasks);
+    if (tasks > 0) pool().run(tasks, std::move(f));
+    pack_tail(seq, nb, codes, mask);
+}
+
+void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask) {
+    int tasks = 0;
+    auto f = pack_tasks(seq, nb, codes, mask, tasks);
+    pack_tail(seq, nb, codes, mask);
+    if (tasks > 0) pool().start(tasks, std::move(f));
+}
+
+void pack_reads_host_wait() { pool().finish(); }
+
+size_t packed_code_words(int64_t nb) { return 2 * (size_t)(nb / 32 + 3); }
+size_t packed_mask_words(int64_t nb) { return (size_t)(nb / 32 + 3); }
+
+}  // namespace shm
+
+// Test hook (not part of the C ABI of include/shmap_gpu.h): the packing of
+// `nb` bytes into caller buffers of packed_code_words / packed_mask_words.
+extern "C" int shm_internal_pack_reads(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask,
+                                       int force_scalar) {
+    if (nb < 0 || (nb > 0 && (!seq || !codes || !mask))) return -1;
+    if (force_scalar) {
+        const int64_t n32 = nb / 32;
+        for (int64_t g = 0; g < n32; g++) shm::pack32_scalar(seq + 32 * g, codes + 2 * g, mask + g, 32);
+        shm::pack32_scalar(seq + 32 * n32, codes + 2 * n32, mask + n32, (int)(nb - 32 * n32));
+        for (int64_t g = n32 + 1; g < n32 + 3; g++) {
+            codes[2 * g] = codes[2 * g + 1] = 0;
+            mask[g] = ~0u;
+        }
+        return 0;
+    }
+    shm::pack_reads_host(seq, nb, codes, mask);
+    return 0;
+}

@@ -1,0 +1,18 @@
+// Host packing of reads into 2-bit codes and a non-ACGT mask (see pack.cpp).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace shm {
+
+// Packs nb bytes; codes needs packed_code_words(nb) words, mask
+// packed_mask_words(nb) (the spare words past the end hold code 0, masked).
+void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask);
+// The same on the host threads in the background: start returns at once,
+// wait returns when the packing is complete (one packing at a time).
+void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask);
+void pack_reads_host_wait();
+size_t packed_code_words(int64_t nb);
+size_t packed_mask_words(int64_t nb);
+
+}  // namespace shm

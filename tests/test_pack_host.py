@@ -1,0 +1,70 @@
+"""Host packing of reads (shmap-rs_b200/host/pack.cpp): 2-bit codes and the
+non-ACGT mask the host-buffer path uploads, checked against a numpy model
+of the definition on every byte value, both cases and ragged lengths; the
+AVX2 form and the scalar form must agree bit for bit."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import shmap_b200 as sb
+
+
+def _lib():
+    lib = sb.lib()
+    f = lib.shm_internal_pack_reads
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    f.restype = ctypes.c_int
+    return f
+
+
+def _model(seq: np.ndarray):
+    """codes[p >> 4] bits 2(p & 15) = (b >> 1) & 3; mask bit p set unless b is ACGT/acgt."""
+    nb = len(seq)
+    groups = nb // 32 + 3
+    code = ((seq >> 1) & 3).astype(np.uint64)
+    ok = np.isin(seq, np.frombuffer(b"ACGTacgt", np.uint8))
+    codes = np.zeros(2 * groups, np.uint64)
+    mask = np.zeros(groups, np.uint64)
+    p = np.arange(nb, dtype=np.int64)
+    np.bitwise_or.at(codes, p >> 4, code << (2 * (p & 15)).astype(np.uint64))
+    np.bitwise_or.at(mask, p >> 5, (~ok).astype(np.uint64) << (p & 31).astype(np.uint64))
+    # positions past the end are masked (codes 0)
+    pos = np.arange(nb, 32 * groups, dtype=np.int64)
+    np.bitwise_or.at(mask, pos >> 5, np.uint64(1) << (pos & 31).astype(np.uint64))
+    return codes.astype(np.uint32), mask.astype(np.uint32)
+
+
+def _pack(seq: np.ndarray, scalar: int):
+    f = _lib()
+    groups = len(seq) // 32 + 3
+    codes = np.full(2 * groups, 0xDEADBEEF, np.uint32)
+    mask = np.full(groups, 0xDEADBEEF, np.uint32)
+    buf = np.ascontiguousarray(seq)
+    assert f(buf.ctypes.data if len(buf) else None, len(buf), codes.ctypes.data, mask.ctypes.data, scalar) == 0
+    return codes, mask
+
+
+@pytest.mark.parametrize("nb", [0, 1, 31, 32, 33, 64, 1000, 1 << 16, (1 << 20) + 7])
+def test_pack_matches_model(nb):
+    rng = np.random.default_rng(nb + 1)
+    # mostly bases of both cases, with every other byte value sprinkled in
+    seq = rng.choice(np.frombuffer(b"ACGTacgt", np.uint8), nb)
+    if nb:
+        k = max(1, nb // 50)
+        seq[rng.integers(0, nb, k)] = rng.integers(0, 256, k).astype(np.uint8)
+    want_c, want_m = _model(seq)
+    for scalar in (0, 1):
+        c, m = _pack(seq, scalar)
+        assert np.array_equal(m, want_m), scalar
+        assert np.array_equal(c, want_c), scalar
+
+
+def test_pack_every_byte_value():
+    seq = np.tile(np.arange(256, dtype=np.uint8), 40)  # 10240 bytes, every value at every offset mod 32
+    want_c, want_m = _model(seq)
+    for scalar in (0, 1):
+        c, m = _pack(seq, scalar)
+        assert np.array_equal(m, want_m) and np.array_equal(c, want_c)
+    ok = np.isin(np.arange(256), np.frombuffer(b"ACGTacgt", np.uint8))
+    assert ok.sum() == 8
