@@ -2123,6 +2123,7 @@ struct MapScratch {
     DevBuf<uint64_t> km_h, pht_key, hw, hw_off, bt_size, bt_off;
     DevBuf<SeedRec> sd;
     DevBuf<uint32_t> pk_codes[2], pk_mask[2];  // host-buffer batches, packed (host/pack.hpp)
+    DevBuf<uint32_t> pk_list[2];               // their nonzero mask words as uploaded (index, word)
     DevBuf<uint64_t> sd_h;
     DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
         cidx, cfar, sort_scr, ovf_list, r_flags;
@@ -2828,6 +2829,12 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
     }
 }
 
+// The nonzero mask words of a packed batch into its zeroed mask.
+__global__ void k_mask_scatter(const uint32_t* __restrict__ pairs, uint32_t n, uint32_t* __restrict__ mask) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        mask[pairs[2 * i]] = pairs[2 * i + 1];
+}
+
 // Batches of at most max_reads reads and max_bases bases (one read at a time
 // in the plain form).
 static std::vector<std::pair<int32_t, int32_t>> cut_batches(const int64_t* offs, int32_t n, bool plain,
@@ -2908,9 +2915,10 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         max_nb = std::max<int64_t>(max_nb, offs[j] - offs[i]);
         max_n = std::max(max_n, j - i);
     }
-    // reads go up packed: two pinned slots on the host, two device buffers
+    // reads go up packed: two pinned slots on the host (codes, then the
+    // nonzero mask words as pairs), two device buffers
     const size_t cwords = packed_code_words(max_nb), mwords = packed_mask_words(max_nb);
-    const size_t slot_bytes = (4 * (cwords + mwords) + 63) / 64 * 64;  // slots and their code words 64-byte aligned
+    const size_t slot_bytes = (4 * (cwords + 2 * mwords) + 63) / 64 * 64;  // slots and their code words 64-byte aligned
     if (2 * slot_bytes > c->h_pack_cap) {
         if (c->h_pack) SHM_CUDA(cudaFreeHost(c->h_pack));
         c->h_pack = nullptr;
@@ -2921,24 +2929,37 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     for (int k = 0; k < 2; k++) {
         S.pk_codes[k].reserve(cwords);
         S.pk_mask[k].reserve(mwords);
+        S.pk_list[k].reserve(2 * mwords);
     }
     S.out.reserve((size_t)std::max(max_n, 1));
     auto h_codes = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes); };
-    auto h_mask = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes + 4 * cwords); };
+    auto h_list = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes + 4 * cwords); };
     auto pack = [&](size_t b) {  // on the host threads in the background, once the slot's previous upload left
         const auto [i, j] = batches[b];
         SHM_CUDA(cudaEventSynchronize(c->copied[b & 1]));
-        pack_reads_host_start(seqs + offs[i], offs[j] - offs[i], h_codes(b), h_mask(b));
+        pack_reads_host_start(seqs + offs[i], offs[j] - offs[i], h_codes(b));
+    };
+    size_t n_list = 0;  // nonzero mask words of the packing just waited for
+    auto wait = [&](size_t b) {
+        const auto [i, j] = batches[b];
+        n_list = pack_reads_host_wait(h_list(b), packed_mask_words(offs[j] - offs[i]));
     };
     auto send = [&](size_t b) {  // on the copy stream, after the sketch that last read the buffers
         const auto [i, j] = batches[b];
         const int64_t nb = offs[j] - offs[i];
-        SHM_CUDA(cudaStreamWaitEvent(c->copy_stream, c->sketched[b & 1], 0));
+        cudaStream_t cs = c->copy_stream;
+        SHM_CUDA(cudaStreamWaitEvent(cs, c->sketched[b & 1], 0));
         SHM_CUDA(cudaMemcpyAsync(S.pk_codes[b & 1].p, h_codes(b), 4 * packed_code_words(nb), cudaMemcpyHostToDevice,
-                                 c->copy_stream));
-        SHM_CUDA(cudaMemcpyAsync(S.pk_mask[b & 1].p, h_mask(b), 4 * packed_mask_words(nb), cudaMemcpyHostToDevice,
-                                 c->copy_stream));
-        SHM_CUDA(cudaEventRecord(c->copied[b & 1], c->copy_stream));
+                                 cs));
+        SHM_CUDA(cudaMemsetAsync(S.pk_mask[b & 1].p, 0, 4 * packed_mask_words(nb), cs));
+        if (n_list) {  // the nonzero mask words into the zeroed mask
+            SHM_CUDA(cudaMemcpyAsync(S.pk_list[b & 1].p, h_list(b), 8 * n_list, cudaMemcpyHostToDevice, cs));
+            k_mask_scatter<<<grid_for(n_list, 256, 4), 256, 0, cs>>>(S.pk_list[b & 1].p, (uint32_t)n_list,
+                                                                    S.pk_mask[b & 1].p);
+            SHM_CUDA(cudaGetLastError());
+            count_launch();
+        }
+        SHM_CUDA(cudaEventRecord(c->copied[b & 1], cs));
     };
     std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
     const std::vector<uint8_t*> plans = plan_blocks(c, batches);
@@ -2948,7 +2969,7 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     // maps and b goes up
     if (!batches.empty()) {
         pack(0);
-        pack_reads_host_wait();
+        wait(0);
         send(0);
         if (batches.size() > 1) pack(1);
     }
@@ -2962,7 +2983,7 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s));
         if (b + 1 < batches.size()) {
-            pack_reads_host_wait();
+            wait(b + 1);
             send(b + 1);
             if (b + 2 < batches.size()) pack(b + 2);
         }

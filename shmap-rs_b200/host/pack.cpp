@@ -44,7 +44,12 @@ inline void pack32_scalar(const uint8_t* s, uint32_t* codes, uint32_t* mask, int
     mask[0] = m;
 }
 
-__attribute__((target("avx2"))) void pack_range_avx2(const uint8_t* s, int64_t n32, uint32_t* codes, uint32_t* mask) {
+// Nonzero mask words (group index, word) of the sparse form, one list per task.
+using MaskList = std::vector<std::pair<uint32_t, uint32_t>>;
+
+template <bool SPARSE>
+__attribute__((target("avx2"))) void pack_range_avx2(const uint8_t* s, int64_t n32, uint32_t* codes, uint32_t* mask,
+                                                     int64_t g_base, MaskList* list) {
     const __m256i k3 = _mm256_set1_epi8(3), kdf = _mm256_set1_epi8((char)0xdf), k41 = _mm256_set1_epi8(0x41),
                   k15 = _mm256_set1_epi8(15), k2 = _mm256_set1_epi8(2);
     const __m256i m1 = _mm256_set1_epi16(0x0401), m2 = _mm256_set1_epi32(0x00100001);
@@ -66,13 +71,23 @@ __attribute__((target("avx2"))) void pack_range_avx2(const uint8_t* s, int64_t n
         const uint64_t cw = (uint64_t)(uint32_t)_mm256_extract_epi32(q, 0) |
                             ((uint64_t)(uint32_t)_mm256_extract_epi32(q, 4) << 32);
         _mm_stream_si64((long long*)(codes + 2 * g), (long long)cw);
-        _mm_stream_si32((int*)(mask + g), (int)~good);
+        if (SPARSE) {
+            if (~good) list->emplace_back((uint32_t)(g_base + g), ~good);
+        } else {
+            _mm_stream_si32((int*)(mask + g), (int)~good);
+        }
     }
     _mm_sfence();
 }
 
-void pack_range_scalar(const uint8_t* s, int64_t n32, uint32_t* codes, uint32_t* mask) {
-    for (int64_t g = 0; g < n32; g++) pack32_scalar(s + 32 * g, codes + 2 * g, mask + g, 32);
+template <bool SPARSE>
+void pack_range_scalar(const uint8_t* s, int64_t n32, uint32_t* codes, uint32_t* mask, int64_t g_base,
+                       MaskList* list) {
+    for (int64_t g = 0; g < n32; g++) {
+        uint32_t m = 0;
+        pack32_scalar(s + 32 * g, codes + 2 * g, SPARSE ? &m : mask + g, 32);
+        if (SPARSE && m) list->emplace_back((uint32_t)(g_base + g), m);
+    }
 }
 
 bool have_avx2() {
@@ -175,45 +190,81 @@ Pool& pool() {
 
 // The whole 32-byte groups as pool tasks; the tail and two spare groups
 // (codes 0, every position masked) by the caller.
-static void pack_tail(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask) {
+template <bool SPARSE>
+static void pack_tail(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask, MaskList* list) {
     const int64_t n32 = nb / 32;
-    pack32_scalar(seq + 32 * n32, codes + 2 * n32, mask + n32, (int)(nb - 32 * n32));
+    uint32_t m = 0;
+    pack32_scalar(seq + 32 * n32, codes + 2 * n32, SPARSE ? &m : mask + n32, (int)(nb - 32 * n32));
+    if (SPARSE && m) list->emplace_back((uint32_t)n32, m);
     for (int64_t g = n32 + 1; g < n32 + 3; g++) {
         codes[2 * g] = codes[2 * g + 1] = 0;
-        mask[g] = ~0u;
+        if (SPARSE) list->emplace_back((uint32_t)g, ~0u);
+        else mask[g] = ~0u;
     }
 }
 
+static std::vector<MaskList>& task_lists() {
+    static std::vector<MaskList> v;
+    return v;
+}
+
+template <bool SPARSE>
 static std::function<void(int)> pack_tasks(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask,
                                            int& tasks) {
     const int64_t n32 = nb / 32;
     const int64_t per = std::max<int64_t>(1 << 15, (n32 + 4 * pool().size() - 1) / (4 * pool().size()));
     tasks = (int)((n32 + per - 1) / per);
     const bool avx2 = have_avx2();
+    std::vector<MaskList>& lists = task_lists();
+    if (SPARSE) {
+        if ((int)lists.size() < tasks + 1) lists.resize(tasks + 1);
+        for (auto& l : lists) l.clear();
+    }
+    MaskList* L = lists.data();
     return [=](int t) {
         const int64_t g0 = per * t, g1 = std::min(n32, g0 + per);
-        if (avx2) pack_range_avx2(seq + 32 * g0, g1 - g0, codes + 2 * g0, mask + g0);
-        else pack_range_scalar(seq + 32 * g0, g1 - g0, codes + 2 * g0, mask + g0);
+        if (avx2)
+            pack_range_avx2<SPARSE>(seq + 32 * g0, g1 - g0, codes + 2 * g0, SPARSE ? nullptr : mask + g0, g0,
+                                    SPARSE ? L + t : nullptr);
+        else
+            pack_range_scalar<SPARSE>(seq + 32 * g0, g1 - g0, codes + 2 * g0, SPARSE ? nullptr : mask + g0, g0,
+                                      SPARSE ? L + t : nullptr);
     };
 }
+
+int g_sparse_tasks = 0;  // task lists of the sparse packing in flight (the tail's is the last)
 
 }  // namespace
 
 void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask) {
     int tasks = 0;
-    auto f = pack_tasks(seq, nb, codes, mask, tasks);
+    auto f = pack_tasks<false>(seq, nb, codes, mask, tasks);
     if (tasks > 0) pool().run(tasks, std::move(f));
-    pack_tail(seq, nb, codes, mask);
+    pack_tail<false>(seq, nb, codes, mask, nullptr);
 }
 
-void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask) {
+void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes) {
+    pool().finish();
     int tasks = 0;
-    auto f = pack_tasks(seq, nb, codes, mask, tasks);
-    pack_tail(seq, nb, codes, mask);
+    auto f = pack_tasks<true>(seq, nb, codes, nullptr, tasks);
+    pack_tail<true>(seq, nb, codes, nullptr, &task_lists()[tasks]);
+    g_sparse_tasks = tasks;
     if (tasks > 0) pool().start(tasks, std::move(f));
 }
 
-void pack_reads_host_wait() { pool().finish(); }
+size_t pack_reads_host_wait(uint32_t* pairs, size_t cap) {
+    pool().finish();
+    size_t n = 0;
+    for (int t = 0; t <= g_sparse_tasks; t++)
+        for (const auto& e : task_lists()[t]) {
+            if (n < cap) {
+                pairs[2 * n] = e.first;
+                pairs[2 * n + 1] = e.second;
+            }
+            n++;
+        }
+    return n;
+}
 
 size_t packed_code_words(int64_t nb) { return 2 * (size_t)(nb / 32 + 3); }
 size_t packed_mask_words(int64_t nb) { return (size_t)(nb / 32 + 3); }

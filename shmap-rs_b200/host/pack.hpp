@@ -8,10 +8,13 @@ namespace shm {
 // Packs nb bytes; codes needs packed_code_words(nb) words, mask
 // packed_mask_words(nb) (the spare words past the end hold code 0, masked).
 void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask);
-// The same on the host threads in the background: start returns at once,
-// wait returns when the packing is complete (one packing at a time).
-void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask);
-void pack_reads_host_wait();
+// The same on the host threads in the background with the mask in sparse
+// form: start returns at once; wait returns when the packing is complete,
+// writing the nonzero mask words as (word index, word) pairs, at most cap of
+// them (never more than packed_mask_words(nb)), and returns their number.
+// One packing at a time.
+void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes);
+size_t pack_reads_host_wait(uint32_t* pairs, size_t cap);
 size_t packed_code_words(int64_t nb);
 size_t packed_mask_words(int64_t nb);
 
