@@ -2041,10 +2041,17 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
 }
 
 // ------------------------------------------------------------------ host side
+// A host<->device copy on stream s, counted in the context's work counters.
+static void copy_async(MapCtx* c, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+    SHM_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s));
+    if (kind == cudaMemcpyHostToDevice) c->work[W_H2D_BYTES] += (int64_t)bytes;
+    else if (kind == cudaMemcpyDeviceToHost) c->work[W_D2H_BYTES] += (int64_t)bytes;
+}
+
 const char* const STAGE_NAMES[N_STAGES] = {"sketch", "seedprep", "contrib", "bscan", "extend", "refine", "sweep", "aux"};
 const char* const WORK_NAMES[N_WORK] = {"reads", "bases", "kmers", "distinct_seeds", "processed_seeds",
                                         "seed_hits", "buckets", "bucket_jobs", "extension_seeds", "candidates",
-                                        "refine_kmers"};
+                                        "refine_kmers", "h2d_bytes", "d2h_bytes"};
 
 // Event pairs around each stage of a batch, read back once the batch is done.
 // Host-side phase clock, printed per batch when SHMAP_HOSTPROF is set.
@@ -2379,7 +2386,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     const uint64_t kcap = bp.kcap_off[(size_t)n], phtn = bp.pht_off[(size_t)n];
     // the plan goes up in one copy from its own pinned block
     S.plan.reserve(bp.bytes);
-    SHM_CUDA(cudaMemcpyAsync(S.plan.p, h_plan, bp.bytes, cudaMemcpyHostToDevice, s));
+    copy_async(c, S.plan.p, h_plan, bp.bytes, cudaMemcpyHostToDevice, s);
     BatchPlan dp;
     dp.carve(S.plan.p, n);
     S.kcnt.reserve((size_t)n);
@@ -2573,9 +2580,9 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     uint64_t bt_slots_alloc;
     uint32_t job_cap, m_max, nu_max, half_max;
     if (exact || debug) {
-        SHM_CUDA(cudaMemcpyAsync(&R.totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        SHM_CUDA(cudaMemcpyAsync(&R.totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        SHM_CUDA(cudaMemcpyAsync(&R.hm, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
+        copy_async(c, &R.totals[0], S.hw_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+        copy_async(c, &R.totals[1], S.bt_off.p + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+        copy_async(c, &R.hm, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s);
         H.mark("enq1");
         SHM_CUDA(cudaStreamSynchronize(s));
         H.mark("sync1");
@@ -2687,10 +2694,10 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     SHM_CUDA(cudaGetLastError());
     T.end();
 
-    SHM_CUDA(cudaMemcpyAsync(&R.fin, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s));
-    SHM_CUDA(cudaMemcpyAsync(&R.nj, S.n_jobs.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    SHM_CUDA(cudaMemcpyAsync(&R.nc, S.coff.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    SHM_CUDA(cudaMemcpyAsync(sl.ovf, S.ovf_list.p, 2 * sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    copy_async(c, &R.fin, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s);
+    copy_async(c, &R.nj, S.n_jobs.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    copy_async(c, &R.nc, S.coff.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    copy_async(c, sl.ovf, S.ovf_list.p, 2 * sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s);
     H.mark("enq_rest");
     if (debug) {
         SHM_CUDA(cudaStreamSynchronize(s));
@@ -2779,7 +2786,7 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
             lst[3 * (size_t)i + 2] = o[(size_t)i + 1] - o[(size_t)i];
         }
         S.retry_list.reserve(3 * (size_t)n);
-        SHM_CUDA(cudaMemcpyAsync(S.retry_list.p, lst, 24 * (size_t)n, cudaMemcpyHostToDevice, s));
+        copy_async(c, S.retry_list.p, lst, 24 * (size_t)n, cudaMemcpyHostToDevice, s);
         k_gather_reads<<<(unsigned)std::min<int32_t>(n, 1184), 256, 0, s>>>(io.d_seq, S.retry_list.p, n,
                                                                            S.retry_seq.p);
         SHM_CUDA(cudaGetLastError());
@@ -2787,7 +2794,7 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
     } else {  // host reads: gathered into pinned memory, one copy
         for (int32_t i = 0; i < n; i++)
             std::memcpy(pin + o[(size_t)i], io.h_seq + offs[ovf[i].read], (size_t)(o[(size_t)i + 1] - o[(size_t)i]));
-        SHM_CUDA(cudaMemcpyAsync(S.retry_seq.p, pin, (size_t)nb, cudaMemcpyHostToDevice, s));
+        copy_async(c, S.retry_seq.p, pin, (size_t)nb, cudaMemcpyHostToDevice, s);
     }
     S.retry_out.reserve((size_t)n);
     StageTimer T(c);
@@ -2811,14 +2818,14 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
         int32_t* h_idx = (int32_t*)(pin + idx_at);
         for (int32_t i = 0; i < n; i++) h_idx[i] = ovf[i].read;
         S.retry_idx.reserve((size_t)n);
-        SHM_CUDA(cudaMemcpyAsync(S.retry_idx.p, h_idx, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, s));
+        copy_async(c, S.retry_idx.p, h_idx, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, s);
         k_scatter_records<<<grid_for((size_t)n, 256), 256, 0, s>>>(S.retry_out.p, S.retry_idx.p, n, io.d_out);
         SHM_CUDA(cudaGetLastError());
         count_launch();
         SHM_CUDA(cudaStreamSynchronize(s));
     } else {  // records to their slots on the host, through pinned memory
         shm_map_record* h_rec = (shm_map_record*)pinned_stage(c, sizeof(shm_map_record) * (size_t)n);
-        SHM_CUDA(cudaMemcpyAsync(h_rec, S.retry_out.p, sizeof(shm_map_record) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        copy_async(c, h_rec, S.retry_out.p, sizeof(shm_map_record) * (size_t)n, cudaMemcpyDeviceToHost, s);
         SHM_CUDA(cudaStreamSynchronize(s));
         for (int32_t i = 0; i < n; i++) io.h_out[ovf[i].read] = h_rec[i];
     }
@@ -2949,11 +2956,11 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         const int64_t nb = offs[j] - offs[i];
         cudaStream_t cs = c->copy_stream;
         SHM_CUDA(cudaStreamWaitEvent(cs, c->sketched[b & 1], 0));
-        SHM_CUDA(cudaMemcpyAsync(S.pk_codes[b & 1].p, h_codes(b), 4 * packed_code_words(nb), cudaMemcpyHostToDevice,
-                                 cs));
+        copy_async(c, S.pk_codes[b & 1].p, h_codes(b), 4 * packed_code_words(nb), cudaMemcpyHostToDevice,
+                                 cs);
         SHM_CUDA(cudaMemsetAsync(S.pk_mask[b & 1].p, 0, 4 * packed_mask_words(nb), cs));
         if (n_list) {  // the nonzero mask words into the zeroed mask
-            SHM_CUDA(cudaMemcpyAsync(S.pk_list[b & 1].p, h_list(b), 8 * n_list, cudaMemcpyHostToDevice, cs));
+            copy_async(c, S.pk_list[b & 1].p, h_list(b), 8 * n_list, cudaMemcpyHostToDevice, cs);
             k_mask_scatter<<<grid_for(n_list, 256, 4), 256, 0, cs>>>(S.pk_list[b & 1].p, (uint32_t)n_list,
                                                                     S.pk_mask[b & 1].p);
             SHM_CUDA(cudaGetLastError());
@@ -2980,8 +2987,8 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         run_batch(c, ix, p, nullptr, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b],
                   S.pk_codes[b & 1].p, S.pk_mask[b & 1].p);
         c->sketch_done = nullptr;
-        SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
-                                 s));
+        copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
+                                 s);
         if (b + 1 < batches.size()) {
             wait(b + 1);
             send(b + 1);
@@ -2998,10 +3005,10 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         const int64_t nb = offs[j] - offs[i];
         S.seqb[0].reserve((size_t)nb + 32);
         SHM_CUDA(cudaMemsetAsync(S.seqb[0].p + nb, 0, 32, s));
-        SHM_CUDA(cudaMemcpyAsync(S.seqb[0].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, s));
+        copy_async(c, S.seqb[0].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, s);
         run_batch(c, ix, p, S.seqb[0].p, offs + i, j - i, S.out.p, nullptr, true, plans[b], T, slots[b]);
-        SHM_CUDA(cudaMemcpyAsync(out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
-                                 s));
+        copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
+                                 s);
         SHM_CUDA(cudaStreamSynchronize(s));
     }
     T.collect();

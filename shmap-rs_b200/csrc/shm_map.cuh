@@ -36,9 +36,10 @@ enum Stage { STG_SKETCH, STG_SEEDPREP, STG_CONTRIB, STG_BSCAN, STG_EXTEND, STG_R
 extern const char* const STAGE_NAMES[N_STAGES];
 
 // Work done, accumulated over every batch of a context: the units the
-// roofline's algorithmic bytes are counted in.
+// roofline's algorithmic bytes are counted in, and the bytes copied between
+// host and device.
 enum Work { W_READS, W_BASES, W_KMERS, W_DISTINCT, W_PROC_SEEDS, W_HITS, W_BUCKETS, W_JOBS, W_EXT_SEEDS, W_CANDS,
-            W_REFINE_KMERS, N_WORK };
+            W_REFINE_KMERS, W_H2D_BYTES, W_D2H_BYTES, N_WORK };
 extern const char* const WORK_NAMES[N_WORK];
 
 struct MapCtx {
