@@ -2846,14 +2846,19 @@ __global__ void k_mask_scatter(const uint32_t* __restrict__ pairs, uint32_t n, u
 // in the plain form).
 static std::vector<std::pair<int32_t, int32_t>> cut_batches(const int64_t* offs, int32_t n, bool plain,
                                                             int32_t max_reads, int64_t max_bases,
-                                                            int32_t first_max_reads = 0) {
+                                                            int32_t first_max_reads = 0, bool taper = false) {
     std::vector<std::pair<int32_t, int32_t>> b;
     int32_t i = 0;
+    int64_t lim_b = max_bases;
     while (i < n) {
         int32_t j = i + 1;
         const int32_t lim = (i == 0 && first_max_reads > 0) ? first_max_reads : max_reads;
+        // taper: the rest, once it fits one batch, in about four (the last
+        // batch's upload and mapping are what nothing overlaps)
+        if (taper && lim_b == max_bases && offs[n] - offs[i] <= max_bases)
+            lim_b = std::max<int64_t>((offs[n] - offs[i]) / 4 + 1, (int64_t)1 << 24);
         if (!plain)
-            while (j < n && j - i < lim && offs[j + 1] - offs[i] <= max_bases) j++;
+            while (j < n && j - i < lim && offs[j + 1] - offs[i] <= lim_b) j++;
         b.emplace_back(i, j);
         i = j;
     }
@@ -2915,7 +2920,8 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     SHM_CUDA(cudaSetDevice(c->device));
     MapScratch& S = *c->scr;
     cudaStream_t s = c->stream;
-    const auto batches = cut_batches(offs, n, plain, HOST_BATCH_READS, HOST_BATCH_BASES, HOST_FIRST_BATCH_READS);
+    const auto batches =
+        cut_batches(offs, n, plain, HOST_BATCH_READS, HOST_BATCH_BASES, HOST_FIRST_BATCH_READS, true);
     int64_t max_nb = 0;
     int32_t max_n = 0;
     for (auto [i, j] : batches) {

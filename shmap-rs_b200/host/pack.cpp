@@ -137,6 +137,16 @@ class Pool {
         work(job_);
         finish();
     }
+    // finish(), the caller taking tasks of the job in flight first
+    void help_finish() {
+        bool have;
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            have = cur_ != nullptr;
+        }
+        if (have) work(job_);
+        finish();
+    }
     int size() const { return (int)th_.size() + 1; }
 
   private:
@@ -253,7 +263,7 @@ void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes) {
 }
 
 size_t pack_reads_host_wait(uint32_t* pairs, size_t cap) {
-    pool().finish();
+    pool().help_finish();  // the caller packs too while it waits
     size_t n = 0;
     for (int t = 0; t <= g_sparse_tasks; t++)
         for (const auto& e : task_lists()[t]) {
