@@ -191,6 +191,21 @@ def run_ours(args, rank, world, local):
     index_s = time.time() - t0
     st = idx.stats()
     log(f"[bench] rank {rank}: index on device in {index_s:.2f}s: {st}")
+    index_file = None
+    if rank == 0:  # the index written to a file and read back (shm_index_save / shm_index_load)
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "ref.shmapidx")
+            t0 = time.time()
+            idx.save(path)
+            save_s = time.time() - t0
+            t0 = time.time()
+            back = sb.SketchIndex.load(ctx, path)
+            torch.cuda.synchronize()
+            load_s = time.time() - t0
+            if back.stats() != st:
+                raise RuntimeError("the index read back differs from the one built")
+            index_file = {"bytes": os.path.getsize(path), "save_s": round(save_s, 3), "load_s": round(load_s, 3)}
+            back.close()
     p = sb.Params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=wk["metric"])
     n = len(names)
     nbytes = int(offs[-1])
@@ -320,6 +335,7 @@ def run_ours(args, rank, world, local):
             "mbp_per_s": round(mbp, 1),
             "mapped_fraction": round(mapped, 4),
             "index_build_s": round(index_s, 3),
+            "index_file": index_file,
             "index": st,
             "stages_ms": {k: round(v[0] / args.steps, 3) for k, v in stages.items()},
             "work_per_step": {k: v // max(1, args.steps) for k, v in work.items()},

@@ -110,6 +110,19 @@ int shm_index_build(shm_ctx* ctx, const uint8_t* seq, const int64_t* seg_off, in
 int shm_index_destroy(shm_index* idx);
 int shm_index_stats_get(const shm_index* idx, shm_index_stats* out);
 
+/* No counterpart in the reference, which sketches and indexes the reference on
+ * every run (src/main.rs:45-57): a built index written to a file, and read
+ * back onto the device of ctx, so that a service starts mapping without the
+ * reference's sequence or a rebuild. The file holds the segments, every
+ * reference k-mer and the hash CSR (about 20 bytes per reference k-mer plus
+ * the names); the derived tables are rebuilt on load. Load answers
+ * SHM_ERR_INVALID, with a message, for a file that is missing, of another
+ * kind or version, or truncated. shm_index_info gives the k, hash ratio and
+ * -M (-1 = none) the index was built with. */
+int shm_index_save(const shm_index* idx, const char* path);
+int shm_index_load(shm_ctx* ctx, const char* path, shm_index** out);
+int shm_index_info(const shm_index* idx, int32_t* k, double* h_frac, int32_t* max_matches);
+
 /* SketchIndex::count (src/index.rs:204-213) for n hashes. */
 int shm_index_count(shm_ctx* ctx, const shm_index* idx, const uint64_t* h, int64_t n, int32_t* out);
 

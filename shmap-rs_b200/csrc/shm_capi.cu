@@ -258,6 +258,45 @@ int shm_index_destroy(shm_index* idx) {
     return SHM_OK;
 }
 
+int shm_index_save(const shm_index* idx, const char* path) {
+    if (!idx || !path) return fail(SHM_ERR_INVALID, "null argument");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(idx->s->device));
+    try {
+        shm::save_index(idx->s, path);
+    } catch (const shm::IndexFileError& e) {
+        return fail(SHM_ERR_INVALID, e.what);
+    }
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_index_load(shm_ctx* ctx, const char* path, shm_index** out) {
+    if (!ctx || !path || !out) return fail(SHM_ERR_INVALID, "null argument");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(ctx->m->device));
+    shm::IndexStorage* s = nullptr;
+    try {
+        s = shm::load_index(path, ctx->m->stream);
+    } catch (const shm::IndexFileError& e) {
+        return fail(SHM_ERR_INVALID, e.what);
+    }
+    ctx->m->launches += 8;
+    auto* ix = new shm_index();
+    ix->s = s;
+    *out = ix;
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_index_info(const shm_index* idx, int32_t* k, double* h_frac, int32_t* max_matches) {
+    if (!idx) return fail(SHM_ERR_INVALID, "null argument");
+    if (k) *k = idx->s->k;
+    if (h_frac) *h_frac = idx->s->h_frac;
+    if (max_matches) *max_matches = idx->s->max_matches;
+    return SHM_OK;
+}
+
 int shm_index_stats_get(const shm_index* idx, shm_index_stats* out) {
     if (!idx || !out) return fail(SHM_ERR_INVALID, "null argument");
     *out = idx->s->stats;

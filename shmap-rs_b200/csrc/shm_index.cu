@@ -174,6 +174,69 @@ __global__ void k_btab_fill(const uint64_t* __restrict__ keys, const uint32_t* _
     }
 }
 
+// The arrays derived from the reference k-mers and the CSR (forward-strand
+// prefix of the hits, hash directory, bucket table) and the device view;
+// build_index and load_index end here. ix holds k, the segments, ref_h,
+// ref_rs, keys[n_kept], key_off[n_kept+1] and hits[n_hits] on the device.
+static void finish_index(IndexStorage* ix, uint64_t thr, uint32_t n_kept, uint32_t n_kmers, uint32_t n_hits,
+                         uint32_t highest, cudaStream_t s) {
+    DevBuf<uint32_t> flag;
+    flag.reserve((size_t)n_hits + 1);
+    ix->hit_fw.reserve((size_t)n_hits + 1);
+    k_fw_flags<<<grid_for(n_hits, 256), 256, 0, s>>>(ix->hits.p, n_hits, ix->ref_rs.p, flag.p);
+    SHM_CUDA(cudaGetLastError());
+    exclusive_scan_u32(flag.p, ix->hit_fw.p, n_hits, s);
+    int bits = 1;
+    while (bits < 30 && (1u << bits) < n_kept) bits++;
+    const int64_t nb = (int64_t)1 << bits;
+    // mul = floor(2^64 * nb / (thr + 1)): h <= thr maps monotonically onto [0, nb)
+    unsigned __int128 m128 = ((unsigned __int128)nb << 64) / ((unsigned __int128)thr + 1);
+    const uint64_t mul = m128 > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)m128;
+    ix->dir.reserve((size_t)nb + 1);
+    k_dir_fill<<<grid_for((size_t)std::max<int64_t>(nb, (int64_t)n_kept), 256), 256, 0, s>>>(ix->keys.p, n_kept,
+                                                                                           ix->dir.p, nb, mul);
+    SHM_CUDA(cudaGetLastError());
+    // the bucket table: two buckets per key (at most 2^28), when no hash is
+    // all ones (thr below the maximum) and every count fits in 31 bits
+    int tbits = 0;
+    uint64_t tmul = 0;
+    if (thr != UINT64_MAX && n_kept > 0 && highest < (1u << 31)) {
+        tbits = std::min(bits + 1, 28);
+        const int64_t nt = (int64_t)1 << tbits;
+        unsigned __int128 t128 = ((unsigned __int128)nt << 64) / ((unsigned __int128)thr + 1);
+        tmul = t128 > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)t128;
+        ix->btab.reserve(2 * (size_t)nt);
+        k_btab_clear<<<grid_for((size_t)nt, 256), 256, 0, s>>>(ix->btab.p, nt);
+        SHM_CUDA(cudaGetLastError());
+        k_btab_fill<<<grid_for((size_t)n_kept, 256), 256, 0, s>>>(ix->keys.p, ix->key_off.p, n_kept, ix->btab.p,
+                                                                 tmul);
+        SHM_CUDA(cudaGetLastError());
+    }
+    SHM_CUDA(cudaStreamSynchronize(s));
+
+    DevIndex& d = ix->dev;
+    d.k = ix->k;
+    d.n_seg = (int32_t)ix->seg_len.size();
+    d.thr = thr;
+    d.seg_off = ix->seg_off.p;
+    d.seg_sz = ix->seg_sz.p;
+    d.ref_h = ix->ref_h.p;
+    d.ref_rs = ix->ref_rs.p;
+    d.keys = ix->keys.p;
+    d.key_off = ix->key_off.p;
+    d.hits = ix->hits.p;
+    d.hit_fw = ix->hit_fw.p;
+    d.dir = ix->dir.p;
+    d.dir_bits = bits;
+    d.dir_mul = mul;
+    d.btab = tbits ? ix->btab.p : nullptr;
+    d.btab_bits = tbits;
+    d.btab_mul = tmul;
+    d.n_keys = n_kept;
+    d.n_kmers = n_kmers;
+    d.n_hits = n_hits;
+}
+
 IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_t n_seg,
                           const std::vector<std::string>& names, int32_t k, double h_frac, int32_t max_matches,
                           cudaStream_t s) {
@@ -317,60 +380,8 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
                                                         hits_scan.p, ix->hits.p);
         SHM_CUDA(cudaGetLastError());
 
-        // 4. forward-strand prefix and the hash directory
-        ix->hit_fw.reserve((size_t)n_hits + 1);
-        k_fw_flags<<<grid_for(n_hits, 256), 256, 0, s>>>(ix->hits.p, n_hits, ix->ref_rs.p, flag.p);
-        SHM_CUDA(cudaGetLastError());
-        exclusive_scan_u32(flag.p, ix->hit_fw.p, n_hits, s);
-        int bits = 1;
-        while (bits < 30 && (1u << bits) < n_kept) bits++;
-        const int64_t nb = (int64_t)1 << bits;
-        // mul = floor(2^64 * nb / (thr + 1)): h <= thr maps monotonically onto [0, nb)
-        unsigned __int128 m128 = ((unsigned __int128)nb << 64) / ((unsigned __int128)thr + 1);
-        const uint64_t mul = m128 > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)m128;
-        ix->dir.reserve((size_t)nb + 1);
-        k_dir_fill<<<grid_for((size_t)std::max<int64_t>(nb, (int64_t)n_kept), 256), 256, 0, s>>>(ix->keys.p, n_kept,
-                                                                                               ix->dir.p, nb, mul);
-        SHM_CUDA(cudaGetLastError());
-        // the bucket table: two buckets per key (at most 2^28), when no hash is
-        // all ones (thr below the maximum) and every count fits in 31 bits
-        int tbits = 0;
-        uint64_t tmul = 0;
-        if (thr != UINT64_MAX && n_kept > 0 && hst.highest < (1LL << 31)) {
-            tbits = std::min(bits + 1, 28);
-            const int64_t nt = (int64_t)1 << tbits;
-            unsigned __int128 t128 = ((unsigned __int128)nt << 64) / ((unsigned __int128)thr + 1);
-            tmul = t128 > (unsigned __int128)UINT64_MAX ? UINT64_MAX : (uint64_t)t128;
-            ix->btab.reserve(2 * (size_t)nt);
-            k_btab_clear<<<grid_for((size_t)nt, 256), 256, 0, s>>>(ix->btab.p, nt);
-            SHM_CUDA(cudaGetLastError());
-            k_btab_fill<<<grid_for((size_t)n_kept, 256), 256, 0, s>>>(ix->keys.p, ix->key_off.p, n_kept, ix->btab.p,
-                                                                     tmul);
-            SHM_CUDA(cudaGetLastError());
-        }
-        SHM_CUDA(cudaStreamSynchronize(s));
-
-        DevIndex& d = ix->dev;
-        d.k = k;
-        d.n_seg = n_seg;
-        d.thr = thr;
-        d.seg_off = ix->seg_off.p;
-        d.seg_sz = ix->seg_sz.p;
-        d.ref_h = ix->ref_h.p;
-        d.ref_rs = ix->ref_rs.p;
-        d.keys = ix->keys.p;
-        d.key_off = ix->key_off.p;
-        d.hits = ix->hits.p;
-        d.hit_fw = ix->hit_fw.p;
-        d.dir = ix->dir.p;
-        d.dir_bits = bits;
-        d.dir_mul = mul;
-        d.btab = tbits ? ix->btab.p : nullptr;
-        d.btab_bits = tbits;
-        d.btab_mul = tmul;
-        d.n_keys = n_kept;
-        d.n_kmers = n_kmers;
-        d.n_hits = n_hits;
+        // 4. forward-strand prefix, hash directory, bucket table, device view
+        finish_index(ix, thr, n_kept, n_kmers, n_hits, hst.highest, s);
 
         shm_index_stats& st = ix->stats;
         st.segments = n_seg;
@@ -383,6 +394,166 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
         st.sketched_kmers = n_kmers;
         return ix;
     } catch (...) {
+        delete ix;
+        throw;
+    }
+}
+
+// ------------------------------------------------------------------ index files
+// A built index written to a file and read back, so that a service can start
+// mapping without the reference's sequence and without rebuilding (the
+// reference itself sketches and indexes on every run, src/main.rs:45-57).
+// The file holds what the index answers from: the segments, every reference
+// k-mer and the CSR over distinct hashes; the derived arrays (forward-strand
+// prefix, directory, bucket table) are rebuilt on load by finish_index.
+// Layout, little endian, no padding:
+//   "SHMAPIX1", u32 version = 1, i32 k, f64 h_frac, i32 max_matches,
+//   i32 n_seg, u32 n_keys, u32 n_kmers, u32 n_hits, shm_index_stats (8 i64);
+//   per segment: u32 name length, the name's bytes, i32 length in bases;
+//   u32 seg_off[n_seg+1], u64 ref_h[n_kmers], u32 ref_rs[n_kmers],
+//   u64 keys[n_keys], u32 key_off[n_keys+1], u32 hits[n_hits];
+//   u64 total byte count of everything before it (a truncation check).
+static const char IDX_MAGIC[8] = {'S', 'H', 'M', 'A', 'P', 'I', 'X', '1'};
+static const uint32_t IDX_VERSION = 1;
+
+namespace {
+struct FileW {
+    std::FILE* f;
+    uint64_t n = 0;
+    void put(const void* p, size_t bytes) {
+        if (bytes && std::fwrite(p, 1, bytes, f) != bytes) throw IndexFileError{"write failed"};
+        n += bytes;
+    }
+    template <class T>
+    void val(const T& v) {
+        put(&v, sizeof v);
+    }
+    template <class T>
+    void dev(const T* d, size_t count) {  // a device array, in slices through host memory
+        std::vector<T> h(std::min<size_t>(count, (size_t)1 << 24));
+        for (size_t i = 0; i < count; i += h.size()) {
+            const size_t c = std::min(h.size(), count - i);
+            SHM_CUDA(cudaMemcpy(h.data(), d + i, sizeof(T) * c, cudaMemcpyDeviceToHost));
+            put(h.data(), sizeof(T) * c);
+        }
+    }
+};
+struct FileR {
+    std::FILE* f;
+    uint64_t n = 0;
+    void get(void* p, size_t bytes) {
+        if (bytes && std::fread(p, 1, bytes, f) != bytes) throw IndexFileError{"truncated or unreadable index file"};
+        n += bytes;
+    }
+    template <class T>
+    T val() {
+        T v;
+        get(&v, sizeof v);
+        return v;
+    }
+    template <class T>
+    void dev(DevBuf<T>& d, size_t count, size_t reserve) {  // into a device buffer, in slices
+        d.reserve(reserve);
+        std::vector<T> h(std::min<size_t>(std::max<size_t>(count, 1), (size_t)1 << 24));
+        for (size_t i = 0; i < count; i += h.size()) {
+            const size_t c = std::min(h.size(), count - i);
+            get(h.data(), sizeof(T) * c);
+            SHM_CUDA(cudaMemcpy(d.p + i, h.data(), sizeof(T) * c, cudaMemcpyHostToDevice));
+        }
+    }
+};
+}  // namespace
+
+void save_index(const IndexStorage* ix, const char* path) {
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) throw IndexFileError{std::string("cannot open for writing: ") + path};
+    FileW w{f};
+    try {
+        const DevIndex& d = ix->dev;
+        const int32_t n_seg = (int32_t)ix->seg_len.size();
+        w.put(IDX_MAGIC, 8);
+        w.val(IDX_VERSION);
+        w.val((int32_t)ix->k);
+        w.val(ix->h_frac);
+        w.val((int32_t)ix->max_matches);
+        w.val(n_seg);
+        w.val(d.n_keys);
+        w.val(d.n_kmers);
+        w.val(d.n_hits);
+        w.val(ix->stats);
+        for (int32_t i = 0; i < n_seg; i++) {
+            const std::string& nm = ix->names[(size_t)i];
+            w.val((uint32_t)nm.size());
+            w.put(nm.data(), nm.size());
+            w.val(ix->seg_len[(size_t)i]);
+        }
+        w.put(ix->h_seg_off.data(), sizeof(uint32_t) * ((size_t)n_seg + 1));
+        w.dev(ix->ref_h.p, d.n_kmers);
+        w.dev(ix->ref_rs.p, d.n_kmers);
+        w.dev(ix->keys.p, d.n_keys);
+        w.dev(ix->key_off.p, (size_t)d.n_keys + 1);
+        w.dev(ix->hits.p, d.n_hits);
+        const uint64_t total = w.n;
+        w.val(total);
+    } catch (...) {
+        std::fclose(f);
+        throw;
+    }
+    if (std::fclose(f) != 0) throw IndexFileError{"write failed"};
+}
+
+IndexStorage* load_index(const char* path, cudaStream_t s) {
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) throw IndexFileError{std::string("cannot open index file: ") + path};
+    FileR r{f};
+    auto* ix = new IndexStorage();
+    try {
+        char magic[8];
+        r.get(magic, 8);
+        if (std::memcmp(magic, IDX_MAGIC, 8) != 0) throw IndexFileError{"not a shmap-b200 index file"};
+        if (r.val<uint32_t>() != IDX_VERSION) throw IndexFileError{"unsupported index file version"};
+        SHM_CUDA(cudaGetDevice(&ix->device));
+        ix->k = r.val<int32_t>();
+        ix->h_frac = r.val<double>();
+        ix->max_matches = r.val<int32_t>();
+        const int32_t n_seg = r.val<int32_t>();
+        const uint32_t n_keys = r.val<uint32_t>(), n_kmers = r.val<uint32_t>(), n_hits = r.val<uint32_t>();
+        if (ix->k <= 0 || !(ix->h_frac > 0.0) || ix->h_frac > 1.0 || n_seg < 0 || n_keys > n_kmers ||
+            n_hits > n_kmers)
+            throw IndexFileError{"corrupt index file header"};
+        ix->stats = r.val<shm_index_stats>();
+        for (int32_t i = 0; i < n_seg; i++) {
+            const uint32_t len = r.val<uint32_t>();
+            if (len > (1u << 20)) throw IndexFileError{"corrupt index file (segment name)"};
+            std::string nm(len, '\0');
+            r.get(&nm[0], len);
+            ix->names.push_back(std::move(nm));
+            ix->seg_len.push_back(r.val<int32_t>());
+        }
+        ix->h_seg_off.resize((size_t)n_seg + 1);
+        r.get(ix->h_seg_off.data(), sizeof(uint32_t) * ((size_t)n_seg + 1));
+        if (ix->h_seg_off[0] != 0 || ix->h_seg_off[(size_t)n_seg] != n_kmers)
+            throw IndexFileError{"corrupt index file (segment offsets)"};
+        ix->seg_off.reserve((size_t)n_seg + 1);
+        SHM_CUDA(cudaMemcpy(ix->seg_off.p, ix->h_seg_off.data(), sizeof(uint32_t) * ((size_t)n_seg + 1),
+                            cudaMemcpyHostToDevice));
+        ix->seg_sz.reserve((size_t)n_seg + 1);
+        if (n_seg)
+            SHM_CUDA(cudaMemcpy(ix->seg_sz.p, ix->seg_len.data(), sizeof(int32_t) * (size_t)n_seg,
+                                cudaMemcpyHostToDevice));
+        r.dev(ix->ref_h, n_kmers, (size_t)n_kmers + 1);
+        r.dev(ix->ref_rs, n_kmers, (size_t)n_kmers + 1);
+        r.dev(ix->keys, n_keys, (size_t)n_keys + 1);
+        r.dev(ix->key_off, (size_t)n_keys + 1, (size_t)n_keys + 1);
+        r.dev(ix->hits, n_hits, (size_t)n_hits + 1);
+        const uint64_t expect = r.n;
+        if (r.val<uint64_t>() != expect) throw IndexFileError{"corrupt or truncated index file"};
+        std::fclose(f);
+        f = nullptr;
+        finish_index(ix, h_thres(ix->h_frac), n_keys, n_kmers, n_hits, (uint32_t)ix->stats.highest_freq_kmer, s);
+        return ix;
+    } catch (...) {
+        if (f) std::fclose(f);
         delete ix;
         throw;
     }

@@ -66,6 +66,14 @@ struct IndexStorage {
     int device = 0;
 };
 
+// An index written to a file and read back (shm_index.cu); failures throw
+// IndexFileError with a message.
+struct IndexFileError {
+    std::string what;
+};
+void save_index(const IndexStorage* ix, const char* path);
+IndexStorage* load_index(const char* path, cudaStream_t s);
+
 IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off, int32_t n_seg,
                           const std::vector<std::string>& names, int32_t k, double h_frac, int32_t max_matches,
                           cudaStream_t s);

@@ -86,6 +86,9 @@ def lib() -> ctypes.CDLL:
         "shm_sketch": (ctypes.c_int, [P, P, i64, i32, dbl, i32, P, P, P, i64, P]),
         "shm_index_build": (ctypes.c_int, [P, P, P, i32, ctypes.c_char_p, i32, dbl, i32, P]),
         "shm_index_destroy": (ctypes.c_int, [P]),
+        "shm_index_save": (ctypes.c_int, [P, ctypes.c_char_p]),
+        "shm_index_load": (ctypes.c_int, [P, ctypes.c_char_p, P]),
+        "shm_index_info": (ctypes.c_int, [P, P, P, P]),
         "shm_index_stats_get": (ctypes.c_int, [P, P]),
         "shm_index_count": (ctypes.c_int, [P, P, P, i64, P]),
         "shm_index_hits": (ctypes.c_int, [P, P, u64, P, P, P, P, i64, P]),
@@ -237,6 +240,34 @@ class SketchIndex:
                      max_matches: Optional[int] = None) -> "SketchIndex":
         seq, off = pack([s for _, s in records])
         return cls(ctx, [n for n, _ in records], seq, off, k, h_frac, max_matches)
+
+    def save(self, path: str) -> None:
+        """Writes the index to a file (shm_index_save)."""
+        _check(lib().shm_index_save(self.h, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, ctx: Context, path: str) -> "SketchIndex":
+        """Reads an index written by save onto ctx's device (shm_index_load)."""
+        obj = cls.__new__(cls)
+        obj.ctx = ctx
+        obj.h = None
+        h = ctypes.c_void_p()
+        _check(lib().shm_index_load(ctx.h, os.fsencode(path), ctypes.byref(h)))
+        obj.h = h
+        k, hf, mm = ctypes.c_int32(), ctypes.c_double(), ctypes.c_int32()
+        _check(lib().shm_index_info(h, ctypes.byref(k), ctypes.byref(hf), ctypes.byref(mm)))
+        obj.k, obj.h_frac = k.value, hf.value
+        # the segment names, from the file's header (layout in shm_index.cu)
+        with open(path, "rb") as f:
+            head = f.read(8 + 4 + 4 + 8 + 4 + 4 + 12 + 64)
+            n_seg = int(np.frombuffer(head, np.int32, 1, 28)[0])
+            names = []
+            for _ in range(n_seg):
+                ln = int(np.frombuffer(f.read(4), np.uint32)[0])
+                names.append(f.read(ln).decode())
+                f.read(4)
+        obj.names = names
+        return obj
 
     def close(self) -> None:
         if self.h:
