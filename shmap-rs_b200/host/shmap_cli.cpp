@@ -4,6 +4,9 @@
 // ends and '\r' removed), builds the index on the device, maps the reads in
 // batches and writes PAF to stdout in input order; with -z, unmapped reads go
 // to <z>.unmapped.paf (src/shmap/mod.rs:388-394, src/mapping.rs:82-84).
+// Two options the reference does not have: --index-out FILE writes the built
+// index to FILE; --index-in FILE takes the index from FILE instead of -s, and
+// its k, -r and -M replace those given on the command line.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -92,7 +95,7 @@ std::string join(const std::vector<std::string>& v, size_t a, size_t b) {
 int main(int argc, char** argv) {
     shm_params p;
     shm_params_default(&p);
-    std::string t_file, p_file, z_file;
+    std::string t_file, p_file, z_file, ix_in, ix_out;
     int threads = 1, verbose = 0, device = 0;
     for (int i = 1; i < argc; i++) {
         std::string a = argv[i];
@@ -117,6 +120,10 @@ int main(int argc, char** argv) {
         else if (a == "-B" || a == "--one_sweep") p.one_sweep = 1;
         else if (a == "-F" || a == "--abs_pos") p.abs_pos = 1;
         else if (a == "--device") device = std::atoi(val().c_str());
+        // index files (not flags of the reference): write the built index, or
+        // start from one instead of -s (its k, -r and -M then apply)
+        else if (a == "--index-out") ix_out = val();
+        else if (a == "--index-in") ix_in = val();
         else if (a == "-m" || a == "--metric") {
             std::string m = val();
             if (m == "Containment") p.metric = SHM_CONTAINMENT;
@@ -126,22 +133,34 @@ int main(int argc, char** argv) {
             else die("invalid value '" + m + "' for '--metric <METRIC>'");
         } else die("unexpected argument '" + a + "'");
     }
-    if (t_file.empty() || p_file.empty()) die("the following required arguments were not provided: --pattern, --text");
+    if ((t_file.empty() && ix_in.empty()) || p_file.empty()) {
+        std::string miss = p_file.empty() ? "--pattern" : "";
+        if (t_file.empty() && ix_in.empty()) miss += std::string(miss.empty() ? "" : ", ") + "--text";
+        die("the following required arguments were not provided: " + miss);
+    }
     if (shm_params_validate(&p) != SHM_OK) die(shm_last_error());
     if (threads <= 0) die("The number of threads (-@) should be positive. You provided " + std::to_string(threads) + ".");
     if (verbose < 0 || verbose > 2) die("--verbose (-v) should be 0, 1, or 2.");
 
     Records ref, reads;
     std::string err;
-    if (!read_fastx(t_file, ref, err)) die(err);
+    if (ix_in.empty() && !read_fastx(t_file, ref, err)) die(err);
     if (!read_fastx(p_file, reads, err)) die(err);
     shm_ctx* ctx = nullptr;
     if (shm_ctx_create(device, 0, &ctx) != SHM_OK) die(std::string("CUDA: ") + shm_last_error());
     shm_index* idx = nullptr;
-    std::string rnames = join(ref.names, 0, ref.names.size());
-    if (shm_index_build(ctx, (const uint8_t*)ref.seq.data(), ref.off.data(), (int32_t)ref.names.size(), rnames.c_str(),
-                        p.k, p.h_frac, p.max_matches, &idx) != SHM_OK)
-        die(std::string("failed to build index from ") + t_file + ": " + shm_last_error());
+    if (!ix_in.empty()) {
+        if (shm_index_load(ctx, ix_in.c_str(), &idx) != SHM_OK)
+            die(std::string("failed to load index from ") + ix_in + ": " + shm_last_error());
+        shm_index_info(idx, &p.k, &p.h_frac, &p.max_matches);
+    } else {
+        std::string rnames = join(ref.names, 0, ref.names.size());
+        if (shm_index_build(ctx, (const uint8_t*)ref.seq.data(), ref.off.data(), (int32_t)ref.names.size(),
+                            rnames.c_str(), p.k, p.h_frac, p.max_matches, &idx) != SHM_OK)
+            die(std::string("failed to build index from ") + t_file + ": " + shm_last_error());
+    }
+    if (!ix_out.empty() && shm_index_save(idx, ix_out.c_str()) != SHM_OK)
+        die(std::string("failed to write index to ") + ix_out + ": " + shm_last_error());
 
     FILE* unm = nullptr;
     if (!z_file.empty()) {
