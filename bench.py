@@ -136,10 +136,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def make_workload(name: str, rank: int, scale: float):
+def make_workload(name: str, rank: int, scale: float, metric_override: str | None = None):
     from shmap_b200 import synth
 
     rp, qp, k, r, theta, metric, desc = WORKLOADS[name]
+    if metric_override and metric_override != metric:
+        desc = f"{desc}; -m {metric_override} in place of {metric}"
+        metric = metric_override
     rspec = synth.REFS[rp]
     qspec = synth.READS[qp]
     if scale != 1.0:
@@ -183,7 +186,7 @@ def run_ours(args, rank, world, local):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    gen, names, seq, offs, wk = make_workload(args.workload, rank, args.scale)
+    gen, names, seq, offs, wk = make_workload(args.workload, rank, args.scale, args.metric)
     ctx = sb.Context(local)
     t0 = time.time()
     idx = sb.SketchIndex(ctx, gen.names, gen.seq, gen.seg_off, wk["k"], wk["r"])
@@ -389,6 +392,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="hifi")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests and profiling)")
+    ap.add_argument("--metric", choices=["Containment", "Jaccard", "bucket_SH", "bucket_LCS"], default=None,
+                    help="map with this -m instead of the workload's")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size, in seconds of work")
     ap.add_argument("--plain-sample", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -399,7 +404,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        gen, names, seq, offs, wk = make_workload(args.workload, 0, args.scale)
+        gen, names, seq, offs, wk = make_workload(args.workload, 0, args.scale, args.metric)
         per_step = max(2.0, 150.0 / max(1, args.steps + args.warmup))
         rates, sample = cpu_reference(gen, names, seq, offs, wk, per_step, threads, steps=args.warmup + args.steps)
         timed = rates[args.warmup:] or rates

@@ -32,8 +32,8 @@ enum {
     SHM_ERR_TIMEOUT = -5    /* a bounded device wait ran out */
 };
 
-/* Metric (src/types.rs:299-322). bucket_LCS is not on the device path. */
-enum { SHM_CONTAINMENT = 0, SHM_JACCARD = 1, SHM_BUCKET_SH = 2 };
+/* Metric (src/types.rs:299-322). */
+enum { SHM_CONTAINMENT = 0, SHM_JACCARD = 1, SHM_BUCKET_SH = 2, SHM_BUCKET_LCS = 3 };
 
 /* Mapping parameters: the fields of Params (src/params.rs:20-186) that the
  * mapping path reads. Defaults are the CLI defaults (shm_params_default). */

@@ -80,6 +80,18 @@ int64_t orc_sketch(const uint8_t* seq, int64_t len, int32_t k, double h_frac, in
     return (int64_t)v.size();
 }
 
+// bucket_LCS's count over window [bgn, end) of the sketch (t_r, t_h); seed i
+// has hash seed_h[i] and positions pos[pos_off[i] .. pos_off[i + 1]).
+int32_t orc_lcs(const int32_t* t_r, const uint64_t* t_h, int32_t n_t, int32_t bgn, int32_t end, const uint64_t* seed_h,
+                const int32_t* pos_off, const int32_t* pos, int32_t n_seeds) {
+    std::vector<Kmer> t((size_t)n_t);
+    for (int32_t i = 0; i < n_t; i++) t[(size_t)i] = Kmer{t_r[i], t_h[i], false};
+    std::vector<Hash> sh(seed_h, seed_h + n_seeds);
+    std::vector<std::vector<QPos>> sp((size_t)n_seeds);
+    for (int32_t i = 0; i < n_seeds; i++) sp[(size_t)i].assign(pos + pos_off[i], pos + pos_off[i + 1]);
+    return lcs_window(t, bgn, end, sh, sp);
+}
+
 uint64_t orc_h_thres(int32_t k, double h_frac) { return FracMinHash(k, h_frac).h_thres(); }
 
 void* orc_index_build(const uint8_t* seq, const int64_t* seg_off, int32_t n_seg, const char* names_joined,

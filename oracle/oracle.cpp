@@ -776,11 +776,13 @@ Mapping best_fixed_length(Ctx& cx, const RefSegment& segm, RPos from, RPos to, c
     return best;
 }
 
-// src/shmap/scoring.rs:114-170 (bucket_LCS; kept for completeness of the oracle)
-QPos lcs(const std::vector<Kmer>& t, const Buckets& bk, const BucketLoc& b, const PHt& p_ht,
-         const std::vector<Seed>& pu, const std::vector<std::vector<QPos>>& pmatches) {
+// src/shmap/scoring.rs:114-170 (bucket_LCS): the read positions of every
+// window k-mer found in p_ht (each seed's in decreasing order), then the
+// longest strictly increasing subsequence of that list and of its reverse.
+QPos lcs(const std::vector<Kmer>& t, RPos bgn, RPos bucket_end, const PHt& p_ht, const std::vector<Seed>& pu,
+         const std::vector<std::vector<QPos>>& pmatches) {
     std::vector<QPos> pp;
-    RPos bgn = bk.begin(b), end = std::min((RPos)t.size(), bk.end(b));
+    RPos end = std::min((RPos)t.size(), bucket_end);
     for (RPos l = bgn; l < end; l++)
         if (const int32_t* si = p_ht.get(t[(size_t)l].h))
             for (QPos q : pmatches[(size_t)pu[(size_t)*si].seed_num]) pp.push_back(q);
@@ -840,7 +842,7 @@ Mapping find_best_mapping(Ctx& cx, const Buckets& bk, BucketLoc b, const BucketC
         mp.update(0, p_sz - 1, content.r_min, content.r_max, segm, content.matches, sh, content.codirection,
                   content.r_max - content.r_min);
     } else if (metric == Metric::BucketLcs) {
-        QPos c = lcs(segm.kmers, bk, b, rs.p_ht, rs.pu, rs.pmatches);
+        QPos c = lcs(segm.kmers, bk.begin(b), bk.end(b), rs.p_ht, rs.pu, rs.pmatches);
         mp.update(0, p_sz - 1, content.r_min, content.r_max, segm, content.matches, (double)c / (double)m,
                   content.codirection, content.r_max - content.r_min);
     } else {
@@ -897,6 +899,18 @@ bool match_rest(Ctx& cx, QPos p_sz, QPos m, QPos lmax, const Buckets& bk,
 }
 
 }  // namespace
+
+QPos lcs_window(const std::vector<Kmer>& t, RPos bgn, RPos end, const std::vector<Hash>& seed_h,
+                const std::vector<std::vector<QPos>>& seed_pos) {
+    PHt p_ht;
+    std::vector<Seed> pu(seed_h.size());
+    for (size_t i = 0; i < seed_h.size(); i++) {
+        bool ins;
+        p_ht.get_or_insert(seed_h[i], &ins) = (int32_t)i;
+        pu[i].seed_num = (QPos)i;
+    }
+    return lcs(t, bgn, end, p_ht, pu, seed_pos);
+}
 
 // src/shmap/mod.rs:653-971
 ReadResult map_read(const SketchIndex& tidx, const FracMinHash& sk, const Params& p, const uint8_t* seq, size_t len,

@@ -236,4 +236,9 @@ struct FastaRecord {
 };
 bool read_fasta(const std::string& path, std::vector<FastaRecord>& out, std::string* err);
 
+// bucket_LCS's count for the window [bgn, end) of a reference sketch t, with
+// the read's seeds given as hashes and their positions (scoring.rs:114-170).
+QPos lcs_window(const std::vector<Kmer>& t, RPos bgn, RPos end, const std::vector<Hash>& seed_h,
+                const std::vector<std::vector<QPos>>& seed_pos);
+
 }  // namespace oracle

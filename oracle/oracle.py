@@ -54,6 +54,7 @@ def lib():
         for name, res, args in [
             ("orc_sketch", i64, [P, i64, i32, dbl, i32, P, P, P, i64]),
             ("orc_h_thres", u64, [i32, dbl]),
+            ("orc_lcs", i32, [P, P, i32, i32, i32, P, P, P, i32]),
             ("orc_index_build", P, [P, P, i32, ctypes.c_char_p, i32, dbl, i32, i32]),
             ("orc_index_free", None, [P]),
             ("orc_index_stats", None, [P, P]),
@@ -89,6 +90,18 @@ def sketch(seq: bytes, k: int, h_frac: float, offset: int = 0):
     st = np.zeros(cap, np.uint8)
     n = lib().orc_sketch(_p(buf), len(seq), k, h_frac, offset, _p(r), _p(h), _p(st), cap)
     return r[:n], h[:n], st[:n]
+
+
+def lcs(t, bgn: int, end: int, seeds) -> int:
+    """bucket_LCS's count over window [bgn, end) of the sketch t = [(r, h), ...]
+    for a read whose seeds are {hash: [positions, in pmatches order]}."""
+    t_r = np.array([r for r, _ in t], np.int32)
+    t_h = np.array([h for _, h in t], np.uint64)
+    sh = np.array(list(seeds), np.uint64)
+    lens = [len(v) for v in seeds.values()]
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    pos = np.array([x for v in seeds.values() for x in v] + [0], np.int32)
+    return int(lib().orc_lcs(_p(t_r), _p(t_h), len(t), bgn, end, _p(sh), _p(off), _p(pos), len(sh)))
 
 
 def h_thres(h_frac: float, k: int = 15) -> int:

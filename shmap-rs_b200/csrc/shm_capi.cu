@@ -93,8 +93,8 @@ int shm_params_validate(const shm_params* p) {
         return fail(SHM_ERR_INVALID, "The minimum difference (-d) should be >= 0. You provided " + fmt_g(p->min_diff) + ".");
     if (p->max_overlap < 0.0 || p->max_overlap > 1.0)
         return fail(SHM_ERR_INVALID, "The maximum overlap (-o) should be between 0 and 1. You provided " + fmt_g(p->max_overlap) + ".");
-    if (p->metric < SHM_CONTAINMENT || p->metric > SHM_BUCKET_SH)
-        return fail(SHM_ERR_INVALID, "unsupported metric on the device path (bucket_LCS is not implemented)");
+    if (p->metric < SHM_CONTAINMENT || p->metric > SHM_BUCKET_LCS)
+        return fail(SHM_ERR_INVALID, "unknown metric " + std::to_string(p->metric));
     return SHM_OK;
 }
 

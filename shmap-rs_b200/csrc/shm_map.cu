@@ -62,6 +62,7 @@ struct BatchMax {
     unsigned long long kmers, distinct, proc_seeds, hits, buckets, ext_seeds, refine_kmers;
     unsigned int refine_next;  // next candidate chunk k_refine_chip takes
     unsigned int n_far;        // candidates refined by k_refine (listed in cfar)
+    unsigned int lcs_next;     // next candidate k_refine takes under bucket_LCS
 };
 
 // Small device-to-host reads of a batch, landing in pinned memory.
@@ -112,6 +113,7 @@ struct BatchView {
     uint32_t* ovf_list;
     BatchMax* mx;
     shm_map_record* out;
+    uint32_t* lcs_pos;  // bucket_LCS: each seed's read positions, decreasing (at kb + its ooff)
 };
 
 // ------------------------------------------------------------------ helpers
@@ -196,6 +198,13 @@ __device__ void bitonic_u64(uint64_t* A, uint32_t P) {
         }
 }
 
+// Metrics (src/types.rs:299-322). The bucket metrics report a bucket's own
+// content (position range, matches, codirection) rather than a refined
+// window: bucket_SH scores it by its seed heuristic, bucket_LCS by the
+// longest common subsequence of read and window positions.
+constexpr int32_t MET_BUCKET_SH = 2;  // bucket_LCS is 3
+__device__ __forceinline__ bool bucket_metric(const DevParams& P) { return P.metric >= MET_BUCKET_SH; }
+
 // Reads refined on chip (k_refine_chip): Containment or Jaccard without
 // absolute positions, m and the bucket half-length at most RCHIP_M, so that
 // the read's seed table, per-seed state and a window's difference array fit
@@ -204,7 +213,7 @@ __device__ void bitonic_u64(uint64_t* A, uint32_t P) {
 // global table and k_refine.
 constexpr int RCHIP_M = 248;
 __device__ __forceinline__ bool refine_on_chip(const DevParams& P, uint32_t m, int32_t halflen) {
-    return !P.ap && P.metric != 2 && m <= (uint32_t)RCHIP_M && halflen <= RCHIP_M;
+    return !P.ap && !bucket_metric(P) && m <= (uint32_t)RCHIP_M && halflen <= RCHIP_M;
 }
 
 // The sketch hashes are uniform in [0, thr], so their low bits pick the slot.
@@ -379,7 +388,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
     }
     uint32_t po = block_scan_excl<uint32_t>(so, sw32, &t32);
     uint64_t pc = block_scan_excl<uint64_t>(sc, sw64, &t64);
-    const bool pht = v.P.metric != 2;  // bucket_SH refines nothing (these reads are never on chip)
+    const bool pht = v.P.metric != MET_BUCKET_SH;  // bucket_SH looks nothing up (these reads are never on chip)
     if (pht) {  // the read's probe table starts empty
         const uint64_t pb = v.pht_off[q], pe = v.pht_off[q + 1];
         for (uint64_t i = pb + tid; i < pe; i += nt) v.pht_val[i] = 0xffffffffu;
@@ -768,7 +777,7 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
     // seeding prefix: seed i is processed iff sum(occs before i) < S
     // (seeding.rs:101); the processed seeds are a prefix of the order
     const bool chip = refine_on_chip(v.P, m, halflen);
-    const bool pht = !chip && v.P.metric != 2;  // bucket_SH refines nothing
+    const bool pht = !chip && v.P.metric != MET_BUCKET_SH;  // bucket_SH looks nothing up
     if (pht) {  // the read's probe table starts empty (written before the inserts below)
         const uint64_t pb = v.pht_off[q], pe = v.pht_off[q + 1];
         for (uint64_t i = pb + lane; i < pe; i += 32) v.pht_val[i] = 0xffffffffu;
@@ -933,8 +942,8 @@ struct Agg {
 };
 
 // The hits [A, B) of a seed: their count and, when `full`, their
-// codirection and position range (only bucket_SH reports those: every other
-// metric leaves them unread).
+// codirection and position range (only the bucket metrics report those:
+// Containment and Jaccard leave them unread).
 __device__ __forceinline__ Agg range_agg(const DevIndex& I, uint32_t A, uint32_t B, uint32_t seed_strand,
                                          bool full = true) {
     Agg r;
@@ -991,7 +1000,7 @@ __device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t se
         i = (i + 1) & mask;
     }
     atomicAdd(&s->mc, bt_pack(matches, codir));
-    if (v.P.metric == 2) {  // the position range is read by bucket_SH only
+    if (bucket_metric(v.P)) {  // the position range is read by the bucket metrics only
         atomicMin(&s->rmin, rmin);
         atomicMax(&s->rmax, rmax);
     }
@@ -1042,7 +1051,7 @@ __device__ __forceinline__ int32_t seg_step(const DevIndex& I, uint32_t g, int32
 __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
     const uint64_t total = v.hw_off[v.n];
     const bool ap = v.P.ap != 0;
-    const bool sh_out = v.P.metric == 2;  // codirection and positions are reported (bucket_SH)
+    const bool sh_out = bucket_metric(v.P);  // codirection and positions are reported (bucket metrics)
     const DevIndex& I = v.I;
     const uint64_t nrun = (total + CONTRIB_RUN - 1) / CONTRIB_RUN;
     for (uint64_t rn = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; rn < nrun;
@@ -1237,7 +1246,7 @@ __global__ void __launch_bounds__(256) k_extend(BatchView v) {
                 if (cnt > 0) {
                     uint32_t A, B;
                     seed_range(v.I, sr.a, cnt, seg, (int64_t)bb * h, ((int64_t)bb + 2) * h, ap, A, B);
-                    Agg g = range_agg(v.I, A, B, os & 1u, v.P.metric == 2);
+                    Agg g = range_agg(v.I, A, B, os & 1u, bucket_metric(v.P));
                     dm = min(g.count, ds);
                     dc = g.codir;
                     rmn = g.rmin;
@@ -1350,6 +1359,199 @@ __device__ __forceinline__ void pht_lookup_u(const BatchView& v, int32_t q, cons
 
 constexpr int REFINE_WARPS = 8;
 constexpr int REFINE_U = 2;  // position chunks whose seeds are fetched together
+
+// ------------------------------------------------------------------ bucket_LCS
+// Each seed's read positions in decreasing order (its pmatches,
+// src/shmap/seeding.rs:28-56), stored at the seed's occurrence offset:
+// pos[kb + ooff + j] is the j-th largest r among the read's k-mers with the
+// seed's hash. One CTA per read; reads that stopped before their seeds were
+// laid out, or that are mapped again, are skipped.
+__global__ void __launch_bounds__(256) k_lcs_occ(BatchView v, uint32_t* __restrict__ pos, uint32_t* __restrict__ cnt) {
+    for (int32_t q = blockIdx.x; q < v.n; q += gridDim.x) {
+        const int32_t n_u = v.r_nu[q], m = v.r_m[q];
+        if (n_u == 0 || v.r_status[q] == ST_OVERFLOW) continue;  // the same for every thread
+        const uint64_t kb = v.kcap_off[q];
+        for (int32_t i = threadIdx.x; i < n_u; i += blockDim.x) cnt[kb + i] = 0;
+        __syncthreads();
+        for (int32_t j = threadIdx.x; j < m; j += blockDim.x) {
+            const uint64_t h[1] = {v.km_h[kb + j]};
+            const bool on[1] = {true};
+            int32_t sx[1];
+            pht_lookup_u<1>(v, q, h, on, sx);
+            if (sx[0] < 0) continue;  // every sketch hash is a seed's: not taken
+            const uint32_t at = v.sd[kb + sx[0]].ooff + atomicAdd(cnt + kb + sx[0], 1u);
+            pos[kb + at] = v.km_rs[kb + j] >> 1;
+        }
+        __syncthreads();
+        for (int32_t i = threadIdx.x; i < n_u; i += blockDim.x) {  // each seed's positions, decreasing
+            const SeedRec sr = v.sd[kb + i];
+            const uint32_t occ = sr.os >> 1;
+            uint32_t* a = pos + kb + sr.ooff;
+            for (uint32_t x = 1; x < occ; x++) {
+                const uint32_t val = a[x];
+                uint32_t y = x;
+                for (; y > 0 && a[y - 1] < val; y--) a[y] = a[y - 1];
+                a[y] = val;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Places of x in sorted Ti[0, li) and of y in sorted Td[0, ld) (the first
+// index whose value is >= the key), found together: lanes 0-15 search Ti,
+// lanes 16-31 Td. At each level a half's lane 15 compares the range's last
+// value and lanes 0-14 the first values of 15 pieces; the ballot settles the
+// place (past the last value, or at the first) or leaves the rest of the
+// piece after the last first value below the key. A key beyond either end
+// of its range, the common case when read and window are collinear, takes
+// one level.
+__device__ __forceinline__ void half_warp_places(const int32_t* Ti, int32_t li, int32_t x, const int32_t* Td,
+                                                 int32_t ld, int32_t y, int lane, int32_t& pi, int32_t& pd) {
+    const int hf = lane >> 4, hl = lane & 15;
+    const int32_t* T = hf ? Td : Ti;
+    const int32_t key = hf ? y : x;
+    int32_t lo = 0, hi = hf ? ld : li;  // the place lies in [lo, hi]; T[lo, hi) is still unread
+    while (__any_sync(0xffffffffu, lo < hi)) {
+        const bool act = lo < hi;
+        const int32_t step = (hi - lo + 14) / 15;
+        bool below = false;
+        if (act) {
+            if (hl == 15) {
+                below = T[hi - 1] < key;
+            } else {
+                const int32_t st = lo + hl * step;
+                below = st < hi && T[st] < key;
+            }
+        }
+        const unsigned bits = (__ballot_sync(0xffffffffu, below) >> (hf * 16)) & 0xffffu;
+        if (act) {
+            const int32_t nb = __popc(bits & 0x7fffu);
+            if (bits & 0x8000u) {
+                lo = hi;
+            } else if (nb == 0) {
+                hi = lo;
+            } else {  // after piece nb-1's first value, before piece nb's first and the last value
+                const int32_t first = lo + (nb - 1) * step;
+                hi = min(lo + nb * step, hi - 1);
+                lo = first + 1;
+            }
+        }
+    }
+    pi = __shfl_sync(0xffffffffu, lo, 0);
+    pd = __shfl_sync(0xffffffffu, lo, 16);
+}
+
+// First index of sorted T[0, len) whose value is >= x, by one lane.
+__device__ __forceinline__ int32_t lane_lower_bound(const int32_t* T, int32_t len, int32_t x) {
+    int32_t lo = 0;
+    while (len > 0) {
+        const int32_t half = len >> 1;
+        if (T[lo + half] < x) {
+            lo += half + 1;
+            len -= half + 1;
+        } else {
+            len = half;
+        }
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int32_t warp_inclusive_max(int32_t x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    return x;
+}
+
+// bucket_LCS for one candidate (src/shmap/scoring.rs:114-170, 326-344): the
+// read positions of every window k-mer found among the read's seeds, each
+// seed's in decreasing order, are fed in window order to two patience-sorting
+// tail arrays at once, Ti for the longest strictly increasing subsequence of
+// the list and Td (values negated) for that of its reverse, the longest
+// strictly decreasing one. Tails hold distinct read positions: at most m
+// each. The record takes the bucket's own content, as bucket_SH's does.
+//
+// A seed with one read position is placed by half_warp_places. The
+// positions of a seed with several are placed 32 at a time, each lane
+// searching for its own, which gives the sequential result because
+//  * in Ti the group's values decrease, so none can extend a tail another
+//    one of the group set: each value's place is its place among the tails
+//    before the group, places do not increase along the group, and of the
+//    values that share a place the last (smallest) stays;
+//  * in Td the group's values increase, and value t's place is the first
+//    one past value t-1's: p_t = max(q_t, p_(t-1) + 1) with q_t its place
+//    among the tails before it, a running maximum of q_j - j.
+__device__ __forceinline__ void lcs_one(const BatchView& v, BucketJob* J, int32_t q, int32_t* Ti, int32_t* Td,
+                                        int lane) {
+    const DevIndex& I = v.I;
+    const int32_t m = v.r_m[q];
+    const int64_t h = v.r_half[q];
+    const uint64_t kb = v.kcap_off[q];
+    const uint32_t G0 = __ldg(I.seg_off + J->seg), Gend = __ldg(I.seg_off + J->seg + 1);
+    const int64_t from = (int64_t)J->bb * h;
+    const int64_t end = min(((int64_t)J->bb + 2) * h, (int64_t)(Gend - G0));
+    const int32_t W = (int32_t)max(end - from, (int64_t)0);
+    if (lane == 0 && W > 0) atomicAdd(&v.mx->refine_kmers, (unsigned long long)W);
+    int32_t li = 0, ld = 0;
+    for (int32_t c0 = 0; c0 < W; c0 += 32) {
+        const int32_t x = c0 + lane;
+        const bool on[1] = {x < W};
+        const uint64_t hx[1] = {on[0] ? __ldg(I.ref_h + G0 + (uint32_t)(from + x)) : 0};
+        int32_t sx[1];
+        pht_lookup_u<1>(v, q, hx, on, sx);
+        uint32_t occ = 0, ooff = 0;
+        if (sx[0] >= 0) {
+            const SeedRec sr = v.sd[kb + sx[0]];
+            occ = sr.os >> 1;
+            ooff = sr.ooff;
+        }
+        for (unsigned mk = __ballot_sync(0xffffffffu, occ > 0); mk; mk &= mk - 1) {
+            const int src = __ffs(mk) - 1;
+            const uint32_t o = __shfl_sync(0xffffffffu, occ, src), off = __shfl_sync(0xffffffffu, ooff, src);
+            if (o == 1) {
+                const int32_t val = (int32_t)v.lcs_pos[kb + off];
+                int32_t pi, pd;
+                half_warp_places(Ti, li, val, Td, ld, -val, lane, pi, pd);
+                if (lane == 0) Ti[pi] = val;
+                if (lane == 16) Td[pd] = -val;
+                li += pi == li;
+                ld += pd == ld;
+                __syncwarp();
+                continue;
+            }
+            int32_t cd = -1;  // Td place of the group's previous value
+            for (uint32_t c0 = 0; c0 < o; c0 += 32) {
+                const uint32_t idx = c0 + (uint32_t)lane;
+                const bool valid = idx < o;
+                const int32_t val = valid ? (int32_t)v.lcs_pos[kb + off + idx] : 0;
+                const int32_t qi = valid ? lane_lower_bound(Ti, li, val) : 0;
+                const int32_t qd = valid ? lane_lower_bound(Td, ld, -val) : 0;
+                const int32_t qn = __shfl_down_sync(0xffffffffu, qi, 1);
+                const bool run_end = idx + 1 == o || lane == 31 || qn != qi;
+                const int32_t pd = lane + max(cd + 1, warp_inclusive_max(valid ? qd - lane : INT32_MIN));
+                __syncwarp();  // every search has read the tails
+                if (valid && run_end) Ti[qi] = val;
+                if (valid) Td[pd] = -val;
+                li = max(li, __shfl_sync(0xffffffffu, qi, 0) + 1);
+                cd = __shfl_sync(0xffffffffu, pd, (int)min(31u, o - 1 - c0));
+                ld = max(ld, cd + 1);
+                __syncwarp();
+            }
+        }
+    }
+    if (lane == 0) {
+        J->score = __ddiv_rn((double)max(li, ld), (double)m);
+        J->t_l = J->rmin;
+        J->t_r = J->rmax;
+        J->inter = J->matches;
+        J->same = J->codir;
+        J->s_sz = J->rmax - J->rmin;
+    }
+}
 
 // One candidate window (best_fixed_length, src/shmap/scoring.rs:189-291).
 // cntA (per seed: occurrences seen) and ring (per seed: positions of its last
@@ -1559,7 +1761,7 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
     for (uint32_t ci = wid; ci < nfar; ci += nwarps) {
         BucketJob* J = v.jobs + v.cfar[ci];
         const int32_t q = J->read;
-        if (v.P.metric == 2) {  // bucket_SH (scoring.rs:311-325)
+        if (v.P.metric == MET_BUCKET_SH) {  // bucket_SH (scoring.rs:311-325)
             if (lane == 0) {
                 J->score = J->sh;
                 J->t_l = J->rmin;
@@ -1574,6 +1776,34 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
             refine_one(v, J, q, s_cnt[wib], D, PC, s_ring[wib], lane, lt);
         else
             refine_one(v, J, q, cntA, D, PC, ring, lane, lt);
+        __syncwarp();
+    }
+}
+
+// bucket_LCS over the candidates in cfar, a warp at a time, taken from a
+// queue (their costs differ by orders of magnitude: a window in a tandem
+// repeat feeds each seed's many read positions once per k-mer). The two tail
+// arrays of a read of at most LCS_SM k-mers are in the warp's shared slice,
+// those of larger reads in its global scratch.
+constexpr int LCS_WARPS = 8;
+constexpr int LCS_SM = 512;
+__global__ void __launch_bounds__(LCS_WARPS * 32, 5) k_refine_lcs(BatchView v, RefScratch rsc) {
+    __shared__ int32_t s_tails[LCS_WARPS][2 * LCS_SM];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nfar = v.mx->n_far;
+    int32_t* const D = rsc.base + (size_t)wid * rsc.per_warp + rsc.nu_max;
+    for (;;) {
+        uint32_t ci = 0;
+        if (lane == 0) ci = atomicAdd(&v.mx->lcs_next, 1u);
+        ci = __shfl_sync(0xffffffffu, ci, 0);
+        if (ci >= nfar) break;
+        BucketJob* J = v.jobs + v.cfar[ci];
+        const int32_t q = J->read, m = v.r_m[q];
+        if (m <= LCS_SM)
+            lcs_one(v, J, q, s_tails[wib], s_tails[wib] + LCS_SM, lane);
+        else
+            lcs_one(v, J, q, D, D + m, lane);
         __syncwarp();
     }
 }
@@ -2011,7 +2241,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
                     rec.score = B.score;
                     rec.sh = B.sh;
                     rec.p_start = 0;
-                    rec.p_end = v.P.metric == 2 ? rec.read_len - 1 : rec.read_len - v.P.k - 1;
+                    rec.p_end = bucket_metric(v.P) ? rec.read_len - 1 : rec.read_len - v.P.k - 1;
                     rec.segm_id = B.seg;
                     rec.t_l = B.t_l;
                     rec.t_r = B.t_r;
@@ -2134,6 +2364,7 @@ struct MapScratch {
     DevBuf<uint64_t> sd_h;
     DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
         cidx, cfar, sort_scr, ovf_list, r_flags;
+    DevBuf<uint32_t> lcs_pos, lcs_cnt;  // bucket_LCS only
     DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
     DevBuf<BSlot> bt;
@@ -2674,20 +2905,37 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     rsc.per_warp = (size_t)rsc.nu_max + 2 * ((size_t)rsc.wmax + 1) + (size_t)m_max + 1;
     size_t warps = (size_t)wide * 8;
     const size_t budget_ints = (size_t)1 << 28;  // 1 GiB of refinement scratch at most
-    while (warps > 8 && warps * rsc.per_warp > budget_ints) warps /= 2;
+    while (warps >= 16 && warps * rsc.per_warp > budget_ints) warps /= 2;  // stays >= 8: a block's worth
     S.ref_scr.reserve(warps * rsc.per_warp);
     H.mark("ref_res");
     rsc.base = S.ref_scr.p;
     T.begin(STG_REFINE);
+    if (p.metric == SHM_BUCKET_LCS) {
+        S.lcs_pos.reserve(kcap + 1);
+        S.lcs_cnt.reserve(kcap + 1);
+        v.lcs_pos = S.lcs_pos.p;
+        k_lcs_occ<<<grid_for((size_t)n * 256, 256, 8), 256, 0, s>>>(v, S.lcs_pos.p, S.lcs_cnt.p);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+    }
     if (!c->rchip_smem_set) {
         SHM_CUDA(cudaFuncSetAttribute(k_refine_chip, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(RCHIP_WARPS * RCHIP_SLICE)));
         c->rchip_smem_set = 1;
     }
-    k_refine_chip<<<grid_for((size_t)n * 32, RCHIP_WARPS * 32, 4), RCHIP_WARPS * 32, RCHIP_WARPS * RCHIP_SLICE, s>>>(v);
-    SHM_CUDA(cudaGetLastError());
-    k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, 0, s>>>(v, rsc);
-    SHM_CUDA(cudaGetLastError());
+    if (p.metric == SHM_BUCKET_LCS) {  // no read is refined on chip under the bucket metrics
+        k_refine_lcs<<<(unsigned)std::max<size_t>(1, warps / LCS_WARPS), LCS_WARPS * 32, 0, s>>>(v, rsc);
+        SHM_CUDA(cudaGetLastError());
+    } else {
+        if (p.metric != SHM_BUCKET_SH) {
+            k_refine_chip<<<grid_for((size_t)n * 32, RCHIP_WARPS * 32, 4), RCHIP_WARPS * 32, RCHIP_WARPS * RCHIP_SLICE,
+                            s>>>(v);
+            SHM_CUDA(cudaGetLastError());
+            count_launch();
+        }
+        k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, 0, s>>>(v, rsc);
+        SHM_CUDA(cudaGetLastError());
+    }
     T.end();
     T.begin(STG_SWEEP);
     k_sweep<<<grid_for((size_t)n * 32, SWEEP_WARPS * 32, 16), SWEEP_WARPS * 32, 0, s>>>(v, S.sweep_scr.p);

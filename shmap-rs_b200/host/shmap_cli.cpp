@@ -129,7 +129,7 @@ int main(int argc, char** argv) {
             if (m == "Containment") p.metric = SHM_CONTAINMENT;
             else if (m == "Jaccard") p.metric = SHM_JACCARD;
             else if (m == "bucket_SH") p.metric = SHM_BUCKET_SH;
-            else if (m == "bucket_LCS") die("bucket_LCS is not implemented on the device path");
+            else if (m == "bucket_LCS") p.metric = SHM_BUCKET_LCS;
             else die("invalid value '" + m + "' for '--metric <METRIC>'");
         } else die("unexpected argument '" + a + "'");
     }

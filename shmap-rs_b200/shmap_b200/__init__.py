@@ -26,8 +26,8 @@ SYNTH_PATH = os.path.join(LIB_DIR, "libshmapsynth.so")
 CLI_PATH = os.path.join(PKG_ROOT, "bin", "shmap")
 
 SHM_OK = 0
-CONTAINMENT, JACCARD, BUCKET_SH = 0, 1, 2
-METRICS = {"Containment": CONTAINMENT, "Jaccard": JACCARD, "bucket_SH": BUCKET_SH}
+CONTAINMENT, JACCARD, BUCKET_SH, BUCKET_LCS = 0, 1, 2, 3
+METRICS = {"Containment": CONTAINMENT, "Jaccard": JACCARD, "bucket_SH": BUCKET_SH, "bucket_LCS": BUCKET_LCS}
 
 # shm_map_record (include/shmap_gpu.h)
 RECORD_DTYPE = np.dtype(

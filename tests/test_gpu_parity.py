@@ -125,6 +125,44 @@ def test_golden_paf(gpu_ctx, golden_dir):
     assert strip_t(paf) == strip_t(want)
 
 
+@pytest.mark.parametrize("metric", ["bucket_LCS", "bucket_SH"])
+def test_golden_inputs_bucket_metrics(gpu_ctx, golden_dir, metric):
+    """The golden fixture's inputs under the bucket metrics (scoring.rs:311-344):
+    records and PAF as the oracle's."""
+    refs = fasta.read_fastx(os.path.join(golden_dir, "tiny_ref.fa"))
+    reads = fasta.read_fastx(os.path.join(golden_dir, "tiny_reads.fa"))
+    g, o = _both_indexes(gpu_ctx, refs, 8, 1.0)
+    rec, paf = _compare_mapping(g, o, reads, k=8, h_frac=1.0, theta=0.1, metric=metric)
+    assert len(paf.splitlines()) == 2
+
+
+def test_lcs_repeats(gpu_ctx):
+    """bucket_LCS where seeds repeat: tandem copies of a 60-mer in read and
+    reference give hashes with many read positions each (long pmatches),
+    reads of both strands, sketches below and above 512 k-mers."""
+    unit = xorshift_dna(11, 60)
+    rng = np.random.default_rng(5)
+    ref = xorshift_dna(12, 30000) + unit * 150 + xorshift_dna(13, 30000)
+    comp = bytes.maketrans(b"ACGT", b"TGCA")
+    reads = []
+    for i, (a, L) in enumerate([(29000, 4000), (30500, 6000), (25000, 14000), (100, 1500), (36000, 30000)]):
+        s = ref[a:a + L]
+        reads.append((f"r{i}", s if i % 2 == 0 else s.translate(comp)[::-1]))
+    reads.append(("tandem", unit * 40))
+    reads.append(("swapped", ref[14000:17000] + ref[9000:12000]))  # collinear halves in the wrong order
+    for i in range(len(reads)):  # 3% substitutions
+        r = bytearray(reads[i][1])
+        for j in rng.integers(0, len(r), len(r) * 3 // 100):
+            r[j] = b"ACGT"[int(rng.integers(0, 4))]
+        reads[i] = (reads[i][0], bytes(r))
+    g, o = _both_indexes(gpu_ctx, [("chrA", ref)], 12, 0.25)
+    for theta in (0.2, 0.5):
+        rec, _ = _compare_mapping(g, o, reads, k=12, h_frac=0.25, theta=theta, metric="bucket_LCS")
+    ok = rec["status"] == 0
+    assert ok.sum() >= 4 and (rec["score"][ok] < 1.0).all()
+    assert rec["sketch_size"].max() > 512 and rec["sketch_size"].min() < 512
+
+
 def test_thread_parity_workload(gpu_ctx):
     refs, reads = thread_parity_workload()
     g, o = _both_indexes(gpu_ctx, refs, 12, 0.5)
@@ -157,6 +195,7 @@ def uniform(gpu_ctx):
     dict(theta=0.4, min_diff=0.075, max_overlap=0.3),
     dict(theta=0.4, metric="Jaccard"),
     dict(theta=0.4, metric="bucket_SH"),
+    dict(theta=0.4, metric="bucket_LCS"),
     dict(theta=0.9),
     dict(theta=0.0),
     dict(theta=0.4, min_diff=1.5),
@@ -181,6 +220,7 @@ def test_const_generic_variants(gpu_ctx, uniform, flags):
     g2, o2 = _both_indexes(gpu_ctx, refs, 12, 0.5)
     _compare_mapping(g2, o2, tr, k=12, h_frac=0.5, theta=0.2, **flags)
     _compare_mapping(g2, o2, tr, k=12, h_frac=0.5, theta=0.2, metric="bucket_SH", **flags)
+    _compare_mapping(g2, o2, tr, k=12, h_frac=0.5, theta=0.2, metric="bucket_LCS", **flags)
 
 
 @pytest.fixture(scope="module")
@@ -194,6 +234,8 @@ def human_small(gpu_ctx):
                                                    ("ont", 0.01, "Containment", 0.05),
                                                    ("ont", 0.01, "Jaccard", 0.05),
                                                    ("dense", 0.10, "bucket_SH", 0.4),
+                                                   ("dense", 0.10, "bucket_LCS", 0.4),
+                                                   ("ont", 0.01, "bucket_LCS", 0.05),
                                                    ("dense", 0.10, "Containment", 0.4)])
 def test_human_like_workloads(gpu_ctx, human_small, preset, r, metric, theta):
     """Satellite arrays, interspersed repeats, HiFi/ONT/dense read shapes at 1% scale.

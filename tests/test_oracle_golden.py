@@ -207,3 +207,35 @@ def test_records_and_paf_agree():
     assert strip_t(paf) == strip_t(cli)
     rec = idx.map_reads(p, rs, ro)
     assert (rec["status"] == 0).sum() == len(paf.splitlines())
+
+
+def test_lcs_known_answer():
+    """src/shmap/scoring.rs:498-535: bucket 1 at half-length 2 over seven
+    reference k-mers, three seeds with pmatches [5, 1], [4, 2], [3] -> 3."""
+    t = [(10, 0x111111), (20, 0x222222), (30, 0x111111), (40, 0x444444), (50, 0x555555), (60, 0x111111),
+         (70, 0x222222)]
+    assert O.lcs(t, 2, 6, {0x111111: [5, 1], 0x222222: [4, 2], 0x444444: [3]}) == 3
+
+
+def _lis_brute(xs):
+    """Longest strictly increasing subsequence by the quadratic recurrence."""
+    best = [1] * len(xs)
+    for i in range(len(xs)):
+        for j in range(i):
+            if xs[j] < xs[i]:
+                best[i] = max(best[i], best[j] + 1)
+    return max(best, default=0)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_lcs_matches_the_definition(seed):
+    """scoring.rs:114-170 restated: positions of every window k-mer's seed,
+    then the longer of the increasing runs forward and backward."""
+    rng = np.random.default_rng(seed)
+    hashes = [int(x) for x in rng.integers(1, 1 << 40, 12)]
+    t = [(10 * i, hashes[int(rng.integers(0, 12))]) for i in range(60)]
+    seeds = {h: sorted(rng.choice(200, int(rng.integers(1, 4)), replace=False).tolist(), reverse=True)
+             for h in hashes[:8]}
+    for bgn, end in [(0, 60), (7, 31), (40, 80), (59, 60), (5, 5)]:
+        pp = [x for _, h in t[bgn:min(end, len(t))] if h in seeds for x in seeds[h]]
+        assert O.lcs(t, bgn, end, seeds) == max(_lis_brute(pp), _lis_brute(pp[::-1]))
