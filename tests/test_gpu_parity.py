@@ -321,3 +321,41 @@ def test_capacity_fallbacks(gpu_ctx, human_small, env, monkeypatch):
     g.map_reads_device(p, d_seq.data_ptr(), poffs, d_out.data_ptr())
     torch.cuda.synchronize()
     assert not record_mismatches(d_out.cpu().numpy().view(sb.RECORD_DTYPE), rec)
+
+
+def test_pinned_host_batches(gpu_ctx):
+    """Reads in pinned host memory, over five host-buffer batches: the records
+    equal those of the same reads in pageable memory and of the
+    device-resident call."""
+    import torch
+
+    ref = bytearray(xorshift_dna(77, 2_000_000))
+    for a in range(1000, len(ref), 50_000):
+        ref[a:a + 40] = b"N" * 40
+    ref = bytes(ref)
+    g = sb.SketchIndex.from_records(gpu_ctx, [("chrU", ref)], 15, 0.1)
+    rng = np.random.default_rng(8)
+    comp = bytes.maketrans(b"ACGTN", b"TGCAN")
+    reads = []
+    for i in range(100_000):
+        a = int(rng.integers(0, len(ref) - 400))
+        r = bytearray(ref[a:a + int(rng.integers(250, 400))])
+        if i % 7 == 0:
+            r[5:9] = b"acgt"
+        r = bytes(r)
+        reads.append(r.translate(comp)[::-1] if i % 2 else r)
+    seq, offs = pack(reads)
+    p = sb.Params(k=15, h_frac=0.1, theta=0.4)
+    want = g.map_reads(p, seq, offs)
+    assert (want["status"] == 0).mean() > 0.9
+    pinned = torch.empty(len(seq) + 32, dtype=torch.uint8).pin_memory()
+    pinned[: len(seq)].copy_(torch.from_numpy(np.ascontiguousarray(seq)))
+    got = g.map_reads(p, pinned.numpy()[: len(seq)], offs)
+    assert not record_mismatches(got, want)
+    d_seq = torch.zeros(len(seq) + 32, dtype=torch.uint8, device="cuda:0")
+    d_seq[: len(seq)].copy_(pinned[: len(seq)])
+    d_out = torch.empty(len(reads) * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8, device="cuda:0")
+    g.map_reads_device(p, d_seq.data_ptr(), offs, d_out.data_ptr())
+    torch.cuda.synchronize()
+    dev = d_out.cpu().numpy().view(sb.RECORD_DTYPE)
+    assert not record_mismatches(dev, want)
