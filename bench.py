@@ -290,6 +290,12 @@ def run_ours(args, rank, world, local):
     if not np.array_equal(h_out.view(np.uint8), rec.view(np.uint8)):
         raise RuntimeError("e2e records differ from the device-resident records")
 
+    serving = None
+    if rank == 0 and args.serve_seconds > 0:
+        serving = serve_load(ctx, idx, p, h_seq_np, offs, rec, [10_000, 50_000, 200_000, 1_000_000],
+                             args.serve_seconds, 11)
+        log(f"[bench] serving: {serving}")
+
     # plain one-read-per-launch form on a sample
     plain = None
     if rank == 0 and args.plain_sample > 0:
@@ -352,6 +358,8 @@ def run_ours(args, rank, world, local):
             "gpu_launches": int(launches),
             "clocks": clk,
         }
+        if serving:
+            result["serving"] = serving
         if plain:
             result["plain_form"] = {"reads_per_s": round(plain["reads_per_s"], 1), "sample_reads": plain["sample_reads"],
                                     "batched_e2e_over_plain": round(e2e_value / plain["reads_per_s"], 1)}
@@ -360,6 +368,80 @@ def run_ours(args, rank, world, local):
     idx.close()
     ctx.close()
     return result, (gen, names, seq, offs, wk)
+
+
+def serve_load(ctx, idx, p, h_seq_np, offs, rec, rates, seconds: float, seed: int):
+    """Serving (shm_server_*): requests of 1-4,096 reads (uniform), each a run of
+    the workload's reads read in place from the pinned buffer, arrive as a
+    Poisson process at each offered rate (reads/s) for `seconds`. Reports the
+    achieved rate and the per-read latency percentiles (a read's latency is its
+    request's, submit to records written), and checks every request's records
+    against the same reads' records mapped alone in one call."""
+    import threading
+
+    import shmap_b200 as sb
+
+    n = len(offs) - 1
+    rng = np.random.default_rng(seed)
+    out = []
+    same = True
+    with sb.Server(ctx, idx, p, slots=2) as srv:
+        # warm-up: full batches on both slots, so that their buffers are grown
+        warm = []
+        for _ in range(8):
+            size = min(4096, n)
+            a = int(rng.integers(0, n - size + 1))
+            warm.append(srv.submit(h_seq_np, offs[a:a + size + 1]))
+        for t in warm:
+            if srv.poll(t, 120_000) is None:
+                raise RuntimeError("a serving warm-up request did not finish within 120 s")
+        for rate in rates:
+            plan, t = [], 0.0
+            while True:
+                t += rng.exponential(2048.5 / rate)
+                if t > seconds:
+                    break
+                size = int(rng.integers(1, min(4096, n) + 1))
+                a = int(rng.integers(0, n - size + 1))
+                plan.append((t, a, size))
+            tickets = [None] * len(plan)
+            ready = threading.Semaphore(0)
+
+            def submitter():
+                t0 = time.perf_counter()
+                for i, (at, a, size) in enumerate(plan):
+                    delay = at - (time.perf_counter() - t0)
+                    if delay > 0:
+                        time.sleep(delay)
+                    tickets[i] = srv.submit(h_seq_np, offs[a:a + size + 1])
+                    ready.release()
+
+            w0 = time.perf_counter()
+            th = threading.Thread(target=submitter)
+            th.start()
+            lat, sizes, batch_req = [], [], []
+            for i, (at, a, size) in enumerate(plan):
+                ready.acquire()
+                done = srv.poll(tickets[i], 120_000)
+                if done is None:
+                    raise RuntimeError("a serving request did not finish within 120 s")
+                got, stt = done
+                lat.append(stt["total_ms"])
+                sizes.append(size)
+                batch_req.append(stt["batch_requests"])
+                if not np.array_equal(got.view(np.uint8), rec[a:a + size].view(np.uint8)):
+                    same = False
+            wall = time.perf_counter() - w0
+            th.join()
+            per_read = np.repeat(np.array(lat), np.array(sizes))
+            out.append({"offered_reads_per_s": rate, "arrived_reads_per_s": round(sum(sizes) / seconds, 1),
+                        "achieved_reads_per_s": round(sum(sizes) / wall, 1),
+                        "requests": len(plan), "reads": int(sum(sizes)),
+                        "p50_ms": round(float(np.percentile(per_read, 50)), 3),
+                        "p99_ms": round(float(np.percentile(per_read, 99)), 3),
+                        "mean_requests_per_batch": round(float(np.mean(batch_req)), 2)})
+    return {"arrivals": f"Poisson, requests of 1-4,096 reads (uniform), {seconds:g} s per offered rate",
+            "slots": 2, "rates": out, "records_same_as_alone": same}
 
 
 def cpu_reference(gen, names, seq, offs, wk, target_s: float, threads: int, steps: int = 1):
@@ -397,6 +479,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size, in seconds of work")
     ap.add_argument("--plain-sample", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="seconds of Poisson arrivals per offered rate in the serving measurement (0 skips it)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     threads = os.cpu_count() or 1

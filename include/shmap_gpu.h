@@ -201,6 +201,53 @@ const char* shm_work_stat_name(int i);
 int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, double h_frac, int32_t offset,
                               uint64_t* d_h, uint32_t* d_rs, int64_t cap, int64_t* n_out, void* stream);
 
+/* Serving with continuous batching. The reference maps one file per run
+ * through Mapper::map_reads (src/mapper.rs:15-17; src/shmap/mod.rs:458-636:
+ * mapping workers over the shared immutable index, output in input order);
+ * a server keeps the index resident and maps requests (a caller's reads)
+ * submitted at any time from any thread, each request's records in its
+ * input order. Its slots, each a device context with its own stream, take
+ * the queued requests in arrival order, as many as fit max_batch_reads reads
+ * and, in bases, the slot's share of hbm_budget, and map them as one batch;
+ * requests that arrive meanwhile join the next batch a slot takes, and the
+ * slots' batches run on the device at the same time. A read's record does
+ * not depend on the requests it is batched with. */
+typedef struct shm_server shm_server;
+
+typedef struct shm_server_config {
+    int32_t slots;            /* device slots (default 2) */
+    int32_t max_batch_reads;  /* most reads a slot takes at once (default 16384) */
+    int64_t max_batch_bases;  /* most bases a slot takes at once (default 2^28) */
+    size_t hbm_budget;        /* device bytes the slots may use together; 0 = half the free memory */
+} shm_server_config;
+
+typedef struct shm_request_stats {
+    int32_t status;          /* SHM_OK, or the error of the batch that carried the request */
+    int32_t reads;           /* reads of the request */
+    int32_t batch_reads;     /* reads of the batch it was mapped in */
+    int32_t batch_requests;  /* requests of that batch */
+    double queued_ms;        /* submitted -> taken by a slot */
+    double mapped_ms;        /* taken -> records written */
+    double total_ms;         /* submitted -> records written */
+} shm_request_stats;
+
+void shm_server_config_default(shm_server_config* cfg);
+/* The server maps on ctx's device with idx (built or loaded there) and p; ctx
+ * and idx must outlive it. cfg = NULL takes the defaults. */
+int shm_server_create(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const shm_server_config* cfg,
+                      shm_server** out);
+/* Queues n reads (seqs/offs as in shm_map_batch; host memory, pinned or
+ * not). seqs, offs and out must stay valid until shm_poll reports the
+ * request done; out[0..n) is written then. */
+int shm_submit(shm_server* srv, const uint8_t* seqs, const int64_t* offs, int32_t n, shm_map_record* out,
+               uint64_t* ticket);
+/* Waits up to wait_ms (< 0: until done) for a request. Done: returns its
+ * status (SHM_OK or its batch's error), fills st (may be NULL) and releases
+ * the ticket. Not done yet: SHM_ERR_TIMEOUT. Unknown ticket: SHM_ERR_INVALID. */
+int shm_poll(shm_server* srv, uint64_t ticket, int32_t wait_ms, shm_request_stats* st);
+/* Maps every request still queued, then stops. Unpolled tickets are dropped. */
+int shm_server_destroy(shm_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,6 +12,7 @@
 #include "shm_internal.hpp"
 #include "shm_map.cuh"
 #include "shm_prims.cuh"
+#include "shm_serve.hpp"
 #include "shm_sketch.cuh"
 
 struct shm_ctx {
@@ -441,6 +442,86 @@ int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const
     shm::map_host(ctx->m, idx->s, *p, seqs, offs, n, out, true);
     return SHM_OK;
     SHM_GUARD_END
+}
+
+void shm_server_config_default(shm_server_config* cfg) {
+    if (!cfg) return;
+    cfg->slots = 2;
+    cfg->max_batch_reads = 16384;
+    cfg->max_batch_bases = (int64_t)1 << 28;
+    cfg->hbm_budget = 0;
+}
+
+struct shm_server {
+    shm::Server* s = nullptr;
+    int32_t k = 0;
+};
+
+int shm_server_create(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const shm_server_config* cfg,
+                      shm_server** out) {
+    if (!out) return fail(SHM_ERR_INVALID, "null out");
+    *out = nullptr;
+    int v = check_map_args(ctx, idx, p, 0);
+    if (v != SHM_OK) return v;
+    shm_server_config c;
+    shm_server_config_default(&c);
+    if (cfg) c = *cfg;
+    if (c.slots < 1 || c.slots > 64 || c.max_batch_reads < 1 || c.max_batch_bases < 1)
+        return fail(SHM_ERR_INVALID, "server config out of range");
+    SHM_GUARD_BEGIN
+    auto* h = new shm_server();
+    h->s = shm::server_create(ctx->m->device, idx->s, *p,
+                              shm::ServeConfig{c.slots, c.max_batch_reads, c.max_batch_bases, c.hbm_budget});
+    *out = h;
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_submit(shm_server* srv, const uint8_t* seqs, const int64_t* offs, int32_t n, shm_map_record* out,
+               uint64_t* ticket) {
+    if (!srv || !ticket || n < 0) return fail(SHM_ERR_INVALID, "null argument");
+    if (n > 0 && (!seqs || !offs || !out)) return fail(SHM_ERR_INVALID, "null argument");
+    int v = check_reads(offs, n);
+    if (v != SHM_OK) return v;
+    SHM_GUARD_BEGIN
+    *ticket = shm::server_submit(srv->s, seqs, offs, n, out);
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_poll(shm_server* srv, uint64_t ticket, int32_t wait_ms, shm_request_stats* st) {
+    if (!srv) return fail(SHM_ERR_INVALID, "null argument");
+    shm::ServeStats s{};
+    std::string err;
+    const int r = shm::server_poll(srv->s, ticket, wait_ms, st ? &s : nullptr, &err);
+    if (st && r != SHM_ERR_INVALID && r != SHM_ERR_TIMEOUT) {
+        st->status = s.status;
+        st->reads = s.reads;
+        st->batch_reads = s.batch_reads;
+        st->batch_requests = s.batch_requests;
+        st->queued_ms = s.queued_ms;
+        st->mapped_ms = s.mapped_ms;
+        st->total_ms = s.total_ms;
+    }
+    if (r == SHM_ERR_TIMEOUT) return fail(r, "not done yet");
+    if (r != SHM_OK) return fail(r, err);
+    return SHM_OK;
+}
+
+int shm_server_destroy(shm_server* srv) {
+    if (!srv) return SHM_OK;
+    SHM_GUARD_BEGIN
+    shm::server_destroy(srv->s);
+    delete srv;
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+// Test hook: the admission rule of a server slot (how many of the queued
+// requests one batch takes), with no device involved.
+int64_t shm_internal_serve_admit(const int64_t* reads, const int64_t* bases, int64_t n, int64_t max_reads,
+                                 int64_t max_bases) {
+    return (int64_t)shm::admit_count(reads, bases, (size_t)n, max_reads, max_bases);
 }
 
 int shm_map_batch_device(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* d_seqs,

@@ -25,12 +25,15 @@ struct DevBuf {
     T* p = nullptr;
     size_t cap = 0;  // elements
     // Grows (never shrinks). Queued work may still use the old buffer, so a
-    // growth waits for the device first.
+    // growth waits for the device first; a buffer that grows again takes a
+    // quarter more than asked, so that batches of varying size (a server's)
+    // stop growing it soon.
     void reserve(size_t n) {
         if (n <= cap && p) return;
         if (p) {
             SHM_CUDA(cudaDeviceSynchronize());
             SHM_CUDA(cudaFree(p));
+            n += n / 4;
         }
         if (std::getenv("SHMAP_HOSTPROF"))
             std::fprintf(stderr, "[shmap-host] grow %zu -> %zu bytes\n", cap * sizeof(T), n * sizeof(T));

@@ -1,0 +1,42 @@
+// Serving with continuous batching (see shm_serve.cu).
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/shmap_gpu.h"
+
+namespace shm {
+
+struct IndexStorage;
+
+struct ServeConfig {
+    int slots;
+    int32_t max_batch_reads;
+    int64_t max_batch_bases;
+    size_t hbm_budget;
+};
+
+struct ServeStats {
+    int32_t status, reads, batch_reads, batch_requests;
+    double queued_ms, mapped_ms, total_ms;
+};
+
+struct Server;
+
+// How many requests, from the front of a queue whose requests hold reads[i]
+// reads and bases[i] bases, one batch takes: in order, while both totals
+// stay within the limits, and always the first.
+size_t admit_count(const int64_t* reads, const int64_t* bases, size_t n, int64_t max_reads, int64_t max_bases);
+
+Server* server_create(int device, const IndexStorage* ix, const shm_params& p, const ServeConfig& cfg);
+uint64_t server_submit(Server* s, const uint8_t* seqs, const int64_t* offs, int32_t n, shm_map_record* out);
+// SHM_OK (or the request's error) once it is done, then the ticket is
+// released; SHM_ERR_TIMEOUT while it is not; SHM_ERR_INVALID for an unknown
+// ticket. wait_ms < 0 waits until it is done.
+int server_poll(Server* s, uint64_t ticket, int32_t wait_ms, ServeStats* st, std::string* err);
+// Maps what is still queued, then stops the slots.
+void server_destroy(Server* s);
+
+}  // namespace shm

@@ -26,6 +26,7 @@ SYNTH_PATH = os.path.join(LIB_DIR, "libshmapsynth.so")
 CLI_PATH = os.path.join(PKG_ROOT, "bin", "shmap")
 
 SHM_OK = 0
+SHM_ERR_INVALID, SHM_ERR_CUDA, SHM_ERR_NOMEM, SHM_ERR_CAPACITY, SHM_ERR_TIMEOUT = -1, -2, -3, -4, -5
 CONTAINMENT, JACCARD, BUCKET_SH, BUCKET_LCS = 0, 1, 2, 3
 METRICS = {"Containment": CONTAINMENT, "Jaccard": JACCARD, "bucket_SH": BUCKET_SH, "bucket_LCS": BUCKET_LCS}
 
@@ -55,6 +56,17 @@ class CParams(ctypes.Structure):
                 ("theta", ctypes.c_double), ("min_diff", ctypes.c_double), ("max_overlap", ctypes.c_double),
                 ("metric", ctypes.c_int32), ("no_bucket_pruning", ctypes.c_int32), ("one_sweep", ctypes.c_int32),
                 ("abs_pos", ctypes.c_int32)]
+
+
+class CServerConfig(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int32), ("max_batch_reads", ctypes.c_int32), ("max_batch_bases", ctypes.c_int64),
+                ("hbm_budget", ctypes.c_size_t)]
+
+
+class CRequestStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("reads", ctypes.c_int32), ("batch_reads", ctypes.c_int32),
+                ("batch_requests", ctypes.c_int32), ("queued_ms", ctypes.c_double), ("mapped_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
 
 
 class CIndexStats(ctypes.Structure):
@@ -104,6 +116,11 @@ def lib() -> ctypes.CDLL:
         "shm_ctx_work_stats": (ctypes.c_int, [P, P, ctypes.c_int]),
         "shm_work_stat_name": (ctypes.c_char_p, [ctypes.c_int]),
         "shm_sketch_device_noalloc": (ctypes.c_int, [P, i64, i32, dbl, i32, P, P, i64, P, P]),
+        "shm_server_config_default": (None, [P]),
+        "shm_server_create": (ctypes.c_int, [P, P, P, P, P]),
+        "shm_submit": (ctypes.c_int, [P, P, P, i32, P, P]),
+        "shm_poll": (ctypes.c_int, [P, u64, i32, P]),
+        "shm_server_destroy": (ctypes.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -349,6 +366,58 @@ class SketchIndex:
         _check(lib().shm_format_paf(self.h, ctypes.byref(cp), _ptr(records), len(records), joined,
                                     0 if mt is None else _ptr(mt), buf, need.value, ctypes.byref(need)))
         return buf.raw[:need.value].decode()
+
+
+class Server:
+    """Serving with continuous batching (shm_server_create / shm_submit /
+    shm_poll): the index stays resident and requests submitted from any thread
+    are mapped in batches that device slots take as they free up. A request's
+    arrays are kept alive here until it is polled done."""
+
+    def __init__(self, ctx: "Context", index: "SketchIndex", params: Params, slots: int = 2,
+                 max_batch_reads: int = 16384, max_batch_bases: int = 1 << 28, hbm_budget: int = 0):
+        cfg = CServerConfig(slots, max_batch_reads, max_batch_bases, hbm_budget)
+        self._cp = params.c()
+        h = ctypes.c_void_p()
+        _check(lib().shm_server_create(ctx.h, index.h, ctypes.byref(self._cp), ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self._live = {}
+
+    def submit(self, seq: np.ndarray, offs: np.ndarray, out: Optional[np.ndarray] = None) -> int:
+        """Queues reads (bytes and n+1 offsets, as map_reads takes them); returns a ticket."""
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        n = len(offs) - 1
+        if out is None:
+            out = np.zeros(n, RECORD_DTYPE)
+        t = ctypes.c_uint64()
+        _check(lib().shm_submit(self.h, _ptr(seq), _ptr(offs), n, _ptr(out), ctypes.byref(t)))
+        self._live[t.value] = (seq, offs, out)
+        return t.value
+
+    def poll(self, ticket: int, wait_ms: int = -1):
+        """(records, stats dict) once the request is done; None while it is not
+        (wait_ms >= 0); raises ShmError if its batch failed."""
+        st = CRequestStats()
+        rc = lib().shm_poll(self.h, ticket, wait_ms, ctypes.byref(st))
+        if rc == SHM_ERR_TIMEOUT:
+            return None
+        arrays = self._live.pop(ticket, None)
+        _check(rc)
+        stats = {f: getattr(st, f) for f, _ in CRequestStats._fields_}
+        return arrays[2], stats
+
+    def close(self) -> None:
+        if self.h:
+            _check(lib().shm_server_destroy(self.h))
+            self.h = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def strip_timing(paf: str) -> str:
