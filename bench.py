@@ -290,6 +290,32 @@ def run_ours(args, rank, world, local):
     if not np.array_equal(h_out.view(np.uint8), rec.view(np.uint8)):
         raise RuntimeError("e2e records differ from the device-resident records")
 
+    paf = None
+    if rank == 0:  # the PAF text of the step's records: shm_format_paf (host) and shm_format_paf_device
+        joined = "\n".join(names).encode()
+        cp = p.c()
+        need = ctypes.c_int64()
+        _ = sb.lib().shm_format_paf(idx.h, ctypes.byref(cp), rec.ctypes.data, n, joined, None, None, 0,
+                                    ctypes.byref(need))
+        cap = need.value
+        buf_h = np.empty(cap, np.uint8)
+        buf_d = torch.empty(cap, dtype=torch.uint8).pin_memory().numpy()
+        t0 = time.perf_counter()
+        sb._check(sb.lib().shm_format_paf(idx.h, ctypes.byref(cp), rec.ctypes.data, n, joined, None,
+                                          buf_h.ctypes.data, cap, ctypes.byref(need)))
+        t_h = time.perf_counter() - t0
+        ts = []
+        for _ in range(3):  # the first call grows the device buffers
+            t0 = time.perf_counter()
+            sb._check(sb.lib().shm_format_paf_device(ctx.h, idx.h, ctypes.byref(cp), rec.ctypes.data, n, joined,
+                                                     None, buf_d.ctypes.data, cap, ctypes.byref(need)))
+            ts.append(time.perf_counter() - t0)
+        if not np.array_equal(buf_h, buf_d):
+            raise RuntimeError("PAF text rendered on the device differs from the host's")
+        paf = {"bytes": cap, "lines": int((rec["status"] == 0).sum()), "host_s": round(t_h, 4),
+               "device_s": round(min(ts[1:]), 4), "host_over_device": round(t_h / min(ts[1:]), 1)}
+        log(f"[bench] PAF text: {paf}")
+
     serving = None
     if rank == 0 and args.serve_seconds > 0:
         serving = serve_load(ctx, idx, p, h_seq_np, offs, rec, [10_000, 50_000, 200_000, 1_000_000],
@@ -360,6 +386,8 @@ def run_ours(args, rank, world, local):
         }
         if serving:
             result["serving"] = serving
+        if paf:
+            result["paf_text"] = paf
         if plain:
             result["plain_form"] = {"reads_per_s": round(plain["reads_per_s"], 1), "sample_reads": plain["sample_reads"],
                                     "batched_e2e_over_plain": round(e2e_value / plain["reads_per_s"], 1)}

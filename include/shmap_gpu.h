@@ -159,6 +159,13 @@ int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const
  * *n_out; writes at most cap bytes. */
 int shm_format_paf(const shm_index* idx, const shm_params* p, const shm_map_record* rec, int32_t n, const char* names,
                    const double* map_time, char* buf, int64_t cap, int64_t* n_out);
+/* The same text, byte for byte, rendered on ctx's device (one thread per
+ * read; f64 fields rounded exactly, half to even). Same arguments, all in
+ * host memory; buf = NULL only measures. SHM_ERR_CAPACITY when the text
+ * exceeds cap (its first cap bytes are written). */
+int shm_format_paf_device(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const shm_map_record* rec,
+                          int32_t n, const char* names, const double* map_time, char* buf, int64_t cap,
+                          int64_t* n_out);
 
 /* Kernel launches this library issued so far in this process (the bench
  * reports the count inside its timed region). */

@@ -11,6 +11,7 @@
 #include "shm_common.cuh"
 #include "shm_internal.hpp"
 #include "shm_map.cuh"
+#include "shm_paf.hpp"
 #include "shm_prims.cuh"
 #include "shm_serve.hpp"
 #include "shm_sketch.cuh"
@@ -440,6 +441,21 @@ int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const
     if ((v = check_reads(offs, n)) != SHM_OK) return v;
     SHM_GUARD_BEGIN
     shm::map_host(ctx->m, idx->s, *p, seqs, offs, n, out, true);
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_format_paf_device(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const shm_map_record* rec,
+                          int32_t n, const char* names, const double* map_time, char* buf, int64_t cap,
+                          int64_t* n_out) {
+    if (!ctx || !idx || !p || !n_out || n < 0 || (n > 0 && !rec)) return fail(SHM_ERR_INVALID, "null argument");
+    for (int32_t i = 0; i < n; i++)
+        if (rec[i].status == 0 && (rec[i].segm_id < 0 || (size_t)rec[i].segm_id >= idx->s->names.size()))
+            return fail(SHM_ERR_INVALID, "record with a segment the index does not have");
+    SHM_GUARD_BEGIN
+    const int64_t total = shm::format_paf_device(ctx->m, *idx->s, *p, rec, n, names, map_time, buf, cap);
+    *n_out = total;
+    if (buf && total > cap) return fail(SHM_ERR_CAPACITY, "output buffer too small");
     return SHM_OK;
     SHM_GUARD_END
 }

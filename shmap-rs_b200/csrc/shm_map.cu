@@ -51,6 +51,7 @@
 
 #include "shm_common.cuh"
 #include "shm_map.cuh"
+#include "shm_paf.hpp"
 #include "../host/pack.hpp"
 #include "shm_prims.cuh"
 #include "shm_sketch.cuh"
@@ -2402,6 +2403,7 @@ void mapctx_destroy(MapCtx* c) {
         if (c->scr->luts) cudaFree(c->scr->luts);
         delete c->scr;
     }
+    paf_scratch_free(c->paf);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->h_slots) cudaFreeHost(c->h_slots);
     if (c->h_pack) cudaFreeHost(c->h_pack);

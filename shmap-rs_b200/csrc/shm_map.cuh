@@ -30,6 +30,7 @@ struct BucketJob {
 };
 
 struct MapScratch;  // grow-only device buffers owned by a context
+struct PafScratch;  // those of the PAF formatting (shm_paf.cu)
 
 // Stages timed with CUDA events on the context's stream when timing is on.
 enum Stage { STG_SKETCH, STG_SEEDPREP, STG_CONTRIB, STG_BSCAN, STG_EXTEND, STG_REFINE, STG_SWEEP, STG_AUX, N_STAGES };
@@ -52,6 +53,7 @@ struct MapCtx {
     cudaStream_t side_stream = nullptr;  // seed preparation of the few reads with large sketches
     cudaEvent_t fork = nullptr, join = nullptr;
     MapScratch* scr = nullptr;
+    PafScratch* paf = nullptr;
     size_t hbm_budget = 0;
     int64_t launches = 0;
     // host staging (pinned): the plan of the batch in flight, small readbacks

@@ -183,9 +183,14 @@ int main(int argc, char** argv) {
         tms.assign(b - a, per);
         std::string names = join(reads.names, a, b);
         int64_t need = 0;
-        shm_format_paf(idx, &p, rec.data(), (int32_t)(b - a), names.c_str(), tms.data(), nullptr, 0, &need);
+        // the PAF text is rendered on the device, byte for byte shm_format_paf's
+        if (shm_format_paf_device(ctx, idx, &p, rec.data(), (int32_t)(b - a), names.c_str(), tms.data(), nullptr, 0,
+                                  &need) != SHM_OK)
+            die(std::string("failed to format PAF: ") + shm_last_error());
         buf.resize((size_t)need);
-        shm_format_paf(idx, &p, rec.data(), (int32_t)(b - a), names.c_str(), tms.data(), buf.data(), need, &need);
+        if (need && shm_format_paf_device(ctx, idx, &p, rec.data(), (int32_t)(b - a), names.c_str(), tms.data(),
+                                          buf.data(), need, &need) != SHM_OK)
+            die(std::string("failed to format PAF: ") + shm_last_error());
         std::fwrite(buf.data(), 1, buf.size(), stdout);
         if (unm)
             for (size_t i = a; i < b; i++)

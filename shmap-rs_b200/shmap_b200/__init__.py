@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
         "shm_ctx_work_stats": (ctypes.c_int, [P, P, ctypes.c_int]),
         "shm_work_stat_name": (ctypes.c_char_p, [ctypes.c_int]),
         "shm_sketch_device_noalloc": (ctypes.c_int, [P, i64, i32, dbl, i32, P, P, i64, P, P]),
+        "shm_format_paf_device": (ctypes.c_int, [P, P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
         "shm_server_config_default": (None, [P]),
         "shm_server_create": (ctypes.c_int, [P, P, P, P, P]),
         "shm_submit": (ctypes.c_int, [P, P, P, i32, P, P]),
@@ -418,6 +419,28 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+def format_paf_device(index: "SketchIndex", params: Params, records: np.ndarray, names: Sequence[str],
+                      map_time: Optional[np.ndarray] = None) -> str:
+    """SketchIndex.format_paf's text, rendered on the index's device (shm_format_paf_device)."""
+    records = np.ascontiguousarray(records, dtype=RECORD_DTYPE)
+    joined = "\n".join(names).encode()
+    cp = params.c()
+    mt = None if map_time is None else np.ascontiguousarray(map_time, dtype=np.float64)
+    need = ctypes.c_int64()
+    f = lib().shm_format_paf_device
+    cap = 640 * len(records) + len(joined) + 1  # a line is about 480 bytes plus its names
+    buf = ctypes.create_string_buffer(cap)
+    rc = f(index.ctx.h, index.h, ctypes.byref(cp), _ptr(records), len(records), joined,
+           0 if mt is None else _ptr(mt), buf, cap, ctypes.byref(need))
+    if rc == SHM_ERR_CAPACITY:  # very long numbers: once more with the exact size
+        cap = need.value + 1
+        buf = ctypes.create_string_buffer(cap)
+        rc = f(index.ctx.h, index.h, ctypes.byref(cp), _ptr(records), len(records), joined,
+               0 if mt is None else _ptr(mt), buf, cap, ctypes.byref(need))
+    _check(rc)
+    return ctypes.string_at(buf, need.value).decode()
 
 
 def strip_timing(paf: str) -> str:
