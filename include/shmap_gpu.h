@@ -208,6 +208,29 @@ const char* shm_work_stat_name(int i);
 int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, double h_frac, int32_t offset,
                               uint64_t* d_h, uint32_t* d_rs, int64_t cap, int64_t* n_out, void* stream);
 
+/* FASTA parsed on the device: the reference reads its inputs with
+ * needletail (src/io/mod.rs:383-427, src/index.rs:384-393). The file's bytes
+ * (host memory) go up once and are parsed on ctx's device: a record per '>'
+ * header line, its name the header up to the first space or tab, its
+ * sequence its lines joined without '\n' and without one '\r' before a line's
+ * end. The sequences stay in device memory, for shm_index_build_fasta and
+ * shm_map_fasta. Files with a line starting with '@' (FASTQ) or text before
+ * the first header are refused with SHM_ERR_INVALID: read those on the host. */
+typedef struct shm_fasta shm_fasta;
+int shm_fasta_parse_device(shm_ctx* ctx, const uint8_t* file, int64_t len, shm_fasta** out);
+/* n records; offs (n+1 entries) and names ('\n'-joined) stay owned by fa. */
+int shm_fasta_records(const shm_fasta* fa, int32_t* n, const int64_t** offs, const char** names);
+/* All records' bases, back to back (offs[n] bytes), to host memory. */
+int shm_fasta_copy_seq(const shm_fasta* fa, uint8_t* dst);
+int shm_fasta_destroy(shm_fasta* fa);
+/* shm_index_build over the parsed records (segments in file order). */
+int shm_index_build_fasta(shm_ctx* ctx, const shm_fasta* fa, int32_t k, double h_frac, int32_t max_matches,
+                          shm_index** out);
+/* shm_map_batch over records [first, first + n) of the parsed reads, from
+ * device memory; out (host) gets their records. */
+int shm_map_fasta(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const shm_fasta* fa, int32_t first,
+                  int32_t n, shm_map_record* out);
+
 /* Serving with continuous batching. The reference maps one file per run
  * through Mapper::map_reads (src/mapper.rs:15-17; src/shmap/mod.rs:458-636:
  * mapping workers over the shared immutable index, output in input order);

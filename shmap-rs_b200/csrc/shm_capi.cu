@@ -9,6 +9,7 @@
 
 #include "../../include/shmap_gpu.h"
 #include "shm_common.cuh"
+#include "shm_fasta.hpp"
 #include "shm_internal.hpp"
 #include "shm_map.cuh"
 #include "shm_paf.hpp"
@@ -227,9 +228,24 @@ int shm_sketch(shm_ctx* ctx, const uint8_t* seq, int64_t len, int32_t k, double 
     SHM_GUARD_END
 }
 
+static int check_index_args(const int64_t* seg_off, int32_t n_seg, int32_t k, double h_frac, int32_t max_matches);
+
 int shm_index_build(shm_ctx* ctx, const uint8_t* seq, const int64_t* seg_off, int32_t n_seg, const char* names,
                     int32_t k, double h_frac, int32_t max_matches, shm_index** out) {
     if (!ctx || !out || !seg_off || n_seg < 0) return fail(SHM_ERR_INVALID, "null argument");
+    const int v = check_index_args(seg_off, n_seg, k, h_frac, max_matches);
+    if (v != SHM_OK) return v;
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(ctx->m->device));
+    auto* ix = new shm_index();
+    ix->s = shm::build_index(seq, seg_off, n_seg, split_names(names, n_seg), k, h_frac, max_matches, ctx->m->stream);
+    ctx->m->launches += 40;
+    *out = ix;
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+static int check_index_args(const int64_t* seg_off, int32_t n_seg, int32_t k, double h_frac, int32_t max_matches) {
     if (k <= 0) return fail(SHM_ERR_INVALID, "K-mer length (-k) should be positive.");
     if (!(h_frac > 0.0) || h_frac > 1.0) return fail(SHM_ERR_INVALID, "Given hash ratio (-r) should be between 0 and 1.");
     if (max_matches != -1 && max_matches <= 0) return fail(SHM_ERR_INVALID, "The number of seed matches (-M) should be positive.");
@@ -240,10 +256,64 @@ int shm_index_build(shm_ctx* ctx, const uint8_t* seq, const int64_t* seg_off, in
         if (L >= k) windows += (uint64_t)(L - k + 1);
     }
     if (windows >= 0xfffffff0ULL) return fail(SHM_ERR_INVALID, "more than 2^32 reference windows");
+    return SHM_OK;
+}
+
+struct shm_fasta {
+    shm::FastaDev* f = nullptr;
+};
+
+int shm_fasta_parse_device(shm_ctx* ctx, const uint8_t* file, int64_t len, shm_fasta** out) {
+    if (!ctx || !out || len < 0 || (len > 0 && !file)) return fail(SHM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    SHM_GUARD_BEGIN
+    std::string why;
+    shm::FastaDev* f = shm::fasta_parse_device(ctx->m->device, ctx->m->stream, file, len, &why);
+    if (!f) return fail(SHM_ERR_INVALID, "not parsed on the device: " + why);
+    auto* h = new shm_fasta();
+    h->f = f;
+    *out = h;
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_fasta_records(const shm_fasta* fa, int32_t* n, const int64_t** offs, const char** names) {
+    if (!fa) return fail(SHM_ERR_INVALID, "null argument");
+    if (n) *n = fa->f->n;
+    if (offs) *offs = fa->f->offs.data();
+    if (names) *names = fa->f->names.c_str();
+    return SHM_OK;
+}
+
+int shm_fasta_copy_seq(const shm_fasta* fa, uint8_t* dst) {
+    if (!fa || !dst) return fail(SHM_ERR_INVALID, "null argument");
+    SHM_GUARD_BEGIN
+    SHM_CUDA(cudaSetDevice(fa->f->device));
+    const int64_t total = fa->f->offs.back();
+    if (total) SHM_CUDA(cudaMemcpy(dst, fa->f->seq.p, (size_t)total, cudaMemcpyDeviceToHost));
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_fasta_destroy(shm_fasta* fa) {
+    if (!fa) return SHM_OK;
+    cudaSetDevice(fa->f->device);
+    delete fa->f;
+    delete fa;
+    return SHM_OK;
+}
+
+int shm_index_build_fasta(shm_ctx* ctx, const shm_fasta* fa, int32_t k, double h_frac, int32_t max_matches,
+                          shm_index** out) {
+    if (!ctx || !fa || !out) return fail(SHM_ERR_INVALID, "null argument");
+    if (fa->f->device != ctx->m->device) return fail(SHM_ERR_INVALID, "the FASTA is on another device");
+    const int v = check_index_args(fa->f->offs.data(), fa->f->n, k, h_frac, max_matches);
+    if (v != SHM_OK) return v;
     SHM_GUARD_BEGIN
     SHM_CUDA(cudaSetDevice(ctx->m->device));
     auto* ix = new shm_index();
-    ix->s = shm::build_index(seq, seg_off, n_seg, split_names(names, n_seg), k, h_frac, max_matches, ctx->m->stream);
+    ix->s = shm::build_index(nullptr, fa->f->offs.data(), fa->f->n, split_names(fa->f->names.c_str(), fa->f->n), k,
+                             h_frac, max_matches, ctx->m->stream, fa->f->seq.p);
     ctx->m->launches += 40;
     *out = ix;
     return SHM_OK;
@@ -538,6 +608,27 @@ int shm_server_destroy(shm_server* srv) {
 int64_t shm_internal_serve_admit(const int64_t* reads, const int64_t* bases, int64_t n, int64_t max_reads,
                                  int64_t max_bases) {
     return (int64_t)shm::admit_count(reads, bases, (size_t)n, max_reads, max_bases);
+}
+
+int shm_map_fasta(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const shm_fasta* fa, int32_t first,
+                  int32_t n, shm_map_record* out) {
+    int v = check_map_args(ctx, idx, p, n);
+    if (v != SHM_OK) return v;
+    if (!fa || (n > 0 && !out) || first < 0 || (int64_t)first + n > fa->f->n)
+        return fail(SHM_ERR_INVALID, "null argument or records out of range");
+    if (fa->f->device != ctx->m->device) return fail(SHM_ERR_INVALID, "the FASTA is on another device");
+    const int64_t* offs = fa->f->offs.data() + first;
+    if ((v = check_reads(offs, n)) != SHM_OK) return v;
+    if (n == 0) return SHM_OK;
+    SHM_GUARD_BEGIN
+    shm::FastaDev* f = fa->f;
+    f->rec.reserve((size_t)n);
+    shm::map_device(ctx->m, idx->s, *p, f->seq.p + offs[0], offs, n, f->rec.p, false);
+    SHM_CUDA(cudaMemcpyAsync(out, f->rec.p, sizeof(shm_map_record) * (size_t)n, cudaMemcpyDeviceToHost,
+                             ctx->m->stream));
+    SHM_CUDA(cudaStreamSynchronize(ctx->m->stream));
+    return SHM_OK;
+    SHM_GUARD_END
 }
 
 int shm_map_batch_device(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* d_seqs,

@@ -239,7 +239,7 @@ static void finish_index(IndexStorage* ix, uint64_t thr, uint32_t n_kept, uint32
 
 IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_t n_seg,
                           const std::vector<std::string>& names, int32_t k, double h_frac, int32_t max_matches,
-                          cudaStream_t s) {
+                          cudaStream_t s, const uint8_t* d_seq_in) {
     auto* ix = new IndexStorage();
     try {
         SHM_CUDA(cudaGetDevice(&ix->device));
@@ -267,9 +267,11 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
         DevBuf<int64_t> d_soff;
         DevBuf<uint64_t> d_chunk_off;
         DevBuf<uint32_t> d_ccnt, d_cout;
-        d_seq.reserve((size_t)total_bases + 32);
-        SHM_CUDA(cudaMemsetAsync(d_seq.p + total_bases, 0, 32, s));
-        SHM_CUDA(cudaMemcpyAsync(d_seq.p, h_seq + seg_off_b[0], (size_t)total_bases, cudaMemcpyHostToDevice, s));
+        if (!d_seq_in) {
+            d_seq.reserve((size_t)total_bases + 32);
+            SHM_CUDA(cudaMemsetAsync(d_seq.p + total_bases, 0, 32, s));
+            SHM_CUDA(cudaMemcpyAsync(d_seq.p, h_seq + seg_off_b[0], (size_t)total_bases, cudaMemcpyHostToDevice, s));
+        }
         d_soff.reserve((size_t)n_seg + 1);
         SHM_CUDA(cudaMemcpyAsync(d_soff.p, soff.data(), sizeof(int64_t) * ((size_t)n_seg + 1), cudaMemcpyHostToDevice, s));
         d_chunk_off.reserve((size_t)n_seg + 1);
@@ -280,7 +282,7 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
 
         SketchLuts* luts = create_device_luts(k, s);
         SketchArgs a{};
-        a.seq = d_seq.p;
+        a.seq = d_seq_in ? d_seq_in + seg_off_b[0] : d_seq.p;
         a.seq_off = d_soff.p;
         a.chunk_off = d_chunk_off.p;
         a.n_seq = n_seg;

@@ -77,9 +77,11 @@ struct IndexFileError {
 void save_index(const IndexStorage* ix, const char* path);
 IndexStorage* load_index(const char* path, cudaStream_t s);
 
+// The segments' bases are read from h_seq (host) or, when d_seq is given,
+// from device memory (d_seq + seg_off[i], 32 readable bytes past the end).
 IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off, int32_t n_seg,
                           const std::vector<std::string>& names, int32_t k, double h_frac, int32_t max_matches,
-                          cudaStream_t s);
+                          cudaStream_t s, const uint8_t* d_seq = nullptr);
 
 }  // namespace shm
 

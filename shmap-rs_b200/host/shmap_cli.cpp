@@ -4,9 +4,11 @@
 // ends and '\r' removed), builds the index on the device, maps the reads in
 // batches and writes PAF to stdout in input order; with -z, unmapped reads go
 // to <z>.unmapped.paf (src/shmap/mod.rs:388-394, src/mapping.rs:82-84).
-// Two options the reference does not have: --index-out FILE writes the built
+// Options the reference does not have: --index-out FILE writes the built
 // index to FILE; --index-in FILE takes the index from FILE instead of -s, and
-// its k, -r and -M replace those given on the command line.
+// its k, -r and -M replace those given on the command line; --host-fasta
+// parses FASTA on the host (by default the device parses it and keeps the
+// sequences; FASTQ is always read on the host).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -30,13 +32,17 @@ struct Records {
     std::exit(1);
 }
 
-bool read_fastx(const std::string& path, Records& out, std::string& err) {
+bool read_file(const std::string& path, std::string& data, std::string& err) {
     std::ifstream f(path, std::ios::binary);
     if (!f) {
         err = "failed to open " + path;
         return false;
     }
-    std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    data.assign((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    return true;
+}
+
+bool parse_fastx(const std::string& data, const std::string& path, Records& out, std::string& err) {
     size_t pos = 0, n = data.size();
     auto line = [&](size_t& a, size_t& b) {  // next line [a, b) without '\n' / trailing '\r'
         a = pos;
@@ -97,6 +103,7 @@ int main(int argc, char** argv) {
     shm_params_default(&p);
     std::string t_file, p_file, z_file, ix_in, ix_out;
     int threads = 1, verbose = 0, device = 0;
+    bool host_fasta = false;
     for (int i = 1; i < argc; i++) {
         std::string a = argv[i];
         auto val = [&]() -> std::string {
@@ -124,6 +131,7 @@ int main(int argc, char** argv) {
         // start from one instead of -s (its k, -r and -M then apply)
         else if (a == "--index-out") ix_out = val();
         else if (a == "--index-in") ix_in = val();
+        else if (a == "--host-fasta") host_fasta = true;  // parse FASTA on the host (same records)
         else if (a == "-m" || a == "--metric") {
             std::string m = val();
             if (m == "Containment") p.metric = SHM_CONTAINMENT;
@@ -143,22 +151,55 @@ int main(int argc, char** argv) {
     if (verbose < 0 || verbose > 2) die("--verbose (-v) should be 0, 1, or 2.");
 
     Records ref, reads;
-    std::string err;
-    if (ix_in.empty() && !read_fastx(t_file, ref, err)) die(err);
-    if (!read_fastx(p_file, reads, err)) die(err);
+    std::string err, t_data, p_data;
+    if (ix_in.empty() && !read_file(t_file, t_data, err)) die(err);
+    if (!read_file(p_file, p_data, err)) die(err);
     shm_ctx* ctx = nullptr;
     if (shm_ctx_create(device, 0, &ctx) != SHM_OK) die(std::string("CUDA: ") + shm_last_error());
+    // FASTA is parsed on the device, its sequences left there; FASTQ (and
+    // files the host reader rejects) go through the host reader
+    auto parse = [&](const std::string& data, const std::string& path, Records& rec) -> shm_fasta* {
+        shm_fasta* fa = nullptr;
+        if (!host_fasta && shm_fasta_parse_device(ctx, (const uint8_t*)data.data(), (int64_t)data.size(), &fa) ==
+                               SHM_OK) {
+            int32_t nr = 0;
+            const int64_t* offs = nullptr;
+            const char* names = nullptr;
+            shm_fasta_records(fa, &nr, &offs, &names);
+            rec.off.assign(offs, offs + nr + 1);
+            const char* q = names;
+            for (int32_t i = 0; i < nr; i++) {
+                const char* e = std::strchr(q, '\n');
+                if (!e) e = q + std::strlen(q);
+                rec.names.emplace_back(q, (size_t)(e - q));
+                q = *e ? e + 1 : e;
+            }
+            return fa;
+        }
+        if (!parse_fastx(data, path, rec, err)) die(err);
+        return nullptr;
+    };
     shm_index* idx = nullptr;
     if (!ix_in.empty()) {
         if (shm_index_load(ctx, ix_in.c_str(), &idx) != SHM_OK)
             die(std::string("failed to load index from ") + ix_in + ": " + shm_last_error());
         shm_index_info(idx, &p.k, &p.h_frac, &p.max_matches);
     } else {
-        std::string rnames = join(ref.names, 0, ref.names.size());
-        if (shm_index_build(ctx, (const uint8_t*)ref.seq.data(), ref.off.data(), (int32_t)ref.names.size(),
-                            rnames.c_str(), p.k, p.h_frac, p.max_matches, &idx) != SHM_OK)
-            die(std::string("failed to build index from ") + t_file + ": " + shm_last_error());
+        shm_fasta* tfa = parse(t_data, t_file, ref);
+        std::string().swap(t_data);
+        int rc;
+        if (tfa) {
+            rc = shm_index_build_fasta(ctx, tfa, p.k, p.h_frac, p.max_matches, &idx);
+        } else {
+            std::string rnames = join(ref.names, 0, ref.names.size());
+            rc = shm_index_build(ctx, (const uint8_t*)ref.seq.data(), ref.off.data(), (int32_t)ref.names.size(),
+                                 rnames.c_str(), p.k, p.h_frac, p.max_matches, &idx);
+        }
+        shm_fasta_destroy(tfa);
+        if (rc != SHM_OK) die(std::string("failed to build index from ") + t_file + ": " + shm_last_error());
     }
+    shm_fasta* pfa = parse(p_data, p_file, reads);
+    std::string().swap(p_data);
     if (!ix_out.empty() && shm_index_save(idx, ix_out.c_str()) != SHM_OK)
         die(std::string("failed to write index to ") + ix_out + ": " + shm_last_error());
 
@@ -177,8 +218,10 @@ int main(int argc, char** argv) {
         rec.resize(b - a);
         auto t0 = std::chrono::steady_clock::now();
         std::vector<int64_t> off(reads.off.begin() + (long)a, reads.off.begin() + (long)b + 1);
-        if (shm_map_batch(ctx, idx, &p, (const uint8_t*)reads.seq.data(), off.data(), (int32_t)(b - a), rec.data()) != SHM_OK)
-            die(std::string("failed while mapping reads from ") + p_file + ": " + shm_last_error());
+        const int rc = pfa ? shm_map_fasta(ctx, idx, &p, pfa, (int32_t)a, (int32_t)(b - a), rec.data())
+                           : shm_map_batch(ctx, idx, &p, (const uint8_t*)reads.seq.data(), off.data(),
+                                           (int32_t)(b - a), rec.data());
+        if (rc != SHM_OK) die(std::string("failed while mapping reads from ") + p_file + ": " + shm_last_error());
         double per = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() / (double)(b - a);
         tms.assign(b - a, per);
         std::string names = join(reads.names, a, b);
@@ -199,6 +242,7 @@ int main(int argc, char** argv) {
                                  (long long)(reads.off[i + 1] - reads.off[i]));
     }
     if (unm) std::fclose(unm);
+    shm_fasta_destroy(pfa);
     shm_index_destroy(idx);
     shm_ctx_destroy(ctx);
     return 0;

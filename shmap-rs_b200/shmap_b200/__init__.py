@@ -117,6 +117,12 @@ def lib() -> ctypes.CDLL:
         "shm_work_stat_name": (ctypes.c_char_p, [ctypes.c_int]),
         "shm_sketch_device_noalloc": (ctypes.c_int, [P, i64, i32, dbl, i32, P, P, i64, P, P]),
         "shm_format_paf_device": (ctypes.c_int, [P, P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
+        "shm_fasta_parse_device": (ctypes.c_int, [P, P, i64, P]),
+        "shm_fasta_records": (ctypes.c_int, [P, P, P, P]),
+        "shm_fasta_copy_seq": (ctypes.c_int, [P, P]),
+        "shm_fasta_destroy": (ctypes.c_int, [P]),
+        "shm_index_build_fasta": (ctypes.c_int, [P, P, i32, dbl, i32, P]),
+        "shm_map_fasta": (ctypes.c_int, [P, P, P, P, i32, i32, P]),
         "shm_server_config_default": (None, [P]),
         "shm_server_create": (ctypes.c_int, [P, P, P, P, P]),
         "shm_submit": (ctypes.c_int, [P, P, P, i32, P, P]),
@@ -259,6 +265,30 @@ class SketchIndex:
         seq, off = pack([s for _, s in records])
         return cls(ctx, [n for n, _ in records], seq, off, k, h_frac, max_matches)
 
+    @classmethod
+    def from_device_fasta(cls, ctx: Context, fa: "DeviceFasta", k: int, h_frac: float,
+                          max_matches: Optional[int] = None) -> "SketchIndex":
+        """The index of a FASTA parsed on the device (shm_index_build_fasta)."""
+        obj = cls.__new__(cls)
+        obj.ctx = ctx
+        obj.h = None
+        obj.names = list(fa.names)
+        obj.k, obj.h_frac = k, h_frac
+        h = ctypes.c_void_p()
+        _check(lib().shm_index_build_fasta(ctx.h, fa.h, k, h_frac, -1 if max_matches is None else max_matches,
+                                           ctypes.byref(h)))
+        obj.h = h
+        return obj
+
+    def map_device_fasta(self, params: Params, fa: "DeviceFasta", first: int = 0,
+                         n: Optional[int] = None) -> np.ndarray:
+        """Records of reads [first, first + n) of a FASTA parsed on the device (shm_map_fasta)."""
+        n = fa.n - first if n is None else n
+        out = np.zeros(n, RECORD_DTYPE)
+        cp = params.c()
+        _check(lib().shm_map_fasta(self.ctx.h, self.h, ctypes.byref(cp), fa.h, first, n, _ptr(out)))
+        return out
+
     def save(self, path: str) -> None:
         """Writes the index to a file (shm_index_save)."""
         _check(lib().shm_index_save(self.h, os.fsencode(path)))
@@ -367,6 +397,41 @@ class SketchIndex:
         _check(lib().shm_format_paf(self.h, ctypes.byref(cp), _ptr(records), len(records), joined,
                                     0 if mt is None else _ptr(mt), buf, need.value, ctypes.byref(need)))
         return buf.raw[:need.value].decode()
+
+
+class DeviceFasta:
+    """A FASTA file's bytes parsed on the device (shm_fasta_parse_device): the
+    sequences stay in device memory; names and offsets come back."""
+
+    def __init__(self, ctx: Context, data: bytes):
+        buf = np.frombuffer(data, np.uint8)
+        h = ctypes.c_void_p()
+        _check(lib().shm_fasta_parse_device(ctx.h, _ptr(buf), len(buf), ctypes.byref(h)))
+        self.h = h
+        n = ctypes.c_int32()
+        offs = ctypes.POINTER(ctypes.c_int64)()
+        names = ctypes.c_char_p()
+        _check(lib().shm_fasta_records(h, ctypes.byref(n), ctypes.byref(offs), ctypes.byref(names)))
+        self.n = n.value
+        self.offs = np.ctypeslib.as_array(offs, (self.n + 1,)).copy()
+        self.names = names.value.decode(errors="replace").split("\n") if self.n else []
+
+    def seq(self) -> np.ndarray:
+        out = np.zeros(int(self.offs[-1]), np.uint8)
+        if out.size:
+            _check(lib().shm_fasta_copy_seq(self.h, _ptr(out)))
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            lib().shm_fasta_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:
