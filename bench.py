@@ -316,6 +316,31 @@ def run_ours(args, rank, world, local):
                "device_s": round(min(ts[1:]), 4), "host_over_device": round(t_h / min(ts[1:]), 1)}
         log(f"[bench] PAF text: {paf}")
 
+    fasta_parse = None
+    if rank == 0:  # reads as FASTA bytes (pinned host memory), parsed on the device
+        m = min(n, 20000)
+        parts = []
+        for i in range(m):
+            parts.append(b">read%d\n" % i)
+            parts.append(seq[offs[i]:offs[i + 1]].tobytes())
+            parts.append(b"\n")
+        raw = b"".join(parts)
+        del parts
+        pin = torch.empty(len(raw), dtype=torch.uint8).pin_memory()
+        pin.copy_(torch.frombuffer(bytearray(raw), dtype=torch.uint8))
+        pin_np = pin.numpy()
+        sb.DeviceFasta(ctx, pin_np).close()  # warm-up
+        t0 = time.perf_counter()
+        fa = sb.DeviceFasta(ctx, pin_np)
+        t_fa = time.perf_counter() - t0
+        if fa.n != m or not np.array_equal(fa.offs, offs[: m + 1] - offs[0]):
+            raise RuntimeError("reads parsed on the device differ from the workload's")
+        fa.close()
+        fasta_parse = {"reads": m, "bytes": len(raw), "s": round(t_fa, 4),
+                       "gb_per_s": round(len(raw) / t_fa / 1e9, 1),
+                       "what": "shm_fasta_parse_device from pinned host memory, upload included"}
+        log(f"[bench] FASTA parse: {fasta_parse}")
+
     serving = None
     if rank == 0 and args.serve_seconds > 0:
         serving = serve_load(ctx, idx, p, h_seq_np, offs, rec, [10_000, 50_000, 200_000, 1_000_000],
@@ -388,6 +413,8 @@ def run_ours(args, rank, world, local):
             result["serving"] = serving
         if paf:
             result["paf_text"] = paf
+        if fasta_parse:
+            result["fasta_parse"] = fasta_parse
         if plain:
             result["plain_form"] = {"reads_per_s": round(plain["reads_per_s"], 1), "sample_reads": plain["sample_reads"],
                                     "batched_e2e_over_plain": round(e2e_value / plain["reads_per_s"], 1)}
