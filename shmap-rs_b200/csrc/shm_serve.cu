@@ -26,6 +26,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <exception>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -170,6 +171,9 @@ static void run_slot(Server* S, Slot* sl) {
         } catch (const std::bad_alloc&) {
             status = SHM_ERR_NOMEM;
             err = "host allocation failed";
+        } catch (const std::exception& e) {  // reported to the batch's requests; the slot carries on
+            status = SHM_ERR_CUDA;
+            err = std::string("internal error: ") + e.what();
         }
         {
             std::lock_guard<std::mutex> lk(S->mu);
