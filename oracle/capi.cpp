@@ -32,6 +32,7 @@ struct orc_params {
     double theta, min_diff, max_overlap;
     int32_t metric;  // 0 Containment, 1 Jaccard, 2 bucket_SH, 3 bucket_LCS
     int32_t no_bucket_pruning, one_sweep, abs_pos;
+    double rarity_weight, rarity_tiebreak, rarity_alpha;  // params.rs:76-112
 };
 
 static Params to_params(const orc_params* p) {
@@ -46,6 +47,9 @@ static Params to_params(const orc_params* p) {
     q.no_bucket_pruning = p->no_bucket_pruning != 0;
     q.one_sweep = p->one_sweep != 0;
     q.abs_pos = p->abs_pos != 0;
+    q.rarity_weight = p->rarity_weight;
+    q.rarity_tiebreak = p->rarity_tiebreak;
+    q.rarity_alpha = p->rarity_alpha;
     return q;
 }
 

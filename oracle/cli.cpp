@@ -38,6 +38,9 @@ int main(int argc, char** argv) {
         else if (a == "-P" || a == "--no_bucket_pruning") p.no_bucket_pruning = true;
         else if (a == "-B" || a == "--one_sweep") p.one_sweep = true;
         else if (a == "-F" || a == "--abs_pos") p.abs_pos = true;
+        else if (a == "--rarity-weight") p.rarity_weight = std::atof(val().c_str());
+        else if (a == "--rarity-tiebreak") p.rarity_tiebreak = std::atof(val().c_str());
+        else if (a == "--rarity-alpha") p.rarity_alpha = std::atof(val().c_str());
         else if (a == "-m" || a == "--metric") {
             std::string m = val();
             if (m == "Containment") p.metric = Metric::Containment;
@@ -53,6 +56,10 @@ int main(int argc, char** argv) {
     if (p.max_matches != -1 && p.max_matches <= 0) die("The number of seed matches (-M) should be positive.");
     if (p.theta < 0.0 || p.theta > 1.0) die("The threshold (-t) should be between 0 and 1.");
     if (p.min_diff < 0.0) die("The minimum difference (-d) should be >= 0.");
+    if (p.rarity_weight < 0.0 || p.rarity_weight > 4.0)
+        die("The rarity weight (--rarity-weight) should be between 0 and 4.");
+    if (p.rarity_weight > 0.0 && p.metric != Metric::Containment)
+        die("--rarity-weight is only defined for -m Containment.");
     if (p.max_overlap < 0.0 || p.max_overlap > 1.0) die("The maximum overlap (-o) should be between 0 and 1.");
     if (p.threads <= 0) die("The number of threads (-@) should be positive.");
     if (t_file.empty() || p_file.empty()) die("both -s and -p are required");

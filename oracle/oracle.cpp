@@ -572,6 +572,10 @@ struct Ctx {
     const SketchIndex& tidx;
     const Params& p;
     int64_t total_matches = 0, seed_matches = 0, max_seed_matches = 0, final_buckets = 0;
+    // rarity weights of the read's seeds by seed_num and their total over its
+    // k-mers (src/shmap/mod.rs:341-352, 694-723); empty when no rarity flag is on
+    std::vector<double> rarity;
+    double m_weight = 0.0;
 };
 
 // p_ht: hash -> index into p_unique (the reference stores a Seed clone; same content)
@@ -733,7 +737,9 @@ inline double mapping_score(QPos inter, QPos m, QPos s_sz, Metric metric) {
     return (double)inter / (double)m;
 }
 
-// src/shmap/scoring.rs:189-291 (the rarity weighting is not part of this path)
+// src/shmap/scoring.rs:189-291; the rarity-weighted support runs beside
+// the count (scoring.rs:214-217, 240, 259, 280) and, under --rarity-weight,
+// is the score
 Mapping best_fixed_length(Ctx& cx, const RefSegment& segm, RPos from, RPos to, const PHt& p_ht,
                           const std::vector<Seed>& pu, std::vector<QPos>& diff_hist, QPos p_sz, QPos m,
                           Metric metric) {
@@ -743,6 +749,9 @@ Mapping best_fixed_length(Ctx& cx, const RefSegment& segm, RPos from, RPos to, c
     QPos inter = 0;
     int32_t same = 0;
     Mapping best;
+    const bool weighted = !cx.rarity.empty();
+    const bool score_weighted = weighted && cx.p.rarity_weight > 0.0;
+    double w_inter = 0.0;
     while (l < end) {
         const Kmer& tl = t[(size_t)l];
         while (r < end) {
@@ -754,13 +763,18 @@ Mapping best_fixed_length(Ctx& cx, const RefSegment& segm, RPos from, RPos to, c
                 same += seed.kmer.strand == tr.strand ? 1 : -1;
                 QPos& cnt = diff_hist[(size_t)seed.seed_num];
                 cnt -= 1;
-                if (cnt >= 0) inter += 1;
+                if (cnt >= 0) {
+                    inter += 1;
+                    if (weighted) w_inter += cx.rarity[(size_t)seed.seed_num];
+                }
             }
             r += 1;
         }
         QPos s_kmers = r - l;
-        double score = mapping_score(inter, m, s_kmers, metric);
+        double score = score_weighted ? std::min(std::max(w_inter / cx.m_weight, 0.0), 1.0)
+                                      : mapping_score(inter, m, s_kmers, metric);
         if (l < r && score > best.score()) {
+            best.rarity_support = w_inter;
             best.update(0, p_sz - 1, t[(size_t)l].r, t[(size_t)(r - 1)].r, segm, inter, score, same,
                         t[(size_t)(r - 1)].r - t[(size_t)l].r + 1);
         }
@@ -769,7 +783,10 @@ Mapping best_fixed_length(Ctx& cx, const RefSegment& segm, RPos from, RPos to, c
             same -= seed.kmer.strand == tl.strand ? 1 : -1;
             QPos& cnt = diff_hist[(size_t)seed.seed_num];
             cnt += 1;
-            if (cnt >= 1) inter -= 1;
+            if (cnt >= 1) {
+                inter -= 1;
+                if (weighted) w_inter -= cx.rarity[(size_t)seed.seed_num];
+            }
         }
         l += 1;
     }
@@ -865,7 +882,10 @@ bool match_rest(Ctx& cx, QPos p_sz, QPos m, QPos lmax, const Buckets& bk,
         BucketContent& content = sorted[idx].second;
         double sh = 1.0;
         if (!seed_heuristic_pass(cx, bk, rs.pu, m, b, content, sh, thr)) continue;
-        const double admit = thr;
+        // scoring.rs:412-416: under a tie-break band a bucket slightly below
+        // the incumbent is still scored
+        const double tb = cx.p.rarity_tiebreak;
+        const double admit = tb > 0.0 ? thr - tb * std::fabs(thr) : thr;
         long memo = memoizable ? cache.lookup((uint32_t)idx) : -1;
         bool got = false;
         Mapping bib;
@@ -886,7 +906,11 @@ bool match_rest(Ctx& cx, QPos p_sz, QPos m, QPos lmax, const Buckets& bk,
         if (got) {
             cx.final_buckets += 1;
             if (!forbidden || Mapping::overlap(bib, *forbidden) < max_overlap) {
-                bool take = !have || bib.score() > best.score();
+                bool take = !have;
+                if (have) {  // scoring.rs:453-470: scores within the band are decided by rarity support
+                    const bool tied = tb > 0.0 && std::fabs(bib.score() - best.score()) <= tb * std::fabs(best.score());
+                    take = tied ? bib.rarity_support > best.rarity_support : bib.score() > best.score();
+                }
                 if (take) {
                     thr = std::max(thr, bib.score());
                     best = bib;
@@ -916,7 +940,7 @@ QPos lcs_window(const std::vector<Kmer>& t, RPos bgn, RPos end, const std::vecto
 ReadResult map_read(const SketchIndex& tidx, const FracMinHash& sk, const Params& p, const uint8_t* seq, size_t len,
                     Buckets& bk) {
     ReadResult rr;
-    Ctx cx{tidx, p};
+    Ctx cx{tidx, p, 0, 0, 0, 0, {}, 0.0};
     bk.clear();
     std::vector<Kmer> pk = sk.sketch(seq, len);
     const QPos m = (QPos)pk.size();
@@ -942,6 +966,21 @@ ReadResult map_read(const SketchIndex& tidx, const FracMinHash& sk, const Params
         bool ins;
         p_ht.get_or_insert(pu[i].kmer.h, &ins) = (int32_t)i;
         diff_hist[(size_t)pu[i].seed_num] = pu[i].occs_in_p;
+    }
+    // src/shmap/mod.rs:694-723: rarity weights 1 / max(hits, 1)^alpha, in
+    // rarest-first seed order; alpha follows --rarity-alpha, else
+    // --rarity-weight, else 1 when only the tie-break is on
+    const double alpha = p.rarity_alpha > 0.0    ? p.rarity_alpha
+                         : p.rarity_weight > 0.0 ? p.rarity_weight
+                         : p.rarity_tiebreak > 0.0 ? 1.0
+                                                   : 0.0;
+    if (alpha > 0.0) {
+        cx.rarity.assign(pu.size(), 0.0);
+        for (const Seed& sd : pu) {
+            const double w = std::pow((double)std::max<RPos>(sd.hits_in_t, 1), -alpha);
+            cx.rarity[(size_t)sd.seed_num] = w;
+            cx.m_weight += w * (double)sd.occs_in_p;
+        }
     }
     const QPos lmax = m;
     const double theta = p.theta;

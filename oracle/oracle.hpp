@@ -161,6 +161,9 @@ struct Params {
     bool no_bucket_pruning = false;  // -P (NBP)
     bool one_sweep = false;          // -B (OS)
     bool abs_pos = false;            // -F (AP)
+    double rarity_weight = 0.0;      // --rarity-weight (params.rs:76-77)
+    double rarity_tiebreak = 0.0;    // --rarity-tiebreak (params.rs:95-96)
+    double rarity_alpha = 0.0;       // --rarity-alpha (params.rs:111-112)
     int threads = 1;
 };
 
@@ -184,6 +187,7 @@ struct Mapping {
     BucketLoc bucket, bucket2;
     QPos intersection2 = -1;
     double sigmas_diff = -1.0;
+    double rarity_support = 0.0;  // mapping.rs:124-128 (never printed)
     // GlobalMappingStats
     bool has_global = false;
     QPos g_k = -1, g_seeds = -1;

@@ -28,7 +28,8 @@ class OParams(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int32), ("h_frac", ctypes.c_double), ("max_matches", ctypes.c_int32),
                 ("theta", ctypes.c_double), ("min_diff", ctypes.c_double), ("max_overlap", ctypes.c_double),
                 ("metric", ctypes.c_int32), ("no_bucket_pruning", ctypes.c_int32), ("one_sweep", ctypes.c_int32),
-                ("abs_pos", ctypes.c_int32)]
+                ("abs_pos", ctypes.c_int32), ("rarity_weight", ctypes.c_double), ("rarity_tiebreak", ctypes.c_double),
+                ("rarity_alpha", ctypes.c_double)]
 
 
 RECORD_DTYPE = np.dtype(
@@ -77,9 +78,11 @@ def _p(a: np.ndarray) -> int:
 
 
 def params(k=15, h_frac=0.05, max_matches=None, theta=0.9, min_diff=0.02, max_overlap=0.5, metric="Containment",
-           no_bucket_pruning=False, one_sweep=False, abs_pos=False) -> OParams:
+           no_bucket_pruning=False, one_sweep=False, abs_pos=False, rarity_weight=0.0, rarity_tiebreak=0.0,
+           rarity_alpha=0.0) -> OParams:
     return OParams(k, h_frac, -1 if max_matches is None else max_matches, theta, min_diff, max_overlap,
-                   METRICS[metric], int(no_bucket_pruning), int(one_sweep), int(abs_pos))
+                   METRICS[metric], int(no_bucket_pruning), int(one_sweep), int(abs_pos), rarity_weight,
+                   rarity_tiebreak, rarity_alpha)
 
 
 def sketch(seq: bytes, k: int, h_frac: float, offset: int = 0):

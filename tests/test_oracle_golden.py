@@ -239,3 +239,67 @@ def test_lcs_matches_the_definition(seed):
     for bgn, end in [(0, 60), (7, 31), (40, 80), (59, 60), (5, 5)]:
         pp = [x for _, h in t[bgn:min(end, len(t))] if h in seeds for x in seeds[h]]
         assert O.lcs(t, bgn, end, seeds) == max(_lis_brute(pp), _lis_brute(pp[::-1]))
+
+
+def _rarity_workload(seed=31, n=150):
+    ref = lcg_dna(seed, 400_000)
+    rep = lcg_dna(seed + 1, 3000)
+    ref_rep = ref[:100_000] + rep * 6 + ref[100_000:200_000] + rep * 4 + ref[200_000:]  # copies of one repeat
+    rng = np.random.default_rng(seed)
+    comp = bytes.maketrans(b"ACGT", b"TGCA")
+    reads = []
+    for i in range(n):
+        L = int(rng.integers(2000, 6000))
+        a = int(rng.integers(0, len(ref_rep) - L))
+        r = bytearray(ref_rep[a:a + L])
+        for j in rng.integers(0, L, L // 50):
+            r[j] = b"ACGT"[int(rng.integers(0, 4))]
+        r = bytes(r)
+        reads.append(r.translate(comp)[::-1] if i % 2 else r)
+    return ref, ref_rep, reads
+
+
+def test_rarity_weight_is_containment_when_every_kmer_is_unique():
+    """src/shmap/mod.rs:694-723, scoring.rs:214-281: with hits_in_t = 1 for
+    every seed all weights are 1, the weighted support is the count and the
+    weighted score is Containment's, record for record."""
+    ref, _, reads = _rarity_workload()
+    idx = O.Index.from_records([("u", ref)], 21, 0.1)
+    # the reads none of whose sketched k-mers occurs twice in the reference
+    unique = [r for r in reads if (idx.count(O.sketch(r, 21, 0.1)[1]) <= 1).all()]
+    assert len(unique) >= 40
+    seq, offs = pack(unique)
+    base = idx.map_reads(O.params(k=21, h_frac=0.1, theta=0.3), seq, offs, threads=4)
+    assert (base["status"] == 0).mean() > 0.9
+    for alpha in (0.5, 1.0, 2.0):
+        w = idx.map_reads(O.params(k=21, h_frac=0.1, theta=0.3, rarity_weight=alpha), seq, offs, threads=4)
+        assert np.array_equal(w.view(np.uint8), base.view(np.uint8)), alpha
+
+
+def test_rarity_tiebreak_only_admits_more():
+    """scoring.rs:409-481: the band lowers the admission bar and decides near
+    ties by rarity support; a read mapped without it stays mapped."""
+    _, ref_rep, reads = _rarity_workload()
+    idx = O.Index.from_records([("r", ref_rep)], 15, 0.2)
+    seq, offs = pack(reads)
+    base = idx.map_reads(O.params(k=15, h_frac=0.2, theta=0.3), seq, offs, threads=4)
+    for band, alpha in ((0.01, 0.0), (0.05, 1.0), (0.2, 2.0)):
+        tb = idx.map_reads(O.params(k=15, h_frac=0.2, theta=0.3, rarity_tiebreak=band, rarity_alpha=alpha), seq,
+                           offs, threads=4)
+        mapped_base = base["status"] == 0
+        assert (tb["status"][mapped_base] == 0).all(), band
+    wt = idx.map_reads(O.params(k=15, h_frac=0.2, theta=0.3, rarity_weight=1.0), seq, offs, threads=4)
+    ok = wt["status"] == 0
+    assert ok.any() and ((wt["score"][ok] >= 0.0) & (wt["score"][ok] <= 1.0)).all()
+    assert not np.array_equal(wt["score"][ok], base["score"][ok])  # repeats are down-weighted
+
+
+def test_rarity_flag_validation(golden_dir):
+    """src/params.rs:223-242."""
+    args = ["-s", os.path.join(golden_dir, "tiny_ref.fa"), "-p", os.path.join(golden_dir, "tiny_reads.fa"), "-k", "8"]
+    r = O.run_cli(args + ["--rarity-weight", "5"])
+    assert r.returncode != 0 and "rarity weight" in r.stderr
+    r = O.run_cli(args + ["--rarity-weight", "1", "-m", "Jaccard"])
+    assert r.returncode != 0 and "only defined for -m Containment" in r.stderr
+    r = O.run_cli(args + ["-r", "1.0", "-t", "0.1", "--rarity-tiebreak", "0.01"])
+    assert r.returncode == 0 and len(r.stdout.splitlines()) == 2
