@@ -549,9 +549,12 @@ def main():
         timed = rates[args.warmup:] or rates
         v = statistics.mean(timed)
         line = {"metric": "reads/s (mapping, byte-identical PAF records)", "value": round(v, 1), "unit": "reads/s",
-                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(len(names) / v * 1e3, 3), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
-                "config": {"workload": args.workload, "description": wk["desc"]},
+                "config": {"workload": args.workload, "description": wk["desc"], "reads_per_gpu": len(names),
+                           "bases_per_gpu": int(offs[-1]), "k": wk["k"], "r": wk["r"], "theta": wk["theta"],
+                           "metric": wk["metric"], "scale": args.scale, "host_cores": threads},
                 "cpu_baseline": {"value": round(v, 1), "unit": "reads/s", "cores": threads, "kind": "port",
                                  "sample": sample},
                 "e2e": {"value": round(v, 1), "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
