@@ -136,6 +136,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def _extra(name: str, fn):
+    """Runs one of the side measurements (index file, PAF text, FASTA parse,
+    serving); a failure is reported under its key in the JSON line instead of
+    ending the run."""
+    try:
+        return fn()
+    except Exception as e:  # noqa: BLE001 - reported, not hidden
+        log(f"[bench] {name} failed: {e!r}")
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def make_workload(name: str, rank: int, scale: float, metric_override: str | None = None):
     from shmap_b200 import synth
 
@@ -194,8 +205,7 @@ def run_ours(args, rank, world, local):
     index_s = time.time() - t0
     st = idx.stats()
     log(f"[bench] rank {rank}: index on device in {index_s:.2f}s: {st}")
-    index_file = None
-    if rank == 0:  # the index written to a file and read back (shm_index_save / shm_index_load)
+    def _index_file():  # the index written to a file and read back (shm_index_save / shm_index_load)
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "ref.shmapidx")
             t0 = time.time()
@@ -207,8 +217,12 @@ def run_ours(args, rank, world, local):
             load_s = time.time() - t0
             if back.stats() != st:
                 raise RuntimeError("the index read back differs from the one built")
-            index_file = {"bytes": os.path.getsize(path), "save_s": round(save_s, 3), "load_s": round(load_s, 3)}
+            res = {"bytes": os.path.getsize(path), "save_s": round(save_s, 3), "load_s": round(load_s, 3)}
             back.close()
+            return res
+
+    index_file = _extra("index_file", _index_file) if rank == 0 else None
+
     p = sb.Params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=wk["metric"])
     n = len(names)
     nbytes = int(offs[-1])
@@ -290,8 +304,7 @@ def run_ours(args, rank, world, local):
     if not np.array_equal(h_out.view(np.uint8), rec.view(np.uint8)):
         raise RuntimeError("e2e records differ from the device-resident records")
 
-    paf = None
-    if rank == 0:  # the PAF text of the step's records: shm_format_paf (host) and shm_format_paf_device
+    def _paf():  # the PAF text of the step's records: shm_format_paf (host) and shm_format_paf_device
         joined = "\n".join(names).encode()
         cp = p.c()
         need = ctypes.c_int64()
@@ -312,12 +325,14 @@ def run_ours(args, rank, world, local):
             ts.append(time.perf_counter() - t0)
         if not np.array_equal(buf_h, buf_d):
             raise RuntimeError("PAF text rendered on the device differs from the host's")
-        paf = {"bytes": cap, "lines": int((rec["status"] == 0).sum()), "host_s": round(t_h, 4),
+        res = {"bytes": cap, "lines": int((rec["status"] == 0).sum()), "host_s": round(t_h, 4),
                "device_s": round(min(ts[1:]), 4), "host_over_device": round(t_h / min(ts[1:]), 1)}
-        log(f"[bench] PAF text: {paf}")
+        log(f"[bench] PAF text: {res}")
+        return res
 
-    fasta_parse = None
-    if rank == 0:  # reads as FASTA bytes (pinned host memory), parsed on the device
+    paf = _extra("paf", _paf) if rank == 0 else None
+
+    def _fasta_parse():  # reads as FASTA bytes (pinned host memory), parsed on the device
         m = min(n, 20000)
         parts = []
         for i in range(m):
@@ -336,16 +351,20 @@ def run_ours(args, rank, world, local):
         if fa.n != m or not np.array_equal(fa.offs, offs[: m + 1] - offs[0]):
             raise RuntimeError("reads parsed on the device differ from the workload's")
         fa.close()
-        fasta_parse = {"reads": m, "bytes": len(raw), "s": round(t_fa, 4),
-                       "gb_per_s": round(len(raw) / t_fa / 1e9, 1),
-                       "what": "shm_fasta_parse_device from pinned host memory, upload included"}
-        log(f"[bench] FASTA parse: {fasta_parse}")
+        res = {"reads": m, "bytes": len(raw), "s": round(t_fa, 4), "gb_per_s": round(len(raw) / t_fa / 1e9, 1),
+               "what": "shm_fasta_parse_device from pinned host memory, upload included"}
+        log(f"[bench] FASTA parse: {res}")
+        return res
 
-    serving = None
-    if rank == 0 and args.serve_seconds > 0:
-        serving = serve_load(ctx, idx, p, h_seq_np, offs, rec, [10_000, 50_000, 200_000, 1_000_000],
-                             args.serve_seconds, 11)
-        log(f"[bench] serving: {serving}")
+    fasta_parse = _extra("fasta_parse", _fasta_parse) if rank == 0 else None
+
+    def _serving():
+        res = serve_load(ctx, idx, p, h_seq_np, offs, rec, [10_000, 50_000, 200_000, 1_000_000],
+                         args.serve_seconds, 11)
+        log(f"[bench] serving: {res}")
+        return res
+
+    serving = _extra("serving", _serving) if rank == 0 and args.serve_seconds > 0 else None
 
     # plain one-read-per-launch form on a sample
     plain = None
