@@ -8,6 +8,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
+#include <string>
 #include <thread>
 
 namespace oracle {
@@ -322,6 +324,8 @@ public:
         prop_seeds = 0;
         merged = true;
     }
+    bool dense_on = false;  // the dense accumulator is in use (read by the tests)
+
     bool set_halflen(QPos h) {  // buckets.rs:348-356
         halflen = h;
         if (halflen < MIN_HALFLEN) {
@@ -388,7 +392,6 @@ private:
     QPos prop_seeds = 0;
     std::vector<Slot> dense;
     std::vector<uint32_t> seg_base;
-    bool dense_on = false;
     std::vector<uint32_t> touched;
     size_t dense_slots = 0;
     bool dense_dirty = false;
@@ -936,6 +939,20 @@ QPos lcs_window(const std::vector<Kmer>& t, RPos bgn, RPos end, const std::vecto
     return lcs(t, bgn, end, p_ht, pu, seed_pos);
 }
 
+// The positions of each run of equal hashes of a sketch sorted by
+// (h asc, r desc), by seed_num: the pmatches of src/shmap/seeding.rs:45-56.
+static std::vector<std::vector<QPos>> group_positions(const std::vector<Kmer>& pk, size_t n_groups) {
+    std::vector<std::vector<QPos>> pm(n_groups);
+    size_t gs = 0, gi = 0;
+    for (size_t ppos = 0; ppos < pk.size(); ppos++)
+        if (ppos + 1 == pk.size() || pk[ppos].h != pk[ppos + 1].h) {
+            for (size_t q = gs; q <= ppos; q++) pm[gi].push_back(pk[q].r);
+            gi++;
+            gs = ppos + 1;
+        }
+    return pm;
+}
+
 // src/shmap/mod.rs:653-971
 ReadResult map_read(const SketchIndex& tidx, const FracMinHash& sk, const Params& p, const uint8_t* seq, size_t len,
                     Buckets& bk) {
@@ -949,16 +966,7 @@ ReadResult map_read(const SketchIndex& tidx, const FracMinHash& sk, const Params
     // pmatches (positions of each distinct hash, decreasing) for bucket_LCS only
     std::vector<std::vector<QPos>> pmatches;
     std::vector<Seed> pu = unique_elements_with_info(cx, pk);
-    if (p.metric == Metric::BucketLcs) {
-        pmatches.resize(pu.size());
-        size_t gs = 0, gi = 0;
-        for (size_t ppos = 0; ppos < pk.size(); ppos++)
-            if (ppos + 1 == pk.size() || pk[ppos].h != pk[ppos + 1].h) {
-                for (size_t q = gs; q <= ppos; q++) pmatches[gi].push_back(pk[q].r);
-                gi++;
-                gs = ppos + 1;
-            }
-    }
+    if (p.metric == Metric::BucketLcs) pmatches = group_positions(pk, pu.size());
     PHt p_ht;
     p_ht.reserve(pu.size());
     std::vector<QPos> diff_hist(pu.size(), 0);
@@ -1100,3 +1108,108 @@ bool read_fasta(const std::string& path, std::vector<FastaRecord>& out, std::str
 }
 
 }  // namespace oracle
+
+// Test hooks (test infrastructure): the bucket accumulator, Mapping and the
+// seed grouping driven directly, for the reference's own unit tests of them
+// (src/buckets.rs:748-957, src/mapping.rs:445-495, src/shmap/seeding.rs:221-245).
+namespace {
+struct OrcBuckets {
+    oracle::SketchIndex idx;
+    oracle::Buckets b;
+    OrcBuckets(int32_t sz, int32_t n_kmers, bool ap) : b(idx, ap) {
+        oracle::RefSegment sg;
+        sg.kmers.assign((size_t)n_kmers, oracle::Kmer{0, 0, false});
+        sg.name = "seg0";
+        sg.sz = sz;
+        sg.id = 0;
+        idx.segments.push_back(std::move(sg));
+    }
+};
+struct OrcMapping {
+    oracle::Mapping m;
+    std::vector<std::unique_ptr<oracle::RefSegment>> segs;
+};
+}  // namespace
+
+extern "C" {
+void* orc_buckets_new(int32_t seg_sz, int32_t n_kmers, int32_t ap) { return new OrcBuckets(seg_sz, n_kmers, ap != 0); }
+void orc_buckets_free(void* p) { delete (OrcBuckets*)p; }
+int32_t orc_buckets_set_halflen(void* p, int32_t h) { return ((OrcBuckets*)p)->b.set_halflen(h) ? 1 : 0; }
+int32_t orc_buckets_dense_on(void* p) { return ((OrcBuckets*)p)->b.dense_on ? 1 : 0; }
+int32_t orc_buckets_begin(void* p, int32_t segm, int32_t bb) {
+    return ((OrcBuckets*)p)->b.begin(oracle::BucketLoc{segm, bb});
+}
+int32_t orc_buckets_end(void* p, int32_t segm, int32_t bb) { return ((OrcBuckets*)p)->b.end(oracle::BucketLoc{segm, bb}); }
+void orc_buckets_add_to_pos(void* p, int32_t r, int32_t tpos, int32_t segm, int32_t matches, int32_t seeds,
+                            int32_t codir, int32_t rmin, int32_t rmax) {
+    oracle::BucketContent c;
+    c.matches = matches;
+    c.seeds = seeds;
+    c.codirection = codir;
+    c.r_min = rmin;
+    c.r_max = rmax;
+    ((OrcBuckets*)p)->b.add_to_pos(oracle::Hit{r, tpos, false, segm}, c);
+}
+void orc_buckets_propagate(void* p) { ((OrcBuckets*)p)->b.propagate_seeds_to_buckets(); }
+void orc_buckets_clear(void* p) { ((OrcBuckets*)p)->b.clear(); }
+// Sorted buckets as 6 ints each: segm_id, b, matches, codirection, r_min, r_max.
+int64_t orc_buckets_sorted(void* p, int32_t* out, int64_t cap) {
+    auto v = ((OrcBuckets*)p)->b.get_sorted_buckets();
+    for (size_t i = 0; i < v.size() && (int64_t)i < cap; i++) {
+        const auto& [loc, c] = v[i];
+        int32_t* o = out + 6 * i;
+        o[0] = loc.segm_id;
+        o[1] = loc.b;
+        o[2] = c.matches;
+        o[3] = c.codirection;
+        o[4] = c.r_min;
+        o[5] = c.r_max;
+    }
+    return (int64_t)v.size();
+}
+
+void* orc_mapping_new(void) { return new OrcMapping(); }
+void orc_mapping_free(void* p) { delete (OrcMapping*)p; }
+void orc_mapping_update(void* p, int32_t ps, int32_t pe, int32_t tl, int32_t tr, int32_t seg_id, int32_t seg_sz,
+                        int32_t inter, double score, int32_t same, int32_t sz) {
+    auto* o = (OrcMapping*)p;
+    auto sg = std::make_unique<oracle::RefSegment>();
+    sg->name = "chr" + std::to_string(seg_id + 1);
+    sg->sz = seg_sz;
+    sg->id = seg_id;
+    o->m.update(ps, pe, tl, tr, *sg, inter, score, same, sz);
+    o->segs.push_back(std::move(sg));
+}
+void orc_mapping_get(void* p, double* score, int32_t* t_l, char* strand) {
+    auto* o = (OrcMapping*)p;
+    *score = o->m.score();
+    *t_l = o->m.t_l;
+    *strand = o->m.strand;
+}
+double orc_mapping_overlap(void* a, void* b) { return oracle::Mapping::overlap(((OrcMapping*)a)->m, ((OrcMapping*)b)->m); }
+int32_t orc_mapping_calc_mapq(void* p, double theta2, double min_diff) {
+    return ((OrcMapping*)p)->m.calc_mapq(theta2, min_diff);
+}
+// Seeds of a sketch (r, h, strand) against an empty index, in the order
+// unique_elements_with_info returns them: hash, occurrences and pmatches
+// (pm[pm_off[i] .. pm_off[i + 1])). Returns the number of seeds.
+int64_t orc_seed_groups(const int32_t* r, const uint64_t* h, const uint8_t* strand, int32_t n, uint64_t* out_h,
+                        int32_t* out_occ, int32_t* pm_off, int32_t* pm) {
+    oracle::SketchIndex idx;
+    oracle::Params prm;
+    oracle::Ctx cx{idx, prm, 0, 0, 0, 0, {}, 0.0};
+    std::vector<oracle::Kmer> pk((size_t)n);
+    for (int32_t i = 0; i < n; i++) pk[(size_t)i] = oracle::Kmer{r[i], h[i], strand[i] != 0};
+    std::vector<oracle::Seed> pu = oracle::unique_elements_with_info(cx, pk);
+    std::vector<std::vector<oracle::QPos>> pmv = oracle::group_positions(pk, pu.size());
+    int32_t at = 0;
+    for (size_t i = 0; i < pu.size(); i++) {
+        out_h[i] = pu[i].kmer.h;
+        out_occ[i] = pu[i].occs_in_p;
+        pm_off[i] = at;
+        for (oracle::QPos q : pmv[(size_t)pu[i].seed_num]) pm[at++] = q;
+    }
+    pm_off[pu.size()] = at;
+    return (int64_t)pu.size();
+}
+}  // extern "C"

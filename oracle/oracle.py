@@ -56,6 +56,23 @@ def lib():
             ("orc_sketch", i64, [P, i64, i32, dbl, i32, P, P, P, i64]),
             ("orc_h_thres", u64, [i32, dbl]),
             ("orc_lcs", i32, [P, P, i32, i32, i32, P, P, P, i32]),
+            ("orc_buckets_new", P, [i32, i32, i32]),
+            ("orc_buckets_free", None, [P]),
+            ("orc_buckets_set_halflen", i32, [P, i32]),
+            ("orc_buckets_dense_on", i32, [P]),
+            ("orc_buckets_begin", i32, [P, i32, i32]),
+            ("orc_buckets_end", i32, [P, i32, i32]),
+            ("orc_buckets_add_to_pos", None, [P, i32, i32, i32, i32, i32, i32, i32, i32]),
+            ("orc_buckets_propagate", None, [P]),
+            ("orc_buckets_clear", None, [P]),
+            ("orc_buckets_sorted", i64, [P, P, i64]),
+            ("orc_mapping_new", P, []),
+            ("orc_mapping_free", None, [P]),
+            ("orc_mapping_update", None, [P, i32, i32, i32, i32, i32, i32, i32, dbl, i32, i32]),
+            ("orc_mapping_get", None, [P, P, P, P]),
+            ("orc_mapping_overlap", dbl, [P, P]),
+            ("orc_mapping_calc_mapq", i32, [P, dbl, dbl]),
+            ("orc_seed_groups", i64, [P, P, P, i32, P, P, P, P]),
             ("orc_index_build", P, [P, P, i32, ctypes.c_char_p, i32, dbl, i32, i32]),
             ("orc_index_free", None, [P]),
             ("orc_index_stats", None, [P, P]),
@@ -105,6 +122,89 @@ def lcs(t, bgn: int, end: int, seeds) -> int:
     off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
     pos = np.array([x for v in seeds.values() for x in v] + [0], np.int32)
     return int(lib().orc_lcs(_p(t_r), _p(t_h), len(t), bgn, end, _p(sh), _p(off), _p(pos), len(sh)))
+
+
+class Buckets:
+    """The bucket accumulator (src/buckets.rs:305-724) over one segment 'seg0'
+    of sz bases holding n_kmers k-mers (test hook)."""
+
+    def __init__(self, sz: int, n_kmers: Optional[int] = None, ap: bool = False):
+        self.h = lib().orc_buckets_new(sz, sz if n_kmers is None else n_kmers, int(ap))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_buckets_free(self.h)
+
+    def set_halflen(self, h: int) -> bool:
+        return bool(lib().orc_buckets_set_halflen(self.h, h))
+
+    @property
+    def dense_on(self) -> bool:
+        return bool(lib().orc_buckets_dense_on(self.h))
+
+    def begin(self, segm: int, b: int) -> int:
+        return lib().orc_buckets_begin(self.h, segm, b)
+
+    def end(self, segm: int, b: int) -> int:
+        return lib().orc_buckets_end(self.h, segm, b)
+
+    def add_to_pos(self, r: int, tpos: int, segm: int, matches: int, seeds: int, codir: int, rmin: int, rmax: int):
+        lib().orc_buckets_add_to_pos(self.h, r, tpos, segm, matches, seeds, codir, rmin, rmax)
+
+    def propagate(self):
+        lib().orc_buckets_propagate(self.h)
+
+    def clear(self):
+        lib().orc_buckets_clear(self.h)
+
+    def sorted(self):
+        """[(segm_id, b, matches, codirection, r_min, r_max)] in get_sorted_buckets order."""
+        n = lib().orc_buckets_sorted(self.h, None, 0)
+        out = np.zeros(6 * max(n, 1), np.int32)
+        lib().orc_buckets_sorted(self.h, _p(out), n)
+        return [tuple(int(x) for x in out[6 * i:6 * i + 6]) for i in range(n)]
+
+
+class Mapping:
+    """A Mapping (src/mapping.rs:299-420) driven directly (test hook)."""
+
+    def __init__(self):
+        self.h = lib().orc_mapping_new()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_mapping_free(self.h)
+
+    def update(self, p_start, p_end, t_l, t_r, seg_id, seg_sz, intersection, score, same_strand, sz):
+        lib().orc_mapping_update(self.h, p_start, p_end, t_l, t_r, seg_id, seg_sz, intersection, score,
+                                 same_strand, sz)
+
+    def state(self):
+        sc, tl, st = ctypes.c_double(), ctypes.c_int32(), ctypes.c_char()
+        lib().orc_mapping_get(self.h, ctypes.byref(sc), ctypes.byref(tl), ctypes.byref(st))
+        return sc.value, tl.value, st.value.decode()
+
+    @staticmethod
+    def overlap(a: "Mapping", b: "Mapping") -> float:
+        return lib().orc_mapping_overlap(a.h, b.h)
+
+    def calc_mapq(self, theta2: float, min_diff: float) -> int:
+        return lib().orc_mapping_calc_mapq(self.h, theta2, min_diff)
+
+
+def seed_groups(kmers):
+    """unique_elements_with_info (src/shmap/seeding.rs:26-77) of [(r, h, strand)]
+    against an empty index: [(hash, occurrences, pmatches)] in seed order."""
+    n = len(kmers)
+    r = np.array([k[0] for k in kmers], np.int32)
+    h = np.array([k[1] for k in kmers], np.uint64)
+    st = np.array([int(k[2]) for k in kmers], np.uint8)
+    oh = np.zeros(max(n, 1), np.uint64)
+    occ = np.zeros(max(n, 1), np.int32)
+    off = np.zeros(n + 1, np.int32)
+    pm = np.zeros(max(n, 1), np.int32)
+    m = lib().orc_seed_groups(_p(r), _p(h), _p(st), n, _p(oh), _p(occ), _p(off), _p(pm))
+    return [(int(oh[i]), int(occ[i]), [int(x) for x in pm[off[i]:off[i + 1]]]) for i in range(m)]
 
 
 def h_thres(h_frac: float, k: int = 15) -> int:
