@@ -1212,4 +1212,35 @@ int64_t orc_seed_groups(const int32_t* r, const uint64_t* h, const uint8_t* stra
     pm_off[pu.size()] = at;
     return (int64_t)pu.size();
 }
+// read_fasta (src/io/mod.rs:383-427) of a file: *n records, *name_bytes
+// bytes of '\n'-joined names, *seq_bytes bases; with buffers given, also the
+// names, the bases back to back and n+1 offsets. Returns 0, or -1 with the
+// message in names (when it fits) on a read error.
+int32_t orc_read_fasta(const char* path, int64_t* n, int64_t* name_bytes, int64_t* seq_bytes, char* names,
+                       uint8_t* seq, int64_t* offs) {
+    std::vector<oracle::FastaRecord> recs;
+    std::string err;
+    if (!oracle::read_fasta(path, recs, &err)) return -1;
+    std::string joined;
+    int64_t total = 0;
+    for (size_t i = 0; i < recs.size(); i++) {
+        if (i) joined += '\n';
+        joined += recs[i].name;
+        total += (int64_t)recs[i].seq.size();
+    }
+    *n = (int64_t)recs.size();
+    *name_bytes = (int64_t)joined.size();
+    *seq_bytes = total;
+    if (names) std::memcpy(names, joined.data(), joined.size());
+    if (seq && offs) {
+        int64_t at = 0;
+        offs[0] = 0;
+        for (size_t i = 0; i < recs.size(); i++) {
+            std::memcpy(seq + at, recs[i].seq.data(), recs[i].seq.size());
+            at += (int64_t)recs[i].seq.size();
+            offs[i + 1] = at;
+        }
+    }
+    return 0;
+}
 }  // extern "C"

@@ -73,6 +73,7 @@ def lib():
             ("orc_mapping_overlap", dbl, [P, P]),
             ("orc_mapping_calc_mapq", i32, [P, dbl, dbl]),
             ("orc_seed_groups", i64, [P, P, P, i32, P, P, P, P]),
+            ("orc_read_fasta", i32, [ctypes.c_char_p, P, P, P, P, P, P]),
             ("orc_index_build", P, [P, P, i32, ctypes.c_char_p, i32, dbl, i32, i32]),
             ("orc_index_free", None, [P]),
             ("orc_index_stats", None, [P, P]),
@@ -205,6 +206,21 @@ def seed_groups(kmers):
     pm = np.zeros(max(n, 1), np.int32)
     m = lib().orc_seed_groups(_p(r), _p(h), _p(st), n, _p(oh), _p(occ), _p(off), _p(pm))
     return [(int(oh[i]), int(occ[i]), [int(x) for x in pm[off[i]:off[i + 1]]]) for i in range(m)]
+
+
+def read_fasta(path: str):
+    """The oracle's read_fasta (src/io/mod.rs:383-427): [(name, bases)]."""
+    n, nb, sb_ = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    if lib().orc_read_fasta(os.fsencode(path), ctypes.byref(n), ctypes.byref(nb), ctypes.byref(sb_), None, None,
+                            None) != 0:
+        raise ValueError(f"invalid FASTA record in {path}")
+    names = ctypes.create_string_buffer(nb.value + 1)
+    seq = np.zeros(max(sb_.value, 1), np.uint8)
+    offs = np.zeros(n.value + 1, np.int64)
+    lib().orc_read_fasta(os.fsencode(path), ctypes.byref(n), ctypes.byref(nb), ctypes.byref(sb_), names, _p(seq),
+                         _p(offs))
+    nm = names.raw[:nb.value].decode().split("\n") if n.value else []
+    return [(nm[i], seq[offs[i]:offs[i + 1]].tobytes()) for i in range(n.value)]
 
 
 def h_thres(h_frac: float, k: int = 15) -> int:

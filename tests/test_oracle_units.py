@@ -1,7 +1,9 @@
-"""The reference's own unit tests of the bucket accumulator, Mapping and the
-seed grouping, restated on the oracle through its test hooks: the known
-answers of src/buckets.rs:748-957, src/mapping.rs:445-495 and
-src/shmap/seeding.rs:221-245."""
+"""The reference's own unit tests of the bucket accumulator, bucket content,
+Mapping, the seed grouping and the FASTA reader, restated on the oracle
+through its test hooks (and, for the reader, on the package's reader that the
+device parser is compared with): the known answers of src/buckets.rs:748-957,
+src/types.rs:329-339, src/mapping.rs:445-495, src/shmap/seeding.rs:221-245
+and src/io/mod.rs:435-580."""
 import oracle as O
 
 
@@ -103,6 +105,17 @@ def test_an_abandoned_read_does_not_leak_into_the_next_dense_read():
     assert len(out) == 2 and all(x[2] == 1 for x in out)
 
 
+def test_bucket_content_add_assign_merges_ranges_and_sums():
+    """src/types.rs:329-339, through the accumulator: two contents in one bucket."""
+    b = O.Buckets(100)
+    b.set_halflen(10)
+    b.add_to_pos(12, 12, 0, 2, 1, 1, 10, 20)
+    b.add_to_pos(15, 15, 0, 3, 2, -1, 5, 15)
+    b.propagate()
+    for seg, bb, matches, codir, rmin, rmax in b.sorted():  # bucket 1 and its predecessor 0
+        assert (matches, codir, rmin, rmax) == (5, 0, 5, 20)
+
+
 # ---------------------------------------------------------------- mapping.rs:445-495
 def test_update_only_overwrites_on_improvement():
     m = O.Mapping()
@@ -147,3 +160,52 @@ def test_unique_elements_groups_by_hash_and_collects_pmatches():
     got = {tuple(pm) for _, _, pm in seeds}
     assert got == {(60, 30, 10), (70, 20), (40,), (50,)}
     assert sorted(occ for _, occ, _ in seeds) == [1, 1, 2, 3]
+
+
+# ---------------------------------------------------------------- io/mod.rs:435-580
+def _synthetic_fasta(n_segments, seed):
+    """The reference test's generator (src/io/mod.rs:457-482), restated: names,
+    lengths and line widths from its LCG, bases (i * 7 + s) % 4 of ACGT."""
+    state = seed
+
+    def rnd():
+        nonlocal state
+        state = (state * 6364136223846793005 + 1442695040888963407) & 0xFFFFFFFFFFFFFFFF
+        return state >> 33
+
+    text, expect = bytearray(), []
+    for s in range(n_segments):
+        name = f"chr{s}_" + "x" * (rnd() % 40)
+        length = 1 + rnd() % 900
+        width = 1 + rnd() % 97
+        seq = bytes(b"ACGT"[(i * 7 + s) % 4] for i in range(length))
+        text += f">{name} some description here\n".encode()
+        for j in range(0, length, width):
+            text += seq[j:j + width] + b"\n"
+        expect.append((name, seq))
+    return bytes(text), expect
+
+
+def _readers(tmp_path, data):
+    from shmap_b200 import fasta
+
+    p = tmp_path / "t.fa"
+    p.write_bytes(data)
+    return fasta.read_fastx(str(p)), O.read_fasta(str(p))
+
+
+def test_reads_records_and_truncates_id_at_whitespace(tmp_path):
+    for got in _readers(tmp_path, b">read1 some description\nACGT\n>read2\nGGGG\n"):
+        assert got == [("read1", b"ACGT"), ("read2", b"GGGG")]
+
+
+def test_crlf_and_a_missing_final_newline(tmp_path):
+    for got in _readers(tmp_path, b">a desc\r\nACGT\r\nGGTT\r\n>b\r\nTTTT"):
+        assert got == [("a", b"ACGTGGTT"), ("b", b"TTTT")]
+
+
+def test_synthetic_files_of_the_reference(tmp_path):
+    for n, seed in ((24, 0xC0FFEE), (6, 42)):
+        data, expect = _synthetic_fasta(n, seed)
+        for got in _readers(tmp_path, data):
+            assert got == expect, (n, seed)
