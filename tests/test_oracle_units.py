@@ -209,3 +209,36 @@ def test_synthetic_files_of_the_reference(tmp_path):
         data, expect = _synthetic_fasta(n, seed)
         for got in _readers(tmp_path, data):
             assert got == expect, (n, seed)
+
+
+# ---------------------------------------------------------------- shmap/mod.rs:1033-1047
+def test_all_eight_const_generic_combinations_run():
+    """Every (NBP, OS, AP) combination, under every metric, maps the golden
+    fixture's reads, and the same call twice gives the same records."""
+    import itertools
+    import os
+
+    from helpers import pack
+    from shmap_b200 import fasta
+
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    refs = fasta.read_fastx(os.path.join(here, "tiny_ref.fa"))
+    reads = fasta.read_fastx(os.path.join(here, "tiny_reads.fa"))
+    idx = O.Index.from_records(refs, 8, 1.0)
+    seq, offs = pack([s for _, s in reads])
+    for nbp, os_, ap in itertools.product((False, True), repeat=3):
+        for metric in ("Containment", "Jaccard", "bucket_SH", "bucket_LCS"):
+            p = O.params(k=8, h_frac=1.0, theta=0.1, metric=metric, no_bucket_pruning=nbp, one_sweep=os_,
+                         abs_pos=ap)
+            a = idx.map_reads(p, seq, offs)
+            b = idx.map_reads(p, seq, offs, threads=3)
+            assert a.tobytes() == b.tobytes(), (nbp, os_, ap, metric)
+            assert (a["status"] == 0).any(), (nbp, os_, ap, metric)
+    # the reference test's own inputs: a tandem ACGT reference and reads
+    tand = O.Index.from_records([("ref", b"ACGT" * 50)], 8, 1.0)
+    tseq, toffs = pack([b"ACGT" * 14, b"CGTA" * 14])
+    for nbp, os_, ap in itertools.product((False, True), repeat=3):
+        for metric in ("Containment", "Jaccard", "bucket_SH", "bucket_LCS"):
+            p = O.params(k=8, h_frac=1.0, theta=0.1, metric=metric, no_bucket_pruning=nbp, one_sweep=os_,
+                         abs_pos=ap)
+            assert tand.map_reads(p, tseq, toffs).tobytes() == tand.map_reads(p, tseq, toffs, threads=2).tobytes()
