@@ -21,6 +21,14 @@ before timing. Inputs (3.4 GB of reads, a 1 GB index) are larger than L2.
             the reference's Rust binary cannot be built here) on a bounded
             sample of the same reads with every host core
 
+Side measurements (rank 0, outside the timed steps; a failure is reported
+under its key): index_file (shm_index_save / shm_index_load of the built
+index), paf_text (shm_format_paf against shm_format_paf_device on the step's
+records, same bytes), fasta_parse (shm_fasta_parse_device on the first 20,000
+reads as FASTA), serving (shm_server_* under Poisson arrivals: achieved
+reads/s and per-read p50/p99 latency, records checked against the step's),
+plain_form (one read per launch on a sample). --metric maps with another -m.
+
 --impl reference times that CPU implementation alone (rank 0) on the same
 workload, each step a bounded sample.
 Multi-GPU: one process per GPU, each builds its own replica of the index and
