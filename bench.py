@@ -7,19 +7,27 @@ arrays and 5% interspersed 6 kb repeats, and 150,000 lognormal(23 kb, 6 kb)
 reads clipped to 1-60 kb with 0.5% errors; k=25, r=0.01, t=0.4, Containment.
 A step maps every read of the workload once. The index is built on the device
 before timing. Inputs (3.4 GB of reads, a 1 GB index) are larger than L2.
+--workload ont / dense run the ONT-like (Containment, then Jaccard) and the
+r=0.10 dense (Containment, then bucket_SH) configurations.
 
   value     reads/s with the reads already resident in HBM (device events,
             max over ranks)
-  e2e       the same through shm_map_batch from pinned host buffers: the
-            host->device copy of the reads and the device->host copy of the
-            records are inside the timed region
+  e2e       the same through shm_map_paf from pinned host buffers: reads in,
+            PAF text out. The host->device copy of the reads and the
+            device->host copy of the records and the PAF text are inside the
+            timed region (e2e.records_only: shm_map_batch, records out)
+  parity    every read of the workload mapped by the CPU oracle (the C++
+            restatement of the reference path): its records must equal the
+            device's bit for bit and its PAF text the e2e text byte for byte
+            (t:f: aside); any difference ends the run with status 1
   roofline  the stage that takes the most device time, its algorithmic
             bytes per launch over its average launch time (CUDA events on the
             library's stream during the timed steps), against the measured
-            HBM copy bandwidth
-  cpu_baseline  the CPU oracle (the C++ restatement of the reference path;
-            the reference's Rust binary cannot be built here) on a bounded
-            sample of the same reads with every host core
+            HBM copy bandwidth; the sketch, bound by integer issue, also
+            reports its warp-instruction issue rate against the SMs' peak
+  cpu_baseline  that oracle run, every read mapped and its PAF rendered with
+            every host core; cpu_baseline_1t: a bounded sample with one
+            thread (the reference's -@1)
 
 Side measurements (rank 0, outside the timed steps; a failure is reported
 under its key): index_file (shm_index_save / shm_index_load of the built
@@ -27,10 +35,11 @@ index), paf_text (shm_format_paf against shm_format_paf_device on the step's
 records, same bytes), fasta_parse (shm_fasta_parse_device on the first 20,000
 reads as FASTA), serving (shm_server_* under Poisson arrivals: achieved
 reads/s and per-read p50/p99 latency, records checked against the step's),
-plain_form (one read per launch on a sample). --metric maps with another -m.
+plain_form (one read per launch on a sample), other_metrics (the workload's
+second -m, timed and checked the same way). --metric maps with another -m.
 
 --impl reference times that CPU implementation alone (rank 0) on the same
-workload, each step a bounded sample.
+workload, each step a bounded sample, with every host core and with one.
 Multi-GPU: one process per GPU, each builds its own replica of the index and
 maps its own read set (weak scaling); no collective on the data path.
 """
@@ -39,6 +48,7 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
+import re
 import os
 import statistics
 import subprocess
@@ -50,6 +60,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "shmap-rs_b200"))
 
 import numpy as np  # noqa: E402
+
+# the workload's further -m, timed and checked after the first
+EXTRA_METRICS = {"hifi": [], "uniform": [], "ont": ["Jaccard"], "dense": ["bucket_SH"]}
 
 WORKLOADS = {
     # name: (reference preset, read preset, k, r, theta, metric, description)
@@ -178,21 +191,185 @@ def make_workload(name: str, rank: int, scale: float, metric_override: str | Non
     return gen, names, seq, offs, dict(k=k, r=r, theta=theta, metric=metric, desc=desc)
 
 
-def algorithmic_bytes(stage: str, w: dict) -> tuple[float, str]:
-    """Bytes a stage must move at the least, over the counted work: its inputs
-    read once and its outputs written once."""
+def algorithmic_bytes(stage: str, w: dict, seq_bytes: float) -> tuple[float, str]:
+    """Bytes a stage must move at the least over the counted work: its inputs
+    read once and its outputs written once. seq_bytes is the reads' sum of
+    ceil(L/4) + ceil(L/8) (2-bit codes and a 1-bit non-ACGT mask)."""
     if stage == "sketch":
-        return (1.0 * w["bases"] + 12.0 * w["kmers"],
-                "1 B per read base + 12 B per selected k-mer (hash, r << 1 | strand)")
+        return (seq_bytes + 16.0 * w["kmers"],
+                "sum over reads of ceil(L/4) + ceil(L/8) (2-bit codes, 1-bit non-ACGT mask) in + 16 B per "
+                "selected k-mer out")
     if stage == "seedprep":
-        return (12.0 * w["kmers"] + 68.0 * w["distinct_seeds"],
-                "12 B per read k-mer + 32 B per count() probe + 36 B of seed record and probe-table entry per seed")
+        return (16.0 * w["kmers"] + 32.0 * w["distinct_seeds"],
+                "16 B per read k-mer in + 32 B (one sector) per count() probe")
     if stage in ("contrib", "extend", "bscan"):
-        return (32.0 * w["distinct_seeds"] + 12.0 * (w["seed_hits"] + w["extension_seeds"]),
-                "32 B per count() probe + 12 B per hit touched")
+        return (12.0 * (w["seed_hits"] + w["extension_seeds"]),
+                "12 B per hit touched (match_seeds and matches_in_bucket hits)")
     if stage == "refine":
-        return 12.0 * w["refine_kmers"], "12 B per reference k-mer of every refined window"
+        return 12.0 * w["refine_kmers"], "12 B per reference k-mer of every refined window (8 B hash + 4 B r)"
     return 0.0, "n/a"
+
+
+def packed_bytes(offs: np.ndarray) -> float:
+    lens = np.diff(offs)
+    return float(((lens + 3) // 4).sum() + ((lens + 7) // 8).sum())
+
+
+def workload_config(args, wk: dict, n: int, nbytes: int, world: int) -> dict:
+    """The config object of both arms' JSON lines (the same keys and values)."""
+    return {"workload": args.workload, "description": wk["desc"], "reads_per_gpu": n, "bases_per_gpu": nbytes,
+            "k": wk["k"], "r": wk["r"], "theta": wk["theta"], "metric": wk["metric"],
+            "l2": "inputs larger than L2 (reads and index are GB-sized), no flush",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "scale": args.scale}
+
+
+def time_device(ctx, idx, p, d_seq, offs, d_out, stream, steps: int, warmup: int, world: int, local: int,
+                clocks=None):
+    """W untimed steps, then K steps of the device-resident path between CUDA
+    events on the library's stream (barrier + synchronize on both sides; max
+    over ranks). Returns (ms, launches, stage times, work counters, clocks)."""
+    import torch
+
+    def step():
+        idx.map_reads_device(p, d_seq.data_ptr(), offs, d_out.data_ptr())
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.set_timing(False)
+    ctx.set_timing(True)
+    if clocks:
+        clocks.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launches - launches0
+    clk = clocks.stop() if clocks else None
+    stages = ctx.stage_times()
+    work = ctx.work_stats()
+    ctx.set_timing(False)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, launches, stages, work, clk
+
+
+def time_e2e(ctx, idx, p, h_seq_np, offs, joined, h_out, h_text, steps: int, world: int, local: int,
+             with_paf: bool = True):
+    """K steps through the public C ABI from pinned host memory: shm_map_paf
+    (reads in, records and PAF text out) or shm_map_batch (records out).
+    Every step's host->device and device->host copies are inside the timed
+    region. Returns (ms, h2d bytes per step, d2h bytes per step, text length)."""
+    import torch
+
+    import shmap_b200 as sb
+
+    n = len(offs) - 1
+    cp = p.c()
+    need = ctypes.c_int64()
+
+    def step():
+        if with_paf:
+            sb._check(sb.lib().shm_map_paf(ctx.h, idx.h, ctypes.byref(cp), h_seq_np.ctypes.data, offs.ctypes.data,
+                                           n, joined, h_out.ctypes.data, h_text.ctypes.data, len(h_text),
+                                           ctypes.byref(need)))
+        else:
+            sb._check(sb.lib().shm_map_batch(ctx.h, idx.h, ctypes.byref(cp), h_seq_np.ctypes.data,
+                                             offs.ctypes.data, n, h_out.ctypes.data))
+
+    step()  # grows the buffers of this call shape
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    io0 = ctx.work_stats()  # bytes copied between host and device, counted by the library
+    w0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max(e0.elapsed_time(e1), (time.perf_counter() - w0) * 1e3)
+    io1 = ctx.work_stats()
+    h2d = (io1.get("h2d_bytes", 0) - io0.get("h2d_bytes", 0)) // max(1, steps)
+    d2h = (io1.get("d2h_bytes", 0) - io0.get("d2h_bytes", 0)) // max(1, steps)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, int(h2d), int(d2h), int(need.value) if with_paf else 0
+
+
+_T_TAG = re.compile(rb"\tt:f:[^\t\n]*")
+
+
+def oracle_check(oi, wk: dict, metric: str, names, seq, offs, rec, text: bytes, threads: int) -> tuple[dict, float]:
+    """Every read mapped by the CPU oracle with `threads` host threads, its PAF
+    rendered: records compared with the device's bit for bit, PAF text with
+    the e2e text byte for byte (the wall-clock t:f: tag removed from both, as
+    the reference's own golden test does). Returns (parity, oracle seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # the checker, never the measured product
+
+    op = O.params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=metric)
+    orec, otext, secs = oi.map_paf(op, seq, offs, names, threads)
+    same_rec = orec.tobytes() == rec.tobytes()
+    bad_fields, bad_reads = {}, np.zeros(len(rec), bool)
+    if not same_rec:
+        for f in rec.dtype.names:
+            x, y = rec[f], orec[f]
+            d = (x.view(np.int64) != y.view(np.int64)) if x.dtype.kind == "f" else (x != y)
+            if d.any():
+                bad_fields[f] = int(d.sum())
+                bad_reads |= d
+    a, b = _T_TAG.sub(b"", text), _T_TAG.sub(b"", otext)
+    res = {"reads": int(len(rec)), "mapped": int((rec["status"] == 0).sum()),
+           "record_mismatches": int(bad_reads.sum()), "mismatched_fields": bad_fields,
+           "first_mismatched_reads": [int(i) for i in np.nonzero(bad_reads)[0][:5]],
+           "records_equal": bool(same_rec),
+           "paf_bytes": len(text), "paf_lines": text.count(b"\n"), "paf_bytes_equal": a == b,
+           "against": "CPU oracle (C++ restatement of the reference path), every read of the workload; PAF "
+                      "compared without the wall-clock t:f: tag"}
+    return res, secs
+
+
+def cpu_one_thread(oi, wk: dict, names, seq, offs, target_s: float, rate_all: float, threads_all: int) -> dict:
+    """The oracle with one host thread (the reference's -@1) on a bounded
+    sample of the workload's reads sized to about target_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    op = O.params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=wk["metric"])
+    n = len(offs) - 1
+    m = int(max(16, min(n, rate_all / max(1, threads_all) * target_s)))
+    a = (n - m) // 2
+    sub = offs[a:a + m + 1] - offs[a]
+    _, _, secs = oi.map_paf(op, seq[offs[a]:offs[a + m]], sub, names[a:a + m], 1, records=False)
+    return {"value": round(m / secs, 1), "unit": "reads/s", "cores": 1, "kind": "port",
+            "sample": f"reads {a}..{a + m} of the workload's {n}, mapped and PAF rendered by the C++ oracle "
+                      f"with one thread ({secs:.1f} s)"}
+
+
+def oracle_index(gen, wk: dict, threads: int):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    t0 = time.time()
+    oi = O.Index(gen.names, gen.seq, gen.seg_off, wk["k"], wk["r"], threads=threads)
+    log(f"[bench] CPU oracle index in {time.time() - t0:.1f}s with {threads} threads")
+    return oi
 
 
 def run_ours(args, rank, world, local):
@@ -229,11 +406,12 @@ def run_ours(args, rank, world, local):
             back.close()
             return res
 
-    index_file = _extra("index_file", _index_file) if rank == 0 else None
+    index_file = _extra("index_file", _index_file) if rank == 0 and args.side else None
 
     p = sb.Params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=wk["metric"])
     n = len(names)
     nbytes = int(offs[-1])
+    joined = "\n".join(names).encode()
 
     # device-resident inputs
     d_seq = torch.empty(nbytes + 32, dtype=torch.uint8, device=f"cuda:{local}")
@@ -242,78 +420,32 @@ def run_ours(args, rank, world, local):
     d_out = torch.empty(n * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
     stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
 
-    def device_step():
-        idx.map_reads_device(p, d_seq.data_ptr(), offs, d_out.data_ptr())
-
-    for _ in range(args.warmup):
-        device_step()
-    torch.cuda.synchronize()
-    ctx.set_timing(False)
-    ctx.set_timing(True)
     clocks = ClockSampler(local)
-    clocks.start()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    launches0 = ctx.launches
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        device_step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    launches = ctx.launches - launches0
-    clk = clocks.stop()
-    stages = ctx.stage_times()
-    work = ctx.work_stats()
-    ctx.set_timing(False)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    rec = d_out.cpu().numpy().view(sb.RECORD_DTYPE)
+    ms, launches, stages, work, clk = time_device(ctx, idx, p, d_seq, offs, d_out, stream, args.steps, args.warmup,
+                                                  world, local, clocks)
+    rec = d_out.cpu().numpy().view(sb.RECORD_DTYPE).copy()
     mapped = float((rec["status"] == 0).mean())
 
-    # end to end through the public C ABI, from pinned host memory
+    # end to end through the public C ABI, from pinned host memory: reads in, PAF text out
     h_seq = torch.empty(nbytes + 32, dtype=torch.uint8).pin_memory()
     h_seq[:nbytes].copy_(torch.from_numpy(np.ascontiguousarray(seq)))
     h_out_t = torch.empty(n * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
     h_seq_np = h_seq.numpy()
     h_out = h_out_t.numpy().view(sb.RECORD_DTYPE)
-
-    def e2e_step():
-        cp = p.c()
-        sb._check(sb.lib().shm_map_batch(ctx.h, idx.h, ctypes.byref(cp), h_seq_np.ctypes.data,
-                                         offs.ctypes.data, n, h_out.ctypes.data))
-
-    e2e_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    io0 = ctx.work_stats()  # bytes copied between host and device, counted by the library
-    w0 = time.perf_counter()
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - w0) * 1e3)
-    io1 = ctx.work_stats()
-    h2d_step = (io1.get("h2d_bytes", 0) - io0.get("h2d_bytes", 0)) // max(1, args.steps)
-    d2h_step = (io1.get("d2h_bytes", 0) - io0.get("d2h_bytes", 0)) // max(1, args.steps)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    h_text = torch.empty(640 * n + len(joined) + 64, dtype=torch.uint8).pin_memory().numpy()
+    e2e_ms, h2d_step, d2h_step, text_len = time_e2e(ctx, idx, p, h_seq_np, offs, joined, h_out, h_text,
+                                                    args.steps, world, local, True)
     if not np.array_equal(h_out.view(np.uint8), rec.view(np.uint8)):
         raise RuntimeError("e2e records differ from the device-resident records")
+    text = h_text[:text_len].tobytes()
+    if rank == 0 and text != idx.format_paf(p, rec, names).encode():
+        raise RuntimeError("e2e PAF text differs from the host formatter's text over the same records")
+    rec_ms, rec_h2d, rec_d2h, _ = time_e2e(ctx, idx, p, h_seq_np, offs, joined, h_out, h_text, args.steps, world,
+                                           local, False)
+    if not np.array_equal(h_out.view(np.uint8), rec.view(np.uint8)):
+        raise RuntimeError("e2e (records only) records differ from the device-resident records")
 
     def _paf():  # the PAF text of the step's records: shm_format_paf (host) and shm_format_paf_device
-        joined = "\n".join(names).encode()
         cp = p.c()
         need = ctypes.c_int64()
         _ = sb.lib().shm_format_paf(idx.h, ctypes.byref(cp), rec.ctypes.data, n, joined, None, None, 0,
@@ -338,7 +470,7 @@ def run_ours(args, rank, world, local):
         log(f"[bench] PAF text: {res}")
         return res
 
-    paf = _extra("paf", _paf) if rank == 0 else None
+    paf = _extra("paf", _paf) if rank == 0 and args.side else None
 
     def _fasta_parse():  # reads as FASTA bytes (pinned host memory), parsed on the device
         m = min(n, 20000)
@@ -364,7 +496,7 @@ def run_ours(args, rank, world, local):
         log(f"[bench] FASTA parse: {res}")
         return res
 
-    fasta_parse = _extra("fasta_parse", _fasta_parse) if rank == 0 else None
+    fasta_parse = _extra("fasta_parse", _fasta_parse) if rank == 0 and args.side else None
 
     def _serving():
         res = serve_load(ctx, idx, p, h_seq_np, offs, rec, [10_000, 50_000, 200_000, 1_000_000],
@@ -372,7 +504,7 @@ def run_ours(args, rank, world, local):
         log(f"[bench] serving: {res}")
         return res
 
-    serving = _extra("serving", _serving) if rank == 0 and args.serve_seconds > 0 else None
+    serving = _extra("serving", _serving) if rank == 0 and args.serve_seconds > 0 and args.side else None
 
     # plain one-read-per-launch form on a sample
     plain = None
@@ -387,6 +519,28 @@ def run_ours(args, rank, world, local):
             raise RuntimeError("plain records differ from the batched records")
         plain = {"reads_per_s": m / pt, "sample_reads": m}
 
+    # the workload's further metrics, timed the same way (device-resident and e2e with PAF)
+    others = {}
+    for om in EXTRA_METRICS.get(args.workload, []) if args.metric is None else []:
+        po = sb.Params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=om)
+        oms, olaunch, ostages, _, _ = time_device(ctx, idx, po, d_seq, offs, d_out, stream, args.steps,
+                                                  args.warmup, world, local)
+        orec = d_out.cpu().numpy().view(sb.RECORD_DTYPE).copy()
+        oe_ms, oh2d, od2h, olen = time_e2e(ctx, idx, po, h_seq_np, offs, joined, h_out, h_text, args.steps, world,
+                                           local, True)
+        if not np.array_equal(h_out.view(np.uint8), orec.view(np.uint8)):
+            raise RuntimeError(f"{om}: e2e records differ from the device-resident records")
+        others[om] = {"value": round(n * world * args.steps / (oms / 1e3), 1), "unit": "reads/s",
+                      "ms_per_step": round(oms / args.steps, 3), "gpu_launches": int(olaunch),
+                      "stages_ms": {k: round(v[0] / args.steps, 3) for k, v in ostages.items()},
+                      "mapped_fraction": round(float((orec["status"] == 0).mean()), 4),
+                      "e2e": {"value": round(n * world * args.steps / (oe_ms / 1e3), 1), "unit": "reads/s",
+                              "ms_per_step": round(oe_ms / args.steps, 3), "h2d_bytes_per_step": oh2d,
+                              "d2h_bytes_per_step": od2h},
+                      "_rec": orec, "_text": h_text[:olen].tobytes()}
+        log(f"[bench] -m {om}: {others[om]['value']:.0f} reads/s device-resident, "
+            f"{others[om]['e2e']['value']:.0f} e2e")
+
     result = None
     if rank == 0:
         reads_total = n * world
@@ -397,7 +551,7 @@ def run_ours(args, rank, world, local):
         top = max((s for s in stages if s != "aux"), key=lambda s: stages[s][0])
         top_ms, top_calls = stages[top]
         per_launch_s = top_ms / 1e3 / max(1, top_calls)
-        alg, alg_desc = algorithmic_bytes(top, work)
+        alg, alg_desc = algorithmic_bytes(top, work, packed_bytes(offs) * args.steps)
         alg_per_launch = alg / max(1, top_calls)
         achieved = alg_per_launch / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
         tr = None
@@ -409,16 +563,31 @@ def run_ours(args, rank, world, local):
                 "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
                 "avg_launch_ms": round(per_launch_s * 1e3, 4), "launches": top_calls,
                 "algorithmic_bytes_per_launch": round(alg_per_launch), "algorithmic_bytes": alg_desc}
+        if top == "sketch":
+            # integer-issue bound: warp instructions per base (ncu's smsp__inst_executed on a
+            # one-kernel capture, profiles/traffic.json) times the bases of a launch, over the
+            # launch time, against four warp instructions per clock on each of the 148 SMs
+            ipb = traffic.get(args.workload, {}).get("sketch_warp_inst_per_base")
+            mhz = (clk or {}).get("sm_mhz") or 1965.0
+            roof["bound"] = "int_issue"
+            if ipb:
+                inst = ipb * work["bases"] / max(1, top_calls)
+                ach_i = inst / per_launch_s / 1e12
+                pk_i = 148 * 4 * mhz * 1e6 / 1e12
+                roof["issue"] = {"achieved": round(ach_i, 4), "peak": round(pk_i, 4), "unit": "T warp-inst/s",
+                                 "frac": round(ach_i / pk_i, 4), "warp_inst_per_base": ipb,
+                                 "peak_def": f"148 SMs x 4 warp instructions per clock at the sampled {mhz:.0f} MHz"}
+            roof["note"] = ("bound by integer instruction issue, not HBM: its HBM fraction is small by "
+                            "construction; reaching 60% of HBM at this instruction count would need several "
+                            "times the SMs' issue rate")
         e2e_value = reads_total * args.steps / (e2e_ms / 1e3)
+        rec_value = reads_total * args.steps / (rec_ms / 1e3)
         result = {
             "metric": "reads/s (mapping, byte-identical PAF records)", "value": round(value, 1), "unit": "reads/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded generator, shapes of the benchmark configuration)",
-            "config": {"workload": args.workload, "description": wk["desc"], "reads_per_gpu": n,
-                       "bases_per_gpu": nbytes, "k": wk["k"], "r": wk["r"], "theta": wk["theta"],
-                       "metric": wk["metric"], "l2": "inputs larger than L2 (reads and index are GB-sized)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "scale": args.scale},
+            "config": workload_config(args, wk, n, nbytes, world),
             "mbp_per_s": round(mbp, 1),
             "mapped_fraction": round(mapped, 4),
             "index_build_s": round(index_s, 3),
@@ -428,11 +597,16 @@ def run_ours(args, rank, world, local):
             "work_per_step": {k: v // max(1, args.steps) for k, v in work.items()},
             "roofline": roof,
             # h2d/d2h: the bytes the call copied (the reads go up packed: 2-bit codes, the nonzero
-            # words of the non-ACGT mask, the batch plans); ascii_gb_per_s: the reads' own bytes
-            # taken in per second
-            "e2e": {"value": round(e2e_value, 1), "unit": "reads/s", "h2d_bytes_per_step": int(h2d_step),
-                    "d2h_bytes_per_step": int(d2h_step), "ms_per_step": round(e2e_ms / args.steps, 3),
-                    "ascii_gb_per_s": round(nbytes * args.steps / (e2e_ms / 1e3) / 1e9, 1)},
+            # words of the non-ACGT mask, the batch plans, the names; records and PAF text come
+            # down); ascii_gb_per_s: the reads' own bytes taken in per second
+            "e2e": {"value": round(e2e_value, 1), "unit": "reads/s", "h2d_bytes_per_step": h2d_step,
+                    "d2h_bytes_per_step": d2h_step, "ms_per_step": round(e2e_ms / args.steps, 3),
+                    "ascii_gb_per_s": round(nbytes * args.steps / (e2e_ms / 1e3) / 1e9, 1),
+                    "paf_bytes_per_step": text_len,
+                    "what": "shm_map_paf: reads from pinned host memory in, records and PAF text out",
+                    "records_only": {"value": round(rec_value, 1), "unit": "reads/s",
+                                     "ms_per_step": round(rec_ms / args.steps, 3), "h2d_bytes_per_step": rec_h2d,
+                                     "d2h_bytes_per_step": rec_d2h, "what": "shm_map_batch: records out"}},
             "gpu_launches": int(launches),
             "clocks": clk,
         }
@@ -445,11 +619,14 @@ def run_ours(args, rank, world, local):
         if plain:
             result["plain_form"] = {"reads_per_s": round(plain["reads_per_s"], 1), "sample_reads": plain["sample_reads"],
                                     "batched_e2e_over_plain": round(e2e_value / plain["reads_per_s"], 1)}
+        if others:
+            result["other_metrics"] = others
     if world > 1:
         torch.distributed.barrier()
     idx.close()
     ctx.close()
-    return result, (gen, names, seq, offs, wk)
+    return result, (gen, names, seq, offs, wk, rec, text)
+
 
 
 def serve_load(ctx, idx, p, h_seq_np, offs, rec, rates, seconds: float, seed: int):
@@ -526,26 +703,30 @@ def serve_load(ctx, idx, p, h_seq_np, offs, rec, rates, seconds: float, seed: in
             "slots": 2, "rates": out, "records_same_as_alone": same}
 
 
-def cpu_reference(gen, names, seq, offs, wk, target_s: float, threads: int, steps: int = 1):
-    """The CPU oracle on a bounded sample: returns (reads/s, sample description, threads)."""
+
+
+def cpu_reference(gen, names, seq, offs, wk, target_s: float, threads: int, steps: int = 1, oi=None):
+    """The CPU oracle on bounded samples, mapping and rendering PAF: returns
+    (reads/s per step, sample description)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O  # the checker / CPU baseline, never the measured product
 
-    t0 = time.time()
-    oi = O.Index(gen.names, gen.seq, gen.seg_off, wk["k"], wk["r"], threads=threads)
-    log(f"[bench] CPU oracle index in {time.time() - t0:.1f}s with {threads} threads")
+    if oi is None:
+        oi = oracle_index(gen, wk, threads)
     p = O.params(k=wk["k"], h_frac=wk["r"], theta=wk["theta"], metric=wk["metric"])
-    m = min(len(names), max(threads * 8, 256))
-    t = oi.time_map(p, seq, offs[: m + 1], threads)
+    n = len(names)
+    m = min(n, max(threads * 8, 256))
+    _, _, t = oi.map_paf(p, seq, offs[: m + 1], names[:m], threads, records=False)
     rate = m / max(t, 1e-6)
-    m = int(min(len(names), max(m, rate * target_s)))
+    m = int(min(n, max(m, rate * target_s)))
     rates = []
     for s in range(steps):
-        a = (s * m) % max(1, len(names) - m + 1)
+        a = (s * m) % max(1, n - m + 1)
         sub = offs[a: a + m + 1] - offs[a]
-        t = oi.time_map(p, seq[offs[a]:], sub, threads)
+        _, _, t = oi.map_paf(p, seq[offs[a]:offs[a + m]], sub, names[a:a + m], threads, records=False)
         rates.append(m / t)
-    return rates, f"{m} of the workload's {len(names)} reads per step, mapped by the C++ oracle with {threads} threads"
+    return rates, (f"{m} of the workload's {n} reads per step, mapped and PAF rendered by the C++ oracle "
+                   f"with {threads} threads")
 
 
 def main():
@@ -557,10 +738,14 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="hifi")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests and profiling)")
     ap.add_argument("--metric", choices=["Containment", "Jaccard", "bucket_SH", "bucket_LCS"], default=None,
-                    help="map with this -m instead of the workload's")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size, in seconds of work")
+                    help="map with this -m instead of the workload's (its further -m are then not run)")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="one-thread CPU baseline sample size, in seconds of work")
     ap.add_argument("--plain-sample", type=int, default=400)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the oracle runs (and with them the full-size parity check)")
+    ap.add_argument("--no-side", dest="side", action="store_false",
+                    help="skip the side measurements (index file, PAF formatter, FASTA, serving)")
     ap.add_argument("--serve-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals per offered rate in the serving measurement (0 skips it)")
     args = ap.parse_args()
@@ -571,34 +756,61 @@ def main():
         if rank != 0:
             return
         gen, names, seq, offs, wk = make_workload(args.workload, 0, args.scale, args.metric)
+        oi = oracle_index(gen, wk, threads)
         per_step = max(2.0, 150.0 / max(1, args.steps + args.warmup))
-        rates, sample = cpu_reference(gen, names, seq, offs, wk, per_step, threads, steps=args.warmup + args.steps)
+        rates, sample = cpu_reference(gen, names, seq, offs, wk, per_step, threads, steps=args.warmup + args.steps,
+                                      oi=oi)
         timed = rates[args.warmup:] or rates
         v = statistics.mean(timed)
+        one = cpu_one_thread(oi, wk, names, seq, offs, args.cpu_seconds, v, threads)
         line = {"metric": "reads/s (mapping, byte-identical PAF records)", "value": round(v, 1), "unit": "reads/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(len(names) / v * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
-                "config": {"workload": args.workload, "description": wk["desc"], "reads_per_gpu": len(names),
-                           "bases_per_gpu": int(offs[-1]), "k": wk["k"], "r": wk["r"], "theta": wk["theta"],
-                           "metric": wk["metric"], "scale": args.scale, "host_cores": threads},
+                "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded generator, shapes of the benchmark "
+                                                             "configuration)", "impl": "reference",
+                "config": workload_config(args, wk, len(names), int(offs[-1]), args.gpus),
+                "host_cores": threads,
                 "cpu_baseline": {"value": round(v, 1), "unit": "reads/s", "cores": threads, "kind": "port",
                                  "sample": sample},
+                "cpu_baseline_1t": one,
                 "e2e": {"value": round(v, 1), "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "note": "the reference is Rust and no Rust toolchain exists on this image; this arm times the C++ "
-                        "restatement of its mapping path (oracle/) with every host core"}
+                        "restatement of its mapping path (oracle/), reads in and PAF text out, with every host core "
+                        "(value) and with one (cpu_baseline_1t)"}
         print(json.dumps(line), flush=True)
         return
 
     result, data = run_ours(args, rank, world, local)
+    failed = False
     if rank == 0:
+        result["host_cores"] = threads
         if world == 1 and not args.no_cpu_baseline:
-            gen, names, seq, offs, wk = data
-            rates, sample = cpu_reference(gen, names, seq, offs, wk, args.cpu_seconds, threads)
-            result["cpu_baseline"] = {"value": round(rates[0], 1), "unit": "reads/s", "cores": threads, "kind": "port",
-                                      "sample": sample}
-            result["cpu_baseline"]["e2e_speedup"] = round(result["e2e"]["value"] / rates[0], 2)
+            gen, names, seq, offs, wk, rec, text = data
+            oi = oracle_index(gen, wk, threads)
+            parity, secs = oracle_check(oi, wk, wk["metric"], names, seq, offs, rec, text, threads)
+            rate = len(names) / secs
+            result["parity"] = parity
+            result["cpu_baseline"] = {"value": round(rate, 1), "unit": "reads/s", "cores": threads, "kind": "port",
+                                      "sample": f"all {len(names)} reads of the workload, mapped and PAF rendered "
+                                                f"by the C++ oracle with {threads} threads ({secs:.1f} s)",
+                                      "e2e_speedup": round(result["e2e"]["value"] / rate, 2)}
+            result["cpu_baseline_1t"] = cpu_one_thread(oi, wk, names, seq, offs, args.cpu_seconds, rate, threads)
+            result["cpu_baseline_1t"]["e2e_speedup"] = round(result["e2e"]["value"] /
+                                                             result["cpu_baseline_1t"]["value"], 1)
+            failed = not (parity["records_equal"] and parity["paf_bytes_equal"])
+            for om, o in result.get("other_metrics", {}).items():
+                par, osecs = oracle_check(oi, wk, om, names, seq, offs, o.pop("_rec"), o.pop("_text"), threads)
+                o["parity"] = par
+                o["cpu_baseline"] = {"value": round(len(names) / osecs, 1), "unit": "reads/s", "cores": threads,
+                                     "kind": "port", "sample": f"all {len(names)} reads, oracle with {threads} threads"}
+                failed = failed or not (par["records_equal"] and par["paf_bytes_equal"])
+        for o in result.get("other_metrics", {}).values():
+            o.pop("_rec", None)
+            o.pop("_text", None)
         print(json.dumps(result), flush=True)
+    if failed:
+        log("[bench] PARITY FAILED: the device's records or PAF differ from the CPU oracle's")
+        sys.exit(1)
 
 
 if __name__ == "__main__":

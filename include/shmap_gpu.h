@@ -115,12 +115,18 @@ int shm_index_stats_get(const shm_index* idx, shm_index_stats* out);
  * back onto the device of ctx, so that a service starts mapping without the
  * reference's sequence or a rebuild. The file holds the segments, every
  * reference k-mer and the hash CSR (about 20 bytes per reference k-mer plus
- * the names); the derived tables are rebuilt on load. Load answers
- * SHM_ERR_INVALID, with a message, for a file that is missing, of another
- * kind or version, or truncated. shm_index_info gives the k, hash ratio and
- * -M (-1 = none) the index was built with. */
+ * the names, and a checksum); the derived tables are rebuilt on load. Load
+ * checks every section on the host before any of it reaches the device and
+ * answers SHM_ERR_INVALID, with a message, for a file that is missing, of
+ * another kind or version, truncated, fails its checksum, or holds arrays an
+ * index cannot have (offsets out of order, hashes above the threshold,
+ * positions outside their segment, hits that are no reference k-mer).
+ * shm_index_file_check makes the same checks on the host alone (no device
+ * needed). shm_index_info gives the k, hash ratio and -M (-1 = none) the
+ * index was built with. */
 int shm_index_save(const shm_index* idx, const char* path);
 int shm_index_load(shm_ctx* ctx, const char* path, shm_index** out);
+int shm_index_file_check(const char* path);
 int shm_index_info(const shm_index* idx, int32_t* k, double* h_frac, int32_t* max_matches);
 
 /* SketchIndex::count (src/index.rs:204-213) for n hashes. */
@@ -167,6 +173,20 @@ int shm_format_paf_device(shm_ctx* ctx, const shm_index* idx, const shm_params* 
                           int32_t n, const char* names, const double* map_time, char* buf, int64_t cap,
                           int64_t* n_out);
 
+/* Mapper::map_reads as the command line runs it (src/mapper.rs:15-17,
+ * src/shmap/mod.rs:374-650 with the in-order collector's output,
+ * mod.rs:868-963): n host reads in (seqs/offs as in shm_map_batch, names
+ * '\n'-joined), the PAF text of the mapped reads out, in input order: the
+ * bytes shm_format_paf gives for the same records, t:f: printed as 0 (the
+ * batched path keeps no per-read wall clock). The text of each device batch
+ * is rendered on the device as soon as the batch is mapped, so it overlaps
+ * the next batches. out (may be NULL) gets the records too. *n_out = the
+ * text's length; at most cap bytes go to buf (NULL only measures, after
+ * mapping everything); SHM_ERR_CAPACITY when the text exceeds cap. Pinned
+ * seqs, out and buf keep every copy asynchronous. */
+int shm_map_paf(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
+                int32_t n, const char* names, shm_map_record* out, char* buf, int64_t cap, int64_t* n_out);
+
 /* Kernel launches this library issued so far in this process (the bench
  * reports the count inside its timed region). */
 int64_t shm_ctx_launches(const shm_ctx* ctx);
@@ -204,7 +224,9 @@ const char* shm_work_stat_name(int i);
  * than 4,194,304 windows (4,194,304 + k - 1 bases) are rejected with
  * SHM_ERR_INVALID. The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture. stream = NULL runs on the default stream. */
+ * call before any stream capture. Every call synchronizes `stream` before it
+ * returns: it reads the k-mer count back to the host between its counting
+ * and its writing pass. stream = NULL runs on the default stream. */
 int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, double h_frac, int32_t offset,
                               uint64_t* d_h, uint32_t* d_rs, int64_t cap, int64_t* n_out, void* stream);
 

@@ -1,5 +1,6 @@
 // TEST INFRASTRUCTURE ONLY: C entry points of the CPU oracle for the Python
 // tests and bench.py's CPU baseline (ctypes). Not part of the product.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <string>
@@ -230,6 +231,42 @@ int64_t orc_paf(void* p, const orc_params* prm, const uint8_t* seqs, const int64
         if (res[(size_t)i].mapped) text += render_paf(res[(size_t)i], names[(size_t)i], q, 0.0) + "\n";
     if (buf && cap > 0) std::memcpy(buf, text.data(), (size_t)std::min<int64_t>(cap, (int64_t)text.size()));
     return (int64_t)text.size();
+}
+
+// Maps n reads with `threads` host threads and renders their PAF text in input
+// order (mapped reads only, t:f: as 0), timed from the first read taken to the
+// joined text: records to out[n] (may be NULL), the text's length to
+// *text_len. Returns the wall-clock seconds. The text stays in this file's
+// buffer until orc_take_text copies it out (bench.py's CPU baseline and its
+// full-size parity check).
+static std::string g_text;
+double orc_map_paf(void* p, const orc_params* prm, const uint8_t* seqs, const int64_t* offs, const char* names_joined,
+                   int32_t n, int32_t threads, orc_record* out, int64_t* text_len) {
+    OrcIndex* o = (OrcIndex*)p;
+    Params q = to_params(prm);
+    std::vector<const uint8_t*> s;
+    std::vector<size_t> l;
+    for (int32_t i = 0; i < n; i++) {
+        s.push_back(seqs + offs[i]);
+        l.push_back((size_t)(offs[i + 1] - offs[i]));
+    }
+    auto names = split_names(names_joined, n);
+    std::vector<ReadResult> res;
+    auto t0 = std::chrono::steady_clock::now();
+    map_reads_paf(o->idx, o->sk, q, s, l, names, threads, res, g_text);
+    auto t1 = std::chrono::steady_clock::now();
+    if (out)
+        for (int32_t i = 0; i < n; i++) fill(out[i], res[(size_t)i]);
+    if (text_len) *text_len = (int64_t)g_text.size();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Copies the text of the last orc_map_paf (up to cap bytes) and releases it.
+int64_t orc_take_text(char* buf, int64_t cap) {
+    const int64_t n = std::min<int64_t>(cap, (int64_t)g_text.size());
+    if (buf && n > 0) std::memcpy(buf, g_text.data(), (size_t)n);
+    std::string().swap(g_text);
+    return n;
 }
 
 // Wall-clock seconds to map a sample with `threads` host threads (bench.py's CPU baseline).

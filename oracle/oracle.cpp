@@ -1051,6 +1051,40 @@ std::vector<ReadResult> map_reads(const SketchIndex& tidx, const FracMinHash& sk
     return out;
 }
 
+// src/shmap/mod.rs:374-650 with the collector's output (mod.rs:868-963): the
+// workers map reads and render each mapped read's PAF line (t:f: printed as
+// map_time = 0); the lines are then joined in input order, as the in-order
+// collector writes them. Results keep the state before render_paf's
+// post-processing (second best, mapq) in `res`; `lines` get the text.
+void map_reads_paf(const SketchIndex& tidx, const FracMinHash& sk, const Params& p,
+                   const std::vector<const uint8_t*>& seqs, const std::vector<size_t>& lens,
+                   const std::vector<std::string>& names, int threads, std::vector<ReadResult>& res,
+                   std::string& text) {
+    res.assign(seqs.size(), ReadResult());
+    std::vector<std::string> lines(seqs.size());
+    std::atomic<size_t> next{0};
+    threads = std::max(1, threads);
+    auto work = [&]() {
+        Buckets bk(tidx, p.abs_pos);
+        for (size_t i; (i = next.fetch_add(1)) < seqs.size();) {
+            res[i] = map_read(tidx, sk, p, seqs[i], lens[i], bk);
+            if (res[i].mapped) {
+                ReadResult copy = res[i];
+                lines[i] = render_paf(copy, names[i], p, 0.0);
+                lines[i] += '\n';
+            }
+        }
+    };
+    std::vector<std::thread> ts;
+    for (int t = 0; t < threads; t++) ts.emplace_back(work);
+    for (auto& t : ts) t.join();
+    size_t total = 0;
+    for (auto& l : lines) total += l.size();
+    text.clear();
+    text.reserve(total);
+    for (auto& l : lines) text += l;
+}
+
 // src/shmap/mod.rs:871-943 with mapping.rs:356-408
 std::string render_paf(ReadResult& rr, const std::string& query_id, const Params& p, double map_time) {
     Mapping& best = rr.best;

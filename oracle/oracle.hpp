@@ -226,6 +226,13 @@ std::vector<ReadResult> map_reads(const SketchIndex& tidx, const FracMinHash& sk
                                   const std::vector<const uint8_t*>& seqs,
                                   const std::vector<size_t>& lens, int threads);
 
+// map_reads plus the collector's in-order PAF text (mod.rs:374-650, 868-963):
+// every mapped read's line, t:f: printed as 0, joined in input order.
+void map_reads_paf(const SketchIndex& tidx, const FracMinHash& sk, const Params& p,
+                   const std::vector<const uint8_t*>& seqs, const std::vector<size_t>& lens,
+                   const std::vector<std::string>& names, int threads, std::vector<ReadResult>& res,
+                   std::string& text);
+
 // Fills the global stats and renders the reference's PAF line (mod.rs:871-943).
 std::string render_paf(ReadResult& rr, const std::string& query_id, const Params& p, double map_time);
 

@@ -83,6 +83,8 @@ def lib():
             ("orc_map", i32, [P, P, P, P, i32, i32, P]),
             ("orc_paf", i64, [P, P, P, P, ctypes.c_char_p, i32, i32, P, i64]),
             ("orc_time_map", dbl, [P, P, P, P, i32, i32]),
+            ("orc_map_paf", dbl, [P, P, P, P, ctypes.c_char_p, i32, i32, P, P]),
+            ("orc_take_text", i64, [P, i64]),
         ]:
             f = getattr(L, name)
             f.restype = res
@@ -295,6 +297,23 @@ class Index:
         buf = ctypes.create_string_buffer(n + 1)
         lib().orc_paf(self.h, ctypes.byref(p), _p(seq), _p(offs), joined, len(offs) - 1, threads, buf, n)
         return buf.raw[:n].decode()
+
+    def map_paf(self, p: OParams, seq: np.ndarray, offs: np.ndarray, names: Sequence[str], threads: int,
+                records: bool = True):
+        """Maps the reads with `threads` host threads and renders their PAF text
+        in input order (t:f: as 0): (records or None, text bytes, seconds of
+        mapping and rendering)."""
+        seq = np.ascontiguousarray(seq, np.uint8)
+        offs = np.ascontiguousarray(offs, np.int64)
+        n = len(offs) - 1
+        out = np.zeros(n, RECORD_DTYPE) if records else None
+        tl = ctypes.c_int64()
+        joined = "\n".join(names).encode()
+        secs = lib().orc_map_paf(self.h, ctypes.byref(p), _p(seq), _p(offs), joined, n, threads,
+                                 _p(out) if records else None, ctypes.byref(tl))
+        buf = np.empty(max(tl.value, 1), np.uint8)
+        lib().orc_take_text(_p(buf), tl.value)
+        return out, buf[:tl.value].tobytes(), float(secs)
 
     def time_map(self, p: OParams, seq: np.ndarray, offs: np.ndarray, threads: int) -> float:
         seq = np.ascontiguousarray(seq, np.uint8)

@@ -361,6 +361,18 @@ int shm_index_load(shm_ctx* ctx, const char* path, shm_index** out) {
     SHM_GUARD_END
 }
 
+int shm_index_file_check(const char* path) {
+    if (!path) return fail(SHM_ERR_INVALID, "null argument");
+    try {
+        shm::check_index_file(path);
+    } catch (const shm::IndexFileError& e) {
+        return fail(SHM_ERR_INVALID, e.what);
+    } catch (const std::exception& e) {
+        return fail(SHM_ERR_INVALID, e.what());
+    }
+    return SHM_OK;
+}
+
 int shm_index_info(const shm_index* idx, int32_t* k, double* h_frac, int32_t* max_matches) {
     if (!idx) return fail(SHM_ERR_INVALID, "null argument");
     if (k) *k = idx->s->k;
@@ -524,6 +536,21 @@ int shm_format_paf_device(shm_ctx* ctx, const shm_index* idx, const shm_params* 
             return fail(SHM_ERR_INVALID, "record with a segment the index does not have");
     SHM_GUARD_BEGIN
     const int64_t total = shm::format_paf_device(ctx->m, *idx->s, *p, rec, n, names, map_time, buf, cap);
+    *n_out = total;
+    if (buf && total > cap) return fail(SHM_ERR_CAPACITY, "output buffer too small");
+    return SHM_OK;
+    SHM_GUARD_END
+}
+
+int shm_map_paf(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
+                int32_t n, const char* names, shm_map_record* out, char* buf, int64_t cap, int64_t* n_out) {
+    int v = check_map_args(ctx, idx, p, n);
+    if (v != SHM_OK) return v;
+    if (!n_out || cap < 0) return fail(SHM_ERR_INVALID, "null argument");
+    if (n > 0 && (!seqs || !offs)) return fail(SHM_ERR_INVALID, "null argument");
+    if ((v = check_reads(offs, n)) != SHM_OK) return v;
+    SHM_GUARD_BEGIN
+    const int64_t total = shm::map_paf_host(ctx->m, *idx->s, *p, seqs, offs, n, names, out, buf, cap);
     *n_out = total;
     if (buf && total > cap) return fail(SHM_ERR_CAPACITY, "output buffer too small");
     return SHM_OK;

@@ -409,21 +409,74 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
 // k-mer and the CSR over distinct hashes; the derived arrays (forward-strand
 // prefix, directory, bucket table) are rebuilt on load by finish_index.
 // Layout, little endian, no padding:
-//   "SHMAPIX1", u32 version = 1, i32 k, f64 h_frac, i32 max_matches,
+//   "SHMAPIX1", u32 version = 2, i32 k, f64 h_frac, i32 max_matches,
 //   i32 n_seg, u32 n_keys, u32 n_kmers, u32 n_hits, shm_index_stats (8 i64);
 //   per segment: u32 name length, the name's bytes, i32 length in bases;
 //   u32 seg_off[n_seg+1], u64 ref_h[n_kmers], u32 ref_rs[n_kmers],
 //   u64 keys[n_keys], u32 key_off[n_keys+1], u32 hits[n_hits];
-//   u64 total byte count of everything before it (a truncation check).
+//   u64 byte count of everything before it (a truncation check), u64
+//   checksum of those bytes (IdxSum).
+// Reading checks every section on the host before any of it reaches the
+// device, so a damaged or hand-made file is refused instead of steering a
+// kernel outside its arrays: the checksum, then segment offsets ascending,
+// every reference k-mer's hash at most the threshold and its position inside
+// its segment and after the previous one, keys strictly ascending and at most
+// the threshold, hit-list offsets strictly ascending from 0 to n_hits, and
+// every hit a reference k-mer id, ascending within its list.
 static const char IDX_MAGIC[8] = {'S', 'H', 'M', 'A', 'P', 'I', 'X', '1'};
-static const uint32_t IDX_VERSION = 1;
+static const uint32_t IDX_VERSION = 2;
 
 namespace {
+
+// A 64-bit checksum of a byte stream fed in pieces of any size: 8-byte words
+// go round-robin into four multiply-rotate lanes (independent, so the host
+// overlaps them), the tail and the length close it.
+struct IdxSum {
+    uint64_t lane[4] = {0x9e3779b97f4a7c15ULL, 0xbf58476d1ce4e5b9ULL, 0x94d049bb133111ebULL, 0x2545f4914f6cdd1dULL};
+    uint64_t part = 0, words = 0, bytes = 0;
+    unsigned np = 0;
+    static uint64_t rotl(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+    void word(uint64_t w) {
+        uint64_t& h = lane[words & 3];
+        h = rotl(h ^ (w * 0xff51afd7ed558ccdULL), 29) * 0xc4ceb9fe1a85ec53ULL;
+        words++;
+    }
+    void add(const void* data, size_t n) {
+        const uint8_t* p = (const uint8_t*)data;
+        bytes += n;
+        while (np && n) {  // finish a word begun by an earlier piece
+            part |= (uint64_t)*p++ << (8 * np);
+            n--;
+            if (++np == 8) {
+                word(part);
+                part = 0;
+                np = 0;
+            }
+        }
+        for (; n >= 8; p += 8, n -= 8) {
+            uint64_t w;
+            std::memcpy(&w, p, 8);
+            word(w);
+        }
+        for (; n; n--) part |= (uint64_t)*p++ << (8 * np++);
+    }
+    uint64_t value() const {
+        IdxSum t = *this;
+        t.word(t.part ^ ((uint64_t)t.np << 56));
+        t.word(t.bytes);
+        uint64_t h = t.lane[0];
+        for (int i = 1; i < 4; i++) h = rotl(h, 17) ^ (t.lane[i] * 0x9e3779b97f4a7c15ULL);
+        return h ^ (h >> 31);
+    }
+};
+
 struct FileW {
     std::FILE* f;
     uint64_t n = 0;
+    IdxSum sum;
     void put(const void* p, size_t bytes) {
         if (bytes && std::fwrite(p, 1, bytes, f) != bytes) throw IndexFileError{"write failed"};
+        sum.add(p, bytes);
         n += bytes;
     }
     template <class T>
@@ -440,11 +493,14 @@ struct FileW {
         }
     }
 };
+
 struct FileR {
     std::FILE* f;
     uint64_t n = 0;
+    IdxSum sum;
     void get(void* p, size_t bytes) {
         if (bytes && std::fread(p, 1, bytes, f) != bytes) throw IndexFileError{"truncated or unreadable index file"};
+        sum.add(p, bytes);
         n += bytes;
     }
     template <class T>
@@ -453,17 +509,194 @@ struct FileR {
         get(&v, sizeof v);
         return v;
     }
+};
+
+[[noreturn]] void corrupt(const char* what) { throw IndexFileError{std::string("corrupt index file (") + what + ")"}; }
+
+// Where the checked sections go: device buffers on load, nowhere on a check.
+struct IdxUpload {
+    IndexStorage* ix;  // null: check only
     template <class T>
-    void dev(DevBuf<T>& d, size_t count, size_t reserve) {  // into a device buffer, in slices
-        d.reserve(reserve);
-        std::vector<T> h(std::min<size_t>(std::max<size_t>(count, 1), (size_t)1 << 24));
-        for (size_t i = 0; i < count; i += h.size()) {
-            const size_t c = std::min(h.size(), count - i);
-            get(h.data(), sizeof(T) * c);
-            SHM_CUDA(cudaMemcpy(d.p + i, h.data(), sizeof(T) * c, cudaMemcpyHostToDevice));
-        }
+    void slice(DevBuf<T>* d, size_t at, const T* h, size_t c) {
+        if (ix && c) SHM_CUDA(cudaMemcpy(d->p + at, h, sizeof(T) * c, cudaMemcpyHostToDevice));
+    }
+    template <class T>
+    void reserve(DevBuf<T>* d, size_t n) {
+        if (ix) d->reserve(n);
     }
 };
+
+// Reads the file at path, checking every section (see the layout above), into
+// ix when up.ix is set. Throws IndexFileError on any failure.
+void read_index_file(const char* path, IndexStorage& hx, IdxUpload up) {
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) throw IndexFileError{std::string("cannot open index file: ") + path};
+    FileR r{f};
+    try {
+        // the checksum first: a damaged file is refused before any array is examined
+        {
+            if (std::fseek(f, 0, SEEK_END) != 0) throw IndexFileError{"unreadable index file"};
+            const long size = std::ftell(f);
+            if (size < 16 + 8) throw IndexFileError{"truncated or unreadable index file"};
+            std::rewind(f);
+            IdxSum s;
+            std::vector<uint8_t> buf((size_t)1 << 22);
+            uint64_t left = (uint64_t)size - 16;
+            while (left) {
+                const size_t c = (size_t)std::min<uint64_t>(left, buf.size());
+                if (std::fread(buf.data(), 1, c, f) != c) throw IndexFileError{"truncated or unreadable index file"};
+                if (left == (uint64_t)size - 16 && c >= 12) {  // the magic and version decide the message
+                    if (std::memcmp(buf.data(), IDX_MAGIC, 8) != 0) throw IndexFileError{"not a shmap-b200 index file"};
+                    uint32_t v;
+                    std::memcpy(&v, buf.data() + 8, 4);
+                    if (v != IDX_VERSION) throw IndexFileError{"unsupported index file version"};
+                }
+                s.add(buf.data(), c);
+                left -= c;
+            }
+            uint64_t tail[2];
+            if (std::fread(tail, 1, 16, f) != 16) throw IndexFileError{"truncated or unreadable index file"};
+            if (tail[0] != (uint64_t)size - 16) throw IndexFileError{"corrupt or truncated index file"};
+            if (tail[1] != s.value()) throw IndexFileError{"corrupt index file (checksum)"};
+            std::rewind(f);
+        }
+        char magic[8];
+        r.get(magic, 8);
+        if (std::memcmp(magic, IDX_MAGIC, 8) != 0) throw IndexFileError{"not a shmap-b200 index file"};
+        if (r.val<uint32_t>() != IDX_VERSION) throw IndexFileError{"unsupported index file version"};
+        hx.k = r.val<int32_t>();
+        hx.h_frac = r.val<double>();
+        hx.max_matches = r.val<int32_t>();
+        const int32_t n_seg = r.val<int32_t>();
+        const uint32_t n_keys = r.val<uint32_t>(), n_kmers = r.val<uint32_t>(), n_hits = r.val<uint32_t>();
+        if (hx.k <= 0 || !(hx.h_frac > 0.0) || hx.h_frac > 1.0 || n_seg < 0 || n_keys > n_kmers ||
+            n_hits > n_kmers || n_keys > n_hits || hx.max_matches < -1)
+            throw IndexFileError{"corrupt index file header"};
+        const uint64_t thr = h_thres(hx.h_frac);
+        hx.stats = r.val<shm_index_stats>();
+        for (int32_t i = 0; i < n_seg; i++) {
+            const uint32_t len = r.val<uint32_t>();
+            if (len > (1u << 20)) corrupt("segment name");
+            std::string nm(len, '\0');
+            r.get(&nm[0], len);
+            hx.names.push_back(std::move(nm));
+            const int32_t sl = r.val<int32_t>();
+            if (sl < 0) corrupt("segment length");
+            hx.seg_len.push_back(sl);
+        }
+        hx.h_seg_off.resize((size_t)n_seg + 1);
+        r.get(hx.h_seg_off.data(), sizeof(uint32_t) * ((size_t)n_seg + 1));
+        if (hx.h_seg_off[0] != 0 || hx.h_seg_off[(size_t)n_seg] != n_kmers) corrupt("segment offsets");
+        for (int32_t i = 0; i < n_seg; i++) {
+            const uint32_t c = hx.h_seg_off[(size_t)i + 1] - hx.h_seg_off[(size_t)i];
+            if (hx.h_seg_off[(size_t)i + 1] < hx.h_seg_off[(size_t)i] ||
+                (int64_t)c > std::max<int64_t>(0, (int64_t)hx.seg_len[(size_t)i] - hx.k + 1))
+                corrupt("segment offsets");
+        }
+        IndexStorage* ix = up.ix;
+        if (ix) {
+            ix->seg_off.reserve((size_t)n_seg + 1);
+            SHM_CUDA(cudaMemcpy(ix->seg_off.p, hx.h_seg_off.data(), sizeof(uint32_t) * ((size_t)n_seg + 1),
+                                cudaMemcpyHostToDevice));
+            ix->seg_sz.reserve((size_t)n_seg + 1);
+            if (n_seg)
+                SHM_CUDA(cudaMemcpy(ix->seg_sz.p, hx.seg_len.data(), sizeof(int32_t) * (size_t)n_seg,
+                                    cudaMemcpyHostToDevice));
+        }
+        const size_t SL = (size_t)1 << 24;  // elements a slice
+        // reference k-mers: hashes at most the threshold
+        {
+            std::vector<uint64_t> h(std::min<size_t>(std::max<size_t>(n_kmers, 1), SL));
+            up.reserve(ix ? &ix->ref_h : nullptr, (size_t)n_kmers + 1);
+            for (size_t i = 0; i < n_kmers; i += h.size()) {
+                const size_t c = std::min(h.size(), (size_t)n_kmers - i);
+                r.get(h.data(), 8 * c);
+                for (size_t j = 0; j < c; j++)
+                    if (h[j] > thr) corrupt("reference k-mer hash above the threshold");
+                up.slice(ix ? &ix->ref_h : nullptr, i, h.data(), c);
+            }
+        }
+        // r << 1 | strand: inside the segment, after the previous k-mer of the segment
+        {
+            std::vector<uint32_t> v(std::min<size_t>(std::max<size_t>(n_kmers, 1), SL));
+            up.reserve(ix ? &ix->ref_rs : nullptr, (size_t)n_kmers + 1);
+            int32_t g = 0;
+            int64_t prev = -1;
+            for (size_t i = 0; i < n_kmers; i += v.size()) {
+                const size_t c = std::min(v.size(), (size_t)n_kmers - i);
+                r.get(v.data(), 4 * c);
+                for (size_t j = 0; j < c; j++) {
+                    const uint64_t gi = i + j;
+                    while (g < n_seg && gi >= hx.h_seg_off[(size_t)g + 1]) {
+                        g++;
+                        prev = -1;
+                    }
+                    const int64_t pos = (int64_t)(v[j] >> 1);
+                    if (g >= n_seg || pos < hx.k - 1 || pos >= hx.seg_len[(size_t)g] || pos <= prev)
+                        corrupt("reference k-mer position");
+                    prev = pos;
+                }
+                up.slice(ix ? &ix->ref_rs : nullptr, i, v.data(), c);
+            }
+        }
+        // keys: strictly ascending, at most the threshold
+        {
+            std::vector<uint64_t> h(std::min<size_t>(std::max<size_t>(n_keys, 1), SL));
+            up.reserve(ix ? &ix->keys : nullptr, (size_t)n_keys + 1);
+            bool first = true;
+            uint64_t prev = 0;
+            for (size_t i = 0; i < n_keys; i += h.size()) {
+                const size_t c = std::min(h.size(), (size_t)n_keys - i);
+                r.get(h.data(), 8 * c);
+                for (size_t j = 0; j < c; j++) {
+                    if (h[j] > thr || (!first && h[j] <= prev)) corrupt("keys");
+                    prev = h[j];
+                    first = false;
+                }
+                up.slice(ix ? &ix->keys : nullptr, i, h.data(), c);
+            }
+        }
+        // hit-list offsets: 0, strictly ascending, n_hits (kept on the host for the hits' check)
+        std::vector<uint32_t> ko((size_t)n_keys + 1);
+        r.get(ko.data(), 4 * ko.size());
+        if (ko[0] != 0 || ko[(size_t)n_keys] != n_hits) corrupt("hit-list offsets");
+        for (size_t i = 0; i < n_keys; i++) {
+            if (ko[i + 1] <= ko[i]) corrupt("hit-list offsets");
+            hx.max_list = std::max(hx.max_list, ko[i + 1] - ko[i]);
+        }
+        up.reserve(ix ? &ix->key_off : nullptr, (size_t)n_keys + 1);
+        up.slice(ix ? &ix->key_off : nullptr, 0, ko.data(), ko.size());
+        // hits: reference k-mer ids, ascending within each list
+        {
+            std::vector<uint32_t> v(std::min<size_t>(std::max<size_t>(n_hits, 1), SL));
+            up.reserve(ix ? &ix->hits : nullptr, (size_t)n_hits + 1);
+            size_t key = 0;
+            uint32_t prev = 0;
+            for (size_t i = 0; i < n_hits; i += v.size()) {
+                const size_t c = std::min(v.size(), (size_t)n_hits - i);
+                r.get(v.data(), 4 * c);
+                for (size_t j = 0; j < c; j++) {
+                    const size_t gi = i + j;
+                    while (gi >= ko[key + 1]) key++;
+                    if (v[j] >= n_kmers || (gi > ko[key] && v[j] <= prev)) corrupt("hits");
+                    prev = v[j];
+                }
+                up.slice(ix ? &ix->hits : nullptr, i, v.data(), c);
+            }
+        }
+        const uint64_t expect = r.n;
+        if (r.val<uint64_t>() != expect) throw IndexFileError{"corrupt or truncated index file"};
+        std::fclose(f);
+        f = nullptr;
+        hx.dev.n_keys = n_keys;
+        hx.dev.n_kmers = n_kmers;
+        hx.dev.n_hits = n_hits;
+    } catch (...) {
+        if (f) std::fclose(f);
+        throw;
+    }
+}
+
 }  // namespace
 
 void save_index(const IndexStorage* ix, const char* path) {
@@ -495,8 +728,9 @@ void save_index(const IndexStorage* ix, const char* path) {
         w.dev(ix->keys.p, d.n_keys);
         w.dev(ix->key_off.p, (size_t)d.n_keys + 1);
         w.dev(ix->hits.p, d.n_hits);
-        const uint64_t total = w.n;
+        const uint64_t total = w.n, sum = w.sum.value();  // both cover the bytes before them
         w.val(total);
+        w.val(sum);
     } catch (...) {
         std::fclose(f);
         throw;
@@ -504,58 +738,19 @@ void save_index(const IndexStorage* ix, const char* path) {
     if (std::fclose(f) != 0) throw IndexFileError{"write failed"};
 }
 
+void check_index_file(const char* path) {
+    IndexStorage hx;
+    read_index_file(path, hx, IdxUpload{nullptr});
+}
+
 IndexStorage* load_index(const char* path, cudaStream_t s) {
-    std::FILE* f = std::fopen(path, "rb");
-    if (!f) throw IndexFileError{std::string("cannot open index file: ") + path};
-    FileR r{f};
     auto* ix = new IndexStorage();
     try {
-        char magic[8];
-        r.get(magic, 8);
-        if (std::memcmp(magic, IDX_MAGIC, 8) != 0) throw IndexFileError{"not a shmap-b200 index file"};
-        if (r.val<uint32_t>() != IDX_VERSION) throw IndexFileError{"unsupported index file version"};
         SHM_CUDA(cudaGetDevice(&ix->device));
-        ix->k = r.val<int32_t>();
-        ix->h_frac = r.val<double>();
-        ix->max_matches = r.val<int32_t>();
-        const int32_t n_seg = r.val<int32_t>();
-        const uint32_t n_keys = r.val<uint32_t>(), n_kmers = r.val<uint32_t>(), n_hits = r.val<uint32_t>();
-        if (ix->k <= 0 || !(ix->h_frac > 0.0) || ix->h_frac > 1.0 || n_seg < 0 || n_keys > n_kmers ||
-            n_hits > n_kmers)
-            throw IndexFileError{"corrupt index file header"};
-        ix->stats = r.val<shm_index_stats>();
-        for (int32_t i = 0; i < n_seg; i++) {
-            const uint32_t len = r.val<uint32_t>();
-            if (len > (1u << 20)) throw IndexFileError{"corrupt index file (segment name)"};
-            std::string nm(len, '\0');
-            r.get(&nm[0], len);
-            ix->names.push_back(std::move(nm));
-            ix->seg_len.push_back(r.val<int32_t>());
-        }
-        ix->h_seg_off.resize((size_t)n_seg + 1);
-        r.get(ix->h_seg_off.data(), sizeof(uint32_t) * ((size_t)n_seg + 1));
-        if (ix->h_seg_off[0] != 0 || ix->h_seg_off[(size_t)n_seg] != n_kmers)
-            throw IndexFileError{"corrupt index file (segment offsets)"};
-        ix->seg_off.reserve((size_t)n_seg + 1);
-        SHM_CUDA(cudaMemcpy(ix->seg_off.p, ix->h_seg_off.data(), sizeof(uint32_t) * ((size_t)n_seg + 1),
-                            cudaMemcpyHostToDevice));
-        ix->seg_sz.reserve((size_t)n_seg + 1);
-        if (n_seg)
-            SHM_CUDA(cudaMemcpy(ix->seg_sz.p, ix->seg_len.data(), sizeof(int32_t) * (size_t)n_seg,
-                                cudaMemcpyHostToDevice));
-        r.dev(ix->ref_h, n_kmers, (size_t)n_kmers + 1);
-        r.dev(ix->ref_rs, n_kmers, (size_t)n_kmers + 1);
-        r.dev(ix->keys, n_keys, (size_t)n_keys + 1);
-        r.dev(ix->key_off, (size_t)n_keys + 1, (size_t)n_keys + 1);
-        r.dev(ix->hits, n_hits, (size_t)n_hits + 1);
-        const uint64_t expect = r.n;
-        if (r.val<uint64_t>() != expect) throw IndexFileError{"corrupt or truncated index file"};
-        std::fclose(f);
-        f = nullptr;
-        finish_index(ix, h_thres(ix->h_frac), n_keys, n_kmers, n_hits, (uint32_t)ix->stats.highest_freq_kmer, s);
+        read_index_file(path, *ix, IdxUpload{ix});
+        finish_index(ix, h_thres(ix->h_frac), ix->dev.n_keys, ix->dev.n_kmers, ix->dev.n_hits, ix->max_list, s);
         return ix;
     } catch (...) {
-        if (f) std::fclose(f);
         delete ix;
         throw;
     }

@@ -67,6 +67,7 @@ struct IndexStorage {
     double h_frac = 0;
     int32_t max_matches = -1;
     int device = 0;
+    uint32_t max_list = 0;  // longest hit list (set when read from a file)
 };
 
 // An index written to a file and read back (shm_index.cu); failures throw
@@ -76,6 +77,8 @@ struct IndexFileError {
 };
 void save_index(const IndexStorage* ix, const char* path);
 IndexStorage* load_index(const char* path, cudaStream_t s);
+// The checks load_index makes, on the host alone (no device is touched).
+void check_index_file(const char* path);
 
 // The segments' bases are read from h_seq (host) or, when d_seq is given,
 // from device memory (d_seq + seg_off[i], 32 readable bytes past the end).

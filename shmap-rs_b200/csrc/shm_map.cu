@@ -3165,8 +3165,8 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
 // is mapped (two device buffers, each reused once the sketch of the batch
 // before has read it), so the transfer of the reads overlaps the mapping when
 // `seqs` is pinned; records come back batch by batch.
-void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
-              int32_t n, shm_map_record* out, bool plain) {
+bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
+              int32_t n, shm_map_record* out, bool plain, BatchSink* sink) {
     SHM_CUDA(cudaSetDevice(c->device));
     MapScratch& S = *c->scr;
     cudaStream_t s = c->stream;
@@ -3243,6 +3243,7 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         run_batch(c, ix, p, nullptr, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b],
                   S.pk_codes[b & 1].p, S.pk_mask[b & 1].p);
         c->sketch_done = nullptr;
+        if (sink) sink->batch(i, j, S.out.p, s);
         copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s);
         if (b + 1 < batches.size()) {
@@ -3255,8 +3256,10 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     SHM_CUDA(cudaStreamSynchronize(s));
     H.mark("drain");
     // a batch with more bucket jobs than its capacity is mapped again with exact sizes
+    bool changed = false;
     for (size_t b = 0; b < batches.size(); b++) {
         if (slots[b].R->nj <= slots[b].job_cap) continue;
+        changed = true;
         const auto [i, j] = batches[b];
         const int64_t nb = offs[j] - offs[i];
         S.seqb[0].reserve((size_t)nb + 32);
@@ -3273,6 +3276,7 @@ void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     retry_overflows(c, ix, p, ovf_all, offs, RetryIO{nullptr, nullptr, seqs, out});
     H.mark("retry");
     H.print("host-form", n);
+    return changed || !ovf_all.empty();
 }
 
 }  // namespace shm

@@ -84,8 +84,19 @@ void mapctx_destroy(MapCtx* c);
 void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
                 int32_t n, shm_map_record* d_out, bool plain);
 
-// Host-buffer form: copies each batch in, maps it, copies records out.
-void map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
-              int32_t n, shm_map_record* out, bool plain);
+// Takes each batch's records while they are still on the device: batch(i, j,
+// d_rec, s) is called, in batch order, right after reads [i, j) are mapped,
+// with their records at d_rec (device) valid for work queued on stream s.
+struct BatchSink {
+    virtual void batch(int32_t i, int32_t j, const shm_map_record* d_rec, cudaStream_t s) = 0;
+    virtual ~BatchSink() = default;
+};
+
+// Host-buffer form: copies each batch in, maps it, copies records out. With a
+// sink, returns true when some records changed after the sink had taken them
+// (a batch mapped again with exact sizes, or reads retried); out then holds
+// the final records.
+bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
+              int32_t n, shm_map_record* out, bool plain, BatchSink* sink = nullptr);
 
 }  // namespace shm

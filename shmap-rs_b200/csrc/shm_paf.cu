@@ -289,6 +289,29 @@ __global__ void k_paf_write(PafView v, const uint64_t* __restrict__ off, char* _
     }
 }
 
+// Lines of a batch at their places in one text buffer: line i at base +
+// off[i], where base (device) is the length of the batches' text before this
+// one. A line that would end past cap is not written; *overflow is set.
+__global__ void k_paf_write_at(PafView v, const uint64_t* __restrict__ off, const uint64_t* __restrict__ base,
+                               char* __restrict__ text, uint64_t cap, uint32_t* __restrict__ overflow) {
+    const uint64_t b0 = *base;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < v.n; i += gridDim.x * blockDim.x) {
+        const uint64_t at = b0 + off[i], end = b0 + off[i + 1];
+        if (end == at) continue;
+        if (end > cap) {
+            atomicOr(overflow, 1u);
+            continue;
+        }
+        Out o{text + at, 0};
+        render(o, v, i);
+    }
+}
+
+// The text of the batch just written moves the base past it.
+__global__ void k_paf_advance(uint64_t* __restrict__ base, const uint64_t* __restrict__ off, int32_t n) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *base += off[n];
+}
+
 }  // namespace
 
 struct PafScratch {
@@ -297,7 +320,15 @@ struct PafScratch {
     DevBuf<int64_t> qse, soff;
     DevBuf<int32_t> slen;
     DevBuf<double> mt;
-    DevBuf<uint64_t> len, off;
+    DevBuf<uint64_t> len, off, base;
+    DevBuf<uint32_t> flag;
+    shm_map_record* h_rec = nullptr;  // pinned records of shm_map_paf calls that pass none
+    size_t h_rec_cap = 0;
+    uint64_t* h_small = nullptr;  // pinned readback: text length, overflow flag
+    ~PafScratch() {
+        if (h_rec) cudaFreeHost(h_rec);
+        if (h_small) cudaFreeHost(h_small);
+    }
 };
 
 void paf_scratch_free(PafScratch* p) { delete p; }
@@ -307,11 +338,11 @@ static PafScratch& paf_scratch(MapCtx* c) {
     return *c->paf;
 }
 
-int64_t format_paf_device(MapCtx* c, const IndexStorage& ix, const shm_params& p, const shm_map_record* rec,
-                          int32_t n, const char* names, const double* map_time, char* buf, int64_t cap) {
-    SHM_CUDA(cudaSetDevice(c->device));
-    cudaStream_t s = c->stream;
-    // query names: split on '\n' as shm_format_paf does; name i is q[qse[2i], qse[2i+1])
+// Query names split on '\n' as shm_format_paf does (name i is q[qse[2i],
+// qse[2i+1])), the segment names joined with their offsets, all uploaded on
+// stream s; returns the view of them (records, count and map times unset).
+static PafView upload_names(MapCtx* c, PafScratch& P, const IndexStorage& ix, const shm_params& p, int32_t n,
+                            const char* names, cudaStream_t s) {
     const char* q = names ? names : "";
     const size_t qlen = std::strlen(q);
     std::vector<int64_t> qse(2 * (size_t)n + 1, 0);
@@ -328,8 +359,6 @@ int64_t format_paf_device(MapCtx* c, const IndexStorage& ix, const shm_params& p
         sn += x;
         soff.push_back((int64_t)sn.size());
     }
-    PafScratch& P = paf_scratch(c);
-    P.rec.reserve((size_t)std::max(n, 1));
     P.q.reserve(qlen + 1);
     P.sn.reserve(sn.size() + 1);
     P.qse.reserve(qse.size());
@@ -337,8 +366,6 @@ int64_t format_paf_device(MapCtx* c, const IndexStorage& ix, const shm_params& p
     P.slen.reserve(ix.seg_len.size() + 1);
     P.len.reserve((size_t)n + 1);
     P.off.reserve((size_t)n + 1);
-    if (map_time && n) P.mt.reserve((size_t)n);
-    if (n) SHM_CUDA(cudaMemcpyAsync(P.rec.p, rec, sizeof(shm_map_record) * (size_t)n, cudaMemcpyHostToDevice, s));
     if (qlen) SHM_CUDA(cudaMemcpyAsync(P.q.p, q, qlen, cudaMemcpyHostToDevice, s));
     if (!sn.empty()) SHM_CUDA(cudaMemcpyAsync(P.sn.p, sn.data(), sn.size(), cudaMemcpyHostToDevice, s));
     SHM_CUDA(cudaMemcpyAsync(P.qse.p, qse.data(), sizeof(int64_t) * qse.size(), cudaMemcpyHostToDevice, s));
@@ -346,21 +373,36 @@ int64_t format_paf_device(MapCtx* c, const IndexStorage& ix, const shm_params& p
     if (!ix.seg_len.empty())
         SHM_CUDA(cudaMemcpyAsync(P.slen.p, ix.seg_len.data(), sizeof(int32_t) * ix.seg_len.size(),
                                  cudaMemcpyHostToDevice, s));
-    if (map_time && n)
-        SHM_CUDA(cudaMemcpyAsync(P.mt.p, map_time, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
-    c->work[W_H2D_BYTES] += (int64_t)(sizeof(shm_map_record) * (size_t)n + qlen + sn.size());
+    // the query and segment names and their offset tables
+    c->work[W_H2D_BYTES] += (int64_t)(qlen + sn.size() + sizeof(int64_t) * (qse.size() + soff.size()) +
+                                      sizeof(int32_t) * ix.seg_len.size());
     PafView v{};
-    v.rec = P.rec.p;
-    v.n = n;
     v.qnames = P.q.p;
     v.qse = P.qse.p;
     v.snames = P.sn.p;
     v.soff = P.soff.p;
     v.slen = P.slen.p;
-    v.map_time = map_time && n ? P.mt.p : nullptr;
     v.k = p.k;
     v.theta = p.theta;
     v.min_diff = p.min_diff;
+    return v;
+}
+
+int64_t format_paf_device(MapCtx* c, const IndexStorage& ix, const shm_params& p, const shm_map_record* rec,
+                          int32_t n, const char* names, const double* map_time, char* buf, int64_t cap) {
+    SHM_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    PafScratch& P = paf_scratch(c);
+    P.rec.reserve((size_t)std::max(n, 1));
+    if (map_time && n) P.mt.reserve((size_t)n);
+    PafView v = upload_names(c, P, ix, p, n, names, s);
+    if (n) SHM_CUDA(cudaMemcpyAsync(P.rec.p, rec, sizeof(shm_map_record) * (size_t)n, cudaMemcpyHostToDevice, s));
+    if (map_time && n)
+        SHM_CUDA(cudaMemcpyAsync(P.mt.p, map_time, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
+    c->work[W_H2D_BYTES] += (int64_t)((sizeof(shm_map_record) + (map_time ? sizeof(double) : 0)) * (size_t)n);
+    v.rec = P.rec.p;
+    v.n = n;
+    v.map_time = map_time && n ? P.mt.p : nullptr;
     int64_t total = 0;
     if (n) {
         k_paf_len<<<grid_for((size_t)n, 128, 8), 128, 0, s>>>(v, P.len.p);
@@ -377,6 +419,91 @@ int64_t format_paf_device(MapCtx* c, const IndexStorage& ix, const shm_params& p
         k_paf_write<<<grid_for((size_t)n, 128, 8), 128, 0, s>>>(v, P.off.p, P.text.p);
         SHM_CUDA(cudaGetLastError());
         count_launch();
+        const int64_t take = std::min(cap, total);
+        SHM_CUDA(cudaMemcpyAsync(buf, P.text.p, (size_t)take, cudaMemcpyDeviceToHost, s));
+        c->work[W_D2H_BYTES] += take;
+        SHM_CUDA(cudaStreamSynchronize(s));
+    }
+    return total;
+}
+
+namespace {
+
+// Renders each batch's lines as soon as its records are on the device, into
+// one text buffer, in read order.
+struct PafSink : BatchSink {
+    MapCtx* c;
+    PafScratch* P;
+    PafView v0;
+    uint64_t cap;
+    void batch(int32_t i, int32_t j, const shm_map_record* d_rec, cudaStream_t s) override {
+        const int32_t n = j - i;
+        if (n <= 0) return;
+        PafView v = v0;
+        v.rec = d_rec;
+        v.n = n;
+        v.qse = P->qse.p + 2 * (size_t)i;
+        k_paf_len<<<grid_for((size_t)n, 128, 8), 128, 0, s>>>(v, P->len.p);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+        exclusive_scan_u64(P->len.p, P->off.p, (size_t)n, s);
+        k_paf_write_at<<<grid_for((size_t)n, 128, 8), 128, 0, s>>>(v, P->off.p, P->base.p, P->text.p, cap,
+                                                                   P->flag.p);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+        k_paf_advance<<<1, 32, 0, s>>>(P->base.p, P->off.p, n);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+    }
+};
+
+}  // namespace
+
+int64_t map_paf_host(MapCtx* c, const IndexStorage& ix, const shm_params& p, const uint8_t* seqs,
+                     const int64_t* offs, int32_t n, const char* names, shm_map_record* out, char* buf,
+                     int64_t cap) {
+    SHM_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    PafScratch& P = paf_scratch(c);
+    shm_map_record* rec = out;
+    if (!rec) {  // records land in pinned memory, so that their copies stay asynchronous
+        if (P.h_rec_cap < (size_t)n || !P.h_rec) {
+            if (P.h_rec) SHM_CUDA(cudaFreeHost(P.h_rec));
+            P.h_rec = nullptr;
+            P.h_rec_cap = 0;
+            SHM_CUDA(cudaHostAlloc(&P.h_rec, sizeof(shm_map_record) * (size_t)std::max(n, 1), cudaHostAllocDefault));
+            P.h_rec_cap = (size_t)std::max(n, 1);
+        }
+        rec = P.h_rec;
+    }
+    if (!P.h_small) SHM_CUDA(cudaHostAlloc(&P.h_small, 2 * sizeof(uint64_t), cudaHostAllocDefault));
+    PafView v = upload_names(c, P, ix, p, n, names, s);
+    v.map_time = nullptr;
+    // room for every line: a line is its query name, a segment name and at
+    // most about 700 bytes of numbers and tags (t:f: is 0 here); a line that
+    // would not fit sends the call to the two-pass path below
+    size_t seg_name = 0;
+    for (const std::string& x : ix.names) seg_name = std::max(seg_name, x.size());
+    const uint64_t tcap = (uint64_t)std::strlen(names ? names : "") + (uint64_t)n * (seg_name + 1024) + 64;
+    P.text.reserve((size_t)tcap);
+    P.base.reserve(1);
+    P.flag.reserve(1);
+    SHM_CUDA(cudaMemsetAsync(P.base.p, 0, sizeof(uint64_t), s));
+    SHM_CUDA(cudaMemsetAsync(P.flag.p, 0, sizeof(uint32_t), s));
+    PafSink sink;
+    sink.c = c;
+    sink.P = &P;
+    sink.v0 = v;
+    sink.cap = tcap;
+    const bool changed = map_host(c, &ix, p, seqs, offs, n, rec, false, &sink);
+    if (changed)  // records replaced after their batch's text was written: render from the final records
+        return format_paf_device(c, ix, p, rec, n, names, nullptr, buf, cap);
+    SHM_CUDA(cudaMemcpyAsync(P.h_small, P.base.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaMemcpyAsync(P.h_small + 1, P.flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SHM_CUDA(cudaStreamSynchronize(s));
+    if ((uint32_t)P.h_small[1] != 0) return format_paf_device(c, ix, p, rec, n, names, nullptr, buf, cap);
+    const int64_t total = (int64_t)P.h_small[0];
+    if (buf && cap > 0 && total > 0) {
         const int64_t take = std::min(cap, total);
         SHM_CUDA(cudaMemcpyAsync(buf, P.text.p, (size_t)take, cudaMemcpyDeviceToHost, s));
         c->work[W_D2H_BYTES] += take;

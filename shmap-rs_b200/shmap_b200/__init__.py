@@ -101,6 +101,7 @@ def lib() -> ctypes.CDLL:
         "shm_index_save": (ctypes.c_int, [P, ctypes.c_char_p]),
         "shm_index_load": (ctypes.c_int, [P, ctypes.c_char_p, P]),
         "shm_index_info": (ctypes.c_int, [P, P, P, P]),
+        "shm_index_file_check": (ctypes.c_int, [ctypes.c_char_p]),
         "shm_index_stats_get": (ctypes.c_int, [P, P]),
         "shm_index_count": (ctypes.c_int, [P, P, P, i64, P]),
         "shm_index_hits": (ctypes.c_int, [P, P, u64, P, P, P, P, i64, P]),
@@ -108,6 +109,7 @@ def lib() -> ctypes.CDLL:
         "shm_map_batch": (ctypes.c_int, [P, P, P, P, P, i32, P]),
         "shm_map_plain": (ctypes.c_int, [P, P, P, P, P, i32, P]),
         "shm_map_batch_device": (ctypes.c_int, [P, P, P, P, P, P, i32, P]),
+        "shm_map_paf": (ctypes.c_int, [P, P, P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
         "shm_format_paf": (ctypes.c_int, [P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
         "shm_ctx_stream": (P, [P]),
         "shm_ctx_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
@@ -382,6 +384,30 @@ class SketchIndex:
         cp = params.c()
         _check(lib().shm_map_batch_device(self.ctx.h, self.h, ctypes.byref(cp), d_seq_ptr, 0, _ptr(h_offs),
                                           len(h_offs) - 1, d_out_ptr))
+
+    def map_paf(self, params: Params, seq: np.ndarray, offs: np.ndarray, names: Sequence[str],
+                with_records: bool = True):
+        """Mapper.map_reads as the command line runs it (shm_map_paf): reads
+        in, the PAF text of the mapped ones out, rendered on the device batch
+        by batch (t:f: as 0). Returns (text, records or None)."""
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        offs = np.ascontiguousarray(offs, dtype=np.int64)
+        n = len(offs) - 1
+        joined = "\n".join(names).encode()
+        out = np.zeros(n, RECORD_DTYPE) if with_records else None
+        cp = params.c()
+        need = ctypes.c_int64()
+        cap = 640 * n + len(joined) + 1  # a line is about 480 bytes plus its names
+        buf = ctypes.create_string_buffer(cap)
+        rc = lib().shm_map_paf(self.ctx.h, self.h, ctypes.byref(cp), _ptr(seq), _ptr(offs), n, joined,
+                               0 if out is None else _ptr(out), buf, cap, ctypes.byref(need))
+        if rc == SHM_ERR_CAPACITY:
+            cap = need.value + 1
+            buf = ctypes.create_string_buffer(cap)
+            rc = lib().shm_map_paf(self.ctx.h, self.h, ctypes.byref(cp), _ptr(seq), _ptr(offs), n, joined,
+                                   0 if out is None else _ptr(out), buf, cap, ctypes.byref(need))
+        _check(rc)
+        return ctypes.string_at(buf, need.value).decode(), out
 
     def format_paf(self, params: Params, records: np.ndarray, names: Sequence[str],
                    map_time: Optional[np.ndarray] = None) -> str:

@@ -359,3 +359,24 @@ def test_pinned_host_batches(gpu_ctx):
     torch.cuda.synchronize()
     dev = d_out.cpu().numpy().view(sb.RECORD_DTYPE)
     assert not record_mismatches(dev, want)
+
+
+def test_hifi_five_percent_scale(gpu_ctx):
+    """The hifi configuration at 5% scale: a 155 Mbp reference with its
+    satellite arrays and interspersed repeats, 7,500 HiFi-like reads (lists of
+    hundreds of hits per k-mer, reads up to 60 kb). Every record equals the
+    oracle's bit for bit, and the PAF text of shm_map_paf (reads in, text out)
+    equals the oracle's byte for byte, t:f: aside (tests/golden_paf.rs:13-53)."""
+    gen = synth.Genome(synth.scaled(synth.REFS["human31"], 0.05))
+    names, seq, offs = gen.reads(synth.scaled(synth.READS["hifi"], 0.05))
+    assert len(names) == 7500
+    g = sb.SketchIndex(gpu_ctx, gen.names, gen.seq, gen.seg_off, 25, 0.01)
+    o = O.Index(gen.names, gen.seq, gen.seg_off, 25, 0.01, threads=os.cpu_count() or 4)
+    assert g.stats() == o.stats()
+    text, rec = g.map_paf(sb.Params(k=25, h_frac=0.01, theta=0.4), seq, offs, names)
+    orec, otext, _ = o.map_paf(O.params(k=25, h_frac=0.01, theta=0.4), seq, offs, names, os.cpu_count() or 4)
+    mm = record_mismatches(rec, orec)
+    assert not mm, f"record mismatches (read, field, gpu, oracle): {mm}"
+    assert strip_t(text) == strip_t(otext.decode())
+    assert (rec["status"] == 0).mean() > 0.9
+    g.close()

@@ -83,3 +83,26 @@ def test_bad_index_files_are_refused(gpu_ctx, tmp_path):
             sb.SketchIndex.load(gpu_ctx, path)
         assert e.value.code == -1, name  # SHM_ERR_INVALID
     g.close()
+
+
+def test_file_written_from_the_oracle_loads_as_the_built_index(gpu_ctx, tmp_path):
+    """A file written in the library's format from the CPU oracle's index
+    (tests/test_index_file_check.py's writer) loads and answers as the index
+    built on the device: the file format is the oracle's index, section for
+    section."""
+    from test_index_file_check import index_sections, write_index
+
+    recs = _records()
+    path = str(tmp_path / "oracle.shmapidx")
+    write_index(path, index_sections(recs, 12, 0.2))
+    g = sb.SketchIndex.from_records(gpu_ctx, recs, 12, 0.2)
+    h = sb.SketchIndex.load(gpu_ctx, path)
+    assert h.stats() == g.stats()
+    hs = np.unique(np.concatenate([g.segment(i)[1] for i in range(len(recs))]))
+    assert np.array_equal(g.count(hs), h.count(hs))
+    reads = _reads(recs, 100)
+    seq, offs = pack([s for _, s in reads])
+    p = sb.Params(k=12, h_frac=0.2, theta=0.4)
+    assert not record_mismatches(g.map_reads(p, seq, offs), h.map_reads(p, seq, offs))
+    h.close()
+    g.close()

@@ -93,3 +93,35 @@ def test_capacity(gpu_ctx, golden_dir):
                                         "\n".join(names).encode(), None, buf, 50, ctypes.byref(need))
     assert rc == sb.SHM_ERR_CAPACITY and need.value == len(full)
     assert buf.raw[:50] == full[:50]
+
+
+@pytest.mark.parametrize("env", [{}, {"SHMAP_FAST_JOB_CAP": "7"}])
+@pytest.mark.parametrize("metric", ["Containment", "bucket_SH"])
+def test_map_paf(gpu_ctx, monkeypatch, metric, env):
+    """shm_map_paf (reads in, PAF text out, each batch rendered on the device
+    as soon as it is mapped) gives the host formatter's bytes over the same
+    records, and the oracle's PAF (t:f: aside). More reads than one host batch
+    holds, so several batches write into the one text; with a tiny bucket-job
+    capacity batches are mapped again and the call renders from the final
+    records instead."""
+    import oracle as O
+
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    gen = synth.Genome(synth.REFS["uniform5m"])
+    names, seq, offs = gen.reads(synth.scaled(synth.READS["fixed10k"], 2.5))  # 5,000 reads, 50 Mbp
+    names = [f"{n} extra-{i}" if i % 7 == 0 else n for i, n in enumerate(names)]
+    g = sb.SketchIndex.from_records(gpu_ctx, gen.records(), 25, 0.01)
+    p = sb.Params(k=25, h_frac=0.01, theta=0.4, metric=metric)
+    text, rec = g.map_paf(p, seq, offs, names)
+    assert not np.any(rec["status"] == 3)
+    assert text == g.format_paf(p, rec, names)
+    o = O.Index.from_records(gen.records(), 25, 0.01, threads=8)
+    orec, otext, _ = o.map_paf(O.params(k=25, h_frac=0.01, theta=0.4, metric=metric), seq, offs, names, 8)
+    assert rec.tobytes() == orec.tobytes()
+    assert sb.strip_timing(text) == sb.strip_timing(otext.decode())
+    assert len(text.splitlines()) == int((rec["status"] == 0).sum()) > 4000
+    t2, r2 = g.map_paf(p, seq[: offs[3]], offs[:4], names[:3], with_records=False)
+    assert r2 is None and t2 == g.format_paf(p, rec[:3], names[:3])
+    t0, _ = g.map_paf(p, seq[:0], offs[:1], [])
+    assert t0 == ""
