@@ -499,8 +499,23 @@ def run_ours(args, rank, world, local):
     fasta_parse = _extra("fasta_parse", _fasta_parse) if rank == 0 and args.side else None
 
     def _serving():
-        res = serve_load(ctx, idx, p, h_seq_np, offs, rec, [10_000, 50_000, 200_000, 1_000_000],
-                         args.serve_seconds, 11)
+        # the configuration's mix: HiFi-like requests from the workload's reads and
+        # ONT-like ones from a second read set of the same genome
+        from shmap_b200 import synth
+
+        sets = [("hifi" if args.workload == "hifi" else args.workload, h_seq_np, offs, rec)]
+        if args.workload == "hifi":
+            qs = synth.READS["ont"]
+            if args.scale != 1.0:
+                qs = synth.scaled(qs, args.scale)
+            qs = synth.scaled(qs, min(1.0, 20_000 / qs.n_reads))
+            o_names, o_seq, o_offs = gen.reads(qs)
+            o_h = torch.empty(int(o_offs[-1]) + 32, dtype=torch.uint8).pin_memory()
+            o_h[: int(o_offs[-1])].copy_(torch.from_numpy(np.ascontiguousarray(o_seq)))
+            o_h_np = o_h.numpy()
+            o_rec = idx.map_reads(p, o_h_np[: int(o_offs[-1])], o_offs)
+            sets.append(("ont", o_h_np, o_offs, o_rec))
+        res = serve_load(ctx, idx, p, sets, [10_000, 50_000, 200_000, 1_000_000], args.serve_seconds, 11)
         log(f"[bench] serving: {res}")
         return res
 
@@ -629,28 +644,39 @@ def run_ours(args, rank, world, local):
 
 
 
-def serve_load(ctx, idx, p, h_seq_np, offs, rec, rates, seconds: float, seed: int):
-    """Serving (shm_server_*): requests of 1-4,096 reads (uniform), each a run of
-    the workload's reads read in place from the pinned buffer, arrive as a
-    Poisson process at each offered rate (reads/s) for `seconds`. Reports the
-    achieved rate and the per-read latency percentiles (a read's latency is its
-    request's, submit to records written), and checks every request's records
-    against the same reads' records mapped alone in one call."""
+def serve_load(ctx, idx, p, sets, rates, seconds: float, seed: int):
+    """Serving (shm_server_*): requests of 1-4,096 reads (uniform), each a run
+    of reads of one of the read sets (HiFi-like or ONT-like, chosen at random
+    per request) read in place from pinned memory, arrive as a Poisson process
+    at each offered rate (reads/s) for `seconds`. Reports the achieved rate,
+    the per-read latency percentiles (a read's latency is its request's,
+    submit to records written), how many requests a batch carried, and
+    checks every request's records against the same reads mapped alone in
+    one call. sets: [(name, pinned bytes, offsets, records alone)]."""
     import threading
 
     import shmap_b200 as sb
 
-    n = len(offs) - 1
     rng = np.random.default_rng(seed)
     out = []
     same = True
+
+    def draw():
+        si = int(rng.integers(0, len(sets)))
+        _, _, o, _ = sets[si]
+        n = len(o) - 1
+        size = int(rng.integers(1, min(4096, n) + 1))
+        a = int(rng.integers(0, n - size + 1))
+        return si, a, size
+
     with sb.Server(ctx, idx, p, slots=2) as srv:
         # warm-up: full batches on both slots, so that their buffers are grown
         warm = []
         for _ in range(8):
-            size = min(4096, n)
-            a = int(rng.integers(0, n - size + 1))
-            warm.append(srv.submit(h_seq_np, offs[a:a + size + 1]))
+            si = len(warm) % len(sets)
+            _, hs, o, _ = sets[si]
+            size = min(4096, len(o) - 1)
+            warm.append(srv.submit(hs, o[:size + 1]))
         for t in warm:
             if srv.poll(t, 120_000) is None:
                 raise RuntimeError("a serving warm-up request did not finish within 120 s")
@@ -660,26 +686,25 @@ def serve_load(ctx, idx, p, h_seq_np, offs, rec, rates, seconds: float, seed: in
                 t += rng.exponential(2048.5 / rate)
                 if t > seconds:
                     break
-                size = int(rng.integers(1, min(4096, n) + 1))
-                a = int(rng.integers(0, n - size + 1))
-                plan.append((t, a, size))
+                plan.append((t,) + draw())
             tickets = [None] * len(plan)
             ready = threading.Semaphore(0)
 
             def submitter():
                 t0 = time.perf_counter()
-                for i, (at, a, size) in enumerate(plan):
+                for i, (at, si, a, size) in enumerate(plan):
                     delay = at - (time.perf_counter() - t0)
                     if delay > 0:
                         time.sleep(delay)
-                    tickets[i] = srv.submit(h_seq_np, offs[a:a + size + 1])
+                    _, hs, o, _ = sets[si]
+                    tickets[i] = srv.submit(hs, o[a:a + size + 1])
                     ready.release()
 
             w0 = time.perf_counter()
             th = threading.Thread(target=submitter)
             th.start()
-            lat, sizes, batch_req = [], [], []
-            for i, (at, a, size) in enumerate(plan):
+            lat, sizes, batch_req, kinds = [], [], [], []
+            for i, (at, si, a, size) in enumerate(plan):
                 ready.acquire()
                 done = srv.poll(tickets[i], 120_000)
                 if done is None:
@@ -688,21 +713,24 @@ def serve_load(ctx, idx, p, h_seq_np, offs, rec, rates, seconds: float, seed: in
                 lat.append(stt["total_ms"])
                 sizes.append(size)
                 batch_req.append(stt["batch_requests"])
-                if not np.array_equal(got.view(np.uint8), rec[a:a + size].view(np.uint8)):
+                kinds.append(si)
+                if not np.array_equal(got.view(np.uint8), sets[si][3][a:a + size].view(np.uint8)):
                     same = False
             wall = time.perf_counter() - w0
             th.join()
             per_read = np.repeat(np.array(lat), np.array(sizes))
+            br = np.array(batch_req)
             out.append({"offered_reads_per_s": rate, "arrived_reads_per_s": round(sum(sizes) / seconds, 1),
                         "achieved_reads_per_s": round(sum(sizes) / wall, 1),
                         "requests": len(plan), "reads": int(sum(sizes)),
+                        "requests_by_kind": {sets[j][0]: int(sum(1 for x in kinds if x == j)) for j in range(len(sets))},
                         "p50_ms": round(float(np.percentile(per_read, 50)), 3),
                         "p99_ms": round(float(np.percentile(per_read, 99)), 3),
-                        "mean_requests_per_batch": round(float(np.mean(batch_req)), 2)})
-    return {"arrivals": f"Poisson, requests of 1-4,096 reads (uniform), {seconds:g} s per offered rate",
+                        "mean_requests_per_batch": round(float(br.mean()), 2) if len(br) else 0.0,
+                        "requests_in_merged_batches": round(float((br > 1).mean()), 3) if len(br) else 0.0})
+    return {"arrivals": f"Poisson, requests of 1-4,096 reads (uniform) of one kind each "
+                        f"({' or '.join(x[0] for x in sets)}, at random), {seconds:g} s per offered rate",
             "slots": 2, "rates": out, "records_same_as_alone": same}
-
-
 
 
 def cpu_reference(gen, names, seq, offs, wk, target_s: float, threads: int, steps: int = 1, oi=None):

@@ -260,7 +260,9 @@ int shm_map_fasta(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const
  * submitted at any time from any thread, each request's records in its
  * input order. Its slots, each a device context with its own stream, take
  * the queued requests in arrival order, as many as fit max_batch_reads reads
- * and, in bases, the slot's share of hbm_budget, and map them as one batch;
+ * and, in bases, the slot's share of hbm_budget, and map them as one batch (a
+ * request larger than that is mapped in parts, so no batch exceeds the
+ * budget; shm_submit refuses a single read longer than a batch holds);
  * requests that arrive meanwhile join the next batch a slot takes, and the
  * slots' batches run on the device at the same time. A read's record does
  * not depend on the requests it is batched with. */

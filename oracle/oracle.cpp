@@ -1108,6 +1108,48 @@ std::string render_paf(ReadResult& rr, const std::string& query_id, const Params
 }
 
 // ---------------------------------------------------------------- io
+// String::from_utf8_lossy, which src/io/mod.rs:408-410 applies to every
+// record id: each maximal subpart of an ill-formed UTF-8 sequence becomes one
+// U+FFFD, per the Unicode standard's well-formed byte sequence table.
+static std::string from_utf8_lossy(const std::string& s) {
+    std::string out;
+    size_t i = 0;
+    const size_t n = s.size();
+    while (i < n) {
+        const unsigned char c = (unsigned char)s[i];
+        if (c < 0x80) {
+            out.push_back((char)c);
+            i++;
+            continue;
+        }
+        int len = 0;
+        unsigned char first_lo = 0x80, first_hi = 0xbf;
+        if (c >= 0xc2 && c <= 0xdf) {
+            len = 2;
+        } else if (c >= 0xe0 && c <= 0xef) {
+            len = 3;
+            if (c == 0xe0) first_lo = 0xa0;
+            if (c == 0xed) first_hi = 0x9f;
+        } else if (c >= 0xf0 && c <= 0xf4) {
+            len = 4;
+            if (c == 0xf0) first_lo = 0x90;
+            if (c == 0xf4) first_hi = 0x8f;
+        }
+        size_t k = 1;
+        if (len) {
+            for (; k < (size_t)len && i + k < n; k++) {
+                const unsigned char d = (unsigned char)s[i + k];
+                const unsigned char lo = k == 1 ? first_lo : 0x80, hi = k == 1 ? first_hi : 0xbf;
+                if (d < lo || d > hi) break;
+            }
+        }
+        if (len && k == (size_t)len) out.append(s, i, k);
+        else out += "\xef\xbf\xbd";
+        i += k;
+    }
+    return out;
+}
+
 bool read_fasta(const std::string& path, std::vector<FastaRecord>& out, std::string* err) {
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) {
@@ -1128,7 +1170,8 @@ bool read_fasta(const std::string& path, std::vector<FastaRecord>& out, std::str
         if (le > pos && data[pos] == '>') {
             std::string hdr = data.substr(pos + 1, le - pos - 1);
             size_t cut = hdr.find_first_of(" \t");
-            out.push_back(FastaRecord{cut == std::string::npos ? hdr : hdr.substr(0, cut), std::string()});
+            out.push_back(FastaRecord{from_utf8_lossy(cut == std::string::npos ? hdr : hdr.substr(0, cut)),
+                                      std::string()});
             cur = &out.back();
         } else if (cur) {
             cur->seq.append(data, pos, le - pos);

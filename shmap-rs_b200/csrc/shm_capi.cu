@@ -596,6 +596,11 @@ int shm_submit(shm_server* srv, const uint8_t* seqs, const int64_t* offs, int32_
     if (n > 0 && (!seqs || !offs || !out)) return fail(SHM_ERR_INVALID, "null argument");
     int v = check_reads(offs, n);
     if (v != SHM_OK) return v;
+    const int64_t mb = shm::server_max_bases(srv->s);
+    for (int32_t i = 0; i < n; i++)
+        if (offs[i + 1] - offs[i] > mb)
+            return fail(SHM_ERR_INVALID, "read " + std::to_string(i) + " has " + std::to_string(offs[i + 1] - offs[i]) +
+                                             " bases, more than a server batch holds (" + std::to_string(mb) + ")");
     SHM_GUARD_BEGIN
     *ticket = shm::server_submit(srv->s, seqs, offs, n, out);
     return SHM_OK;
@@ -631,10 +636,11 @@ int shm_server_destroy(shm_server* srv) {
 }
 
 // Test hook: the admission rule of a server slot (how many of the queued
-// requests one batch takes), with no device involved.
-int64_t shm_internal_serve_admit(const int64_t* reads, const int64_t* bases, int64_t n, int64_t max_reads,
-                                 int64_t max_bases) {
-    return (int64_t)shm::admit_count(reads, bases, (size_t)n, max_reads, max_bases);
+// requests one batch takes whole, and how many reads of the front request
+// when it alone is too large), with no device involved.
+int64_t shm_internal_serve_admit(const int64_t* reads, const int64_t* bases, int64_t n, const int64_t* front_lens,
+                                 int64_t max_reads, int64_t max_bases, int64_t* part) {
+    return (int64_t)shm::admit_parts(reads, bases, (size_t)n, front_lens, max_reads, max_bases, part);
 }
 
 int shm_map_fasta(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const shm_fasta* fa, int32_t first,

@@ -28,6 +28,7 @@
 #include "shm_common.cuh"
 #include "shm_fasta.hpp"
 #include "shm_internal.hpp"
+#include "../host/utf8.hpp"
 #include "shm_prims.cuh"
 
 namespace shm {
@@ -404,6 +405,10 @@ FastaDev* fasta_parse_device(int device, cudaStream_t s, const uint8_t* file, in
             SHM_CUDA(cudaMemcpyAsync(F->offs.data(), hdr_seq.p, sizeof(int64_t) * n_rec, cudaMemcpyDeviceToHost, s));
             SHM_CUDA(cudaStreamSynchronize(s));
             if (!F->names.empty()) F->names.pop_back();  // the last name's terminator
+            // names as String::from_utf8_lossy gives them (src/io/mod.rs:408-410)
+            bool ascii = true;
+            for (char ch : F->names) ascii = ascii && (unsigned char)ch < 0x80;
+            if (!ascii) F->names = utf8_lossy(F->names);
         }
         F->n = (int32_t)n_rec;
         return F;

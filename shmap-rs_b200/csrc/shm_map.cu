@@ -51,6 +51,7 @@
 
 #include "shm_common.cuh"
 #include "shm_map.cuh"
+#include "shm_pack.cuh"
 #include "shm_paf.hpp"
 #include "../host/pack.hpp"
 #include "shm_prims.cuh"
@@ -2324,8 +2325,9 @@ struct StageTimer {
         used++;
         return e;
     }
-    void begin(int st) {
-        count_launch();
+    // counts = the launch that follows is not counted by a helper of its own
+    void begin(int st, bool counts = true) {
+        if (counts) count_launch();
         if (!c->timing) return;
         cur = st;
         a = get();
@@ -2362,6 +2364,7 @@ struct MapScratch {
     DevBuf<SeedRec> sd;
     DevBuf<uint32_t> pk_codes[2], pk_mask[2];  // host-buffer batches, packed (host/pack.hpp)
     DevBuf<uint32_t> pk_list[2];               // their nonzero mask words as uploaded (index, word)
+    DevBuf<uint32_t> dpk_codes, dpk_mask;      // device-resident batches, packed on the device
     DevBuf<uint64_t> sd_h;
     DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
         cidx, cfar, sort_scr, ovf_list, r_flags;
@@ -2727,9 +2730,21 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     a.kmer_cnt = S.kcnt.p;
     a.out_h = S.km_h.p;
     a.out_rs = S.km_rs.p;
+    const int64_t batch_bytes = h_offs[n] - h_offs[0];
+    static const bool letters = std::getenv("SHMAP_SKETCH_LETTERS") != nullptr;
+    if (!pk_codes && d_seq && !letters) {  // reads in device memory are packed there first
+        S.dpk_codes.reserve(packed_code_words(batch_bytes));
+        S.dpk_mask.reserve(packed_mask_words(batch_bytes));
+        T.begin(STG_SKETCH, false);
+        pack_reads_device(d_seq, batch_bytes, S.dpk_codes.p, S.dpk_mask.p, s);
+        T.end();
+        pk_codes = S.dpk_codes.p;
+        pk_mask = S.dpk_mask.p;
+    }
     a.pk_codes = pk_codes;  // packed reads instead of d_seq when set
     a.pk_mask = pk_mask;
-    T.begin(STG_SKETCH);
+    a.pk_words = pk_codes ? packed_code_words(batch_bytes) : 0;
+    T.begin(STG_SKETCH, false);
     launch_sketch(SK_APPEND, a, S.luts, s);
     T.end();
     if (c->sketch_done) SHM_CUDA(cudaEventRecord(c->sketch_done, s));  // the batch's bytes are free again

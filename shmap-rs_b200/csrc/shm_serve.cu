@@ -10,8 +10,11 @@
 // at the same time. A free slot takes the queued requests in arrival order,
 // as many as fit its limits: at most max_batch_reads reads and, in bases, its
 // share of the HBM budget divided by the device bytes a base costs at the
-// index's hash ratio. Requests that arrive while the slots are busy wait in
-// the queue and join the next batch a slot takes.
+// index's hash ratio. A request larger than those limits is taken in parts,
+// each the longest run of its next reads that fits (a single read longer than
+// the base limit is refused when submitted), so no batch exceeds the budget.
+// Requests that arrive while the slots are busy wait in the queue and join
+// the next batch a slot takes.
 //
 // Each request of a batch is copied from the caller's memory straight to its
 // place in the slot's device buffer (one copy a request, direct from pinned
@@ -46,13 +49,20 @@ static double ms_between(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
-size_t admit_count(const int64_t* reads, const int64_t* bases, size_t n, int64_t max_reads, int64_t max_bases) {
+size_t admit_parts(const int64_t* reads, const int64_t* bases, size_t n, const int64_t* front_lens,
+                   int64_t max_reads, int64_t max_bases, int64_t* part) {
+    *part = 0;
     size_t k = 0;
     int64_t r = 0, b = 0;
     for (; k < n; k++) {
-        if (k > 0 && (r + reads[k] > max_reads || b + bases[k] > max_bases)) break;
+        if (r + reads[k] > max_reads || b + bases[k] > max_bases) break;
         r += reads[k];
         b += bases[k];
+    }
+    if (k == 0 && n > 0) {  // the front request alone is larger than a batch: its first reads that fit
+        int64_t c = 0, cb = 0;
+        while (c < reads[0] && c < max_reads && cb + front_lens[c] <= max_bases) cb += front_lens[c++];
+        *part = std::max<int64_t>(c, 1);
     }
     return k;
 }
@@ -63,11 +73,20 @@ struct Request {
     int32_t n;
     shm_map_record* out;
     Clock::time_point t_submit, t_start, t_done;
-    bool done = false;
+    int32_t taken = 0;    // reads handed to slots so far (a request larger than a batch goes in parts)
+    int32_t written = 0;  // reads whose records are in out
+    bool started = false, done = false;
     int status = 0;
     std::string err;
     int32_t batch_reads = 0, batch_requests = 0;
-    int64_t bases() const { return n ? offs[n] - offs[0] : 0; }
+    int64_t bases_from(int32_t i) const { return n ? offs[n] - offs[i] : 0; }
+};
+
+// Reads [first, first + count) of a request, mapped in one batch.
+struct Part {
+    Request* r;
+    int32_t first, count;
+    int64_t bases() const { return r->offs[first + count] - r->offs[first]; }
 };
 
 struct Slot {
@@ -107,8 +126,8 @@ static void grow_pinned(void** p, size_t* cap, size_t want) {
 
 static void run_slot(Server* S, Slot* sl) {
     cudaSetDevice(S->device);
-    std::vector<Request*> batch;
-    std::vector<int64_t> rq_reads, rq_bases;
+    std::vector<Part> batch;
+    std::vector<int64_t> rq_reads, rq_bases, front_lens;
     for (;;) {
         batch.clear();
         {
@@ -118,22 +137,41 @@ static void run_slot(Server* S, Slot* sl) {
             rq_reads.clear();
             rq_bases.clear();
             for (Request* r : S->queue) {
-                rq_reads.push_back(r->n);
-                rq_bases.push_back(r->bases());
+                rq_reads.push_back(r->n - r->taken);
+                rq_bases.push_back(r->bases_from(r->taken));
                 if ((int64_t)rq_reads.size() > S->max_reads) break;  // enough to decide
             }
-            const size_t k = admit_count(rq_reads.data(), rq_bases.data(), rq_reads.size(), S->max_reads, S->max_bases);
+            Request* f = S->queue.front();
+            front_lens.clear();
+            if (rq_reads[0] > S->max_reads || rq_bases[0] > S->max_bases)
+                for (int32_t i = f->taken; i < f->n && (int64_t)front_lens.size() < S->max_reads; i++)
+                    front_lens.push_back(f->offs[i + 1] - f->offs[i]);
+            int64_t part = 0;
+            const size_t k = admit_parts(rq_reads.data(), rq_bases.data(), rq_reads.size(), front_lens.data(),
+                                         S->max_reads, S->max_bases, &part);
             const auto now = Clock::now();
+            auto start = [&](Request* r) {
+                if (!r->started) r->t_start = now;
+                r->started = true;
+            };
             for (size_t i = 0; i < k; i++) {
-                batch.push_back(S->queue.front());
+                Request* r = S->queue.front();
                 S->queue.pop_front();
-                batch.back()->t_start = now;
+                start(r);
+                batch.push_back(Part{r, r->taken, r->n - r->taken});
+                r->taken = r->n;
+            }
+            if (part > 0) {
+                start(f);
+                batch.push_back(Part{f, f->taken, (int32_t)part});
+                f->taken += (int32_t)part;
+                if (f->taken == f->n) S->queue.pop_front();
             }
         }
         int64_t nreads = 0, nbases = 0;
-        for (Request* r : batch) {
-            nreads += r->n;
-            nbases += r->bases();
+        for (const Part& q : batch) {
+            nreads += q.count;
+            nbases += q.bases();
         }
         int status = SHM_OK;
         std::string err;
@@ -144,12 +182,13 @@ static void run_slot(Server* S, Slot* sl) {
             sl->d_out.reserve((size_t)std::max<int64_t>(nreads, 1));
             sl->offs.assign(1, 0);
             int64_t at = 0;
-            for (Request* r : batch) {  // each request's reads to their place in the batch
-                const int64_t b = r->bases();
+            for (const Part& q : batch) {  // each part's reads to their place in the batch
+                const Request* r = q.r;
+                const int64_t b = q.bases(), o0 = r->offs[q.first];
                 if (b)
-                    SHM_CUDA(cudaMemcpyAsync(sl->d_seq.p + at, r->seqs + r->offs[0], (size_t)b, cudaMemcpyHostToDevice,
+                    SHM_CUDA(cudaMemcpyAsync(sl->d_seq.p + at, r->seqs + o0, (size_t)b, cudaMemcpyHostToDevice,
                                              c->stream));
-                for (int32_t i = 0; i < r->n; i++) sl->offs.push_back(at + (r->offs[i + 1] - r->offs[0]));
+                for (int32_t i = q.first; i < q.first + q.count; i++) sl->offs.push_back(at + (r->offs[i + 1] - o0));
                 at += b;
             }
             SHM_CUDA(cudaMemsetAsync(sl->d_seq.p + at, 0, 32, c->stream));
@@ -160,9 +199,10 @@ static void run_slot(Server* S, Slot* sl) {
             c->work[W_D2H_BYTES] += (int64_t)sizeof(shm_map_record) * nreads;
             SHM_CUDA(cudaStreamSynchronize(c->stream));
             int64_t pos = 0;
-            for (Request* r : batch) {  // scatter: each request's records into its own output
-                if (r->n) std::memcpy(r->out, sl->h_out + pos, sizeof(shm_map_record) * (size_t)r->n);
-                pos += r->n;
+            for (const Part& q : batch) {  // scatter: each part's records into its request's output
+                if (q.count)
+                    std::memcpy(q.r->out + q.first, sl->h_out + pos, sizeof(shm_map_record) * (size_t)q.count);
+                pos += q.count;
             }
         } catch (const shm_cuda_error& e) {
             status = e.err == cudaErrorMemoryAllocation ? SHM_ERR_NOMEM : SHM_ERR_CUDA;
@@ -178,13 +218,19 @@ static void run_slot(Server* S, Slot* sl) {
         {
             std::lock_guard<std::mutex> lk(S->mu);
             const auto now = Clock::now();
-            for (Request* r : batch) {
-                r->t_done = now;
-                r->status = status;
-                r->err = err;
+            for (const Part& q : batch) {
+                Request* r = q.r;
+                if (status != SHM_OK && r->status == SHM_OK) {
+                    r->status = status;
+                    r->err = err;
+                }
                 r->batch_reads = (int32_t)nreads;
                 r->batch_requests = (int32_t)batch.size();
-                r->done = true;
+                r->written += q.count;
+                if (r->written == r->n) {
+                    r->t_done = now;
+                    r->done = true;
+                }
             }
         }
         S->cv_done.notify_all();
@@ -226,6 +272,8 @@ Server* server_create(int device, const IndexStorage* ix, const shm_params& p, c
     }
     return S;
 }
+
+int64_t server_max_bases(const Server* S) { return S->max_bases; }
 
 uint64_t server_submit(Server* S, const uint8_t* seqs, const int64_t* offs, int32_t n, shm_map_record* out) {
     auto* r = new Request();

@@ -25,10 +25,16 @@ struct ServeStats {
 
 struct Server;
 
-// How many requests, from the front of a queue whose requests hold reads[i]
-// reads and bases[i] bases, one batch takes: in order, while both totals
-// stay within the limits, and always the first.
-size_t admit_count(const int64_t* reads, const int64_t* bases, size_t n, int64_t max_reads, int64_t max_bases);
+// One batch's share of a queue whose requests hold reads[i] reads and
+// bases[i] bases (what is left of them): whole requests from the front, in
+// order, while both totals stay within the limits (the count is returned).
+// When the front request alone does not fit, none is taken whole and *part
+// gets the number of its first reads (lengths front_lens[], at least
+// min(reads[0], max_reads) of them) that fit, at least one; else *part = 0.
+size_t admit_parts(const int64_t* reads, const int64_t* bases, size_t n, const int64_t* front_lens,
+                   int64_t max_reads, int64_t max_bases, int64_t* part);
+// The longest read, in bases, a request may hold.
+int64_t server_max_bases(const Server* s);
 
 Server* server_create(int device, const IndexStorage* ix, const shm_params& p, const ServeConfig& cfg);
 uint64_t server_submit(Server* s, const uint8_t* seqs, const int64_t* offs, int32_t n, shm_map_record* out);

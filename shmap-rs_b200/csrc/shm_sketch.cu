@@ -13,7 +13,9 @@
 #include "shm_prims.cuh"
 #include "shm_sketch.cuh"
 
+#include <cstdlib>
 #include <mutex>
+#include <vector>
 
 namespace shm {
 
@@ -402,6 +404,276 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
     }
 }
 
+// ------------------------------------------------------------------ packed reads
+// The sketch of reads packed as 2-bit codes (A, C, T, G = 0..3) with a
+// non-ACGT mask, rolled without rotating the state. With X_t and Y_t the
+// table values window t XORs in (forward: fw of the entering base and fw<<k
+// of the leaving one; reverse: rc<<(k-1) of the entering base and rc>>1 of
+// the leaving one), the rolling step is F_t = rotl1(F_{t-1}) ^ X_t and
+// R_t = rotr1(R_{t-1}) ^ Y_t. In the frame F~_t = rotr(F_t, t),
+// R~_t = rotl(R_t, t) the step is a plain XOR: F~_t = F~_{t-1} ^ rotr(X_t, t),
+// R~_t = R~_{t-1} ^ rotl(Y_t, t), and the tables hold the rotated values for
+// every entering/leaving code pair. Rotation by 32 swaps a value's halves,
+// so the state is kept half-swapped during every other group of 32 windows
+// and the tables need 32 rows: row jj holds rotr(X, jj) and rotl(Y, jj).
+// The selection test needs only the high word of h_t = F_t ^ R_t, two funnel
+// shifts of the stored state by jj; the full hash and the strand are formed
+// for the rare windows that pass it. A run starts from the hash of the
+// window one base before its first (warm-up, four bases a step), so the
+// leaving base of its first window is read like every other.
+struct PkTables {
+    uint2 pf[32][16];  // [jj][ci * 4 + co]: rotr(fw[ci] ^ fw_k[co], jj), as (lo, hi)
+    uint2 pr[32][16];  // rotl(rc_k1[ci] ^ rc_r1[co], jj)
+    uint4 w4[256];     // four bases c0..c3 (c0 the earliest, bits 0-1): rolled-in (F, R) as (Flo, Fhi, Rlo, Rhi)
+    uint4 w1[4];       // one base: (fw, rc_k1)
+};
+
+__device__ __forceinline__ uint64_t u64_of(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
+
+__device__ void build_pk_tables(PkTables& P, const SketchLuts* __restrict__ L) {
+    const unsigned char let[4] = {'A', 'C', 'T', 'G'};
+    for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+        const int jj = e >> 4, ci = (e >> 2) & 3, co = e & 3;
+        const uint64_t x = L->fw[let[ci]] ^ L->fw_k[let[co]];
+        const uint64_t y = L->rc_k1[let[ci]] ^ L->rc_r1[let[co]];
+        const uint64_t rx = rotr64(x, (uint32_t)jj), ly = rotl64(y, (uint32_t)jj);
+        P.pf[jj][ci * 4 + co] = make_uint2((uint32_t)rx, (uint32_t)(rx >> 32));
+        P.pr[jj][ci * 4 + co] = make_uint2((uint32_t)ly, (uint32_t)(ly >> 32));
+    }
+    for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
+        uint64_t f = 0, r = 0;
+        for (int i = 0; i < 4; i++) {
+            const unsigned char c = let[(idx >> (2 * i)) & 3];
+            f ^= rotl64(L->fw[c], (uint32_t)(3 - i));
+            r ^= rotr64(L->rc_k1[c], (uint32_t)(3 - i));
+        }
+        P.w4[idx] = make_uint4((uint32_t)f, (uint32_t)(f >> 32), (uint32_t)r, (uint32_t)(r >> 32));
+    }
+    if (threadIdx.x < 4) {
+        const unsigned char c = let[threadIdx.x];
+        const uint64_t f = L->fw[c], r = L->rc_k1[c];
+        P.w1[threadIdx.x] = make_uint4((uint32_t)f, (uint32_t)(f >> 32), (uint32_t)r, (uint32_t)(r >> 32));
+    }
+}
+
+// Code word wi of the batch; words before the batch and past its padding read as 0.
+__device__ __forceinline__ uint32_t pk_word(const uint32_t* __restrict__ codes, int64_t wi, uint64_t n_words) {
+    return (wi >= 0 && (uint64_t)wi < n_words) ? __ldg(codes + wi) : 0u;
+}
+
+// True when bases [b, e) of the batch hold no masked (non-ACGT) base.
+__device__ __forceinline__ bool pk_unmasked(const uint32_t* __restrict__ mask, int64_t b, int64_t e) {
+    if (e <= b) return true;
+    const int64_t w0 = b >> 5, w1 = (e - 1) >> 5;
+    uint32_t acc = 0;
+    for (int64_t w = w0; w <= w1; w++) {
+        uint32_t m = __ldg(mask + w);
+        if (w == w0) m &= ~0u << (b & 31);
+        if (w == w1) m &= ~0u >> (31 - ((e - 1) & 31));
+        acc |= m;
+    }
+    return acc == 0;
+}
+
+// One group of 32 windows, t = t0 + jj: in and out hold the entering and
+// leaving bases' codes (32 each, the earliest in bits 0-1 of the low word).
+template <int MODE>
+__device__ __forceinline__ void pk_group(const SketchArgs& a, const PkTables& P, uint2 in, uint2 out,
+                                         uint32_t& Flo, uint32_t& Fhi, uint32_t& Rlo, uint32_t& Rhi,
+                                         uint32_t thr_hi, uint64_t thr, int32_t q, int32_t r_t0, int32_t lim,
+                                         Emit& e) {
+#pragma unroll
+    for (int jj = 0; jj < 32; jj++) {
+        const uint32_t xi = jj < 16 ? in.x : in.y, xo = jj < 16 ? out.x : out.y;
+        const int s = 2 * (jj & 15);
+        // entering code * 32 + leaving code * 8: the byte offset in row jj
+        const uint32_t ci32 = (s >= 5 ? (xi >> (s - 5)) : (xi << (5 - s))) & 0x60u;
+        const uint32_t co8 = (s >= 3 ? (xo >> (s - 3)) : (xo << (3 - s))) & 0x18u;
+        const uint32_t off = ci32 | co8;
+        const uint2 ef = *(const uint2*)((const char*)&P.pf[jj][0] + off);
+        const uint2 er = *(const uint2*)((const char*)&P.pr[jj][0] + off);
+        Flo ^= ef.x;
+        Fhi ^= ef.y;
+        Rlo ^= er.x;
+        Rhi ^= er.y;
+        const uint32_t hh = __funnelshift_l(Flo, Fhi, jj) ^ __funnelshift_r(Rhi, Rlo, jj);
+        if (hh <= thr_hi) {
+            const uint64_t F = rotl64(u64_of(Flo, Fhi), (uint32_t)jj), R = rotr64(u64_of(Rlo, Rhi), (uint32_t)jj);
+            const uint64_t h = F ^ R;
+            if (h <= thr && jj < lim) emit_kmer<MODE>(a, q, h, ((uint32_t)(r_t0 + jj) << 1) | (F > R ? 1u : 0u), e);
+        }
+    }
+}
+
+// The windows [0, cnt) (cnt <= SKETCH_WIN) of the run whose first window
+// starts at base p0 of the batch, all of whose bases are unmasked.
+template <int MODE>
+__device__ __forceinline__ void pk_run(const SketchArgs& a, const PkTables& P, int64_t p0, int32_t cnt, int k,
+                                       uint64_t thr, int32_t q, int32_t r0, Emit& e) {
+    const uint32_t* __restrict__ codes = a.pk_codes;
+    const uint64_t nw = a.pk_words;
+    // warm-up: the window of bases [p0 - 1, p0 + k - 1), four bases a step
+    uint64_t F = 0, R = 0;
+    {
+        const int64_t b = p0 - 1;
+        int64_t wi = b >> 4;  // arithmetic: -1 for b = -1
+        const uint32_t sh = (uint32_t)(b & 15) * 2;
+        uint32_t w0 = pk_word(codes, wi, nw), w1 = pk_word(codes, wi + 1, nw);
+        int i = 0;
+        for (; i + 16 <= k; i += 16) {
+            const uint32_t c16 = __funnelshift_r(w0, w1, sh);  // 16 codes from base b + i
+            w0 = w1;
+            w1 = pk_word(codes, wi + 2 + (i >> 4), nw);
+#pragma unroll
+            for (int g = 0; g < 4; g++) {
+                const uint4 t = P.w4[__byte_perm(c16, 0u, 0x4440u + (uint32_t)g)];
+                F = rotl64(F, 4) ^ u64_of(t.x, t.y);
+                R = rotr64(R, 4) ^ u64_of(t.z, t.w);
+            }
+        }
+        if (i < k) {  // the last k - i < 16 bases
+            const uint32_t c16 = __funnelshift_r(w0, w1, sh);
+            int j = 0;
+            for (; i + 4 <= k; i += 4, j++) {
+                const uint4 t = P.w4[__byte_perm(c16, 0u, 0x4440u + (uint32_t)j)];
+                F = rotl64(F, 4) ^ u64_of(t.x, t.y);
+                R = rotr64(R, 4) ^ u64_of(t.z, t.w);
+            }
+            for (int u = 4 * j; i < k; i++, u++) {
+                const uint4 t = P.w1[(c16 >> (2 * u)) & 3u];
+                F = rotl64(F, 1) ^ u64_of(t.x, t.y);
+                R = rotr64(R, 1) ^ u64_of(t.z, t.w);
+            }
+        }
+    }
+    // the frame at t = -1: F~ = rotl1(F), R~ = rotr1(R)
+    F = rotl64(F, 1);
+    R = rotr64(R, 1);
+    uint32_t Flo = (uint32_t)F, Fhi = (uint32_t)(F >> 32), Rlo = (uint32_t)R, Rhi = (uint32_t)(R >> 32);
+    const uint32_t thr_hi = (uint32_t)(thr >> 32);
+    // entering bases from p0 + k - 1, leaving bases from p0 - 1; 32 of each a group
+    const int64_t bi = p0 + k - 1, bo = p0 - 1;
+    int64_t wi = bi >> 4, wo = bo >> 4;
+    const uint32_t shi = (uint32_t)(bi & 15) * 2, sho = (uint32_t)(bo & 15) * 2;
+    uint32_t i0 = pk_word(codes, wi, nw), i1 = pk_word(codes, wi + 1, nw), i2 = pk_word(codes, wi + 2, nw);
+    uint32_t o0 = pk_word(codes, wo, nw), o1 = pk_word(codes, wo + 1, nw), o2 = pk_word(codes, wo + 2, nw);
+#pragma unroll 1
+    for (int t0 = 0; t0 < cnt; t0 += 64) {
+        // the next group's words, loaded while this one rolls
+        const uint32_t i3 = pk_word(codes, wi + 3, nw), i4 = pk_word(codes, wi + 4, nw);
+        const uint32_t o3 = pk_word(codes, wo + 3, nw), o4 = pk_word(codes, wo + 4, nw);
+        uint2 in = make_uint2(__funnelshift_r(i0, i1, shi), __funnelshift_r(i1, i2, shi));
+        uint2 out = make_uint2(__funnelshift_r(o0, o1, sho), __funnelshift_r(o1, o2, sho));
+        pk_group<MODE>(a, P, in, out, Flo, Fhi, Rlo, Rhi, thr_hi, thr, q, r0 + t0, cnt - t0, e);
+        // windows t0 + 32 .. t0 + 63: the state half-swapped (rotation by 32)
+        const uint32_t i5 = pk_word(codes, wi + 5, nw), i6 = pk_word(codes, wi + 6, nw);
+        const uint32_t o5 = pk_word(codes, wo + 5, nw), o6 = pk_word(codes, wo + 6, nw);
+        in = make_uint2(__funnelshift_r(i2, i3, shi), __funnelshift_r(i3, i4, shi));
+        out = make_uint2(__funnelshift_r(o2, o3, sho), __funnelshift_r(o3, o4, sho));
+        pk_group<MODE>(a, P, in, out, Fhi, Flo, Rhi, Rlo, thr_hi, thr, q, r0 + t0 + 32, cnt - t0 - 32, e);
+        i0 = i4;
+        i1 = i5;
+        i2 = i6;
+        o0 = o4;
+        o1 = o5;
+        o2 = o6;
+        wi += 4;
+        wo += 4;
+    }
+}
+
+// Each thread one run of SKETCH_WIN windows of packed reads (tiles of
+// SK_THREADS consecutive runs a CTA, as k_sketch). A run with a masked base
+// among its bases rolls through the letter tables instead (GlobalPacked).
+template <int MODE>
+__global__ void __launch_bounds__(SK_THREADS) k_sketch_pk(SketchArgs a, const SketchLuts* __restrict__ luts) {
+    __shared__ PkTables P;
+    __shared__ LutPair Lin[256], Lout[256];
+    __shared__ int32_t s_q[2];
+    build_pk_tables(P, luts);
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        Lin[i] = LutPair{luts->fw[i], luts->rc_k1[i]};
+        Lout[i] = LutPair{luts->fw_k[i], luts->rc_r1[i]};
+    }
+    Emit e;
+    const int lane = threadIdx.x & 31;
+    const int k = a.k;
+    const uint64_t thr = a.thr;
+    const uint64_t n_chunks = a.n_chunks;
+    const uint64_t n_tiles = (n_chunks + SK_THREADS - 1) / SK_THREADS;
+    for (uint64_t tl = blockIdx.x; tl < n_tiles; tl += gridDim.x) {
+        const uint64_t c0 = tl * SK_THREADS, c = c0 + threadIdx.x;
+        const uint64_t c_last = min(c0 + SK_THREADS, n_chunks) - 1;
+        if (threadIdx.x == 0 || threadIdx.x == 32) {  // sequences of the tile's first and last runs
+            const uint64_t cc = threadIdx.x == 0 ? c0 : c_last;
+            int32_t lo = 0, hi = a.n_seq;
+            while (hi - lo > 1) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (__ldg(a.chunk_off + mid) <= cc) lo = mid;
+                else hi = mid;
+            }
+            s_q[threadIdx.x == 0 ? 0 : 1] = lo;
+        }
+        __syncthreads();  // also: the tables are built
+        int32_t q = 0, cnt = 0;
+        int64_t p0 = 0, w0 = 0;
+        if (c < n_chunks) {
+            int32_t lo = s_q[0], hi = s_q[1] + 1;
+            while (hi - lo > 1) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (__ldg(a.chunk_off + mid) <= c) lo = mid;
+                else hi = mid;
+            }
+            q = lo;
+            const int64_t s0 = __ldg(a.seq_off + q), nwin = __ldg(a.seq_off + q + 1) - s0 - k + 1;
+            w0 = (int64_t)(c - __ldg(a.chunk_off + q)) * SKETCH_WIN;
+            cnt = (int32_t)(min(w0 + (int64_t)SKETCH_WIN, nwin) - w0);
+            p0 = s0 + w0;
+        }
+        __syncthreads();  // s_q read by every thread before the next tile writes it
+        e.n_sel = 0;
+        e.out_base = 0;
+        e.out_cap = 0;
+        if (cnt > 0) {
+            if (MODE == SK_WRITE) e.out_base = a.chunk_out[c];
+            if (MODE == SK_APPEND) {
+                e.out_base = a.kmer_off[q];
+                e.out_cap = (uint32_t)(a.kmer_off[q + 1] - e.out_base);
+            }
+        }
+        const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;
+        const bool fast = cnt > 0 && pk_unmasked(a.pk_mask, p0, p0 + cnt + k - 1);
+        if (fast)
+            pk_run<MODE>(a, P, p0, cnt, k, thr, q, r0, e);
+        else if (cnt > 0)
+            sketch_run<MODE>(a, Lin, Lout, GlobalPacked{a.pk_codes, a.pk_mask, 0, p0, p0 + cnt + k - 1}, p0, cnt, k,
+                             thr, q, r0, e);
+        if (MODE == SK_COUNT && c < n_chunks) a.chunk_cnt[c] = e.n_sel;
+        if (MODE == SK_APPEND) {
+            const uint32_t nb = e.n_sel;
+            uint32_t incl = nb;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, cnt > 0 ? q : -1);
+            const int leader = __ffs(peers) - 1, last = 31 - __clz(peers);
+            const uint32_t g0 = __shfl_sync(0xffffffffu, incl - nb, leader);
+            const uint32_t gtot = __shfl_sync(0xffffffffu, incl, last) - g0;
+            uint32_t base = 0;
+            if (lane == leader && cnt > 0 && gtot) base = atomicAdd(a.kmer_cnt + q, gtot);
+            base = __shfl_sync(0xffffffffu, base, leader) + (incl - nb) - g0;
+            for (uint32_t j = 0; j < nb && j < (uint32_t)SK_LB; j++) {
+                if (base + j < e.out_cap) {
+                    a.out_h[e.out_base + base + j] = e.bh[j];
+                    a.out_rs[e.out_base + base + j] = e.br[j];
+                }
+            }
+        }
+    }
+}
+
 SketchLuts* create_device_luts(int32_t k, cudaStream_t s) {
     SketchLuts h;
     build_luts(k, &h);
@@ -416,6 +688,16 @@ void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStrea
     if (a.n_chunks == 0) return;
     const bool pk = a.pk_codes != nullptr;
     if (pk && mode != SK_APPEND) throw shm_cuda_error(cudaErrorInvalidValue);
+    // packed reads roll in the rotated frame (k_sketch_pk); SHMAP_SKETCH_LETTERS=1
+    // rolls them through the letter tables instead (the same selections)
+    static const bool letters = std::getenv("SHMAP_SKETCH_LETTERS") != nullptr;
+    if (pk && !letters) {
+        const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
+        k_sketch_pk<SK_APPEND><<<grid_for(n_tiles, 1, 8), SK_THREADS, 0, s>>>(a, L);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+        return;
+    }
     const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
     const int grid = grid_for(n_tiles, 1, 5);  // tiles, at most 5 resident CTAs per SM
     const size_t dyn = sk_dyn_bytes(mode);
@@ -485,3 +767,89 @@ void launch_fill_luts(SketchLuts* d, int32_t k, cudaStream_t s) {
 }
 
 }  // namespace shm
+
+// Test hook (not part of the C ABI of include/shmap_gpu.h): the read sketch
+// of the mapping path (SK_APPEND) for n host reads on `device`, from the
+// reads packed on the host (packed != 0, the host-buffer path's layout) or
+// from their bytes. Read i's k-mers go unordered to out_h/out_rs from
+// cap_off[i] (at most cap_off[i+1] - cap_off[i] of them); out_cnt[i] gets
+// their number. Allocates its own device buffers.
+#include "../host/pack.hpp"
+#include "shm_internal.hpp"
+
+extern "C" int shm_internal_sketch_reads(int device, const uint8_t* seqs, const int64_t* offs, int32_t n, int32_t k,
+                                         double h_frac, int packed, const uint64_t* cap_off, uint64_t* out_h,
+                                         uint32_t* out_rs, uint32_t* out_cnt) {
+    using namespace shm;
+    if (n < 0 || k <= 0 || !offs || (n > 0 && (!seqs || !cap_off || !out_cnt))) return -1;
+    std::vector<void*> bufs;
+    auto dalloc = [&](size_t bytes) {
+        void* p = nullptr;
+        SHM_CUDA(cudaMalloc(&p, bytes < 16 ? 16 : bytes));
+        bufs.push_back(p);
+        return p;
+    };
+    try {
+        SHM_CUDA(cudaSetDevice(device));
+        const int64_t nb = offs[n] - offs[0];
+        std::vector<int64_t> so((size_t)n + 1);
+        std::vector<uint64_t> co((size_t)n + 1, 0);
+        for (int32_t i = 0; i <= n; i++) so[(size_t)i] = offs[i] - offs[0];
+        for (int32_t i = 0; i < n; i++) {
+            const int64_t nw = so[(size_t)i + 1] - so[(size_t)i] - k + 1;
+            co[(size_t)i + 1] = co[(size_t)i] + (nw > 0 ? (uint64_t)((nw + SKETCH_WIN - 1) / SKETCH_WIN) : 0);
+        }
+        SketchArgs a{};
+        a.n_seq = n;
+        a.n_chunks = co[(size_t)n];
+        a.k = k;
+        a.thr = h_thres(h_frac);
+        auto* d_so = (int64_t*)dalloc(8 * so.size());
+        auto* d_co = (uint64_t*)dalloc(8 * co.size());
+        auto* d_ko = (uint64_t*)dalloc(8 * ((size_t)n + 1));
+        auto* d_kc = (uint32_t*)dalloc(4 * (size_t)std::max(n, 1));
+        const uint64_t total = cap_off[n];
+        auto* d_h = (uint64_t*)dalloc(8 * (size_t)total);
+        auto* d_rs = (uint32_t*)dalloc(4 * (size_t)total);
+        SHM_CUDA(cudaMemcpy(d_so, so.data(), 8 * so.size(), cudaMemcpyHostToDevice));
+        SHM_CUDA(cudaMemcpy(d_co, co.data(), 8 * co.size(), cudaMemcpyHostToDevice));
+        SHM_CUDA(cudaMemcpy(d_ko, cap_off, 8 * ((size_t)n + 1), cudaMemcpyHostToDevice));
+        SHM_CUDA(cudaMemset(d_kc, 0, 4 * (size_t)std::max(n, 1)));
+        if (packed) {
+            std::vector<uint32_t> cw(packed_code_words(nb)), mw(packed_mask_words(nb));
+            pack_reads_host(seqs + offs[0], nb, cw.data(), mw.data());
+            auto* d_cw = (uint32_t*)dalloc(4 * cw.size());
+            auto* d_mw = (uint32_t*)dalloc(4 * mw.size());
+            SHM_CUDA(cudaMemcpy(d_cw, cw.data(), 4 * cw.size(), cudaMemcpyHostToDevice));
+            SHM_CUDA(cudaMemcpy(d_mw, mw.data(), 4 * mw.size(), cudaMemcpyHostToDevice));
+            a.pk_codes = d_cw;
+            a.pk_mask = d_mw;
+            a.pk_words = cw.size();
+        } else {
+            auto* d_seq = (uint8_t*)dalloc((size_t)nb + 32);
+            SHM_CUDA(cudaMemset(d_seq, 0, (size_t)nb + 32));
+            if (nb) SHM_CUDA(cudaMemcpy(d_seq, seqs + offs[0], (size_t)nb, cudaMemcpyHostToDevice));
+            a.seq = d_seq;
+        }
+        a.seq_off = d_so;
+        a.chunk_off = d_co;
+        a.kmer_off = d_ko;
+        a.kmer_cnt = d_kc;
+        a.out_h = d_h;
+        a.out_rs = d_rs;
+        SketchLuts* L = create_device_luts(k, nullptr);
+        bufs.push_back(L);
+        launch_sketch(SK_APPEND, a, L, nullptr);
+        SHM_CUDA(cudaDeviceSynchronize());
+        SHM_CUDA(cudaMemcpy(out_cnt, d_kc, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+        if (total) {
+            SHM_CUDA(cudaMemcpy(out_h, d_h, 8 * (size_t)total, cudaMemcpyDeviceToHost));
+            SHM_CUDA(cudaMemcpy(out_rs, d_rs, 4 * (size_t)total, cudaMemcpyDeviceToHost));
+        }
+    } catch (const shm_cuda_error&) {
+        for (void* p : bufs) cudaFree(p);
+        return -2;
+    }
+    for (void* p : bufs) cudaFree(p);
+    return 0;
+}

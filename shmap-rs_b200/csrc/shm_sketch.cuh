@@ -38,6 +38,7 @@ struct SketchArgs {
     // of pk_mask[p >> 5] is set; two spare groups of 32 past the end)
     const uint32_t* pk_codes;
     const uint32_t* pk_mask;
+    uint64_t pk_words;  // code words readable at pk_codes (those past it read as 0)
 };
 
 // The five lookup tables of src/sketch.rs:50-97 for one k, in device memory

@@ -9,6 +9,7 @@
 // its k, -r and -M replace those given on the command line; --host-fasta
 // parses FASTA on the host (by default the device parses it and keeps the
 // sequences; FASTQ is always read on the host).
+#include "utf8.hpp"
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -55,7 +56,7 @@ bool parse_fastx(const std::string& data, const std::string& path, Records& out,
     auto add_name = [&](size_t a, size_t b) {
         std::string h = data.substr(a, b - a);
         size_t cut = h.find_first_of(" \t");
-        out.names.push_back(cut == std::string::npos ? h : h.substr(0, cut));
+        out.names.push_back(shm::utf8_lossy(cut == std::string::npos ? h : h.substr(0, cut)));
     };
     bool open = false;
     while (pos < n) {

@@ -59,7 +59,7 @@ def test_records_as_the_host_reads_them(gpu_ctx, tmp_path, seed, n_rec, max_len)
 
 
 @pytest.mark.parametrize("data", [b"", b"\n\n", b">only\n", b">a\r\n\r\nAC\r\nGT\r\n>b\n>c\nTT", b">x y\tz\n" + b"A" * 20000,
-                                  b"\r\n>r\nACGT\r"])
+                                  b"\r\n>r\nACGT\r", b">caf\xe9 x\nACGT\n>\xf0\x90\x80\nGG\n>ok\xe2\x82\xac\xff\nT\n"])
 def test_edge_files(gpu_ctx, tmp_path, data):
     want = _host(tmp_path, data)
     fa = sb.DeviceFasta(gpu_ctx, data)

@@ -380,3 +380,58 @@ def test_hifi_five_percent_scale(gpu_ctx):
     assert strip_t(text) == strip_t(otext.decode())
     assert (rec["status"] == 0).mean() > 0.9
     g.close()
+
+
+def _read_sketches(reads, k, r, packed):
+    """The mapping path's read sketch (SK_APPEND) through the library's test
+    hook: per read, its k-mers sorted by position."""
+    import ctypes
+
+    L = sb.lib()
+    f = L.shm_internal_sketch_reads
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                  ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    seq, offs = pack(reads)
+    caps = np.array([max(0, len(x) - k + 1) for x in reads], np.uint64)
+    cap_off = np.concatenate([[0], np.cumsum(caps)]).astype(np.uint64)
+    tot = max(1, int(cap_off[-1]))
+    h = np.zeros(tot, np.uint64)
+    rs = np.zeros(tot, np.uint32)
+    cnt = np.zeros(max(1, len(reads)), np.uint32)
+    assert f(0, seq.ctypes.data, offs.ctypes.data, len(reads), k, r, int(packed), cap_off.ctypes.data,
+             h.ctypes.data, rs.ctypes.data, cnt.ctypes.data) == 0
+    out = []
+    for i in range(len(reads)):
+        a = int(cap_off[i])
+        m = int(cnt[i])
+        assert m <= caps[i]
+        hh, rr = h[a:a + m], rs[a:a + m]
+        o = np.argsort(rr >> 1, kind="stable")
+        out.append(((rr[o] >> 1).astype(np.int32), hh[o], (rr[o] & 1).astype(np.uint8)))
+    return out
+
+
+@pytest.mark.parametrize("k", [1, 5, 15, 25, 31, 32, 33, 64, 65, 100])
+@pytest.mark.parametrize("r", [1.0, 0.5, 0.1, 0.01])
+def test_read_sketch_packed_and_ascii(gpu_ctx, k, r):
+    """The read sketch from 2-bit packed reads (rotated-frame rolling) and
+    from the reads' bytes equals the oracle's sketch, per read: lengths around
+    the 128-window runs, reads shorter than k, N runs, lower case and IUPAC
+    bytes (which the packed form marks and rolls through the letter tables)."""
+    rng = np.random.default_rng(k * 10 + int(r * 100))
+    reads = []
+    for L in [0, 1, k - 1, k, k + 1, 127 + k, 128 + k, 129 + k, 255 + k, 256 + k, 1000, 5003, 20000]:
+        reads.append(lcg_dna(int(rng.integers(1, 1 << 30)), max(0, L)))
+    s = bytearray(lcg_dna(77, 9000))
+    s[3000:3040] = b"N" * 40
+    s[5000:5400] = bytes(s[5000:5400]).lower()
+    s[7000:7004] = b"RYK-"
+    reads.append(bytes(s))
+    reads.append(b"N" * 300)
+    reads.append(xorshift_dna(5, 4000).lower())
+    for packed in (1, 0):
+        got = _read_sketches(reads, k, r, packed)
+        for i, x in enumerate(reads):
+            want = O.sketch(x, k, r)
+            assert all(np.array_equal(a, b) for a, b in zip(got[i], want)), (packed, i, len(x))

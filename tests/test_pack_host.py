@@ -68,3 +68,23 @@ def test_pack_every_byte_value():
         assert np.array_equal(m, want_m) and np.array_equal(c, want_c)
     ok = np.isin(np.arange(256), np.frombuffer(b"ACGTacgt", np.uint8))
     assert ok.sum() == 8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nb", [0, 1, 31, 32, 33, 100, 4096, 100_003])
+def test_device_packing_equals_the_model(nb):
+    """Reads packed on the device (shm_pack.cu, used for reads that are in
+    device memory) give the host packing's words: every byte value, both
+    cases, ragged lengths, a start that is not 16-byte aligned."""
+    f = sb.lib().shm_internal_pack_reads_device
+    f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    rng = np.random.default_rng(nb)
+    seq = rng.choice(np.frombuffer(b"ACGTacgtACGTACGTN", np.uint8), nb)
+    seq[: min(nb, 256)] = np.arange(min(nb, 256), dtype=np.uint8)  # every byte value
+    groups = nb // 32 + 3
+    codes = np.zeros(2 * groups, np.uint32)
+    mask = np.zeros(groups, np.uint32)
+    assert f(0, seq.ctypes.data, nb, codes.ctypes.data, mask.ctypes.data) == 0
+    want_c, want_m = _model(seq)
+    assert np.array_equal(codes, want_c) and np.array_equal(mask, want_m)

@@ -1,11 +1,12 @@
 """Serving with continuous batching (shm_server_create / shm_submit / shm_poll).
 
 CPU: the admission rule of a slot (requests taken in arrival order while the
-batch stays within its read and base limits, always at least one) against a
-model. GPU: requests submitted from several threads at once, mapped in mixed
-batches by two slots, get exactly the records each gets mapped alone; some
-batches carry several requests; empty requests, unknown tickets and a
-destroy with requests still queued behave as documented."""
+batch stays within its read and base limits; a request too large for one
+batch taken in parts) against a model. GPU: requests submitted from several
+threads at once, mapped in mixed batches by two slots, get exactly the
+records each gets mapped alone; some batches carry several requests; a
+request larger than a batch is mapped in parts; empty requests, unknown
+tickets and a destroy with requests still queued behave as documented."""
 import ctypes
 import threading
 
@@ -16,38 +17,54 @@ import shmap_b200 as sb
 from helpers import pack, record_mismatches, xorshift_dna
 
 
-def _admit(reads, bases, max_reads, max_bases):
+def _admit(reads, bases, max_reads, max_bases, front_lens=()):
     f = sb.lib().shm_internal_serve_admit
-    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                  ctypes.c_void_p]
     f.restype = ctypes.c_int64
     r = np.ascontiguousarray(reads, np.int64)
     b = np.ascontiguousarray(bases, np.int64)
-    return f(r.ctypes.data, b.ctypes.data, len(r), max_reads, max_bases)
+    fl = np.ascontiguousarray(list(front_lens) or [0], np.int64)
+    part = ctypes.c_int64()
+    k = f(r.ctypes.data, b.ctypes.data, len(r), fl.ctypes.data, max_reads, max_bases, ctypes.byref(part))
+    return k, part.value
 
 
-def _admit_model(reads, bases, max_reads, max_bases):
+def _admit_model(reads, bases, max_reads, max_bases, front_lens):
     k = tr = tb = 0
-    while k < len(reads):
-        if k > 0 and (tr + reads[k] > max_reads or tb + bases[k] > max_bases):
-            break
+    while k < len(reads) and tr + reads[k] <= max_reads and tb + bases[k] <= max_bases:
         tr += reads[k]
         tb += bases[k]
         k += 1
-    return k
+    part = 0
+    if k == 0 and reads:
+        c = cb = 0
+        while c < reads[0] and c < max_reads and cb + front_lens[c] <= max_bases:
+            cb += front_lens[c]
+            c += 1
+        part = max(c, 1)
+    return k, part
 
 
 def test_admission_rule():
+    """Whole requests in arrival order while both totals fit; a front request
+    that alone does not fit gives the longest run of its first reads that
+    does (so no batch exceeds the slot's budget)."""
     rng = np.random.default_rng(3)
     for _ in range(2000):
         n = int(rng.integers(0, 12))
         reads = rng.integers(1, 5000, n)
-        bases = reads * rng.integers(100, 30000, n)
         mr = int(rng.integers(1, 20000))
-        mb = int(rng.integers(1, 1 << 28))
-        assert _admit(reads, bases, mr, mb) == _admit_model(list(reads), list(bases), mr, mb)
-    # the first request is taken even when it alone exceeds both limits
-    assert _admit([10**6], [10**9], 10, 10) == 1
-    assert _admit([], [], 10, 10) == 0
+        mb = int(rng.integers(60_000, 1 << 28))
+        lens = [rng.integers(100, 60_000, int(x)) for x in reads]
+        bases = np.array([int(v.sum()) for v in lens], np.int64)
+        front = lens[0][: min(int(reads[0]), mr)] if n else []
+        got = _admit(reads, bases, mr, mb, front)
+        assert got == _admit_model(list(reads), list(bases), mr, mb, list(front))
+        if got[1]:
+            assert got[1] <= mr and sum(front[: got[1]]) <= mb
+    assert _admit([10**6], [10**9], 10, 10**9, [10**3] * 10) == (0, 10)
+    assert _admit([], [], 10, 10) == (0, 0)
 
 
 def _workload():
@@ -125,3 +142,29 @@ def test_destroy_maps_what_is_queued(gpu_ctx):
     srv.close()
     assert not record_mismatches(np.concatenate(outs), want)
     del live
+
+
+@pytest.mark.gpu
+def test_request_larger_than_a_batch_goes_in_parts(gpu_ctx):
+    """A request with more reads and bases than one batch may hold is mapped
+    in parts (each within the slot's limits) and gets the records it gets
+    alone; a single read longer than a batch holds is refused at submit."""
+    refs, reads = _workload()
+    g = sb.SketchIndex.from_records(gpu_ctx, refs, 15, 0.1)
+    p = sb.Params(k=15, h_frac=0.1, theta=0.4)
+    seq, offs = pack(reads[:2500])
+    want = g.map_reads(p, seq, offs)
+    small = pack(reads[2500:2520])
+    want_small = g.map_reads(p, *small)
+    with sb.Server(gpu_ctx, g, p, slots=2, max_batch_reads=400, max_batch_bases=1_000_000) as srv:
+        big = srv.submit(seq, offs)
+        t2 = srv.submit(*small)
+        rec, st = srv.poll(big, 120_000)
+        assert not record_mismatches(rec, want)
+        assert st["batch_reads"] <= 400 and st["reads"] == 2500
+        rec2, _ = srv.poll(t2, 120_000)
+        assert not record_mismatches(rec2, want_small)
+        long_read = pack([xorshift_dna(8, 1_000_001)])
+        with pytest.raises(sb.ShmError) as e:
+            srv.submit(*long_read)
+        assert e.value.code == sb.SHM_ERR_INVALID
