@@ -48,6 +48,9 @@ typedef struct shm_params {
     int32_t no_bucket_pruning; /* -P (NBP) */
     int32_t one_sweep;      /* -B (OS) */
     int32_t abs_pos;        /* -F (AP) */
+    double rarity_weight;   /* --rarity-weight: score = rarity-weighted containment (0 = off) */
+    double rarity_tiebreak; /* --rarity-tiebreak: band of scores decided by rarity support (0 = off) */
+    double rarity_alpha;    /* --rarity-alpha: weights 1 / max(hits, 1)^alpha (0 = follow the others) */
 } shm_params;
 
 /* One read's outcome: everything the reference's PAF line is made of
@@ -154,6 +157,18 @@ int shm_map_batch(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const
 int shm_map_batch_device(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* d_seqs,
                          const int64_t* d_offs, const int64_t* h_offs, int32_t n, shm_map_record* d_out);
 
+/* Mapper::map_reads over several GPUs of one process (src/shmap/mod.rs:458-636:
+ * mapping workers over one shared immutable index, output in input order).
+ * ctxs[d] and idxs[d] (d < n_dev) are a context and an index replica on the
+ * same device (built there, or loaded from one index file); the reads are cut
+ * into n_dev contiguous shares of about equal bases, each mapped by
+ * shm_map_batch on its device, all at the same time (one host thread each),
+ * and every record lands in out at its read's place. shares (may be NULL)
+ * gets each share's read count. Nothing crosses between devices. An error
+ * of any share is returned (with its share named) once all have finished. */
+int shm_map_multi(shm_ctx* const* ctxs, const shm_index* const* idxs, int32_t n_dev, const shm_params* p,
+                  const uint8_t* seqs, const int64_t* offs, int32_t n, shm_map_record* out, int32_t* shares);
+
 /* One read per call, every stage launched for that read alone: the plain
  * one-read-per-launch GPU form the batched path is compared against. */
 int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
@@ -235,9 +250,12 @@ int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, doub
  * (host memory) go up once and are parsed on ctx's device: a record per '>'
  * header line, its name the header up to the first space or tab, its
  * sequence its lines joined without '\n' and without one '\r' before a line's
- * end. The sequences stay in device memory, for shm_index_build_fasta and
- * shm_map_fasta. Files with a line starting with '@' (FASTQ) or text before
- * the first header are refused with SHM_ERR_INVALID: read those on the host. */
+ * end. A file whose first byte is '@' is FASTQ: records of four lines ('@'
+ * header, sequence, '+' line, quality; blank lines only at the file's end).
+ * The sequences stay in device memory, for shm_index_build_fasta and
+ * shm_map_fasta. A FASTA file with a line starting with '@' or text before the
+ * first header, and a FASTQ file whose lines do not make four-line records,
+ * are refused with SHM_ERR_INVALID: read those on the host. */
 typedef struct shm_fasta shm_fasta;
 int shm_fasta_parse_device(shm_ctx* ctx, const uint8_t* file, int64_t len, shm_fasta** out);
 /* n records; offs (n+1 entries) and names ('\n'-joined) stay owned by fa. */

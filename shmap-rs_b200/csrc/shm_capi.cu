@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/shmap_gpu.h"
@@ -70,6 +71,18 @@ void shm_params_default(shm_params* p) {
     p->no_bucket_pruning = 0;
     p->one_sweep = 0;
     p->abs_pos = 0;
+    p->rarity_weight = 0.0;
+    p->rarity_tiebreak = 0.0;
+    p->rarity_alpha = 0.0;
+}
+
+static const char* metric_name(int32_t m) {  // Metric's Display (src/types.rs:312-321)
+    switch (m) {
+        case SHM_CONTAINMENT: return "Containment";
+        case SHM_JACCARD: return "Jaccard";
+        case SHM_BUCKET_SH: return "bucket_SH";
+        default: return "bucket_LCS";
+    }
 }
 
 static std::string fmt_g(double x) {  // Rust `{}` for an f64 that needs no exponent
@@ -94,10 +107,18 @@ int shm_params_validate(const shm_params* p) {
         return fail(SHM_ERR_INVALID, "The threshold (-t) should be between 0 and 1. You provided " + fmt_g(p->theta) + ".");
     if (p->min_diff < 0.0)
         return fail(SHM_ERR_INVALID, "The minimum difference (-d) should be >= 0. You provided " + fmt_g(p->min_diff) + ".");
-    if (p->max_overlap < 0.0 || p->max_overlap > 1.0)
-        return fail(SHM_ERR_INVALID, "The maximum overlap (-o) should be between 0 and 1. You provided " + fmt_g(p->max_overlap) + ".");
     if (p->metric < SHM_CONTAINMENT || p->metric > SHM_BUCKET_LCS)
         return fail(SHM_ERR_INVALID, "unknown metric " + std::to_string(p->metric));
+    if (p->rarity_weight < 0.0 || p->rarity_weight > 4.0)
+        return fail(SHM_ERR_INVALID, "The rarity weight (--rarity-weight) should be between 0 and 4. You provided " +
+                                         fmt_g(p->rarity_weight) + ".");
+    if (p->rarity_weight > 0.0 && p->metric != SHM_CONTAINMENT)
+        return fail(SHM_ERR_INVALID, std::string("--rarity-weight is only defined for -m Containment (got ") +
+                                         metric_name(p->metric) +
+                                         "). Jaccard's denominator includes reference k-mers absent from the read, "
+                                         "which have no frequency to weight by.");
+    if (p->max_overlap < 0.0 || p->max_overlap > 1.0)
+        return fail(SHM_ERR_INVALID, "The maximum overlap (-o) should be between 0 and 1. You provided " + fmt_g(p->max_overlap) + ".");
     return SHM_OK;
 }
 
@@ -513,6 +534,53 @@ int shm_map_batch(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const
     shm::map_host(ctx->m, idx->s, *p, seqs, offs, n, out, false);
     return SHM_OK;
     SHM_GUARD_END
+}
+
+int shm_map_multi(shm_ctx* const* ctxs, const shm_index* const* idxs, int32_t n_dev, const shm_params* p,
+                  const uint8_t* seqs, const int64_t* offs, int32_t n, shm_map_record* out, int32_t* shares) {
+    if (!ctxs || !idxs || n_dev <= 0 || !p || n < 0) return fail(SHM_ERR_INVALID, "null argument");
+    if (n > 0 && (!seqs || !offs || !out)) return fail(SHM_ERR_INVALID, "null argument");
+    for (int32_t d = 0; d < n_dev; d++) {
+        int v = check_map_args(ctxs[d], idxs[d], p, n);
+        if (v != SHM_OK) return v;
+        if (idxs[d]->s->device != ctxs[d]->m->device)
+            return fail(SHM_ERR_INVALID, "index " + std::to_string(d) + " is not on its context's device");
+        for (int32_t e = 0; e < d; e++)
+            if (ctxs[e] == ctxs[d]) return fail(SHM_ERR_INVALID, "a context appears twice");
+    }
+    int v = check_reads(offs, n);
+    if (v != SHM_OK) return v;
+    // contiguous shares of about equal bases, in read order
+    std::vector<int32_t> cut((size_t)n_dev + 1, 0);
+    cut[(size_t)n_dev] = n;
+    const int64_t total = n ? offs[n] - offs[0] : 0;
+    for (int32_t d = 1; d < n_dev; d++) {
+        const int64_t want = offs[0] + total * d / n_dev;
+        int32_t lo = cut[(size_t)d - 1], hi = n;  // first read starting at or after want
+        while (lo < hi) {
+            const int32_t mid = lo + (hi - lo) / 2;
+            if (offs[mid] < want) lo = mid + 1;
+            else hi = mid;
+        }
+        cut[(size_t)d] = lo;
+    }
+    if (shares)
+        for (int32_t d = 0; d < n_dev; d++) shares[d] = cut[(size_t)d + 1] - cut[(size_t)d];
+    std::vector<int> rc((size_t)n_dev, SHM_OK);
+    std::vector<std::string> msg((size_t)n_dev);
+    auto work = [&](int32_t d) {
+        const int32_t a = cut[(size_t)d], b = cut[(size_t)d + 1];
+        if (a == b) return;
+        rc[(size_t)d] = shm_map_batch(ctxs[d], idxs[d], p, seqs, offs + a, b - a, out + a);
+        if (rc[(size_t)d] != SHM_OK) msg[(size_t)d] = shm_last_error();
+    };
+    std::vector<std::thread> th;
+    for (int32_t d = 1; d < n_dev; d++) th.emplace_back(work, d);
+    work(0);
+    for (auto& t : th) t.join();
+    for (int32_t d = 0; d < n_dev; d++)
+        if (rc[(size_t)d] != SHM_OK) return fail(rc[(size_t)d], "device share " + std::to_string(d) + ": " + msg[(size_t)d]);
+    return SHM_OK;
 }
 
 int shm_map_plain(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,

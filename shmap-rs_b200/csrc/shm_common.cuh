@@ -80,6 +80,14 @@ struct DevParams {
     // slot_mul[b] = min(2^64 - 1, floor(2^(64+b) / (thr + 1))): __umul64hi(h, slot_mul[b])
     // maps h <= thr monotonically onto [0, 2^b)
     uint64_t slot_mul[16];
+    // rarity (src/shmap/mod.rs:694-723, scoring.rs:214-281, 409-481): when on,
+    // a seed of c hits weighs wtab[c] = max(c, 1)^-alpha (the host's pow;
+    // c < wtab_n), and refinement reports each bucket's weighted support
+    int32_t rarity;     // a rarity flag is on
+    int32_t rw_score;   // --rarity-weight: the score is the weighted containment
+    double tiebreak;    // --rarity-tiebreak band (0 = off)
+    const double* wtab;
+    uint32_t wtab_n;
 };
 
 __device__ __forceinline__ uint64_t rotl64(uint64_t x, uint32_t n) {

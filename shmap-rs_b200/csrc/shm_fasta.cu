@@ -5,10 +5,12 @@
 // those byte rules, and this parser keeps them exactly. Lines end at '\n'.
 // One '\r' right before a line's end is dropped. A line whose first byte is
 // '>' is a header, and every other line after the first header belongs to
-// the current record, empty lines included. It declines a file that has a
-// line starting with '@' (FASTQ, which the host reader handles) or a
-// non-empty line before the first header (which the host reader reports as
-// an error), so such files go to the host reader.
+// the current record, empty lines included. It declines a FASTA file that
+// has a line starting with '@' or a non-empty line before the first header
+// (which the host reader reports as an error), so such files go to the host
+// reader. A file whose first byte is '@' is FASTQ: records of four lines
+// (header, sequence, '+', quality), parsed by line index (see the FASTQ
+// passes below).
 //
 // The file's bytes are processed in chunks of CHUNK bytes, one CTA per chunk,
 // each thread taking a contiguous run of the chunk (staged in shared memory):
@@ -318,6 +320,140 @@ __global__ void k_fa_name_write(FaView v, const int64_t* __restrict__ hdr_pos, i
     }
 }
 
+// ---------------------------------------------------------------- FASTQ
+// Records of four lines (needletail's FASTQ, src/io/mod.rs:383-427): '@'
+// header, sequence, '+' line, quality. A byte's role follows from the index
+// of its line, counted from the file's start: the lines are counted per
+// chunk, scanned over the chunks, and within a chunk over the threads' runs.
+// A line 4r must start with '@' and a line 4r+2 with '+', and the lines must
+// make whole records (blank lines at the file's end aside): else the file is
+// refused and read on the host.
+enum : uint32_t { FQ_BAD = 4u };
+
+// Pass 1: newlines per chunk.
+__global__ void __launch_bounds__(FA_THREADS) k_fq_lines(FaView v, uint64_t* __restrict__ nl) {
+    __shared__ uint8_t sm[CHUNK];
+    __shared__ int64_t sh[32];
+    __shared__ int64_t tot;
+    for (int64_t c = blockIdx.x; c < v.n_chunks; c += gridDim.x) {
+        const int64_t c0 = c * CHUNK, cend = min(c0 + CHUNK, v.len);
+        stage_chunk(v, c0, cend, sm);
+        const int64_t a = c0 + (int64_t)threadIdx.x * FA_PER_THREAD, b = min(a + FA_PER_THREAD, cend);
+        int64_t k = 0;
+        for (int64_t i = a; i < b; i++) k += sm[i - c0] == '\n';
+        block_scan_excl_op<int64_t>(k, 0, SumOp(), sh, &tot);
+        if (threadIdx.x == 0) nl[c] = (uint64_t)tot;
+        __syncthreads();
+    }
+}
+
+// The index of the line a thread's run starts in (from the chunk's first
+// line's index and the newlines of the runs before it in the chunk).
+__device__ int64_t fq_run_line(const uint8_t* sm, int64_t c0, int64_t a, int64_t b, uint64_t chunk_line, int64_t* sh,
+                               int64_t* tot) {
+    int64_t k = 0;
+    for (int64_t i = a; i < b; i++) k += sm[i - c0] == '\n';
+    return (int64_t)chunk_line + block_scan_excl_op<int64_t>(k, 0, SumOp(), sh, tot);
+}
+
+// Byte i of line `line`: 1 = a sequence byte kept, 2 = the first byte of a
+// header line, 0 = neither; *bad for a line that breaks the record layout.
+__device__ __forceinline__ int fq_classify(const FaView& v, const uint8_t* sm, int64_t c0, int64_t cend, int64_t i,
+                                           int64_t& line, bool* bad) {
+    const uint8_t ch = sm[i - c0];
+    int r = 0;
+    if (ch == '\n') {
+        line++;
+        return 0;
+    }
+    const int role = (int)(line & 3);
+    if (line_start(v, sm, c0, i)) {
+        if (role == 0) {
+            if (ch == '@') r = 2;
+            else *bad = true;
+        } else if (role == 2 && ch != '+') {
+            *bad = true;
+        }
+    }
+    if (role == 1 && !dropped_cr(v, sm, c0, cend, i)) return 1;
+    return r;
+}
+
+// Pass 2: kept bytes and headers per chunk.
+__global__ void __launch_bounds__(FA_THREADS) k_fq_count(FaView v, const uint64_t* __restrict__ nl_off,
+                                                       uint64_t* __restrict__ nkeep, uint32_t* __restrict__ nhdr,
+                                                       uint32_t* __restrict__ flags) {
+    __shared__ uint8_t sm[CHUNK];
+    __shared__ int64_t sh[32];
+    __shared__ int64_t tot;
+    for (int64_t c = blockIdx.x; c < v.n_chunks; c += gridDim.x) {
+        const int64_t c0 = c * CHUNK, cend = min(c0 + CHUNK, v.len);
+        stage_chunk(v, c0, cend, sm);
+        const int64_t a = c0 + (int64_t)threadIdx.x * FA_PER_THREAD, b = min(a + FA_PER_THREAD, cend);
+        int64_t line = fq_run_line(sm, c0, a, b, nl_off[c], sh, &tot);
+        int64_t k = 0, h = 0;
+        bool bad = false;
+        for (int64_t i = a; i < b; i++) {
+            const int r = fq_classify(v, sm, c0, cend, i, line, &bad);
+            k += r == 1;
+            h += r == 2;
+        }
+        if (bad) atomicOr(flags, (uint32_t)FQ_BAD);
+        block_scan_excl_op<int64_t>(k, 0, SumOp(), sh, &tot);
+        const int64_t ck = tot;
+        block_scan_excl_op<int64_t>(h, 0, SumOp(), sh, &tot);
+        if (threadIdx.x == 0) {
+            nkeep[c] = (uint64_t)ck;
+            nhdr[c] = (uint32_t)tot;
+        }
+        __syncthreads();
+    }
+}
+
+// Pass 3: the kept bytes at their place; each header's position and the
+// sequence bytes before it.
+__global__ void __launch_bounds__(FA_THREADS) k_fq_write(FaView v, const uint64_t* __restrict__ nl_off,
+                                                       const uint64_t* __restrict__ keep_off,
+                                                       const uint32_t* __restrict__ hdr_off, uint8_t* __restrict__ out,
+                                                       int64_t* __restrict__ hdr_pos, int64_t* __restrict__ hdr_seq) {
+    __shared__ uint8_t sm[CHUNK];
+    __shared__ uint8_t so[CHUNK];
+    __shared__ int64_t sh[32];
+    __shared__ int64_t tot;
+    for (int64_t c = blockIdx.x; c < v.n_chunks; c += gridDim.x) {
+        const int64_t c0 = c * CHUNK, cend = min(c0 + CHUNK, v.len);
+        stage_chunk(v, c0, cend, sm);
+        const int64_t a = c0 + (int64_t)threadIdx.x * FA_PER_THREAD, b = min(a + FA_PER_THREAD, cend);
+        const int64_t line0 = fq_run_line(sm, c0, a, b, nl_off[c], sh, &tot);
+        int64_t line = line0, k = 0, h = 0;
+        bool bad = false;
+        for (int64_t i = a; i < b; i++) {
+            const int r = fq_classify(v, sm, c0, cend, i, line, &bad);
+            k += r == 1;
+            h += r == 2;
+        }
+        const int64_t kb = block_scan_excl_op<int64_t>(k, 0, SumOp(), sh, &tot);
+        const int64_t ck = tot;
+        const int64_t hb = block_scan_excl_op<int64_t>(h, 0, SumOp(), sh, &tot);
+        line = line0;
+        int64_t kk = kb, hh = (int64_t)hdr_off[c] + hb;
+        for (int64_t i = a; i < b; i++) {
+            const int r = fq_classify(v, sm, c0, cend, i, line, &bad);
+            if (r == 1) {
+                so[kk++] = sm[i - c0];
+            } else if (r == 2) {
+                hdr_pos[hh] = i;
+                hdr_seq[hh] = (int64_t)keep_off[c] + kk;
+                hh++;
+            }
+        }
+        __syncthreads();
+        uint8_t* dst = out + keep_off[c];
+        for (int64_t j = threadIdx.x; j < ck; j += blockDim.x) dst[j] = so[j];
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 FastaDev* fasta_parse_device(int device, cudaStream_t s, const uint8_t* file, int64_t len, std::string* why) {
@@ -325,6 +461,11 @@ FastaDev* fasta_parse_device(int device, cudaStream_t s, const uint8_t* file, in
     auto* F = new FastaDev();
     try {
         FaView v{};
+        // FASTQ when the file starts with '@'; its blank lines at the end are
+        // not part of any record
+        const bool fastq = len > 0 && file[0] == '@';
+        if (fastq)
+            while (len > 0 && (file[len - 1] == '\n' || file[len - 1] == '\r')) len--;
         DevBuf<uint8_t> raw;
         raw.reserve((size_t)len + 1);
         if (len) SHM_CUDA(cudaMemcpyAsync(raw.p, file, (size_t)len, cudaMemcpyHostToDevice, s));
@@ -349,7 +490,30 @@ FastaDev* fasta_parse_device(int device, cudaStream_t s, const uint8_t* file, in
         const int grid = grid_for((size_t)std::max<int64_t>(nc, 1), 1, 4);
         uint64_t total = 0;
         uint32_t n_rec = 0, fl = 0;
-        if (nc) {
+        DevBuf<uint64_t> nl, nl_off;
+        if (fastq) {
+            nl.reserve((size_t)nc + 1);
+            nl_off.reserve((size_t)nc + 1);
+            uint64_t lines = 0;
+            k_fq_lines<<<grid, FA_THREADS, 0, s>>>(v, nl.p);
+            SHM_CUDA(cudaGetLastError());
+            exclusive_scan_u64(nl.p, nl_off.p, (size_t)nc, s);
+            k_fq_count<<<grid, FA_THREADS, 0, s>>>(v, nl_off.p, nkeep.p, nhdr.p, flags.p);
+            SHM_CUDA(cudaGetLastError());
+            exclusive_scan_u64(nkeep.p, keep_off.p, (size_t)nc, s);
+            exclusive_scan_u32(nhdr.p, hdr_off.p, (size_t)nc, s);
+            count_launch(2);
+            SHM_CUDA(cudaMemcpyAsync(&lines, nl_off.p + nc, sizeof lines, cudaMemcpyDeviceToHost, s));
+            SHM_CUDA(cudaMemcpyAsync(&total, keep_off.p + nc, sizeof total, cudaMemcpyDeviceToHost, s));
+            SHM_CUDA(cudaMemcpyAsync(&n_rec, hdr_off.p + nc, sizeof n_rec, cudaMemcpyDeviceToHost, s));
+            SHM_CUDA(cudaMemcpyAsync(&fl, flags.p, sizeof fl, cudaMemcpyDeviceToHost, s));
+            SHM_CUDA(cudaStreamSynchronize(s));
+            if ((fl & FQ_BAD) || (lines + 1) % 4 != 0) {  // the last line (the quality) ends the file
+                *why = "not FASTQ records of four lines";
+                delete F;
+                return nullptr;
+            }
+        } else if (nc) {
             k_fa_marks<<<grid, FA_THREADS, 0, s>>>(v, last_ls.p, any_hdr.p, flags.p);
             SHM_CUDA(cudaGetLastError());
             k_fa_carry<<<1, 1024, 0, s>>>(nc, last_ls.p, any_hdr.p, carry_ls.p, carry_open.p);
@@ -382,8 +546,12 @@ FastaDev* fasta_parse_device(int device, cudaStream_t s, const uint8_t* file, in
             DevBuf<int64_t> hdr_pos, hdr_seq;
             hdr_pos.reserve(n_rec);
             hdr_seq.reserve(n_rec);
-            k_fa_write<<<grid, FA_THREADS, 0, s>>>(v, carry_ls.p, carry_open.p, keep_off.p, hdr_off.p, F->seq.p,
-                                                   hdr_pos.p, hdr_seq.p);
+            if (fastq)
+                k_fq_write<<<grid, FA_THREADS, 0, s>>>(v, nl_off.p, keep_off.p, hdr_off.p, F->seq.p, hdr_pos.p,
+                                                       hdr_seq.p);
+            else
+                k_fa_write<<<grid, FA_THREADS, 0, s>>>(v, carry_ls.p, carry_open.p, keep_off.p, hdr_off.p, F->seq.p,
+                                                       hdr_pos.p, hdr_seq.p);
             SHM_CUDA(cudaGetLastError());
             DevBuf<uint64_t> nlen, noff;
             nlen.reserve(n_rec);

@@ -21,9 +21,10 @@ struct FastaDev {
     DevBuf<shm_map_record> rec;  // records of the reads mapped from it
 };
 
-// Parses the file's bytes (host memory) on the device. Returns null, with the
-// reason in *why, for files the host reader handles instead: FASTQ records, or
-// text before the first header (which the host reader reports).
+// Parses the file's bytes (host memory) on the device: FASTA, or FASTQ when
+// the first byte is '@'. Returns null, with the reason in *why, for files the
+// host reader handles instead: a FASTA file with a line starting with '@' or
+// text before the first header, a FASTQ file not made of four-line records.
 FastaDev* fasta_parse_device(int device, cudaStream_t s, const uint8_t* file, int64_t len, std::string* why);
 
 }  // namespace shm

@@ -383,6 +383,8 @@ IndexStorage* build_index(const uint8_t* h_seq, const int64_t* seg_off_b, int32_
         SHM_CUDA(cudaGetLastError());
 
         // 4. forward-strand prefix, hash directory, bucket table, device view
+        // the longest hit list kept: -M erases every list longer than M
+        ix->max_list = max_matches > 0 ? std::min<uint32_t>(hst.highest, (uint32_t)max_matches) : hst.highest;
         finish_index(ix, thr, n_kept, n_kmers, n_hits, hst.highest, s);
 
         shm_index_stats& st = ix->stats;

@@ -67,7 +67,7 @@ struct IndexStorage {
     double h_frac = 0;
     int32_t max_matches = -1;
     int device = 0;
-    uint32_t max_list = 0;  // longest hit list (set when read from a file)
+    uint32_t max_list = 0;  // longest hit list of the index
 };
 
 // An index written to a file and read back (shm_index.cu); failures throw

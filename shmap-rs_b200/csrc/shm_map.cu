@@ -116,6 +116,7 @@ struct BatchView {
     BatchMax* mx;
     shm_map_record* out;
     uint32_t* lcs_pos;  // bucket_LCS: each seed's read positions, decreasing (at kb + its ooff)
+    double* r_mw;       // rarity: per read, the weighted total of its k-mers (m_weight)
 };
 
 // ------------------------------------------------------------------ helpers
@@ -215,7 +216,7 @@ __device__ __forceinline__ bool bucket_metric(const DevParams& P) { return P.met
 // global table and k_refine.
 constexpr int RCHIP_M = 248;
 __device__ __forceinline__ bool refine_on_chip(const DevParams& P, uint32_t m, int32_t halflen) {
-    return !P.ap && !bucket_metric(P) && m <= (uint32_t)RCHIP_M && halflen <= RCHIP_M;
+    return !P.ap && !bucket_metric(P) && !P.rarity && m <= (uint32_t)RCHIP_M && halflen <= RCHIP_M;
 }
 
 // The sketch hashes are uniform in [0, thr], so their low bits pick the slot.
@@ -1199,6 +1200,7 @@ __global__ void __launch_bounds__(256) k_bscan(BatchView v) {
             jb.rmax = s.rmax;
             jb.pad0 = jb.pad1 = 0;
             jb.score = -1.0;
+            jb.support = 0.0;
             jb.t_l = jb.t_r = jb.inter = jb.same = jb.s_sz = -1;
             if (v.P.nbp) {
                 jb.sh = 1.0;  // seed_heuristic_pass does nothing under NBP (pruning.rs:351)
@@ -1316,6 +1318,8 @@ struct RefScratch {
     int32_t* base;
     size_t per_warp;  // ints
     uint32_t nu_max, wmax;
+    uint32_t ring_n;  // ints of the occurrence rings (m_max + 1)
+    size_t wt_at;     // rarity: ints from a warp's base to its f64 weights (even)
 };
 
 // pht_lookup for U hashes of one lane, the probes issued together; s[u] =
@@ -1782,6 +1786,279 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
     }
 }
 
+// ------------------------------------------------------------------ rarity
+// m_weight of each read (src/shmap/mod.rs:712-722): the sum over its seeds,
+// in rarest-first order, of weight * occurrences, one f64 addition at a time
+// in that order, as the reference adds them.
+__global__ void k_rarity_mw(BatchView v) {
+    for (int32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < v.n; q += gridDim.x * blockDim.x) {
+        const uint64_t kb = v.kcap_off[q];
+        const int32_t n_u = v.r_nu[q];
+        double mw = 0.0;
+        for (int32_t i = 0; i < n_u; i++) {
+            const SeedRec sr = v.sd[kb + i];
+            const uint32_t c = min(sr.cnt, v.P.wtab_n - 1u);
+            mw = __dadd_rn(mw, __dmul_rn(v.P.wtab[c], (double)(sr.os >> 1)));
+        }
+        v.r_mw[q] = mw;
+    }
+}
+
+// best_fixed_length with its rarity-weighted support (src/shmap/scoring.rs:
+// 189-291). The reference keeps the support as one running f64 sum, adding a
+// position's weight when it enters the window and counts (its seed's count in
+// the window is still within the seed's occurrences) and subtracting a
+// position's weight when it leaves the window while it counts; rounding makes
+// that sum depend on the order of those operations, so it is replayed in
+// that order by one lane. Which operations happen is decided in parallel
+// first, from the same per-seed occurrence rings as refine_one:
+//   enters counting: the seed's occs-th previous occurrence p lies before the
+//     window start at which the position enters;
+//   leaves counting: the seed's occs-th next occurrence (the position x whose
+//     p is this one) lies at or past the window end.
+// Without --rarity-weight the window is the one refine_one's arithmetic
+// picks, and the replay runs up to it; with it, the score of every window is
+// the weighted containment clamp(support / m_weight, 0, 1) and the replay
+// takes its first maximum.
+constexpr int RAR_ADD = 1, RAR_SUB = 2;
+
+struct RarScratch {
+    int32_t *cntA, *D, *PC, *ring, *nxt, *flag;
+    double* wt;
+};
+
+__device__ __forceinline__ int32_t window_end(const DevIndex& I, uint32_t G0, int64_t from, int32_t x, int32_t W,
+                                              int32_t m, bool ap) {
+    if (!ap) return min(x + m, W);
+    const int32_t lim = (int32_t)(__ldg(I.ref_rs + G0 + from + x) >> 1) + m;
+    int32_t lo = x, len = W - x;
+    while (len > 0) {
+        const int32_t half = len >> 1;
+        if ((int32_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) < lim) {
+            lo += half + 1;
+            len -= half + 1;
+        } else {
+            len = half;
+        }
+    }
+    return lo;
+}
+
+__device__ void refine_rarity_one(const BatchView& v, BucketJob* J, int32_t q, const RarScratch& R, int lane,
+                                  unsigned lt) {
+    const bool ap = v.P.ap != 0;
+    const DevIndex& I = v.I;
+    const int32_t m = v.r_m[q], n_u = v.r_nu[q];
+    const int64_t h = v.r_half[q];
+    const uint64_t kb = v.kcap_off[q];
+    const int32_t seg = J->seg;
+    const uint32_t G0 = __ldg(I.seg_off + seg), Gend = __ldg(I.seg_off + seg + 1);
+    const int64_t seglen = (int64_t)(Gend - G0);
+    const int64_t from = (int64_t)J->bb * h;
+    const int64_t end = min(((int64_t)J->bb + 2) * h, seglen);
+    const int32_t W = (int32_t)(end - from);
+    if (lane == 0 && W > 0) atomicAdd(&v.mx->refine_kmers, (unsigned long long)W);
+    for (int32_t i = lane; i < n_u; i += 32) R.cntA[i] = 0;
+    for (int32_t i = lane; i <= W; i += 32) {
+        R.D[i] = 0;
+        R.nxt[i] = INT32_MAX;
+    }
+    __syncwarp();
+    int32_t pc_carry = 0;
+    if (lane == 0) R.PC[0] = 0;
+    for (int32_t c0 = 0; c0 < W; c0 += 32) {
+        const int32_t x = c0 + lane;
+        const bool valid = x < W;
+        const uint32_t gid = G0 + (uint32_t)(from + (valid ? x : 0));
+        uint64_t hx[1] = {valid ? __ldg(I.ref_h + gid) : 0};
+        const uint32_t rs = valid ? __ldg(I.ref_rs + gid) : 0;
+        bool on[1] = {valid};
+        int32_t sx[1];
+        pht_lookup_u<1>(v, q, hx, on, sx);
+        const int32_t s = sx[0];
+        const SeedRec sr = s >= 0 ? v.sd[kb + s] : SeedRec{0u, 0u, 0u, 0u};
+        {
+            const int32_t cv = (valid && s >= 0) ? (((sr.os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
+            const int32_t inc = warp_inclusive_scan(cv);
+            if (valid) R.PC[x + 1] = pc_carry + inc;
+            pc_carry += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, s);
+        int32_t t = 0, occ = 1, rho = 0, gsz = 0;
+        int32_t fl = 0;
+        if (s >= 0) {
+            occ = (int32_t)(sr.os >> 1);
+            rho = __popc(peers & lt);
+            gsz = __popc(peers);
+            t = R.cntA[s] + rho;
+            int32_t p = -1;  // the occ-th previous occurrence in the window region, -1 = none
+            if (t >= occ) {
+                if (rho >= occ)
+                    p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
+                else
+                    p = R.ring[sr.ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
+            }
+            int32_t Lj;
+            if (!ap) {
+                Lj = x - m + 1;
+            } else {  // first l with R[l] > R[x] - m
+                const int32_t rv = (int32_t)(rs >> 1) - m;
+                int32_t lo = 0, len = x;
+                while (len > 0) {
+                    int32_t half = len >> 1;
+                    if ((int32_t)(__ldg(I.ref_rs + G0 + from + lo + half) >> 1) <= rv) {
+                        lo += half + 1;
+                        len -= half + 1;
+                    } else {
+                        len = half;
+                    }
+                }
+                Lj = lo;
+            }
+            const int32_t lin = max(Lj, 0);  // the window start at which x enters
+            const int32_t st = max(p + 1, lin);
+            if (st <= x) {
+                atomicAdd(R.D + st, 1);
+                atomicAdd(R.D + x + 1, -1);
+            }
+            if (p < lin) fl |= RAR_ADD;
+            if (p >= 0) R.nxt[p] = x;  // x is p's occs-th next occurrence
+            R.wt[x] = v.P.wtab[min(sr.cnt, v.P.wtab_n - 1u)];
+        }
+        if (valid) R.flag[x] = s >= 0 ? fl : -1;
+        __syncwarp();
+        if (s >= 0) {
+            if (rho >= gsz - occ) R.ring[sr.ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = x;
+            if (rho == gsz - 1) R.cntA[s] = t + 1;
+        }
+        __syncwarp();
+    }
+    // leaves counting: its occs-th next occurrence at or past the window end
+    for (int32_t x = lane; x < W; x += 32) {
+        const int32_t f = R.flag[x];
+        if (f >= 0 && R.nxt[x] >= window_end(I, G0, from, x, W, m, ap)) R.flag[x] = f | RAR_SUB;
+    }
+    // intersection per window start (prefix of D, kept in D) and, without
+    // --rarity-weight, the window refine_one's arithmetic picks
+    const bool jac = v.P.metric == 1;
+    const bool rw = v.P.rw_score != 0;
+    double best = -1.0;
+    int32_t bl = -1, bI = -1;
+    int32_t icarry = 0;
+    for (int32_t c0 = 0; c0 < W; c0 += 32) {
+        const int32_t x = c0 + lane;
+        int32_t dv = x < W ? R.D[x] : 0;
+        int32_t inc = warp_inclusive_scan(dv) + icarry;
+        icarry = __shfl_sync(0xffffffffu, inc, 31);
+        if (x < W) {
+            R.D[x] = inc;
+            if (!rw) {
+                const int32_t r = window_end(I, G0, from, x, W, m, ap);
+                bool better;
+                if (jac) {
+                    const double score = __ddiv_rn((double)inc, (double)(m + (r - x) - inc));
+                    better = score > best;
+                    if (better) best = score;
+                } else {
+                    better = inc > bI;
+                }
+                if (better) {
+                    bl = x;
+                    bI = inc;
+                }
+            }
+        }
+    }
+    if (!rw) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            int32_t obl = __shfl_xor_sync(0xffffffffu, bl, o);
+            int32_t obI = __shfl_xor_sync(0xffffffffu, bI, o);
+            const bool take = jac ? (ob > best || (ob == best && obl >= 0 && (bl < 0 || obl < bl)))
+                                  : (obI > bI || (obI == bI && obl >= 0 && (bl < 0 || obl < bl)));
+            if (take) {
+                best = ob;
+                bl = obl;
+                bI = obI;
+            }
+        }
+        if (!jac && bl >= 0) best = __ddiv_rn((double)bI, (double)m);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        // the reference's running sum, in its order, up to the chosen window
+        // (or over every window, taking the first maximum of the weighted score)
+        const double mw = rw ? v.r_mw[q] : 0.0;
+        const bool mono = mw > 0.0 && mw < INFINITY;
+        double w = 0.0, wbest = 0.0;
+        int32_t r = 0;
+        if (rw) {
+            best = -1.0;
+            bl = -1;
+        }
+        double w_at_best = 0.0;
+        const int32_t last = rw ? W - 1 : bl;
+        for (int32_t l = 0; l <= last; l++) {
+            const int32_t rl = window_end(I, G0, from, l, W, m, ap);
+            for (; r < rl; r++)
+                if (R.flag[r] > 0 && (R.flag[r] & RAR_ADD)) w = __dadd_rn(w, R.wt[r]);
+            if (rw) {
+                // the score is monotone in w (for a positive finite m_weight):
+                // a window can beat the best only with more support
+                if (!mono || bl < 0 || w > w_at_best) {
+                    double sc = __ddiv_rn(w, mw);  // min(max(x, 0), 1), NaN kept, as clamp does
+                    sc = sc < 0.0 ? 0.0 : sc;
+                    sc = 1.0 < sc ? 1.0 : sc;
+                    if (sc > best) {
+                        best = sc;
+                        bl = l;
+                        w_at_best = w;
+                    }
+                }
+            } else if (l == bl) {
+                wbest = w;
+            }
+            if (R.flag[l] > 0 && (R.flag[l] & RAR_SUB)) w = __dsub_rn(w, R.wt[l]);
+        }
+        if (rw) wbest = w_at_best;
+        J->score = best;
+        J->support = wbest;
+        if (bl >= 0) {
+            const int32_t br = window_end(I, G0, from, bl, W, m, ap);
+            const int32_t tl = (int32_t)(__ldg(I.ref_rs + G0 + from + bl) >> 1);
+            const int32_t tr = (int32_t)(__ldg(I.ref_rs + G0 + from + br - 1) >> 1);
+            J->t_l = tl;
+            J->t_r = tr;
+            J->inter = R.D[bl];
+            J->same = R.PC[br] - R.PC[bl];
+            J->s_sz = tr - tl + 1;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine_rarity(BatchView v, RefScratch rsc) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nfar = v.mx->n_far;
+    int32_t* const base = rsc.base + (size_t)wid * rsc.per_warp;
+    RarScratch R;
+    R.cntA = base;
+    R.D = R.cntA + rsc.nu_max;
+    R.PC = R.D + rsc.wmax + 1;
+    R.ring = R.PC + rsc.wmax + 1;
+    R.nxt = R.ring + rsc.ring_n;
+    R.flag = R.nxt + rsc.wmax + 1;
+    R.wt = (double*)(base + rsc.wt_at);
+    for (uint32_t ci = wid; ci < nfar; ci += nwarps) {
+        BucketJob* J = v.jobs + v.cfar[ci];
+        const int32_t q = J->read;
+        refine_rarity_one(v, J, q, R, lane, lt);
+        __syncwarp();
+    }
+}
+
 // bucket_LCS over the candidates in cfar, a warp at a time, taken from a
 // queue (their costs differ by orders of magnitude: a window in a tandem
 // repeat feeds each seed's many read positions once per k-mer). The two tail
@@ -2101,7 +2378,7 @@ constexpr int SWEEP_WARPS = 4;
 constexpr int SWEEP_CAP = 64;
 
 struct SweepCand {
-    double sh, score;
+    double sh, score, support;
     int32_t seg, bb, m0, t_l, t_r, job;
 };
 
@@ -2115,6 +2392,7 @@ __device__ __forceinline__ SweepCand load_cand(const BucketJob& j, uint32_t ji) 
     SweepCand c;
     c.sh = j.sh;
     c.score = j.score;
+    c.support = j.support;
     c.seg = j.seg;
     c.bb = j.bb;
     c.m0 = j.m0;
@@ -2203,15 +2481,25 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
             if (st == ST_UNMAPPED) {
                 const bool nbp = v.P.nbp != 0;
                 int32_t fb = 0;
+                // the rarity tie-break (scoring.rs:409-416, 453-481): a bucket is
+                // admitted above thr - band * |thr|, and one within the band of the
+                // incumbent's score takes over only with more rarity support
+                const double tb = v.P.tiebreak;
+                auto admit_of = [&](double t) { return tb > 0.0 ? __dsub_rn(t, __dmul_rn(tb, fabs(t))) : t; };
+                auto takes = [&](const SweepCand& c, const SweepCand& cur) {
+                    if (tb > 0.0 && fabs(__dsub_rn(c.score, cur.score)) <= __dmul_rn(tb, fabs(cur.score)))
+                        return c.support > cur.support;
+                    return c.score > cur.score;
+                };
                 // pass 1 (mod.rs:816-832): thr = theta, no forbidden region
                 double thr = v.P.theta;
                 int32_t b1 = -1;
                 for (uint32_t i = 0; i < nc; i++) {
                     const SweepCand& c = L[i];
                     if (!nbp && !(c.sh >= thr)) continue;
-                    if (c.score > thr) {
+                    if (c.score > admit_of(thr)) {
                         fb++;
-                        if (b1 < 0 || c.score > L[b1].score) {
+                        if (b1 < 0 || takes(c, L[b1])) {
                             thr = fmax(thr, c.score);
                             b1 = (int32_t)i;
                         }
@@ -2225,10 +2513,10 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
                     for (uint32_t i = 0; i < nc; i++) {
                         const SweepCand& c = L[i];
                         if (!nbp && !(c.sh >= thr)) continue;
-                        if (c.score > thr) {
+                        if (c.score > admit_of(thr)) {
                             fb++;
                             if (overlap_of(c, B1) < v.P.max_overlap) {
-                                if (b2 < 0 || c.score > L[b2].score) {
+                                if (b2 < 0 || takes(c, L[b2])) {
                                     thr = fmax(thr, c.score);
                                     b2 = (int32_t)i;
                                 }
@@ -2380,6 +2668,11 @@ struct MapScratch {
     DevBuf<shm_map_record> out;
     SketchLuts* luts = nullptr;
     int32_t luts_k = -1;
+    // rarity weights max(c, 1)^-alpha for one (index, alpha), and per-read m_weight
+    DevBuf<double> wtab, r_mw;
+    double wtab_alpha = 0.0;
+    const IndexStorage* wtab_ix = nullptr;
+    uint32_t wtab_n = 0;
 };
 
 MapCtx* mapctx_create(int device, size_t hbm_budget) {
@@ -2672,6 +2965,38 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     v.P.nbp = p.no_bucket_pruning;
     v.P.os = p.one_sweep;
     v.P.ap = p.abs_pos;
+    {
+        // rarity (src/shmap/mod.rs:694-723): alpha follows --rarity-alpha, else
+        // --rarity-weight, else 1 when only the tie-break is on
+        const double alpha = p.rarity_alpha > 0.0    ? p.rarity_alpha
+                             : p.rarity_weight > 0.0 ? p.rarity_weight
+                             : p.rarity_tiebreak > 0.0 ? 1.0
+                                                       : 0.0;
+        v.P.tiebreak = p.rarity_tiebreak > 0.0 ? p.rarity_tiebreak : 0.0;
+        v.P.rarity = alpha > 0.0 && p.metric <= SHM_JACCARD;  // the bucket metrics report no support
+        v.P.rw_score = v.P.rarity && p.rarity_weight > 0.0;
+        if (v.P.rarity) {
+            // a seed's hit count is at most the longest hit list of the index
+            const uint32_t n_w = ix->max_list + 1;
+            if (S.wtab_ix != ix || S.wtab_alpha != alpha || S.wtab_n != n_w) {
+                std::vector<double> w(n_w);
+                for (uint32_t c2 = 0; c2 < n_w; c2++) w[c2] = std::pow((double)std::max<uint32_t>(c2, 1u), -alpha);
+                S.wtab.reserve(n_w);
+                SHM_CUDA(cudaMemcpy(S.wtab.p, w.data(), sizeof(double) * n_w, cudaMemcpyHostToDevice));
+                S.wtab_ix = ix;
+                S.wtab_alpha = alpha;
+                S.wtab_n = n_w;
+            }
+            v.P.wtab = S.wtab.p;
+            v.P.wtab_n = n_w;
+        }
+        if (v.P.tiebreak > 0.0) {
+            // the band admits scores below thr: pass 2's threshold can go down to
+            // fl(fl(theta - fl(band * theta)) * fl(1 - d)), so candidates reach that low
+            const double adm = p.theta - v.P.tiebreak * std::fabs(p.theta);
+            v.P.theta_low = std::min(v.P.theta_low, adm * (1.0 - p.min_diff));
+        }
+    }
     for (int b = 0; b < 16; b++) {
         const unsigned __int128 num = (unsigned __int128)1 << (64 + b);
         const unsigned __int128 den = (unsigned __int128)ix->dev.thr + 1;
@@ -2919,7 +3244,12 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     RefScratch rsc{};
     rsc.nu_max = nu_max + 1;
     rsc.wmax = 2 * half_max + 2;
+    rsc.ring_n = m_max + 1;
     rsc.per_warp = (size_t)rsc.nu_max + 2 * ((size_t)rsc.wmax + 1) + (size_t)m_max + 1;
+    if (v.P.rarity) {  // + nxt, flag, and the f64 weights at an even offset (every warp base 8-byte aligned)
+        rsc.wt_at = (rsc.per_warp + 2 * ((size_t)rsc.wmax + 1) + 1) & ~(size_t)1;
+        rsc.per_warp = rsc.wt_at + 2 * ((size_t)rsc.wmax + 1);
+    }
     size_t warps = (size_t)wide * 8;
     const size_t budget_ints = (size_t)1 << 28;  // 1 GiB of refinement scratch at most
     while (warps >= 16 && warps * rsc.per_warp > budget_ints) warps /= 2;  // stays >= 8: a block's worth
@@ -2942,6 +3272,16 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     }
     if (p.metric == SHM_BUCKET_LCS) {  // no read is refined on chip under the bucket metrics
         k_refine_lcs<<<(unsigned)std::max<size_t>(1, warps / LCS_WARPS), LCS_WARPS * 32, 0, s>>>(v, rsc);
+        SHM_CUDA(cudaGetLastError());
+    } else if (v.P.rarity) {  // every candidate through the global path, with its rarity support
+        if (v.P.rw_score) {
+            S.r_mw.reserve((size_t)n);
+            v.r_mw = S.r_mw.p;
+            k_rarity_mw<<<grid_for((size_t)n, 128, 8), 128, 0, s>>>(v);
+            SHM_CUDA(cudaGetLastError());
+            count_launch();
+        }
+        k_refine_rarity<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, 0, s>>>(v, rsc);
         SHM_CUDA(cudaGetLastError());
     } else {
         if (p.metric != SHM_BUCKET_SH) {

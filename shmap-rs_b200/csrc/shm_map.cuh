@@ -27,6 +27,7 @@ struct BucketJob {
     int32_t is_cand, pad0;
     double score;                         // refinement result
     int32_t t_l, t_r, inter, same, s_sz, pad1;
+    double support;                       // rarity-weighted support of the scored window (0 without rarity)
 };
 
 struct MapScratch;  // grow-only device buffers owned by a context

@@ -127,6 +127,9 @@ int main(int argc, char** argv) {
         } else if (a == "-P" || a == "--no_bucket_pruning") p.no_bucket_pruning = 1;
         else if (a == "-B" || a == "--one_sweep") p.one_sweep = 1;
         else if (a == "-F" || a == "--abs_pos") p.abs_pos = 1;
+        else if (a == "--rarity-weight") p.rarity_weight = std::atof(val().c_str());
+        else if (a == "--rarity-tiebreak") p.rarity_tiebreak = std::atof(val().c_str());
+        else if (a == "--rarity-alpha") p.rarity_alpha = std::atof(val().c_str());
         else if (a == "--device") device = std::atoi(val().c_str());
         // index files (not flags of the reference): write the built index, or
         // start from one instead of -s (its k, -r and -M then apply)

@@ -55,7 +55,8 @@ class CParams(ctypes.Structure):
     _fields_ = [("k", ctypes.c_int32), ("h_frac", ctypes.c_double), ("max_matches", ctypes.c_int32),
                 ("theta", ctypes.c_double), ("min_diff", ctypes.c_double), ("max_overlap", ctypes.c_double),
                 ("metric", ctypes.c_int32), ("no_bucket_pruning", ctypes.c_int32), ("one_sweep", ctypes.c_int32),
-                ("abs_pos", ctypes.c_int32)]
+                ("abs_pos", ctypes.c_int32), ("rarity_weight", ctypes.c_double), ("rarity_tiebreak", ctypes.c_double),
+                ("rarity_alpha", ctypes.c_double)]
 
 
 class CServerConfig(ctypes.Structure):
@@ -108,6 +109,7 @@ def lib() -> ctypes.CDLL:
         "shm_index_segment": (ctypes.c_int, [P, P, i32, P, P, P, i64, P, ctypes.c_char_p, i32, P]),
         "shm_map_batch": (ctypes.c_int, [P, P, P, P, P, i32, P]),
         "shm_map_plain": (ctypes.c_int, [P, P, P, P, P, i32, P]),
+        "shm_map_multi": (ctypes.c_int, [P, P, i32, P, P, P, i32, P, P]),
         "shm_map_batch_device": (ctypes.c_int, [P, P, P, P, P, P, i32, P]),
         "shm_map_paf": (ctypes.c_int, [P, P, P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
         "shm_format_paf": (ctypes.c_int, [P, P, P, i32, ctypes.c_char_p, P, P, i64, P]),
@@ -161,13 +163,17 @@ class Params:
     no_bucket_pruning: bool = False
     one_sweep: bool = False
     abs_pos: bool = False
+    rarity_weight: float = 0.0
+    rarity_tiebreak: float = 0.0
+    rarity_alpha: float = 0.0
 
     def c(self) -> CParams:
         if self.metric not in METRICS:
             raise ValueError(f"metric {self.metric!r} is not on the device path")
         return CParams(self.k, self.h_frac, -1 if self.max_matches is None else self.max_matches, self.theta,
                        self.min_diff, self.max_overlap, METRICS[self.metric], int(self.no_bucket_pruning),
-                       int(self.one_sweep), int(self.abs_pos))
+                       int(self.one_sweep), int(self.abs_pos), self.rarity_weight, self.rarity_tiebreak,
+                       self.rarity_alpha)
 
     def validate(self) -> None:
         """Params::validate (src/params.rs:191-263); raises ShmError with the reference's message."""
@@ -510,6 +516,24 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+def map_reads_multi(indexes: Sequence["SketchIndex"], params: Params, seq: np.ndarray, offs: np.ndarray):
+    """shm_map_multi: the reads cut into contiguous shares, one per index
+    replica (each on its own context's device), mapped at the same time;
+    returns (records in read order, reads per share)."""
+    seq = np.ascontiguousarray(seq, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.int64)
+    n = len(offs) - 1
+    k = len(indexes)
+    ctxs = (ctypes.c_void_p * k)(*[ix.ctx.h.value if hasattr(ix.ctx.h, "value") else ix.ctx.h for ix in indexes])
+    idxs = (ctypes.c_void_p * k)(*[ix.h.value if hasattr(ix.h, "value") else ix.h for ix in indexes])
+    out = np.zeros(n, RECORD_DTYPE)
+    shares = np.zeros(k, np.int32)
+    cp = params.c()
+    _check(lib().shm_map_multi(ctxs, idxs, k, ctypes.byref(cp), _ptr(seq), _ptr(offs), n, _ptr(out),
+                               _ptr(shares)))
+    return out, shares
 
 
 def format_paf_device(index: "SketchIndex", params: Params, records: np.ndarray, names: Sequence[str],

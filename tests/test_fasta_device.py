@@ -2,8 +2,11 @@
 (shmap_b200.fasta.read_fastx, the reference's record rules, src/io/mod.rs:383-427):
 the same names, offsets and bases for files of random records, line breaks
 ('\\n', '\\r\\n', none at the end), blank lines, long lines across the parser's
-chunk boundaries and headers with spaces and tabs. FASTQ and text before the
-first header are refused (the host reader takes those). An index built from
+chunk boundaries and headers with spaces and tabs. FASTQ (a first byte '@')
+is parsed as four-line records by line index: quality lines starting with
+'@', CRLF, long reads across chunks, trailing blank lines. A FASTA file with
+'@' lines or text before the first header, and FASTQ that is not four-line
+records, are refused (the host reader takes those). An index built from
 the device copy equals the one built from host records, reads mapped from it
 get the same records, and the command line prints the same PAF either way."""
 import os
@@ -68,7 +71,9 @@ def test_edge_files(gpu_ctx, tmp_path, data):
     assert [seq[fa.offs[i]:fa.offs[i + 1]] for i in range(fa.n)] == [s for _, s in want]
 
 
-@pytest.mark.parametrize("data", [b"@q\nACGT\n+\nIIII\n", b">a\nAC\n@b\nGG\n", b"ACGT\n>a\nAC\n", b" \n>a\nA\n"])
+@pytest.mark.parametrize("data", [b">a\nAC\n@b\nGG\n", b"ACGT\n>a\nAC\n", b" \n>a\nA\n", b"@q\nACGT\n+\n",
+                                  b"@q\nACGT\nIIII\nIIII\n", b"@q\nAC\n+\nII\n\n@r\nGG\n+\nII\n",
+                                  b"@q\nAC\n+\nII\nr\nGG\n+\nII\n"])
 def test_refused_files(gpu_ctx, data):
     with pytest.raises(sb.ShmError) as e:
         sb.DeviceFasta(gpu_ctx, data)
@@ -112,3 +117,31 @@ def test_index_and_mapping_from_the_device_copy(gpu_ctx, tmp_path):
     host = subprocess.run(args + ["--host-fasta"], capture_output=True, text=True, timeout=300)
     assert dev.returncode == 0 and host.returncode == 0, dev.stderr + host.stderr
     assert strip_t(dev.stdout) == strip_t(host.stdout) and len(dev.stdout.splitlines()) > 400
+
+
+def _random_fastq(seed, n_rec, max_len, crlf=False):
+    rng = np.random.default_rng(seed)
+    nl = b"\r\n" if crlf else b"\n"
+    parts = []
+    for i in range(n_rec):
+        L = int(rng.integers(0, max_len + 1))
+        sq = bytes(rng.choice(np.frombuffer(b"ACGTNacgt", np.uint8), L))
+        qual = bytes(rng.choice(np.frombuffer(b"@!#IJ+>", np.uint8), L))  # quality lines may start with '@'
+        hdr = b"@r%d" % i + (b" extra\tx" if i % 3 == 0 else b"")
+        parts.append(hdr + nl + sq + nl + (b"+" if i % 2 else b"+" + hdr[1:]) + nl + qual)
+        if i + 1 < n_rec or i % 2:
+            parts.append(nl)
+    return b"".join(parts) + (b"\n\n" if seed % 2 else b"")
+
+
+@pytest.mark.parametrize("seed,n_rec,max_len,crlf", [(1, 1, 10, False), (2, 300, 3000, True), (3, 40, 60000, False),
+                                                     (4, 2000, 200, True), (5, 3, 0, False)])
+def test_fastq_records_as_the_host_reads_them(gpu_ctx, tmp_path, seed, n_rec, max_len, crlf):
+    data = _random_fastq(seed, n_rec, max_len, crlf)
+    want = _host(tmp_path, data)
+    assert len(want) == n_rec
+    fa = sb.DeviceFasta(gpu_ctx, data)
+    assert fa.n == n_rec and fa.names == [n for n, _ in want]
+    seq = fa.seq().tobytes()
+    assert [seq[fa.offs[i]:fa.offs[i + 1]] for i in range(fa.n)] == [s for _, s in want]
+    fa.close()
