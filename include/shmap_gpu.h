@@ -245,6 +245,23 @@ const char* shm_work_stat_name(int i);
 int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, double h_frac, int32_t offset,
                               uint64_t* d_h, uint32_t* d_rs, int64_t cap, int64_t* n_out, void* stream);
 
+/* No counterpart in the reference: the launch and batch shapes the project's
+ * autotuner measures (shmap_b200/autotune.py) instead of fixing them in the
+ * code: dev_batch_reads, dev_batch_bases, dev_first_batch_reads,
+ * host_batch_reads, host_batch_bases, host_first_batch_reads,
+ * sketch_ctas_per_sm, wide_ctas_per_sm, refine_warps_per_sm. None of them
+ * changes a result. They are read once per process from the file named by
+ * $SHMAP_TUNING, else tuning.conf in the directory above the library's
+ * (key = value lines, '#' comments), else built-in defaults;
+ * shm_tuning_set changes one for later calls, shm_tuning_load (path NULL =
+ * the default place) reads a file again, shm_tuning_source names where the
+ * settings came from. Unknown keys and values out of range are
+ * SHM_ERR_INVALID. */
+int shm_tuning_get(const char* key, int64_t* value);
+int shm_tuning_set(const char* key, int64_t value);
+int shm_tuning_load(const char* path);
+const char* shm_tuning_source(void);
+
 /* FASTA parsed on the device: the reference reads its inputs with
  * needletail (src/io/mod.rs:383-427, src/index.rs:384-393). The file's bytes
  * (host memory) go up once and are parsed on ctx's device: a record per '>'

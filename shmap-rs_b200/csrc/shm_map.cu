@@ -52,6 +52,7 @@
 #include "shm_common.cuh"
 #include "shm_map.cuh"
 #include "shm_pack.cuh"
+#include "shm_tune.hpp"
 #include "shm_paf.hpp"
 #include "../host/pack.hpp"
 #include "shm_prims.cuh"
@@ -3196,7 +3197,9 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         half_max = p.abs_pos ? (uint32_t)bp.max_len : (uint32_t)bp.max_cap;
     }
     sl.job_cap = job_cap;
-    const int wide = grid_for((size_t)1 << 40, 256, 8);  // a full grid for kernels that read their counts on the device
+    const Tuning tu = tuning();
+    // a full grid for kernels that read their counts on the device
+    const int wide = grid_for((size_t)1 << 40, 256, (int)tu.wide_ctas_per_sm);
 
     H.mark("sizes");
     S.bt.reserve(bt_slots_alloc + 1);
@@ -3250,7 +3253,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         rsc.wt_at = (rsc.per_warp + 2 * ((size_t)rsc.wmax + 1) + 1) & ~(size_t)1;
         rsc.per_warp = rsc.wt_at + 2 * ((size_t)rsc.wmax + 1);
     }
-    size_t warps = (size_t)wide * 8;
+    size_t warps = (size_t)grid_for((size_t)1 << 40, 1, (int)tu.refine_warps_per_sm);  // SMs x warps per SM
     const size_t budget_ints = (size_t)1 << 28;  // 1 GiB of refinement scratch at most
     while (warps >= 16 && warps * rsc.per_warp > budget_ints) warps /= 2;  // stays >= 8: a block's worth
     S.ref_scr.reserve(warps * rsc.per_warp);
@@ -3324,16 +3327,11 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
 
 // Batch limits: device-resident reads in few large batches; host reads in
 // smaller ones so that copying batch b+1 overlaps mapping batch b.
-static const int64_t DEV_BATCH_BASES = (int64_t)1 << 31;
-static const int32_t DEV_BATCH_READS = 1 << 17;
-// The first batch of a device-resident call is small, so the device starts
-// while the host plans the next batch (planning costs ~5 ns a read).
-static const int32_t DEV_FIRST_BATCH_READS = 1 << 14;
-static const int64_t HOST_BATCH_BASES = (int64_t)1 << 28;
-static const int32_t HOST_BATCH_READS = 1 << 15;
-// The first batch of a host-buffer call is small: its packing on the host is
-// the part of the call that nothing overlaps.
-static const int32_t HOST_FIRST_BATCH_READS = 1 << 12;
+// Batch sizes come from the measured settings (shm_tune.hpp): device-resident
+// calls cut batches of dev_batch_reads / dev_batch_bases, the first of them
+// smaller (dev_first_batch_reads) so the device starts while the host plans
+// the next (about 5 ns a read); calls from host buffers cut host_batch_*, the
+// first small too, since its packing on the host is what nothing overlaps.
 
 __global__ void k_scatter_records(const shm_map_record* __restrict__ src, const int32_t* __restrict__ idx, int32_t n,
                                   shm_map_record* __restrict__ dst) {
@@ -3487,7 +3485,9 @@ static std::vector<uint8_t*> plan_blocks(MapCtx* c, const std::vector<std::pair<
 void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq, const int64_t* h_offs,
                 int32_t n, shm_map_record* d_out, bool plain) {
     SHM_CUDA(cudaSetDevice(c->device));
-    const auto batches = cut_batches(h_offs, n, plain, DEV_BATCH_READS, DEV_BATCH_BASES, DEV_FIRST_BATCH_READS);
+    const Tuning tu = tuning();
+    const auto batches = cut_batches(h_offs, n, plain, (int32_t)tu.dev_batch_reads, tu.dev_batch_bases,
+                                     (int32_t)tu.dev_first_batch_reads);
     std::vector<BatchSlot> slots = batch_slots(c, batches, h_offs);
     const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
@@ -3526,7 +3526,8 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     MapScratch& S = *c->scr;
     cudaStream_t s = c->stream;
     const auto batches =
-        cut_batches(offs, n, plain, HOST_BATCH_READS, HOST_BATCH_BASES, HOST_FIRST_BATCH_READS, true);
+        cut_batches(offs, n, plain, (int32_t)tuning().host_batch_reads, tuning().host_batch_bases,
+                    (int32_t)tuning().host_first_batch_reads, true);
     int64_t max_nb = 0;
     int32_t max_n = 0;
     for (auto [i, j] : batches) {

@@ -12,6 +12,7 @@
 #include "shm_common.cuh"
 #include "shm_prims.cuh"
 #include "shm_sketch.cuh"
+#include "shm_tune.hpp"
 
 #include <cstdlib>
 #include <mutex>
@@ -693,7 +694,7 @@ void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStrea
     static const bool letters = std::getenv("SHMAP_SKETCH_LETTERS") != nullptr;
     if (pk && !letters) {
         const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
-        k_sketch_pk<SK_APPEND><<<grid_for(n_tiles, 1, 8), SK_THREADS, 0, s>>>(a, L);
+        k_sketch_pk<SK_APPEND><<<grid_for(n_tiles, 1, (int)tuning().sketch_ctas_per_sm), SK_THREADS, 0, s>>>(a, L);
         SHM_CUDA(cudaGetLastError());
         count_launch();
         return;

@@ -103,6 +103,10 @@ def lib() -> ctypes.CDLL:
         "shm_index_load": (ctypes.c_int, [P, ctypes.c_char_p, P]),
         "shm_index_info": (ctypes.c_int, [P, P, P, P]),
         "shm_index_file_check": (ctypes.c_int, [ctypes.c_char_p]),
+        "shm_tuning_get": (ctypes.c_int, [ctypes.c_char_p, P]),
+        "shm_tuning_set": (ctypes.c_int, [ctypes.c_char_p, i64]),
+        "shm_tuning_load": (ctypes.c_int, [ctypes.c_char_p]),
+        "shm_tuning_source": (ctypes.c_char_p, []),
         "shm_index_stats_get": (ctypes.c_int, [P, P]),
         "shm_index_count": (ctypes.c_int, [P, P, P, i64, P]),
         "shm_index_hits": (ctypes.c_int, [P, P, u64, P, P, P, P, i64, P]),

@@ -1,0 +1,83 @@
+"""The measured launch and batch shapes (shm_tuning_*): every setting reads
+back what was set, values out of range and unknown keys are refused, a
+settings file is read with its comments and refused (nothing changed) when a
+line is malformed. The settings change how work is cut, never a result: the
+GPU test maps one read set under very different settings and compares."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import shmap_b200 as sb
+
+KEYS = ["dev_batch_reads", "dev_batch_bases", "dev_first_batch_reads", "host_batch_reads", "host_batch_bases",
+        "host_first_batch_reads", "sketch_ctas_per_sm", "wide_ctas_per_sm", "refine_warps_per_sm"]
+
+
+def _get(k):
+    v = ctypes.c_int64()
+    assert sb.lib().shm_tuning_get(k.encode(), ctypes.byref(v)) == 0
+    return v.value
+
+
+@pytest.fixture
+def saved():
+    before = {k: _get(k) for k in KEYS}
+    yield before
+    for k, v in before.items():
+        assert sb.lib().shm_tuning_set(k.encode(), v) == 0
+
+
+def test_get_set_and_ranges(saved):
+    L = sb.lib()
+    assert all(v > 0 for v in saved.values())
+    assert L.shm_tuning_set(b"sketch_ctas_per_sm", 3) == 0 and _get("sketch_ctas_per_sm") == 3
+    assert L.shm_tuning_set(b"sketch_ctas_per_sm", 0) == sb.SHM_ERR_INVALID
+    assert L.shm_tuning_set(b"sketch_ctas_per_sm", 99) == sb.SHM_ERR_INVALID
+    assert _get("sketch_ctas_per_sm") == 3
+    assert L.shm_tuning_set(b"no_such_knob", 1) == sb.SHM_ERR_INVALID
+    assert b"unknown tuning setting" in L.shm_last_error()
+    assert isinstance(L.shm_tuning_source(), bytes)
+
+
+def test_settings_file(saved, tmp_path):
+    L = sb.lib()
+    good = tmp_path / "t.conf"
+    good.write_text("# measured\nwide_ctas_per_sm = 4   # contrib\n\nhost_batch_reads=20000\n")
+    assert L.shm_tuning_load(str(good).encode()) == 0
+    assert _get("wide_ctas_per_sm") == 4 and _get("host_batch_reads") == 20000
+    assert L.shm_tuning_source() == str(good).encode()
+    bad = tmp_path / "b.conf"
+    bad.write_text("wide_ctas_per_sm = 2\nbogus line\n")
+    assert L.shm_tuning_load(str(bad).encode()) == sb.SHM_ERR_INVALID
+    assert b"not a 'key = value' line" in L.shm_last_error()
+    assert _get("wide_ctas_per_sm") == 4  # nothing of a refused file applies
+    (tmp_path / "c.conf").write_text("refine_warps_per_sm = 1000\n")
+    assert L.shm_tuning_load(str(tmp_path / "c.conf").encode()) == sb.SHM_ERR_INVALID
+
+
+@pytest.mark.gpu
+def test_results_do_not_depend_on_the_settings(gpu_ctx, saved):
+    from helpers import record_mismatches
+    from shmap_b200 import synth
+
+    gen = synth.Genome(synth.REFS["uniform5m"])
+    names, seq, offs = gen.reads(synth.READS["fixed10k"])
+    g = sb.SketchIndex.from_records(gpu_ctx, gen.records(), 25, 0.01)
+    p = sb.Params(k=25, h_frac=0.01, theta=0.4)
+    want = g.map_reads(p, seq, offs)
+    L = sb.lib()
+    for k, v in [("dev_batch_reads", 1024), ("dev_first_batch_reads", 64), ("host_batch_reads", 1024),
+                 ("host_first_batch_reads", 100), ("sketch_ctas_per_sm", 1), ("wide_ctas_per_sm", 1),
+                 ("refine_warps_per_sm", 8)]:
+        assert L.shm_tuning_set(k.encode(), v) == 0
+    got = g.map_reads(p, seq, offs)
+    assert not record_mismatches(got, want)
+    import torch
+
+    d_seq = torch.zeros(len(seq) + 32, dtype=torch.uint8, device="cuda")
+    d_seq[: len(seq)].copy_(torch.from_numpy(np.ascontiguousarray(seq)))
+    d_out = torch.empty(len(names) * sb.RECORD_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    g.map_reads_device(p, d_seq.data_ptr(), offs, d_out.data_ptr())
+    torch.cuda.synchronize()
+    assert not record_mismatches(d_out.cpu().numpy().view(sb.RECORD_DTYPE), want)
