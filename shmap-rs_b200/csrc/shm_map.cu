@@ -60,12 +60,25 @@
 
 namespace shm {
 
+// Candidates refined through the global tables are taken from a queue in
+// cost order, the dearest first (a warp's cost grows with the window region,
+// twice the bucket half-length): half-lengths above FAR_EDGE0, above
+// FAR_EDGE1, the rest.
+constexpr int FAR_BINS = 3;
+constexpr int32_t FAR_EDGE0 = 1024, FAR_EDGE1 = 512;
+__host__ __device__ __forceinline__ int far_bin_of(int32_t half) {
+    return half > FAR_EDGE0 ? 0 : (half > FAR_EDGE1 ? 1 : 2);
+}
+
 struct BatchMax {
     unsigned int m_max, nu_max, half_max, n_overflow;
     unsigned long long kmers, distinct, proc_seeds, hits, buckets, ext_seeds, refine_kmers;
     unsigned int refine_next;  // next candidate chunk k_refine_chip takes
     unsigned int n_far;        // candidates refined by k_refine (listed in cfar)
     unsigned int lcs_next;     // next candidate k_refine takes under bucket_LCS
+    unsigned int far_bin[FAR_BINS];  // candidates of cfar by cost bin (their read's bucket half-length)
+    unsigned int far_cur[FAR_BINS];  // placing them, binned, into cfar_q
+    unsigned int far_next;           // next candidate of cfar_q a refinement warp takes
 };
 
 // Small device-to-host reads of a batch, landing in pinned memory.
@@ -112,7 +125,8 @@ struct BatchView {
     uint32_t* n_jobs;
     uint32_t job_cap;
     uint32_t *ccnt, *coff, *ccur, *cidx;
-    uint32_t* cfar;  // the jobs of the candidates not refined on chip (mx->n_far of them)
+    uint32_t* cfar;    // the jobs of the candidates not refined on chip (mx->n_far of them)
+    uint32_t* cfar_q;  // the same jobs by cost bin, dearest bin first: the refinement queue
     uint32_t* ovf_list;
     BatchMax* mx;
     shm_map_record* out;
@@ -1310,8 +1324,49 @@ __global__ void k_cidx(BatchView v) {
             if (lane == leader) at = atomicAdd(&v.mx->n_far, (uint32_t)__popc(fm));
             at = __shfl_sync(0xffffffffu, at, leader);
             if (far) v.cfar[at + __popc(fm & ((1u << lane) - 1u))] = ji;
+            const int bin = far ? far_bin_of(v.r_half[v.jobs[ji].read]) : -1;
+#pragma unroll
+            for (int b2 = 0; b2 < FAR_BINS; b2++) {
+                const unsigned bm = __ballot_sync(0xffffffffu, bin == b2);
+                if (bm && lane == __ffs(bm) - 1) atomicAdd(&v.mx->far_bin[b2], (uint32_t)__popc(bm));
+            }
         }
     }
+}
+
+// The refinement queue: cfar's candidates placed by cost bin, the dearest
+// bin first, so the longest refinements start first and the short ones fill
+// the end (within a bin, in any order).
+__global__ void k_far_bins(BatchView v) {
+    const uint32_t nfar = v.mx->n_far;
+    const int lane = threadIdx.x & 31;
+    uint32_t base[FAR_BINS];
+    base[0] = 0;
+    for (int b = 1; b < FAR_BINS; b++) base[b] = base[b - 1] + v.mx->far_bin[b - 1];
+    for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < nfar; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + (uint32_t)lane;
+        const uint32_t ji = i < nfar ? v.cfar[i] : 0u;
+        const int bin = i < nfar ? far_bin_of(v.r_half[v.jobs[ji].read]) : -1;
+#pragma unroll
+        for (int b = 0; b < FAR_BINS; b++) {
+            const unsigned bm = __ballot_sync(0xffffffffu, bin == b);
+            if (!bm) continue;
+            const int leader = __ffs(bm) - 1;
+            uint32_t at = 0;
+            if (lane == leader) at = atomicAdd(&v.mx->far_cur[b], (uint32_t)__popc(bm));
+            at = __shfl_sync(0xffffffffu, at, leader);
+            if (bin == b) v.cfar_q[base[b] + at + __popc(bm & ((1u << lane) - 1u))] = ji;
+        }
+    }
+}
+
+// The next candidate of the refinement queue for this warp (UINT32_MAX when
+// the queue is empty).
+__device__ __forceinline__ uint32_t next_far(const BatchView& v, int lane) {
+    uint32_t ci = 0;
+    if (lane == 0) ci = atomicAdd(&v.mx->far_next, 1u);
+    ci = __shfl_sync(0xffffffffu, ci, 0);
+    return ci < v.mx->n_far ? v.cfar_q[ci] : UINT32_MAX;
 }
 
 // ------------------------------------------------------------------ K7 refinement
@@ -1765,8 +1820,10 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
     int32_t* const D = cntA + rsc.nu_max;
     int32_t* const PC = D + rsc.wmax + 1;
     int32_t* const ring = PC + rsc.wmax + 1;
-    for (uint32_t ci = wid; ci < nfar; ci += nwarps) {
-        BucketJob* J = v.jobs + v.cfar[ci];
+    (void)nfar;
+    (void)nwarps;
+    for (uint32_t jq; (jq = next_far(v, lane)) != UINT32_MAX;) {
+        BucketJob* J = v.jobs + jq;
         const int32_t q = J->read;
         if (v.P.metric == MET_BUCKET_SH) {  // bucket_SH (scoring.rs:311-325)
             if (lane == 0) {
@@ -2052,10 +2109,11 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine_rarity(BatchVie
     R.nxt = R.ring + rsc.ring_n;
     R.flag = R.nxt + rsc.wmax + 1;
     R.wt = (double*)(base + rsc.wt_at);
-    for (uint32_t ci = wid; ci < nfar; ci += nwarps) {
-        BucketJob* J = v.jobs + v.cfar[ci];
-        const int32_t q = J->read;
-        refine_rarity_one(v, J, q, R, lane, lt);
+    (void)nfar;
+    (void)nwarps;
+    for (uint32_t jq; (jq = next_far(v, lane)) != UINT32_MAX;) {
+        BucketJob* J = v.jobs + jq;
+        refine_rarity_one(v, J, J->read, R, lane, lt);
         __syncwarp();
     }
 }
@@ -2656,7 +2714,7 @@ struct MapScratch {
     DevBuf<uint32_t> dpk_codes, dpk_mask;      // device-resident batches, packed on the device
     DevBuf<uint64_t> sd_h;
     DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
-        cidx, cfar, sort_scr, ovf_list, r_flags;
+        cidx, cfar, cfar_q, sort_scr, ovf_list, r_flags;
     DevBuf<uint32_t> lcs_pos, lcs_cnt;  // bucket_LCS only
     DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
@@ -3239,9 +3297,14 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     H.mark("cidx_res");
     v.cidx = S.cidx.p;
     v.cfar = S.cfar.p;
+    S.cfar_q.reserve((size_t)job_cap + 1);
+    v.cfar_q = S.cfar_q.p;
     T.begin(STG_AUX);
     k_cidx<<<wide, 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
+    k_far_bins<<<wide, 256, 0, s>>>(v);
+    SHM_CUDA(cudaGetLastError());
+    count_launch();
     T.end();
 
     RefScratch rsc{};
