@@ -1616,11 +1616,13 @@ __device__ __forceinline__ void lcs_one(const BatchView& v, BucketJob* J, int32_
 }
 
 // One candidate window (best_fixed_length, src/shmap/scoring.rs:189-291).
-// cntA (per seed: occurrences seen) and ring (per seed: positions of its last
-// occs occurrences) come from the warp's shared slice when the read is small
-// enough, else from its global scratch; D and PC always from global scratch.
-__device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int32_t q, int32_t* cntA, int32_t* D,
-                                           int32_t* PC, int32_t* ring, int lane, unsigned lt) {
+// cntA (per seed: occurrences seen), ring (per seed: positions of its last
+// occs occurrences), the difference array D and the strand prefix PC come
+// from the warp's shared slice when the read is small enough (16-bit counts,
+// positions and prefix: all below 2^15 there), else from its global scratch.
+template <class CT, class PT>
+__device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int32_t q, CT* cntA, int32_t* D, PT* PC,
+                                           CT* ring, int lane, unsigned lt) {
     const bool ap = v.P.ap != 0;
     const DevIndex& I = v.I;
     const int32_t m = v.r_m[q], n_u = v.r_nu[q];
@@ -1674,7 +1676,7 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
             {
                 const int32_t cv = (valid && s >= 0) ? (((os & 1u) == (rs & 1u)) ? 1 : -1) : 0;
                 const int32_t inc = warp_inclusive_scan(cv);
-                if (valid) PC[x + 1] = pc_carry + inc;
+                if (valid) PC[x + 1] = (PT)(pc_carry + inc);
                 pc_carry += __shfl_sync(0xffffffffu, inc, 31);
             }
             const unsigned peers = __match_any_sync(0xffffffffu, s);
@@ -1684,14 +1686,14 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
                 occ = (int32_t)(os >> 1);
                 rho = __popc(peers & lt);
                 gsz = __popc(peers);
-                t = cntA[s] + rho;
+                t = (int32_t)cntA[s] + rho;
                 int32_t p = -1;  // position (relative) of the occ-th previous occurrence, -1 = none
                 // (positions, r and m are below 2^31: 32-bit arithmetic throughout)
                 if (t >= occ) {
                     if (rho >= occ)  // in this chunk: the peer occ places before this lane
                         p = c0 + (occ == 1 ? 31 - __clz(peers & lt) : (int32_t)__fns(peers, 0, rho - occ + 1));
                     else
-                        p = ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
+                        p = (int32_t)ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))];
                 }
                 int32_t Lj;
                 if (!ap) {
@@ -1718,8 +1720,8 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
             }
             __syncwarp();
             if (s >= 0) {
-                if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = x;
-                if (rho == gsz - 1) cntA[s] = t + 1;
+                if (rho >= gsz - occ) ring[ooff + (occ == 1 ? 0u : (uint32_t)(t % occ))] = (CT)x;
+                if (rho == gsz - 1) cntA[s] = (CT)(t + 1);
             }
             __syncwarp();
         }
@@ -1768,7 +1770,7 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
             if (better) {
                 bl = x;
                 bI = I_;
-                bS = PC[r] - PC[x];
+                bS = (int32_t)PC[r] - (int32_t)PC[x];
                 br = r;
             }
         }
@@ -1805,23 +1807,34 @@ __device__ __forceinline__ void refine_one(const BatchView& v, BucketJob* J, int
     }
 }
 
-// Shared slices for the per-seed state of reads with m <= REFINE_SM: the
-// counts and rings are read back within a chunk's dependent chain, so they
-// are kept on chip; the difference array and the strand prefix stay global.
-constexpr int REFINE_SM = 512;
+// Each warp's shared slice (REFINE_SLICE bytes, 16-bit counts, positions and
+// strand prefix) holds, for reads of at most REFINE_SM k-mers whose window
+// region has at most 2 REFINE_SM + 2 k-mers, all of a candidate's state: the
+// rings and counts, the difference array and the strand prefix, so only the
+// reference k-mers, the probe table and the seed records come from global
+// memory. For larger reads (up to REFINE_SLICE / 4 k-mers) it holds the
+// rings and counts, and the rest stays in the warp's global scratch; the
+// largest reads keep everything there. Four CTAs of REFINE_WARPS warps fit
+// an SM.
+constexpr int REFINE_SM = 384;
+constexpr int REFINE_WA = 2 * REFINE_SM + 2;  // window positions of the all-on-chip layout
+constexpr size_t REFINE_OFF_CNT = 2 * (size_t)REFINE_SM;
+constexpr size_t REFINE_OFF_D = 4 * (size_t)REFINE_SM;
+constexpr size_t REFINE_OFF_PC = REFINE_OFF_D + 4 * (size_t)REFINE_WA;
+constexpr size_t REFINE_SLICE = (REFINE_OFF_PC + 2 * (size_t)REFINE_WA + 15) / 16 * 16;
+static_assert(REFINE_OFF_D % 4 == 0 && REFINE_OFF_PC % 2 == 0, "slice alignment");
+static_assert(REFINE_WARPS * REFINE_SLICE * 4 + 4 * 1024 <= 228 * 1024, "four CTAs per SM");
 
 __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, RefScratch rsc) {
-    __shared__ int32_t s_cnt[REFINE_WARPS][REFINE_SM], s_ring[REFINE_WARPS][REFINE_SM];
+    extern __shared__ __align__(16) uint8_t rf_dyn[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t nfar = v.mx->n_far;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int32_t* const cntA = rsc.base + (size_t)wid * rsc.per_warp;
     int32_t* const D = cntA + rsc.nu_max;
     int32_t* const PC = D + rsc.wmax + 1;
     int32_t* const ring = PC + rsc.wmax + 1;
-    (void)nfar;
-    (void)nwarps;
+    uint8_t* const slice = rf_dyn + (size_t)wib * REFINE_SLICE;
     for (uint32_t jq; (jq = next_far(v, lane)) != UINT32_MAX;) {
         BucketJob* J = v.jobs + jq;
         const int32_t q = J->read;
@@ -1836,10 +1849,19 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
             }
             continue;
         }
-        if (v.r_m[q] <= REFINE_SM)  // then n_u <= m and the rings hold m positions
-            refine_one(v, J, q, s_cnt[wib], D, PC, s_ring[wib], lane, lt);
+        // the candidate's window region (as refine_one forms it): its size picks the layout
+        const int32_t m = v.r_m[q];
+        const int64_t h = v.r_half[q];
+        const int64_t seglen = (int64_t)(__ldg(v.I.seg_off + J->seg + 1) - __ldg(v.I.seg_off + J->seg));
+        const int64_t W = min(((int64_t)J->bb + 2) * h, seglen) - (int64_t)J->bb * h;
+        if (m <= REFINE_SM && W <= REFINE_WA - 1)  // n_u <= m: counts and rings fit
+            refine_one<uint16_t, int16_t>(v, J, q, (uint16_t*)(slice + REFINE_OFF_CNT), (int32_t*)(slice + REFINE_OFF_D),
+                                          (int16_t*)(slice + REFINE_OFF_PC), (uint16_t*)slice, lane, lt);
+        else if (4 * (size_t)m <= REFINE_SLICE && W < 32768)
+            refine_one<uint16_t, int32_t>(v, J, q, (uint16_t*)(slice + 2 * (size_t)m), D, PC, (uint16_t*)slice, lane,
+                                          lt);
         else
-            refine_one(v, J, q, cntA, D, PC, ring, lane, lt);
+            refine_one<int32_t, int32_t>(v, J, q, cntA, D, PC, ring, lane, lt);
         __syncwarp();
     }
 }
@@ -3356,7 +3378,13 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
             SHM_CUDA(cudaGetLastError());
             count_launch();
         }
-        k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, 0, s>>>(v, rsc);
+        if (!c->refine_smem_set) {
+            SHM_CUDA(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)(REFINE_WARPS * REFINE_SLICE)));
+            c->refine_smem_set = 1;
+        }
+        k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, REFINE_WARPS * REFINE_SLICE,
+                   s>>>(v, rsc);
         SHM_CUDA(cudaGetLastError());
     }
     T.end();

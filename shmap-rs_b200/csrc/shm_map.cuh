@@ -68,6 +68,7 @@ struct MapCtx {
     int64_t work[16] = {};
     int seed_smem_set = 0;   // dynamic shared memory the seed kernels have been allowed so far
     int rchip_smem_set = 0;  // k_refine_chip's dynamic shared memory allowed
+    int refine_smem_set = 0; // k_refine's
     int seedc_smem_set = 0;
     // stage timing
     bool timing = false;
