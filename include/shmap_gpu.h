@@ -268,11 +268,13 @@ const char* shm_tuning_source(void);
  * header line, its name the header up to the first space or tab, its
  * sequence its lines joined without '\n' and without one '\r' before a line's
  * end. A file whose first byte is '@' is FASTQ: records of four lines ('@'
- * header, sequence, '+' line, quality; blank lines only at the file's end).
+ * header, sequence, '+' line, quality; blank lines only at the file's end,
+ * which are dropped, so a last record may lack its empty quality line).
  * The sequences stay in device memory, for shm_index_build_fasta and
  * shm_map_fasta. A FASTA file with a line starting with '@' or text before the
- * first header, and a FASTQ file whose lines do not make four-line records,
- * are refused with SHM_ERR_INVALID: read those on the host. */
+ * first header, and a FASTQ file whose line 4r does not start with '@' or
+ * line 4r+2 with '+', are refused with SHM_ERR_INVALID: read those on the
+ * host. */
 typedef struct shm_fasta shm_fasta;
 int shm_fasta_parse_device(shm_ctx* ctx, const uint8_t* file, int64_t len, shm_fasta** out);
 /* n records; offs (n+1 entries) and names ('\n'-joined) stay owned by fa. */

@@ -325,9 +325,11 @@ __global__ void k_fa_name_write(FaView v, const int64_t* __restrict__ hdr_pos, i
 // header, sequence, '+' line, quality. A byte's role follows from the index
 // of its line, counted from the file's start: the lines are counted per
 // chunk, scanned over the chunks, and within a chunk over the threads' runs.
-// A line 4r must start with '@' and a line 4r+2 with '+', and the lines must
-// make whole records (blank lines at the file's end aside): else the file is
-// refused and read on the host.
+// A line 4r must start with '@' and a line 4r+2 with '+' (when not empty),
+// else the file is refused and read on the host. Blank lines at the file's
+// end are dropped first; a last record left without its quality (it was
+// empty) or its '+' line reads as the host reader reads it: an empty or
+// missing line.
 enum : uint32_t { FQ_BAD = 4u };
 
 // Pass 1: newlines per chunk.
@@ -508,7 +510,8 @@ FastaDev* fasta_parse_device(int device, cudaStream_t s, const uint8_t* file, in
             SHM_CUDA(cudaMemcpyAsync(&n_rec, hdr_off.p + nc, sizeof n_rec, cudaMemcpyDeviceToHost, s));
             SHM_CUDA(cudaMemcpyAsync(&fl, flags.p, sizeof fl, cudaMemcpyDeviceToHost, s));
             SHM_CUDA(cudaStreamSynchronize(s));
-            if ((fl & FQ_BAD) || (lines + 1) % 4 != 0) {  // the last line (the quality) ends the file
+            (void)lines;  // a last record may end early (an empty quality line looks like a trailing blank)
+            if (fl & FQ_BAD) {
                 *why = "not FASTQ records of four lines";
                 delete F;
                 return nullptr;

@@ -86,6 +86,7 @@ struct HostReads {
     uint64_t totals[2];  // hit words, bucket-table slots
     BatchMax hm;         // after seed preparation
     uint32_t nj, nc;     // bucket jobs, candidates
+    uint32_t nbk;        // distinct buckets of every read (synchronous sizing)
     BatchMax fin;        // after the sweep
 };
 
@@ -120,6 +121,8 @@ struct BatchView {
     BSlot* bt;
     uint32_t* bt_list;  // per read, the slots of its distinct buckets (r_seeded[q] of them)
     uint64_t bt_cap;    // most slots a read's bucket table gets (a power of two >= 16)
+    uint64_t* r_eb;     // per read: the bound on its distinct buckets (0 until its seeds are prepared)
+    uint64_t ext_total; // reference k-mers (bases under -F): a read's buckets are at most ext_total / half + 2 n_seg + 2
     uint32_t* r_flags;  // per read: nonzero when its bucket table passed its load limit
     BucketJob* jobs;
     uint32_t* n_jobs;
@@ -265,6 +268,13 @@ __device__ __forceinline__ uint64_t seed_bucket_bound(const BatchView& v, uint32
 // (a power of two, at least 16), capped at v.bt_cap. A capped table that
 // fills past its load limit marks the read, which is then mapped again with
 // the full bound.
+// The bound on a read's distinct buckets, no more than the genome has for
+// its half-length (every bucket b of a segment of e k-mers has b <= (e-1)/h).
+__device__ __forceinline__ uint64_t genome_bucket_cap(const BatchView& v, uint64_t ebound, int64_t h) {
+    const uint64_t cap = v.ext_total / (uint64_t)max(h, (int64_t)1) + 2ULL * (uint64_t)v.I.n_seg + 2ULL;
+    return min(ebound, cap);
+}
+
 __device__ __forceinline__ uint64_t bt_slots(const BatchView& v, uint64_t ebound) {
     return min(max((uint64_t)16, pow2_ceil(2 * ebound)), v.bt_cap);
 }
@@ -449,7 +459,9 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
             v.r_status[q] = ST_OVERFLOW;
         } else {
             v.hw[q] = smatch;
-            v.bt_size[q] = smatch ? bt_slots(v, ebound) : 0;
+            const uint64_t eb = genome_bucket_cap(v, ebound, halflen);
+            v.r_eb[q] = eb;
+            v.bt_size[q] = smatch ? bt_slots(v, eb) : 0;
         }
         atomicMax(&v.mx->m_max, m);
         atomicMax(&v.mx->nu_max, n_u);
@@ -868,7 +880,9 @@ __device__ void seedprep_count(const BatchView& v, int32_t q, uint32_t C, uint8_
             v.r_status[q] = ST_OVERFLOW;
         } else {
             v.hw[q] = l_sm;
-            v.bt_size[q] = l_sm ? bt_slots(v, l_eb) : 0;
+            const uint64_t eb = genome_bucket_cap(v, l_eb, halflen);
+            v.r_eb[q] = eb;
+            v.bt_size[q] = l_sm ? bt_slots(v, eb) : 0;
         }
         atomicMax(&v.mx->m_max, m);
         atomicMax(&v.mx->nu_max, n_u);
@@ -2632,8 +2646,11 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
                 }
             } else if (st == ST_OVERFLOW) {
                 uint32_t k = atomicAdd(&v.mx->n_overflow, 1u);
-                v.ovf_list[2 * (size_t)k] = (uint32_t)q;
-                v.ovf_list[2 * (size_t)k + 1] = v.kcnt[q];
+                const uint64_t eb = v.r_eb[q];
+                v.ovf_list[4 * (size_t)k] = (uint32_t)q;
+                v.ovf_list[4 * (size_t)k + 1] = v.kcnt[q];
+                v.ovf_list[4 * (size_t)k + 2] = (uint32_t)eb;
+                v.ovf_list[4 * (size_t)k + 3] = (uint32_t)(eb >> 32);
             }
             v.out[q] = rec;
         }
@@ -2740,6 +2757,7 @@ struct MapScratch {
     DevBuf<uint32_t> lcs_pos, lcs_cnt;  // bucket_LCS only
     DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
+    DevBuf<uint64_t> r_eb;
     DevBuf<BSlot> bt;
     DevBuf<uint32_t> bt_list;
     DevBuf<BucketJob> jobs;
@@ -2891,7 +2909,8 @@ static void plan_batch(uint8_t* h_plan, const int64_t* h_offs, int32_t n, int32_
 // A read that overflowed a capacity, with its sketch size.
 struct Overflow {
     int32_t read;
-    uint32_t m;
+    uint32_t m;   // its counted k-mers (the capacity it is mapped again with)
+    uint64_t eb;  // the bound on its distinct buckets (0: its seeds were not prepared)
 };
 
 // Where a batch's results land on the host (pinned): the small reads, then
@@ -2925,7 +2944,7 @@ static uint32_t fast_job_cap(int32_t n) {
 static std::vector<BatchSlot> batch_slots(MapCtx* c, const std::vector<std::pair<int32_t, int32_t>>& b,
                                           const int64_t* offs) {
     size_t bytes = 0;
-    for (auto [i, j] : b) bytes += (sizeof(HostReads) + 63) / 64 * 64 + (8 * (size_t)(j - i) + 63) / 64 * 64;
+    for (auto [i, j] : b) bytes += (sizeof(HostReads) + 63) / 64 * 64 + (16 * (size_t)(j - i) + 63) / 64 * 64;
     if (bytes > c->h_slots_cap) {
         if (c->h_slots) SHM_CUDA(cudaFreeHost(c->h_slots));
         c->h_slots = nullptr;
@@ -2941,7 +2960,7 @@ static std::vector<BatchSlot> batch_slots(MapCtx* c, const std::vector<std::pair
         sl.R = (HostReads*)at;
         at += (sizeof(HostReads) + 63) / 64 * 64;
         sl.ovf = (uint32_t*)at;
-        at += (8 * (size_t)(j - i) + 63) / 64 * 64;
+        at += (16 * (size_t)(j - i) + 63) / 64 * 64;
         sl.i0 = i;
         sl.n = j - i;
         sl.bases = offs[j] - offs[i];
@@ -2968,7 +2987,8 @@ static void collect_batch(MapCtx* c, const BatchSlot& sl, std::vector<Overflow>&
     c->work[W_REFINE_KMERS] += (int64_t)fin.refine_kmers;
     const size_t at = ovf.size();
     for (uint32_t i = 0; i < fin.n_overflow && i < (uint32_t)sl.n; i++)
-        ovf.push_back(Overflow{sl.i0 + (int32_t)sl.ovf[2 * i], sl.ovf[2 * i + 1]});
+        ovf.push_back(Overflow{sl.i0 + (int32_t)sl.ovf[4 * i], sl.ovf[4 * i + 1],
+                               (uint64_t)sl.ovf[4 * i + 2] | ((uint64_t)sl.ovf[4 * i + 3] << 32)});
     std::sort(ovf.begin() + at, ovf.end(), [](const Overflow& x, const Overflow& y) { return x.read < y.read; });
 }
 
@@ -2978,10 +2998,14 @@ static void collect_batch(MapCtx* c, const BatchSlot& sl, std::vector<Overflow>&
 // The host waits once, for the sizes of the bucket tables; everything after
 // is queued, and the batch's results reach `sl` when the stream drains
 // (collect_batch then lists the reads that overflowed a capacity).
+// exact: sizes are read back as the batch goes (tables of at most bt_lim
+// slots a read, 0 = no limit; the bucket jobs counted before they are
+// allocated), which costs two synchronizations; else host-known caps, with
+// the batch mapped again when its jobs exceed them.
 static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
                       const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps, bool exact,
                       uint8_t* h_plan, StageTimer& T, BatchSlot& sl, const uint32_t* pk_codes = nullptr,
-                      const uint32_t* pk_mask = nullptr) {
+                      const uint32_t* pk_mask = nullptr, uint64_t bt_lim = 0) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
     HostClock H;
@@ -3018,12 +3042,14 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     S.ccnt.reserve((size_t)n);
     S.coff.reserve((size_t)n + 1);
     S.ccur.reserve((size_t)n);
-    S.ovf_list.reserve(2 * (size_t)n);
+    S.ovf_list.reserve(4 * (size_t)n);
+    S.r_eb.reserve((size_t)n);
     S.n_jobs.reserve(1);
     S.mx.reserve(1);
     SHM_CUDA(cudaMemsetAsync(S.kcnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.r_seeded.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.r_flags.p, 0, sizeof(uint32_t) * (size_t)n, s));
+    SHM_CUDA(cudaMemsetAsync(S.r_eb.p, 0, sizeof(uint64_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.ccnt.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.ccur.p, 0, sizeof(uint32_t) * (size_t)n, s));
     SHM_CUDA(cudaMemsetAsync(S.n_jobs.p, 0, sizeof(uint32_t), s));
@@ -3109,7 +3135,10 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     v.r_smatch = S.r_smatch.p;
     v.r_seeded = S.r_seeded.p;
     v.r_flags = S.r_flags.p;
-    v.bt_cap = exact ? ((uint64_t)1 << 62) : fast_bt_slots();
+    // synchronous sizing: tables of at most bt_lim slots a read (0: the full bound)
+    v.bt_cap = exact ? (bt_lim ? bt_lim : ((uint64_t)1 << 62)) : fast_bt_slots();
+    v.r_eb = S.r_eb.p;
+    v.ext_total = p.abs_pos ? (uint64_t)ix->stats.total_nucls : (uint64_t)ix->dev.n_kmers;
     v.hw = S.hw.p;
     v.hw_off = S.hw_off.p;
     v.bt_size = S.bt_size.p;
@@ -3264,9 +3293,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     }
     if (exact) {
         bt_slots_alloc = R.totals[1];
-        // a job per touched bucket-table slot at most: the total bounds the jobs
-        if (bt_slots_alloc + 1 > (uint64_t)UINT32_MAX) throw shm_cuda_error(cudaErrorMemoryAllocation);
-        job_cap = (uint32_t)(bt_slots_alloc + 1);
+        job_cap = 0;  // counted after the contributions: a job per distinct bucket at most
         m_max = R.hm.m_max;
         nu_max = R.hm.nu_max;
         half_max = R.hm.half_max;
@@ -3296,6 +3323,14 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     SHM_CUDA(cudaGetLastError());
     T.end();
     H.mark("contrib");
+    if (exact) {  // the distinct buckets of every read, counted: they bound the jobs
+        S.sort_scr.reserve((size_t)n + 1);
+        exclusive_scan_u32(S.r_seeded.p, S.sort_scr.p, (size_t)n, s);
+        copy_async(c, &R.nbk, S.sort_scr.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        SHM_CUDA(cudaStreamSynchronize(s));
+        job_cap = R.nbk + 1;
+        sl.job_cap = job_cap;
+    }
     S.jobs.reserve(job_cap);
     H.mark("jobs_res");
     v.jobs = S.jobs.p;
@@ -3396,7 +3431,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     copy_async(c, &R.fin, S.mx.p, sizeof(BatchMax), cudaMemcpyDeviceToHost, s);
     copy_async(c, &R.nj, S.n_jobs.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     copy_async(c, &R.nc, S.coff.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    copy_async(c, sl.ovf, S.ovf_list.p, 2 * sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    copy_async(c, sl.ovf, S.ovf_list.p, 4 * sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s);
     H.mark("enq_rest");
     if (debug) {
         SHM_CUDA(cudaStreamSynchronize(s));
@@ -3449,12 +3484,13 @@ struct RetryIO {
     shm_map_record* h_out;
 };
 
-// Reads that beat their k-mer capacity estimate are mapped again, together,
-// with their counts as capacities: first as a queued batch (capped bucket
-// tables), then, for any read that overflows again, with exact sizes.
-static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params& p, const std::vector<Overflow>& ovf,
-                            const int64_t* offs, const RetryIO& io, bool exact = false) {
-    if (ovf.empty()) return;
+// One group of reads mapped again (exact: synchronous sizing, bucket tables
+// of at most bt_lim slots a read, 0 = the full bound): their bytes gathered
+// into one batch, their records scattered back to their places; the reads
+// that overflow again go to *again (with their read indices in the call).
+static void retry_group(MapCtx* c, const IndexStorage* ix, const shm_params& p, const std::vector<Overflow>& ovf,
+                        const int64_t* offs, const RetryIO& io, bool exact, uint64_t bt_lim,
+                        std::vector<Overflow>* again_out) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
     const int32_t n = (int32_t)ovf.size();
@@ -3494,20 +3530,17 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
     StageTimer T(c);
     const std::vector<std::pair<int32_t, int32_t>> one{{0, n}};
     std::vector<BatchSlot> sl = batch_slots(c, one, o.data());
-    run_batch(c, ix, p, S.retry_seq.p, o.data(), n, S.retry_out.p, caps.data(), exact, pin + plan_at, T, sl[0]);
+    run_batch(c, ix, p, S.retry_seq.p, o.data(), n, S.retry_out.p, caps.data(), exact, pin + plan_at, T, sl[0],
+              nullptr, nullptr, bt_lim);
     SHM_CUDA(cudaStreamSynchronize(s));
-    if (sl[0].R->nj > sl[0].job_cap) {  // too many bucket jobs for the queued sizes
-        run_batch(c, ix, p, S.retry_seq.p, o.data(), n, S.retry_out.p, caps.data(), true, pin + plan_at, T, sl[0]);
+    if (!exact && sl[0].R->nj > sl[0].job_cap) {  // too many bucket jobs for the queued sizes: counted this time
+        run_batch(c, ix, p, S.retry_seq.p, o.data(), n, S.retry_out.p, caps.data(), true, pin + plan_at, T, sl[0],
+                  nullptr, nullptr, fast_bt_slots());
         SHM_CUDA(cudaStreamSynchronize(s));
     }
     T.collect();
     std::vector<Overflow> again;
     collect_batch(c, sl[0], again);
-    if (exact && !again.empty()) {
-        std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n",
-                     ovf[again[0].read].read);
-        throw shm_cuda_error(cudaErrorMemoryAllocation);
-    }
     if (io.d_out) {  // records to their slots on the device
         int32_t* h_idx = (int32_t*)(pin + idx_at);
         for (int32_t i = 0; i < n; i++) h_idx[i] = ovf[i].read;
@@ -3523,11 +3556,62 @@ static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params&
         SHM_CUDA(cudaStreamSynchronize(s));
         for (int32_t i = 0; i < n; i++) io.h_out[ovf[i].read] = h_rec[i];
     }
-    if (!again.empty()) {  // a capped bucket table filled up: those reads once more, with exact sizes
-        std::vector<Overflow> sub;
-        for (const Overflow& a : again) sub.push_back(Overflow{ovf[a.read].read, a.m});
-        retry_overflows(c, ix, p, sub, offs, io, true);
+    for (const Overflow& a : again) again_out->push_back(Overflow{ovf[a.read].read, a.m, a.eb});
+}
+
+// The retry ladder's bucket-table limits, in slots a read: a read whose table
+// filled up is mapped again with eight times the slots (never more than its
+// bound), and the last step takes its full bound.
+static const uint64_t RETRY_BT[] = {4096, 32768, 262144, 0};
+constexpr int RETRY_STEPS = (int)(sizeof(RETRY_BT) / sizeof(RETRY_BT[0]));
+
+// Reads that overflowed a capacity are mapped again. Those that beat their
+// k-mer capacity estimate (their seeds never prepared) go first as a queued
+// batch with their counts as capacities. Those whose bucket table filled up
+// climb the ladder, each step synchronous and cut into groups whose tables
+// and per-read buffers fit a share of the device's free memory, so that many
+// reads of huge bucket counts (reads from tandem arrays at high -r) never ask
+// for all their memory at once.
+static void retry_overflows(MapCtx* c, const IndexStorage* ix, const shm_params& p, const std::vector<Overflow>& ovf,
+                            const int64_t* offs, const RetryIO& io, int step = -1) {
+    if (ovf.empty()) return;
+    std::vector<Overflow> next;
+    if (step < 0) {  // k-mer capacity overflows: one queued batch; table overflows climb from the first step
+        std::vector<Overflow> kmer;
+        for (const Overflow& o : ovf) (o.eb == 0 ? kmer : next).push_back(o);
+        if (!kmer.empty()) retry_group(c, ix, p, kmer, offs, io, false, 0, &next);
+        retry_overflows(c, ix, p, next, offs, io, 0);
+        return;
     }
+    if (step >= RETRY_STEPS) {
+        std::fprintf(stderr, "shmap-b200: read %d exceeds a device capacity even with exact bounds\n", ovf[0].read);
+        throw shm_cuda_error(cudaErrorMemoryAllocation);
+    }
+    const uint64_t lim = RETRY_BT[step];
+    size_t free_b = 0, total_b = 0;
+    SHM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const uint64_t budget = std::max<uint64_t>((uint64_t)1 << 29, free_b / 3);
+    std::vector<Overflow> group;
+    uint64_t used = 0;
+    auto flush = [&]() {
+        if (group.empty()) return;
+        retry_group(c, ix, p, group, offs, io, true, lim, &next);
+        group.clear();
+        used = 0;
+    };
+    for (const Overflow& o : ovf) {
+        const uint64_t full = std::max<uint64_t>(16, pow2_host(2 * std::max<uint64_t>(o.eb, 1)));
+        const uint64_t slots = lim ? std::min(lim, full) : full;
+        // the table (slot, list entry), a job and its lists and sweep scratch per slot,
+        // the k-mer, seed and probe arrays per k-mer of capacity
+        const uint64_t bytes = slots * (sizeof(BSlot) + 4 + sizeof(BucketJob) + 12 + 2 * 48) +
+                               (uint64_t)o.m * 160 + ((uint64_t)offs[o.read + 1] - (uint64_t)offs[o.read]) + 4096;
+        if (!group.empty() && used + bytes > budget) flush();
+        group.push_back(o);
+        used += bytes;
+    }
+    flush();
+    retry_overflows(c, ix, p, next, offs, io, step + 1);
 }
 
 // The nonzero mask words of a packed batch into its zeroed mask.
@@ -3590,12 +3674,12 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
                   slots[b]);
     }
     SHM_CUDA(cudaStreamSynchronize(c->stream));
-    // a batch with more bucket jobs than its capacity is mapped again with exact sizes
+    // a batch with more bucket jobs than its capacity is mapped again, its jobs counted first
     for (size_t b = 0; b < batches.size(); b++) {
         if (slots[b].R->nj <= slots[b].job_cap) continue;
         const auto [i, j] = batches[b];
         run_batch(c, ix, p, d_seq + (h_offs[i] - h_offs[0]), h_offs + i, j - i, d_out + i, nullptr, true, plans[b], T,
-                  slots[b]);
+                  slots[b], nullptr, nullptr, fast_bt_slots());
         SHM_CUDA(cudaStreamSynchronize(c->stream));
     }
     T.collect();
@@ -3675,6 +3759,9 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
     HostClock H;
+    struct PackRelease {  // a packing started and never waited for (an error) is ended
+        ~PackRelease() { pack_reads_host_release(); }
+    } pack_release;
     // batch b+1 is packed on the host threads while batch b is queued, b-1
     // maps and b goes up
     if (!batches.empty()) {
@@ -3702,7 +3789,7 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     H.mark("enqueue");
     SHM_CUDA(cudaStreamSynchronize(s));
     H.mark("drain");
-    // a batch with more bucket jobs than its capacity is mapped again with exact sizes
+    // a batch with more bucket jobs than its capacity is mapped again, its jobs counted first
     bool changed = false;
     for (size_t b = 0; b < batches.size(); b++) {
         if (slots[b].R->nj <= slots[b].job_cap) continue;
@@ -3712,7 +3799,8 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         S.seqb[0].reserve((size_t)nb + 32);
         SHM_CUDA(cudaMemsetAsync(S.seqb[0].p + nb, 0, 32, s));
         copy_async(c, S.seqb[0].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, s);
-        run_batch(c, ix, p, S.seqb[0].p, offs + i, j - i, S.out.p, nullptr, true, plans[b], T, slots[b]);
+        run_batch(c, ix, p, S.seqb[0].p, offs + i, j - i, S.out.p, nullptr, true, plans[b], T, slots[b], nullptr,
+                  nullptr, fast_bt_slots());
         copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s);
         SHM_CUDA(cudaStreamSynchronize(s));

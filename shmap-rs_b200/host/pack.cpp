@@ -246,14 +246,28 @@ int g_sparse_tasks = 0;  // task lists of the sparse packing in flight (the tail
 
 }  // namespace
 
+// The pool and the task lists serve one packing at a time: a thread holds
+// this lock from pack_reads_host_start to pack_reads_host_wait (or
+// pack_reads_host_release), or for the whole of pack_reads_host, so calls
+// from several host threads (one per device, say) take turns.
+static std::mutex g_pack_mu;
+static thread_local bool t_pack_held = false;
+
 void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask) {
+    const bool own = !t_pack_held;
+    if (own) g_pack_mu.lock();
     int tasks = 0;
     auto f = pack_tasks<false>(seq, nb, codes, mask, tasks);
     if (tasks > 0) pool().run(tasks, std::move(f));
     pack_tail<false>(seq, nb, codes, mask, nullptr);
+    if (own) g_pack_mu.unlock();
 }
 
 void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes) {
+    if (!t_pack_held) {
+        g_pack_mu.lock();
+        t_pack_held = true;
+    }
     pool().finish();
     int tasks = 0;
     auto f = pack_tasks<true>(seq, nb, codes, nullptr, tasks);
@@ -273,7 +287,18 @@ size_t pack_reads_host_wait(uint32_t* pairs, size_t cap) {
             }
             n++;
         }
+    if (t_pack_held) {
+        t_pack_held = false;
+        g_pack_mu.unlock();
+    }
     return n;
+}
+
+void pack_reads_host_release() {
+    if (!t_pack_held) return;
+    pool().finish();
+    t_pack_held = false;
+    g_pack_mu.unlock();
 }
 
 size_t packed_code_words(int64_t nb) { return 2 * (size_t)(nb / 32 + 3); }

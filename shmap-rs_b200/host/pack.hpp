@@ -12,9 +12,13 @@ void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* 
 // form: start returns at once; wait returns when the packing is complete,
 // writing the nonzero mask words as (word index, word) pairs, at most cap of
 // them (never more than packed_mask_words(nb)), and returns their number.
-// One packing at a time.
+// One packing at a time: a thread's start waits for another thread's packing
+// to be waited for.
 void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes);
 size_t pack_reads_host_wait(uint32_t* pairs, size_t cap);
+// Ends a packing that will not be waited for (an error in between): the
+// packing calls of other threads may start again.
+void pack_reads_host_release();
 size_t packed_code_words(int64_t nb);
 size_t packed_mask_words(int64_t nb);
 

@@ -71,7 +71,7 @@ def test_edge_files(gpu_ctx, tmp_path, data):
     assert [seq[fa.offs[i]:fa.offs[i + 1]] for i in range(fa.n)] == [s for _, s in want]
 
 
-@pytest.mark.parametrize("data", [b">a\nAC\n@b\nGG\n", b"ACGT\n>a\nAC\n", b" \n>a\nA\n", b"@q\nACGT\n+\n",
+@pytest.mark.parametrize("data", [b">a\nAC\n@b\nGG\n", b"ACGT\n>a\nAC\n", b" \n>a\nA\n",
                                   b"@q\nACGT\nIIII\nIIII\n", b"@q\nAC\n+\nII\n\n@r\nGG\n+\nII\n",
                                   b"@q\nAC\n+\nII\nr\nGG\n+\nII\n"])
 def test_refused_files(gpu_ctx, data):
@@ -144,4 +144,16 @@ def test_fastq_records_as_the_host_reads_them(gpu_ctx, tmp_path, seed, n_rec, ma
     assert fa.n == n_rec and fa.names == [n for n, _ in want]
     seq = fa.seq().tobytes()
     assert [seq[fa.offs[i]:fa.offs[i + 1]] for i in range(fa.n)] == [s for _, s in want]
+    fa.close()
+
+
+@pytest.mark.parametrize("data", [b"@q\nACGT\n+\n", b"@q\nACGT\n+\n\n\n", b"@q x\nAC\r\n+\r\n\r\n@r\nGG", b"@q\n"])
+def test_fastq_short_last_records(gpu_ctx, tmp_path, data):
+    """A last record without its (empty) quality line, or with only its
+    header, reads as the host reader reads it."""
+    want = _host(tmp_path, data)
+    fa = sb.DeviceFasta(gpu_ctx, data)
+    seq = fa.seq().tobytes()
+    assert fa.names == [n for n, _ in want]
+    assert [seq[fa.offs[i]:fa.offs[i + 1]] for i in range(fa.n)] == [s2 for _, s2 in want]
     fa.close()

@@ -44,7 +44,7 @@ def _compare(g, o, names, seq, offs, **kw):
 CASES = [dict(rarity_weight=1.0), dict(rarity_weight=0.5, rarity_alpha=2.0), dict(rarity_tiebreak=0.01),
          dict(rarity_tiebreak=0.05, rarity_alpha=0.5), dict(rarity_tiebreak=0.2, rarity_alpha=2.0),
          dict(rarity_weight=1.0, rarity_tiebreak=0.02), dict(rarity_tiebreak=0.05, metric="Jaccard"),
-         dict(rarity_tiebreak=0.05, metric="bucket_SH"), dict(rarity_weight=2.0, abs_pos=True),
+         dict(rarity_tiebreak=0.05, metric="bucket_SH"), dict(rarity_weight=0.5, abs_pos=True, theta=0.05),
          dict(rarity_tiebreak=0.03, no_bucket_pruning=True), dict(rarity_weight=1.0, one_sweep=True)]
 
 
@@ -56,7 +56,7 @@ def test_rarity_on_repeats(gpu_ctx, kw):
     o = O.Index.from_records([("r", ref_rep)], 15, 0.2, threads=4)
     seq, offs = pack(reads)
     names = [f"q{i}" for i in range(len(reads))]
-    rec = _compare(g, o, names, seq, offs, k=15, h_frac=0.2, theta=0.3, **kw)
+    rec = _compare(g, o, names, seq, offs, **{"k": 15, "h_frac": 0.2, "theta": 0.3, **kw})
     assert (rec["status"] == 0).mean() > 0.5
 
 
