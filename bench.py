@@ -71,8 +71,11 @@ WORKLOADS = {
              "(lognormal 23+-6 kb, 0.5% errors), k=25 r=0.01 t=0.4 Containment"),
     "uniform": ("uniform5m", "fixed10k", 25, 0.01, 0.4, "Containment",
                 "5 Mbp uniform reference in 4 contigs, 2,000 x 10 kb reads with 1% errors, k=25 r=0.01 t=0.4"),
-    "ont": ("human31", "ont", 25, 0.01, 0.4, "Containment",
-            "3.1 Gbp human-scale reference, 92,000 ONT-like reads (lognormal 24+-15 kb, 7% errors)"),
+    # at 7% errors only about 0.93^25 = 16% of a read's 25-mers survive, so no
+    # read clears -t 0.4: the ONT-like workload maps at -t 0.1
+    "ont": ("human31", "ont", 25, 0.01, 0.1, "Containment",
+            "3.1 Gbp human-scale reference, 92,000 ONT-like reads (lognormal 24+-15 kb, 7% errors), k=25 r=0.01 "
+            "t=0.1"),
     "dense": ("human31", "dense", 25, 0.10, 0.4, "Containment",
               "3.1 Gbp human-scale reference at r=0.10, 125,000 reads of 15 kb (1% errors, 20% satellite)"),
 }

@@ -249,7 +249,9 @@ int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, doub
  * autotuner measures (shmap_b200/autotune.py) instead of fixing them in the
  * code: dev_batch_reads, dev_batch_bases, dev_first_batch_reads,
  * host_batch_reads, host_batch_bases, host_first_batch_reads,
- * sketch_ctas_per_sm, wide_ctas_per_sm, refine_warps_per_sm. None of them
+ * sketch_ctas_per_sm, wide_ctas_per_sm, refine_warps_per_sm, device_pack
+ * (reads in device memory packed there before sketching: 1, or sketched
+ * from their bytes: 0). None of them
  * changes a result. They are read once per process from the file named by
  * $SHMAP_TUNING, else tuning.conf in the directory above the library's
  * (key = value lines, '#' comments), else built-in defaults;

@@ -2473,7 +2473,7 @@ constexpr int SWEEP_WARPS = 4;
 constexpr int SWEEP_CAP = 64;
 
 struct SweepCand {
-    double sh, score, support;
+    double sh, score;
     int32_t seg, bb, m0, t_l, t_r, job;
 };
 
@@ -2487,7 +2487,6 @@ __device__ __forceinline__ SweepCand load_cand(const BucketJob& j, uint32_t ji) 
     SweepCand c;
     c.sh = j.sh;
     c.score = j.score;
-    c.support = j.support;
     c.seg = j.seg;
     c.bb = j.bb;
     c.m0 = j.m0;
@@ -2583,7 +2582,7 @@ __global__ void __launch_bounds__(SWEEP_WARPS * 32) k_sweep(BatchView v, SweepCa
                 auto admit_of = [&](double t) { return tb > 0.0 ? __dsub_rn(t, __dmul_rn(tb, fabs(t))) : t; };
                 auto takes = [&](const SweepCand& c, const SweepCand& cur) {
                     if (tb > 0.0 && fabs(__dsub_rn(c.score, cur.score)) <= __dmul_rn(tb, fabs(cur.score)))
-                        return c.support > cur.support;
+                        return v.jobs[c.job].support > v.jobs[cur.job].support;
                     return c.score > cur.score;
                 };
                 // pass 1 (mod.rs:816-832): thr = theta, no forbidden region
@@ -3167,7 +3166,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     a.out_rs = S.km_rs.p;
     const int64_t batch_bytes = h_offs[n] - h_offs[0];
     static const bool letters = std::getenv("SHMAP_SKETCH_LETTERS") != nullptr;
-    if (!pk_codes && d_seq && !letters) {  // reads in device memory are packed there first
+    if (!pk_codes && d_seq && !letters && tuning().device_pack) {  // reads in device memory packed there first
         S.dpk_codes.reserve(packed_code_words(batch_bytes));
         S.dpk_mask.reserve(packed_mask_words(batch_bytes));
         T.begin(STG_SKETCH, false);

@@ -35,6 +35,7 @@ const Knob KNOBS[] = {
     {"sketch_ctas_per_sm", &Tuning::sketch_ctas_per_sm, 1, 8},
     {"wide_ctas_per_sm", &Tuning::wide_ctas_per_sm, 1, 8},
     {"refine_warps_per_sm", &Tuning::refine_warps_per_sm, 8, 64},
+    {"device_pack", &Tuning::device_pack, 0, 1},
 };
 
 std::mutex g_mu;

@@ -14,6 +14,8 @@ struct Tuning {
     int64_t sketch_ctas_per_sm = 8;   // packed-read sketch: resident CTAs a grid fills per SM
     int64_t wide_ctas_per_sm = 8;     // bucket kernels that read their counts on the device
     int64_t refine_warps_per_sm = 64; // refinement warps in flight per SM (global-table path)
+    int64_t device_pack = 0;          // reads in device memory: 1 = packed there and sketched from codes,
+                                      // 0 = sketched from their bytes
 };
 
 // The settings in force (read once per process, then as set).

@@ -26,12 +26,13 @@ from . import Context, Params, RECORD_DTYPE, SketchIndex, _check, lib, synth
 
 PRESETS = {  # reference preset, read preset, k, r, theta, metric
     "hifi": ("human31", "hifi", 25, 0.01, 0.4, "Containment"),
-    "ont": ("human31", "ont", 25, 0.01, 0.4, "Containment"),
+    "ont": ("human31", "ont", 25, 0.01, 0.1, "Containment"),
     "dense": ("human31", "dense", 25, 0.10, 0.4, "Containment"),
     "uniform": ("uniform5m", "fixed10k", 25, 0.01, 0.4, "Containment"),
 }
 
 DEVICE_KNOBS = [
+    ("device_pack", [0, 1]),
     ("sketch_ctas_per_sm", [2, 4, 6, 8]),
     ("wide_ctas_per_sm", [2, 4, 6, 8]),
     ("refine_warps_per_sm", [16, 32, 48, 64]),
