@@ -73,12 +73,15 @@ __host__ __device__ __forceinline__ int far_bin_of(int32_t half) {
 struct BatchMax {
     unsigned int m_max, nu_max, half_max, n_overflow;
     unsigned long long kmers, distinct, proc_seeds, hits, buckets, ext_seeds, refine_kmers;
-    unsigned int refine_next;  // next candidate chunk k_refine_chip takes
+    unsigned int refine_next[2];  // next candidate chunk k_refine_chip takes, per refinement pass
     unsigned int n_far;        // candidates refined by k_refine (listed in cfar)
     unsigned int lcs_next;     // next candidate k_refine takes under bucket_LCS
     unsigned int far_bin[FAR_BINS];  // candidates of cfar by cost bin (their read's bucket half-length)
     unsigned int far_cur[FAR_BINS];  // placing them, binned, into cfar_q
-    unsigned int far_next;           // next candidate of cfar_q a refinement warp takes
+    unsigned int far_next[2];        // next candidate of cfar_q a refinement warp takes, per pass
+    unsigned long long refined;      // candidates refined (the reads' leads and those that can still score)
+    unsigned long long bt2_next;     // spare bucket-table slots handed out (second tables)
+    unsigned int bt2_n;              // reads given a second table (listed in bt2_list)
 };
 
 // Small device-to-host reads of a batch, landing in pinned memory.
@@ -119,7 +122,12 @@ struct BatchView {
     uint32_t* r_seeded;
     uint64_t *hw, *hw_off, *bt_size, *bt_off;
     BSlot* bt;
+    ulonglong2* bt_tab; // per read: its bucket table's first slot and slot mask (k_bt_init, k_bt_second)
     uint32_t* bt_list;  // per read, the slots of its distinct buckets (r_seeded[q] of them)
+    uint64_t bt_pool;   // slots of the first tables; bt2_spare more follow for second tables
+    uint64_t bt2_spare;
+    uint32_t* bt2_list; // the reads given a second table
+    uint64_t* bt2_off;  // their first runs of hit work items for k_contrib2 (exclusive prefix, nl + 1)
     uint64_t bt_cap;    // most slots a read's bucket table gets (a power of two >= 16)
     uint64_t* r_eb;     // per read: the bound on its distinct buckets (0 until its seeds are prepared)
     uint64_t ext_total; // reference k-mers (bases under -F): a read's buckets are at most ext_total / half + 2 n_seg + 2
@@ -130,6 +138,8 @@ struct BatchView {
     uint32_t *ccnt, *coff, *ccur, *cidx;
     uint32_t* cfar;    // the jobs of the candidates not refined on chip (mx->n_far of them)
     uint32_t* cfar_q;  // the same jobs by cost bin, dearest bin first: the refinement queue
+    uint32_t* r_lead;  // per read: its lead candidate's job (refined first), UINT32_MAX for none
+    int32_t lead_on;   // candidates refined in two passes (the leads, then those that can still score)
     uint32_t* ovf_list;
     BatchMax* mx;
     shm_map_record* out;
@@ -1009,10 +1019,10 @@ __device__ __forceinline__ void bt_unpack(unsigned long long mc, int32_t& matche
 
 __device__ __forceinline__ void bt_add(const BatchView& v, int32_t q, int32_t seg, int64_t bb, int32_t matches,
                                        int32_t codir, int32_t rmin, int32_t rmax) {
-    const uint64_t base = v.bt_off[q];
-    const uint64_t mask = v.bt_off[q + 1] - base - 1;
+    if (v.r_flags[q]) return;  // the read is mapped again, or given a second table first
+    const ulonglong2 tb = v.bt_tab[q];
+    const uint64_t base = tb.x, mask = tb.y;
     const unsigned long long key = ((unsigned long long)(uint32_t)seg << 32) | (uint32_t)bb;
-    if (v.r_flags[q]) return;  // the read is mapped again
     uint64_t i = mix64(key) & mask;
     BSlot* s;
     for (uint64_t probe = 0;; probe++) {
@@ -1080,117 +1090,195 @@ __device__ __forceinline__ int32_t seg_step(const DevIndex& I, uint32_t g, int32
     return seg;
 }
 
-__global__ void __launch_bounds__(256) k_contrib(BatchView v) {
-    const uint64_t total = v.hw_off[v.n];
+// The hit work items [w, wend) (of one read or of consecutive reads), added
+// to their reads' bucket tables.
+__device__ __forceinline__ void contrib_span(const BatchView& v, uint64_t w, const uint64_t wend) {
     const bool ap = v.P.ap != 0;
     const bool sh_out = bucket_metric(v.P);  // codirection and positions are reported (bucket metrics)
     const DevIndex& I = v.I;
-    const uint64_t nrun = (total + CONTRIB_RUN - 1) / CONTRIB_RUN;
-    for (uint64_t rn = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; rn < nrun;
-         rn += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t w = rn * CONTRIB_RUN;
-        const uint64_t wend = min(w + CONTRIB_RUN, total);
-        int32_t q = (int32_t)ub_u64(v.hw_off, (uint32_t)v.n + 1, w) - 1;
-        uint64_t kb = v.kcap_off[q];
-        uint32_t np = (uint32_t)v.r_nproc[q];
-        uint32_t h = (uint32_t)v.r_half[q];
-        uint32_t j = ub_u32(v.sd_hpre + kb, np, (uint32_t)(w - v.hw_off[q])) - 1;
-        uint32_t t = (uint32_t)(w - v.hw_off[q]) - v.sd_hpre[kb + j];
-        SeedRec sr = v.sd[kb + j];
-        uint32_t a = sr.a, cnt = sr.cnt, os = sr.os;
-        int32_t seg = -1;
-        uint32_t s_lo = 0, s_hi = 0;
-        int32_t seg_p = -1;  // bucket of the seed's previous hit (seg_p < 0: none)
-        uint32_t b_p = 0;
-        if (t > 0) {
-            const uint32_t g_p = __ldg(I.hits + a + t - 1);
-            seg_p = seg = seg_step(I, g_p, seg, s_lo, s_hi);
-            b_p = (ap ? (__ldg(I.ref_rs + g_p) >> 1) : g_p - s_lo) / h;
-        }
-        for (;;) {
-            const uint32_t occs = os >> 1, sstr = os & 1u;
-            const uint32_t g_t = __ldg(I.hits + a + t);
-            seg = seg_step(I, g_t, seg, s_lo, s_hi);
-            const uint32_t b_t = (ap ? (__ldg(I.ref_rs + g_t) >> 1) : g_t - s_lo) / h;
-            const bool first = !(seg_p == seg && b_p == b_t);
-            const bool prev_is_bm1 = seg_p == seg && b_p + 1 == b_t;
-            if (first) {
-                if (cnt == 1) {
-                    const uint32_t rs = sh_out ? __ldg(I.ref_rs + g_t) : 0u;
-                    const int32_t cd = ((rs & 1u) == sstr) ? 1 : -1, r = (int32_t)(rs >> 1);
-                    bt_add(v, q, seg, b_t, 1, cd, r, r);  // add_to_pos (buckets.rs:642-662)
-                    if (b_t > 0) bt_add(v, q, seg, (int64_t)b_t - 1, 1, cd, r, r);
-                } else if (!ap) {
-                    // streamed multi-hit seed: one clamped contribution per bucket
-                    // (seeding.rs:113-205). Both of this hit's ranges, buckets b_t
-                    // and b_t - 1 (the latter unless the previous hit is in it),
-                    // start at this hit: the previous hit lies in a lower bucket
-                    // (below b_t - 1 when b_t - 1 is added) or an earlier segment.
-                    // Their ends are found by galloping forward.
-                    const uint32_t A = a + t, E = a + cnt;
-                    const uint64_t up1 = (uint64_t)s_lo + (uint64_t)(b_t + 1) * h, up0 = up1 + h;
-                    const uint32_t B1 = hits_gallop(I.hits, A + 1, E, (uint32_t)min(up1, (uint64_t)s_hi));
-                    const uint32_t B0 = hits_gallop(I.hits, B1, E, (uint32_t)min(up0, (uint64_t)s_hi));
-                    if (!sh_out) {  // matches only
-                        bt_add(v, q, seg, b_t, min((int32_t)(B0 - A), (int32_t)occs), 0, 0, 0);
-                        if (b_t > 0 && !prev_is_bm1)
-                            bt_add(v, q, seg, (int64_t)b_t - 1, min((int32_t)(B1 - A), (int32_t)occs), 0, 0, 0);
-                    } else {
-                        const int32_t r0 = (int32_t)(__ldg(I.ref_rs + g_t) >> 1);
-                        const uint32_t fwA = __ldg(I.hit_fw + A);
-                        {
-                            const int32_t c = (int32_t)(B0 - A), fw = (int32_t)(__ldg(I.hit_fw + B0) - fwA);
-                            const int32_t same = sstr ? c - fw : fw;
-                            const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B0 - 1)) >> 1);
-                            bt_add(v, q, seg, b_t, min(c, (int32_t)occs), 2 * same - c, r0, r1);
-                        }
-                        if (b_t > 0 && !prev_is_bm1) {
-                            const int32_t c = (int32_t)(B1 - A), fw = (int32_t)(__ldg(I.hit_fw + B1) - fwA);
-                            const int32_t same = sstr ? c - fw : fw;
-                            const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B1 - 1)) >> 1);
-                            bt_add(v, q, seg, (int64_t)b_t - 1, min(c, (int32_t)occs), 2 * same - c, r0, r1);
-                        }
-                    }
+    int32_t q = (int32_t)ub_u64(v.hw_off, (uint32_t)v.n + 1, w) - 1;
+    uint64_t kb = v.kcap_off[q];
+    uint32_t np = (uint32_t)v.r_nproc[q];
+    uint32_t h = (uint32_t)v.r_half[q];
+    uint32_t j = ub_u32(v.sd_hpre + kb, np, (uint32_t)(w - v.hw_off[q])) - 1;
+    uint32_t t = (uint32_t)(w - v.hw_off[q]) - v.sd_hpre[kb + j];
+    SeedRec sr = v.sd[kb + j];
+    uint32_t a = sr.a, cnt = sr.cnt, os = sr.os;
+    int32_t seg = -1;
+    uint32_t s_lo = 0, s_hi = 0;
+    int32_t seg_p = -1;  // bucket of the seed's previous hit (seg_p < 0: none)
+    uint32_t b_p = 0;
+    if (t > 0) {
+        const uint32_t g_p = __ldg(I.hits + a + t - 1);
+        seg_p = seg = seg_step(I, g_p, seg, s_lo, s_hi);
+        b_p = (ap ? (__ldg(I.ref_rs + g_p) >> 1) : g_p - s_lo) / h;
+    }
+    for (;;) {
+        const uint32_t occs = os >> 1, sstr = os & 1u;
+        const uint32_t g_t = __ldg(I.hits + a + t);
+        seg = seg_step(I, g_t, seg, s_lo, s_hi);
+        const uint32_t b_t = (ap ? (__ldg(I.ref_rs + g_t) >> 1) : g_t - s_lo) / h;
+        const bool first = !(seg_p == seg && b_p == b_t);
+        const bool prev_is_bm1 = seg_p == seg && b_p + 1 == b_t;
+        if (first) {
+            if (cnt == 1) {
+                const uint32_t rs = sh_out ? __ldg(I.ref_rs + g_t) : 0u;
+                const int32_t cd = ((rs & 1u) == sstr) ? 1 : -1, r = (int32_t)(rs >> 1);
+                bt_add(v, q, seg, b_t, 1, cd, r, r);  // add_to_pos (buckets.rs:642-662)
+                if (b_t > 0) bt_add(v, q, seg, (int64_t)b_t - 1, 1, cd, r, r);
+            } else if (!ap) {
+                // streamed multi-hit seed: one clamped contribution per bucket
+                // (seeding.rs:113-205). Both of this hit's ranges, buckets b_t
+                // and b_t - 1 (the latter unless the previous hit is in it),
+                // start at this hit: the previous hit lies in a lower bucket
+                // (below b_t - 1 when b_t - 1 is added) or an earlier segment.
+                // Their ends are found by galloping forward.
+                const uint32_t A = a + t, E = a + cnt;
+                const uint64_t up1 = (uint64_t)s_lo + (uint64_t)(b_t + 1) * h, up0 = up1 + h;
+                const uint32_t B1 = hits_gallop(I.hits, A + 1, E, (uint32_t)min(up1, (uint64_t)s_hi));
+                const uint32_t B0 = hits_gallop(I.hits, B1, E, (uint32_t)min(up0, (uint64_t)s_hi));
+                if (!sh_out) {  // matches only
+                    bt_add(v, q, seg, b_t, min((int32_t)(B0 - A), (int32_t)occs), 0, 0, 0);
+                    if (b_t > 0 && !prev_is_bm1)
+                        bt_add(v, q, seg, (int64_t)b_t - 1, min((int32_t)(B1 - A), (int32_t)occs), 0, 0, 0);
                 } else {
-                    // streamed multi-hit seed, absolute positions: the ranges by search
-                    for (int e = 0; e < 2; e++) {
-                        const int64_t bb = (int64_t)b_t - e;
-                        if (bb < 0) break;
-                        if (e == 1 && prev_is_bm1) break;
-                        uint32_t A, B;
-                        seed_range(I, a, cnt, seg, bb * (int64_t)h, (bb + 2) * (int64_t)h, ap, A, B);
-                        Agg g = range_agg(I, A, B, sstr, sh_out);
-                        bt_add(v, q, seg, bb, min(g.count, (int32_t)occs), g.codir, g.rmin, g.rmax);
+                    const int32_t r0 = (int32_t)(__ldg(I.ref_rs + g_t) >> 1);
+                    const uint32_t fwA = __ldg(I.hit_fw + A);
+                    {
+                        const int32_t c = (int32_t)(B0 - A), fw = (int32_t)(__ldg(I.hit_fw + B0) - fwA);
+                        const int32_t same = sstr ? c - fw : fw;
+                        const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B0 - 1)) >> 1);
+                        bt_add(v, q, seg, b_t, min(c, (int32_t)occs), 2 * same - c, r0, r1);
+                    }
+                    if (b_t > 0 && !prev_is_bm1) {
+                        const int32_t c = (int32_t)(B1 - A), fw = (int32_t)(__ldg(I.hit_fw + B1) - fwA);
+                        const int32_t same = sstr ? c - fw : fw;
+                        const int32_t r1 = (int32_t)(__ldg(I.ref_rs + __ldg(I.hits + B1 - 1)) >> 1);
+                        bt_add(v, q, seg, (int64_t)b_t - 1, min(c, (int32_t)occs), 2 * same - c, r0, r1);
                     }
                 }
-            }
-            if (++w >= wend) break;
-            seg_p = seg;
-            b_p = b_t;
-            if (++t == cnt) {  // next seed of the read, or the next read with hits
-                t = 0;
-                seg_p = -1;
-                if (++j == np) {
-                    do {
-                        q++;
-                    } while (v.hw_off[q + 1] <= w);
-                    kb = v.kcap_off[q];
-                    np = (uint32_t)v.r_nproc[q];
-                    h = (uint32_t)v.r_half[q];
-                    j = ub_u32(v.sd_hpre + kb, np, 0u) - 1;  // past the seeds without hits
+            } else {
+                // streamed multi-hit seed, absolute positions: the ranges by search
+                for (int e = 0; e < 2; e++) {
+                    const int64_t bb = (int64_t)b_t - e;
+                    if (bb < 0) break;
+                    if (e == 1 && prev_is_bm1) break;
+                    uint32_t A, B;
+                    seed_range(I, a, cnt, seg, bb * (int64_t)h, (bb + 2) * (int64_t)h, ap, A, B);
+                    Agg g = range_agg(I, A, B, sstr, sh_out);
+                    bt_add(v, q, seg, bb, min(g.count, (int32_t)occs), g.codir, g.rmin, g.rmax);
                 }
-                sr = v.sd[kb + j];
-                a = sr.a;
-                cnt = sr.cnt;
-                os = sr.os;
             }
+        }
+        if (++w >= wend) break;
+        seg_p = seg;
+        b_p = b_t;
+        if (++t == cnt) {  // next seed of the read, or the next read with hits
+            t = 0;
+            seg_p = -1;
+            if (++j == np) {
+                do {
+                    q++;
+                } while (v.hw_off[q + 1] <= w);
+                kb = v.kcap_off[q];
+                np = (uint32_t)v.r_nproc[q];
+                h = (uint32_t)v.r_half[q];
+                j = ub_u32(v.sd_hpre + kb, np, 0u) - 1;  // past the seeds without hits
+            }
+            sr = v.sd[kb + j];
+            a = sr.a;
+            cnt = sr.cnt;
+            os = sr.os;
         }
     }
 }
 
+__global__ void __launch_bounds__(256) k_contrib(BatchView v) {
+    const uint64_t total = v.hw_off[v.n];
+    const uint64_t nrun = (total + CONTRIB_RUN - 1) / CONTRIB_RUN;
+    for (uint64_t rn = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; rn < nrun;
+         rn += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t w = rn * CONTRIB_RUN;
+        contrib_span(v, w, min(w + CONTRIB_RUN, total));
+    }
+}
+
+// The runs of CONTRIB_RUN hit work items of the reads given a second bucket
+// table (k_bt_second), as an exclusive prefix over the list (one CTA; the
+// list is short unless many reads filled their tables).
+__global__ void __launch_bounds__(1024) k_bt2_scan(BatchView v) {
+    __shared__ unsigned long long wsum[32];
+    __shared__ unsigned long long carry;
+    const uint32_t nl = v.mx->bt2_n;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < nl; c0 += 1024) {
+        const uint32_t i = c0 + threadIdx.x;
+        unsigned long long x = 0;
+        if (i < nl) {
+            const int32_t q = (int32_t)v.bt2_list[i];
+            x = (v.hw_off[q + 1] - v.hw_off[q] + CONTRIB_RUN - 1) / CONTRIB_RUN;
+        }
+        unsigned long long inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) wsum[wid] = inc;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned long long t = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            wsum[lane] = t;  // inclusive over warps
+        }
+        __syncthreads();
+        const unsigned long long before = carry + (wid ? wsum[wid - 1] : 0ULL) + inc - x;
+        if (i < nl) v.bt2_off[i] = before;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += wsum[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) v.bt2_off[nl] = carry;
+}
+
+// Those runs over the whole grid: each finds its read in the list by the
+// prefix and contributes into the read's second table.
+__global__ void __launch_bounds__(256) k_contrib2(BatchView v) {
+    const uint32_t nl = v.mx->bt2_n;
+    if (nl == 0) return;
+    const uint64_t nrun = v.bt2_off[nl];
+    for (uint64_t rn = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; rn < nrun;
+         rn += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nl;  // the last list entry whose first run is <= rn
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (v.bt2_off[mid] <= rn) lo = mid;
+            else hi = mid;
+        }
+        const int32_t q = (int32_t)v.bt2_list[lo];
+        const uint64_t w = v.hw_off[q] + (rn - v.bt2_off[lo]) * CONTRIB_RUN;
+        contrib_span(v, w, min(w + CONTRIB_RUN, v.hw_off[q + 1]));
+    }
+}
+
 // Empties the first *total slots (the total is read on the device).
-__global__ void k_bt_init(BSlot* bt, const uint64_t* __restrict__ total) {
-    const uint64_t n = *total;
+// Clears the batch's bucket tables, the first `pool` slots at most: a read
+// whose table would end past the pool is flagged (mapped again) before any
+// kernel touches it.
+__global__ void k_bt_init(BSlot* bt, const uint64_t* __restrict__ bt_off, int32_t n_reads, uint64_t pool,
+                          uint32_t* __restrict__ r_flags, ulonglong2* __restrict__ bt_tab) {
+    const uint64_t n = min(bt_off[n_reads], pool);
+    for (int32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n_reads; q += gridDim.x * blockDim.x) {
+        const uint64_t b = bt_off[q], e = bt_off[q + 1];
+        bt_tab[q] = make_ulonglong2(b, e - b - 1);
+        if (e > pool) r_flags[q] = 1u;
+    }
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         BSlot s;
         s.key = EMPTY_KEY;
@@ -1201,18 +1289,58 @@ __global__ void k_bt_init(BSlot* bt, const uint64_t* __restrict__ total) {
     }
 }
 
+// Second tables (a batch mapped without waiting for its sizes): a read whose
+// bucket table filled up, or lay past the pool, gets a table of twice the
+// bound on its distinct buckets (a power of two, at most BT2_MAX slots) from
+// the spare slots after the pool, emptied here, and is listed for k_contrib2
+// to contribute again; a read that finds no room stays flagged and is mapped
+// again by the host. A warp takes 32 reads, each flagged one in turn.
+constexpr uint64_t BT2_MAX = 32768;
+__global__ void __launch_bounds__(256) k_bt_second(BatchView v) {
+    const int lane = threadIdx.x & 31;
+    const int32_t nwarps = (int32_t)((gridDim.x * blockDim.x) >> 5);
+    for (int32_t q0 = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; q0 < v.n; q0 += nwarps * 32) {
+        const int32_t q = q0 + lane;
+        const bool fl = q < v.n && v.r_flags[q] != 0 && v.r_status[q] != ST_OVERFLOW;
+        for (unsigned bal = __ballot_sync(0xffffffffu, fl); bal; bal &= bal - 1) {
+            const int src = __ffs(bal) - 1;
+            const int32_t r = q0 + src;
+            const uint64_t slots = min(max((uint64_t)16, pow2_ceil(2 * max(v.r_eb[r], (uint64_t)1))), BT2_MAX);
+            unsigned long long off = 0;
+            if (lane == 0) off = atomicAdd(&v.mx->bt2_next, (unsigned long long)slots);
+            off = __shfl_sync(0xffffffffu, off, 0);
+            if (off + slots > v.bt2_spare) continue;  // no room: the host maps it again
+            const uint64_t base = v.bt_pool + off;
+            for (uint64_t i = lane; i < slots; i += 32) {
+                BSlot e;
+                e.key = EMPTY_KEY;
+                e.mc = 0;
+                e.rmin = INT32_MAX;
+                e.rmax = -1;
+                v.bt[base + i] = e;
+            }
+            if (lane == 0) {
+                v.bt_tab[r] = make_ulonglong2(base, slots - 1);
+                v.r_seeded[r] = 0;
+                v.r_flags[r] = 0;
+                v.bt2_list[atomicAdd(&v.mx->bt2_n, 1u)] = (uint32_t)r;
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ K4 distinct buckets
 __global__ void __launch_bounds__(256) k_bscan(BatchView v) {
     const int lane = threadIdx.x & 31;
     const int32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int32_t q = wid; q < v.n; q += nwarps) {
         const uint32_t nb = v.r_seeded[q];
-        if (nb == 0) continue;
-        if (v.r_flags[q]) {  // its capped bucket table filled up: mapped again with the full bound
+        if (v.r_flags[q]) {  // its capped bucket table filled up, or lay past the pool: mapped again
             if (lane == 0) v.r_status[q] = ST_OVERFLOW;
             continue;
         }
-        const uint64_t base = v.bt_off[q];
+        if (nb == 0) continue;
+        const uint64_t base = v.bt_tab[q].x;
         if (lane == 0) atomicAdd(&v.mx->buckets, (unsigned long long)nb);
         for (uint32_t j = lane; j < nb; j += 32) {
             const BSlot s = v.bt[base + v.bt_list[base + j]];
@@ -1376,11 +1504,76 @@ __global__ void k_far_bins(BatchView v) {
 
 // The next candidate of the refinement queue for this warp (UINT32_MAX when
 // the queue is empty).
-__device__ __forceinline__ uint32_t next_far(const BatchView& v, int lane) {
+__device__ __forceinline__ uint32_t next_far(const BatchView& v, int lane, int pass = 0) {
     uint32_t ci = 0;
-    if (lane == 0) ci = atomicAdd(&v.mx->far_next, 1u);
+    if (lane == 0) ci = atomicAdd(&v.mx->far_next[pass], 1u);
     ci = __shfl_sync(0xffffffffu, ci, 0);
     return ci < v.mx->n_far ? v.cfar_q[ci] : UINT32_MAX;
+}
+
+// ------------------------------------------------------------------ which candidates are refined
+// Under Containment with bucket pruning, the sweep (k_sweep, as
+// match_rest) scores a candidate only while its sh is at least the running
+// threshold. The first candidate of a read's sweep order whose sh is at
+// least theta (its lead) is always scored; after it the threshold of pass 1
+// is at least T1 = max(theta, s1) when the lead's score s1 clears theta's
+// admission bar (else theta), and pass 2 starts from best * (1 - d), where
+// best clears the admission bar of a threshold >= T1. So every candidate
+// either pass scores has sh >= L = admit(T1) * (1 - d), rounded as the sweep
+// rounds (both roundings are monotone), and a read with no lead scores none.
+// The leads are refined first (pass 0), then the other candidates with sh >=
+// L (pass 1); the rest are never consulted. Without the two passes
+// (lead_on = 0) pass 0 refines every candidate.
+__global__ void k_lead(BatchView v) {
+    const int lane = threadIdx.x & 31;
+    const int32_t nwarps = (int32_t)((gridDim.x * blockDim.x) >> 5);
+    const double theta = v.P.theta;
+    for (int32_t q = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); q < v.n; q += nwarps) {
+        const uint32_t c0 = v.coff[q], nc = v.coff[q + 1] - c0;
+        // the first in sweep order (m0 desc, then (seg, bb) asc) with sh >= theta
+        int32_t bm = INT32_MIN, bs = INT32_MAX, bb = INT32_MAX;
+        uint32_t bj = UINT32_MAX;
+        for (uint32_t i = lane; i < nc; i += 32) {
+            const uint32_t ji = v.cidx[c0 + i];
+            const BucketJob& J = v.jobs[ji];
+            if (!(J.sh >= theta)) continue;
+            if (J.m0 > bm || (J.m0 == bm && (J.seg < bs || (J.seg == bs && J.bb < bb)))) {
+                bm = J.m0;
+                bs = J.seg;
+                bb = J.bb;
+                bj = ji;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int32_t om = __shfl_xor_sync(0xffffffffu, bm, o), os = __shfl_xor_sync(0xffffffffu, bs, o),
+                          ob = __shfl_xor_sync(0xffffffffu, bb, o);
+            const uint32_t oj = __shfl_xor_sync(0xffffffffu, bj, o);
+            if (om > bm || (om == bm && (os < bs || (os == bs && ob < bb)))) {
+                bm = om;
+                bs = os;
+                bb = ob;
+                bj = oj;
+            }
+        }
+        if (lane == 0) v.r_lead[q] = bj;
+    }
+}
+
+// Whether candidate ji (job J) is refined in refinement pass `pass`.
+__device__ __forceinline__ bool refined_in(const BatchView& v, const BucketJob& J, uint32_t ji, int pass) {
+    if (!v.lead_on) return pass == 0;
+    const uint32_t ld = v.r_lead[J.read];
+    if (pass == 0) return ji == ld;
+    if (ld == UINT32_MAX || ji == ld) return false;
+    const double theta = v.P.theta, tb = v.P.tiebreak, s1 = v.jobs[ld].score;
+    auto admit_of = [&](double t) { return tb > 0.0 ? __dsub_rn(t, __dmul_rn(tb, fabs(t))) : t; };
+    const double T1 = s1 > admit_of(theta) ? fmax(theta, s1) : theta;
+    const double L = __dmul_rn(admit_of(T1), __dsub_rn(1.0, v.P.min_diff));
+    // one ulp of slack below L (a candidate more is harmless)
+    const long long b = __double_as_longlong(L);
+    const double Ls = L > 0.0 ? __longlong_as_double(b - 1) : (L < 0.0 ? __longlong_as_double(b + 1) : -4.9e-324);
+    return J.sh >= Ls;
 }
 
 // ------------------------------------------------------------------ K7 refinement
@@ -1839,7 +2032,7 @@ constexpr size_t REFINE_SLICE = (REFINE_OFF_PC + 2 * (size_t)REFINE_WA + 15) / 1
 static_assert(REFINE_OFF_D % 4 == 0 && REFINE_OFF_PC % 2 == 0, "slice alignment");
 static_assert(REFINE_WARPS * REFINE_SLICE * 4 + 4 * 1024 <= 228 * 1024, "four CTAs per SM");
 
-__global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, RefScratch rsc) {
+__global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, RefScratch rsc, int pass) {
     extern __shared__ __align__(16) uint8_t rf_dyn[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -1849,8 +2042,10 @@ __global__ void __launch_bounds__(REFINE_WARPS * 32, 4) k_refine(BatchView v, Re
     int32_t* const PC = D + rsc.wmax + 1;
     int32_t* const ring = PC + rsc.wmax + 1;
     uint8_t* const slice = rf_dyn + (size_t)wib * REFINE_SLICE;
-    for (uint32_t jq; (jq = next_far(v, lane)) != UINT32_MAX;) {
+    for (uint32_t jq; (jq = next_far(v, lane, pass)) != UINT32_MAX;) {
         BucketJob* J = v.jobs + jq;
+        if (!refined_in(v, *J, jq, pass)) continue;
+        if (lane == 0) atomicAdd(&v.mx->refined, 1ULL);
         const int32_t q = J->read;
         if (v.P.metric == MET_BUCKET_SH) {  // bucket_SH (scoring.rs:311-325)
             if (lane == 0) {
@@ -2406,7 +2601,7 @@ __device__ __forceinline__ void refine_chip_one(const BatchView& v, BucketJob* J
     }
 }
 
-__global__ void __launch_bounds__(RCHIP_WARPS * 32, 4) k_refine_chip(BatchView v) {
+__global__ void __launch_bounds__(RCHIP_WARPS * 32, 4) k_refine_chip(BatchView v, int pass) {
     extern __shared__ __align__(16) uint8_t rc_smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -2424,23 +2619,27 @@ __global__ void __launch_bounds__(RCHIP_WARPS * 32, 4) k_refine_chip(BatchView v
     // only when the read changes
     const uint32_t ncand = v.coff[v.n];
     uint32_t nxt = 0;
-    if (lane == 0) nxt = atomicAdd(&v.mx->refine_next, 1u);
+    if (lane == 0) nxt = atomicAdd(&v.mx->refine_next[pass], 1u);
     int32_t cur = -1;  // the read whose table is staged
     uint32_t T = 32;
     for (;;) {
         const uint32_t ci0 = __shfl_sync(0xffffffffu, nxt, 0) * (uint32_t)RCHIP_CHUNK;
         if (ci0 >= ncand) break;
-        if (lane == 0) nxt = atomicAdd(&v.mx->refine_next, 1u);
+        if (lane == 0) nxt = atomicAdd(&v.mx->refine_next[pass], 1u);
         int32_t ql = -1;
         bool onl = false;
         if (lane < RCHIP_CHUNK && ci0 + lane < ncand) {
-            ql = v.jobs[v.cidx[ci0 + lane]].read;
-            onl = refine_on_chip(v.P, (uint32_t)v.r_m[ql], v.r_half[ql]);
+            const uint32_t ji = v.cidx[ci0 + lane];
+            const BucketJob& Jl = v.jobs[ji];
+            ql = Jl.read;
+            onl = refine_on_chip(v.P, (uint32_t)v.r_m[ql], v.r_half[ql]) && refined_in(v, Jl, ji, pass);
         }
+        const unsigned on_mask = __ballot_sync(0xffffffffu, onl);
+        if (lane == 0 && on_mask) atomicAdd(&v.mx->refined, (unsigned long long)__popc(on_mask));
         const uint32_t nc = min((uint32_t)RCHIP_CHUNK, ncand - ci0);
         for (uint32_t j = 0; j < nc; j++) {
             const int32_t q = __shfl_sync(0xffffffffu, ql, (int)j);
-            if (!__shfl_sync(0xffffffffu, onl, (int)j)) continue;  // k_refine's
+            if (!__shfl_sync(0xffffffffu, onl, (int)j)) continue;  // k_refine's, or not refined in this pass
             const int32_t m = v.r_m[q], n_u = v.r_nu[q];  // n_u <= m <= RCHIP_M
             if (q != cur) {
                 const uint64_t kb = v.kcap_off[q];
@@ -2668,33 +2867,11 @@ static void copy_async(MapCtx* c, void* dst, const void* src, size_t bytes, cuda
 const char* const STAGE_NAMES[N_STAGES] = {"sketch", "seedprep", "contrib", "bscan", "extend", "refine", "sweep", "aux"};
 const char* const WORK_NAMES[N_WORK] = {"reads", "bases", "kmers", "distinct_seeds", "processed_seeds",
                                         "seed_hits", "buckets", "bucket_jobs", "extension_seeds", "candidates",
-                                        "refine_kmers", "h2d_bytes", "d2h_bytes"};
+                                        "refine_kmers", "h2d_bytes", "d2h_bytes", "refined_candidates",
+                                        "second_tables"};
+
 
 // Event pairs around each stage of a batch, read back once the batch is done.
-// Host-side phase clock, printed per batch when SHMAP_HOSTPROF is set.
-struct HostClock {
-    bool on;
-    std::chrono::steady_clock::time_point t0, last;
-    std::string line;
-    HostClock() : on(std::getenv("SHMAP_HOSTPROF") != nullptr) {
-        if (on) t0 = last = std::chrono::steady_clock::now();
-    }
-    void mark(const char* what) {
-        if (!on) return;
-        auto now = std::chrono::steady_clock::now();
-        char b[64];
-        std::snprintf(b, sizeof b, " %s=%.3f", what, std::chrono::duration<double, std::milli>(now - last).count());
-        line += b;
-        last = now;
-    }
-    void print(const char* tag, int32_t n) {
-        if (!on) return;
-        std::fprintf(stderr, "[shmap-host] %s n=%d total=%.3f%s\n", tag, n,
-                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(),
-                     line.c_str());
-    }
-};
-
 struct StageTimer {
     MapCtx* c;
     size_t used = 0;
@@ -2754,11 +2931,14 @@ struct MapScratch {
     DevBuf<uint32_t> kcnt, km_rs, sd_hpre, pht_val, r_seeded, n_jobs, ccnt, coff, ccur,
         cidx, cfar, cfar_q, sort_scr, ovf_list, r_flags;
     DevBuf<uint32_t> lcs_pos, lcs_cnt;  // bucket_LCS only
+    DevBuf<uint32_t> r_lead;
     DevBuf<int32_t> r_i32, ref_scr;
     DevBuf<int64_t> r_smatch;
     DevBuf<uint64_t> r_eb;
     DevBuf<BSlot> bt;
-    DevBuf<uint32_t> bt_list;
+    DevBuf<uint32_t> bt_list, bt2_list;
+    DevBuf<ulonglong2> bt_tab;
+    DevBuf<uint64_t> bt2_off;
     DevBuf<BucketJob> jobs;
     DevBuf<BatchMax> mx;
     DevBuf<SweepCand> sweep_scr;
@@ -2923,14 +3103,35 @@ struct BatchSlot {
 };
 
 // The bucket tables of a batch mapped without waiting for its sizes get at
-// most 512 slots a read (reads needing more are mapped again), and at most 64
+// most 512 slots a read (twice the bound on the read's distinct buckets, as
+// in exact sizing, when that is less), laid out in read order in a pool of
+// 512 slots a read; a read whose table fills up gets a second table from
+// spare slots after the pool (k_bt_second), and is mapped again by the host
+// only when that fills up too or finds no room. A batch has at most 64
 // bucket jobs a read on average (a batch with more is mapped again). The
-// environment variables SHMAP_BT_FAST_SLOTS (a power of two >= 16) and
-// SHMAP_FAST_JOB_CAP lower them, so that tests reach both fallbacks.
-static uint64_t fast_bt_slots() {
-    const char* e = std::getenv("SHMAP_BT_FAST_SLOTS");
+// environment variables SHMAP_BT_FAST_SLOTS (the pool and per-read limit, a
+// power of two >= 16), SHMAP_BT_FAST_READ (a larger per-read limit, so that
+// tables can run past the pool), SHMAP_BT_SPARE_SLOTS and SHMAP_FAST_JOB_CAP
+// lower them, so that tests reach every fallback.
+static uint64_t env_pow2(const char* name, uint64_t lo, uint64_t hi) {
+    const char* e = std::getenv(name);
     const uint64_t v = e ? std::strtoull(e, nullptr, 10) : 0;
-    return (v >= 16 && (v & (v - 1)) == 0 && v <= 512) ? v : 512;
+    return (v >= lo && (v & (v - 1)) == 0 && v <= hi) ? v : 0;
+}
+static uint64_t fast_bt_slots() {
+    const uint64_t v = env_pow2("SHMAP_BT_FAST_SLOTS", 16, 512);
+    return v ? v : 512;
+}
+static uint64_t fast_bt_read_cap() {
+    const uint64_t r = env_pow2("SHMAP_BT_FAST_READ", 16, 4096);
+    return r ? r : fast_bt_slots();
+}
+// Spare slots for second tables: 16 a read and a million more
+// (SHMAP_BT_SPARE_SLOTS sets the number; 0 turns second tables off).
+static uint64_t bt_spare_slots(int32_t n) {
+    const char* e = std::getenv("SHMAP_BT_SPARE_SLOTS");
+    if (e) return std::strtoull(e, nullptr, 10);
+    return 16 * (uint64_t)n + ((uint64_t)1 << 20);
 }
 static uint32_t fast_job_cap(int32_t n) {
     const char* e = std::getenv("SHMAP_FAST_JOB_CAP");
@@ -2984,6 +3185,8 @@ static void collect_batch(MapCtx* c, const BatchSlot& sl, std::vector<Overflow>&
     c->work[W_EXT_SEEDS] += (int64_t)fin.ext_seeds;
     c->work[W_CANDS] += R.nc;
     c->work[W_REFINE_KMERS] += (int64_t)fin.refine_kmers;
+    c->work[W_REFINED] += (int64_t)fin.refined;
+    c->work[W_BT2_READS] += (int64_t)fin.bt2_n;
     const size_t at = ovf.size();
     for (uint32_t i = 0; i < fin.n_overflow && i < (uint32_t)sl.n; i++)
         ovf.push_back(Overflow{sl.i0 + (int32_t)sl.ovf[4 * i], sl.ovf[4 * i + 1],
@@ -3134,8 +3337,9 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     v.r_smatch = S.r_smatch.p;
     v.r_seeded = S.r_seeded.p;
     v.r_flags = S.r_flags.p;
-    // synchronous sizing: tables of at most bt_lim slots a read (0: the full bound)
-    v.bt_cap = exact ? (bt_lim ? bt_lim : ((uint64_t)1 << 62)) : fast_bt_slots();
+    // synchronous sizing: tables of at most bt_lim slots a read (0: the full bound);
+    // queued sizing: at most fast_bt_read_cap() a read, from a pool of fast_bt_slots() a read
+    v.bt_cap = exact ? (bt_lim ? bt_lim : ((uint64_t)1 << 62)) : fast_bt_read_cap();
     v.r_eb = S.r_eb.p;
     v.ext_total = p.abs_pos ? (uint64_t)ix->stats.total_nucls : (uint64_t)ix->dev.n_kmers;
     v.hw = S.hw.p;
@@ -3297,7 +3501,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         nu_max = R.hm.nu_max;
         half_max = R.hm.half_max;
     } else {
-        bt_slots_alloc = v.bt_cap * (uint64_t)n;
+        bt_slots_alloc = fast_bt_slots() * (uint64_t)n;
         job_cap = fast_job_cap(n);
         m_max = nu_max = (uint32_t)bp.max_cap;  // m <= capacity, distinct seeds <= m
         half_max = p.abs_pos ? (uint32_t)bp.max_len : (uint32_t)bp.max_cap;
@@ -3308,19 +3512,43 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     const int wide = grid_for((size_t)1 << 40, 256, (int)tu.wide_ctas_per_sm);
 
     H.mark("sizes");
-    S.bt.reserve(bt_slots_alloc + 1);
-    S.bt_list.reserve(bt_slots_alloc + 1);
+    // spare slots after the pool for second tables (queued sizing only)
+    const uint64_t spare = exact ? 0 : bt_spare_slots(n);
+    S.bt.reserve(bt_slots_alloc + spare + 1);
+    S.bt_list.reserve(bt_slots_alloc + spare + 1);
+    S.bt_tab.reserve((size_t)n);
+    S.bt2_list.reserve((size_t)n);
+    S.bt2_off.reserve((size_t)n + 1);
     H.mark("bt_res");
     v.bt = S.bt.p;
     v.bt_list = S.bt_list.p;
+    v.bt_tab = S.bt_tab.p;
+    v.bt2_list = S.bt2_list.p;
+    v.bt2_off = S.bt2_off.p;
+    v.bt_pool = bt_slots_alloc;
+    v.bt2_spare = spare;
     T.begin(STG_AUX);
-    k_bt_init<<<wide, 256, 0, s>>>(S.bt.p, S.bt_off.p + n);
+    k_bt_init<<<wide, 256, 0, s>>>(S.bt.p, S.bt_off.p, n, bt_slots_alloc, S.r_flags.p, S.bt_tab.p);
     SHM_CUDA(cudaGetLastError());
     T.end();
     T.begin(STG_CONTRIB);
     k_contrib<<<wide, 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
     T.end();
+    if (spare) {  // reads whose table filled up: a second table and their contributions again
+        T.begin(STG_CONTRIB);
+        k_bt_second<<<wide, 256, 0, s>>>(v);
+        SHM_CUDA(cudaGetLastError());
+        T.end();
+        T.begin(STG_CONTRIB);
+        k_bt2_scan<<<1, 1024, 0, s>>>(v);
+        SHM_CUDA(cudaGetLastError());
+        T.end();
+        T.begin(STG_CONTRIB);
+        k_contrib2<<<wide, 256, 0, s>>>(v);
+        SHM_CUDA(cudaGetLastError());
+        T.end();
+    }
     H.mark("contrib");
     if (exact) {  // the distinct buckets of every read, counted: they bound the jobs
         S.sort_scr.reserve((size_t)n + 1);
@@ -3355,12 +3583,24 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     v.cfar = S.cfar.p;
     S.cfar_q.reserve((size_t)job_cap + 1);
     v.cfar_q = S.cfar_q.p;
+    // two refinement passes (the reads' leads, then the candidates that can
+    // still be scored) where the sweep's thresholds bound what it scores
+    // (Containment only: a Jaccard score sits well below the sh of its bucket,
+    // so its bound prunes little and the second pass only adds a tail)
+    v.lead_on = p.metric == SHM_CONTAINMENT && !p.no_bucket_pruning && !v.P.rarity;
+    S.r_lead.reserve((size_t)n);
+    v.r_lead = S.r_lead.p;
     T.begin(STG_AUX);
     k_cidx<<<wide, 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
     k_far_bins<<<wide, 256, 0, s>>>(v);
     SHM_CUDA(cudaGetLastError());
     count_launch();
+    if (v.lead_on) {
+        k_lead<<<grid_for((size_t)n * 32, 256, 8), 256, 0, s>>>(v);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+    }
     T.end();
 
     RefScratch rsc{};
@@ -3406,20 +3646,23 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         k_refine_rarity<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, 0, s>>>(v, rsc);
         SHM_CUDA(cudaGetLastError());
     } else {
-        if (p.metric != SHM_BUCKET_SH) {
-            k_refine_chip<<<grid_for((size_t)n * 32, RCHIP_WARPS * 32, 4), RCHIP_WARPS * 32, RCHIP_WARPS * RCHIP_SLICE,
-                            s>>>(v);
-            SHM_CUDA(cudaGetLastError());
-            count_launch();
-        }
         if (!c->refine_smem_set) {
             SHM_CUDA(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)(REFINE_WARPS * REFINE_SLICE)));
             c->refine_smem_set = 1;
         }
-        k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32, REFINE_WARPS * REFINE_SLICE,
-                   s>>>(v, rsc);
-        SHM_CUDA(cudaGetLastError());
+        for (int pass = 0; pass < (v.lead_on ? 2 : 1); pass++) {
+            if (p.metric != SHM_BUCKET_SH) {
+                k_refine_chip<<<grid_for((size_t)n * 32, RCHIP_WARPS * 32, 4), RCHIP_WARPS * 32,
+                                RCHIP_WARPS * RCHIP_SLICE, s>>>(v, pass);
+                SHM_CUDA(cudaGetLastError());
+                count_launch();
+            }
+            k_refine<<<(unsigned)std::max<size_t>(1, warps / REFINE_WARPS), REFINE_WARPS * 32,
+                       REFINE_WARPS * REFINE_SLICE, s>>>(v, rsc, pass);
+            SHM_CUDA(cudaGetLastError());
+            if (pass == 0 && v.lead_on) count_launch();  // the last launch is counted by the stage timer
+        }
     }
     T.end();
     T.begin(STG_SWEEP);
@@ -3534,7 +3777,7 @@ static void retry_group(MapCtx* c, const IndexStorage* ix, const shm_params& p, 
     SHM_CUDA(cudaStreamSynchronize(s));
     if (!exact && sl[0].R->nj > sl[0].job_cap) {  // too many bucket jobs for the queued sizes: counted this time
         run_batch(c, ix, p, S.retry_seq.p, o.data(), n, S.retry_out.p, caps.data(), true, pin + plan_at, T, sl[0],
-                  nullptr, nullptr, fast_bt_slots());
+                  nullptr, nullptr, fast_bt_read_cap());
         SHM_CUDA(cudaStreamSynchronize(s));
     }
     T.collect();
@@ -3678,7 +3921,7 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
         if (slots[b].R->nj <= slots[b].job_cap) continue;
         const auto [i, j] = batches[b];
         run_batch(c, ix, p, d_seq + (h_offs[i] - h_offs[0]), h_offs + i, j - i, d_out + i, nullptr, true, plans[b], T,
-                  slots[b], nullptr, nullptr, fast_bt_slots());
+                  slots[b], nullptr, nullptr, fast_bt_read_cap());
         SHM_CUDA(cudaStreamSynchronize(c->stream));
     }
     T.collect();
@@ -3799,7 +4042,7 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         SHM_CUDA(cudaMemsetAsync(S.seqb[0].p + nb, 0, 32, s));
         copy_async(c, S.seqb[0].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, s);
         run_batch(c, ix, p, S.seqb[0].p, offs + i, j - i, S.out.p, nullptr, true, plans[b], T, slots[b], nullptr,
-                  nullptr, fast_bt_slots());
+                  nullptr, fast_bt_read_cap());
         copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s);
         SHM_CUDA(cudaStreamSynchronize(s));

@@ -1,5 +1,9 @@
 // Batched mapping on the device (see shm_map.cu).
 #pragma once
+#include <string>
+#include <cstdlib>
+#include <cstdio>
+#include <chrono>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -41,8 +45,32 @@ extern const char* const STAGE_NAMES[N_STAGES];
 // roofline's algorithmic bytes are counted in, and the bytes copied between
 // host and device.
 enum Work { W_READS, W_BASES, W_KMERS, W_DISTINCT, W_PROC_SEEDS, W_HITS, W_BUCKETS, W_JOBS, W_EXT_SEEDS, W_CANDS,
-            W_REFINE_KMERS, W_H2D_BYTES, W_D2H_BYTES, N_WORK };
+            W_REFINE_KMERS, W_H2D_BYTES, W_D2H_BYTES, W_REFINED, W_BT2_READS, N_WORK };
 extern const char* const WORK_NAMES[N_WORK];
+
+// Host-side phase clock, printed per batch when SHMAP_HOSTPROF is set.
+struct HostClock {
+    bool on;
+    std::chrono::steady_clock::time_point t0, last;
+    std::string line;
+    HostClock() : on(std::getenv("SHMAP_HOSTPROF") != nullptr) {
+        if (on) t0 = last = std::chrono::steady_clock::now();
+    }
+    void mark(const char* what) {
+        if (!on) return;
+        auto now = std::chrono::steady_clock::now();
+        char b[64];
+        std::snprintf(b, sizeof b, " %s=%.3f", what, std::chrono::duration<double, std::milli>(now - last).count());
+        line += b;
+        last = now;
+    }
+    void print(const char* tag, int32_t n) {
+        if (!on) return;
+        std::fprintf(stderr, "[shmap-host] %s n=%d total=%.3f%s\n", tag, n,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(),
+                     line.c_str());
+    }
+};
 
 struct MapCtx {
     int device = 0;

@@ -61,7 +61,9 @@ struct __align__(16) LutPair {
 
 constexpr int SK_THREADS = 256;                                  // one run of SKETCH_WIN windows per thread
 constexpr int SK_TILE_CAP = SK_THREADS * SKETCH_WIN + 1024;       // bytes a CTA stages per tile
-constexpr int SK_TILE_WORDS = SK_TILE_CAP / 4 + 8;                // + slack for the word past the last byte
+// + slack for the words past the last byte: the rotated-frame runs read up to
+// 36 bytes past it (their last group of 32 windows, and the word after)
+constexpr int SK_TILE_WORDS = SK_TILE_CAP / 4 + 16;
 constexpr int SK_TILE_PWORDS = SK_TILE_WORDS + SK_TILE_WORDS / 32 + 1;
 constexpr int SK_TILE_BYTES = (SK_TILE_PWORDS * 4 + 15) / 16 * 16; // the tile, rounded to 16 bytes
 
@@ -237,6 +239,202 @@ __device__ __forceinline__ void sketch_run(const SketchArgs& a, const LutPair* _
     }
 }
 
+// ------------------------------------------------------------------ packed reads
+// The sketch of reads packed as 2-bit codes (A, C, T, G = 0..3) with a
+// non-ACGT mask, rolled without rotating the state. With X_t and Y_t the
+// table values window t XORs in (forward: fw of the entering base and fw<<k
+// of the leaving one; reverse: rc<<(k-1) of the entering base and rc>>1 of
+// the leaving one), the rolling step is F_t = rotl1(F_{t-1}) ^ X_t and
+// R_t = rotr1(R_{t-1}) ^ Y_t. In the frame F~_t = rotr(F_t, t),
+// R~_t = rotl(R_t, t) the step is a plain XOR: F~_t = F~_{t-1} ^ rotr(X_t, t),
+// R~_t = R~_{t-1} ^ rotl(Y_t, t), and the tables hold the rotated values for
+// every entering/leaving code pair. Rotation by 32 swaps a value's halves,
+// so the state is kept half-swapped during every other group of 32 windows
+// and the tables need 32 rows: row jj holds rotr(X, jj) and rotl(Y, jj).
+// The selection test needs only the high word of h_t = F_t ^ R_t, two funnel
+// shifts of the stored state by jj; the full hash and the strand are formed
+// for the rare windows that pass it. A run starts from the hash of the
+// window one base before its first (warm-up, four bases a step), so the
+// leaving base of its first window is read like every other.
+struct PkTables {
+    uint2 pf[32][16];  // [jj][ci * 4 + co]: rotr(fw[ci] ^ fw_k[co], jj), as (lo, hi)
+    uint2 pr[32][16];  // rotl(rc_k1[ci] ^ rc_r1[co], jj)
+    uint4 w4[256];     // four bases c0..c3 (c0 the earliest, bits 0-1): rolled-in (F, R) as (Flo, Fhi, Rlo, Rhi)
+    uint4 w1[4];       // one base: (fw, rc_k1)
+};
+
+__device__ __forceinline__ uint64_t u64_of(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
+
+__device__ void build_pk_tables(PkTables& P, const SketchLuts* __restrict__ L) {
+    const unsigned char let[4] = {'A', 'C', 'T', 'G'};
+    for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
+        const int jj = e >> 4, ci = (e >> 2) & 3, co = e & 3;
+        const uint64_t x = L->fw[let[ci]] ^ L->fw_k[let[co]];
+        const uint64_t y = L->rc_k1[let[ci]] ^ L->rc_r1[let[co]];
+        const uint64_t rx = rotr64(x, (uint32_t)jj), ly = rotl64(y, (uint32_t)jj);
+        P.pf[jj][ci * 4 + co] = make_uint2((uint32_t)rx, (uint32_t)(rx >> 32));
+        P.pr[jj][ci * 4 + co] = make_uint2((uint32_t)ly, (uint32_t)(ly >> 32));
+    }
+    for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
+        uint64_t f = 0, r = 0;
+        for (int i = 0; i < 4; i++) {
+            const unsigned char c = let[(idx >> (2 * i)) & 3];
+            f ^= rotl64(L->fw[c], (uint32_t)(3 - i));
+            r ^= rotr64(L->rc_k1[c], (uint32_t)(3 - i));
+        }
+        P.w4[idx] = make_uint4((uint32_t)f, (uint32_t)(f >> 32), (uint32_t)r, (uint32_t)(r >> 32));
+    }
+    if (threadIdx.x < 4) {
+        const unsigned char c = let[threadIdx.x];
+        const uint64_t f = L->fw[c], r = L->rc_k1[c];
+        P.w1[threadIdx.x] = make_uint4((uint32_t)f, (uint32_t)(f >> 32), (uint32_t)r, (uint32_t)(r >> 32));
+    }
+}
+
+// ------------------------------------------------------------------ staged letters in the rotated frame
+// The windows of a run whose bytes are all A, C, G or T (either case) roll
+// in the frame of k_sketch_pk: each letter's code is (byte >> 1) & 3 (A, C,
+// T, G = 0..3), so four windows' table offsets (entering code * 32 + leaving
+// code * 8) come from one entering and one leaving word with two shifts and
+// masks, and a window is one byte permute, two 8-byte table loads, four
+// XORs and the high-word test. A window that passes the test keeps its
+// state in a thread-local buffer; the full hash, strand and selection are
+// formed for those after the run, once every byte the run read is known to
+// be a letter. A run with any other byte (or more than FR_CAP such windows)
+// returns false having selected nothing, and rolls through the byte tables
+// instead. The window before the run's first (which includes the byte
+// before it, whatever it holds) is the warm-up's: that byte enters and
+// leaves through the same code, so it cancels.
+constexpr int FR_CAP = 32;
+
+// Code byte of four letters (the earliest in bits 0-1): the codes sit at
+// bits 0-1 of each byte after the shift and mask; the multiply gathers byte
+// i's code at bits 24 + 2i with no carry into them from the other products.
+__device__ __forceinline__ uint32_t codes4(uint32_t w) { return (((w >> 1) & 0x03030303u) * 0x01041040u) >> 24; }
+
+// Nonzero unless the four bytes of w are letters A, C, G, T of either case:
+// the byte that a letter of the same code would be (A, C, T, G = 0x41 +
+// 2c, plus 15 for c = 2), against the byte with its case bit cleared.
+__device__ __forceinline__ uint32_t not_acgt4(uint32_t w) {
+    const uint32_t d = w & 0x06060606u;                        // 2c per byte
+    const uint32_t t = (d >> 2) & ~(d >> 1) & 0x01010101u;      // c == 2
+    const uint32_t want = t * 15u + d + 0x41414141u;            // no carries between bytes
+    return (w & 0xdfdfdfdfu) ^ want;
+}
+
+// Tile word w (words before the tile read as 0: only the byte before a run
+// at the tile's first byte reaches them, and that byte cancels).
+__device__ __forceinline__ uint32_t tile_word(const uint32_t* tile, int w) { return w < 0 ? 0u : tile[pword(w)]; }
+
+template <int MODE>
+__device__ __forceinline__ bool sketch_run_frame(const SketchArgs& a, const PkTables& P, const uint32_t* tile, int x,
+                                                 int32_t cnt, int k, uint64_t thr, int32_t q, int32_t r0, Emit& e) {
+    uint32_t bad = 0;
+    // warm-up: the window of bytes [x - 1, x + k - 1), four letters a step
+    uint64_t F = 0, R = 0;
+    {
+        const int b = x - 1;
+        const uint32_t sh = (uint32_t)(b & 3) * 8;
+        int w = b >> 2;  // -1 for b = -1
+        uint32_t lw = tile_word(tile, w);
+        int i = 0;
+        for (; i + 4 <= k; i += 4) {
+            const uint32_t hw = tile_word(tile, ++w);
+            const uint32_t b4 = __funnelshift_r(lw, hw, sh);
+            lw = hw;
+            // the byte before the run is not checked (it cancels); the rest are
+            bad |= i == 0 ? (not_acgt4(b4) & 0xffffff00u) : not_acgt4(b4);
+            const uint4 t = P.w4[codes4(b4)];
+            F = rotl64(F, 4) ^ u64_of(t.x, t.y);
+            R = rotr64(R, 4) ^ u64_of(t.z, t.w);
+        }
+        if (i < k) {
+            const uint32_t hw = tile_word(tile, ++w);
+            const uint32_t b4 = __funnelshift_r(lw, hw, sh);
+            const int rem = k - i;  // 1..3 bytes
+            const uint32_t keep = (1u << (8 * rem)) - 1u;
+            bad |= (i == 0 ? (not_acgt4(b4) & 0xffffff00u) : not_acgt4(b4)) & keep;
+            for (int u = 0; u < rem; u++) {
+                const uint4 t = P.w1[(b4 >> (8 * u + 1)) & 3u];
+                F = rotl64(F, 1) ^ u64_of(t.x, t.y);
+                R = rotr64(R, 1) ^ u64_of(t.z, t.w);
+            }
+        }
+    }
+    F = rotl64(F, 1);  // the frame at t = -1
+    R = rotr64(R, 1);
+    uint32_t Flo = (uint32_t)F, Fhi = (uint32_t)(F >> 32), Rlo = (uint32_t)R, Rhi = (uint32_t)(R >> 32);
+    const uint32_t thr_hi = (uint32_t)(thr >> 32);
+    // entering bytes from x + k - 1, leaving bytes from x - 1
+    const int bi = x + k - 1, bo = x - 1;
+    const uint32_t shi = (uint32_t)(bi & 3) * 8, sho = (uint32_t)(bo & 3) * 8;
+    int wi = bi >> 2, wo = bo >> 2;
+    uint32_t li = tile_word(tile, wi), lo_ = tile_word(tile, wo);
+    uint4 buf[FR_CAP];
+    uint32_t n = 0, m0 = 0, m1 = 0, m2 = 0, m3 = 0;  // passing windows of the last four groups (m0 the latest)
+    int32_t groups = 0;
+#pragma unroll 1
+    for (int32_t t0 = 0; t0 < cnt; t0 += 32) {
+        uint32_t mg = 0;
+#pragma unroll
+        for (int s4 = 0; s4 < 8; s4++) {
+            const uint32_t hi_i = tile[pword(++wi)], hi_o = tile[pword(++wo)];  // wo >= -1 before the increment
+            const uint32_t win = __funnelshift_r(li, hi_i, shi), wout = __funnelshift_r(lo_, hi_o, sho);
+            li = hi_i;
+            lo_ = hi_o;
+            bad |= not_acgt4(win);
+            // byte j: entering code * 32 + leaving code * 8, the entry's offset in its row
+            const uint32_t comb = ((win << 4) & 0x60606060u) | ((wout << 2) & 0x18181818u);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int jj = 4 * s4 + j;
+                const uint32_t off = __byte_perm(comb, 0u, 0x4440u + (uint32_t)j);
+                const uint2 ef = *(const uint2*)((const char*)&P.pf[jj][0] + off);
+                const uint2 er = *(const uint2*)((const char*)&P.pr[jj][0] + off);
+                Flo ^= ef.x;
+                Fhi ^= ef.y;
+                Rlo ^= er.x;
+                Rhi ^= er.y;
+                const uint32_t hh = __funnelshift_l(Flo, Fhi, jj) ^ __funnelshift_r(Rhi, Rlo, jj);
+                if (hh <= thr_hi) {
+                    buf[n & (FR_CAP - 1)] = make_uint4(Flo, Fhi, Rlo, Rhi);
+                    n++;
+                    mg |= 1u << jj;
+                }
+            }
+        }
+        m3 = m2;
+        m2 = m1;
+        m1 = m0;
+        m0 = mg;
+        groups++;
+        uint32_t y = Flo;  // rotation by 32: the next group's rows apply to the swapped halves
+        Flo = Fhi;
+        Fhi = y;
+        y = Rlo;
+        Rlo = Rhi;
+        Rhi = y;
+    }
+    if (bad != 0 || n > (uint32_t)FR_CAP) return false;
+    // the passing windows in order: group g's mask is m_(groups - 1 - g)
+    // (windows past the run's last one, rolled in its last group, are skipped)
+    uint32_t at = 0;
+    for (int32_t g = 0; g < groups; g++) {
+        const int back = groups - 1 - g;
+        uint32_t mk = back == 0 ? m0 : back == 1 ? m1 : back == 2 ? m2 : m3;
+        if (32 * g + 32 > cnt) mk &= (1u << (cnt - 32 * g)) - 1u;  // cnt - 32g in 1..31 here
+        while (mk) {
+            const uint32_t jj = (uint32_t)__ffs(mk) - 1;
+            mk &= mk - 1;
+            const uint4 st = buf[at++];
+            const uint64_t Fv = rotl64(u64_of(st.x, st.y), jj), Rv = rotr64(u64_of(st.z, st.w), jj);
+            const uint64_t h = Fv ^ Rv;
+            if (h <= thr) emit_kmer<MODE>(a, q, h, ((uint32_t)(r0 + 32 * g + (int32_t)jj) << 1) | (Fv > Rv ? 1u : 0u), e);
+        }
+    }
+    return true;
+}
+
 // Dynamic shared memory of a k_sketch CTA: the staged tile.
 constexpr size_t sk_dyn_bytes(int) { return (size_t)SK_TILE_BYTES; }
 
@@ -253,11 +451,13 @@ constexpr size_t sk_dyn_bytes(int) { return (size_t)SK_TILE_BYTES; }
 template <int MODE, bool PK>
 __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const SketchLuts* __restrict__ luts) {
     __shared__ LutPair Lin[256], Lout[256];
+    __shared__ PkTables P;
     __shared__ uint32_t s_unpack[PK ? 256 : 1];
     __shared__ int64_t s_lo, s_hi;
     __shared__ int32_t s_q[2];
     extern __shared__ __align__(16) uint8_t sk_dyn[];
     uint32_t* tile = (uint32_t*)sk_dyn;
+    build_pk_tables(P, luts);
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         Lin[i] = LutPair{luts->fw[i], luts->rc_k1[i]};
         Lout[i] = LutPair{luts->fw_k[i], luts->rc_r1[i]};
@@ -368,9 +568,10 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
         }
         const int64_t x = PK ? start - B0 : (int64_t)((a.seq + start) - A0);  // the run's first byte in the tile
         const int32_t r0 = (int32_t)(w0 + k - 1) + a.r_offset;              // r of the run's first window
-        if (staged)
-            sketch_run<MODE>(a, Lin, Lout, StagedBytes{tile}, (int)x, cnt, k, thr, q, r0, e);
-        else if (PK)
+        if (staged) {
+            if (cnt > 0 && !sketch_run_frame<MODE>(a, P, tile, (int)x, cnt, k, thr, q, r0, e))
+                sketch_run<MODE>(a, Lin, Lout, StagedBytes{tile}, (int)x, cnt, k, thr, q, r0, e);
+        } else if (PK)
             sketch_run<MODE>(a, Lin, Lout, GlobalPacked{a.pk_codes, a.pk_mask, B0, first, lim}, x, cnt, k, thr, q, r0,
                              e);
         else
@@ -402,58 +603,6 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
             }
         }
         __syncthreads();  // the tile is free for the next one
-    }
-}
-
-// ------------------------------------------------------------------ packed reads
-// The sketch of reads packed as 2-bit codes (A, C, T, G = 0..3) with a
-// non-ACGT mask, rolled without rotating the state. With X_t and Y_t the
-// table values window t XORs in (forward: fw of the entering base and fw<<k
-// of the leaving one; reverse: rc<<(k-1) of the entering base and rc>>1 of
-// the leaving one), the rolling step is F_t = rotl1(F_{t-1}) ^ X_t and
-// R_t = rotr1(R_{t-1}) ^ Y_t. In the frame F~_t = rotr(F_t, t),
-// R~_t = rotl(R_t, t) the step is a plain XOR: F~_t = F~_{t-1} ^ rotr(X_t, t),
-// R~_t = R~_{t-1} ^ rotl(Y_t, t), and the tables hold the rotated values for
-// every entering/leaving code pair. Rotation by 32 swaps a value's halves,
-// so the state is kept half-swapped during every other group of 32 windows
-// and the tables need 32 rows: row jj holds rotr(X, jj) and rotl(Y, jj).
-// The selection test needs only the high word of h_t = F_t ^ R_t, two funnel
-// shifts of the stored state by jj; the full hash and the strand are formed
-// for the rare windows that pass it. A run starts from the hash of the
-// window one base before its first (warm-up, four bases a step), so the
-// leaving base of its first window is read like every other.
-struct PkTables {
-    uint2 pf[32][16];  // [jj][ci * 4 + co]: rotr(fw[ci] ^ fw_k[co], jj), as (lo, hi)
-    uint2 pr[32][16];  // rotl(rc_k1[ci] ^ rc_r1[co], jj)
-    uint4 w4[256];     // four bases c0..c3 (c0 the earliest, bits 0-1): rolled-in (F, R) as (Flo, Fhi, Rlo, Rhi)
-    uint4 w1[4];       // one base: (fw, rc_k1)
-};
-
-__device__ __forceinline__ uint64_t u64_of(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
-
-__device__ void build_pk_tables(PkTables& P, const SketchLuts* __restrict__ L) {
-    const unsigned char let[4] = {'A', 'C', 'T', 'G'};
-    for (int e = threadIdx.x; e < 32 * 16; e += blockDim.x) {
-        const int jj = e >> 4, ci = (e >> 2) & 3, co = e & 3;
-        const uint64_t x = L->fw[let[ci]] ^ L->fw_k[let[co]];
-        const uint64_t y = L->rc_k1[let[ci]] ^ L->rc_r1[let[co]];
-        const uint64_t rx = rotr64(x, (uint32_t)jj), ly = rotl64(y, (uint32_t)jj);
-        P.pf[jj][ci * 4 + co] = make_uint2((uint32_t)rx, (uint32_t)(rx >> 32));
-        P.pr[jj][ci * 4 + co] = make_uint2((uint32_t)ly, (uint32_t)(ly >> 32));
-    }
-    for (int idx = threadIdx.x; idx < 256; idx += blockDim.x) {
-        uint64_t f = 0, r = 0;
-        for (int i = 0; i < 4; i++) {
-            const unsigned char c = let[(idx >> (2 * i)) & 3];
-            f ^= rotl64(L->fw[c], (uint32_t)(3 - i));
-            r ^= rotr64(L->rc_k1[c], (uint32_t)(3 - i));
-        }
-        P.w4[idx] = make_uint4((uint32_t)f, (uint32_t)(f >> 32), (uint32_t)r, (uint32_t)(r >> 32));
-    }
-    if (threadIdx.x < 4) {
-        const unsigned char c = let[threadIdx.x];
-        const uint64_t f = L->fw[c], r = L->rc_k1[c];
-        P.w1[threadIdx.x] = make_uint4((uint32_t)f, (uint32_t)(f >> 32), (uint32_t)r, (uint32_t)(r >> 32));
     }
 }
 
@@ -558,28 +707,31 @@ __device__ __forceinline__ void pk_run(const SketchArgs& a, const PkTables& P, i
     const uint32_t shi = (uint32_t)(bi & 15) * 2, sho = (uint32_t)(bo & 15) * 2;
     uint32_t i0 = pk_word(codes, wi, nw), i1 = pk_word(codes, wi + 1, nw), i2 = pk_word(codes, wi + 2, nw);
     uint32_t o0 = pk_word(codes, wo, nw), o1 = pk_word(codes, wo + 1, nw), o2 = pk_word(codes, wo + 2, nw);
+    // one group body (32 windows) in the loop: after each group the state's
+    // halves are swapped (rotation by 32), so the next group's rows apply as
+    // they are; a single body keeps the kernel's code within the instruction cache
 #pragma unroll 1
-    for (int t0 = 0; t0 < cnt; t0 += 64) {
+    for (int t0 = 0; t0 < cnt; t0 += 32) {
         // the next group's words, loaded while this one rolls
         const uint32_t i3 = pk_word(codes, wi + 3, nw), i4 = pk_word(codes, wi + 4, nw);
         const uint32_t o3 = pk_word(codes, wo + 3, nw), o4 = pk_word(codes, wo + 4, nw);
-        uint2 in = make_uint2(__funnelshift_r(i0, i1, shi), __funnelshift_r(i1, i2, shi));
-        uint2 out = make_uint2(__funnelshift_r(o0, o1, sho), __funnelshift_r(o1, o2, sho));
+        const uint2 in = make_uint2(__funnelshift_r(i0, i1, shi), __funnelshift_r(i1, i2, shi));
+        const uint2 out = make_uint2(__funnelshift_r(o0, o1, sho), __funnelshift_r(o1, o2, sho));
         pk_group<MODE>(a, P, in, out, Flo, Fhi, Rlo, Rhi, thr_hi, thr, q, r0 + t0, cnt - t0, e);
-        // windows t0 + 32 .. t0 + 63: the state half-swapped (rotation by 32)
-        const uint32_t i5 = pk_word(codes, wi + 5, nw), i6 = pk_word(codes, wi + 6, nw);
-        const uint32_t o5 = pk_word(codes, wo + 5, nw), o6 = pk_word(codes, wo + 6, nw);
-        in = make_uint2(__funnelshift_r(i2, i3, shi), __funnelshift_r(i3, i4, shi));
-        out = make_uint2(__funnelshift_r(o2, o3, sho), __funnelshift_r(o3, o4, sho));
-        pk_group<MODE>(a, P, in, out, Fhi, Flo, Rhi, Rlo, thr_hi, thr, q, r0 + t0 + 32, cnt - t0 - 32, e);
-        i0 = i4;
-        i1 = i5;
-        i2 = i6;
-        o0 = o4;
-        o1 = o5;
-        o2 = o6;
-        wi += 4;
-        wo += 4;
+        uint32_t x = Flo;
+        Flo = Fhi;
+        Fhi = x;
+        x = Rlo;
+        Rlo = Rhi;
+        Rhi = x;
+        i0 = i2;
+        i1 = i3;
+        i2 = i4;
+        o0 = o2;
+        o1 = o3;
+        o2 = o4;
+        wi += 2;
+        wo += 2;
     }
 }
 
@@ -700,7 +852,7 @@ void launch_sketch(int mode, const SketchArgs& a, const SketchLuts* L, cudaStrea
         return;
     }
     const uint64_t n_tiles = (a.n_chunks + SK_THREADS - 1) / SK_THREADS;
-    const int grid = grid_for(n_tiles, 1, 5);  // tiles, at most 5 resident CTAs per SM
+    const int grid = grid_for(n_tiles, 1, 4);  // tiles, at most 4 resident CTAs per SM (shared memory)
     const size_t dyn = sk_dyn_bytes(mode);
     {  // the dynamic shared memory limit, once per device and kernel
         static std::mutex mu;

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -78,6 +79,52 @@ __attribute__((target("avx2"))) void pack_range_avx2(const uint8_t* s, int64_t n
         }
     }
     _mm_sfence();
+}
+
+// AVX-512 (BW, VBMI): 64 bytes a step, groups g and g + 1. A byte is ACGT
+// (either case) iff its low seven bits index a set byte of a 128-entry table
+// (one two-register byte permute) and its top bit is clear. The codes of
+// four bases gather into one byte of a 32-bit lane by two multiply-adds (c0 +
+// 4 c1, then + 16 (c2 + 4 c3)); narrowing the sixteen lanes to bytes gives the
+// 64 bases' 16 bytes of codes. n32 is even; codes + 2 g0 is 16-byte aligned
+// when `aligned` (streaming stores), else plain stores are used.
+template <bool SPARSE>
+__attribute__((target("avx512f,avx512bw,avx512vbmi"))) void pack_range_avx512(const uint8_t* s, int64_t n32,
+                                                                              uint32_t* codes, uint32_t* mask,
+                                                                              int64_t g_base, MaskList* list,
+                                                                              bool aligned) {
+    alignas(64) uint8_t lut[128];
+    for (int i = 0; i < 128; i++) {
+        const int u = i & 0xdf;
+        lut[i] = (u == 0x41 || u == 0x43 || u == 0x47 || u == 0x54) ? 0xff : 0x00;
+    }
+    const __m512i lut_lo = _mm512_load_si512((const void*)lut), lut_hi = _mm512_load_si512((const void*)(lut + 64));
+    const __m512i k3 = _mm512_set1_epi8(3), m1 = _mm512_set1_epi16(0x0401), m2 = _mm512_set1_epi32(0x00100001);
+    for (int64_t g = 0; g < n32; g += 2) {
+        const __m512i v = _mm512_loadu_si512((const void*)(s + 32 * g));
+        const __m512i c = _mm512_and_si512(_mm512_srli_epi16(v, 1), k3);
+        const __m512i t = _mm512_permutex2var_epi8(lut_lo, v, lut_hi);
+        const uint64_t good = _mm512_test_epi8_mask(t, t) & ~_mm512_movepi8_mask(v);
+        const __m128i q = _mm512_cvtepi32_epi8(_mm512_madd_epi16(_mm512_maddubs_epi16(c, m1), m2));
+        if (aligned) _mm_stream_si128((__m128i*)(codes + 2 * g), q);
+        else _mm_storeu_si128((__m128i*)(codes + 2 * g), q);
+        const uint64_t bad = ~good;
+        if (SPARSE) {
+            if (bad) {
+                if ((uint32_t)bad) list->emplace_back((uint32_t)(g_base + g), (uint32_t)bad);
+                if ((uint32_t)(bad >> 32)) list->emplace_back((uint32_t)(g_base + g + 1), (uint32_t)(bad >> 32));
+            }
+        } else {
+            _mm_stream_si64((long long*)(mask + g), (long long)bad);
+        }
+    }
+    _mm_sfence();
+}
+
+bool have_avx512() {
+    static const bool v = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw") &&
+                          __builtin_cpu_supports("avx512vbmi");
+    return v;
 }
 
 template <bool SPARSE>
@@ -222,9 +269,11 @@ template <bool SPARSE>
 static std::function<void(int)> pack_tasks(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask,
                                            int& tasks) {
     const int64_t n32 = nb / 32;
-    const int64_t per = std::max<int64_t>(1 << 15, (n32 + 4 * pool().size() - 1) / (4 * pool().size()));
+    // an even number of groups a task (the AVX-512 form takes two at a time)
+    const int64_t per = (std::max<int64_t>(1 << 15, (n32 + 4 * pool().size() - 1) / (4 * pool().size())) + 1) & ~1LL;
     tasks = (int)((n32 + per - 1) / per);
-    const bool avx2 = have_avx2();
+    const bool avx2 = have_avx2(), avx512 = have_avx512() && !std::getenv("SHMAP_PACK_AVX2");
+    const bool aligned = ((uintptr_t)codes & 15) == 0;
     std::vector<MaskList>& lists = task_lists();
     if (SPARSE) {
         if ((int)lists.size() < tasks + 1) lists.resize(tasks + 1);
@@ -233,7 +282,14 @@ static std::function<void(int)> pack_tasks(const uint8_t* seq, int64_t nb, uint3
     MaskList* L = lists.data();
     return [=](int t) {
         const int64_t g0 = per * t, g1 = std::min(n32, g0 + per);
-        if (avx2)
+        if (avx512) {
+            const int64_t ge = g0 + ((g1 - g0) & ~1LL);  // pairs of groups; an odd last one by AVX2
+            pack_range_avx512<SPARSE>(seq + 32 * g0, ge - g0, codes + 2 * g0, SPARSE ? nullptr : mask + g0, g0,
+                                      SPARSE ? L + t : nullptr, aligned);
+            if (ge < g1)
+                pack_range_avx2<SPARSE>(seq + 32 * ge, g1 - ge, codes + 2 * ge, SPARSE ? nullptr : mask + ge, ge,
+                                        SPARSE ? L + t : nullptr);
+        } else if (avx2)
             pack_range_avx2<SPARSE>(seq + 32 * g0, g1 - g0, codes + 2 * g0, SPARSE ? nullptr : mask + g0, g0,
                                     SPARSE ? L + t : nullptr);
         else

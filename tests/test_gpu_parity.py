@@ -296,13 +296,22 @@ def test_device_resident_entry(gpu_ctx, uniform):
     assert not record_mismatches(rec, want)
 
 
-@pytest.mark.parametrize("env", [{"SHMAP_BT_FAST_SLOTS": "16"}, {"SHMAP_FAST_JOB_CAP": "7"},
-                                 {"SHMAP_BT_FAST_SLOTS": "32", "SHMAP_FAST_JOB_CAP": "40"}])
+@pytest.mark.parametrize("env", [{"SHMAP_BT_FAST_SLOTS": "16", "SHMAP_BT_SPARE_SLOTS": "0"},
+                                 {"SHMAP_BT_FAST_SLOTS": "16"},
+                                 {"SHMAP_BT_FAST_SLOTS": "16", "SHMAP_BT_SPARE_SLOTS": "4096"},
+                                 {"SHMAP_FAST_JOB_CAP": "7"},
+                                 {"SHMAP_BT_FAST_SLOTS": "32", "SHMAP_FAST_JOB_CAP": "40"},
+                                 {"SHMAP_BT_FAST_SLOTS": "16", "SHMAP_BT_FAST_READ": "4096",
+                                  "SHMAP_BT_SPARE_SLOTS": "0"},
+                                 {"SHMAP_BT_FAST_SLOTS": "16", "SHMAP_BT_FAST_READ": "4096"}])
 def test_capacity_fallbacks(gpu_ctx, human_small, env, monkeypatch):
     """Batches are queued without waiting for their sizes: bucket tables are
-    capped per read (a read whose table fills is mapped again with the full
-    bound) and bucket jobs per batch (a batch with more is mapped again with
-    exact sizes). Tiny caps force both paths; the records must not change."""
+    capped per read and share a pool; a read whose table fills up (or would
+    end past the pool) gets a second table from spare slots and contributes
+    again, and is mapped again by the host with the full bound when that
+    fills up or there is no room; bucket jobs per batch are capped (a batch
+    with more is mapped again with exact sizes). Tiny caps, pools and spares
+    force every path; the records must not change."""
     for key, val in env.items():
         monkeypatch.setenv(key, val)
     gen = human_small

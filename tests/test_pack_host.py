@@ -1,7 +1,8 @@
 """Host packing of reads (shmap-rs_b200/host/pack.cpp): 2-bit codes and the
 non-ACGT mask the host-buffer path uploads, checked against a numpy model
 of the definition on every byte value, both cases and ragged lengths; the
-AVX2 form and the scalar form must agree bit for bit."""
+AVX-512 form (where the CPU has it), the AVX2 form (SHMAP_PACK_AVX2) and the
+scalar form must agree bit for bit."""
 import ctypes
 
 import numpy as np
@@ -45,8 +46,11 @@ def _pack(seq: np.ndarray, scalar: int):
     return codes, mask
 
 
-@pytest.mark.parametrize("nb", [0, 1, 31, 32, 33, 64, 1000, 1 << 16, (1 << 20) + 7])
-def test_pack_matches_model(nb):
+@pytest.mark.parametrize("avx2", [False, True])
+@pytest.mark.parametrize("nb", [0, 1, 31, 32, 33, 64, 95, 1000, 1 << 16, (1 << 20) + 7, (1 << 21) + 40])
+def test_pack_matches_model(nb, avx2, monkeypatch):
+    if avx2:
+        monkeypatch.setenv("SHMAP_PACK_AVX2", "1")
     rng = np.random.default_rng(nb + 1)
     # mostly bases of both cases, with every other byte value sprinkled in
     seq = rng.choice(np.frombuffer(b"ACGTacgt", np.uint8), nb)
@@ -60,7 +64,10 @@ def test_pack_matches_model(nb):
         assert np.array_equal(c, want_c), scalar
 
 
-def test_pack_every_byte_value():
+@pytest.mark.parametrize("avx2", [False, True])
+def test_pack_every_byte_value(avx2, monkeypatch):
+    if avx2:
+        monkeypatch.setenv("SHMAP_PACK_AVX2", "1")
     seq = np.tile(np.arange(256, dtype=np.uint8), 40)  # 10240 bytes, every value at every offset mod 32
     want_c, want_m = _model(seq)
     for scalar in (0, 1):
