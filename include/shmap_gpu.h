@@ -198,7 +198,10 @@ int shm_format_paf_device(shm_ctx* ctx, const shm_index* idx, const shm_params* 
  * the next batches. out (may be NULL) gets the records too. *n_out = the
  * text's length; at most cap bytes go to buf (NULL only measures, after
  * mapping everything); SHM_ERR_CAPACITY when the text exceeds cap. Pinned
- * seqs, out and buf keep every copy asynchronous. */
+ * seqs, out and buf keep every copy asynchronous: a pinned buf receives each
+ * batch's text while later batches map, and pinned seqs let a share of the
+ * batches go up as bytes (the host_raw_share setting). The names are split
+ * and uploaded by a helper thread while the first batch is packed. */
 int shm_map_paf(shm_ctx* ctx, const shm_index* idx, const shm_params* p, const uint8_t* seqs, const int64_t* offs,
                 int32_t n, const char* names, shm_map_record* out, char* buf, int64_t cap, int64_t* n_out);
 

@@ -3968,15 +3968,34 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         S.pk_list[k].reserve(2 * mwords);
     }
     S.out.reserve((size_t)std::max(max_n, 1));
+    // a share of the batches (host_raw_share percent, spread evenly) goes up as
+    // ASCII straight from the caller's buffer when that is pinned: the copy
+    // engine reads 1 byte a base where packing reads 1, writes 1/4 and the
+    // copy engine reads that 1/4, so moving a share off the host threads eases
+    // the host's memory bandwidth while the link takes more bytes
+    int64_t raw_pct = tuning().host_raw_share;
+    if (raw_pct > 0) {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, seqs) != cudaSuccess || pa.type != cudaMemoryTypeHost) {
+            cudaGetLastError();
+            raw_pct = 0;
+        }
+    }
+    std::vector<char> raw(batches.size(), 0);
+    for (size_t b = 0; b < batches.size(); b++)
+        raw[b] = ((int64_t)(b + 1) * raw_pct / 100) > ((int64_t)b * raw_pct / 100);
+    for (int k = 0; k < 2 && raw_pct > 0; k++) S.seqb[k].reserve((size_t)max_nb + 32);
     auto h_codes = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes); };
     auto h_list = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes + 4 * cwords); };
     auto pack = [&](size_t b) {  // on the host threads in the background, once the slot's previous upload left
+        if (raw[b]) return;
         const auto [i, j] = batches[b];
         SHM_CUDA(cudaEventSynchronize(c->copied[b & 1]));
         pack_reads_host_start(seqs + offs[i], offs[j] - offs[i], h_codes(b));
     };
     size_t n_list = 0;  // nonzero mask words of the packing just waited for
     auto wait = [&](size_t b) {
+        if (raw[b]) return;
         const auto [i, j] = batches[b];
         n_list = pack_reads_host_wait(h_list(b), packed_mask_words(offs[j] - offs[i]));
     };
@@ -3985,6 +4004,12 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         const int64_t nb = offs[j] - offs[i];
         cudaStream_t cs = c->copy_stream;
         SHM_CUDA(cudaStreamWaitEvent(cs, c->sketched[b & 1], 0));
+        if (raw[b]) {  // the bytes as they are, and the zero pad the sketch reads past the end
+            copy_async(c, S.seqb[b & 1].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, cs);
+            SHM_CUDA(cudaMemsetAsync(S.seqb[b & 1].p + nb, 0, 32, cs));
+            SHM_CUDA(cudaEventRecord(c->copied[b & 1], cs));
+            return;
+        }
         copy_async(c, S.pk_codes[b & 1].p, h_codes(b), 4 * packed_code_words(nb), cudaMemcpyHostToDevice,
                                  cs);
         SHM_CUDA(cudaMemsetAsync(S.pk_mask[b & 1].p, 0, 4 * packed_mask_words(nb), cs));
@@ -4016,8 +4041,11 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
         const auto [i, j] = batches[b];
         SHM_CUDA(cudaStreamWaitEvent(s, c->copied[b & 1], 0));
         c->sketch_done = c->sketched[b & 1];
-        run_batch(c, ix, p, nullptr, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b],
-                  S.pk_codes[b & 1].p, S.pk_mask[b & 1].p);
+        if (raw[b])
+            run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b]);
+        else
+            run_batch(c, ix, p, nullptr, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b],
+                      S.pk_codes[b & 1].p, S.pk_mask[b & 1].p);
         c->sketch_done = nullptr;
         if (sink) sink->batch(i, j, S.out.p, s);
         copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
@@ -4027,6 +4055,7 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
             send(b + 1);
             if (b + 2 < batches.size()) pack(b + 2);
         }
+        if (sink) sink->poll();
     }
     H.mark("enqueue");
     SHM_CUDA(cudaStreamSynchronize(s));

@@ -119,6 +119,8 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
 // with their records at d_rec (device) valid for work queued on stream s.
 struct BatchSink {
     virtual void batch(int32_t i, int32_t j, const shm_map_record* d_rec, cudaStream_t s) = 0;
+    // called between batches: work that waits for earlier batches, without blocking
+    virtual void poll() {}
     virtual ~BatchSink() = default;
 };
 

@@ -16,6 +16,9 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <thread>
+#include <functional>
+#include <exception>
 
 #include "shm_common.cuh"
 #include "shm_internal.hpp"
@@ -308,9 +311,18 @@ __global__ void k_paf_write_at(PafView v, const uint64_t* __restrict__ off, cons
 }
 
 // The text of the batch just written moves the base past it.
-__global__ void k_paf_advance(uint64_t* __restrict__ base, const uint64_t* __restrict__ off, int32_t n) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) *base += off[n];
+__global__ void k_paf_advance(uint64_t* __restrict__ base, const uint64_t* __restrict__ off, int32_t n,
+                              uint64_t* __restrict__ range) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint64_t a = *base;
+        *base = a + off[n];
+        if (range) {  // the batch's text span
+            range[0] = a;
+            range[1] = a + off[n];
+        }
+    }
 }
+
 
 }  // namespace
 
@@ -325,9 +337,28 @@ struct PafScratch {
     shm_map_record* h_rec = nullptr;  // pinned records of shm_map_paf calls that pass none
     size_t h_rec_cap = 0;
     uint64_t* h_small = nullptr;  // pinned readback: text length, overflow flag
+    DevBuf<uint64_t> ranges;      // per batch of a shm_map_paf call: its text span
+    cudaStream_t ns = nullptr;    // the names' upload of a shm_map_paf call, beside its first batch
+    cudaEvent_t nev = nullptr;
+    int64_t names_h2d = 0;        // bytes of the last names upload
+    uint64_t* h_ranges = nullptr; // the text spans, pinned, read once the batch's event completes
+    size_t h_ranges_cap = 0;      // (pairs)
+    std::vector<cudaEvent_t> evs; // one per batch in flight
+    cudaStream_t ts = nullptr;    // the text's copies to the caller's buffer, batch by batch
     ~PafScratch() {
         if (h_rec) cudaFreeHost(h_rec);
         if (h_small) cudaFreeHost(h_small);
+        if (ts) {
+            cudaStreamSynchronize(ts);
+            cudaStreamDestroy(ts);
+        }
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+        if (h_ranges) cudaFreeHost(h_ranges);
+        if (ns) {
+            cudaStreamSynchronize(ns);
+            cudaStreamDestroy(ns);
+        }
+        if (nev) cudaEventDestroy(nev);
     }
 };
 
@@ -339,12 +370,35 @@ static PafScratch& paf_scratch(MapCtx* c) {
 }
 
 // Query names split on '\n' as shm_format_paf does (name i is q[qse[2i],
-// qse[2i+1])), the segment names joined with their offsets, all uploaded on
-// stream s; returns the view of them (records, count and map times unset).
-static PafView upload_names(MapCtx* c, PafScratch& P, const IndexStorage& ix, const shm_params& p, int32_t n,
-                            const char* names, cudaStream_t s) {
+// qse[2i+1])), the segment names joined with their offsets. names_view
+// sizes the device buffers and returns the view of them (records, count and
+// map times unset); names_upload fills them on stream s (the host work: a
+// scan of the names and pageable copies), from any host thread.
+static PafView names_view(PafScratch& P, const IndexStorage& ix, const shm_params& p, int32_t n, size_t qlen) {
+    size_t sn = 0;
+    for (const std::string& x : ix.names) sn += x.size();
+    P.q.reserve(qlen + 1);
+    P.sn.reserve(sn + 1);
+    P.qse.reserve(2 * (size_t)n + 1);
+    P.soff.reserve(ix.names.size() + 1);
+    P.slen.reserve(ix.seg_len.size() + 1);
+    P.len.reserve((size_t)n + 1);
+    P.off.reserve((size_t)n + 1);
+    PafView v{};
+    v.qnames = P.q.p;
+    v.qse = P.qse.p;
+    v.snames = P.sn.p;
+    v.soff = P.soff.p;
+    v.slen = P.slen.p;
+    v.k = p.k;
+    v.theta = p.theta;
+    v.min_diff = p.min_diff;
+    return v;
+}
+
+static void names_upload(MapCtx* c, PafScratch& P, const IndexStorage& ix, int32_t n, const char* names, size_t qlen,
+                         cudaStream_t s) {
     const char* q = names ? names : "";
-    const size_t qlen = std::strlen(q);
     std::vector<int64_t> qse(2 * (size_t)n + 1, 0);
     for (size_t i = 0, at = 0; i < (size_t)n; i++) {
         const char* e = (const char*)std::memchr(q + at, '\n', qlen - at);
@@ -359,13 +413,6 @@ static PafView upload_names(MapCtx* c, PafScratch& P, const IndexStorage& ix, co
         sn += x;
         soff.push_back((int64_t)sn.size());
     }
-    P.q.reserve(qlen + 1);
-    P.sn.reserve(sn.size() + 1);
-    P.qse.reserve(qse.size());
-    P.soff.reserve(soff.size());
-    P.slen.reserve(ix.seg_len.size() + 1);
-    P.len.reserve((size_t)n + 1);
-    P.off.reserve((size_t)n + 1);
     if (qlen) SHM_CUDA(cudaMemcpyAsync(P.q.p, q, qlen, cudaMemcpyHostToDevice, s));
     if (!sn.empty()) SHM_CUDA(cudaMemcpyAsync(P.sn.p, sn.data(), sn.size(), cudaMemcpyHostToDevice, s));
     SHM_CUDA(cudaMemcpyAsync(P.qse.p, qse.data(), sizeof(int64_t) * qse.size(), cudaMemcpyHostToDevice, s));
@@ -373,18 +420,18 @@ static PafView upload_names(MapCtx* c, PafScratch& P, const IndexStorage& ix, co
     if (!ix.seg_len.empty())
         SHM_CUDA(cudaMemcpyAsync(P.slen.p, ix.seg_len.data(), sizeof(int32_t) * ix.seg_len.size(),
                                  cudaMemcpyHostToDevice, s));
-    // the query and segment names and their offset tables
-    c->work[W_H2D_BYTES] += (int64_t)(qlen + sn.size() + sizeof(int64_t) * (qse.size() + soff.size()) +
-                                      sizeof(int32_t) * ix.seg_len.size());
-    PafView v{};
-    v.qnames = P.q.p;
-    v.qse = P.qse.p;
-    v.snames = P.sn.p;
-    v.soff = P.soff.p;
-    v.slen = P.slen.p;
-    v.k = p.k;
-    v.theta = p.theta;
-    v.min_diff = p.min_diff;
+    // the query and segment names and their offset tables (counted by the caller's thread)
+    P.names_h2d = (int64_t)(qlen + sn.size() + sizeof(int64_t) * (qse.size() + soff.size()) +
+                            sizeof(int32_t) * ix.seg_len.size());
+}
+
+// Both, on stream s.
+static PafView upload_names(MapCtx* c, PafScratch& P, const IndexStorage& ix, const shm_params& p, int32_t n,
+                            const char* names, cudaStream_t s) {
+    const size_t qlen = std::strlen(names ? names : "");
+    PafView v = names_view(P, ix, p, n, qlen);
+    names_upload(c, P, ix, n, names, qlen, s);
+    c->work[W_H2D_BYTES] += P.names_h2d;
     return v;
 }
 
@@ -436,9 +483,18 @@ struct PafSink : BatchSink {
     PafScratch* P;
     PafView v0;
     uint64_t cap;
+    char* hbuf = nullptr;  // the caller's buffer when it is pinned (each batch's text copied as it is done)
+    uint64_t hcap = 0;
+    int32_t nb = 0;        // batches rendered
+    int32_t ncopied = 0;   // batches whose text copy is queued
+    std::function<void()> names_ready;  // waits for the names' upload (once, before the first kernel)
     void batch(int32_t i, int32_t j, const shm_map_record* d_rec, cudaStream_t s) override {
         const int32_t n = j - i;
         if (n <= 0) return;
+        if (names_ready) {
+            names_ready();
+            names_ready = nullptr;
+        }
         PafView v = v0;
         v.rec = d_rec;
         v.n = n;
@@ -451,11 +507,59 @@ struct PafSink : BatchSink {
                                                                    P->flag.p);
         SHM_CUDA(cudaGetLastError());
         count_launch();
-        k_paf_advance<<<1, 32, 0, s>>>(P->base.p, P->off.p, n);
+        uint64_t* range = hbuf ? P->ranges.p + 2 * (size_t)nb : nullptr;
+        k_paf_advance<<<1, 32, 0, s>>>(P->base.p, P->off.p, n, range);
         SHM_CUDA(cudaGetLastError());
         count_launch();
+        if (hbuf) {  // the batch's text span, read back; its copy is queued by poll() once known
+            SHM_CUDA(cudaMemcpyAsync(P->h_ranges + 2 * (size_t)nb, range, 2 * sizeof(uint64_t),
+                                     cudaMemcpyDeviceToHost, s));
+            if ((size_t)nb >= P->evs.size()) {
+                cudaEvent_t e;
+                SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                P->evs.push_back(e);
+            }
+            SHM_CUDA(cudaEventRecord(P->evs[(size_t)nb], s));
+        }
+        nb++;
+    }
+    // the text of every finished batch to the caller's buffer, on the text
+    // stream (the copy engine, beside the uploads of later batches)
+    void copy_batch(int32_t b) {
+        const uint64_t a = P->h_ranges[2 * (size_t)b], e = std::min(P->h_ranges[2 * (size_t)b + 1], hcap);
+        if (e > a) SHM_CUDA(cudaMemcpyAsync(hbuf + a, P->text.p + a, (size_t)(e - a), cudaMemcpyDeviceToHost, P->ts));
+    }
+    void poll() override {
+        while (hbuf && ncopied < nb) {
+            const cudaError_t q = cudaEventQuery(P->evs[(size_t)ncopied]);
+            if (q == cudaErrorNotReady) return;
+            SHM_CUDA(q);
+            copy_batch(ncopied++);
+        }
+    }
+    void finish() {
+        while (hbuf && ncopied < nb) {
+            SHM_CUDA(cudaEventSynchronize(P->evs[(size_t)ncopied]));
+            copy_batch(ncopied++);
+        }
+        if (hbuf) SHM_CUDA(cudaStreamSynchronize(P->ts));
+    }
+    ~PafSink() override {  // no copy into the caller's buffer outlives the call (an error path)
+        if (hbuf) cudaStreamSynchronize(P->ts);
     }
 };
+
+// True for a pinned (page-locked) host buffer, which copies can fill
+// asynchronously.
+bool pinned_host(const char* buf) {
+    if (!buf) return false;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, buf) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
 
 }  // namespace
 
@@ -477,7 +581,35 @@ int64_t map_paf_host(MapCtx* c, const IndexStorage& ix, const shm_params& p, con
         rec = P.h_rec;
     }
     if (!P.h_small) SHM_CUDA(cudaHostAlloc(&P.h_small, 2 * sizeof(uint64_t), cudaHostAllocDefault));
-    PafView v = upload_names(c, P, ix, p, n, names, s);
+    HostClock H;
+    // the names go up from a helper thread on their own stream while the
+    // first batch is packed; the sink joins it before its first kernel
+    const size_t qlen = std::strlen(names ? names : "");
+    PafView v = names_view(P, ix, p, n, qlen);
+    if (!P.ns) SHM_CUDA(cudaStreamCreateWithFlags(&P.ns, cudaStreamNonBlocking));
+    if (!P.nev) SHM_CUDA(cudaEventCreateWithFlags(&P.nev, cudaEventDisableTiming));
+    std::exception_ptr names_err;
+    std::thread names_th([&] {
+        try {
+            SHM_CUDA(cudaSetDevice(c->device));
+            names_upload(c, P, ix, n, names, qlen, P.ns);
+            SHM_CUDA(cudaEventRecord(P.nev, P.ns));
+        } catch (...) {
+            names_err = std::current_exception();
+        }
+    });
+    struct Join {  // joined on every path out of this function
+        std::thread& t;
+        ~Join() {
+            if (t.joinable()) t.join();
+        }
+    } names_join{names_th};
+    auto names_ready = [&] {
+        if (names_th.joinable()) names_th.join();
+        if (names_err) std::rethrow_exception(names_err);
+        SHM_CUDA(cudaStreamWaitEvent(s, P.nev, 0));
+    };
+    H.mark("names");
     v.map_time = nullptr;
     // room for every line: a line is its query name, a segment name and at
     // most about 700 bytes of numbers and tags (t:f: is 0 here); a line that
@@ -495,20 +627,44 @@ int64_t map_paf_host(MapCtx* c, const IndexStorage& ix, const shm_params& p, con
     sink.P = &P;
     sink.v0 = v;
     sink.cap = tcap;
+    sink.names_ready = names_ready;
+    // a pinned caller buffer takes each batch's text as soon as it is written
+    sink.hbuf = cap > 0 && pinned_host(buf) ? buf : nullptr;
+    sink.hcap = sink.hbuf ? (uint64_t)cap : 0;
+    if (sink.hbuf) {
+        if (!P.ts) SHM_CUDA(cudaStreamCreateWithFlags(&P.ts, cudaStreamNonBlocking));
+        P.ranges.reserve(2 * ((size_t)n + 1));
+        if (P.h_ranges_cap < (size_t)n + 1) {
+            if (P.h_ranges) SHM_CUDA(cudaFreeHost(P.h_ranges));
+            P.h_ranges = nullptr;
+            P.h_ranges_cap = 0;
+            SHM_CUDA(cudaHostAlloc((void**)&P.h_ranges, 2 * sizeof(uint64_t) * ((size_t)n + 1), cudaHostAllocDefault));
+            P.h_ranges_cap = (size_t)n + 1;
+        }
+    }
     const bool changed = map_host(c, &ix, p, seqs, offs, n, rec, false, &sink);
+    names_ready();  // (no batch: n = 0)
+    c->work[W_H2D_BYTES] += P.names_h2d;
+    H.mark("map");
+    sink.finish();  // (a fallback below writes buf again)
     if (changed)  // records replaced after their batch's text was written: render from the final records
         return format_paf_device(c, ix, p, rec, n, names, nullptr, buf, cap);
     SHM_CUDA(cudaMemcpyAsync(P.h_small, P.base.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaMemcpyAsync(P.h_small + 1, P.flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     SHM_CUDA(cudaStreamSynchronize(s));
+    H.mark("sync");
     if ((uint32_t)P.h_small[1] != 0) return format_paf_device(c, ix, p, rec, n, names, nullptr, buf, cap);
     const int64_t total = (int64_t)P.h_small[0];
     if (buf && cap > 0 && total > 0) {
         const int64_t take = std::min(cap, total);
-        SHM_CUDA(cudaMemcpyAsync(buf, P.text.p, (size_t)take, cudaMemcpyDeviceToHost, s));
+        if (!sink.hbuf) {
+            SHM_CUDA(cudaMemcpyAsync(buf, P.text.p, (size_t)take, cudaMemcpyDeviceToHost, s));
+            SHM_CUDA(cudaStreamSynchronize(s));
+        }
         c->work[W_D2H_BYTES] += take;
-        SHM_CUDA(cudaStreamSynchronize(s));
     }
+    H.mark("text");
+    H.print("paf", n);
     return total;
 }
 

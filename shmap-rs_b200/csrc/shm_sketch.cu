@@ -363,7 +363,9 @@ __device__ __forceinline__ bool sketch_run_frame(const SketchArgs& a, const PkTa
     }
     F = rotl64(F, 1);  // the frame at t = -1
     R = rotr64(R, 1);
-    uint32_t Flo = (uint32_t)F, Fhi = (uint32_t)(F >> 32), Rlo = (uint32_t)R, Rhi = (uint32_t)(R >> 32);
+    // the frame state as one register quad (F~ low, high; R~ low, high): a
+    // passing window stores it with one 16-byte store, no moves
+    uint4 st = make_uint4((uint32_t)F, (uint32_t)(F >> 32), (uint32_t)R, (uint32_t)(R >> 32));
     const uint32_t thr_hi = (uint32_t)(thr >> 32);
     // entering bytes from x + k - 1, leaving bytes from x - 1
     const int bi = x + k - 1, bo = x - 1;
@@ -391,13 +393,13 @@ __device__ __forceinline__ bool sketch_run_frame(const SketchArgs& a, const PkTa
                 const uint32_t off = __byte_perm(comb, 0u, 0x4440u + (uint32_t)j);
                 const uint2 ef = *(const uint2*)((const char*)&P.pf[jj][0] + off);
                 const uint2 er = *(const uint2*)((const char*)&P.pr[jj][0] + off);
-                Flo ^= ef.x;
-                Fhi ^= ef.y;
-                Rlo ^= er.x;
-                Rhi ^= er.y;
-                const uint32_t hh = __funnelshift_l(Flo, Fhi, jj) ^ __funnelshift_r(Rhi, Rlo, jj);
+                st.x ^= ef.x;
+                st.y ^= ef.y;
+                st.z ^= er.x;
+                st.w ^= er.y;
+                const uint32_t hh = __funnelshift_l(st.x, st.y, jj) ^ __funnelshift_r(st.w, st.z, jj);
                 if (hh <= thr_hi) {
-                    buf[n & (FR_CAP - 1)] = make_uint4(Flo, Fhi, Rlo, Rhi);
+                    buf[n & (FR_CAP - 1)] = st;
                     n++;
                     mg |= 1u << jj;
                 }
@@ -408,12 +410,7 @@ __device__ __forceinline__ bool sketch_run_frame(const SketchArgs& a, const PkTa
         m1 = m0;
         m0 = mg;
         groups++;
-        uint32_t y = Flo;  // rotation by 32: the next group's rows apply to the swapped halves
-        Flo = Fhi;
-        Fhi = y;
-        y = Rlo;
-        Rlo = Rhi;
-        Rhi = y;
+        st = make_uint4(st.y, st.x, st.w, st.z);  // rotation by 32: the next group's rows apply to the swapped halves
     }
     if (bad != 0 || n > (uint32_t)FR_CAP) return false;
     // the passing windows in order: group g's mask is m_(groups - 1 - g)
@@ -433,6 +430,21 @@ __device__ __forceinline__ bool sketch_run_frame(const SketchArgs& a, const PkTa
         }
     }
     return true;
+}
+
+// The last i in [0, n) with off[i] <= key (off[0] = 0 <= key), by one warp:
+// each step tests 32 evenly spaced places at once, so n = 2^17 sequences
+// take four dependent loads instead of seventeen.
+__device__ __forceinline__ int32_t warp_last_le(const uint64_t* __restrict__ off, int32_t n, uint64_t key, int lane) {
+    int32_t lo = 0, hi = n;  // the answer lies in [lo, hi)
+    while (hi - lo > 1) {
+        const int32_t step = (hi - lo + 31) / 32;
+        const int32_t i = lo + lane * step;
+        const unsigned b = __ballot_sync(0xffffffffu, i < hi && __ldg(off + i) <= key);  // bit 0 is set
+        lo += (31 - __clz(b)) * step;
+        hi = min(hi, lo + step);
+    }
+    return lo;
 }
 
 // Dynamic shared memory of a k_sketch CTA: the staged tile.
@@ -476,15 +488,9 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch(SketchArgs a, const Sketc
     for (uint64_t tl = blockIdx.x; tl < n_tiles; tl += gridDim.x) {
         const uint64_t c0 = tl * SK_THREADS, c = c0 + threadIdx.x;
         const uint64_t c_last = min(c0 + SK_THREADS, n_chunks) - 1;
-        if (threadIdx.x == 0 || threadIdx.x == 32) {  // sequences of the tile's first and last runs
-            const uint64_t cc = threadIdx.x == 0 ? c0 : c_last;
-            int32_t lo = 0, hi = a.n_seq;  // upper_bound over chunk_off
-            while (hi - lo > 1) {
-                const int32_t mid = (lo + hi) >> 1;
-                if (__ldg(a.chunk_off + mid) <= cc) lo = mid;
-                else hi = mid;
-            }
-            s_q[threadIdx.x == 0 ? 0 : 1] = lo;
+        if (threadIdx.x < 64) {  // sequences of the tile's first and last runs: warps 0 and 1
+            const int32_t lo = warp_last_le(a.chunk_off, a.n_seq, threadIdx.x < 32 ? c0 : c_last, lane);
+            if (lane == 0) s_q[threadIdx.x < 32 ? 0 : 1] = lo;
         }
         __syncthreads();
         int32_t q = 0, cnt = 0;
@@ -757,15 +763,9 @@ __global__ void __launch_bounds__(SK_THREADS) k_sketch_pk(SketchArgs a, const Sk
     for (uint64_t tl = blockIdx.x; tl < n_tiles; tl += gridDim.x) {
         const uint64_t c0 = tl * SK_THREADS, c = c0 + threadIdx.x;
         const uint64_t c_last = min(c0 + SK_THREADS, n_chunks) - 1;
-        if (threadIdx.x == 0 || threadIdx.x == 32) {  // sequences of the tile's first and last runs
-            const uint64_t cc = threadIdx.x == 0 ? c0 : c_last;
-            int32_t lo = 0, hi = a.n_seq;
-            while (hi - lo > 1) {
-                const int32_t mid = (lo + hi) >> 1;
-                if (__ldg(a.chunk_off + mid) <= cc) lo = mid;
-                else hi = mid;
-            }
-            s_q[threadIdx.x == 0 ? 0 : 1] = lo;
+        if (threadIdx.x < 64) {  // sequences of the tile's first and last runs: warps 0 and 1
+            const int32_t lo = warp_last_le(a.chunk_off, a.n_seq, threadIdx.x < 32 ? c0 : c_last, lane);
+            if (lane == 0) s_q[threadIdx.x < 32 ? 0 : 1] = lo;
         }
         __syncthreads();  // also: the tables are built
         int32_t q = 0, cnt = 0;

@@ -36,6 +36,7 @@ const Knob KNOBS[] = {
     {"wide_ctas_per_sm", &Tuning::wide_ctas_per_sm, 1, 8},
     {"refine_warps_per_sm", &Tuning::refine_warps_per_sm, 8, 64},
     {"device_pack", &Tuning::device_pack, 0, 1},
+    {"host_raw_share", &Tuning::host_raw_share, 0, 100},
 };
 
 std::mutex g_mu;

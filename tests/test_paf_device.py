@@ -4,6 +4,7 @@ same bytes for the mapped reads of all four metrics, for the golden fixture,
 and for records whose f64 fields are ties at the printed precision (1/64 at
 five places, 1/16 at three), NaN, infinities, negative zero, subnormals,
 huge values and random doubles; a short buffer gives SHM_ERR_CAPACITY."""
+import ctypes
 import os
 
 import numpy as np
@@ -125,3 +126,39 @@ def test_map_paf(gpu_ctx, monkeypatch, metric, env):
     assert r2 is None and t2 == g.format_paf(p, rec[:3], names[:3])
     t0, _ = g.map_paf(p, seq[:0], offs[:1], [])
     assert t0 == ""
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("env", [{}, {"SHMAP_FAST_JOB_CAP": "7"}])
+def test_map_paf_pinned_buffer(gpu_ctx, monkeypatch, env):
+    """Into a pinned, aligned caller buffer shm_map_paf writes each batch's
+    text through the buffer's device mapping while later batches map; the
+    bytes equal those written into pageable memory, also at an offset of one
+    byte (no mapping used), with a capacity short of the text (its first cap
+    bytes), and when batches are mapped again (the call renders from the
+    final records)."""
+    import torch
+
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    gen = synth.Genome(synth.REFS["uniform5m"])
+    names, seq, offs = gen.reads(synth.scaled(synth.READS["fixed10k"], 2.5))  # 5,000 reads
+    g = sb.SketchIndex.from_records(gpu_ctx, gen.records(), 25, 0.01)
+    p = sb.Params(k=25, h_frac=0.01, theta=0.4)
+    want, _ = g.map_paf(p, seq, offs, names)
+    want_b = want.encode()
+    seq = np.ascontiguousarray(seq, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.int64)
+    joined = "\n".join(names).encode()
+    cp = p.c()
+    pin = torch.zeros(len(want_b) + 64, dtype=torch.uint8).pin_memory()
+    base = pin.data_ptr()
+    for shift, cap in ((0, len(want_b) + 32), (1, len(want_b) + 32), (0, len(want_b) // 3)):
+        pin.fill_(0)
+        need = ctypes.c_int64()
+        rc = sb.lib().shm_map_paf(gpu_ctx.h, g.h, ctypes.byref(cp), seq.ctypes.data, offs.ctypes.data, len(names),
+                                  joined, None, base + shift, cap, ctypes.byref(need))
+        assert need.value == len(want_b)
+        got = bytes(pin.numpy()[shift:shift + min(cap, need.value)])
+        assert got == want_b[:min(cap, need.value)], (shift, cap)
+        assert rc == (0 if cap >= need.value else sb.SHM_ERR_CAPACITY)

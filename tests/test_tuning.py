@@ -11,7 +11,8 @@ import pytest
 import shmap_b200 as sb
 
 KEYS = ["dev_batch_reads", "dev_batch_bases", "dev_first_batch_reads", "host_batch_reads", "host_batch_bases",
-        "host_first_batch_reads", "sketch_ctas_per_sm", "wide_ctas_per_sm", "refine_warps_per_sm", "device_pack"]
+        "host_first_batch_reads", "sketch_ctas_per_sm", "wide_ctas_per_sm", "refine_warps_per_sm", "device_pack",
+        "host_raw_share"]
 
 
 def _get(k):
@@ -81,3 +82,14 @@ def test_results_do_not_depend_on_the_settings(gpu_ctx, saved):
     g.map_reads_device(p, d_seq.data_ptr(), offs, d_out.data_ptr())
     torch.cuda.synchronize()
     assert not record_mismatches(d_out.cpu().numpy().view(sb.RECORD_DTYPE), want)
+    # reads in pinned host memory, a share of the batches sent up as ASCII
+    pin = torch.zeros(len(seq) + 32, dtype=torch.uint8).pin_memory()
+    pin[: len(seq)].copy_(torch.from_numpy(np.ascontiguousarray(seq)))
+    offs64 = np.ascontiguousarray(offs, dtype=np.int64)
+    cp = p.c()
+    for share in (40, 100):
+        assert L.shm_tuning_set(b"host_raw_share", share) == 0
+        out = np.zeros(len(names), sb.RECORD_DTYPE)
+        sb._check(L.shm_map_batch(gpu_ctx.h, g.h, ctypes.byref(cp), pin.data_ptr(), offs64.ctypes.data, len(names),
+                                  out.ctypes.data))
+        assert not record_mismatches(out, want), share
