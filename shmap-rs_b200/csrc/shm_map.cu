@@ -1090,13 +1090,12 @@ __device__ __forceinline__ int32_t seg_step(const DevIndex& I, uint32_t g, int32
     return seg;
 }
 
-// The hit work items [w, wend) (of one read or of consecutive reads), added
-// to their reads' bucket tables.
-__device__ __forceinline__ void contrib_span(const BatchView& v, uint64_t w, const uint64_t wend) {
+// The hit work items [w, wend) (of one read or of consecutive reads, the
+// first of them read q), added to their reads' bucket tables.
+__device__ __forceinline__ void contrib_span(const BatchView& v, uint64_t w, const uint64_t wend, int32_t q) {
     const bool ap = v.P.ap != 0;
     const bool sh_out = bucket_metric(v.P);  // codirection and positions are reported (bucket metrics)
     const DevIndex& I = v.I;
-    int32_t q = (int32_t)ub_u64(v.hw_off, (uint32_t)v.n + 1, w) - 1;
     uint64_t kb = v.kcap_off[q];
     uint32_t np = (uint32_t)v.r_nproc[q];
     uint32_t h = (uint32_t)v.r_half[q];
@@ -1196,10 +1195,18 @@ __device__ __forceinline__ void contrib_span(const BatchView& v, uint64_t w, con
 __global__ void __launch_bounds__(256) k_contrib(BatchView v) {
     const uint64_t total = v.hw_off[v.n];
     const uint64_t nrun = (total + CONTRIB_RUN - 1) / CONTRIB_RUN;
-    for (uint64_t rn = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; rn < nrun;
-         rn += (uint64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    // a warp takes 32 consecutive runs: the read of its first by a 32-way
+    // search, each lane's own by walking on from there (runs of one warp
+    // rarely cross more than a read or two)
+    for (uint64_t r0 = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); r0 < nrun;
+         r0 += (uint64_t)gridDim.x * blockDim.x) {
+        int32_t q = warp_last_le(v.hw_off, v.n + 1, r0 * CONTRIB_RUN, lane);
+        const uint64_t rn = r0 + (uint64_t)lane;
+        if (rn >= nrun) continue;
         const uint64_t w = rn * CONTRIB_RUN;
-        contrib_span(v, w, min(w + CONTRIB_RUN, total));
+        while (v.hw_off[q + 1] <= w) q++;
+        contrib_span(v, w, min(w + CONTRIB_RUN, total), q);
     }
 }
 
@@ -1263,7 +1270,7 @@ __global__ void __launch_bounds__(256) k_contrib2(BatchView v) {
         }
         const int32_t q = (int32_t)v.bt2_list[lo];
         const uint64_t w = v.hw_off[q] + (rn - v.bt2_off[lo]) * CONTRIB_RUN;
-        contrib_span(v, w, min(w + CONTRIB_RUN, v.hw_off[q + 1]));
+        contrib_span(v, w, min(w + CONTRIB_RUN, v.hw_off[q + 1]), q);
     }
 }
 
