@@ -483,8 +483,9 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
     }
 }
 
+constexpr int SEEDP_THREADS = 512;  // a CTA per read: one CTA an SM fits (160 KB of shared memory at P = 4096)
 template <bool GLOBAL>
-__global__ void __launch_bounds__(256) k_seedprep(BatchView v, const int32_t* __restrict__ list,
+__global__ void __launch_bounds__(SEEDP_THREADS) k_seedprep(BatchView v, const int32_t* __restrict__ list,
                                                   const uint32_t* __restrict__ n_list_d, uint32_t P, uint8_t* gscr,
                                                   size_t gscr_per_cta) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -3428,7 +3429,8 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
             SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
             c->seed_smem_set = (int)bytes;
         }
-        k_seedprep<false><<<grid_for((size_t)bp.n_cap_1024 * 256, 256, 1), 256, bytes, s2>>>(v, LB + 3 * (size_t)n,
+        k_seedprep<false><<<grid_for((size_t)bp.n_cap_1024 * SEEDP_THREADS, SEEDP_THREADS, 1), SEEDP_THREADS, bytes,
+                            s2>>>(v, LB + 3 * (size_t)n,
                                                                                                NB + 3, P, nullptr, 0);
         SHM_CUDA(cudaGetLastError());
         count_launch();
