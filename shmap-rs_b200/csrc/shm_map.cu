@@ -3111,9 +3111,9 @@ struct BatchSlot {
 };
 
 // The bucket tables of a batch mapped without waiting for its sizes get at
-// most 512 slots a read (twice the bound on the read's distinct buckets, as
-// in exact sizing, when that is less), laid out in read order in a pool of
-// 512 slots a read; a read whose table fills up gets a second table from
+// most bt_fast_slots slots a read (twice the bound on the read's distinct
+// buckets, as in exact sizing, when that is less), laid out in read order in
+// a pool of that many slots a read; a read whose table fills up gets a second table from
 // spare slots after the pool (k_bt_second), and is mapped again by the host
 // only when that fills up too or finds no room. A batch has at most 64
 // bucket jobs a read on average (a batch with more is mapped again). The
@@ -3128,7 +3128,9 @@ static uint64_t env_pow2(const char* name, uint64_t lo, uint64_t hi) {
 }
 static uint64_t fast_bt_slots() {
     const uint64_t v = env_pow2("SHMAP_BT_FAST_SLOTS", 16, 512);
-    return v ? v : 512;
+    if (v) return v;
+    const uint64_t t = (uint64_t)tuning().bt_fast_slots;  // a power of two in [16, 512] (rounded down)
+    return (uint64_t)1 << (63 - __builtin_clzll(t));
 }
 static uint64_t fast_bt_read_cap() {
     const uint64_t r = env_pow2("SHMAP_BT_FAST_READ", 16, 4096);
@@ -3144,7 +3146,8 @@ static uint64_t bt_spare_slots(int32_t n) {
 static uint32_t fast_job_cap(int32_t n) {
     const char* e = std::getenv("SHMAP_FAST_JOB_CAP");
     const uint64_t v = e ? std::strtoull(e, nullptr, 10) : 0;
-    const uint64_t cap = std::min<uint64_t>(fast_bt_slots() * (uint64_t)n + 1, 64 * (uint64_t)n + (1u << 20));
+    const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(fast_bt_slots(), 512) * (uint64_t)n + 1,
+                                            64 * (uint64_t)n + (1u << 20));
     return (uint32_t)(v >= 1 ? std::min(v, cap) : cap);
 }
 

@@ -37,6 +37,7 @@ const Knob KNOBS[] = {
     {"refine_warps_per_sm", &Tuning::refine_warps_per_sm, 8, 64},
     {"device_pack", &Tuning::device_pack, 0, 1},
     {"host_raw_share", &Tuning::host_raw_share, 0, 100},
+    {"bt_fast_slots", &Tuning::bt_fast_slots, 16, 512},
 };
 
 std::mutex g_mu;

@@ -16,6 +16,8 @@ struct Tuning {
     int64_t refine_warps_per_sm = 64; // refinement warps in flight per SM (global-table path)
     int64_t device_pack = 0;          // reads in device memory: 1 = packed there and sketched from codes,
                                       // 0 = sketched from their bytes
+    int64_t bt_fast_slots = 512;      // bucket-table slots a read (a power of two) when a batch is queued
+                                      // without waiting for its sizes; fuller tables take a second table
     int64_t host_raw_share = 0;       // reads in pinned host memory: the percent of batches sent up as
                                       // ASCII by the copy engine instead of packed on the host threads
 };

@@ -38,6 +38,7 @@ DEVICE_KNOBS = [
     ("refine_warps_per_sm", [16, 32, 48, 64]),
     ("dev_batch_reads", [16384, 32768, 65536, 131072, 262144]),
     ("dev_first_batch_reads", [1024, 4096, 16384, 65536]),
+    ("bt_fast_slots", [64, 128, 256, 512]),
 ]
 HOST_KNOBS = [
     ("host_batch_reads", [8192, 16384, 32768, 65536]),

@@ -12,7 +12,7 @@ import shmap_b200 as sb
 
 KEYS = ["dev_batch_reads", "dev_batch_bases", "dev_first_batch_reads", "host_batch_reads", "host_batch_bases",
         "host_first_batch_reads", "sketch_ctas_per_sm", "wide_ctas_per_sm", "refine_warps_per_sm", "device_pack",
-        "host_raw_share"]
+        "host_raw_share", "bt_fast_slots"]
 
 
 def _get(k):
@@ -70,7 +70,7 @@ def test_results_do_not_depend_on_the_settings(gpu_ctx, saved):
     L = sb.lib()
     for k, v in [("dev_batch_reads", 1024), ("dev_first_batch_reads", 64), ("host_batch_reads", 1024),
                  ("host_first_batch_reads", 100), ("sketch_ctas_per_sm", 1), ("wide_ctas_per_sm", 1),
-                 ("refine_warps_per_sm", 8), ("device_pack", 1)]:
+                 ("refine_warps_per_sm", 8), ("device_pack", 1), ("bt_fast_slots", 16)]:
         assert L.shm_tuning_set(k.encode(), v) == 0
     got = g.map_reads(p, seq, offs)
     assert not record_mismatches(got, want)
