@@ -1303,7 +1303,7 @@ __global__ void k_bt_init(BSlot* bt, const uint64_t* __restrict__ bt_off, int32_
 // the spare slots after the pool, emptied here, and is listed for k_contrib2
 // to contribute again; a read that finds no room stays flagged and is mapped
 // again by the host. A warp takes 32 reads, each flagged one in turn.
-constexpr uint64_t BT2_MAX = 32768;
+constexpr uint64_t BT2_MAX = 4096;  // (a read needing more climbs the host's ladder)
 __global__ void __launch_bounds__(256) k_bt_second(BatchView v) {
     const int lane = threadIdx.x & 31;
     const int32_t nwarps = (int32_t)((gridDim.x * blockDim.x) >> 5);
@@ -3136,12 +3136,15 @@ static uint64_t fast_bt_read_cap() {
     const uint64_t r = env_pow2("SHMAP_BT_FAST_READ", 16, 4096);
     return r ? r : fast_bt_slots();
 }
-// Spare slots for second tables: 16 a read and a million more
+// Spare slots for second tables: 1,024 a read and a million more, room for
+// a full-size second table for a quarter of a batch (at r = 0.10 a fifth of
+// the reads, those from satellite arrays, fill their first table); the spare
+// is only written where a second table is handed out
 // (SHMAP_BT_SPARE_SLOTS sets the number; 0 turns second tables off).
 static uint64_t bt_spare_slots(int32_t n) {
     const char* e = std::getenv("SHMAP_BT_SPARE_SLOTS");
     if (e) return std::strtoull(e, nullptr, 10);
-    return 16 * (uint64_t)n + ((uint64_t)1 << 20);
+    return 1024 * (uint64_t)n + ((uint64_t)1 << 20);
 }
 static uint32_t fast_job_cap(int32_t n) {
     const char* e = std::getenv("SHMAP_FAST_JOB_CAP");
