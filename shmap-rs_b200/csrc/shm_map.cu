@@ -327,7 +327,9 @@ __device__ __forceinline__ bool seed_prologue(const BatchView& v, int32_t q, uin
 
 // One CTA per read. Arrays (P = power of two >= the read's k-mer capacity):
 // A/B element keys, GA/GB group hash and occs<<1|strand, GF first index then
-// count(), GD hit-list start, E rarest-first sort keys.
+// count(), GD hit-list start, E rarest-first sort keys. A and B are dead once
+// the groups are formed, so E lives in A's place and GD in B's: 28 bytes an
+// element, two CTAs an SM at P = 4096.
 struct SeedArrays {
     uint64_t *A, *GA, *E;
     uint32_t *B, *GB, *GF, *GD;
@@ -337,14 +339,14 @@ __device__ SeedArrays carve(uint8_t* base, uint32_t P) {
     SeedArrays s;
     s.A = (uint64_t*)base;
     s.GA = s.A + P;
-    s.E = s.GA + P;
-    s.B = (uint32_t*)(s.E + P);
+    s.E = s.A;
+    s.B = (uint32_t*)(s.GA + P);
     s.GB = s.B + P;
     s.GF = s.GB + P;
-    s.GD = s.GF + P;
+    s.GD = s.B;
     return s;
 }
-constexpr size_t SEED_BYTES_PER_ELEM = 3 * 8 + 4 * 4;
+constexpr size_t SEED_BYTES_PER_ELEM = 2 * 8 + 3 * 4;
 
 __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const SeedArrays& S_) {
     __shared__ uint64_t sw64[32];
@@ -483,7 +485,7 @@ __device__ void seedprep_one(const BatchView& v, int32_t q, uint32_t P, const Se
     }
 }
 
-constexpr int SEEDP_THREADS = 512;  // a CTA per read: one CTA an SM fits (160 KB of shared memory at P = 4096)
+constexpr int SEEDP_THREADS = 512;  // a CTA per read: two CTAs an SM (112 KB of shared memory each at P = 4096)
 template <bool GLOBAL>
 __global__ void __launch_bounds__(SEEDP_THREADS) k_seedprep(BatchView v, const int32_t* __restrict__ list,
                                                   const uint32_t* __restrict__ n_list_d, uint32_t P, uint8_t* gscr,
@@ -3435,7 +3437,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
             SHM_CUDA(cudaFuncSetAttribute(k_seedprep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
             c->seed_smem_set = (int)bytes;
         }
-        k_seedprep<false><<<grid_for((size_t)bp.n_cap_1024 * SEEDP_THREADS, SEEDP_THREADS, 1), SEEDP_THREADS, bytes,
+        k_seedprep<false><<<grid_for((size_t)bp.n_cap_1024 * SEEDP_THREADS, SEEDP_THREADS, 2), SEEDP_THREADS, bytes,
                             s2>>>(v, LB + 3 * (size_t)n,
                                                                                                NB + 3, P, nullptr, 0);
         SHM_CUDA(cudaGetLastError());
