@@ -931,6 +931,25 @@ __device__ __forceinline__ int64_t hit_pos(const DevIndex& I, uint32_t g, int32_
     return ap ? (int64_t)(__ldg(I.ref_rs + g) >> 1) : (int64_t)(g - __ldg(I.seg_off + seg));
 }
 
+// First index in [lo, end) whose hit is >= v, or end, when every hit before lo
+// is below v: probes lo, lo+1, lo+3, lo+7, ... then a binary search in the
+// last gap, so a range of c hits costs about 2 log2(c) + 1 loads (one when
+// the next hit is already past v).
+__device__ __forceinline__ uint32_t hits_gallop(const uint32_t* __restrict__ hits, uint32_t lo, uint32_t end,
+                                                uint32_t v) {
+    uint32_t step = 1;
+    while (lo < end) {
+        const uint32_t pr = min(lo + step, end) - 1;
+        if (__ldg(hits + pr) >= v) {
+            end = pr;
+            break;
+        }
+        lo = pr + 1;
+        step <<= 1;
+    }
+    return hits_lower_bound(hits, lo, end - lo, v);
+}
+
 // Hits of one seed's list [a, a+cnt) in segment g with pos in [lo, hi): returns [A, B).
 __device__ __forceinline__ void seed_range(const DevIndex& I, uint32_t a, uint32_t cnt, int32_t g, int64_t lo,
                                            int64_t hi, bool ap, uint32_t& A, uint32_t& B) {
@@ -940,8 +959,9 @@ __device__ __forceinline__ void seed_range(const DevIndex& I, uint32_t a, uint32
         uint64_t ghi = min((uint64_t)s_lo + (uint64_t)max(hi, (int64_t)0), (uint64_t)s_hi);
         glo = min(glo, (uint64_t)s_hi);
         A = hits_lower_bound(I.hits, a, cnt, (uint32_t)glo);
-        B = hits_lower_bound(I.hits, a, cnt, (uint32_t)ghi);
-        if (B < A) B = A;
+        // the range spans two half-lengths, which few hits of a list fall in:
+        // its end is galloped to from A rather than searched for from a
+        B = ghi > glo ? hits_gallop(I.hits, A, a + cnt, (uint32_t)ghi) : A;
         return;
     }
     uint32_t sA = hits_lower_bound(I.hits, a, cnt, s_lo), sB = hits_lower_bound(I.hits, a, cnt, s_hi);
@@ -961,25 +981,6 @@ __device__ __forceinline__ void seed_range(const DevIndex& I, uint32_t a, uint32
     A = lb_r(lo);
     B = lb_r(hi);
     if (B < A) B = A;
-}
-
-// First index in [lo, end) whose hit is >= v, or end, when every hit before lo
-// is below v: probes lo, lo+1, lo+3, lo+7, ... then a binary search in the
-// last gap, so a range of c hits costs about 2 log2(c) + 1 loads (one when
-// the next hit is already past v).
-__device__ __forceinline__ uint32_t hits_gallop(const uint32_t* __restrict__ hits, uint32_t lo, uint32_t end,
-                                                uint32_t v) {
-    uint32_t step = 1;
-    while (lo < end) {
-        const uint32_t pr = min(lo + step, end) - 1;
-        if (__ldg(hits + pr) >= v) {
-            end = pr;
-            break;
-        }
-        lo = pr + 1;
-        step <<= 1;
-    }
-    return hits_lower_bound(hits, lo, end - lo, v);
 }
 
 struct Agg {
