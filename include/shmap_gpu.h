@@ -254,7 +254,10 @@ int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, doub
  * host_batch_reads, host_batch_bases, host_first_batch_reads,
  * sketch_ctas_per_sm, wide_ctas_per_sm, refine_warps_per_sm, device_pack
  * (reads in device memory packed there before sketching: 1, or sketched
- * from their bytes: 0). None of them
+ * from their bytes: 0), bt_fast_slots, host_raw_share (reads in pinned host
+ * memory: the percent of host batches sent up as bytes on their own stream
+ * instead of packed on the host threads) and host_pack_task_kib (KiB of reads
+ * a packing task takes; 0: four tasks a thread). None of them
  * changes a result. They are read once per process from the file named by
  * $SHMAP_TUNING, else tuning.conf in the directory above the library's
  * (key = value lines, '#' comments), else built-in defaults;

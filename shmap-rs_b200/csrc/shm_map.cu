@@ -2976,6 +2976,9 @@ MapCtx* mapctx_create(int device, size_t hbm_budget) {
     SHM_CUDA(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
     for (auto& e : c->copied) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto& e : c->sketched) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    SHM_CUDA(cudaStreamCreateWithFlags(&c->raw_stream, cudaStreamNonBlocking));
+    for (auto& e : c->raw_copied) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : c->raw_sketched) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     c->scr = new MapScratch();
     return c;
 }
@@ -2998,6 +3001,14 @@ void mapctx_destroy(MapCtx* c) {
     for (auto& e : c->sketched)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->raw_stream) {
+        cudaStreamSynchronize(c->raw_stream);
+        cudaStreamDestroy(c->raw_stream);
+    }
+    for (auto& e : c->raw_copied)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->raw_sketched)
+        if (e) cudaEventDestroy(e);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
         cudaStreamDestroy(c->side_stream);
@@ -4003,81 +4014,163 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
     for (size_t b = 0; b < batches.size(); b++)
         raw[b] = ((int64_t)(b + 1) * raw_pct / 100) > ((int64_t)b * raw_pct / 100);
     for (int k = 0; k < 2 && raw_pct > 0; k++) S.seqb[k].reserve((size_t)max_nb + 32);
-    auto h_codes = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes); };
-    auto h_list = [&](size_t b) { return (uint32_t*)(c->h_pack + (b & 1) * slot_bytes + 4 * cwords); };
+    // the packed batches and the raw ones, each in order; a batch's buffers
+    // (host slot and device buffer) alternate within its own kind
+    std::vector<size_t> pk_list, raw_list;
+    std::vector<int> slot(batches.size(), 0), kind_pos(batches.size(), 0);
+    for (size_t b = 0; b < batches.size(); b++) {
+        std::vector<size_t>& L = raw[b] ? raw_list : pk_list;
+        kind_pos[b] = (int)L.size();
+        slot[b] = (int)(L.size() & 1);
+        L.push_back(b);
+    }
+    auto h_codes = [&](size_t b) { return (uint32_t*)(c->h_pack + (size_t)slot[b] * slot_bytes); };
+    auto h_list = [&](size_t b) { return (uint32_t*)(c->h_pack + (size_t)slot[b] * slot_bytes + 4 * cwords); };
+    HostClock H;
+    // per-batch timeline (SHMAP_HOSTPROF): host phases, and device events around each batch's mapping
+    struct Tl {
+        double pack0 = 0, wait0 = 0, wait1 = 0, run0 = 0, run1 = 0;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+    };
+    std::vector<Tl> tl(H.on ? batches.size() : 0);
+    cudaEvent_t tl0 = nullptr;
+    auto ms_now = [&] {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - H.t0).count();
+    };
+    if (H.on) {
+        SHM_CUDA(cudaEventCreate(&tl0));
+        SHM_CUDA(cudaEventRecord(tl0, s));
+        for (auto& t : tl) {
+            SHM_CUDA(cudaEventCreate(&t.e0));
+            SHM_CUDA(cudaEventCreate(&t.e1));
+        }
+    }
+    const int64_t task_groups = tuning().host_pack_task_kib * 1024 / 32;
     auto pack = [&](size_t b) {  // on the host threads in the background, once the slot's previous upload left
-        if (raw[b]) return;
         const auto [i, j] = batches[b];
-        SHM_CUDA(cudaEventSynchronize(c->copied[b & 1]));
-        pack_reads_host_start(seqs + offs[i], offs[j] - offs[i], h_codes(b));
+        SHM_CUDA(cudaEventSynchronize(c->copied[slot[b]]));
+        if (!tl.empty()) tl[b].pack0 = ms_now();
+        pack_reads_host_start(seqs + offs[i], offs[j] - offs[i], h_codes(b), task_groups);
     };
     size_t n_list = 0;  // nonzero mask words of the packing just waited for
     auto wait = [&](size_t b) {
-        if (raw[b]) return;
         const auto [i, j] = batches[b];
+        if (!tl.empty()) tl[b].wait0 = ms_now();
         n_list = pack_reads_host_wait(h_list(b), packed_mask_words(offs[j] - offs[i]));
+        if (!tl.empty()) tl[b].wait1 = ms_now();
     };
     auto send = [&](size_t b) {  // on the copy stream, after the sketch that last read the buffers
         const auto [i, j] = batches[b];
         const int64_t nb = offs[j] - offs[i];
+        const int sl = slot[b];
         cudaStream_t cs = c->copy_stream;
-        SHM_CUDA(cudaStreamWaitEvent(cs, c->sketched[b & 1], 0));
-        if (raw[b]) {  // the bytes as they are, and the zero pad the sketch reads past the end
-            copy_async(c, S.seqb[b & 1].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, cs);
-            SHM_CUDA(cudaMemsetAsync(S.seqb[b & 1].p + nb, 0, 32, cs));
-            SHM_CUDA(cudaEventRecord(c->copied[b & 1], cs));
-            return;
-        }
-        copy_async(c, S.pk_codes[b & 1].p, h_codes(b), 4 * packed_code_words(nb), cudaMemcpyHostToDevice,
-                                 cs);
-        SHM_CUDA(cudaMemsetAsync(S.pk_mask[b & 1].p, 0, 4 * packed_mask_words(nb), cs));
+        SHM_CUDA(cudaStreamWaitEvent(cs, c->sketched[sl], 0));
+        copy_async(c, S.pk_codes[sl].p, h_codes(b), 4 * packed_code_words(nb), cudaMemcpyHostToDevice, cs);
+        SHM_CUDA(cudaMemsetAsync(S.pk_mask[sl].p, 0, 4 * packed_mask_words(nb), cs));
         if (n_list) {  // the nonzero mask words into the zeroed mask
-            copy_async(c, S.pk_list[b & 1].p, h_list(b), 8 * n_list, cudaMemcpyHostToDevice, cs);
-            k_mask_scatter<<<grid_for(n_list, 256, 4), 256, 0, cs>>>(S.pk_list[b & 1].p, (uint32_t)n_list,
-                                                                    S.pk_mask[b & 1].p);
+            copy_async(c, S.pk_list[sl].p, h_list(b), 8 * n_list, cudaMemcpyHostToDevice, cs);
+            k_mask_scatter<<<grid_for(n_list, 256, 4), 256, 0, cs>>>(S.pk_list[sl].p, (uint32_t)n_list,
+                                                                    S.pk_mask[sl].p);
             SHM_CUDA(cudaGetLastError());
             count_launch();
         }
-        SHM_CUDA(cudaEventRecord(c->copied[b & 1], cs));
+        SHM_CUDA(cudaEventRecord(c->copied[sl], cs));
+    };
+    // a raw batch's bytes as they are, and the zero pad the sketch reads past
+    // the end, on the raw stream once the sketch of the raw batch two before
+    // it (the same buffer) has read that buffer, and no earlier than RAW_LEAD
+    // batches before its own: the copy runs while the batches before it are
+    // packed, without taking the link from the first batches' uploads
+    constexpr size_t RAW_LEAD = 3;
+    size_t raw_sent = 0;
+    auto send_raw_ready = [&](size_t mapped_upto) {  // batches [0, mapped_upto) are queued
+        while (raw_sent < raw_list.size() && raw_list[raw_sent] <= mapped_upto + RAW_LEAD &&
+               (raw_sent < 2 || raw_list[raw_sent - 2] < mapped_upto)) {
+            const size_t b = raw_list[raw_sent++];
+            const auto [i, j] = batches[b];
+            const int64_t nb = offs[j] - offs[i];
+            const int sl = slot[b];
+            cudaStream_t rs = c->raw_stream;
+            SHM_CUDA(cudaStreamWaitEvent(rs, c->raw_sketched[sl], 0));
+            copy_async(c, S.seqb[sl].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, rs);
+            SHM_CUDA(cudaMemsetAsync(S.seqb[sl].p + nb, 0, 32, rs));
+            SHM_CUDA(cudaEventRecord(c->raw_copied[sl], rs));
+        }
     };
     std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
     const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
-    HostClock H;
     struct PackRelease {  // a packing started and never waited for (an error) is ended
         ~PackRelease() { pack_reads_host_release(); }
     } pack_release;
-    // batch b+1 is packed on the host threads while batch b is queued, b-1
-    // maps and b goes up
-    if (!batches.empty()) {
-        pack(0);
-        wait(0);
-        send(0);
-        if (batches.size() > 1) pack(1);
+    // the packed batches: k + 1 is packed on the host threads while k is
+    // queued, k - 1 maps and k goes up
+    size_t pk_next = 0;  // the next packed batch to wait for and send
+    send_raw_ready(0);
+    if (!pk_list.empty()) {
+        pack(pk_list[0]);
+        wait(pk_list[0]);
+        send(pk_list[0]);
+        pk_next = 1;
+        if (pk_list.size() > 1) pack(pk_list[1]);
     }
     for (size_t b = 0; b < batches.size(); b++) {
         const auto [i, j] = batches[b];
-        SHM_CUDA(cudaStreamWaitEvent(s, c->copied[b & 1], 0));
-        c->sketch_done = c->sketched[b & 1];
+        const int sl = slot[b];
+        if (!raw[b] && kind_pos[b] >= (int)pk_next) {  // not sent yet (a raw batch came before it)
+            wait(b);
+            send(b);
+            pk_next = (size_t)kind_pos[b] + 1;
+            if (pk_next < pk_list.size()) pack(pk_list[pk_next]);
+        }
+        SHM_CUDA(cudaStreamWaitEvent(s, raw[b] ? c->raw_copied[sl] : c->copied[sl], 0));
+        c->sketch_done = raw[b] ? c->raw_sketched[sl] : c->sketched[sl];
+        if (!tl.empty()) {
+            tl[b].run0 = ms_now();
+            SHM_CUDA(cudaEventRecord(tl[b].e0, s));
+        }
         if (raw[b])
-            run_batch(c, ix, p, S.seqb[b & 1].p, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b]);
+            run_batch(c, ix, p, S.seqb[sl].p, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b]);
         else
             run_batch(c, ix, p, nullptr, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b],
-                      S.pk_codes[b & 1].p, S.pk_mask[b & 1].p);
+                      S.pk_codes[sl].p, S.pk_mask[sl].p);
         c->sketch_done = nullptr;
         if (sink) sink->batch(i, j, S.out.p, s);
         copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost,
                                  s);
-        if (b + 1 < batches.size()) {
+        if (!tl.empty()) {
+            SHM_CUDA(cudaEventRecord(tl[b].e1, s));
+            tl[b].run1 = ms_now();
+        }
+        send_raw_ready(b + 1);
+        // the next packed batch, when it maps next: wait for its packing, send it, start the one after
+        if (b + 1 < batches.size() && !raw[b + 1] && pk_next < pk_list.size() && pk_list[pk_next] == b + 1) {
             wait(b + 1);
             send(b + 1);
-            if (b + 2 < batches.size()) pack(b + 2);
+            pk_next++;
+            if (pk_next < pk_list.size()) pack(pk_list[pk_next]);
         }
         if (sink) sink->poll();
     }
     H.mark("enqueue");
     SHM_CUDA(cudaStreamSynchronize(s));
     H.mark("drain");
+    if (!tl.empty()) {
+        for (size_t b = 0; b < tl.size(); b++) {
+            float d0 = 0, d1 = 0;
+            SHM_CUDA(cudaEventElapsedTime(&d0, tl0, tl[b].e0));
+            SHM_CUDA(cudaEventElapsedTime(&d1, tl0, tl[b].e1));
+            std::fprintf(stderr,
+                         "[shmap-host] batch %zu reads %d MB %.0f%s: pack %.2f wait %.2f-%.2f run %.2f-%.2f "
+                         "device %.2f-%.2f\n",
+                         b, batches[b].second - batches[b].first,
+                         (offs[batches[b].second] - offs[batches[b].first]) / 1e6, raw[b] ? " raw" : "", tl[b].pack0,
+                         tl[b].wait0, tl[b].wait1, tl[b].run0, tl[b].run1, d0, d1);
+            cudaEventDestroy(tl[b].e0);
+            cudaEventDestroy(tl[b].e1);
+        }
+        cudaEventDestroy(tl0);
+    }
     // a batch with more bucket jobs than its capacity is mapped again, its jobs counted first
     bool changed = false;
     for (size_t b = 0; b < batches.size(); b++) {

@@ -78,6 +78,11 @@ struct MapCtx {
     cudaStream_t copy_stream = nullptr;  // host-to-device copies of the next batch
     cudaEvent_t copied[2] = {nullptr, nullptr};
     cudaEvent_t sketched[2] = {nullptr, nullptr};  // the sketch of the batch in each buffer has read it
+    // host-form batches sent up as bytes: their own stream and two buffers, so
+    // their copies run beside the packed batches' without waiting in line
+    cudaStream_t raw_stream = nullptr;
+    cudaEvent_t raw_copied[2] = {nullptr, nullptr};
+    cudaEvent_t raw_sketched[2] = {nullptr, nullptr};
     cudaEvent_t sketch_done = nullptr;             // recorded by run_batch after its sketch when set
     cudaStream_t side_stream = nullptr;  // seed preparation of the few reads with large sketches
     cudaEvent_t fork = nullptr, join = nullptr;

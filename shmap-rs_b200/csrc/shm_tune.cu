@@ -38,6 +38,7 @@ const Knob KNOBS[] = {
     {"device_pack", &Tuning::device_pack, 0, 1},
     {"host_raw_share", &Tuning::host_raw_share, 0, 100},
     {"bt_fast_slots", &Tuning::bt_fast_slots, 16, 512},
+    {"host_pack_task_kib", &Tuning::host_pack_task_kib, 0, 1 << 20},
 };
 
 std::mutex g_mu;

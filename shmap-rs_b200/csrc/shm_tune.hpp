@@ -20,6 +20,8 @@ struct Tuning {
                                       // without waiting for its sizes; fuller tables take a second table
     int64_t host_raw_share = 0;       // reads in pinned host memory: the percent of batches sent up as
                                       // ASCII by the copy engine instead of packed on the host threads
+    int64_t host_pack_task_kib = 1024;  // host packing: KiB of reads a task of the packing threads takes
+                                        // (0: four tasks a thread, at least 1 MiB each)
 };
 
 // The settings in force (read once per process, then as set).

@@ -82,30 +82,33 @@ __attribute__((target("avx2"))) void pack_range_avx2(const uint8_t* s, int64_t n
 }
 
 // AVX-512 (BW, VBMI): 64 bytes a step, groups g and g + 1. A byte is ACGT
-// (either case) iff its low seven bits index a set byte of a 128-entry table
-// (one two-register byte permute) and its top bit is clear. The codes of
-// four bases gather into one byte of a 32-bit lane by two multiply-adds (c0 +
-// 4 c1, then + 16 (c2 + 4 c3)); narrowing the sixteen lanes to bytes gives the
-// 64 bases' 16 bytes of codes. n32 is even; codes + 2 g0 is 16-byte aligned
-// when `aligned` (streaming stores), else plain stores are used.
+// (either case) iff its value with the case bit cleared equals the letter its
+// code names (a 16-byte table indexed by the code, one byte shuffle, one
+// compare into a mask register; a byte with the top bit set never matches).
+// The codes of four bases gather into one byte of a 32-bit lane by two
+// multiply-adds (c0 + 4 c1, then + 16 (c2 + 4 c3)); one byte permute brings
+// the sixteen lanes' low bytes together: the 64 bases' 16 bytes of codes.
+// n32 is even; codes + 2 g0 is 16-byte aligned when `aligned` (streaming
+// stores), else plain stores are used.
 template <bool SPARSE>
 __attribute__((target("avx512f,avx512bw,avx512vbmi"))) void pack_range_avx512(const uint8_t* s, int64_t n32,
                                                                               uint32_t* codes, uint32_t* mask,
                                                                               int64_t g_base, MaskList* list,
                                                                               bool aligned) {
-    alignas(64) uint8_t lut[128];
-    for (int i = 0; i < 128; i++) {
-        const int u = i & 0xdf;
-        lut[i] = (u == 0x41 || u == 0x43 || u == 0x47 || u == 0x54) ? 0xff : 0x00;
-    }
-    const __m512i lut_lo = _mm512_load_si512((const void*)lut), lut_hi = _mm512_load_si512((const void*)(lut + 64));
-    const __m512i k3 = _mm512_set1_epi8(3), m1 = _mm512_set1_epi16(0x0401), m2 = _mm512_set1_epi32(0x00100001);
+    const __m512i k3 = _mm512_set1_epi8(3), kdf = _mm512_set1_epi8((char)0xdf);
+    const __m512i m1 = _mm512_set1_epi16(0x0401), m2 = _mm512_set1_epi32(0x00100001);
+    // the letter of code c (A, C, T, G) at byte c of every 128-bit lane
+    const __m512i letter = _mm512_broadcast_i32x4(_mm_setr_epi8(0x41, 0x43, 0x54, 0x47, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+                                                                0, 0, 0));
+    alignas(64) uint8_t low_bytes[64];
+    for (int i = 0; i < 64; i++) low_bytes[i] = (uint8_t)((4 * i) & 63);  // byte 0 of lane i first
+    const __m512i gather = _mm512_load_si512((const void*)low_bytes);
     for (int64_t g = 0; g < n32; g += 2) {
         const __m512i v = _mm512_loadu_si512((const void*)(s + 32 * g));
         const __m512i c = _mm512_and_si512(_mm512_srli_epi16(v, 1), k3);
-        const __m512i t = _mm512_permutex2var_epi8(lut_lo, v, lut_hi);
-        const uint64_t good = _mm512_test_epi8_mask(t, t) & ~_mm512_movepi8_mask(v);
-        const __m128i q = _mm512_cvtepi32_epi8(_mm512_madd_epi16(_mm512_maddubs_epi16(c, m1), m2));
+        const uint64_t good = _mm512_cmpeq_epi8_mask(_mm512_and_si512(v, kdf), _mm512_shuffle_epi8(letter, c));
+        const __m512i p = _mm512_madd_epi16(_mm512_maddubs_epi16(c, m1), m2);
+        const __m128i q = _mm512_castsi512_si128(_mm512_permutexvar_epi8(gather, p));
         if (aligned) _mm_stream_si128((__m128i*)(codes + 2 * g), q);
         else _mm_storeu_si128((__m128i*)(codes + 2 * g), q);
         const uint64_t bad = ~good;
@@ -267,10 +270,14 @@ static std::vector<MaskList>& task_lists() {
 
 template <bool SPARSE>
 static std::function<void(int)> pack_tasks(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask,
-                                           int& tasks) {
+                                           int& tasks, int64_t task_groups) {
     const int64_t n32 = nb / 32;
-    // an even number of groups a task (the AVX-512 form takes two at a time)
-    const int64_t per = (std::max<int64_t>(1 << 15, (n32 + 4 * pool().size() - 1) / (4 * pool().size())) + 1) & ~1LL;
+    // an even number of groups a task (the AVX-512 form takes two at a time):
+    // task_groups, else a quarter of a thread's share (at least 1 MiB)
+    const int64_t per =
+        task_groups > 0
+            ? std::max<int64_t>(2, task_groups & ~1LL)
+            : (std::max<int64_t>(1 << 15, (n32 + 4 * pool().size() - 1) / (4 * pool().size())) + 1) & ~1LL;
     tasks = (int)((n32 + per - 1) / per);
     const bool avx2 = have_avx2(), avx512 = have_avx512() && !std::getenv("SHMAP_PACK_AVX2");
     const bool aligned = ((uintptr_t)codes & 15) == 0;
@@ -313,20 +320,20 @@ void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* 
     const bool own = !t_pack_held;
     if (own) g_pack_mu.lock();
     int tasks = 0;
-    auto f = pack_tasks<false>(seq, nb, codes, mask, tasks);
+    auto f = pack_tasks<false>(seq, nb, codes, mask, tasks, 0);
     if (tasks > 0) pool().run(tasks, std::move(f));
     pack_tail<false>(seq, nb, codes, mask, nullptr);
     if (own) g_pack_mu.unlock();
 }
 
-void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes) {
+void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes, int64_t task_groups) {
     if (!t_pack_held) {
         g_pack_mu.lock();
         t_pack_held = true;
     }
     pool().finish();
     int tasks = 0;
-    auto f = pack_tasks<true>(seq, nb, codes, nullptr, tasks);
+    auto f = pack_tasks<true>(seq, nb, codes, nullptr, tasks, task_groups);
     pack_tail<true>(seq, nb, codes, nullptr, &task_lists()[tasks]);
     g_sparse_tasks = tasks;
     if (tasks > 0) pool().start(tasks, std::move(f));

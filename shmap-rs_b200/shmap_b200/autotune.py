@@ -44,7 +44,8 @@ HOST_KNOBS = [
     ("host_batch_reads", [8192, 16384, 32768, 65536]),
     ("host_batch_bases", [1 << 26, 1 << 27, 1 << 28, 1 << 29]),
     ("host_first_batch_reads", [1024, 4096, 16384]),
-    ("host_raw_share", [0, 20, 35, 50]),
+    ("host_raw_share", [0, 10, 20, 30]),
+    ("host_pack_task_kib", [0, 256, 1024, 4096]),
 ]
 
 

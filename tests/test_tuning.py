@@ -12,7 +12,7 @@ import shmap_b200 as sb
 
 KEYS = ["dev_batch_reads", "dev_batch_bases", "dev_first_batch_reads", "host_batch_reads", "host_batch_bases",
         "host_first_batch_reads", "sketch_ctas_per_sm", "wide_ctas_per_sm", "refine_warps_per_sm", "device_pack",
-        "host_raw_share", "bt_fast_slots"]
+        "host_raw_share", "bt_fast_slots", "host_pack_task_kib"]
 
 
 def _get(k):
@@ -93,3 +93,13 @@ def test_results_do_not_depend_on_the_settings(gpu_ctx, saved):
         sb._check(L.shm_map_batch(gpu_ctx.h, g.h, ctypes.byref(cp), pin.data_ptr(), offs64.ctypes.data, len(names),
                                   out.ctypes.data))
         assert not record_mismatches(out, want), share
+    # about 20 batches of 1 MiB: a third or two thirds of them sent up as bytes beside the packed
+    # ones (raw batches in a row, each raw buffer reused), packing cut into tasks of 1 KiB to 64 KiB
+    assert L.shm_tuning_set(b"host_batch_bases", 1 << 20) == 0
+    for share, task_kib in ((34, 1), (67, 0), (0, 64)):
+        assert L.shm_tuning_set(b"host_raw_share", share) == 0
+        assert L.shm_tuning_set(b"host_pack_task_kib", task_kib) == 0
+        out = np.zeros(len(names), sb.RECORD_DTYPE)
+        sb._check(L.shm_map_batch(gpu_ctx.h, g.h, ctypes.byref(cp), pin.data_ptr(), offs64.ctypes.data, len(names),
+                                  out.ctypes.data))
+        assert not record_mismatches(out, want), (share, task_kib)
