@@ -40,12 +40,15 @@
 //    of the sequential loop does.
 // All scores use explicit round-to-nearest f64 intrinsics.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <mutex>
 #include <string>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -3009,6 +3012,8 @@ void mapctx_destroy(MapCtx* c) {
         if (e) cudaEventDestroy(e);
     for (auto& e : c->raw_sketched)
         if (e) cudaEventDestroy(e);
+    for (auto& e : c->up_ev) cudaEventDestroy(e);
+    delete c->sink;
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
         cudaStreamDestroy(c->side_stream);
@@ -3077,14 +3082,16 @@ static uint8_t* pinned_stage(MapCtx* c, size_t bytes) {
 // Written into pinned memory at h_plan (BatchPlan::layout(n) bytes). caps =
 // null: capacities from the estimate; else caps[i] k-mers for read i (the
 // counts a previous pass found).
+// roff starts at base0: the batch's first base in the buffer its sketch reads
+// (only differences of roff are read elsewhere).
 static void plan_batch(uint8_t* h_plan, const int64_t* h_offs, int32_t n, int32_t k, double h_frac,
-                       const uint32_t* caps, BatchPlan& bp) {
+                       const uint32_t* caps, BatchPlan& bp, int64_t base0 = 0) {
     bp.carve(h_plan, n);
     bp.P_g = 0;
     bp.max_cap = 0;
     bp.max_len = 0;
     bp.n_cap_512 = bp.n_cap_1024 = bp.n_cap_4096 = 0;
-    bp.roff[0] = 0;
+    bp.roff[0] = base0;
     bp.chunk_off[0] = 0;
     bp.kcap_off[0] = 0;
     bp.pht_off[0] = 0;
@@ -3235,12 +3242,15 @@ static void collect_batch(MapCtx* c, const BatchSlot& sl, std::vector<Overflow>&
 static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* d_seq,
                       const int64_t* h_offs, int32_t n, shm_map_record* d_out, const uint32_t* caps, bool exact,
                       uint8_t* h_plan, StageTimer& T, BatchSlot& sl, const uint32_t* pk_codes = nullptr,
-                      const uint32_t* pk_mask = nullptr, uint64_t bt_lim = 0) {
+                      const uint32_t* pk_mask = nullptr, uint64_t bt_lim = 0, int32_t pk_base = 0,
+                      uint64_t pk_words = 0) {
     cudaStream_t s = c->stream;
     MapScratch& S = *c->scr;
     HostClock H;
     BatchPlan bp;
-    plan_batch(h_plan, h_offs, n, p.k, p.h_frac, caps, bp);
+    // packed reads: the batch's first base is base pk_base (0..31) of pk_codes
+    // / pk_mask, and pk_words code words are readable there (0: the batch's own)
+    plan_batch(h_plan, h_offs, n, p.k, p.h_frac, caps, bp, pk_codes ? pk_base : 0);
     H.mark("plan");
     if (!S.luts || S.luts_k != p.k) {
         if (S.luts) SHM_CUDA(cudaFree(S.luts));
@@ -3409,7 +3419,7 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
     }
     a.pk_codes = pk_codes;  // packed reads instead of d_seq when set
     a.pk_mask = pk_mask;
-    a.pk_words = pk_codes ? packed_code_words(batch_bytes) : 0;
+    a.pk_words = pk_codes ? (pk_words ? pk_words : packed_code_words(batch_bytes)) : 0;
     T.begin(STG_SKETCH, false);
     launch_sketch(SK_APPEND, a, S.luts, s);
     T.end();
@@ -3962,6 +3972,341 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
     H.print("retries", (int32_t)ovf_all.size());
 }
 
+// Pieces of a packing stream sent by the threads that pack them. Each thread
+// packs a piece into one of its own pinned buffers with plain stores and
+// queues the piece's copy into the stream's device codes at once, on its own
+// copy stream, while the piece is still in that core's cache (the copy
+// engine's reads then come from the cache instead of the codes making a round
+// trip through host memory). A buffer is packed again once its last copy has
+// completed. Errors on a packing thread are kept and raised by the next call
+// of the thread that holds the packing.
+struct StreamSink final : PackSink {
+    struct Worker {
+        cudaStream_t st = nullptr;
+        std::vector<cudaEvent_t> ev;  // the last copy out of each buffer
+        cudaEvent_t mark = nullptr;   // every copy queued so far (join)
+        uint32_t* buf = nullptr;      // ring * piece_words words of the pinned block
+        uint32_t next = 0;
+    };
+    int device = 0, ring = 0;
+    size_t piece_words = 0;
+    uint32_t* pinned = nullptr;
+    std::vector<Worker> w;
+    uint32_t* dst = nullptr;  // the device codes of the stream in flight
+    std::atomic<int64_t> bytes{0};
+    std::atomic<bool> failed{false};
+    cudaError_t err = cudaSuccess;
+    std::mutex err_mu;
+
+    void fail(cudaError_t e) {
+        std::lock_guard<std::mutex> g(err_mu);
+        if (failed.load()) return;
+        std::fprintf(stderr, "shmap-b200: CUDA error on a packing thread: %s\n", cudaGetErrorString(e));
+        err = e;
+        failed.store(true);
+    }
+    uint32_t* piece_buffer(int wi) override {
+        if (failed.load() || wi < 0 || wi >= (int)w.size()) {
+            if (!failed.load()) fail(cudaErrorInvalidValue);
+            return nullptr;
+        }
+        Worker& x = w[(size_t)wi];
+        cudaError_t e = cudaSetDevice(device);
+        if (e == cudaSuccess) e = cudaEventSynchronize(x.ev[x.next % ring]);
+        if (e != cudaSuccess) {
+            fail(e);
+            return nullptr;
+        }
+        return x.buf + (size_t)(x.next % ring) * piece_words;
+    }
+    void piece_done(int wi, uint32_t* b, size_t first, size_t words) override {
+        Worker& x = w[(size_t)wi];
+        cudaError_t e = cudaMemcpyAsync(dst + first, b, 4 * words, cudaMemcpyHostToDevice, x.st);
+        if (e == cudaSuccess) e = cudaEventRecord(x.ev[x.next % ring], x.st);
+        if (e != cudaSuccess) fail(e);
+        x.next++;
+        bytes += (int64_t)(4 * words);
+    }
+    void check() {
+        if (failed.load()) throw shm_cuda_error(err);
+    }
+    // (thread holding the packing, no task running) every copy stream waits for e
+    void gate(cudaEvent_t e) {
+        for (Worker& x : w) SHM_CUDA(cudaStreamWaitEvent(x.st, e, 0));
+    }
+    // stream s waits for every copy queued so far
+    void join(cudaStream_t s) {
+        check();
+        for (Worker& x : w) {
+            SHM_CUDA(cudaEventRecord(x.mark, x.st));
+            SHM_CUDA(cudaStreamWaitEvent(s, x.mark, 0));
+        }
+    }
+    ~StreamSink() override {
+        cudaSetDevice(device);
+        for (Worker& x : w) {
+            if (x.st) cudaStreamSynchronize(x.st);
+            for (cudaEvent_t e : x.ev)
+                if (e) cudaEventDestroy(e);
+            if (x.mark) cudaEventDestroy(x.mark);
+            if (x.st) cudaStreamDestroy(x.st);
+        }
+        if (pinned) cudaFreeHost(pinned);
+    }
+};
+
+// The context's stream sink for pieces of piece_words code words and `ring`
+// buffers a packing thread (made again when the settings changed).
+static StreamSink* stream_sink(MapCtx* c, size_t piece_words, int ring) {
+    const int nw = pack_workers();
+    if (c->sink && c->sink->piece_words == piece_words && c->sink->ring == ring && (int)c->sink->w.size() == nw &&
+        !c->sink->failed.load())
+        return c->sink;
+    delete c->sink;
+    c->sink = nullptr;
+    auto* u = new StreamSink();
+    u->device = c->device;
+    u->ring = ring;
+    u->piece_words = piece_words;
+    c->sink = u;  // released with the context even if a step below fails
+    SHM_CUDA(cudaHostAlloc((void**)&u->pinned, 4 * piece_words * (size_t)ring * (size_t)nw, cudaHostAllocDefault));
+    u->w.resize((size_t)nw);
+    for (int i = 0; i < nw; i++) {
+        StreamSink::Worker& x = u->w[(size_t)i];
+        x.buf = u->pinned + piece_words * (size_t)ring * (size_t)i;
+        SHM_CUDA(cudaStreamCreateWithFlags(&x.st, cudaStreamNonBlocking));
+        x.ev.assign((size_t)ring, nullptr);
+        for (auto& e : x.ev) SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        SHM_CUDA(cudaEventCreateWithFlags(&x.mark, cudaEventDisableTiming));
+    }
+    return u;
+}
+
+// Device batches over one packing stream: the first of about first_bases,
+// each next twice the one before (at most max_reads reads and max_bases
+// bases), and once the rest fits two of the current size, halves of the rest
+// down to last_bases: the device starts early, maps most of the stream in
+// large batches and ends soon after the packing does. (A batch has a fixed
+// device cost, about 0.7 ms on the hifi workload, so batches below a few
+// hundred MB would map slower than the host packs the next one.)
+static std::vector<std::pair<int32_t, int32_t>> cut_stream_batches(const int64_t* offs, int32_t r0, int32_t r1,
+                                                                   int64_t first_bases, int64_t last_bases,
+                                                                   int64_t max_bases, int32_t max_reads) {
+    std::vector<std::pair<int32_t, int32_t>> b;
+    int64_t tgt = std::max<int64_t>(1, first_bases);
+    for (int32_t i = r0; i < r1;) {
+        const int64_t rest = offs[r1] - offs[i];
+        const int64_t lim = rest <= 2 * tgt ? std::max(rest / 2, last_bases) : tgt;
+        int32_t j = i + 1;
+        while (j < r1 && j - i < max_reads && offs[j + 1] - offs[i] <= lim) j++;
+        b.emplace_back(i, j);
+        i = j;
+        tgt = std::min(2 * tgt, max_bases);
+    }
+    return b;
+}
+
+// Host-buffer form, streamed. The reads of a call (in parts of at most
+// host_stream_bases) are packed in order by the host threads into one pinned
+// buffer, in tasks of host_pack_task_kib with no wait between batches; each
+// chunk of host_stream_chunk_kib goes up on the copy stream as soon as all
+// its tasks are done (codes, then its nonzero mask words scattered into the
+// zeroed device mask). The device maps batches over the packed copy
+// (cut_stream_batches), each once the chunk holding its last base is up: a
+// batch starts at any base of the stream, its sketch reading the codes from
+// the batch's first 32-base group with the base offset in its plan. The
+// calling thread uploads chunks, queues batches and packs tasks in between.
+static bool map_host_stream(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs,
+                            const int64_t* offs, int32_t n, shm_map_record* out, BatchSink* sink) {
+    MapScratch& S = *c->scr;
+    cudaStream_t s = c->stream, cs = c->copy_stream;
+    const Tuning tu = tuning();
+    const bool by_piece = tu.host_stream == 2;  // pieces sent by the packing threads
+    const int64_t task_kib = by_piece ? tu.host_stream_piece_kib : (tu.host_pack_task_kib > 0 ? tu.host_pack_task_kib : 256);
+    const int64_t task_groups = std::max<int64_t>(2, (task_kib * 1024 / 32) & ~(int64_t)1);
+    const int chunk_tasks = (int)std::max<int64_t>(1, tu.host_stream_chunk_kib * 1024 / 32 / task_groups);
+    const int64_t chunk_groups = task_groups * chunk_tasks;
+    const int LIST_SLOTS = 8;
+    // the parts: whole reads, at most host_stream_bases each (a longer read alone)
+    std::vector<std::pair<int32_t, int32_t>> parts;
+    for (int32_t i = 0; i < n;) {
+        int32_t j = i + 1;
+        while (j < n && offs[j + 1] - offs[i] <= tu.host_stream_bases) j++;
+        parts.emplace_back(i, j);
+        i = j;
+    }
+    // every device batch of the call, part by part (their plans and result slots)
+    std::vector<std::pair<int32_t, int32_t>> batches;
+    std::vector<size_t> part_first;
+    for (auto [r0, r1] : parts) {
+        part_first.push_back(batches.size());
+        auto b = cut_stream_batches(offs, r0, r1, tu.host_stream_first_kib * 1024, tu.host_stream_last_kib * 1024,
+                                    tu.dev_batch_bases, (int32_t)tu.dev_batch_reads);
+        batches.insert(batches.end(), b.begin(), b.end());
+    }
+    part_first.push_back(batches.size());
+    int64_t max_nb = 0;
+    int32_t max_n = 1;
+    for (auto [r0, r1] : parts) max_nb = std::max<int64_t>(max_nb, offs[r1] - offs[r0]);
+    for (auto [i, j] : batches) max_n = std::max(max_n, j - i);
+    const size_t cwords = packed_code_words(max_nb), mwords = packed_mask_words(max_nb);
+    const size_t list_cap = (size_t)chunk_groups + 3;  // mask words of a chunk at most (the last: + tail)
+    // pinned: the codes of a part, then LIST_SLOTS chunk lists (pairs)
+    // (by piece, the codes go up from the packing threads' own buffers: only the six tail words stay here)
+    const size_t codes_bytes = by_piece ? 64 : (4 * cwords + 63) / 64 * 64, list_bytes = (8 * list_cap + 63) / 64 * 64;
+    const size_t need = codes_bytes + LIST_SLOTS * list_bytes;
+    if (need > c->h_pack_cap) {
+        if (c->h_pack) SHM_CUDA(cudaFreeHost(c->h_pack));
+        c->h_pack = nullptr;
+        c->h_pack_cap = 0;
+        SHM_CUDA(cudaHostAlloc(&c->h_pack, need, cudaHostAllocDefault));
+        c->h_pack_cap = need;
+    }
+    uint32_t* h_codes = (uint32_t*)c->h_pack;
+    auto h_list = [&](int slot) { return (uint32_t*)(c->h_pack + codes_bytes + (size_t)slot * list_bytes); };
+    S.pk_codes[0].reserve(cwords);
+    S.pk_mask[0].reserve(mwords);
+    S.pk_list[0].reserve(2 * list_cap * LIST_SLOTS);
+    S.out.reserve((size_t)max_n);
+    StreamSink* sink_up = by_piece ? stream_sink(c, 2 * (size_t)task_groups, (int)tu.host_stream_ring) : nullptr;
+    if (sink_up) sink_up->dst = S.pk_codes[0].p;
+    std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
+    const std::vector<uint8_t*> plans = plan_blocks(c, batches);
+    StageTimer T(c);
+    HostClock H;
+    // per-batch timeline (SHMAP_HOSTPROF): when each batch was queued, and its device span
+    struct Tl {
+        double run0 = 0;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+    };
+    std::vector<Tl> tl(H.on ? batches.size() : 0);
+    cudaEvent_t tl0 = nullptr;
+    if (H.on) {
+        SHM_CUDA(cudaEventCreate(&tl0));
+        SHM_CUDA(cudaEventRecord(tl0, s));
+        for (auto& t : tl) {
+            SHM_CUDA(cudaEventCreate(&t.e0));
+            SHM_CUDA(cudaEventCreate(&t.e1));
+        }
+    }
+    struct StreamEnd {  // a packing started and never finished (an error) is ended
+        bool on = false;
+        ~StreamEnd() {
+            if (on) pack_stream_finish();
+        }
+    } stream_end;
+    for (size_t pi = 0; pi < parts.size(); pi++) {
+        const auto [r0, r1] = parts[pi];
+        const int64_t nb = offs[r1] - offs[r0];
+        const size_t pw = packed_code_words(nb);
+        // the pinned codes and lists are free once the part before is up; the
+        // device buffers once its last sketch has read them
+        if (pi > 0) SHM_CUDA(cudaStreamSynchronize(cs));
+        SHM_CUDA(cudaStreamWaitEvent(cs, c->sketched[0], 0));
+        SHM_CUDA(cudaMemsetAsync(S.pk_mask[0].p, 0, 4 * packed_mask_words(nb), cs));
+        if (sink_up) sink_up->gate(c->sketched[0]);
+        stream_end.on = true;
+        const int chunks = pack_stream_start(seqs + offs[r0], nb, h_codes, task_groups, chunk_tasks, sink_up);
+        while (c->up_ev.size() < (size_t)chunks) {
+            cudaEvent_t e;
+            SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            c->up_ev.push_back(e);
+        }
+        auto chunk_of = [&](int64_t g) { return (int)std::min<int64_t>(chunks - 1, g / chunk_groups); };
+        auto upload = [&](int ch) {  // chunk ch's codes and mask words, on the copy stream
+            const size_t w0 = 2 * (size_t)ch * (size_t)chunk_groups;
+            const size_t w1 = ch + 1 == chunks ? pw : std::min(pw, 2 * (size_t)(ch + 1) * (size_t)chunk_groups);
+            const int sl = ch % LIST_SLOTS;
+            if (ch >= LIST_SLOTS) SHM_CUDA(cudaEventSynchronize(c->up_ev[(size_t)(ch - LIST_SLOTS)]));
+            const size_t nl = pack_stream_chunk_list(ch, h_list(sl), list_cap);
+            if (nl > list_cap) throw shm_cuda_error(cudaErrorInvalidValue);  // cannot happen: a word a group
+            if (sink_up) {  // the pieces went up from the packing threads; the tail words from here
+                if (ch + 1 == chunks)
+                    copy_async(c, S.pk_codes[0].p + 2 * (size_t)(nb / 32), h_codes, 4 * 6, cudaMemcpyHostToDevice, cs);
+            } else if (w1 > w0) {
+                copy_async(c, S.pk_codes[0].p + w0, h_codes + w0, 4 * (w1 - w0), cudaMemcpyHostToDevice, cs);
+            }
+            if (nl) {
+                uint32_t* dl = S.pk_list[0].p + 2 * list_cap * (size_t)sl;
+                copy_async(c, dl, h_list(sl), 8 * nl, cudaMemcpyHostToDevice, cs);
+                k_mask_scatter<<<grid_for(nl, 256, 4), 256, 0, cs>>>(dl, (uint32_t)nl, S.pk_mask[0].p);
+                SHM_CUDA(cudaGetLastError());
+                count_launch();
+            }
+            SHM_CUDA(cudaEventRecord(c->up_ev[(size_t)ch], cs));
+        };
+        int up_next = 0;
+        for (size_t b = part_first[pi]; b < part_first[pi + 1];) {
+            while (up_next < chunks && pack_stream_chunk_ready(up_next)) upload(up_next++);
+            const auto [i, j] = batches[b];
+            const int64_t o = offs[i] - offs[r0], e = offs[j] - offs[r0];
+            const int need_ch = chunk_of(std::max<int64_t>(0, e - 1) / 32);
+            if (need_ch >= up_next) {  // its last chunk is not up yet: pack a task meanwhile
+                if (!pack_stream_help()) std::this_thread::yield();
+                continue;
+            }
+            SHM_CUDA(cudaStreamWaitEvent(s, c->up_ev[(size_t)need_ch], 0));
+            if (sink_up) sink_up->join(s);  // every piece queued so far (those of its chunks among them)
+            c->sketch_done = c->sketched[0];
+            if (!tl.empty()) {
+                tl[b].run0 = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - H.t0).count();
+                SHM_CUDA(cudaEventRecord(tl[b].e0, s));
+            }
+            const int64_t g0 = o / 32;
+            run_batch(c, ix, p, nullptr, offs + i, j - i, S.out.p, nullptr, false, plans[b], T, slots[b],
+                      S.pk_codes[0].p + 2 * g0, S.pk_mask[0].p + g0, 0, (int32_t)(o - 32 * g0), pw - 2 * (size_t)g0);
+            c->sketch_done = nullptr;
+            if (sink) sink->batch(i, j, S.out.p, s);
+            copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost, s);
+            if (!tl.empty()) SHM_CUDA(cudaEventRecord(tl[b].e1, s));
+            if (sink) sink->poll();
+            b++;
+        }
+        stream_end.on = false;
+        pack_stream_finish();
+        if (sink_up) sink_up->check();
+    }
+    if (sink_up) c->work[W_H2D_BYTES] += sink_up->bytes.exchange(0);
+    H.mark("enqueue");
+    SHM_CUDA(cudaStreamSynchronize(s));
+    H.mark("drain");
+    if (!tl.empty()) {
+        for (size_t b = 0; b < tl.size(); b++) {
+            float d0 = 0, d1 = 0;
+            SHM_CUDA(cudaEventElapsedTime(&d0, tl0, tl[b].e0));
+            SHM_CUDA(cudaEventElapsedTime(&d1, tl0, tl[b].e1));
+            std::fprintf(stderr, "[shmap-host] stream batch %zu reads %d MB %.0f: queued %.2f device %.2f-%.2f\n", b,
+                         batches[b].second - batches[b].first,
+                         (offs[batches[b].second] - offs[batches[b].first]) / 1e6, tl[b].run0, d0, d1);
+            cudaEventDestroy(tl[b].e0);
+            cudaEventDestroy(tl[b].e1);
+        }
+        cudaEventDestroy(tl0);
+    }
+    // a batch with more bucket jobs than its capacity is mapped again, its jobs counted first
+    bool changed = false;
+    for (size_t b = 0; b < batches.size(); b++) {
+        if (slots[b].R->nj <= slots[b].job_cap) continue;
+        changed = true;
+        const auto [i, j] = batches[b];
+        const int64_t nb = offs[j] - offs[i];
+        S.seqb[0].reserve((size_t)nb + 32);
+        SHM_CUDA(cudaMemsetAsync(S.seqb[0].p + nb, 0, 32, s));
+        copy_async(c, S.seqb[0].p, seqs + offs[i], (size_t)nb, cudaMemcpyHostToDevice, s);
+        run_batch(c, ix, p, S.seqb[0].p, offs + i, j - i, S.out.p, nullptr, true, plans[b], T, slots[b], nullptr,
+                  nullptr, fast_bt_read_cap());
+        copy_async(c, out + i, S.out.p, sizeof(shm_map_record) * (size_t)(j - i), cudaMemcpyDeviceToHost, s);
+        SHM_CUDA(cudaStreamSynchronize(s));
+    }
+    T.collect();
+    std::vector<Overflow> ovf_all;
+    for (const BatchSlot& sl : slots) collect_batch(c, sl, ovf_all);
+    retry_overflows(c, ix, p, ovf_all, offs, RetryIO{nullptr, nullptr, seqs, out});
+    H.mark("retry");
+    H.print("host-stream", n);
+    return changed || !ovf_all.empty();
+}
+
 // Host-buffer form. Batch b+1's bytes go up on the copy stream while batch b
 // is mapped (two device buffers, each reused once the sketch of the batch
 // before has read it), so the transfer of the reads overlaps the mapping when
@@ -3969,6 +4314,8 @@ void map_device(MapCtx* c, const IndexStorage* ix, const shm_params& p, const ui
 bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint8_t* seqs, const int64_t* offs,
               int32_t n, shm_map_record* out, bool plain, BatchSink* sink) {
     SHM_CUDA(cudaSetDevice(c->device));
+    if (!plain && n > 0 && tuning().host_stream && tuning().host_raw_share == 0)
+        return map_host_stream(c, ix, p, seqs, offs, n, out, sink);
     MapScratch& S = *c->scr;
     cudaStream_t s = c->stream;
     const auto batches =

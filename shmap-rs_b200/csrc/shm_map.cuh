@@ -36,6 +36,7 @@ struct BucketJob {
 
 struct MapScratch;  // grow-only device buffers owned by a context
 struct PafScratch;  // those of the PAF formatting (shm_paf.cu)
+struct StreamSink;  // pinned piece buffers and copy streams of the host packing threads
 
 // Stages timed with CUDA events on the context's stream when timing is on.
 enum Stage { STG_SKETCH, STG_SEEDPREP, STG_CONTRIB, STG_BSCAN, STG_EXTEND, STG_REFINE, STG_SWEEP, STG_AUX, N_STAGES };
@@ -83,6 +84,8 @@ struct MapCtx {
     cudaStream_t raw_stream = nullptr;
     cudaEvent_t raw_copied[2] = {nullptr, nullptr};
     cudaEvent_t raw_sketched[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> up_ev;  // the streamed host form: one per chunk uploaded in a call
+    StreamSink* sink = nullptr;      // the streamed host form with pieces sent by the packing threads
     cudaEvent_t sketch_done = nullptr;             // recorded by run_batch after its sketch when set
     cudaStream_t side_stream = nullptr;  // seed preparation of the few reads with large sketches
     cudaEvent_t fork = nullptr, join = nullptr;

@@ -39,6 +39,13 @@ const Knob KNOBS[] = {
     {"host_raw_share", &Tuning::host_raw_share, 0, 100},
     {"bt_fast_slots", &Tuning::bt_fast_slots, 16, 512},
     {"host_pack_task_kib", &Tuning::host_pack_task_kib, 0, 1 << 20},
+    {"host_stream", &Tuning::host_stream, 0, 2},
+    {"host_stream_piece_kib", &Tuning::host_stream_piece_kib, 64, 1 << 16},
+    {"host_stream_ring", &Tuning::host_stream_ring, 2, 16},
+    {"host_stream_bases", &Tuning::host_stream_bases, 1 << 24, (int64_t)1 << 36},
+    {"host_stream_chunk_kib", &Tuning::host_stream_chunk_kib, 256, 1 << 20},
+    {"host_stream_first_kib", &Tuning::host_stream_first_kib, 256, 1 << 22},
+    {"host_stream_last_kib", &Tuning::host_stream_last_kib, 256, 1 << 22},
 };
 
 std::mutex g_mu;

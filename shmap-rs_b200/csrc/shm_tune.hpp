@@ -22,6 +22,19 @@ struct Tuning {
                                       // ASCII by the copy engine instead of packed on the host threads
     int64_t host_pack_task_kib = 1024;  // host packing: KiB of reads a task of the packing threads takes
                                         // (0: four tasks a thread, at least 1 MiB each)
+    int64_t host_stream = 1;            // host reads: one packing stream per call, its chunks sent from
+                                        // one pinned buffer (1) or each piece sent by its packing thread
+                                        // from a ring of small pinned buffers (2); or host batches packed
+                                        // and sent whole, one after another (0)
+    int64_t host_stream_piece_kib = 2048;  // host_stream 2: KiB of reads a piece (a packing task)
+    int64_t host_stream_ring = 4;          // host_stream 2: piece buffers a packing thread cycles through
+    int64_t host_stream_bases = (int64_t)1 << 32;  // bases a packing stream covers at most (a longer
+                                                   // call is streamed in parts)
+    int64_t host_stream_chunk_kib = 32768;  // KiB of reads a chunk of the stream: sent up as soon as
+                                            // all its tasks are packed
+    int64_t host_stream_first_kib = 65536;  // KiB of reads the first device batch of a stream maps;
+                                            // the batches double from there and halve at the end
+    int64_t host_stream_last_kib = 262144;  // ... down to about this many KiB
 };
 
 // The settings in force (read once per process, then as set).

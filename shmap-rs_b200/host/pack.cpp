@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -145,6 +146,10 @@ bool have_avx2() {
     return v;
 }
 
+// Index of the calling thread among the packing threads: 0 for the thread
+// that holds the packing (one at a time), 1.. for the pool's own.
+thread_local int t_worker = 0;
+
 // Persistent workers. start(n, f) has them call f(0..n-1) and returns at
 // once; finish() waits until every call has returned and no worker holds
 // the job; run(n, f) does both, the caller working too. One job at a time.
@@ -152,7 +157,11 @@ class Pool {
   public:
     Pool() {
         const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
-        for (unsigned i = 1; i < hc; i++) th_.emplace_back([this] { loop(); });
+        for (unsigned i = 1; i < hc; i++)
+            th_.emplace_back([this, i] {
+                t_worker = (int)i;
+                loop();
+            });
     }
     ~Pool() {
         finish();
@@ -198,6 +207,19 @@ class Pool {
         finish();
     }
     int size() const { return (int)th_.size() + 1; }
+    // One task of the job in flight on the calling thread; false when none is left to take.
+    bool help_one() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (!cur_) return false;
+        }
+        const int i = job_.next.fetch_add(1);
+        if (i >= job_.n) return false;
+        job_.f(i);
+        std::lock_guard<std::mutex> g(mu_);
+        if (++job_.done == job_.n) done_cv_.notify_all();
+        return true;
+    }
 
   private:
     struct Job {
@@ -251,15 +273,17 @@ Pool& pool() {
 // The whole 32-byte groups as pool tasks; the tail and two spare groups
 // (codes 0, every position masked) by the caller.
 template <bool SPARSE>
-static void pack_tail(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask, MaskList* list) {
+// (tail: the six code words of groups n32 .. n32 + 2; mask_tail their three
+// mask words, or the list)
+static void pack_tail(const uint8_t* seq, int64_t nb, uint32_t* tail, uint32_t* mask_tail, MaskList* list) {
     const int64_t n32 = nb / 32;
     uint32_t m = 0;
-    pack32_scalar(seq + 32 * n32, codes + 2 * n32, SPARSE ? &m : mask + n32, (int)(nb - 32 * n32));
+    pack32_scalar(seq + 32 * n32, tail, SPARSE ? &m : mask_tail, (int)(nb - 32 * n32));
     if (SPARSE && m) list->emplace_back((uint32_t)n32, m);
-    for (int64_t g = n32 + 1; g < n32 + 3; g++) {
-        codes[2 * g] = codes[2 * g + 1] = 0;
-        if (SPARSE) list->emplace_back((uint32_t)g, ~0u);
-        else mask[g] = ~0u;
+    for (int64_t g = 1; g < 3; g++) {
+        tail[2 * g] = tail[2 * g + 1] = 0;
+        if (SPARSE) list->emplace_back((uint32_t)(n32 + g), ~0u);
+        else mask_tail[g] = ~0u;
     }
 }
 
@@ -305,7 +329,46 @@ static std::function<void(int)> pack_tasks(const uint8_t* seq, int64_t nb, uint3
     };
 }
 
+// The streamed form with a sink: a task is one piece of `per` groups, packed
+// with plain stores into the buffer the sink hands the packing thread (so the
+// piece is still in that core's cache when the sink sends it on) and handed
+// back with its place among the stream's code words.
+static std::function<void(int)> pack_tasks_sink(const uint8_t* seq, int64_t nb, PackSink* sink, int64_t per,
+                                                int& tasks) {
+    const int64_t n32 = nb / 32;
+    per = std::max<int64_t>(2, per & ~1LL);
+    tasks = (int)((n32 + per - 1) / per);
+    const bool avx2 = have_avx2(), avx512 = have_avx512() && !std::getenv("SHMAP_PACK_AVX2");
+    std::vector<MaskList>& lists = task_lists();
+    if ((int)lists.size() < tasks + 1) lists.resize(tasks + 1);
+    for (auto& l : lists) l.clear();
+    MaskList* L = lists.data();
+    return [=](int t) {
+        const int64_t g0 = per * t, g1 = std::min(n32, g0 + per);
+        const int w = t_worker;
+        uint32_t* buf = sink->piece_buffer(w);
+        if (!buf) return;  // the sink failed; it reports that itself
+        if (avx512) {
+            const int64_t ge = g0 + ((g1 - g0) & ~1LL);
+            pack_range_avx512<true>(seq + 32 * g0, ge - g0, buf, nullptr, g0, L + t, false);
+            if (ge < g1) pack_range_avx2<true>(seq + 32 * ge, g1 - ge, buf + 2 * (ge - g0), nullptr, ge, L + t);
+        } else if (avx2)
+            pack_range_avx2<true>(seq + 32 * g0, g1 - g0, buf, nullptr, g0, L + t);
+        else
+            pack_range_scalar<true>(seq + 32 * g0, g1 - g0, buf, nullptr, g0, L + t);
+        sink->piece_done(w, buf, (size_t)(2 * g0), (size_t)(2 * (g1 - g0)));
+    };
+}
+
 int g_sparse_tasks = 0;  // task lists of the sparse packing in flight (the tail's is the last)
+
+// The streamed packing in flight: its tasks in order, chunk_tasks a chunk,
+// and how many tasks of each chunk are still to finish.
+struct Stream {
+    int tasks = 0, chunk_tasks = 1, chunks = 0;
+    std::unique_ptr<std::atomic<int>[]> left;
+};
+Stream g_stream;
 
 }  // namespace
 
@@ -322,7 +385,7 @@ void pack_reads_host(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* 
     int tasks = 0;
     auto f = pack_tasks<false>(seq, nb, codes, mask, tasks, 0);
     if (tasks > 0) pool().run(tasks, std::move(f));
-    pack_tail<false>(seq, nb, codes, mask, nullptr);
+    pack_tail<false>(seq, nb, codes + 2 * (nb / 32), mask + nb / 32, nullptr);
     if (own) g_pack_mu.unlock();
 }
 
@@ -334,9 +397,72 @@ void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes, int6
     pool().finish();
     int tasks = 0;
     auto f = pack_tasks<true>(seq, nb, codes, nullptr, tasks, task_groups);
-    pack_tail<true>(seq, nb, codes, nullptr, &task_lists()[tasks]);
+    pack_tail<true>(seq, nb, codes + 2 * (nb / 32), nullptr, &task_lists()[tasks]);
     g_sparse_tasks = tasks;
     if (tasks > 0) pool().start(tasks, std::move(f));
+}
+
+int pack_stream_start(const uint8_t* seq, int64_t nb, uint32_t* codes, int64_t task_groups, int chunk_tasks,
+                      PackSink* sink) {
+    if (!t_pack_held) {
+        g_pack_mu.lock();
+        t_pack_held = true;
+    }
+    pool().finish();
+    int tasks = 0;
+    std::function<void(int)> f = sink ? pack_tasks_sink(seq, nb, sink, std::max<int64_t>(2, task_groups), tasks)
+                                      : pack_tasks<true>(seq, nb, codes, nullptr, tasks, std::max<int64_t>(2, task_groups));
+    Stream& S = g_stream;
+    S.tasks = tasks;
+    S.chunk_tasks = std::max(1, chunk_tasks);
+    S.chunks = std::max(1, (tasks + S.chunk_tasks - 1) / S.chunk_tasks);
+    S.left.reset(new std::atomic<int>[(size_t)S.chunks]);
+    for (int c = 0; c < S.chunks; c++)
+        S.left[(size_t)c].store(std::min(S.chunk_tasks, std::max(0, tasks - c * S.chunk_tasks)));
+    // the tail's list joins the last chunk's (with a sink, codes holds only the tail's six words)
+    pack_tail<true>(seq, nb, sink ? codes : codes + 2 * (nb / 32), nullptr, &task_lists()[tasks]);
+    g_sparse_tasks = tasks;
+    if (tasks > 0) {
+        std::atomic<int>* left = S.left.get();
+        const int ct = S.chunk_tasks;
+        pool().start(tasks, [f = std::move(f), left, ct](int t) {
+            f(t);
+            left[t / ct].fetch_sub(1, std::memory_order_release);
+        });
+    }
+    return S.chunks;
+}
+
+bool pack_stream_chunk_ready(int c) {
+    return c >= 0 && c < g_stream.chunks && g_stream.left[(size_t)c].load(std::memory_order_acquire) == 0;
+}
+
+bool pack_stream_help() { return pool().help_one(); }
+
+int pack_workers() { return pool().size(); }
+
+size_t pack_stream_chunk_list(int c, uint32_t* pairs, size_t cap) {
+    const Stream& S = g_stream;
+    const int t0 = c * S.chunk_tasks, t1 = (c + 1 == S.chunks) ? S.tasks + 1 : std::min(S.tasks, t0 + S.chunk_tasks);
+    size_t n = 0;
+    for (int t = t0; t < t1; t++)
+        for (const auto& e : task_lists()[(size_t)t]) {
+            if (n < cap) {
+                pairs[2 * n] = e.first;
+                pairs[2 * n + 1] = e.second;
+            }
+            n++;
+        }
+    return n;
+}
+
+void pack_stream_finish() {
+    pool().help_finish();
+    g_stream.chunks = 0;
+    if (t_pack_held) {
+        t_pack_held = false;
+        g_pack_mu.unlock();
+    }
 }
 
 size_t pack_reads_host_wait(uint32_t* pairs, size_t cap) {
@@ -386,4 +512,26 @@ extern "C" int shm_internal_pack_reads(const uint8_t* seq, int64_t nb, uint32_t*
     }
     shm::pack_reads_host(seq, nb, codes, mask);
     return 0;
+}
+
+// Test hook (not part of the C ABI of include/shmap_gpu.h): the streamed
+// packing of `nb` bytes as the host-buffer path runs it (tasks of task_groups
+// groups, chunk_tasks a chunk, chunks taken in order as they finish), its
+// mask words gathered from the chunks' lists into a dense mask. Returns the
+// number of chunks.
+extern "C" int shm_internal_pack_stream(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t* mask,
+                                        int64_t task_groups, int chunk_tasks) {
+    if (nb < 0 || (nb > 0 && (!seq || !codes || !mask))) return -1;
+    const size_t mw = shm::packed_mask_words(nb);
+    for (size_t i = 0; i < mw; i++) mask[i] = 0;
+    const int chunks = shm::pack_stream_start(seq, nb, codes, task_groups, chunk_tasks, nullptr);
+    std::vector<uint32_t> pairs(2 * (mw + 4));
+    for (int c = 0; c < chunks; c++) {
+        while (!shm::pack_stream_chunk_ready(c))
+            if (!shm::pack_stream_help()) std::this_thread::yield();
+        const size_t n = shm::pack_stream_chunk_list(c, pairs.data(), mw + 4);
+        for (size_t i = 0; i < n && i < mw + 4; i++) mask[pairs[2 * i]] = pairs[2 * i + 1];
+    }
+    shm::pack_stream_finish();
+    return chunks;
 }

@@ -95,3 +95,26 @@ def test_device_packing_equals_the_model(nb):
     assert f(0, seq.ctypes.data, nb, codes.ctypes.data, mask.ctypes.data) == 0
     want_c, want_m = _model(seq)
     assert np.array_equal(codes, want_c) and np.array_equal(mask, want_m)
+
+
+@pytest.mark.parametrize("nb", [0, 1, 31, 32, 33, 64, 95, 1000, 1 << 16, (1 << 20) + 7, (1 << 21) + 40])
+@pytest.mark.parametrize("task_groups,chunk_tasks", [(2, 1), (2, 7), (64, 3), (8192, 128)])
+def test_streamed_packing_equals_the_model(nb, task_groups, chunk_tasks):
+    """The streamed packing of the host-buffer path: tasks packed in the
+    background, chunks taken in order as their tasks finish, each chunk's
+    nonzero mask words (the last chunk's with the tail groups) scattered into
+    a zeroed mask: the same codes and mask as the definition."""
+    f = sb.lib().shm_internal_pack_stream
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int]
+    f.restype = ctypes.c_int
+    rng = np.random.default_rng(nb + 7 * task_groups + chunk_tasks)
+    seq = rng.choice(np.frombuffer(b"ACGTACGTACGTacgtNnRY\x00\xff", np.uint8), nb).astype(np.uint8)
+    groups = nb // 32 + 3
+    codes = np.full(2 * groups, 0xDEADBEEF, np.uint32)
+    mask = np.full(groups, 0xDEADBEEF, np.uint32)
+    buf = np.ascontiguousarray(seq)
+    chunks = f(buf.ctypes.data if nb else None, nb, codes.ctypes.data, mask.ctypes.data, task_groups, chunk_tasks)
+    assert chunks >= 1
+    wc, wm = _model(seq)
+    assert np.array_equal(codes, wc)
+    assert np.array_equal(mask, wm)
