@@ -256,8 +256,14 @@ int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, doub
  * (reads in device memory packed there before sketching: 1, or sketched
  * from their bytes: 0), bt_fast_slots, host_raw_share (reads in pinned host
  * memory: the percent of host batches sent up as bytes on their own stream
- * instead of packed on the host threads) and host_pack_task_kib (KiB of reads
- * a packing task takes; 0: four tasks a thread). None of them
+ * instead of packed on the host threads), host_pack_task_kib (KiB of reads
+ * a packing task takes; 0: four tasks a thread), host_stream (host reads as
+ * one packing stream a call: 1 = chunks sent from one pinned buffer, 2 =
+ * pieces sent by the packing threads; 0 = host batches one after another),
+ * host_stream_bases, host_stream_chunk_kib, host_stream_first_kib,
+ * host_stream_last_kib (the device batches of a stream grow from the first
+ * size and shrink to the last), host_stream_piece_kib and host_stream_ring.
+ * None of them
  * changes a result. They are read once per process from the file named by
  * $SHMAP_TUNING, else tuning.conf in the directory above the library's
  * (key = value lines, '#' comments), else built-in defaults;
