@@ -46,6 +46,11 @@ HOST_KNOBS = [
     ("host_first_batch_reads", [1024, 4096, 16384]),
     ("host_raw_share", [0, 10, 20, 30]),
     ("host_pack_task_kib", [0, 256, 1024, 4096]),
+    ("host_stream", [0, 1, 2]),
+    ("host_stream_piece_kib", [1024, 2048, 4096]),
+    ("host_stream_ring", [2, 4]),
+    ("host_stream_first_kib", [32768, 65536, 131072]),
+    ("host_stream_last_kib", [131072, 262144, 524288]),
 ]
 
 
