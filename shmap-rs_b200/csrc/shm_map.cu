@@ -4086,9 +4086,10 @@ static StreamSink* stream_sink(MapCtx* c, size_t piece_words, int ring) {
 // each next twice the one before (at most max_reads reads and max_bases
 // bases), and once the rest fits two of the current size, halves of the rest
 // down to last_bases: the device starts early, maps most of the stream in
-// large batches and ends soon after the packing does. (A batch has a fixed
-// device cost, about 0.7 ms on the hifi workload, so batches below a few
-// hundred MB would map slower than the host packs the next one.)
+// large batches and ends soon after the packing does; a rest below
+// last_bases joins the batch before it. (A batch has a fixed device cost,
+// about 0.7 ms on the hifi workload, so batches below a few hundred MB would
+// map slower than the host packs the next one.)
 static std::vector<std::pair<int32_t, int32_t>> cut_stream_batches(const int64_t* offs, int32_t r0, int32_t r1,
                                                                    int64_t first_bases, int64_t last_bases,
                                                                    int64_t max_bases, int32_t max_reads) {
@@ -4096,7 +4097,8 @@ static std::vector<std::pair<int32_t, int32_t>> cut_stream_batches(const int64_t
     int64_t tgt = std::max<int64_t>(1, first_bases);
     for (int32_t i = r0; i < r1;) {
         const int64_t rest = offs[r1] - offs[i];
-        const int64_t lim = rest <= 2 * tgt ? std::max(rest / 2, last_bases) : tgt;
+        int64_t lim = rest <= 2 * tgt ? std::max(rest / 2, last_bases) : tgt;
+        if (rest - lim < last_bases) lim = rest;  // no last batch smaller than last_bases (its fixed cost)
         int32_t j = i + 1;
         while (j < r1 && j - i < max_reads && offs[j + 1] - offs[i] <= lim) j++;
         b.emplace_back(i, j);
