@@ -3992,7 +3992,11 @@ struct StreamSink final : PackSink {
     size_t piece_words = 0;
     uint32_t* pinned = nullptr;
     std::vector<Worker> w;
-    uint32_t* dst = nullptr;  // the device codes of the stream in flight
+    uint32_t* dst = nullptr;       // the device codes of the stream in flight
+    uint32_t* mask_dst = nullptr;  // its device mask (raw pieces write their words there)
+    uint8_t* d_raw = nullptr;      // raw pieces: ring * piece bytes a thread, device memory
+    bool raw_ok = false;           // raw pieces taken in this stream
+    cudaEvent_t zeroed = nullptr;  // the stream's device mask is cleared
     std::atomic<int64_t> bytes{0};
     std::atomic<bool> failed{false};
     cudaError_t err = cudaSuccess;
@@ -4027,6 +4031,25 @@ struct StreamSink final : PackSink {
         x.next++;
         bytes += (int64_t)(4 * words);
     }
+    // A raw piece: its bytes copied into the thread's device slot, packed
+    // there into the stream's codes and mask words (the same layout).
+    bool piece_raw(int wi, const uint8_t* src, size_t g0, size_t ng) override {
+        if (!raw_ok || !d_raw || failed.load() || wi < 0 || wi >= (int)w.size() || ng == 0 ||
+            32 * ng > 16 * piece_words)
+            return false;
+        Worker& x = w[(size_t)wi];
+        const uint32_t sl = x.next % ring;
+        uint8_t* d = d_raw + ((size_t)wi * (size_t)ring + sl) * 16 * piece_words;
+        cudaError_t e = cudaSetDevice(device);
+        if (e == cudaSuccess) e = cudaEventSynchronize(x.ev[sl]);  // the slot's last use is done
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d, src, 32 * ng, cudaMemcpyHostToDevice, x.st);
+        if (e == cudaSuccess) e = pack_groups_device(d, (int64_t)ng, dst + 2 * g0, mask_dst + g0, x.st);
+        if (e == cudaSuccess) e = cudaEventRecord(x.ev[sl], x.st);
+        if (e != cudaSuccess) fail(e);  // the call fails at check(); the piece counts as taken
+        x.next++;
+        bytes += (int64_t)(32 * ng);
+        return true;
+    }
     void check() {
         if (failed.load()) throw shm_cuda_error(err);
     }
@@ -4051,17 +4074,22 @@ struct StreamSink final : PackSink {
             if (x.mark) cudaEventDestroy(x.mark);
             if (x.st) cudaStreamDestroy(x.st);
         }
+        if (zeroed) cudaEventDestroy(zeroed);
         if (pinned) cudaFreeHost(pinned);
+        if (d_raw) cudaFree(d_raw);
     }
 };
 
 // The context's stream sink for pieces of piece_words code words and `ring`
 // buffers a packing thread (made again when the settings changed).
-static StreamSink* stream_sink(MapCtx* c, size_t piece_words, int ring) {
+static StreamSink* stream_sink(MapCtx* c, size_t piece_words, int ring, bool raw) {
     const int nw = pack_workers();
     if (c->sink && c->sink->piece_words == piece_words && c->sink->ring == ring && (int)c->sink->w.size() == nw &&
-        !c->sink->failed.load())
+        !c->sink->failed.load()) {
+        if (raw && !c->sink->d_raw)
+            SHM_CUDA(cudaMalloc((void**)&c->sink->d_raw, 16 * piece_words * (size_t)ring * (size_t)nw));
         return c->sink;
+    }
     delete c->sink;
     c->sink = nullptr;
     auto* u = new StreamSink();
@@ -4070,6 +4098,8 @@ static StreamSink* stream_sink(MapCtx* c, size_t piece_words, int ring) {
     u->piece_words = piece_words;
     c->sink = u;  // released with the context even if a step below fails
     SHM_CUDA(cudaHostAlloc((void**)&u->pinned, 4 * piece_words * (size_t)ring * (size_t)nw, cudaHostAllocDefault));
+    if (raw) SHM_CUDA(cudaMalloc((void**)&u->d_raw, 16 * piece_words * (size_t)ring * (size_t)nw));
+    SHM_CUDA(cudaEventCreateWithFlags(&u->zeroed, cudaEventDisableTiming));
     u->w.resize((size_t)nw);
     for (int i = 0; i < nw; i++) {
         StreamSink::Worker& x = u->w[(size_t)i];
@@ -4170,8 +4200,23 @@ static bool map_host_stream(MapCtx* c, const IndexStorage* ix, const shm_params&
     S.pk_mask[0].reserve(mwords);
     S.pk_list[0].reserve(2 * list_cap * LIST_SLOTS);
     S.out.reserve((size_t)max_n);
-    StreamSink* sink_up = by_piece ? stream_sink(c, 2 * (size_t)task_groups, (int)tu.host_stream_ring) : nullptr;
-    if (sink_up) sink_up->dst = S.pk_codes[0].p;
+    // a share of the pieces (host_stream_raw_share percent) goes up as bytes
+    // from the caller's buffer, when that is pinned, and is packed on the device
+    int raw_pct = by_piece ? (int)tu.host_stream_raw_share : 0;
+    if (raw_pct > 0) {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, seqs) != cudaSuccess || pa.type != cudaMemoryTypeHost) {
+            cudaGetLastError();
+            raw_pct = 0;
+        }
+    }
+    StreamSink* sink_up =
+        by_piece ? stream_sink(c, 2 * (size_t)task_groups, (int)tu.host_stream_ring, raw_pct > 0) : nullptr;
+    if (sink_up) {
+        sink_up->dst = S.pk_codes[0].p;
+        sink_up->mask_dst = S.pk_mask[0].p;
+        sink_up->raw_ok = raw_pct > 0;
+    }
     std::vector<BatchSlot> slots = batch_slots(c, batches, offs);
     const std::vector<uint8_t*> plans = plan_blocks(c, batches);
     StageTimer T(c);
@@ -4206,9 +4251,14 @@ static bool map_host_stream(MapCtx* c, const IndexStorage* ix, const shm_params&
         if (pi > 0) SHM_CUDA(cudaStreamSynchronize(cs));
         SHM_CUDA(cudaStreamWaitEvent(cs, c->sketched[0], 0));
         SHM_CUDA(cudaMemsetAsync(S.pk_mask[0].p, 0, 4 * packed_mask_words(nb), cs));
-        if (sink_up) sink_up->gate(c->sketched[0]);
+        if (sink_up) {  // the threads' copies go after the last sketch of the buffers and the mask's clearing
+            SHM_CUDA(cudaEventRecord(sink_up->zeroed, cs));
+            sink_up->gate(c->sketched[0]);
+            sink_up->gate(sink_up->zeroed);
+        }
         stream_end.on = true;
-        const int chunks = pack_stream_start(seqs + offs[r0], nb, h_codes, task_groups, chunk_tasks, sink_up);
+        const int chunks =
+            pack_stream_start(seqs + offs[r0], nb, h_codes, task_groups, chunk_tasks, sink_up, raw_pct);
         while (c->up_ev.size() < (size_t)chunks) {
             cudaEvent_t e;
             SHM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));

@@ -102,6 +102,16 @@ void pack_reads_device(const uint8_t* seq, int64_t nb, uint32_t* codes, uint32_t
     count_launch();
 }
 
+cudaError_t pack_groups_device(const uint8_t* seq, int64_t n_groups, uint32_t* codes, uint32_t* mask,
+                               cudaStream_t s) {
+    if (n_groups <= 0) return cudaSuccess;
+    if (((uintptr_t)seq & 15u) != 0) return cudaErrorInvalidValue;
+    k_pack_ascii<0><<<grid_for((size_t)n_groups, 256, 8), 256, 0, s>>>(seq, 32 * n_groups, n_groups, codes, mask);
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) count_launch();
+    return e;
+}
+
 }  // namespace shm
 
 // Test hook (not part of the C ABI of include/shmap_gpu.h): nb bytes of host

@@ -334,7 +334,7 @@ static std::function<void(int)> pack_tasks(const uint8_t* seq, int64_t nb, uint3
 // piece is still in that core's cache when the sink sends it on) and handed
 // back with its place among the stream's code words.
 static std::function<void(int)> pack_tasks_sink(const uint8_t* seq, int64_t nb, PackSink* sink, int64_t per,
-                                                int& tasks) {
+                                                int& tasks, int raw_pct) {
     const int64_t n32 = nb / 32;
     per = std::max<int64_t>(2, per & ~1LL);
     tasks = (int)((n32 + per - 1) / per);
@@ -346,6 +346,9 @@ static std::function<void(int)> pack_tasks_sink(const uint8_t* seq, int64_t nb, 
     return [=](int t) {
         const int64_t g0 = per * t, g1 = std::min(n32, g0 + per);
         const int w = t_worker;
+        if (raw_pct > 0 && (int64_t)(t + 1) * raw_pct / 100 > (int64_t)t * raw_pct / 100 &&
+            sink->piece_raw(w, seq + 32 * g0, (size_t)g0, (size_t)(g1 - g0)))
+            return;
         uint32_t* buf = sink->piece_buffer(w);
         if (!buf) return;  // the sink failed; it reports that itself
         if (avx512) {
@@ -403,14 +406,14 @@ void pack_reads_host_start(const uint8_t* seq, int64_t nb, uint32_t* codes, int6
 }
 
 int pack_stream_start(const uint8_t* seq, int64_t nb, uint32_t* codes, int64_t task_groups, int chunk_tasks,
-                      PackSink* sink) {
+                      PackSink* sink, int raw_pct) {
     if (!t_pack_held) {
         g_pack_mu.lock();
         t_pack_held = true;
     }
     pool().finish();
     int tasks = 0;
-    std::function<void(int)> f = sink ? pack_tasks_sink(seq, nb, sink, std::max<int64_t>(2, task_groups), tasks)
+    std::function<void(int)> f = sink ? pack_tasks_sink(seq, nb, sink, std::max<int64_t>(2, task_groups), tasks, raw_pct)
                                       : pack_tasks<true>(seq, nb, codes, nullptr, tasks, std::max<int64_t>(2, task_groups));
     Stream& S = g_stream;
     S.tasks = tasks;

@@ -28,6 +28,10 @@ size_t pack_reads_host_wait(uint32_t* pairs, size_t cap);
 struct PackSink {
     virtual uint32_t* piece_buffer(int worker) = 0;
     virtual void piece_done(int worker, uint32_t* buf, size_t first_word, size_t words) = 0;
+    // A task left to the sink as bytes (groups [first_group, first_group +
+    // groups) at src): true when the sink took it (no codes, no mask words
+    // from the host for those groups), false to have it packed here.
+    virtual bool piece_raw(int worker, const uint8_t* src, size_t first_group, size_t groups) { return false; }
     virtual ~PackSink() = default;
 };
 // The number of packing threads (the pool's and the one holding the packing).
@@ -46,8 +50,10 @@ int pack_workers();
 // packing (on every path: it also releases the packing lock).
 // With a sink, each task's code words go to the sink instead, and codes
 // receives only the six tail words (groups nb / 32 .. nb / 32 + 2).
+// raw_pct percent of the tasks (spread evenly) are offered to the sink as
+// bytes first (PackSink::piece_raw).
 int pack_stream_start(const uint8_t* seq, int64_t nb, uint32_t* codes, int64_t task_groups, int chunk_tasks,
-                      PackSink* sink = nullptr);
+                      PackSink* sink = nullptr, int raw_pct = 0);
 bool pack_stream_chunk_ready(int c);
 bool pack_stream_help();
 size_t pack_stream_chunk_list(int c, uint32_t* pairs, size_t cap);

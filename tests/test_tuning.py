@@ -14,7 +14,7 @@ KEYS = ["dev_batch_reads", "dev_batch_bases", "dev_first_batch_reads", "host_bat
         "host_first_batch_reads", "sketch_ctas_per_sm", "wide_ctas_per_sm", "refine_warps_per_sm", "device_pack",
         "host_raw_share", "bt_fast_slots", "host_pack_task_kib", "host_stream", "host_stream_bases",
         "host_stream_chunk_kib", "host_stream_first_kib", "host_stream_piece_kib", "host_stream_ring",
-        "host_stream_last_kib"]
+        "host_stream_last_kib", "host_stream_raw_share"]
 
 
 def _get(k):
@@ -110,14 +110,17 @@ def test_results_do_not_depend_on_the_settings(gpu_ctx, saved):
     # by the packing threads (64 KiB pieces, two buffers a thread; and the defaults); and the
     # batch-by-batch form
     assert L.shm_tuning_set(b"host_raw_share", 0) == 0
-    for stream, bases, chunk, first, task in ((1, 1 << 24, 256, 256, 64), (1, 1 << 32, 32768, 32768, 256),
-                                              (2, 1 << 24, 256, 256, 64), (2, 1 << 32, 32768, 32768, 2048),
-                                              (0, 1 << 32, 32768, 32768, 256)):
+    # (and with a third or all of the pieces sent up as bytes, packed on the device)
+    for stream, bases, chunk, first, task, raw in ((1, 1 << 24, 256, 256, 64, 0), (1, 1 << 32, 32768, 32768, 256, 0),
+                                                   (2, 1 << 24, 256, 256, 64, 0), (2, 1 << 32, 32768, 32768, 2048, 0),
+                                                   (2, 1 << 24, 256, 256, 64, 34), (2, 1 << 32, 32768, 32768, 64, 100),
+                                                   (0, 1 << 32, 32768, 32768, 256, 0)):
         for k, x in (("host_stream", stream), ("host_stream_bases", bases), ("host_stream_chunk_kib", chunk),
+                     ("host_stream_raw_share", raw),
                      ("host_stream_first_kib", first), ("host_stream_last_kib", first), ("host_pack_task_kib", task),
                      ("host_stream_piece_kib", task), ("host_stream_ring", 2 if task == 64 else 4)):
             assert L.shm_tuning_set(k.encode(), x) == 0
         out = np.zeros(len(names), sb.RECORD_DTYPE)
         sb._check(L.shm_map_batch(gpu_ctx.h, g.h, ctypes.byref(cp), pin.data_ptr(), offs64.ctypes.data, len(names),
                                   out.ctypes.data))
-        assert not record_mismatches(out, want), (stream, bases, chunk, first, task)
+        assert not record_mismatches(out, want), (stream, bases, chunk, first, task, raw)
