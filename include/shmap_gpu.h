@@ -264,7 +264,9 @@ int shm_sketch_device_noalloc(const uint8_t* d_seq, int64_t len, int32_t k, doub
  * host_stream_last_kib (the device batches of a stream grow from the first
  * size and shrink to the last), host_stream_piece_kib, host_stream_ring and
  * host_stream_raw_share (percent of the pieces sent up as bytes and packed on
- * the device). None of them
+ * the device) and plan_mapped (a batch's plan read by a kernel through its
+ * pinned block's device mapping instead of copied by the copy engine). None
+ * of them
  * changes a result. They are read once per process from the file named by
  * $SHMAP_TUNING, else tuning.conf in the directory above the library's
  * (key = value lines, '#' comments), else built-in defaults;

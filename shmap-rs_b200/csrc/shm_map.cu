@@ -3082,6 +3082,12 @@ static uint8_t* pinned_stage(MapCtx* c, size_t bytes) {
 // Written into pinned memory at h_plan (BatchPlan::layout(n) bytes). caps =
 // null: capacities from the estimate; else caps[i] k-mers for read i (the
 // counts a previous pass found).
+// words [0, n) of src (device-accessible, e.g. a mapped pinned block) to dst.
+__global__ void k_copy_words(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
 // roff starts at base0: the batch's first base in the buffer its sketch reads
 // (only differences of roff are read elsewhere).
 static void plan_batch(uint8_t* h_plan, const int64_t* h_offs, int32_t n, int32_t k, double h_frac,
@@ -3258,9 +3264,22 @@ static void run_batch(MapCtx* c, const IndexStorage* ix, const shm_params& p, co
         S.luts_k = p.k;
     }
     const uint64_t kcap = bp.kcap_off[(size_t)n], phtn = bp.pht_off[(size_t)n];
-    // the plan goes up in one copy from its own pinned block
-    S.plan.reserve(bp.bytes);
-    copy_async(c, S.plan.p, h_plan, bp.bytes, cudaMemcpyHostToDevice, s);
+    // the plan goes up in one copy from its own pinned block, by the copy
+    // engine, or (plan_mapped) by a kernel reading the block through its
+    // device mapping: then it does not queue behind the other host-to-device
+    // copies of the copy engine (the packing threads' pieces)
+    S.plan.reserve(bp.bytes + 64);
+    void* d_src = nullptr;
+    if (tuning().plan_mapped && cudaHostGetDevicePointer(&d_src, h_plan, 0) == cudaSuccess) {
+        const size_t words = (bp.bytes + 3) / 4;  // the block is padded to 64 bytes
+        k_copy_words<<<grid_for(words, 256, 4), 256, 0, s>>>((uint32_t*)S.plan.p, (const uint32_t*)d_src, words);
+        SHM_CUDA(cudaGetLastError());
+        count_launch();
+        c->work[W_H2D_BYTES] += (int64_t)bp.bytes;
+    } else {
+        cudaGetLastError();
+        copy_async(c, S.plan.p, h_plan, bp.bytes, cudaMemcpyHostToDevice, s);
+    }
     BatchPlan dp;
     dp.carve(S.plan.p, n);
     S.kcnt.reserve((size_t)n);

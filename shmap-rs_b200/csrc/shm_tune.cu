@@ -43,6 +43,7 @@ const Knob KNOBS[] = {
     {"host_stream_piece_kib", &Tuning::host_stream_piece_kib, 64, 1 << 16},
     {"host_stream_ring", &Tuning::host_stream_ring, 2, 16},
     {"host_stream_raw_share", &Tuning::host_stream_raw_share, 0, 100},
+    {"plan_mapped", &Tuning::plan_mapped, 0, 1},
     {"host_stream_bases", &Tuning::host_stream_bases, 1 << 24, (int64_t)1 << 36},
     {"host_stream_chunk_kib", &Tuning::host_stream_chunk_kib, 256, 1 << 20},
     {"host_stream_first_kib", &Tuning::host_stream_first_kib, 256, 1 << 22},

@@ -30,6 +30,8 @@ struct Tuning {
     int64_t host_stream_ring = 4;          // host_stream 2: piece buffers a packing thread cycles through
     int64_t host_stream_raw_share = 0;     // host_stream 2, reads in pinned memory: percent of the pieces
                                            // sent up as bytes and packed on the device
+    int64_t plan_mapped = 1;               // a batch's plan read by a kernel through its pinned block's
+                                           // device mapping (1) instead of copied by the copy engine (0)
     int64_t host_stream_bases = (int64_t)1 << 32;  // bases a packing stream covers at most (a longer
                                                    // call is streamed in parts)
     int64_t host_stream_chunk_kib = 32768;  // KiB of reads a chunk of the stream: sent up as soon as

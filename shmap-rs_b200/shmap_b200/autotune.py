@@ -51,6 +51,7 @@ HOST_KNOBS = [
     ("host_stream_ring", [2, 4]),
     ("host_stream_first_kib", [32768, 65536, 131072]),
     ("host_stream_last_kib", [131072, 262144, 524288]),
+    ("plan_mapped", [0, 1]),
 ]
 
 

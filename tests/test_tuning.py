@@ -14,7 +14,7 @@ KEYS = ["dev_batch_reads", "dev_batch_bases", "dev_first_batch_reads", "host_bat
         "host_first_batch_reads", "sketch_ctas_per_sm", "wide_ctas_per_sm", "refine_warps_per_sm", "device_pack",
         "host_raw_share", "bt_fast_slots", "host_pack_task_kib", "host_stream", "host_stream_bases",
         "host_stream_chunk_kib", "host_stream_first_kib", "host_stream_piece_kib", "host_stream_ring",
-        "host_stream_last_kib", "host_stream_raw_share"]
+        "host_stream_last_kib", "host_stream_raw_share", "plan_mapped"]
 
 
 def _get(k):
@@ -72,7 +72,7 @@ def test_results_do_not_depend_on_the_settings(gpu_ctx, saved):
     L = sb.lib()
     for k, v in [("dev_batch_reads", 1024), ("dev_first_batch_reads", 64), ("host_batch_reads", 1024),
                  ("host_first_batch_reads", 100), ("sketch_ctas_per_sm", 1), ("wide_ctas_per_sm", 1),
-                 ("refine_warps_per_sm", 8), ("device_pack", 1), ("bt_fast_slots", 16)]:
+                 ("refine_warps_per_sm", 8), ("device_pack", 1), ("bt_fast_slots", 16), ("plan_mapped", 1)]:
         assert L.shm_tuning_set(k.encode(), v) == 0
     got = g.map_reads(p, seq, offs)
     assert not record_mismatches(got, want)
