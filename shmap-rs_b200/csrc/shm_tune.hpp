@@ -34,9 +34,9 @@ struct Tuning {
                                            // device mapping (1) instead of copied by the copy engine (0)
     int64_t host_stream_bases = (int64_t)1 << 32;  // bases a packing stream covers at most (a longer
                                                    // call is streamed in parts)
-    int64_t host_stream_chunk_kib = 32768;  // KiB of reads a chunk of the stream: sent up as soon as
+    int64_t host_stream_chunk_kib = 16384;  // KiB of reads a chunk of the stream: sent up as soon as
                                             // all its tasks are packed
-    int64_t host_stream_first_kib = 65536;  // KiB of reads the first device batch of a stream maps;
+    int64_t host_stream_first_kib = 32768;  // KiB of reads the first device batch of a stream maps;
                                             // the batches double from there and halve at the end
     int64_t host_stream_last_kib = 262144;  // ... down to about this many KiB
 };
