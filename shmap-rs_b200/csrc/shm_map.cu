@@ -2967,6 +2967,8 @@ struct MapScratch {
     uint32_t wtab_n = 0;
 };
 
+static void free_stream_sink(StreamSink* u);  // (defined with StreamSink below)
+
 MapCtx* mapctx_create(int device, size_t hbm_budget) {
     SHM_CUDA(cudaSetDevice(device));
     auto* c = new MapCtx();
@@ -3013,7 +3015,7 @@ void mapctx_destroy(MapCtx* c) {
     for (auto& e : c->raw_sketched)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->up_ev) cudaEventDestroy(e);
-    delete c->sink;
+    free_stream_sink(c->sink);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
         cudaStreamDestroy(c->side_stream);
@@ -4098,6 +4100,8 @@ struct StreamSink final : PackSink {
         if (d_raw) cudaFree(d_raw);
     }
 };
+
+static void free_stream_sink(StreamSink* u) { delete u; }
 
 // The context's stream sink for pieces of piece_words code words and `ring`
 // buffers a packing thread (made again when the settings changed).
