@@ -4619,3 +4619,18 @@ bool map_host(MapCtx* c, const IndexStorage* ix, const shm_params& p, const uint
 }
 
 }  // namespace shm
+
+// Test hook (not part of the C ABI of include/shmap_gpu.h): the device batches
+// cut_stream_batches makes of reads [0, n) with offsets offs[0..n]; writes up
+// to cap (first, end) read-index pairs to out and returns their number.
+extern "C" int shm_internal_cut_stream(const int64_t* offs, int32_t n, int64_t first_bases, int64_t last_bases,
+                                       int64_t max_bases, int32_t max_reads, int32_t* out, int32_t cap) {
+    if (n < 0 || (n > 0 && !offs) || first_bases <= 0 || last_bases <= 0 || max_bases <= 0 || max_reads <= 0)
+        return -1;
+    const auto b = shm::cut_stream_batches(offs, 0, n, first_bases, last_bases, max_bases, max_reads);
+    for (size_t i = 0; i < b.size() && (int32_t)i < cap; i++) {
+        out[2 * i] = b[i].first;
+        out[2 * i + 1] = b[i].second;
+    }
+    return (int)b.size();
+}
