@@ -1,8 +1,8 @@
 """The device batches of a host call's packing stream (cut_stream_batches in
 csrc/shm_map.cu): every read in exactly one batch, in order; no batch above
 the read or base limits (a single read may exceed the base limit alone); the
-first near first_bases, sizes doubling, the last no smaller than last_bases
-unless the whole call is."""
+first about first_bases, then sizes growing, then halving, the last taking
+what is left."""
 import ctypes
 
 import numpy as np
